@@ -1,0 +1,478 @@
+"""Seeded synthetic molecular systems and CHARMM file writers.
+
+The benchmark workloads of this package are synthetic: TIP3P water boxes and a
+solvated self-avoiding bead chain.  This module builds them as plain numpy
+arrays (a :class:`System`) and writes them as CHARMM PSF (XPLOR format), CARD
+coordinate and parameter files, which is the only input path the reference
+engine accepts (``CharmmPSF::readCharmmPSF`` src/CharmmPSF.cu:387,
+``CharmmParameters`` src/CharmmParameters.cu, ``CharmmCrd`` src/CharmmCrd.cu).
+
+Conventions follow the reference:
+  * the box is centred on the origin (image centering wraps a molecule when its
+    centroid leaves [-L/2, L/2), src/CharmmContext.cu:276-372);
+  * LJ well depths are written negative (CHARMM convention); the pair
+    parameters are eps_ij = sqrt(eps_i eps_j), rmin_ij = rmin/2_i + rmin/2_j
+    (src/CharmmParameters.cu:739-777);
+  * TIP3P atoms are typed OT/HT so that SETTLE and the degree-of-freedom count
+    engage (src/CharmmPSF.cu:281-296, src/ForceManager.cu:863).
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+import os
+from typing import Dict, List, Sequence, Tuple
+
+import numpy as np
+
+# TIP3P geometry and parameters (values as in the reference's
+# test/data/toppar_water_ions.str:240-242 and the TIP3P paper)
+R_OH = 0.9572
+THETA_HOH = 104.52
+Q_O, Q_H = -0.834, 0.417
+M_O, M_H = 15.9994, 1.008
+LJ_OT = (-0.1521, 1.7682)
+LJ_HT = (-0.046, 0.2245)
+
+
+@dataclasses.dataclass
+class System:
+    """One molecular system as flat arrays (0-based atom indices)."""
+
+    name: str
+    box: Tuple[float, float, float]
+    pos: np.ndarray                 # (N,3) float64, molecules whole
+    charge: np.ndarray              # (N,) float64
+    mass: np.ndarray                # (N,) float64
+    atom_type: List[str]            # CHARMM atom type per atom
+    atom_name: List[str]
+    res_name: List[str]
+    res_id: List[int]
+    seg_id: List[str]
+    bonds: np.ndarray               # (nb,2) int
+    angles: np.ndarray              # (na,3) int
+    dihedrals: np.ndarray           # (nd,4) int
+    impropers: np.ndarray           # (ni,4) int
+    # parameters keyed by CHARMM atom types
+    masses_by_type: Dict[str, float]
+    bond_params: Dict[Tuple[str, str], Tuple[float, float]]          # (kb, b0)
+    angle_params: Dict[Tuple[str, str, str], Tuple[float, float]]    # (ktheta, theta0 deg)
+    dihedral_params: Dict[Tuple[str, str, str, str], List[Tuple[float, int, float]]]  # [(kchi, n, delta deg)]
+    improper_params: Dict[Tuple[str, str, str, str], Tuple[float, float]]  # (kpsi, psi0 deg)
+    lj_params: Dict[str, Tuple[float, float]]                        # (eps<0, rmin/2)
+    lj14_params: Dict[str, Tuple[float, float]]
+    # PME / cutoff settings the workload is quoted with
+    settings: Dict[str, float] = dataclasses.field(default_factory=dict)
+
+    @property
+    def n_atoms(self) -> int:
+        return int(self.pos.shape[0])
+
+
+# --------------------------------------------------------------------------
+# geometry helpers
+# --------------------------------------------------------------------------
+
+def _random_rotations(rng: np.random.Generator, n: int) -> np.ndarray:
+    """Uniform random rotation matrices from unit quaternions (Shoemake)."""
+    u1, u2, u3 = rng.random(n), rng.random(n), rng.random(n)
+    q = np.stack([
+        np.sqrt(1 - u1) * np.sin(2 * np.pi * u2),
+        np.sqrt(1 - u1) * np.cos(2 * np.pi * u2),
+        np.sqrt(u1) * np.sin(2 * np.pi * u3),
+        np.sqrt(u1) * np.cos(2 * np.pi * u3),
+    ], axis=1)
+    x, y, z, w = q.T
+    R = np.empty((n, 3, 3))
+    R[:, 0, 0] = 1 - 2 * (y * y + z * z)
+    R[:, 0, 1] = 2 * (x * y - z * w)
+    R[:, 0, 2] = 2 * (x * z + y * w)
+    R[:, 1, 0] = 2 * (x * y + z * w)
+    R[:, 1, 1] = 1 - 2 * (x * x + z * z)
+    R[:, 1, 2] = 2 * (y * z - x * w)
+    R[:, 2, 0] = 2 * (x * z - y * w)
+    R[:, 2, 1] = 2 * (y * z + x * w)
+    R[:, 2, 2] = 1 - 2 * (x * x + y * y)
+    return R
+
+
+def _water_template() -> np.ndarray:
+    """O, H1, H2 in a frame with the centre of mass at the origin."""
+    half = math.radians(THETA_HOH) / 2
+    o = np.array([0.0, 0.0, 0.0])
+    h1 = np.array([R_OH * math.sin(half), 0.0, R_OH * math.cos(half)])
+    h2 = np.array([-R_OH * math.sin(half), 0.0, R_OH * math.cos(half)])
+    t = np.stack([o, h1, h2])
+    com = (M_O * o + M_H * h1 + M_H * h2) / (M_O + 2 * M_H)
+    return t - com
+
+
+def _lattice_sites(L: float, n_per_edge: int) -> np.ndarray:
+    g = (np.arange(n_per_edge) + 0.5) * (L / n_per_edge) - L / 2
+    X, Y, Z = np.meshgrid(g, g, g, indexing="ij")
+    return np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1)
+
+
+def _place_waters(rng, centres: np.ndarray, jitter: float, L: float) -> np.ndarray:
+    n = centres.shape[0]
+    c = centres + rng.normal(0.0, jitter, size=centres.shape)
+    R = _random_rotations(rng, n)
+    t = _water_template()
+    pos = c[:, None, :] + np.einsum("nij,aj->nai", R, t)
+    return pos.reshape(-1, 3)
+
+
+# --------------------------------------------------------------------------
+# systems
+# --------------------------------------------------------------------------
+
+def _water_topology(n_water: int, first_atom: int = 0, seg: str = "WAT",
+                    first_res: int = 1):
+    idx = first_atom + 3 * np.arange(n_water)
+    bonds = np.concatenate([
+        np.stack([idx, idx + 1], 1), np.stack([idx, idx + 2], 1),
+        np.stack([idx + 1, idx + 2], 1)])
+    # keep the reference's per-molecule order O-H1, O-H2, H1-H2
+    bonds = bonds.reshape(3, n_water, 2).transpose(1, 0, 2).reshape(-1, 2)
+    angles = np.stack([idx + 1, idx, idx + 2], 1)
+    types, names, resn, resi, segs = [], [], [], [], []
+    for m in range(n_water):
+        types += ["OT", "HT", "HT"]
+        names += ["OH2", "H1", "H2"]
+        resn += ["TIP3"] * 3
+        resi += [first_res + m] * 3
+        segs += [seg] * 3
+    return bonds, angles, types, names, resn, resi, segs
+
+
+def _water_params():
+    return dict(
+        masses_by_type={"OT": M_O, "HT": M_H},
+        bond_params={("HT", "HT"): (0.0, 1.5139), ("HT", "OT"): (450.0, R_OH)},
+        angle_params={("HT", "OT", "HT"): (55.0, THETA_HOH)},
+        lj={"OT": LJ_OT, "HT": LJ_HT},
+    )
+
+
+def water_box(n_molecules: int, L: float, seed: int = 2024,
+              jitter: float = 0.3, name: str = "waterbox") -> System:
+    """Cubic TIP3P box: molecules on a jittered lattice, random orientations."""
+    rng = np.random.default_rng(seed)
+    n_edge = int(math.ceil(n_molecules ** (1.0 / 3.0)))
+    sites = _lattice_sites(L, n_edge)
+    if sites.shape[0] > n_molecules:
+        keep = np.sort(rng.choice(sites.shape[0], n_molecules, replace=False))
+        sites = sites[keep]
+    pos = _place_waters(rng, sites, jitter, L)
+    bonds, angles, types, names, resn, resi, segs = _water_topology(n_molecules)
+    p = _water_params()
+    n = 3 * n_molecules
+    return System(
+        name=name, box=(L, L, L), pos=pos,
+        charge=np.tile([Q_O, Q_H, Q_H], n_molecules).astype(np.float64),
+        mass=np.tile([M_O, M_H, M_H], n_molecules).astype(np.float64),
+        atom_type=types, atom_name=names, res_name=resn, res_id=resi, seg_id=segs,
+        bonds=bonds.astype(np.int64), angles=angles.astype(np.int64),
+        dihedrals=np.zeros((0, 4), np.int64), impropers=np.zeros((0, 4), np.int64),
+        masses_by_type=p["masses_by_type"], bond_params=p["bond_params"],
+        angle_params=p["angle_params"], dihedral_params={}, improper_params={},
+        lj_params=p["lj"], lj14_params={},
+    )
+
+
+def _self_avoiding_chain(rng, n_beads: int, L: float, bond: float = 1.53,
+                         theta0: float = 111.0, min_dist: float = 2.6,
+                         margin: float = 1.5) -> np.ndarray:
+    """Confined self-avoiding walk with fixed bond length and angle.
+
+    Beads stay inside [-L/2+margin, L/2-margin]^3 so the molecule never crosses
+    the periodic boundary; non-neighbour beads (|i-j|>3) keep min_dist apart.
+    """
+    half = L / 2 - margin
+    cell = min_dist
+    ncell = max(1, int(L // cell))
+    grid: Dict[Tuple[int, int, int], List[int]] = {}
+
+    def key(p):
+        return tuple(((p + L / 2) // cell).astype(int) % ncell)
+
+    def clash(p, upto):
+        k = key(p)
+        for dx in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dz in (-1, 0, 1):
+                    kk = ((k[0] + dx) % ncell, (k[1] + dy) % ncell, (k[2] + dz) % ncell)
+                    for j in grid.get(kk, ()):
+                        if j < upto - 3 and np.sum((pos[j] - p) ** 2) < min_dist ** 2:
+                            return True
+        return False
+
+    pos = np.zeros((n_beads, 3))
+    pos[0] = rng.uniform(-half / 2, half / 2, 3)
+    d = rng.normal(size=3)
+    pos[1] = pos[0] + bond * d / np.linalg.norm(d)
+    for b in (0, 1):
+        grid.setdefault(key(pos[b]), []).append(b)
+    ct = math.cos(math.radians(180.0 - theta0))
+    st = math.sin(math.radians(180.0 - theta0))
+    i = 2
+    fails = 0
+    while i < n_beads:
+        u = pos[i - 1] - pos[i - 2]
+        u /= np.linalg.norm(u)
+        a = np.cross(u, [1.0, 0.0, 0.0])
+        if np.linalg.norm(a) < 1e-3:
+            a = np.cross(u, [0.0, 1.0, 0.0])
+        a /= np.linalg.norm(a)
+        b2 = np.cross(u, a)
+        ok = False
+        for _ in range(40):
+            phi = rng.uniform(0, 2 * np.pi)
+            d = ct * u + st * (math.cos(phi) * a + math.sin(phi) * b2)
+            p = pos[i - 1] + bond * d
+            if np.all(np.abs(p) < half) and not clash(p, i):
+                ok = True
+                break
+        if ok:
+            pos[i] = p
+            grid.setdefault(key(p), []).append(i)
+            i += 1
+            fails = 0
+        else:
+            # back-track a few beads
+            fails += 1
+            nb = min(i - 2, 2 + fails)
+            for j in range(i - nb, i):
+                grid[key(pos[j])].remove(j)
+            i -= nb
+    return pos
+
+
+def solvated_chain(n_atoms: int = 23558, L: float = 62.23, n_beads: int = 2489,
+                   seed: int = 1234, n_types: int = 8, name: str = "chain") -> System:
+    """Seeded bead chain (bonds, angles, n=3 dihedrals, 1-4 scaled LJ) in TIP3P."""
+    rng = np.random.default_rng(seed)
+    n_water = (n_atoms - n_beads) // 3
+    if n_beads + 3 * n_water != n_atoms:
+        raise ValueError("n_atoms - n_beads must be a multiple of 3")
+    chain = _self_avoiding_chain(rng, n_beads, L)
+    # LJ types: eps in [0.05, 0.2], rmin/2 in [1.3, 2.1]; 1-4 values scaled
+    types = [f"CB{k + 1}" for k in range(n_types)]
+    eps = np.linspace(0.05, 0.2, n_types)
+    rmh = np.linspace(1.3, 2.1, n_types)
+    perm = rng.permutation(n_types)
+    lj = {types[k]: (-float(eps[perm[k]]), float(rmh[k])) for k in range(n_types)}
+    lj14 = {t: (0.5 * lj[t][0], lj[t][1] - 0.1) for t in types}
+    bead_type = [types[k] for k in rng.integers(0, n_types, n_beads)]
+    q = rng.uniform(-0.5, 0.5, n_beads)
+    q -= q.mean()
+    # waters: candidate lattice sites away from the chain
+    n_edge = int(math.ceil((n_water * 1.6) ** (1.0 / 3.0)))
+    sites = _lattice_sites(L, n_edge)
+    # distance to nearest bead (minimum image) via a coarse cell search
+    keep = np.ones(sites.shape[0], bool)
+    cell = 3.0
+    nc = int(L // cell)
+    bins: Dict[Tuple[int, int, int], List[int]] = {}
+    for j, p in enumerate(chain):
+        k = tuple(((p + L / 2) // (L / nc)).astype(int) % nc)
+        bins.setdefault(k, []).append(j)
+    for s_i, s in enumerate(sites):
+        k = ((s + L / 2) // (L / nc)).astype(int) % nc
+        near = False
+        for dx in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dz in (-1, 0, 1):
+                    kk = ((k[0] + dx) % nc, (k[1] + dy) % nc, (k[2] + dz) % nc)
+                    for j in bins.get(kk, ()):
+                        d = chain[j] - s
+                        d -= L * np.round(d / L)
+                        if d @ d < 3.0 ** 2:
+                            near = True
+                            break
+                    if near:
+                        break
+                if near:
+                    break
+        keep[s_i] = not near
+    sites = sites[keep]
+    if sites.shape[0] < n_water:
+        raise RuntimeError("not enough free lattice sites for the solvent")
+    sites = sites[np.sort(rng.choice(sites.shape[0], n_water, replace=False))]
+    wpos = _place_waters(rng, sites, 0.2, L)
+
+    wb, wa, wt, wn, wrn, wri, ws = _water_topology(n_water, first_atom=n_beads)
+    cb = np.stack([np.arange(n_beads - 1), np.arange(1, n_beads)], 1)
+    ca = np.stack([np.arange(n_beads - 2), np.arange(1, n_beads - 1), np.arange(2, n_beads)], 1)
+    cd = np.stack([np.arange(n_beads - 3), np.arange(1, n_beads - 2),
+                   np.arange(2, n_beads - 1), np.arange(3, n_beads)], 1)
+    wp = _water_params()
+    bond_params = dict(wp["bond_params"])
+    angle_params = dict(wp["angle_params"])
+    dihedral_params: Dict[Tuple[str, str, str, str], List[Tuple[float, int, float]]] = {}
+    for a in range(n_types):
+        for b in range(a, n_types):
+            bond_params[(types[a], types[b])] = (222.0, 1.53)
+            dihedral_params[("X", types[a], types[b], "X")] = [(0.2, 3, 0.0)]
+    for a in range(n_types):
+        for b in range(n_types):
+            for c in range(a, n_types):
+                angle_params[(types[a], types[b], types[c])] = (58.0, 111.0)
+    masses_by_type = dict(wp["masses_by_type"])
+    for t in types:
+        masses_by_type[t] = 12.011
+    lj_all = dict(wp["lj"])
+    lj_all.update(lj)
+    return System(
+        name=name, box=(L, L, L),
+        pos=np.concatenate([chain, wpos]),
+        charge=np.concatenate([q, np.tile([Q_O, Q_H, Q_H], n_water)]),
+        mass=np.concatenate([np.full(n_beads, 12.011), np.tile([M_O, M_H, M_H], n_water)]),
+        atom_type=bead_type + wt,
+        atom_name=["CB"] * n_beads + wn,
+        res_name=["BEAD"] * n_beads + wrn,
+        res_id=list(range(1, n_beads + 1)) + wri,
+        seg_id=["CHN"] * n_beads + ws,
+        bonds=np.concatenate([cb, wb]).astype(np.int64),
+        angles=np.concatenate([ca, wa]).astype(np.int64),
+        dihedrals=cd.astype(np.int64), impropers=np.zeros((0, 4), np.int64),
+        masses_by_type=masses_by_type, bond_params=bond_params,
+        angle_params=angle_params, dihedral_params=dihedral_params,
+        improper_params={}, lj_params=lj_all, lj14_params=lj14,
+    )
+
+
+# --------------------------------------------------------------------------
+# named workloads
+# --------------------------------------------------------------------------
+
+def config_small_water(seed: int = 2024) -> System:
+    """12,480-atom TIP3P box, 50 A edge; PME 48^3 order 4, roff 10, ron 8, list 12."""
+    s = water_box(4160, 50.0, seed=seed, name="water12k")
+    s.settings = dict(kappa=0.34, nfft=(48, 48, 48), order=4, ctofnb=10.0,
+                      ctonnb=8.0, cutnb=12.0, dt_ps=0.002)
+    return s
+
+
+def config_solvated_chain(seed: int = 1234) -> System:
+    """23,558-atom bead chain in TIP3P, 62.23 A; PME 64^3 order 6, roff 12, ron 10, list 14."""
+    s = solvated_chain(seed=seed, name="chain23k")
+    s.settings = dict(kappa=0.34, nfft=(64, 64, 64), order=6, ctofnb=12.0,
+                      ctonnb=10.0, cutnb=14.0, dt_ps=0.002)
+    return s
+
+
+def config_large_water(seed: int = 77) -> System:
+    """~1M-atom TIP3P box (333,333 molecules, ~215 A); PME 216^3 order 4."""
+    L = (999999 / 0.1003) ** (1.0 / 3.0)
+    s = water_box(333333, L, seed=seed, name="water1m")
+    s.settings = dict(kappa=0.34, nfft=(216, 216, 216), order=4, ctofnb=10.0,
+                      ctonnb=8.0, cutnb=11.5, dt_ps=0.002)
+    return s
+
+
+def fft_friendly(n: int) -> int:
+    """Smallest even m >= n whose prime factors are 2, 3, 5 and 7."""
+    m = max(2, n)
+    while True:
+        if m % 2 == 0:
+            k = m
+            for p in (2, 3, 5, 7):
+                while k % p == 0:
+                    k //= p
+            if k == 1:
+                return m
+        m += 1
+
+
+# --------------------------------------------------------------------------
+# CHARMM file writers
+# --------------------------------------------------------------------------
+
+def write_psf(sys: System, path: str) -> None:
+    n = sys.n_atoms
+    lines = ["PSF CMAP CHEQ XPLOR", "", "       2 !NTITLE",
+             f"* SYNTHETIC SYSTEM {sys.name}", "* GENERATED BY apocharmm_b200.systems", "",
+             f"{n:8d} !NATOM"]
+    for i in range(n):
+        lines.append(
+            f"{i + 1:8d} {sys.seg_id[i]:<4s} {sys.res_id[i]:<4d} {sys.res_name[i]:<4s} "
+            f"{sys.atom_name[i]:<4s} {sys.atom_type[i]:<4s} {sys.charge[i]:14.6f}"
+            f"{sys.mass[i]:14.4f}           0   0.00000     -0.301140E-02")
+    lines.append("")
+
+    def block(arr, per_line, title):
+        out = ["", f"{arr.shape[0]:8d} !{title}"]
+        flat = (arr + 1).reshape(-1)
+        w = arr.shape[1] if arr.ndim == 2 and arr.shape[0] else 1
+        per = per_line * w
+        for k in range(0, flat.size, per):
+            out.append("".join(f"{v:8d}" for v in flat[k:k + per]))
+        return out
+
+    lines += block(sys.bonds, 4, "NBOND: bonds")
+    lines += block(sys.angles, 3, "NTHETA: angles")
+    lines += block(sys.dihedrals, 2, "NPHI: dihedrals")
+    lines += block(sys.impropers, 2, "NIMPHI: impropers")
+    lines += ["", "       0 !NDON: donors", "", "", "       0 !NACC: acceptors", "", "",
+              "       0 !NNB", "", "", "       0       0 !NGRP NST2", "", "",
+              "       0       0 !NUMLP NUMLPH", "", "       0 !NCRTERM: cross-terms", ""]
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+
+
+def write_crd(sys: System, path: str, pos: np.ndarray | None = None) -> None:
+    pos = sys.pos if pos is None else pos
+    n = sys.n_atoms
+    ext = n >= 100000
+    lines = [f"* SYNTHETIC SYSTEM {sys.name}", "*"]
+    lines.append(f"{n:10d}  EXT" if ext else f"{n:5d}")
+    for i in range(n):
+        x, y, z = pos[i]
+        if ext:
+            lines.append(f"{i + 1:10d}{sys.res_id[i]:10d}  {sys.res_name[i]:<8s}  {sys.atom_name[i]:<8s}"
+                         f"{x:20.10f}{y:20.10f}{z:20.10f}  {sys.seg_id[i]:<8s}  {sys.res_id[i]:<8d}{0.0:20.10f}")
+        else:
+            lines.append(f"{i + 1:5d}{sys.res_id[i]:5d} {sys.res_name[i]:<4s} {sys.atom_name[i]:<4s}"
+                         f"{x:10.5f}{y:10.5f}{z:10.5f} {sys.seg_id[i]:<4s} {sys.res_id[i]:<4d}{0.0:10.5f}")
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+
+
+def write_prm(sys: System, path: str) -> None:
+    L = ["* PARAMETERS FOR SYNTHETIC SYSTEM", "*", "", "ATOMS"]
+    for t, m in sys.masses_by_type.items():
+        L.append(f"MASS  -1  {t:<6s} {m:10.5f}")
+    L += ["", "BONDS"]
+    for (a, b), (k, r0) in sys.bond_params.items():
+        L.append(f"{a:<6s} {b:<6s} {k:10.4f} {r0:10.5f}")
+    L += ["", "ANGLES"]
+    for (a, b, c), (k, t0) in sys.angle_params.items():
+        L.append(f"{a:<6s} {b:<6s} {c:<6s} {k:10.4f} {t0:10.4f}")
+    L += ["", "DIHEDRALS"]
+    for (a, b, c, d), terms in sys.dihedral_params.items():
+        for (k, n, dl) in terms:
+            L.append(f"{a:<6s} {b:<6s} {c:<6s} {d:<6s} {k:10.4f} {n:3d} {dl:10.4f}")
+    L += ["", "IMPROPER"]
+    for (a, b, c, d), (k, p0) in sys.improper_params.items():
+        L.append(f"{a:<6s} {b:<6s} {c:<6s} {d:<6s} {k:10.4f}   0 {p0:10.4f}")
+    L += ["", "NONBONDED nbxmod  5 atom cdiel fshift vatom vdistance vfswitch -",
+          "cutnb 14.0 ctofnb 12.0 ctonnb 10.0 eps 1.0 e14fac 1.0 wmin 1.5", ""]
+    for t, (e, rh) in sys.lj_params.items():
+        if t in sys.lj14_params:
+            e14, r14 = sys.lj14_params[t]
+            L.append(f"{t:<6s} 0.0 {e:10.6f} {rh:10.6f} 0.0 {e14:10.6f} {r14:10.6f}")
+        else:
+            L.append(f"{t:<6s} 0.0 {e:10.6f} {rh:10.6f}")
+    L += ["", "END", ""]
+    with open(path, "w") as f:
+        f.write("\n".join(L) + "\n")
+
+
+def write_charmm_files(sys: System, directory: str) -> Dict[str, str]:
+    os.makedirs(directory, exist_ok=True)
+    paths = {k: os.path.join(directory, f"{sys.name}.{k}") for k in ("psf", "crd", "prm")}
+    write_psf(sys, paths["psf"])
+    write_crd(sys, paths["crd"])
+    write_prm(sys, paths["prm"])
+    return paths
