@@ -1,0 +1,304 @@
+"""Python front-end over the C ABI, mirroring the reference's python/apocharmm
+package (same class and method names: CharmmPsf, CharmmCrd, CharmmParameters,
+ForceManager, CharmmContext, CudaNoseHooverIntegrator, ...), plus accessors
+for forces, energies, coordinates and velocities that the reference exposes
+only in C++.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Dict, Iterable, List, Sequence
+
+import numpy as np
+
+from ._lib import call, lib
+
+ENERGY_TERMS = ("bond", "angle", "ureyb", "dihe", "imdihe", "ewks", "ewse", "ewex", "elec", "vdw")
+
+_vp = ctypes.c_void_p
+_d = ctypes.c_double
+_i = ctypes.c_int
+_sz = ctypes.c_size_t
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _enc(path) -> bytes:
+    return os.fsencode(str(path))
+
+
+class _Handle:
+    _destroy = ""
+
+    def __init__(self):
+        self._h = _vp()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h and self._h.value:
+            getattr(lib(), self._destroy)(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class CharmmPsf(_Handle):
+    _destroy = "apo_charmm_psf_destroy"
+
+    def __init__(self, path):
+        super().__init__()
+        call("apo_charmm_psf_create", ctypes.byref(self._h), _enc(path))
+
+    def _count(self, what):
+        n = _sz()
+        call(f"apo_charmm_psf_get_num_{what}", ctypes.byref(n), self._h)
+        return n.value
+
+    def getNumAtoms(self): return self._count("atoms")
+    def getNumBonds(self): return self._count("bonds")
+    def getNumAngles(self): return self._count("angles")
+    def getNumDihedrals(self): return self._count("dihedrals")
+    def getNumImpropers(self): return self._count("impropers")
+    def getNumCrossTerms(self): return self._count("cross_terms")
+
+    def _names(self, fn):
+        n = self.getNumAtoms()
+        buf = ctypes.create_string_buffer(8 * n)
+        call(fn, buf, _sz(8 * n), self._h)
+        raw = buf.raw.decode()
+        return [raw[8 * i:8 * i + 8].strip() for i in range(n)]
+
+    def getSegmentIdentifiers(self): return self._names("apo_charmm_psf_get_segment_identifiers")
+    def getResidueNames(self): return self._names("apo_charmm_psf_get_residue_names")
+    def getAtomNames(self): return self._names("apo_charmm_psf_get_atom_names")
+    def getAtomTypes(self): return self._names("apo_charmm_psf_get_atom_types")
+
+    def getResidueIdentifiers(self):
+        n = self.getNumAtoms()
+        a = np.zeros(n, np.int32)
+        call("apo_charmm_psf_get_residue_identifiers", _ptr(a), _sz(n), self._h)
+        return a.tolist()
+
+    def getCharges(self):
+        n = self.getNumAtoms()
+        a = np.zeros(n)
+        call("apo_charmm_psf_get_charges", _ptr(a), _sz(n), self._h)
+        return a.tolist()
+
+    def getMasses(self):
+        n = self.getNumAtoms()
+        a = np.zeros(n)
+        call("apo_charmm_psf_get_masses", _ptr(a), _sz(n), self._h)
+        return a.tolist()
+
+    def getNetCharge(self):
+        v = _d()
+        call("apo_charmm_psf_get_net_charge", ctypes.byref(v), self._h)
+        return v.value
+
+    def getTotalMass(self):
+        v = _d()
+        call("apo_charmm_psf_get_total_mass", ctypes.byref(v), self._h)
+        return v.value
+
+    def getFileName(self):
+        buf = ctypes.create_string_buffer(4096)
+        call("apo_charmm_psf_get_file_name", buf, _sz(4096), self._h)
+        return buf.value.decode()
+
+
+class CharmmCrd(_Handle):
+    _destroy = "apo_charmm_crd_destroy"
+
+    def __init__(self, path):
+        super().__init__()
+        call("apo_charmm_crd_create", ctypes.byref(self._h), _enc(path))
+
+    def getNumAtoms(self):
+        n = _sz()
+        call("apo_charmm_crd_get_num_atoms", ctypes.byref(n), self._h)
+        return n.value
+
+    def getCoordinates(self):
+        n = self.getNumAtoms()
+        a = np.zeros(3 * n)
+        call("apo_charmm_crd_get_coordinates", _ptr(a), _sz(3 * n), self._h)
+        return a.reshape(n, 3).tolist()
+
+
+class CharmmParameters(_Handle):
+    _destroy = "apo_charmm_parameters_destroy"
+
+    def __init__(self, paths):
+        super().__init__()
+        if isinstance(paths, (str, bytes, os.PathLike)):
+            call("apo_charmm_parameters_create", ctypes.byref(self._h), _enc(paths))
+        else:
+            enc = [_enc(p) for p in paths]
+            arr = (ctypes.c_char_p * len(enc))(*enc)
+            call("apo_charmm_parameters_create_from_files", ctypes.byref(self._h), arr,
+                 _sz(len(enc)))
+
+
+class ForceManager(_Handle):
+    _destroy = "apo_force_manager_destroy"
+
+    def __init__(self, psf: CharmmPsf, parameters: CharmmParameters):
+        super().__init__()
+        self._psf, self._prm = psf, parameters  # keep the inputs alive
+        call("apo_force_manager_create", ctypes.byref(self._h), psf.handle, parameters.handle)
+
+    def setBoxDimensions(self, box: Sequence[float]):
+        call("apo_force_manager_set_box_dimensions", self._h, _d(box[0]), _d(box[1]), _d(box[2]))
+
+    def setKappa(self, v): call("apo_force_manager_set_kappa", self._h, _d(v))
+    def setCutoff(self, v): call("apo_force_manager_set_cutoff", self._h, _d(v))
+    def setCtonnb(self, v): call("apo_force_manager_set_ctonnb", self._h, _d(v))
+    def setCtofnb(self, v): call("apo_force_manager_set_ctofnb", self._h, _d(v))
+    def setPmeSplineOrder(self, v): call("apo_force_manager_set_spline_order", self._h, _i(v))
+    def setFFTGrid(self, nx, ny, nz): call("apo_force_manager_set_fft_grid", self._h, _i(nx), _i(ny), _i(nz))
+    def setPrecisionMode(self, on: bool): call("apo_force_manager_set_precision_mode", self._h, _i(int(on)))
+    def setTilesPerWork(self, t: int): call("apo_force_manager_set_tiles_per_work", self._h, _i(t))
+    def setComponentMask(self, m: int): call("apo_force_manager_set_component_mask", self._h, _i(m))
+
+    def getFFTGrid(self):
+        a = (ctypes.c_int * 3)()
+        call("apo_force_manager_get_fft_grid", a, self._h)
+        return list(a)
+
+
+class CharmmContext(_Handle):
+    _destroy = "apo_charmm_context_destroy"
+
+    def __init__(self, force_manager: ForceManager):
+        super().__init__()
+        self._fm = force_manager
+        call("apo_charmm_context_create", ctypes.byref(self._h), force_manager.handle)
+
+    def setCoordinates(self, crd):
+        if isinstance(crd, CharmmCrd):
+            call("apo_charmm_context_set_coordinates", self._h, crd.handle)
+        else:
+            a = np.ascontiguousarray(crd, np.float64).reshape(-1)
+            call("apo_charmm_context_set_coordinates_xyz", self._h, _ptr(a), _sz(a.size))
+
+    def setRandomSeedForVelocities(self, seed: int):
+        call("apo_charmm_context_set_random_seed_for_velocities", self._h, ctypes.c_uint64(seed))
+
+    def useHolonomicConstraints(self, flag: bool):
+        call("apo_charmm_context_use_holonomic_constraints", self._h, ctypes.c_bool(flag))
+
+    def assignVelocitiesAtTemperature(self, t: float):
+        call("apo_charmm_context_assign_velocities_at_temperature", self._h, _d(t))
+
+    def computeTemperature(self) -> float:
+        v = _d()
+        call("apo_charmm_context_compute_temperature", ctypes.byref(v), self._h)
+        return v.value
+
+    def getNumAtoms(self) -> int:
+        n = _sz()
+        call("apo_charmm_context_get_num_atoms", ctypes.byref(n), self._h)
+        return n.value
+
+    def getDegreesOfFreedom(self) -> int:
+        n = _i()
+        call("apo_charmm_context_get_degrees_of_freedom", ctypes.byref(n), self._h)
+        return n.value
+
+    def calculateForces(self, reset: bool = False, calcEnergy: bool = True, calcVirial: bool = False):
+        call("apo_charmm_context_calculate_forces", self._h, ctypes.c_bool(reset),
+             ctypes.c_bool(calcEnergy), ctypes.c_bool(calcVirial))
+
+    def calculatePotentialEnergy(self, reset: bool = False) -> float:
+        self.calculateForces(reset, True, False)
+        return self.getPotentialEnergy()
+
+    def getForces(self) -> np.ndarray:
+        """Total gradient dU/dx, (N,3), the reference's force-buffer sign."""
+        n = self.getNumAtoms()
+        a = np.zeros(3 * n)
+        call("apo_charmm_context_get_forces", _ptr(a), _sz(3 * n), self._h)
+        return a.reshape(n, 3)
+
+    def getEnergyComponents(self) -> Dict[str, float]:
+        a = np.zeros(len(ENERGY_TERMS))
+        call("apo_charmm_context_get_energy_components", _ptr(a), _sz(a.size), self._h)
+        return dict(zip(ENERGY_TERMS, a.tolist()))
+
+    def getPotentialEnergy(self) -> float:
+        v = _d()
+        call("apo_charmm_context_get_potential_energy", ctypes.byref(v), self._h)
+        return v.value
+
+    def getCoordinates(self) -> np.ndarray:
+        n = self.getNumAtoms()
+        a = np.zeros(3 * n)
+        call("apo_charmm_context_get_coordinates", _ptr(a), _sz(3 * n), self._h)
+        return a.reshape(n, 3)
+
+    def setVelocities(self, v):
+        a = np.ascontiguousarray(v, np.float64).reshape(-1)
+        call("apo_charmm_context_set_velocities", self._h, _ptr(a), _sz(a.size))
+
+    def getVelocities(self) -> np.ndarray:
+        n = self.getNumAtoms()
+        a = np.zeros(3 * n)
+        call("apo_charmm_context_get_velocities", _ptr(a), _sz(3 * n), self._h)
+        return a.reshape(n, 3)
+
+    def resetNeighborList(self):
+        call("apo_charmm_context_reset_neighbor_list", self._h)
+
+    def getNeighborPairs(self, radius: float) -> np.ndarray:
+        n = _sz()
+        call("apo_charmm_context_get_neighbor_pairs", None, _sz(0), ctypes.byref(n), _d(radius), self._h)
+        a = np.zeros(3 * max(1, n.value), np.int32)
+        call("apo_charmm_context_get_neighbor_pairs", _ptr(a), _sz(a.size), ctypes.byref(n),
+             _d(radius), self._h)
+        return a[:3 * n.value].reshape(-1, 3)
+
+    def getStream(self) -> int:
+        p = _vp()
+        call("apo_charmm_context_get_stream", ctypes.byref(p), self._h)
+        return p.value or 0
+
+
+def system_context(sys, workdir: str, precise: bool = False, settings=None):
+    """Writes `sys` (apocharmm_b200.systems.System) as CHARMM files, loads it
+    through the C ABI and returns (psf, prm, fm, ctx).  `settings` overrides
+    sys.settings (kappa, nfft, order, ctofnb, ctonnb, cutnb)."""
+    from .systems import write_charmm_files
+    st = dict(sys.settings)
+    st.update(settings or {})
+    paths = write_charmm_files(sys, workdir)
+    psf = CharmmPsf(paths["psf"])
+    prm = CharmmParameters(paths["prm"])
+    fm = ForceManager(psf, prm)
+    fm.setBoxDimensions(sys.box)
+    fm.setKappa(st["kappa"])
+    fm.setCutoff(st["cutnb"])
+    fm.setCtonnb(st["ctonnb"])
+    fm.setCtofnb(st["ctofnb"])
+    fm.setFFTGrid(*st["nfft"])
+    fm.setPmeSplineOrder(st["order"])
+    fm.setPrecisionMode(precise)
+    ctx = CharmmContext(fm)
+    ctx.setCoordinates(sys.pos)
+    return psf, prm, fm, ctx

@@ -1,0 +1,211 @@
+// Fused bonded / 1-4 / exclusion-correction kernel; see bonded.h.
+#include "bonded.h"
+
+#include <algorithm>
+
+#include "device_util.cuh"
+
+namespace apo {
+namespace {
+
+constexpr int kThreads = 256;
+enum Seg { kSBond = 0, kSUb, kSAngle, kSDihe, kSImp, kSIn14, kSEx14, kNumSeg };
+
+__device__ __forceinline__ void push(const BondedArgs &a, int atom, float gx, float gy,
+                                     float gz) {
+  const int s = a.glo2loc[atom];
+  add_fixed(a.force + s, to_fixed_force(gx));
+  add_fixed(a.force + a.stride + s, to_fixed_force(gy));
+  add_fixed(a.force + 2 * a.stride + s, to_fixed_force(gz));
+}
+
+// E = k (r - r0)^2, reference src/CudaBondedForce.cu:85-120
+__device__ float bond_term(const BondedArgs &a, int i, int j, float2 p) {
+  const float4 xi = a.xyzq[i], xj = a.xyzq[j];
+  const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+  const float r = sqrtf(dx * dx + dy * dy + dz * dz);
+  const float db = r - p.y;
+  const float f = 2.f * p.x * db / r;
+  push(a, i, f * dx, f * dy, f * dz);
+  push(a, j, -f * dx, -f * dy, -f * dz);
+  return p.x * db * db;
+}
+
+// E = k (theta - theta0)^2 with cos(theta) clamped to +-0.999
+// (src/CudaBondedForce.cu:223-300)
+__device__ float angle_term(const BondedArgs &a, int4 t, float2 p) {
+  const float4 xi = a.xyzq[t.x], xj = a.xyzq[t.y], xk = a.xyzq[t.z];
+  const float ax = xi.x - xj.x, ay = xi.y - xj.y, az = xi.z - xj.z;
+  const float bx = xk.x - xj.x, by = xk.y - xj.y, bz = xk.z - xj.z;
+  const float rai = rsqrtf(ax * ax + ay * ay + az * az);
+  const float rbi = rsqrtf(bx * bx + by * by + bz * bz);
+  const float uax = ax * rai, uay = ay * rai, uaz = az * rai;
+  const float ubx = bx * rbi, uby = by * rbi, ubz = bz * rbi;
+  float cst = uax * ubx + uay * uby + uaz * ubz;
+  cst = fminf(0.999f, fmaxf(-0.999f, cst));
+  const float th = acosf(cst);
+  const float da = th - p.y;
+  const float df = -2.f * p.x * da * rsqrtf(1.f - cst * cst);
+  const float gix = df * rai * (ubx - cst * uax), giy = df * rai * (uby - cst * uay),
+              giz = df * rai * (ubz - cst * uaz);
+  const float gkx = df * rbi * (uax - cst * ubx), gky = df * rbi * (uay - cst * uby),
+              gkz = df * rbi * (uaz - cst * ubz);
+  push(a, t.x, gix, giy, giz);
+  push(a, t.z, gkx, gky, gkz);
+  push(a, t.y, -gix - gkx, -giy - gky, -giz - gkz);
+  return p.x * da * da;
+}
+
+// proper (HARM = false: sum k (1 + cos(n phi - delta))) and improper
+// (HARM = true: k (phi - psi0)^2) dihedrals; gradient expressions of the
+// reference (src/CudaBondedForce.cu:517-640)
+template <bool HARM>
+__device__ float dihedral_term(const BondedArgs &a, int4 t, int2 terms, float2 hp) {
+  const float4 xi = a.xyzq[t.x], xj = a.xyzq[t.y], xk = a.xyzq[t.z], xl = a.xyzq[t.w];
+  const float fx = xi.x - xj.x, fy = xi.y - xj.y, fz = xi.z - xj.z;
+  const float gx = xj.x - xk.x, gy = xj.y - xk.y, gz = xj.z - xk.z;
+  const float hx = xl.x - xk.x, hy = xl.y - xk.y, hz = xl.z - xk.z;
+  const float ax = fy * gz - fz * gy, ay = fz * gx - fx * gz, az = fx * gy - fy * gx;
+  const float bx = hy * gz - hz * gy, by = hz * gx - hx * gz, bz = hx * gy - hy * gx;
+  const float ra2 = ax * ax + ay * ay + az * az, rb2 = bx * bx + by * by + bz * bz;
+  const float rg = sqrtf(gx * gx + gy * gy + gz * gz);
+  const float rgr = 1.f / rg, ra2r = 1.f / ra2, rb2r = 1.f / rb2;
+  const float rabr = sqrtf(ra2r * rb2r);
+  const float ct = (ax * bx + ay * by + az * bz) * rabr;
+  const float st = rg * rabr * (ax * hx + ay * hy + az * hz);
+  float e = 0.f, df = 0.f;
+  if (HARM) {
+    const float c0 = cosf(hp.y), s0 = sinf(hp.y);
+    const float ca = ct * c0 + st * s0, sa = st * c0 - ct * s0;
+    const float ap = atan2f(sa, ca);
+    e = hp.x * ap * ap;
+    df = 2.f * hp.x * ap;
+  } else {
+    for (int q = terms.x; q < terms.x + terms.y; ++q) {
+      const float4 c = a.dihe_coef[q];  // (k, n, cos delta, sin delta)
+      const int n = (int)c.y;
+      // cos(n phi), sin(n phi) by recursion
+      float cn = 1.f, sn = 0.f;
+      for (int m = 0; m < n; ++m) {
+        const float c2 = cn * ct - sn * st;
+        sn = cn * st + sn * ct;
+        cn = c2;
+      }
+      e += c.x * (1.f + cn * c.z + sn * c.w);
+      df += -c.x * (float)n * (sn * c.z - cn * c.w);
+    }
+  }
+  const float fg = fx * gx + fy * gy + fz * gz, hg = hx * gx + hy * gy + hz * gz;
+  const float ra2d = ra2r * df, rb2d = rb2r * df;
+  const float fga = fg * ra2d * rgr, hgb = hg * rb2d * rgr;
+  const float gaa = ra2d * rg, gbb = rb2d * rg;
+  const float dfx = -gaa * ax, dfy = -gaa * ay, dfz = -gaa * az;
+  const float dgx = fga * ax - hgb * bx, dgy = fga * ay - hgb * by, dgz = fga * az - hgb * bz;
+  const float dhx = gbb * bx, dhy = gbb * by, dhz = gbb * bz;
+  push(a, t.x, dfx, dfy, dfz);
+  push(a, t.y, dgx - dfx, dgy - dfy, dgz - dfz);
+  push(a, t.z, -dhx - dgx, -dhy - dgy, -dhz - dgz);
+  push(a, t.w, dhx, dhy, dhz);
+  return e;
+}
+
+// 1-4 inclusion (LJ14 with VFSW + qq erfc/r) or exclusion correction
+// (qq (erfc - 1)/r = -qq erf/r); src/CudaDirectForceKernels.cu:643-870
+template <bool INCL>
+__device__ void pair14_term(const BondedArgs &a, int2 p, float &e_el, float &e_vdw) {
+  const float4 xi = a.xyzq[p.x], xj = a.xyzq[p.y];
+  const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+  const float r2 = dx * dx + dy * dy + dz * dz;
+  const float rinv = rsqrtf(r2), r = r2 * rinv, rinv2 = rinv * rinv;
+  const float qq = (float)kCcelec * xi.w * xj.w;
+  const NbSetup &st = a.nb;
+  const float expv = __expf(-st.kappa2 * r2);
+  float fr;
+  if (INCL) {
+    const float ev = qq * erfcf(st.kappa * r) * rinv;
+    fr = -qq * st.two_kappa_sqrtpi * expv - ev;
+    e_el = ev;
+    const float2 cc = a.vdw14[a.vdwtype[p.x] * a.ntype + a.vdwtype[p.y]];
+    const float rinv3 = rinv * rinv2, rinv6 = rinv3 * rinv3;
+    const bool sw = r2 > st.ron2;
+    const float A6 = sw ? st.k6 : 1.f, B6 = sw ? st.roffinv3 : 0.f;
+    const float A12 = sw ? st.k12 : 1.f, B12 = sw ? st.roffinv6 : 0.f;
+    const float C6 = sw ? 0.f : st.dv6, C12 = sw ? 0.f : st.dv12;
+    const float t6 = rinv3 - B6, t12 = rinv6 - B12;
+    fr += cc.x * A6 * t6 * rinv3 - cc.y * A12 * t12 * rinv6;
+    e_vdw = (1.f / 12.f) * cc.y * (A12 * t12 * t12 + C12) - (1.f / 6.f) * cc.x * (A6 * t6 * t6 + C6);
+  } else {
+    const float ev = -qq * erff(st.kappa * r) * rinv;
+    fr = -qq * st.two_kappa_sqrtpi * expv - ev;
+    e_el = ev;
+    e_vdw = 0.f;
+  }
+  const float f = fr * rinv2;
+  push(a, p.x, f * dx, f * dy, f * dz);
+  push(a, p.y, -f * dx, -f * dy, -f * dz);
+}
+
+template <bool ENERGY>
+__global__ void __launch_bounds__(kThreads) bonded_kernel(BondedArgs a) {
+  __shared__ unsigned long long sh_e[kNumEnergyTerms];
+  if (ENERGY) {
+    if (threadIdx.x < kNumEnergyTerms) sh_e[threadIdx.x] = 0ull;
+    __syncthreads();
+  }
+  const int b1 = a.nbond, b2 = b1 + a.nub, b3 = b2 + a.nangle, b4 = b3 + a.ndihe,
+            b5 = b4 + a.nimp, b6 = b5 + a.nin14, b7 = b6 + a.nex14;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < b7; t += gridDim.x * blockDim.x) {
+    float e = 0.f, e2 = 0.f;
+    int slot = -1, slot2 = -1;
+    if (t < b1) {
+      e = bond_term(a, a.bond_ij[t].x, a.bond_ij[t].y, a.bond_p[t]);
+      slot = kEBond;
+    } else if (t < b2) {
+      const int k = t - b1;
+      e = bond_term(a, a.ub_ij[k].x, a.ub_ij[k].y, a.ub_p[k]);
+      slot = kEUreyb;
+    } else if (t < b3) {
+      const int k = t - b2;
+      e = angle_term(a, a.angle_ijk[k], a.angle_p[k]);
+      slot = kEAngle;
+    } else if (t < b4) {
+      const int k = t - b3;
+      e = dihedral_term<false>(a, a.dihe_ijkl[k], a.dihe_terms[k], make_float2(0.f, 0.f));
+      slot = kEDihe;
+    } else if (t < b5) {
+      const int k = t - b4;
+      e = dihedral_term<true>(a, a.imp_ijkl[k], make_int2(0, 0), a.imp_p[k]);
+      slot = kEImdihe;
+    } else if (t < b6) {
+      pair14_term<true>(a, a.in14[t - b5], e, e2);
+      slot = kEElec;
+      slot2 = kEVdw;
+    } else {
+      pair14_term<false>(a, a.ex14[t - b6], e, e2);
+      slot = kEEwex;
+    }
+    if (ENERGY) {
+      atomicAdd(&sh_e[slot], (unsigned long long)__double2ll_rn((double)e * kEnergyScale));
+      if (slot2 >= 0)
+        atomicAdd(&sh_e[slot2], (unsigned long long)__double2ll_rn((double)e2 * kEnergyScale));
+    }
+  }
+  if (ENERGY) {
+    __syncthreads();
+    if (threadIdx.x < kNumEnergyTerms && sh_e[threadIdx.x])
+      add_fixed(a.energy + threadIdx.x, (long long)sh_e[threadIdx.x]);
+  }
+}
+
+}  // namespace
+
+void launch_bonded(const BondedArgs &a, bool energy, cudaStream_t s) {
+  const long long total = (long long)a.nbond + a.nub + a.nangle + a.ndihe + a.nimp + a.nin14 + a.nex14;
+  if (total == 0) return;
+  int blocks = (int)std::min<long long>((total + kThreads - 1) / kThreads, 148 * 16);
+  if (energy) bonded_kernel<true><<<blocks, kThreads, 0, s>>>(a);
+  else bonded_kernel<false><<<blocks, kThreads, 0, s>>>(a);
+  APO_LAUNCH_CHECK();
+}
+
+}  // namespace apo

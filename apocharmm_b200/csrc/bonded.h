@@ -1,0 +1,38 @@
+// Bonded terms, 1-4 inclusions and 1-2/1-3 exclusion corrections in one
+// launch.
+//
+// Replaces CudaBondedForce::calc_force (src/CudaBondedForce.cu:1642-1808,
+// bond/UB :85-220, angle :223-345, dihedral :387-700) and
+// CudaPMEDirectForce::calc_14_force (src/CudaPMEDirectForce.cu:1072,
+// body include/CudaDirectForce14_util.h, pair code
+// src/CudaDirectForceKernels.cu:643-870).  One thread per term over the
+// concatenated term lists; every gradient contribution is rounded to 64-bit
+// fixed point and added with integer atomics (order independent).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "nonbonded.h"
+
+namespace apo {
+
+struct BondedArgs {
+  const float4 *xyzq;     // global atom order
+  const int *glo2loc;     // atom -> force slot
+  long long *force;
+  int stride;
+  long long *energy;
+  int nbond; const int2 *bond_ij; const float2 *bond_p;
+  int nub; const int2 *ub_ij; const float2 *ub_p;
+  int nangle; const int4 *angle_ijk; const float2 *angle_p;
+  int ndihe; const int4 *dihe_ijkl; const int2 *dihe_terms; const float4 *dihe_coef;
+  int nimp; const int4 *imp_ijkl; const float2 *imp_p;
+  int nin14; const int2 *in14;
+  int nex14; const int2 *ex14;
+  const int *vdwtype; const float2 *vdw14; int ntype;
+  NbSetup nb;             // kappa and the VFSW constants for the 1-4 LJ
+};
+
+void launch_bonded(const BondedArgs &a, bool energy, cudaStream_t s);
+
+}  // namespace apo

@@ -1,0 +1,543 @@
+// C ABI over the C++ classes: files, force manager, context.
+//
+// Same conventions as the reference's capi (capi/src/apocharmm_c/*.cpp):
+// opaque handles that own std::shared_ptr objects, `*_create(T **out, ...)`
+// sets *out = NULL before anything else, every call returns apo_status,
+// C++ exceptions become APO_STATUS_RUNTIME_ERROR with the message in a
+// thread-local string read by apo_last_error() (ErrorInternal.h:27-41).
+// CUDA failures are reported as APO_STATUS_CUDA_ERROR.
+#include "capi_internal.h"
+
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+namespace apocapi {
+void clear_error() noexcept { g_last_error.clear(); }
+apo_status set_error(apo_status s, const std::string &m) noexcept {
+  try {
+    g_last_error = m;
+  } catch (...) {
+  }
+  return s;
+}
+}  // namespace apocapi
+
+using namespace apocapi;
+
+extern "C" const char *apo_last_error(void) { return g_last_error.c_str(); }
+
+// ------------------------------------------------------------------ PSF ----
+
+extern "C" apo_status apo_charmm_psf_create(apo_charmm_psf **out, const char *path) {
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(prepare_out(out, "apo_charmm_psf_create"));
+    APO_RETURN_IF(require_string(path, "apo_charmm_psf_create", "path"));
+    auto h = std::make_unique<apo_charmm_psf>();
+    h->object = std::make_shared<apo::CharmmPSF>(path);
+    *out = h.release();
+    return APO_STATUS_OK;
+  }, "apo_charmm_psf_create");
+}
+
+extern "C" void apo_charmm_psf_destroy(apo_charmm_psf *psf) { delete psf; }
+
+#define PSF_COUNT(fname, getter)                                                   \
+  extern "C" apo_status fname(size_t *n, const apo_charmm_psf *psf) {              \
+    return guard([&]() -> apo_status {                                             \
+      APO_RETURN_IF(require_ptr(n, #fname, "output"));                             \
+      *n = 0;                                                                      \
+      APO_RETURN_IF(require_handle(psf, #fname, "CharmmPsf"));                     \
+      *n = (size_t)psf->object->getter();                                          \
+      return APO_STATUS_OK;                                                        \
+    }, #fname);                                                                    \
+  }
+PSF_COUNT(apo_charmm_psf_get_num_atoms, getNumAtoms)
+PSF_COUNT(apo_charmm_psf_get_num_bonds, getNumBonds)
+PSF_COUNT(apo_charmm_psf_get_num_angles, getNumAngles)
+PSF_COUNT(apo_charmm_psf_get_num_dihedrals, getNumDihedrals)
+PSF_COUNT(apo_charmm_psf_get_num_impropers, getNumImpropers)
+PSF_COUNT(apo_charmm_psf_get_num_cross_terms, getNumCrossTerms)
+
+static apo_status fill_names(char *buf, size_t len, const std::vector<std::string> &names,
+                             const char *fn) {
+  const size_t need = 8 * names.size();
+  APO_RETURN_IF(require_buffer(buf, len, need, fn, "name buffer"));
+  for (size_t i = 0; i < names.size(); ++i)
+    for (size_t j = 0; j < 8; ++j) buf[i * 8 + j] = j < names[i].size() ? names[i][j] : ' ';
+  return APO_STATUS_OK;
+}
+
+#define PSF_NAMES(fname, getter)                                                   \
+  extern "C" apo_status fname(char *buf, const size_t len, const apo_charmm_psf *psf) { \
+    return guard([&]() -> apo_status {                                             \
+      APO_RETURN_IF(require_handle(psf, #fname, "CharmmPsf"));                     \
+      return fill_names(buf, len, psf->object->getter(), #fname);                  \
+    }, #fname);                                                                    \
+  }
+PSF_NAMES(apo_charmm_psf_get_segment_identifiers, getSegmentIdentifiers)
+PSF_NAMES(apo_charmm_psf_get_residue_names, getResidueNames)
+PSF_NAMES(apo_charmm_psf_get_atom_names, getAtomNames)
+PSF_NAMES(apo_charmm_psf_get_atom_types, getAtomTypes)
+
+extern "C" apo_status apo_charmm_psf_get_residue_identifiers(int *resis, const size_t len,
+                                                             const apo_charmm_psf *psf) {
+  const char *fn = "apo_charmm_psf_get_residue_identifiers";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(psf, fn, "CharmmPsf"));
+    const auto &v = psf->object->getResidueIdentifiers();
+    APO_RETURN_IF(require_buffer(resis, len, v.size(), fn, "residue id buffer"));
+    std::copy(v.begin(), v.end(), resis);
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+#define PSF_DOUBLES(fname, getter)                                                 \
+  extern "C" apo_status fname(double *out, const size_t len, const apo_charmm_psf *psf) { \
+    return guard([&]() -> apo_status {                                             \
+      APO_RETURN_IF(require_handle(psf, #fname, "CharmmPsf"));                     \
+      const auto &v = psf->object->getter();                                       \
+      APO_RETURN_IF(require_buffer(out, len, v.size(), #fname, "output buffer"));  \
+      std::copy(v.begin(), v.end(), out);                                          \
+      return APO_STATUS_OK;                                                        \
+    }, #fname);                                                                    \
+  }
+PSF_DOUBLES(apo_charmm_psf_get_charges, getCharges)
+PSF_DOUBLES(apo_charmm_psf_get_masses, getMasses)
+
+#define PSF_SCALAR(fname, getter)                                                  \
+  extern "C" apo_status fname(double *out, const apo_charmm_psf *psf) {            \
+    return guard([&]() -> apo_status {                                             \
+      APO_RETURN_IF(require_ptr(out, #fname, "output"));                           \
+      *out = 0.0;                                                                  \
+      APO_RETURN_IF(require_handle(psf, #fname, "CharmmPsf"));                     \
+      *out = psf->object->getter();                                                \
+      return APO_STATUS_OK;                                                        \
+    }, #fname);                                                                    \
+  }
+PSF_SCALAR(apo_charmm_psf_get_net_charge, getNetCharge)
+PSF_SCALAR(apo_charmm_psf_get_total_mass, getTotalMass)
+
+extern "C" apo_status apo_charmm_psf_get_file_name(char *name, const size_t len,
+                                                   const apo_charmm_psf *psf) {
+  const char *fn = "apo_charmm_psf_get_file_name";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(psf, fn, "CharmmPsf"));
+    const std::string &f = psf->object->getFileName();
+    APO_RETURN_IF(require_buffer(name, len, f.size(), fn, "file name buffer"));
+    std::memcpy(name, f.data(), f.size());
+    if (len > f.size()) name[f.size()] = '\0';
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+// ------------------------------------------------------------------ CRD ----
+
+extern "C" apo_status apo_charmm_crd_create(apo_charmm_crd **out, const char *path) {
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(prepare_out(out, "apo_charmm_crd_create"));
+    APO_RETURN_IF(require_string(path, "apo_charmm_crd_create", "path"));
+    auto h = std::make_unique<apo_charmm_crd>();
+    h->object = std::make_shared<apo::CharmmCrd>(path);
+    *out = h.release();
+    return APO_STATUS_OK;
+  }, "apo_charmm_crd_create");
+}
+extern "C" void apo_charmm_crd_destroy(apo_charmm_crd *crd) { delete crd; }
+extern "C" apo_status apo_charmm_crd_get_num_atoms(size_t *n, const apo_charmm_crd *crd) {
+  const char *fn = "apo_charmm_crd_get_num_atoms";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_ptr(n, fn, "num_atoms"));
+    *n = 0;
+    APO_RETURN_IF(require_handle(crd, fn, "CharmmCrd"));
+    *n = (size_t)crd->object->getNumAtoms();
+    return APO_STATUS_OK;
+  }, fn);
+}
+extern "C" apo_status apo_charmm_crd_get_coordinates(double *xyz, const size_t len,
+                                                     const apo_charmm_crd *crd) {
+  const char *fn = "apo_charmm_crd_get_coordinates";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(crd, fn, "CharmmCrd"));
+    const auto &v = crd->object->getCoordinates();
+    APO_RETURN_IF(require_buffer(xyz, len, v.size(), fn, "coordinate buffer"));
+    std::copy(v.begin(), v.end(), xyz);
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+// ----------------------------------------------------------- parameters ----
+
+extern "C" apo_status apo_charmm_parameters_create(apo_charmm_parameters **out, const char *path) {
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(prepare_out(out, "apo_charmm_parameters_create"));
+    APO_RETURN_IF(require_string(path, "apo_charmm_parameters_create", "path"));
+    auto h = std::make_unique<apo_charmm_parameters>();
+    h->object = std::make_shared<apo::CharmmParameters>(std::string(path));
+    *out = h.release();
+    return APO_STATUS_OK;
+  }, "apo_charmm_parameters_create");
+}
+extern "C" apo_status apo_charmm_parameters_create_from_files(apo_charmm_parameters **out,
+                                                              const char *const *paths,
+                                                              const size_t num_paths) {
+  const char *fn = "apo_charmm_parameters_create_from_files";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(prepare_out(out, fn));
+    if (paths == nullptr || num_paths == 0) return invalid(fn, "paths is NULL or empty");
+    std::vector<std::string> v;
+    for (size_t i = 0; i < num_paths; ++i) {
+      APO_RETURN_IF(require_string(paths[i], fn, "paths[i]"));
+      v.emplace_back(paths[i]);
+    }
+    auto h = std::make_unique<apo_charmm_parameters>();
+    h->object = std::make_shared<apo::CharmmParameters>(v);
+    *out = h.release();
+    return APO_STATUS_OK;
+  }, fn);
+}
+extern "C" void apo_charmm_parameters_destroy(apo_charmm_parameters *p) { delete p; }
+
+// -------------------------------------------------------- force manager ----
+
+extern "C" apo_status apo_force_manager_create(apo_force_manager **out, const apo_charmm_psf *psf,
+                                               const apo_charmm_parameters *prm) {
+  const char *fn = "apo_force_manager_create";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(prepare_out(out, fn));
+    APO_RETURN_IF(require_handle(psf, fn, "CharmmPsf"));
+    APO_RETURN_IF(require_handle(prm, fn, "CharmmParameters"));
+    auto h = std::make_unique<apo_force_manager>();
+    h->object = std::make_shared<apo::ForceManager>(psf->object, prm->object);
+    *out = h.release();
+    return APO_STATUS_OK;
+  }, fn);
+}
+extern "C" void apo_force_manager_destroy(apo_force_manager *fm) { delete fm; }
+
+extern "C" apo_status apo_force_manager_set_box_dimensions(apo_force_manager *fm, const double x,
+                                                           const double y, const double z) {
+  const char *fn = "apo_force_manager_set_box_dimensions";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(fm, fn, "ForceManager"));
+    if (!(x > 0 && y > 0 && z > 0) || !std::isfinite(x) || !std::isfinite(y) || !std::isfinite(z))
+      return invalid(fn, "box dimensions must be positive and finite");
+    fm->object->setBoxDimensions({x, y, z});
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+#define FM_SETTER(fname, type, call, check)                                        \
+  extern "C" apo_status fname(apo_force_manager *fm, const type v) {               \
+    return guard([&]() -> apo_status {                                             \
+      APO_RETURN_IF(require_handle(fm, #fname, "ForceManager"));                   \
+      if (!(check)) return invalid(#fname, "value out of range");                  \
+      fm->object->call;                                                            \
+      return APO_STATUS_OK;                                                        \
+    }, #fname);                                                                    \
+  }
+FM_SETTER(apo_force_manager_set_kappa, double, setKappa(v), v > 0 && std::isfinite(v))
+FM_SETTER(apo_force_manager_set_cutoff, double, setCutoff(v), v > 0 && std::isfinite(v))
+FM_SETTER(apo_force_manager_set_ctonnb, double, setCtonnb(v), v > 0 && std::isfinite(v))
+FM_SETTER(apo_force_manager_set_ctofnb, double, setCtofnb(v), v > 0 && std::isfinite(v))
+FM_SETTER(apo_force_manager_set_spline_order, int, setPmeSplineOrder(v), v == 4 || v == 6 || v == 8)
+FM_SETTER(apo_force_manager_set_precision_mode, int, setPrecisionMode(v != 0), true)
+FM_SETTER(apo_force_manager_set_tiles_per_work, int, setTilesPerWork(v), v >= 1 && v <= 1024)
+FM_SETTER(apo_force_manager_set_component_mask, int, setComponentMask(v), v >= 0 && v <= 7)
+
+extern "C" apo_status apo_force_manager_set_fft_grid(apo_force_manager *fm, const int nx,
+                                                     const int ny, const int nz) {
+  const char *fn = "apo_force_manager_set_fft_grid";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(fm, fn, "ForceManager"));
+    if (nx <= 0 || ny <= 0 || nz <= 0) return invalid(fn, "grid dimensions must be positive");
+    fm->object->setFFTGrid(nx, ny, nz);
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_force_manager_get_fft_grid(int *n3, const apo_force_manager *fm) {
+  const char *fn = "apo_force_manager_get_fft_grid";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_ptr(n3, fn, "output"));
+    APO_RETURN_IF(require_handle(fm, fn, "ForceManager"));
+    auto g = fm->object->getFFTGrid();
+    n3[0] = g[0];
+    n3[1] = g[1];
+    n3[2] = g[2];
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+// -------------------------------------------------------------- context ----
+
+extern "C" apo_status apo_charmm_context_create(apo_charmm_context **out,
+                                                const apo_force_manager *fm) {
+  const char *fn = "apo_charmm_context_create";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(prepare_out(out, fn));
+    APO_RETURN_IF(require_handle(fm, fn, "ForceManager"));
+    auto h = std::make_unique<apo_charmm_context>();
+    h->force_manager = fm->object;
+    h->object = std::make_shared<apo::CharmmContext>(fm->object);
+    *out = h.release();
+    return APO_STATUS_OK;
+  }, fn);
+}
+extern "C" void apo_charmm_context_destroy(apo_charmm_context *c) { delete c; }
+
+extern "C" apo_status apo_charmm_context_set_coordinates(apo_charmm_context *c,
+                                                         const apo_charmm_crd *crd) {
+  const char *fn = "apo_charmm_context_set_coordinates";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
+    APO_RETURN_IF(require_handle(crd, fn, "CharmmCrd"));
+    if (crd->object->getNumAtoms() != c->object->getNumAtoms())
+      return invalid(fn, "coordinate count does not match the topology");
+    c->object->setCoordinates(*crd->object);
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_charmm_context_set_random_seed_for_velocities(apo_charmm_context *c,
+                                                                        const uint64_t seed) {
+  const char *fn = "apo_charmm_context_set_random_seed_for_velocities";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
+    c->object->setRandomSeedForVelocities(seed);
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_charmm_context_use_holonomic_constraints(apo_charmm_context *c,
+                                                                   const bool flag) {
+  const char *fn = "apo_charmm_context_use_holonomic_constraints";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
+    c->object->useHolonomicConstraints(flag);
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_charmm_context_assign_velocities_at_temperature(apo_charmm_context *c,
+                                                                          const double t) {
+  const char *fn = "apo_charmm_context_assign_velocities_at_temperature";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
+    if (!(t >= 0) || !std::isfinite(t)) return invalid(fn, "temperature must be >= 0");
+    c->object->assignVelocitiesAtTemperature(t);
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_charmm_context_compute_temperature(double *t, apo_charmm_context *c) {
+  const char *fn = "apo_charmm_context_compute_temperature";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_ptr(t, fn, "temperature"));
+    *t = 0.0;
+    APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
+    *t = c->object->computeTemperature();
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_charmm_context_calculate_forces(apo_charmm_context *c, const bool reset,
+                                                          const bool energy, const bool virial) {
+  const char *fn = "apo_charmm_context_calculate_forces";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
+    c->object->calculateForces(reset, energy, virial);
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_charmm_context_get_forces(double *xyz, const size_t len,
+                                                    apo_charmm_context *c) {
+  const char *fn = "apo_charmm_context_get_forces";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
+    const size_t need = 3 * (size_t)c->object->getNumAtoms();
+    APO_RETURN_IF(require_buffer(xyz, len, need, fn, "force buffer"));
+    std::vector<double> f;
+    c->object->getForceManager()->getForces(f, c->object->stream());
+    std::copy(f.begin(), f.end(), xyz);
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_charmm_context_get_energy_components(double *e, const size_t len,
+                                                               apo_charmm_context *c) {
+  const char *fn = "apo_charmm_context_get_energy_components";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
+    APO_RETURN_IF(require_buffer(e, len, (size_t)apo::kNumEnergyTerms, fn, "energy buffer"));
+    auto m = c->object->getForceManager()->getEnergyComponents(c->object->stream());
+    for (int k = 0; k < apo::kNumEnergyTerms; ++k) e[k] = m[apo::kEnergyNames[k]];
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_charmm_context_get_potential_energy(double *e, apo_charmm_context *c) {
+  const char *fn = "apo_charmm_context_get_potential_energy";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_ptr(e, fn, "energy"));
+    APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
+    *e = c->object->getForceManager()->getPotentialEnergy(c->object->stream());
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_charmm_context_set_coordinates_xyz(apo_charmm_context *c,
+                                                             const double *xyz, const size_t len) {
+  const char *fn = "apo_charmm_context_set_coordinates_xyz";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
+    APO_RETURN_IF(require_ptr(xyz, fn, "xyz"));
+    if (len != 3 * (size_t)c->object->getNumAtoms()) return invalid(fn, "len must be 3*N");
+    c->object->setCoordinates(std::vector<double>(xyz, xyz + len));
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_charmm_context_get_coordinates(double *xyz, const size_t len,
+                                                         apo_charmm_context *c) {
+  const char *fn = "apo_charmm_context_get_coordinates";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
+    APO_RETURN_IF(require_buffer(xyz, len, 3 * (size_t)c->object->getNumAtoms(), fn, "buffer"));
+    auto v = c->object->getCoordinates();
+    std::copy(v.begin(), v.end(), xyz);
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_charmm_context_set_velocities(apo_charmm_context *c, const double *v,
+                                                        const size_t len) {
+  const char *fn = "apo_charmm_context_set_velocities";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
+    APO_RETURN_IF(require_ptr(v, fn, "v"));
+    if (len != 3 * (size_t)c->object->getNumAtoms()) return invalid(fn, "len must be 3*N");
+    c->object->setVelocities(std::vector<double>(v, v + len));
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_charmm_context_get_velocities(double *v, const size_t len,
+                                                        apo_charmm_context *c) {
+  const char *fn = "apo_charmm_context_get_velocities";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
+    APO_RETURN_IF(require_buffer(v, len, 3 * (size_t)c->object->getNumAtoms(), fn, "buffer"));
+    auto w = c->object->getVelocities();
+    std::copy(w.begin(), w.end(), v);
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_charmm_context_get_num_atoms(size_t *n, const apo_charmm_context *c) {
+  const char *fn = "apo_charmm_context_get_num_atoms";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_ptr(n, fn, "num_atoms"));
+    APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
+    *n = (size_t)c->object->getNumAtoms();
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_charmm_context_get_degrees_of_freedom(int *n,
+                                                                const apo_charmm_context *c) {
+  const char *fn = "apo_charmm_context_get_degrees_of_freedom";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_ptr(n, fn, "ndegf"));
+    APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
+    *n = c->object->getDegreesOfFreedom();
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_charmm_context_reset_neighbor_list(apo_charmm_context *c) {
+  const char *fn = "apo_charmm_context_reset_neighbor_list";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
+    c->object->resetNeighborList(c->object->stream());
+    APO_CUDA(cudaStreamSynchronize(c->object->stream()));
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_charmm_context_get_stream(void **stream, const apo_charmm_context *c) {
+  const char *fn = "apo_charmm_context_get_stream";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_ptr(stream, fn, "stream"));
+    APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
+    *stream = (void *)c->object->stream();
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+// Active tile-list pairs within `radius`: (atom i, atom j, image code).
+extern "C" apo_status apo_charmm_context_get_neighbor_pairs(int *pairs, const size_t len,
+                                                            size_t *num_pairs, const double radius,
+                                                            apo_charmm_context *c) {
+  const char *fn = "apo_charmm_context_get_neighbor_pairs";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_ptr(num_pairs, fn, "num_pairs"));
+    APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
+    auto fm = c->object->getForceManager();
+    auto &nl = fm->neighborList();
+    cudaStream_t s = c->object->stream();
+    APO_CUDA(cudaStreamSynchronize(s));
+    nl.sync_counts(s);
+    const int S = nl.h_counts[0], T = nl.h_counts[1];
+    std::vector<int> perm(S);
+    std::vector<float4> xs(S);
+    std::vector<int2> tiles(T);
+    std::vector<unsigned> masks((size_t)T * 32);
+    std::vector<int4> work(nl.h_counts[2]);
+    if (S) {
+      APO_CUDA(cudaMemcpy(perm.data(), nl.perm, S * sizeof(int), cudaMemcpyDeviceToHost));
+      APO_CUDA(cudaMemcpy(xs.data(), nl.xyzq_s, S * sizeof(float4), cudaMemcpyDeviceToHost));
+    }
+    if (T) {
+      APO_CUDA(cudaMemcpy(tiles.data(), nl.tiles, T * sizeof(int2), cudaMemcpyDeviceToHost));
+      APO_CUDA(cudaMemcpy(masks.data(), nl.masks, masks.size() * sizeof(unsigned), cudaMemcpyDeviceToHost));
+    }
+    if (!work.empty())
+      APO_CUDA(cudaMemcpy(work.data(), nl.work, work.size() * sizeof(int4), cudaMemcpyDeviceToHost));
+    auto box = fm->getBoxDimensions();
+    const double r2max = radius * radius;
+    size_t count = 0;
+    for (auto &w : work) {
+      for (int t = w.y; t < w.z; ++t) {
+        const int jc = tiles[t].x, sc = tiles[t].y;
+        const double sx = (sc % 3 - 1) * box[0], sy = ((sc / 3) % 3 - 1) * box[1],
+                     sz = (sc / 9 - 1) * box[2];
+        for (int i = 0; i < 32; ++i) {
+          const unsigned m = masks[(size_t)t * 32 + i];
+          const int si = w.x * 32 + i;
+          for (int j = 0; j < 32; ++j) {
+            if ((m >> j) & 1u) continue;
+            const int sj = jc * 32 + j;
+            const double dx = xs[si].x - (xs[sj].x + sx), dy = xs[si].y - (xs[sj].y + sy),
+                         dz = xs[si].z - (xs[sj].z + sz);
+            if (dx * dx + dy * dy + dz * dz >= r2max) continue;
+            if (pairs && 3 * (count + 1) <= len) {
+              pairs[3 * count] = perm[si];
+              pairs[3 * count + 1] = perm[sj];
+              pairs[3 * count + 2] = sc;
+            }
+            ++count;
+          }
+        }
+      }
+    }
+    *num_pairs = count;
+    if (pairs && 3 * count > len) return invalid(fn, "pair buffer too small");
+    return APO_STATUS_OK;
+  }, fn);
+}

@@ -1,0 +1,440 @@
+// ForceManager / CharmmContext; see engine.h.
+#include "engine.h"
+
+#include <cmath>
+#include <random>
+#include <sstream>
+
+#include "device_util.cuh"
+
+namespace apo {
+namespace {
+
+__global__ void fixed_to_global_kernel(int n, const long long *__restrict__ f, int stride,
+                                       const int *__restrict__ glo2loc, double *__restrict__ out) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n) return;
+  int s = glo2loc[g];
+  out[3 * g + 0] = (double)f[s] * kInvForceScale;
+  out[3 * g + 1] = (double)f[stride + s] * kInvForceScale;
+  out[3 * g + 2] = (double)f[2 * stride + s] * kInvForceScale;
+}
+
+__global__ void image_centering_kernel(double4 *__restrict__ c, float4 *__restrict__ xq,
+                                       const int2 *__restrict__ groups, int ng, double Lx,
+                                       double Ly, double Lz) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ng; i += gridDim.x * blockDim.x) {
+    const int2 g = groups[i];
+    double gx = 0, gy = 0, gz = 0;
+    for (int j = g.x; j <= g.y; ++j) {
+      gx += c[j].x;
+      gy += c[j].y;
+      gz += c[j].z;
+    }
+    const double inv = 1.0 / (double)(g.y - g.x + 1);
+    gx *= inv;
+    gy *= inv;
+    gz *= inv;
+    // shift by one box length when the centroid leaves [-L/2, L/2]
+    // (src/CharmmContext.cu:276-372)
+    const double sx = gx < -0.5 * Lx ? Lx : (gx > 0.5 * Lx ? -Lx : 0.0);
+    const double sy = gy < -0.5 * Ly ? Ly : (gy > 0.5 * Ly ? -Ly : 0.0);
+    const double sz = gz < -0.5 * Lz ? Lz : (gz > 0.5 * Lz ? -Lz : 0.0);
+    if (sx != 0.0 || sy != 0.0 || sz != 0.0) {
+      for (int j = g.x; j <= g.y; ++j) {
+        c[j].x += sx;
+        c[j].y += sy;
+        c[j].z += sz;
+        xq[j].x += (float)sx;
+        xq[j].y += (float)sy;
+        xq[j].z += (float)sz;
+      }
+    }
+  }
+}
+
+__global__ void coords_to_xyzq_kernel(const double4 *__restrict__ c, float4 *__restrict__ xq,
+                                      int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    const double4 v = c[i];
+    xq[i] = make_float4((float)v.x, (float)v.y, (float)v.z, (float)v.w);
+  }
+}
+
+}  // namespace
+
+void launch_image_centering(double4 *coords, float4 *xyzq, const int2 *groups, int ngroups,
+                            double Lx, double Ly, double Lz, cudaStream_t s) {
+  if (ngroups <= 0) return;
+  image_centering_kernel<<<(ngroups + 127) / 128, 128, 0, s>>>(coords, xyzq, groups, ngroups,
+                                                                Lx, Ly, Lz);
+  APO_LAUNCH_CHECK();
+}
+
+void launch_coords_to_xyzq(const double4 *coords, float4 *xyzq, int n, cudaStream_t s) {
+  coords_to_xyzq_kernel<<<(n + 255) / 256, 256, 0, s>>>(coords, xyzq, n);
+  APO_LAUNCH_CHECK();
+}
+
+// ------------------------------------------------------------- ForceManager
+
+ForceManager::ForceManager(std::shared_ptr<CharmmPSF> psf, std::shared_ptr<CharmmParameters> prm)
+    : m_Psf(std::move(psf)), m_Prm(std::move(prm)) {
+  if (!m_Psf || !m_Prm) throw std::invalid_argument("ForceManager: null PSF or parameters");
+}
+
+ForceManager::~ForceManager() {
+  for (cudaStream_t s : {m_SNb, m_SPme, m_SBond})
+    if (s) cudaStreamDestroy(s);
+  for (cudaEvent_t e : {m_EvFork, m_EvNb, m_EvPme, m_EvBond})
+    if (e) cudaEventDestroy(e);
+}
+
+void ForceManager::setBoxDimensions(const std::array<double, 3> &box) {
+  for (double b : box)
+    if (b < 0)
+      throw std::invalid_argument("Box dimensions: " + std::to_string(box[0]) + " x " +
+                                  std::to_string(box[1]) + " x " + std::to_string(box[2]) +
+                                  " are NOT valid");
+  m_Box = box;
+  m_Initialized = false;
+}
+
+void ForceManager::setFFTGrid(int nx, int ny, int nz) {
+  m_Nfft[0] = nx;
+  m_Nfft[1] = ny;
+  m_Nfft[2] = nz;
+  m_Initialized = false;
+}
+
+void ForceManager::setVdwType(int type) {
+  if (type != VDW_VFSW)
+    throw std::invalid_argument("only the VDW_VFSW (force switch) Lennard-Jones model is "
+                                "implemented on this engine");
+  m_VdwType = type;
+}
+
+void ForceManager::setPeriodicBoundaryCondition(PBC pbc) {
+  if (pbc != PBC::P1)
+    throw std::invalid_argument("only P1 periodic boundary conditions are implemented");
+}
+
+std::array<int, 3> ForceManager::computeFFTGridSize() const {
+  // 2 * floor(L/2) (src/ForceManager.cu:923-944)
+  std::array<int, 3> n;
+  for (int d = 0; d < 3; ++d) n[d] = std::max(2, 2 * ((int)m_Box[d] / 2));
+  return n;
+}
+
+void ForceManager::initialize() {
+  if (m_Box[0] == -9999.9999 || m_Box[1] == -9999.9999 || m_Box[2] == -9999.9999)
+    throw std::invalid_argument("Error: Box dimension was not set");
+  if (m_Cutoff <= 0.0 || m_Cutoff > m_Box[0] / 2.0)
+    throw std::invalid_argument("Error: Cutoff value (" + std::to_string(m_Cutoff) +
+                                ") not valid (boxx: " + std::to_string(m_Box[0]) + ")");
+  if (m_Ctofnb > m_Cutoff)
+    throw std::invalid_argument("ctofnb must not exceed the list cutoff (cutnb)");
+  if (m_Nfft[0] <= 0 || m_Nfft[1] <= 0 || m_Nfft[2] <= 0) {
+    auto n = computeFFTGridSize();
+    setFFTGrid(n[0], n[1], n[2]);
+  }
+  m_Top = build_topology(*m_Psf, *m_Prm);
+  const int n = m_Top.natom;
+
+  m_VdwTypeD.upload(m_Top.vdwtype);
+  m_Vdw.upload(m_Top.vdw);
+  m_Vdw14.upload(m_Top.vdw14);
+  m_BondIJ.upload(m_Top.bond_ij);
+  m_BondP.upload(m_Top.bond_p);
+  m_UbIJ.upload(m_Top.ub_ij);
+  m_UbP.upload(m_Top.ub_p);
+  m_AngleIJK.upload(m_Top.angle_ijk);
+  m_AngleP.upload(m_Top.angle_p);
+  m_DiheIJKL.upload(m_Top.dihe_ijkl);
+  m_DiheTerms.upload(m_Top.dihe_terms);
+  m_DiheCoef.upload(m_Top.dihe_coef);
+  m_ImpIJKL.upload(m_Top.imp_ijkl);
+  m_ImpP.upload(m_Top.imp_p);
+  m_In14.upload(m_Top.in14);
+  m_Ex14.upload(m_Top.ex14);
+
+  // the reference's direct-space set-up uses roff = ctofnb, ron = ctonnb
+  // (src/ForceManager.cu:513-514)
+  m_HostSetup = make_nb_setup(m_Box[0], m_Box[1], m_Box[2], m_Kappa, m_Ctofnb, m_Ctonnb);
+  m_Setup.upload(std::vector<NbSetup>{m_HostSetup});
+
+  m_Nbl.setup(n, (float)m_Box[0], (float)m_Box[1], (float)m_Box[2], (float)m_Cutoff,
+              m_Top.excl_ptr, m_Top.excl_idx, m_VdwTypeD.p, m_TilesPerWork);
+  m_Pme.setup(m_Nfft[0], m_Nfft[1], m_Nfft[2], m_Order, m_Kappa, m_Box[0], m_Box[1], m_Box[2]);
+  m_Pme.max_slots = m_Nbl.dims().slot_cap;
+  m_Stride = m_Nbl.dims().slot_cap;
+  m_Force.alloc((size_t)3 * m_Stride);
+  APO_CUDA(cudaMemset(m_Force.p, 0, (size_t)3 * m_Stride * sizeof(long long)));
+  m_Energy.alloc(kNumEnergyTerms);
+  APO_CUDA(cudaMemset(m_Energy.p, 0, kNumEnergyTerms * sizeof(long long)));
+
+  double q2 = 0.0;
+  for (double q : m_Top.charge) q2 += q * q;
+  m_SelfEnergy = -m_Kappa * kCcelec / std::sqrt(M_PI) * q2;
+
+  if (!m_SNb) {
+    APO_CUDA(cudaStreamCreateWithFlags(&m_SNb, cudaStreamNonBlocking));
+    APO_CUDA(cudaStreamCreateWithFlags(&m_SPme, cudaStreamNonBlocking));
+    APO_CUDA(cudaStreamCreateWithFlags(&m_SBond, cudaStreamNonBlocking));
+    for (cudaEvent_t *e : {&m_EvFork, &m_EvNb, &m_EvPme, &m_EvBond})
+      APO_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  }
+  m_ListBuilt = false;
+  m_Initialized = true;
+}
+
+void ForceManager::resetNeighborList(const float4 *d_xyzq, cudaStream_t s) {
+  if (!m_Initialized) throw std::runtime_error("ForceManager is not initialized");
+  if (!m_ListBuilt) {
+    // first build: size the tile buffers from the real demand (synchronous)
+    m_Nbl.ensure_capacity(d_xyzq, s);
+    m_ListBuilt = true;
+  } else {
+    m_Nbl.build(d_xyzq, s);
+  }
+}
+
+void ForceManager::calcForce(const float4 *d_xyzq, bool calcEnergy, bool /*calcVirial*/,
+                             cudaStream_t s, bool clear) {
+  if (!m_Initialized) throw std::runtime_error("ForceManager is not initialized");
+  if (!m_ListBuilt) resetNeighborList(d_xyzq, s);
+  else if (clear) m_Nbl.refresh(d_xyzq, s);
+  if (clear) APO_CUDA(cudaMemsetAsync(m_Force.p, 0, (size_t)3 * m_Stride * sizeof(long long), s));
+  APO_CUDA(cudaMemsetAsync(m_Energy.p, 0, kNumEnergyTerms * sizeof(long long), s));
+  APO_CUDA(cudaEventRecord(m_EvFork, s));
+  if (m_ComponentMask & 2) {
+    APO_CUDA(cudaStreamWaitEvent(m_SNb, m_EvFork, 0));
+    NbArgs a;
+    a.xyzq_s = m_Nbl.xyzq_s;
+    a.type_s = m_Nbl.type_s;
+    a.tiles = m_Nbl.tiles;
+    a.masks = m_Nbl.masks;
+    a.work = m_Nbl.work;
+    a.counts = m_Nbl.counts;
+    a.vdw = m_Vdw.p;
+    a.ntype = (int)m_Top.types.size();
+    a.force = m_Force.p;
+    a.stride = m_Stride;
+    a.energy = m_Energy.p;
+    a.setups = m_Setup.p;
+    launch_nonbonded(a, calcEnergy, m_Precise, m_SNb);
+    APO_CUDA(cudaEventRecord(m_EvNb, m_SNb));
+    APO_CUDA(cudaStreamWaitEvent(s, m_EvNb, 0));
+  }
+  if (m_ComponentMask & 4) {
+    APO_CUDA(cudaStreamWaitEvent(m_SPme, m_EvFork, 0));
+    m_Pme.compute(m_Nbl.xyzq_s, m_Nbl.counts, m_Force.p, m_Stride, m_Energy.p, calcEnergy,
+                  m_Precise, m_SPme);
+    APO_CUDA(cudaEventRecord(m_EvPme, m_SPme));
+    APO_CUDA(cudaStreamWaitEvent(s, m_EvPme, 0));
+  }
+  if (m_ComponentMask & 1) {
+    APO_CUDA(cudaStreamWaitEvent(m_SBond, m_EvFork, 0));
+    BondedArgs b;
+    b.xyzq = d_xyzq;
+    b.glo2loc = m_Nbl.glo2loc;
+    b.force = m_Force.p;
+    b.stride = m_Stride;
+    b.energy = m_Energy.p;
+    b.nbond = (int)m_BondIJ.n; b.bond_ij = m_BondIJ.p; b.bond_p = m_BondP.p;
+    b.nub = (int)m_UbIJ.n; b.ub_ij = m_UbIJ.p; b.ub_p = m_UbP.p;
+    b.nangle = (int)m_AngleIJK.n; b.angle_ijk = m_AngleIJK.p; b.angle_p = m_AngleP.p;
+    b.ndihe = (int)m_DiheIJKL.n; b.dihe_ijkl = m_DiheIJKL.p; b.dihe_terms = m_DiheTerms.p;
+    b.dihe_coef = m_DiheCoef.p;
+    b.nimp = (int)m_ImpIJKL.n; b.imp_ijkl = m_ImpIJKL.p; b.imp_p = m_ImpP.p;
+    b.nin14 = (int)m_In14.n; b.in14 = m_In14.p;
+    b.nex14 = (int)m_Ex14.n; b.ex14 = m_Ex14.p;
+    b.vdwtype = m_VdwTypeD.p;
+    b.vdw14 = m_Vdw14.p;
+    b.ntype = (int)m_Top.types.size();
+    b.nb = m_HostSetup;
+    launch_bonded(b, calcEnergy, m_SBond);
+    APO_CUDA(cudaEventRecord(m_EvBond, m_SBond));
+    APO_CUDA(cudaStreamWaitEvent(s, m_EvBond, 0));
+  }
+}
+
+std::map<std::string, double> ForceManager::getEnergyComponents(cudaStream_t s) {
+  long long e[kNumEnergyTerms];
+  APO_CUDA(cudaMemcpyAsync(e, m_Energy.p, sizeof(e), cudaMemcpyDeviceToHost, s));
+  APO_CUDA(cudaStreamSynchronize(s));
+  std::map<std::string, double> m;
+  for (int k = 0; k < kNumEnergyTerms; ++k) m[kEnergyNames[k]] = (double)e[k] * kInvEnergyScale;
+  m["ewse"] = (m_ComponentMask & 4) ? m_SelfEnergy : 0.0;
+  return m;
+}
+
+double ForceManager::getPotentialEnergy(cudaStream_t s) {
+  double t = 0.0;
+  for (auto &kv : getEnergyComponents(s)) t += kv.second;
+  return t;
+}
+
+void ForceManager::getForces(std::vector<double> &out, cudaStream_t s) {
+  const int n = m_Top.natom;
+  if (m_Scratch.n < (size_t)3 * n) m_Scratch.alloc((size_t)3 * n);
+  fixed_to_global_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, m_Force.p, m_Stride, m_Nbl.glo2loc,
+                                                          m_Scratch.p);
+  APO_LAUNCH_CHECK();
+  out.resize((size_t)3 * n);
+  APO_CUDA(cudaMemcpyAsync(out.data(), m_Scratch.p, (size_t)3 * n * sizeof(double),
+                           cudaMemcpyDeviceToHost, s));
+  APO_CUDA(cudaStreamSynchronize(s));
+}
+
+unsigned ForceManager::readDeviceError(cudaStream_t s) { return m_Nbl.read_error(s); }
+
+// ------------------------------------------------------------ CharmmContext
+
+CharmmContext::CharmmContext(std::shared_ptr<ForceManager> fm) : m_Fm(std::move(fm)) {
+  if (!m_Fm) throw std::invalid_argument("CharmmContext: null ForceManager");
+  if (!m_Fm->isInitialized()) m_Fm->initialize();
+  m_N = m_Fm->getNumAtoms();
+  APO_CUDA(cudaStreamCreateWithFlags(&m_Stream, cudaStreamNonBlocking));
+  m_Coords.alloc(m_N);
+  m_VelMass.alloc(m_N);
+  m_Xyzq.alloc(m_N);
+  const Topology &t = m_Fm->topology();
+  std::vector<double4> vm(m_N);
+  std::vector<double4> c(m_N);
+  for (int i = 0; i < m_N; ++i) {
+    vm[i] = make_double4(0.0, 0.0, 0.0, 1.0 / t.mass[i]);
+    c[i] = make_double4(0.0, 0.0, 0.0, t.charge[i]);
+  }
+  m_VelMass.upload(vm);
+  m_Coords.upload(c);
+  launch_coords_to_xyzq(m_Coords.p, m_Xyzq.p, m_N, m_Stream);
+  m_Groups.upload(t.groups);
+  std::random_device rd;
+  m_Seed = rd();
+  useHolonomicConstraints(true);
+}
+
+CharmmContext::~CharmmContext() {
+  if (m_Stream) cudaStreamDestroy(m_Stream);
+}
+
+void CharmmContext::useHolonomicConstraints(bool flag) {
+  m_Holonomic = flag;
+  m_Ndegf = m_Fm->topology().degrees_of_freedom(flag);
+}
+
+void CharmmContext::setCoordinates(const std::vector<double> &xyz) {
+  if ((int)xyz.size() != 3 * m_N) {
+    std::ostringstream m;
+    m << "setCoordinates: expected " << 3 * m_N << " values, got " << xyz.size();
+    throw std::invalid_argument(m.str());
+  }
+  const Topology &t = m_Fm->topology();
+  std::vector<double4> c(m_N);
+  for (int i = 0; i < m_N; ++i) {
+    if (!std::isfinite(xyz[3 * i]) || !std::isfinite(xyz[3 * i + 1]) || !std::isfinite(xyz[3 * i + 2]))
+      throw std::invalid_argument("setCoordinates: non-finite coordinate for atom " +
+                                  std::to_string(i));
+    c[i] = make_double4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], t.charge[i]);
+  }
+  APO_CUDA(cudaMemcpyAsync(m_Coords.p, c.data(), m_N * sizeof(double4), cudaMemcpyHostToDevice,
+                           m_Stream));
+  launch_coords_to_xyzq(m_Coords.p, m_Xyzq.p, m_N, m_Stream);
+  m_HasCoords = true;
+  resetNeighborList(m_Stream);
+  APO_CUDA(cudaStreamSynchronize(m_Stream));
+}
+
+std::vector<double> CharmmContext::getCoordinates() {
+  std::vector<double4> c(m_N);
+  APO_CUDA(cudaMemcpyAsync(c.data(), m_Coords.p, m_N * sizeof(double4), cudaMemcpyDeviceToHost,
+                           m_Stream));
+  APO_CUDA(cudaStreamSynchronize(m_Stream));
+  std::vector<double> out((size_t)3 * m_N);
+  for (int i = 0; i < m_N; ++i) {
+    out[3 * i] = c[i].x;
+    out[3 * i + 1] = c[i].y;
+    out[3 * i + 2] = c[i].z;
+  }
+  return out;
+}
+
+void CharmmContext::setVelocities(const std::vector<double> &v) {
+  if ((int)v.size() != 3 * m_N) throw std::invalid_argument("setVelocities: wrong length");
+  std::vector<double4> vm = m_VelMass.download();
+  for (int i = 0; i < m_N; ++i) {
+    vm[i].x = v[3 * i];
+    vm[i].y = v[3 * i + 1];
+    vm[i].z = v[3 * i + 2];
+  }
+  APO_CUDA(cudaMemcpy(m_VelMass.p, vm.data(), m_N * sizeof(double4), cudaMemcpyHostToDevice));
+}
+
+std::vector<double> CharmmContext::getVelocities() {
+  APO_CUDA(cudaStreamSynchronize(m_Stream));
+  std::vector<double4> vm = m_VelMass.download();
+  std::vector<double> out((size_t)3 * m_N);
+  for (int i = 0; i < m_N; ++i) {
+    out[3 * i] = vm[i].x;
+    out[3 * i + 1] = vm[i].y;
+    out[3 * i + 2] = vm[i].z;
+  }
+  return out;
+}
+
+// Maxwell-Boltzmann velocities with std::mt19937 and one
+// std::normal_distribution per atom, as src/CharmmContext.cu:478-525
+void CharmmContext::assignVelocitiesAtTemperature(double temperature) {
+  if (!m_HasCoords)
+    throw std::invalid_argument("assignVelocitiesAtTemperature: coordinates not set");
+  APO_CUDA(cudaStreamSynchronize(m_Stream));
+  std::vector<double4> vm = m_VelMass.download();
+  std::mt19937 gen{(std::mt19937::result_type)m_Seed};
+  const double boltz = kBoltz * (float)temperature;
+  for (int i = 0; i < m_N; ++i) {
+    double sd = std::sqrt(boltz * vm[i].w);
+    std::normal_distribution<> d(0, sd);
+    vm[i].x = d(gen);
+    vm[i].y = d(gen);
+    vm[i].z = d(gen);
+  }
+  APO_CUDA(cudaMemcpy(m_VelMass.p, vm.data(), m_N * sizeof(double4), cudaMemcpyHostToDevice));
+}
+
+double CharmmContext::getKineticEnergy() {
+  APO_CUDA(cudaStreamSynchronize(m_Stream));
+  std::vector<double4> vm = m_VelMass.download();
+  double ke = 0.0;
+  for (auto &v : vm) ke += 0.5 * (v.x * v.x + v.y * v.y + v.z * v.z) / v.w;
+  return ke;
+}
+
+double CharmmContext::computeTemperature() {
+  return getKineticEnergy() / (0.5 * m_Ndegf * kBoltz);
+}
+
+void CharmmContext::imageCentering(cudaStream_t s) {
+  auto b = m_Fm->getBoxDimensions();
+  launch_image_centering(m_Coords.p, m_Xyzq.p, m_Groups.p, (int)m_Groups.n, b[0], b[1], b[2], s);
+}
+
+void CharmmContext::resetNeighborList(cudaStream_t s) {
+  imageCentering(s);
+  m_Fm->resetNeighborList(m_Xyzq.p, s);
+}
+
+void CharmmContext::calculateForces(bool reset, bool calcEnergy, bool calcVirial) {
+  if (!m_HasCoords) throw std::runtime_error("calculateForces: coordinates not set");
+  if (reset) resetNeighborList(m_Stream);
+  m_Fm->calcForce(m_Xyzq.p, calcEnergy, calcVirial, m_Stream);
+  APO_CUDA(cudaStreamSynchronize(m_Stream));
+}
+
+double CharmmContext::calculatePotentialEnergy(bool reset, bool /*print*/) {
+  calculateForces(reset, true, true);
+  return m_Fm->getPotentialEnergy(m_Stream);
+}
+
+}  // namespace apo

@@ -1,0 +1,208 @@
+// ForceManager and CharmmContext: the host orchestration of one system.
+//
+// Mirrors the reference's classes of the same names (include/ForceManager.h:115-694,
+// include/CharmmContext.h:36-469) for the P1 / VDW_VFSW / EWALD path:
+// same setters, defaults (kappa 0.34, cutnb 14, ctonnb 12, ctofnb 10, spline
+// order 4, FFT grid 2*floor(L/2)), energy-term names, gradient sign and
+// exceptions on bad input.  Differences by design:
+//   * one int64 fixed-point gradient buffer in neighbour-list slot order is
+//     shared by the bonded, reciprocal and direct parts (the reference keeps
+//     three and adds them into a fourth on the host's command);
+//   * energies are 64-bit fixed-point sums, so the total is order-free;
+//   * a force evaluation issues no host synchronisation, so it can be
+//     captured in a CUDA graph.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <array>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "bonded.h"
+#include "charmm_io.h"
+#include "common.h"
+#include "nblist.h"
+#include "nonbonded.h"
+#include "pme.h"
+#include "topology.h"
+
+namespace apo {
+
+enum class PBC { P1 = 0, P21 = 1 };
+enum VdwModel { VDW_VSH = 1, VDW_VSW = 2, VDW_VFSW = 3, VDW_VGSH = 4, VDW_CUT = 5 };
+
+template <typename T>
+struct DeviceArray {
+  T *p = nullptr;
+  size_t n = 0;
+  DeviceArray() = default;
+  DeviceArray(const DeviceArray &) = delete;
+  DeviceArray &operator=(const DeviceArray &) = delete;
+  ~DeviceArray() { reset(); }
+  void reset() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count) {
+    reset();
+    n = count;
+    if (count) APO_CUDA(cudaMalloc(&p, count * sizeof(T)));
+  }
+  void upload(const std::vector<T> &v) {
+    alloc(v.size());
+    if (!v.empty())
+      APO_CUDA(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  }
+  std::vector<T> download() const {
+    std::vector<T> v(n);
+    if (n) APO_CUDA(cudaMemcpy(v.data(), p, n * sizeof(T), cudaMemcpyDeviceToHost));
+    return v;
+  }
+};
+
+class ForceManager {
+ public:
+  ForceManager(std::shared_ptr<CharmmPSF> psf, std::shared_ptr<CharmmParameters> prm);
+  ~ForceManager();
+
+  void setBoxDimensions(const std::array<double, 3> &box);
+  void setKappa(double k) { m_Kappa = k; m_Initialized = false; }
+  void setCutoff(double c) { m_Cutoff = c; m_Initialized = false; }
+  void setCtonnb(double c) { m_Ctonnb = c; m_Initialized = false; }
+  void setCtofnb(double c) { m_Ctofnb = c; m_Initialized = false; }
+  void setFFTGrid(int nx, int ny, int nz);
+  void setPmeSplineOrder(int order) { m_Order = order; m_Initialized = false; }
+  void setVdwType(int type);
+  void setPeriodicBoundaryCondition(PBC pbc);
+  // precision form: per-pair fixed-point accumulation, FP64 influence function
+  void setPrecisionMode(bool precise) { m_Precise = precise; }
+  bool getPrecisionMode() const { return m_Precise; }
+  void setTilesPerWork(int t) { m_TilesPerWork = t; m_Initialized = false; }
+  // bit mask of the parts evaluated: 1 bonded+1-4, 2 direct, 4 reciprocal
+  void setComponentMask(int mask) { m_ComponentMask = mask; }
+
+  const std::array<double, 3> &getBoxDimensions() const { return m_Box; }
+  double getKappa() const { return m_Kappa; }
+  double getCutoff() const { return m_Cutoff; }
+  double getCtonnb() const { return m_Ctonnb; }
+  double getCtofnb() const { return m_Ctofnb; }
+  std::array<int, 3> getFFTGrid() const { return {m_Nfft[0], m_Nfft[1], m_Nfft[2]}; }
+  int getPmeSplineOrder() const { return m_Order; }
+  int getNumAtoms() const { return m_Psf->getNumAtoms(); }
+  bool isInitialized() const { return m_Initialized; }
+  std::shared_ptr<CharmmPSF> getPsf() const { return m_Psf; }
+  const Topology &topology() const { return m_Top; }
+  std::array<int, 3> computeFFTGridSize() const;
+
+  void initialize();
+  // image-wrapped rebuild of the tile list from global-order coordinates
+  void resetNeighborList(const float4 *d_xyzq, cudaStream_t s);
+  // gradients into the slot-order fixed-point buffer (cleared first unless
+  // clear == false); energies into the fixed-point energy slots
+  void calcForce(const float4 *d_xyzq, bool calcEnergy, bool calcVirial, cudaStream_t s,
+                 bool clear = true);
+
+  std::map<std::string, double> getEnergyComponents(cudaStream_t s);
+  double getPotentialEnergy(cudaStream_t s);
+  // total gradient, global atom order, (N,3) row-major
+  void getForces(std::vector<double> &out, cudaStream_t s);
+
+  // device state used by the integrators
+  long long *forceFixed() const { return m_Force.p; }
+  int forceStride() const { return m_Stride; }
+  long long *energyFixed() const { return m_Energy.p; }
+  NeighborList &neighborList() { return m_Nbl; }
+  Pme &pme() { return m_Pme; }
+  double selfEnergy() const { return m_SelfEnergy; }
+  unsigned readDeviceError(cudaStream_t s);
+
+ private:
+  std::shared_ptr<CharmmPSF> m_Psf;
+  std::shared_ptr<CharmmParameters> m_Prm;
+  std::array<double, 3> m_Box{{-9999.9999, -9999.9999, -9999.9999}};
+  double m_Kappa = 0.34, m_Cutoff = 14.0, m_Ctonnb = 12.0, m_Ctofnb = 10.0;
+  int m_Nfft[3] = {-1, -1, -1};
+  int m_Order = 4;
+  int m_VdwType = VDW_VFSW;
+  bool m_Precise = false;
+  bool m_Initialized = false;
+  bool m_ListBuilt = false;
+  int m_TilesPerWork = 8;
+  int m_ComponentMask = 7;
+  double m_SelfEnergy = 0.0;
+  Topology m_Top;
+
+  NeighborList m_Nbl;
+  Pme m_Pme;
+  int m_Stride = 0;
+  DeviceArray<long long> m_Force, m_Energy;
+  DeviceArray<int> m_VdwTypeD;
+  DeviceArray<float2> m_Vdw, m_Vdw14;
+  DeviceArray<NbSetup> m_Setup;
+  NbSetup m_HostSetup{};
+  DeviceArray<int2> m_BondIJ, m_UbIJ, m_In14, m_Ex14, m_DiheTerms;
+  DeviceArray<float2> m_BondP, m_UbP, m_AngleP, m_ImpP;
+  DeviceArray<int4> m_AngleIJK, m_DiheIJKL, m_ImpIJKL;
+  DeviceArray<float4> m_DiheCoef;
+  DeviceArray<double> m_Scratch;
+  cudaStream_t m_SNb = nullptr, m_SPme = nullptr, m_SBond = nullptr;
+  cudaEvent_t m_EvFork = nullptr, m_EvNb = nullptr, m_EvPme = nullptr, m_EvBond = nullptr;
+};
+
+class CharmmContext {
+ public:
+  explicit CharmmContext(std::shared_ptr<ForceManager> fm);
+  ~CharmmContext();
+
+  void setCoordinates(const std::vector<double> &xyz);
+  void setCoordinates(const CharmmCrd &crd) { setCoordinates(crd.getCoordinates()); }
+  std::vector<double> getCoordinates();
+  void setVelocities(const std::vector<double> &v);
+  std::vector<double> getVelocities();
+  void setRandomSeedForVelocities(uint64_t seed) { m_Seed = seed; }
+  void assignVelocitiesAtTemperature(double temperature);
+  void useHolonomicConstraints(bool flag);
+  bool isUsingHolonomicConstraints() const { return m_Holonomic; }
+  int getDegreesOfFreedom() const { return m_Ndegf; }
+  int getNumAtoms() const { return m_N; }
+  double computeTemperature();
+  double getKineticEnergy();
+
+  void imageCentering(cudaStream_t s);
+  void resetNeighborList(cudaStream_t s);
+  void calculateForces(bool reset, bool calcEnergy, bool calcVirial);
+  double calculatePotentialEnergy(bool reset, bool print);
+
+  std::shared_ptr<ForceManager> getForceManager() const { return m_Fm; }
+  cudaStream_t stream() const { return m_Stream; }
+  // device state: coordinates+charge (double4), velocity + inverse mass
+  // (double4), single-precision coordinates+charge in atom order (float4)
+  double4 *coords() const { return m_Coords.p; }
+  double4 *velMass() const { return m_VelMass.p; }
+  float4 *xyzq() const { return m_Xyzq.p; }
+  const int2 *groups() const { return m_Groups.p; }
+  int numGroups() const { return (int)m_Groups.n; }
+
+ private:
+  std::shared_ptr<ForceManager> m_Fm;
+  int m_N = 0;
+  uint64_t m_Seed = 0;
+  bool m_Holonomic = true;
+  int m_Ndegf = 0;
+  bool m_HasCoords = false;
+  cudaStream_t m_Stream = nullptr;
+  DeviceArray<double4> m_Coords, m_VelMass;
+  DeviceArray<float4> m_Xyzq;
+  DeviceArray<int2> m_Groups;
+};
+
+// device helpers shared with the integrators
+void launch_image_centering(double4 *coords, float4 *xyzq, const int2 *groups, int ngroups,
+                            double Lx, double Ly, double Lz, cudaStream_t s);
+void launch_coords_to_xyzq(const double4 *coords, float4 *xyzq, int n, cudaStream_t s);
+
+}  // namespace apo

@@ -1,0 +1,533 @@
+// Neighbour-list kernels; see nblist.h.
+#include "nblist.h"
+
+#include <algorithm>
+#include <cmath>
+
+#include "device_util.cuh"
+
+namespace apo {
+namespace {
+
+constexpr int kScanThreads = 1024;
+
+__device__ __forceinline__ int floor_div(int a, int b) {
+  return a >= 0 ? a / b : -((-a + b - 1) / b);
+}
+
+// (1) bin atoms into x-y columns; record wrapped z key and image shift
+__global__ void bin_kernel(int n, const float4 *__restrict__ xyzq, NbListDims d,
+                           int *__restrict__ col_count, int *__restrict__ atom_col,
+                           int *__restrict__ atom_rank, float4 *__restrict__ atom_shift,
+                           float *__restrict__ zkey, unsigned *__restrict__ err) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n) return;
+  float4 p = xyzq[g];
+  float sx = 0.f, sy = 0.f, sz = 0.f;
+  int col = 0;
+  float zw = 0.f;
+  if (isfinite(p.x) && isfinite(p.y) && isfinite(p.z)) {
+    float ix = floorf(p.x / d.Lx + 0.5f), iy = floorf(p.y / d.Ly + 0.5f),
+          iz = floorf(p.z / d.Lz + 0.5f);
+    sx = -ix * d.Lx;
+    sy = -iy * d.Ly;
+    sz = -iz * d.Lz;
+    float xw = p.x + sx, yw = p.y + sy;
+    zw = p.z + sz;
+    int cx = (int)((xw + 0.5f * d.Lx) * ((float)d.ncx / d.Lx));
+    int cy = (int)((yw + 0.5f * d.Ly) * ((float)d.ncy / d.Ly));
+    cx = min(max(cx, 0), d.ncx - 1);
+    cy = min(max(cy, 0), d.ncy - 1);
+    col = cx + d.ncx * cy;
+  } else {
+    atomicOr(err, (unsigned)kErrNaN);
+  }
+  atom_col[g] = col;
+  atom_rank[g] = atomicAdd(&col_count[col], 1);
+  atom_shift[g] = make_float4(sx, sy, sz, 0.f);
+  zkey[g] = zw;
+}
+
+// block-wide exclusive scan helper (kScanThreads threads)
+__device__ int block_exclusive_scan(int v, int *sh, int &total) {
+  int t = threadIdx.x;
+  sh[t] = v;
+  __syncthreads();
+  for (int o = 1; o < kScanThreads; o <<= 1) {
+    int a = t >= o ? sh[t - o] : 0;
+    __syncthreads();
+    sh[t] += a;
+    __syncthreads();
+  }
+  total = sh[kScanThreads - 1];
+  int r = sh[t] - v;
+  __syncthreads();
+  return r;
+}
+
+// (2) padded column offsets; slot totals
+__global__ void col_scan_kernel(int ncol, const int *__restrict__ col_count,
+                                int *__restrict__ col_start, int *__restrict__ counts,
+                                int slot_cap, int sort_cap, unsigned *__restrict__ err) {
+  __shared__ int sh[kScanThreads];
+  int carry = 0;
+  bool over = false;
+  for (int base = 0; base < ncol; base += kScanThreads) {
+    int c = base + threadIdx.x;
+    int cnt = c < ncol ? col_count[c] : 0;
+    if (cnt > sort_cap) over = true;
+    int padded = (cnt + kTile - 1) / kTile * kTile;
+    int tot;
+    int ex = block_exclusive_scan(padded, sh, tot);
+    if (c < ncol) col_start[c] = carry + ex;
+    carry += tot;
+  }
+  if (over) atomicOr(err, (unsigned)kErrColumnOverflow);
+  if (threadIdx.x == 0) {
+    col_start[ncol] = carry;
+    if (carry > slot_cap) {
+      atomicOr(err, (unsigned)kErrColumnOverflow);
+      carry = 0;
+    }
+    counts[0] = carry;
+  }
+}
+
+// (3) scatter atoms to their column's slot range (order inside a column is
+// fixed afterwards by the column sort)
+__global__ void scatter_kernel(int n, const int *__restrict__ atom_col,
+                               const int *__restrict__ atom_rank,
+                               const int *__restrict__ col_start,
+                               const float *__restrict__ zkey, float *__restrict__ tkey,
+                               int *__restrict__ tidx, const int *__restrict__ counts) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n || counts[0] == 0) return;
+  int s = col_start[atom_col[g]] + atom_rank[g];
+  tkey[s] = zkey[g];
+  tidx[s] = g;
+}
+
+// (4) one block per column: bitonic sort by (z, atom index); write the
+// permutation, its inverse, shifts, types and the cluster -> column map
+__global__ void col_sort_kernel(int ncol, const int *__restrict__ col_count,
+                                const int *__restrict__ col_start,
+                                const float *__restrict__ tkey, const int *__restrict__ tidx,
+                                const float4 *__restrict__ atom_shift,
+                                const int *__restrict__ vdwtype, int *__restrict__ perm,
+                                int *__restrict__ glo2loc, float4 *__restrict__ slot_shift,
+                                int *__restrict__ type_s, int *__restrict__ cl_col,
+                                const int *__restrict__ counts, int sort_cap) {
+  extern __shared__ unsigned char smem[];
+  float *sk = reinterpret_cast<float *>(smem);
+  int *si = reinterpret_cast<int *>(smem + sizeof(float) * sort_cap);
+  int col = blockIdx.x;
+  if (col >= ncol || counts[0] == 0) return;
+  int cnt = col_count[col];
+  int start = col_start[col];
+  int padded = col_start[col + 1] - start;
+  if (cnt > sort_cap) return;
+  int P = 1;
+  while (P < cnt) P <<= 1;
+  for (int k = threadIdx.x; k < P; k += blockDim.x) {
+    if (k < cnt) {
+      sk[k] = tkey[start + k];
+      si[k] = tidx[start + k];
+    } else {
+      sk[k] = INFINITY;
+      si[k] = 0x7fffffff;
+    }
+  }
+  __syncthreads();
+  for (int size = 2; size <= P; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int k = threadIdx.x; k < P; k += blockDim.x) {
+        int l = k ^ stride;
+        if (l > k) {
+          bool up = (k & size) == 0;
+          float ka = sk[k], kb = sk[l];
+          int ia = si[k], ib = si[l];
+          bool gt = (ka > kb) || (ka == kb && ia > ib);
+          if (gt == up) {
+            sk[k] = kb;
+            sk[l] = ka;
+            si[k] = ib;
+            si[l] = ia;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (int k = threadIdx.x; k < padded; k += blockDim.x) {
+    int s = start + k;
+    if (k < cnt) {
+      int g = si[k];
+      perm[s] = g;
+      glo2loc[g] = s;
+      slot_shift[s] = atom_shift[g];
+      type_s[s] = vdwtype[g];
+    } else {
+      perm[s] = -1;
+      slot_shift[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+      type_s[s] = 0;
+    }
+    if ((k & (kTile - 1)) == 0) cl_col[s / kTile] = col;
+  }
+}
+
+// sorted, wrapped coordinates (runs after every coordinate update)
+__global__ void refresh_kernel(const float4 *__restrict__ xyzq, const int *__restrict__ perm,
+                               const float4 *__restrict__ slot_shift,
+                               float4 *__restrict__ xyzq_s, const int *__restrict__ counts) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= counts[0]) return;
+  int g = perm[s];
+  float4 out = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (g >= 0) {
+    float4 p = xyzq[g], sh = slot_shift[s];
+    out = make_float4(p.x + sh.x, p.y + sh.y, p.z + sh.z, p.w);
+  }
+  xyzq_s[s] = out;
+}
+
+// (5) cluster bounding boxes, one warp per cluster
+__global__ void bbox_kernel(const float4 *__restrict__ xyzq_s, const int *__restrict__ perm,
+                            float4 *__restrict__ bb_c, float4 *__restrict__ bb_h,
+                            const int *__restrict__ counts) {
+  int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (w >= counts[0] / kTile) return;
+  int s = w * kTile + lane;
+  float4 p = xyzq_s[s];
+  bool valid = perm[s] >= 0;
+  float mnx = valid ? p.x : INFINITY, mny = valid ? p.y : INFINITY,
+        mnz = valid ? p.z : INFINITY;
+  float mxx = valid ? p.x : -INFINITY, mxy = valid ? p.y : -INFINITY,
+        mxz = valid ? p.z : -INFINITY;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    mnx = fminf(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
+    mny = fminf(mny, __shfl_xor_sync(0xffffffffu, mny, o));
+    mnz = fminf(mnz, __shfl_xor_sync(0xffffffffu, mnz, o));
+    mxx = fmaxf(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
+    mxy = fmaxf(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
+    mxz = fmaxf(mxz, __shfl_xor_sync(0xffffffffu, mxz, o));
+  }
+  if (lane == 0) {
+    bb_c[w] = make_float4(0.5f * (mnx + mxx), 0.5f * (mny + mxy), 0.5f * (mnz + mxz), 0.f);
+    bb_h[w] = make_float4(0.5f * (mxx - mnx), 0.5f * (mxy - mny), 0.5f * (mxz - mnz), 0.f);
+  }
+}
+
+// (6) tile search.  One warp per i-cluster; lanes test (j-cluster, z-image)
+// candidates of every column within reach, and a ballot compacts the hits in
+// candidate order, so the list is deterministic.  With FILL the tiles, their
+// exclusion masks and the work items are written at the offsets of the scan.
+template <bool FILL>
+__global__ void tiles_kernel(NbListDims d, const int *__restrict__ cl_col,
+                             const int *__restrict__ col_start,
+                             const float4 *__restrict__ bb_c, const float4 *__restrict__ bb_h,
+                             const int *__restrict__ perm, const int *__restrict__ glo2loc,
+                             const int *__restrict__ excl_ptr, const int *__restrict__ excl_idx,
+                             int *__restrict__ tile_count, const int *__restrict__ tile_start,
+                             const int *__restrict__ work_start, int2 *__restrict__ tiles,
+                             unsigned *__restrict__ masks, int4 *__restrict__ work,
+                             const int *__restrict__ counts, int sys) {
+  const int ic = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (ic >= counts[0] / kTile) return;
+  if (FILL && counts[1] == 0) return;  // overflow: nothing to write
+  const int c = cl_col[ic];
+  const int cx = c % d.ncx, cy = c / d.ncx;
+  const float4 ci = bb_c[ic], hi = bb_h[ic];
+  const float cwx = d.Lx / d.ncx, cwy = d.Ly / d.ncy;
+  const int Rx = (int)ceilf(d.rlist / cwx), Ry = (int)ceilf(d.rlist / cwy);
+  const float rl2 = d.rlist * d.rlist;
+  int gi = 0;
+  int nexcl_begin = 0, nexcl_end = 0;
+  if (FILL) {
+    gi = perm[ic * kTile + lane];
+    if (gi >= 0) {
+      nexcl_begin = excl_ptr[gi];
+      nexcl_end = excl_ptr[gi + 1];
+    }
+  }
+  int count = 0;
+  const int base_tile = FILL ? tile_start[ic] : 0;
+  for (int dy = -Ry; dy <= Ry; ++dy) {
+    int yy = cy + dy;
+    int iy = floor_div(yy, d.ncy);
+    if (iy < -1 || iy > 1) continue;
+    int wy = yy - iy * d.ncy;
+    for (int dx = -Rx; dx <= Rx; ++dx) {
+      int xx = cx + dx;
+      int ix = floor_div(xx, d.ncx);
+      if (ix < -1 || ix > 1) continue;
+      int wx = xx - ix * d.ncx;
+      int col = wx + d.ncx * wy;
+      int js = col_start[col] / kTile, je = col_start[col + 1] / kTile;
+      int ncand = (je - js) * 3;
+      for (int b0 = 0; b0 < ncand; b0 += 32) {
+        int cand = b0 + lane;
+        bool ok = false;
+        int jc = 0, sc = 13;
+        if (cand < ncand) {
+          jc = js + cand / 3;
+          int iz = cand % 3 - 1;
+          sc = (ix + 1) + 3 * (iy + 1) + 9 * (iz + 1);
+          if (jc > ic || (jc == ic && sc >= 13)) {
+            float4 cj = bb_c[jc], hj = bb_h[jc];
+            float ddx = fmaxf(0.f, fabsf(ci.x - cj.x - ix * d.Lx) - hi.x - hj.x);
+            float ddy = fmaxf(0.f, fabsf(ci.y - cj.y - iy * d.Ly) - hi.y - hj.y);
+            float ddz = fmaxf(0.f, fabsf(ci.z - cj.z - iz * d.Lz) - hi.z - hj.z);
+            ok = ddx * ddx + ddy * ddy + ddz * ddz < rl2;
+          }
+        }
+        unsigned hits = __ballot_sync(0xffffffffu, ok);
+        if (FILL) {
+          while (hits) {
+            int src = __ffs(hits) - 1;
+            hits &= hits - 1;
+            int tjc = __shfl_sync(0xffffffffu, jc, src);
+            int tsc = __shfl_sync(0xffffffffu, sc, src);
+            int t = base_tile + count;
+            ++count;
+            int pj = perm[tjc * kTile + lane];
+            unsigned word = __ballot_sync(0xffffffffu, pj < 0);
+            if (gi < 0) {
+              word = 0xffffffffu;
+            } else {
+              if (tjc == ic && tsc == 13)
+                word |= (lane == 31) ? 0xffffffffu : ((2u << lane) - 1u);
+              for (int e = nexcl_begin; e < nexcl_end; ++e) {
+                int lp = glo2loc[excl_idx[e]];
+                if ((lp >> 5) == tjc) word |= 1u << (lp & 31);
+              }
+            }
+            if (lane == 0) tiles[t] = make_int2(tjc, tsc);
+            masks[(size_t)t * kTile + lane] = word;
+          }
+        } else {
+          count += __popc(hits);
+        }
+      }
+    }
+  }
+  if (!FILL) {
+    if (lane == 0) tile_count[ic] = count;
+  } else if (lane == 0) {
+    int w0 = work_start[ic];
+    int tpw = d.tiles_per_work;
+    for (int k = 0; k * tpw < count; ++k)
+      work[w0 + k] = make_int4(ic, base_tile + k * tpw, base_tile + min(count, (k + 1) * tpw), sys);
+  }
+}
+
+// (7) offsets of tiles and work items per i-cluster
+__global__ void tile_scan_kernel(const int *__restrict__ tile_count, int *__restrict__ tile_start,
+                                 int *__restrict__ work_start, int *__restrict__ counts,
+                                 int tile_cap, int work_cap, int tpw, unsigned *__restrict__ err) {
+  __shared__ int sh[kScanThreads];
+  int ncl = counts[0] / kTile;
+  int carry_t = 0, carry_w = 0;
+  for (int base = 0; base < ncl; base += kScanThreads) {
+    int c = base + threadIdx.x;
+    int nt = c < ncl ? tile_count[c] : 0;
+    int nw = (nt + tpw - 1) / tpw;
+    int tot;
+    int ex = block_exclusive_scan(nt, sh, tot);
+    if (c < ncl) tile_start[c] = carry_t + ex;
+    carry_t += tot;
+    ex = block_exclusive_scan(nw, sh, tot);
+    if (c < ncl) work_start[c] = carry_w + ex;
+    carry_w += tot;
+  }
+  if (threadIdx.x == 0) {
+    if (carry_t > tile_cap || carry_w > work_cap) {
+      atomicOr(err, (unsigned)(carry_t > tile_cap ? kErrTileOverflow : kErrWorkOverflow));
+      // record the demand so the host can grow the buffers, but publish empty
+      // lists so nothing is written out of bounds
+      counts[3] = carry_t;
+      counts[4] = carry_w;
+      carry_t = carry_w = 0;
+    } else {
+      counts[3] = carry_t;
+      counts[4] = carry_w;
+    }
+    counts[1] = carry_t;
+    counts[2] = carry_w;
+  }
+}
+
+template <typename T>
+void dalloc(T *&p, size_t n) {
+  if (p) APO_CUDA(cudaFree(p));
+  p = nullptr;
+  if (n) APO_CUDA(cudaMalloc(&p, n * sizeof(T)));
+}
+template <typename T>
+void dfree(T *&p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+}  // namespace
+
+NeighborList::~NeighborList() { release(); }
+
+void NeighborList::release() {
+  dfree(perm); dfree(glo2loc); dfree(slot_shift); dfree(xyzq_s); dfree(type_s);
+  dfree(tiles); dfree(masks); dfree(work); dfree(counts); dfree(error);
+  dfree(m_excl_ptr); dfree(m_excl_idx); dfree(m_col_count); dfree(m_col_start);
+  dfree(m_atom_col); dfree(m_atom_rank); dfree(m_atom_shift); dfree(m_atom_z); dfree(m_tmp_key);
+  dfree(m_tmp_idx); dfree(m_cl_col); dfree(m_bb_c); dfree(m_bb_h);
+  dfree(m_tile_count); dfree(m_tile_start); dfree(m_work_start);
+}
+
+void NeighborList::setup(int natom, float Lx, float Ly, float Lz, float rlist,
+                         const std::vector<int> &excl_ptr, const std::vector<int> &excl_idx,
+                         const int *d_vdwtype, int tiles_per_work) {
+  if (natom <= 0) throw std::invalid_argument("NeighborList: no atoms");
+  m_d.natom = natom;
+  m_d.Lx = Lx;
+  m_d.Ly = Ly;
+  m_d.Lz = Lz;
+  m_d.rlist = rlist;
+  m_d.tiles_per_work = tiles_per_work;
+  m_vdwtype = d_vdwtype;
+  {
+    static bool attr = false;
+    if (!attr) {
+      APO_CUDA(cudaFuncSetAttribute(col_sort_kernel,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+      attr = true;
+    }
+  }
+  // columns whose cross-section holds ~32 atoms per z-slab of equal height:
+  // clusters come out close to cubic
+  double rho = natom / ((double)Lx * Ly * Lz);
+  double edge = std::cbrt(32.0 / rho);
+  m_d.ncx = std::max(1, (int)std::floor(Lx / edge));
+  m_d.ncy = std::max(1, (int)std::floor(Ly / edge));
+  m_ncol = m_d.ncx * m_d.ncy;
+  double per_col = natom / (double)m_ncol;
+  m_d.sort_cap = 1024;
+  while (m_d.sort_cap < 1.6 * per_col + 64) m_d.sort_cap *= 2;
+  m_d.slot_cap = natom + kTile * m_ncol;
+  m_d.slot_cap = (m_d.slot_cap + kTile - 1) / kTile * kTile;
+  // tile estimate: clusters within rlist + two cluster edges, half list
+  int ncl = m_d.slot_cap / kTile;
+  double reach = rlist + 2.0 * edge;
+  double per_cl = rho * 4.18879 * reach * reach * reach / 32.0 * 0.5 + 16.0;
+  m_d.tile_cap = (int)std::min<double>(ncl * per_cl, 2.0e9 / 128.0);
+  m_d.work_cap = m_d.tile_cap / std::max(1, tiles_per_work) + ncl + 16;
+  alloc();
+  dalloc(m_excl_ptr, excl_ptr.size());
+  dalloc(m_excl_idx, std::max<size_t>(1, excl_idx.size()));
+  APO_CUDA(cudaMemcpy(m_excl_ptr, excl_ptr.data(), excl_ptr.size() * sizeof(int),
+                      cudaMemcpyHostToDevice));
+  if (!excl_idx.empty())
+    APO_CUDA(cudaMemcpy(m_excl_idx, excl_idx.data(), excl_idx.size() * sizeof(int),
+                        cudaMemcpyHostToDevice));
+}
+
+void NeighborList::alloc() {
+  const int n = m_d.natom, S = m_d.slot_cap, ncl = S / kTile;
+  dalloc(perm, S); dalloc(glo2loc, n); dalloc(slot_shift, S); dalloc(xyzq_s, S);
+  dalloc(type_s, S); dalloc(tiles, m_d.tile_cap); dalloc(masks, (size_t)m_d.tile_cap * kTile);
+  dalloc(work, m_d.work_cap); dalloc(counts, 8); dalloc(error, 1);
+  dalloc(m_col_count, m_ncol); dalloc(m_col_start, m_ncol + 1); dalloc(m_atom_col, n);
+  dalloc(m_atom_rank, n); dalloc(m_atom_shift, n); dalloc(m_atom_z, n);
+  dalloc(m_tmp_key, S); dalloc(m_tmp_idx, S);
+  dalloc(m_cl_col, ncl); dalloc(m_bb_c, ncl); dalloc(m_bb_h, ncl);
+  dalloc(m_tile_count, ncl); dalloc(m_tile_start, ncl); dalloc(m_work_start, ncl);
+  APO_CUDA(cudaMemset(counts, 0, 8 * sizeof(int)));
+  APO_CUDA(cudaMemset(error, 0, sizeof(unsigned)));
+  APO_CUDA(cudaMemset(xyzq_s, 0, (size_t)S * sizeof(float4)));
+  APO_CUDA(cudaMemset(perm, 0xff, (size_t)S * sizeof(int)));
+  APO_CUDA(cudaMemset(type_s, 0, (size_t)S * sizeof(int)));
+}
+
+void NeighborList::build(const float4 *d_xyzq, cudaStream_t s) {
+  const int n = m_d.natom;
+  const int S = m_d.slot_cap;
+  const int ncl = S / kTile;
+  APO_CUDA(cudaMemsetAsync(m_col_count, 0, m_ncol * sizeof(int), s));
+  bin_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, d_xyzq, m_d, m_col_count, m_atom_col,
+                                              m_atom_rank, m_atom_shift, m_atom_z, error);
+  APO_LAUNCH_CHECK();
+  col_scan_kernel<<<1, kScanThreads, 0, s>>>(m_ncol, m_col_count, m_col_start, counts, S,
+                                             m_d.sort_cap, error);
+  APO_LAUNCH_CHECK();
+  scatter_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, m_atom_col, m_atom_rank, m_col_start,
+                                                  m_atom_z, m_tmp_key, m_tmp_idx, counts);
+  APO_LAUNCH_CHECK();
+  size_t sm = (size_t)m_d.sort_cap * (sizeof(float) + sizeof(int));
+  col_sort_kernel<<<m_ncol, 512, sm, s>>>(m_ncol, m_col_count, m_col_start, m_tmp_key,
+                                          m_tmp_idx, m_atom_shift, m_vdwtype, perm, glo2loc,
+                                          slot_shift, type_s, m_cl_col, counts, m_d.sort_cap);
+  APO_LAUNCH_CHECK();
+  refresh(d_xyzq, s);
+  bbox_kernel<<<(ncl * 32 + 255) / 256, 256, 0, s>>>(xyzq_s, perm, m_bb_c, m_bb_h, counts);
+  APO_LAUNCH_CHECK();
+  tiles_kernel<false><<<(ncl * 32 + 127) / 128, 128, 0, s>>>(
+      m_d, m_cl_col, m_col_start, m_bb_c, m_bb_h, perm, glo2loc, m_excl_ptr, m_excl_idx,
+      m_tile_count, m_tile_start, m_work_start, tiles, masks, work, counts, 0);
+  APO_LAUNCH_CHECK();
+  tile_scan_kernel<<<1, kScanThreads, 0, s>>>(m_tile_count, m_tile_start, m_work_start,
+                                              counts, m_d.tile_cap, m_d.work_cap,
+                                              m_d.tiles_per_work, error);
+  APO_LAUNCH_CHECK();
+  tiles_kernel<true><<<(ncl * 32 + 127) / 128, 128, 0, s>>>(
+      m_d, m_cl_col, m_col_start, m_bb_c, m_bb_h, perm, glo2loc, m_excl_ptr, m_excl_idx,
+      m_tile_count, m_tile_start, m_work_start, tiles, masks, work, counts, m_sys);
+  APO_LAUNCH_CHECK();
+}
+
+void NeighborList::refresh(const float4 *d_xyzq, cudaStream_t s) {
+  refresh_kernel<<<(m_d.slot_cap + 255) / 256, 256, 0, s>>>(d_xyzq, perm, slot_shift, xyzq_s,
+                                                             counts);
+  APO_LAUNCH_CHECK();
+}
+
+void NeighborList::sync_counts(cudaStream_t s) {
+  int c[8];
+  APO_CUDA(cudaMemcpyAsync(c, counts, sizeof(c), cudaMemcpyDeviceToHost, s));
+  APO_CUDA(cudaStreamSynchronize(s));
+  h_counts[0] = c[0];
+  h_counts[1] = c[1];
+  h_counts[2] = c[2];
+}
+
+unsigned NeighborList::read_error(cudaStream_t s) {
+  unsigned e = 0;
+  APO_CUDA(cudaMemcpyAsync(&e, error, sizeof(e), cudaMemcpyDeviceToHost, s));
+  APO_CUDA(cudaStreamSynchronize(s));
+  return e;
+}
+
+bool NeighborList::ensure_capacity(const float4 *d_xyzq, cudaStream_t s, double fill) {
+  build(d_xyzq, s);
+  int c[8];
+  APO_CUDA(cudaMemcpyAsync(c, counts, sizeof(c), cudaMemcpyDeviceToHost, s));
+  APO_CUDA(cudaStreamSynchronize(s));
+  unsigned e = read_error(s);
+  if (e & (kErrColumnOverflow | kErrNaN))
+    throw std::runtime_error("neighbour list: column overflow or non-finite coordinates");
+  bool grew = false;
+  if (c[3] > fill * m_d.tile_cap || c[4] > fill * m_d.work_cap) {
+    m_d.tile_cap = (int)(std::max<double>(c[3], 1) / fill * 1.25) + 1024;
+    m_d.work_cap = (int)(std::max<double>(c[4], 1) / fill * 1.25) + 1024;
+    dalloc(tiles, m_d.tile_cap);
+    dalloc(masks, (size_t)m_d.tile_cap * kTile);
+    dalloc(work, m_d.work_cap);
+    APO_CUDA(cudaMemsetAsync(error, 0, sizeof(unsigned), s));
+    build(d_xyzq, s);
+    APO_CUDA(cudaStreamSynchronize(s));
+    grew = true;
+  }
+  sync_counts(s);
+  return grew;
+}
+
+}  // namespace apo

@@ -1,0 +1,90 @@
+// Tiled neighbour list: column sort into 32-atom clusters, warp-ballot tile
+// search over cluster bounding boxes, per-tile 32x32 exclusion bitmasks.
+//
+// Replaces the reference's CudaNeighborList<32> (sort: src/CudaNeighborListSort.cu,
+// build: src/CudaNeighborListBuild.cu:337-1700).  Differences by design:
+//  * no host round trips: every size lives in device memory, so a rebuild
+//    can sit inside a CUDA graph;
+//  * the atom order inside a column is fully determined by (z, atom index),
+//    so the sorted order, the tile list and the masks are deterministic;
+//  * a tile carries its own periodic image code and its own mask word per
+//    i-lane: bit j of word i set = pair (i, j) is skipped (padding, the lower
+//    triangle of a self tile, or a topological 1-2/1-3/1-4 exclusion).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "common.h"
+
+namespace apo {
+
+struct NbListDims {
+  int natom = 0;
+  int ncx = 1, ncy = 1;           // cell columns in x, y
+  float Lx = 0, Ly = 0, Lz = 0;   // box
+  float rlist = 0;                // list radius (cutnb)
+  int slot_cap = 0;               // padded sorted slots
+  int tile_cap = 0, work_cap = 0;
+  int tiles_per_work = 8;
+  int sort_cap = 4096;            // max atoms in one column
+};
+
+class NeighborList {
+ public:
+  NeighborList() = default;
+  ~NeighborList();
+  NeighborList(const NeighborList &) = delete;
+  NeighborList &operator=(const NeighborList &) = delete;
+
+  // topology-dependent set-up; box/rlist may be changed with set_box
+  void setup(int natom, float Lx, float Ly, float Lz, float rlist,
+             const std::vector<int> &excl_ptr, const std::vector<int> &excl_idx,
+             const int *d_vdwtype, int tiles_per_work = 8);
+  // full rebuild from global-order coordinates (device float4 x,y,z,q)
+  void build(const float4 *d_xyzq, cudaStream_t s);
+  // refresh sorted coordinates from global-order coordinates
+  void refresh(const float4 *d_xyzq, cudaStream_t s);
+  // grow capacities if the last build used more than `fill` of them (sync)
+  bool ensure_capacity(const float4 *d_xyzq, cudaStream_t s, double fill = 0.8);
+
+  const NbListDims &dims() const { return m_d; }
+  int num_columns() const { return m_ncol; }
+  void set_system_index(int sys) { m_sys = sys; }
+  // device arrays
+  int *perm = nullptr;          // slot -> atom (-1 = padding)
+  int *glo2loc = nullptr;       // atom -> slot
+  float4 *slot_shift = nullptr; // image shift added to the atom's coordinates
+  float4 *xyzq_s = nullptr;     // sorted, wrapped coordinates + charge
+  int *type_s = nullptr;        // sorted LJ type
+  int2 *tiles = nullptr;        // (j cluster, image code)
+  unsigned *masks = nullptr;    // 32 words per tile
+  int4 *work = nullptr;         // (i cluster, first tile, end tile, system)
+  int *counts = nullptr;        // [0] slots, [1] tiles, [2] work items
+  unsigned *error = nullptr;    // DeviceError bits
+
+  // host copies of the counts (valid after sync_counts)
+  int h_counts[3] = {0, 0, 0};
+  void sync_counts(cudaStream_t s);
+  unsigned read_error(cudaStream_t s);
+
+ private:
+  void alloc();
+  void release();
+  NbListDims m_d;
+  int m_ncol = 0;
+  int m_sys = 0;
+  const int *m_vdwtype = nullptr;
+  int *m_excl_ptr = nullptr, *m_excl_idx = nullptr;
+  int *m_col_count = nullptr, *m_col_start = nullptr;
+  int *m_atom_col = nullptr, *m_atom_rank = nullptr;
+  float4 *m_atom_shift = nullptr;
+  float *m_tmp_key = nullptr, *m_atom_z = nullptr;
+  int *m_tmp_idx = nullptr;
+  int *m_cl_col = nullptr;
+  float4 *m_bb_c = nullptr, *m_bb_h = nullptr;
+  int *m_tile_count = nullptr, *m_tile_start = nullptr, *m_work_start = nullptr;
+};
+
+}  // namespace apo

@@ -1,0 +1,257 @@
+// Direct-space tile kernel; see nonbonded.h.
+//
+// One warp per work item (an i-cluster and a run of up to tiles_per_work of
+// its j-tiles), persistent grid.  Lane l owns i-atom l for the whole work
+// item: its force lives in registers.  For each tile the 32 j-atoms are
+// staged in shared memory and read back as warp-wide broadcasts, so the pair
+// loop costs one LDS.128 + one LDS.32 + one table LDS.64 per pair and no
+// shuffles.  The j-forces of a tile are combined across the warp with a
+// transpose reduction: 9 shuffles per component for every 8 j-atoms, after
+// which lane L holds the full force of j-atom (L&3)*8 + (L>>2).
+#include "nonbonded.h"
+
+#include <cmath>
+#include <type_traits>
+
+#include "device_util.cuh"
+
+namespace apo {
+
+NbSetup make_nb_setup(double Lx, double Ly, double Lz, double kappa, double roff,
+                      double ron) {
+  NbSetup s;
+  s.Lx = (float)Lx;
+  s.Ly = (float)Ly;
+  s.Lz = (float)Lz;
+  s.roff2 = (float)(roff * roff);
+  s.ron2 = (float)(ron * ron);
+  s.kappa = (float)kappa;
+  s.kappa2 = (float)(kappa * kappa);
+  s.two_kappa_sqrtpi = (float)(2.0 * kappa / std::sqrt(M_PI));
+  // VDW_VFSW constants (src/CudaPMEDirectForce.cu:318-330)
+  double roff3 = roff * roff * roff, ron3 = ron * ron * ron;
+  double roff6 = roff3 * roff3, ron6 = ron3 * ron3;
+  s.roffinv3 = (float)(1.0 / roff3);
+  s.roffinv6 = (float)(1.0 / roff6);
+  if (ron < roff) {
+    s.k6 = (float)(roff3 / (roff3 - ron3));
+    s.k12 = (float)(roff6 / (roff6 - ron6));
+    s.dv6 = (float)(-1.0 / (ron3 * roff3));
+    s.dv12 = (float)(-1.0 / (ron6 * roff6));
+  } else {
+    s.k6 = 1.f;
+    s.k12 = 1.f;
+    s.dv6 = (float)(-1.0 / roff6);
+    s.dv12 = (float)(-1.0 / (roff6 * roff6));
+  }
+  return s;
+}
+
+namespace {
+
+constexpr int kWarps = 4;
+constexpr int kThreads = kWarps * 32;
+
+// sum of v[jj] over the 32 lanes; on return lane L holds the total of
+// jj = L >> 2 (every lane of a quad holds the same value)
+template <typename T>
+__device__ __forceinline__ T transpose_reduce8(T (&v)[8], int lane) {
+  const bool b16 = lane & 16, b8 = lane & 8, b4 = lane & 4;
+  T u[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    T send = b16 ? v[k] : v[k + 4];
+    T keep = b16 ? v[k + 4] : v[k];
+    u[k] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+  }
+  T w[2];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    T send = b8 ? u[k] : u[k + 2];
+    T keep = b8 ? u[k + 2] : u[k];
+    w[k] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+  }
+  T send = b4 ? w[0] : w[1];
+  T z = (b4 ? w[1] : w[0]) + __shfl_xor_sync(0xffffffffu, send, 4);
+  z += __shfl_xor_sync(0xffffffffu, z, 2);
+  z += __shfl_xor_sync(0xffffffffu, z, 1);
+  return z;
+}
+
+template <bool ENERGY, bool PER_PAIR>
+__global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
+  __shared__ float4 sh_xq[kWarps][32];
+  __shared__ int sh_t[kWarps][32];
+  extern __shared__ float2 sh_vdw[];
+  const int T = a.ntype;
+  for (int k = threadIdx.x; k < T * T; k += blockDim.x) sh_vdw[k] = a.vdw[k];
+  __syncthreads();
+
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const int nwork = a.counts[2];
+  const int stride = a.stride;
+  double e_elec = 0.0, e_vdw = 0.0;
+  using Acc = typename std::conditional<PER_PAIR, long long, float>::type;
+
+  for (int w = blockIdx.x * kWarps + wib; w < nwork; w += gridDim.x * kWarps) {
+    const int4 wk = a.work[w];
+    const NbSetup st = a.setups[wk.w];
+    const int islot = wk.x * kTile + lane;
+    const float4 xi = a.xyzq_s[islot];
+    const float qi = xi.w * (float)kCcelec;
+    const int ti = a.type_s[islot] * T;
+    Acc fix = 0, fiy = 0, fiz = 0;
+
+    for (int t = wk.y; t < wk.z; ++t) {
+      const int2 tl = a.tiles[t];
+      float sx, sy, sz;
+      shift_code(tl.y, st.Lx, st.Ly, st.Lz, sx, sy, sz);
+      const unsigned excl = a.masks[(size_t)t * kTile + lane];
+      const int jslot = tl.x * kTile + lane;
+      float4 xj = a.xyzq_s[jslot];
+      xj.x += sx;
+      xj.y += sy;
+      xj.z += sz;
+      __syncwarp();
+      sh_xq[wib][lane] = xj;
+      sh_t[wib][lane] = a.type_s[jslot];
+      __syncwarp();
+
+      Acc fjx = 0, fjy = 0, fjz = 0;  // force of j-atom (lane&3)*8 + (lane>>2)
+#pragma unroll
+      for (int jb = 0; jb < 4; ++jb) {
+        Acc fx[8], fy[8], fz[8];
+#pragma unroll
+        for (int jj = 0; jj < 8; ++jj) {
+          const int j = jb * 8 + jj;
+          const float4 pj = sh_xq[wib][j];
+          const float dx = xi.x - pj.x, dy = xi.y - pj.y, dz = xi.z - pj.z;
+          const float r2 = dx * dx + dy * dy + dz * dz;
+          fx[jj] = 0;
+          fy[jj] = 0;
+          fz[jj] = 0;
+          if (!((excl >> j) & 1u) && r2 < st.roff2) {
+            const float rinv = rsqrtf(r2);
+            const float r = r2 * rinv;
+            const float rinv2 = rinv * rinv;
+            // erfc-Ewald (src/CudaDirectForceKernels.cu:479-489)
+            const float qq = qi * pj.w;
+            const float erfc_v = erfcf(st.kappa * r);
+            const float exp_v = __expf(-st.kappa2 * r2);
+            const float e_el = qq * erfc_v * rinv;
+            const float fr_el = -qq * st.two_kappa_sqrtpi * exp_v - e_el;
+            // VDW_VFSW (src/CudaDirectForceKernels.cu:263-286)
+            const float2 cc = sh_vdw[ti + sh_t[wib][j]];
+            const float rinv3 = rinv * rinv2, rinv6 = rinv3 * rinv3;
+            const bool sw = r2 > st.ron2;
+            const float A6 = sw ? st.k6 : 1.f, B6 = sw ? st.roffinv3 : 0.f;
+            const float A12 = sw ? st.k12 : 1.f, B12 = sw ? st.roffinv6 : 0.f;
+            const float t6 = rinv3 - B6, t12 = rinv6 - B12;
+            const float fr_vdw = cc.x * A6 * t6 * rinv3 - cc.y * A12 * t12 * rinv6;
+            const float fij = (fr_vdw + fr_el) * rinv2;
+            if (ENERGY) {
+              const float C6 = sw ? 0.f : st.dv6, C12 = sw ? 0.f : st.dv12;
+              e_elec += (double)e_el;
+              e_vdw += (double)((1.f / 12.f) * cc.y * (A12 * t12 * t12 + C12) -
+                                (1.f / 6.f) * cc.x * (A6 * t6 * t6 + C6));
+            }
+            if (PER_PAIR) {
+              const long long gx = to_fixed_force(fij * dx);
+              const long long gy = to_fixed_force(fij * dy);
+              const long long gz = to_fixed_force(fij * dz);
+              fix += gx;
+              fiy += gy;
+              fiz += gz;
+              fx[jj] = -gx;
+              fy[jj] = -gy;
+              fz[jj] = -gz;
+            } else {
+              fix += fij * dx;
+              fiy += fij * dy;
+              fiz += fij * dz;
+              fx[jj] = -fij * dx;
+              fy[jj] = -fij * dy;
+              fz[jj] = -fij * dz;
+            }
+          }
+        }
+        const Acc rx = transpose_reduce8(fx, lane);
+        const Acc ry = transpose_reduce8(fy, lane);
+        const Acc rz = transpose_reduce8(fz, lane);
+        if ((lane & 3) == jb) {
+          fjx = rx;
+          fjy = ry;
+          fjz = rz;
+        }
+      }
+      const int jown = tl.x * kTile + (lane & 3) * 8 + (lane >> 2);
+      if (PER_PAIR) {
+        add_fixed(a.force + jown, (long long)fjx);
+        add_fixed(a.force + stride + jown, (long long)fjy);
+        add_fixed(a.force + 2 * stride + jown, (long long)fjz);
+      } else {
+        add_fixed(a.force + jown, to_fixed_force((float)fjx));
+        add_fixed(a.force + stride + jown, to_fixed_force((float)fjy));
+        add_fixed(a.force + 2 * stride + jown, to_fixed_force((float)fjz));
+      }
+    }
+    if (PER_PAIR) {
+      add_fixed(a.force + islot, (long long)fix);
+      add_fixed(a.force + stride + islot, (long long)fiy);
+      add_fixed(a.force + 2 * stride + islot, (long long)fiz);
+    } else {
+      add_fixed(a.force + islot, to_fixed_force((float)fix));
+      add_fixed(a.force + stride + islot, to_fixed_force((float)fiy));
+      add_fixed(a.force + 2 * stride + islot, to_fixed_force((float)fiz));
+    }
+  }
+  if (ENERGY) {
+    // per-lane sums rounded to fixed point, then integer sums: order-free
+    long long ie = __double2ll_rn(e_elec * kEnergyScale);
+    long long iv = __double2ll_rn(e_vdw * kEnergyScale);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      ie += __shfl_xor_sync(0xffffffffu, ie, o);
+      iv += __shfl_xor_sync(0xffffffffu, iv, o);
+    }
+    if (lane == 0) {
+      add_fixed(a.energy + kEElec, ie);
+      add_fixed(a.energy + kEVdw, iv);
+    }
+  }
+}
+
+template <bool E, bool P>
+void launch_t(const NbArgs &a, cudaStream_t s) {
+  static int grid = 0;
+  size_t sm = (size_t)a.ntype * a.ntype * sizeof(float2);
+  if (!grid) {
+    int dev, nsm, per = 0;
+    APO_CUDA(cudaGetDevice(&dev));
+    APO_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    APO_CUDA(cudaFuncSetAttribute(nb_kernel<E, P>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+    APO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, nb_kernel<E, P>, kThreads,
+                                                           64 * 1024 > sm ? sm : 64 * 1024));
+    grid = nsm * (per > 0 ? per : 1);
+  }
+  nb_kernel<E, P><<<grid, kThreads, sm, s>>>(a);
+  APO_LAUNCH_CHECK();
+}
+
+}  // namespace
+
+void launch_nonbonded(const NbArgs &a, bool energy, bool per_pair, cudaStream_t s) {
+  if (a.ntype * a.ntype * sizeof(float2) > 64 * 1024)
+    throw std::invalid_argument("nonbonded: too many LJ types for the shared table");
+  if (per_pair) {
+    if (energy) launch_t<true, true>(a, s);
+    else launch_t<false, true>(a, s);
+  } else {
+    if (energy) launch_t<true, false>(a, s);
+    else launch_t<false, false>(a, s);
+  }
+}
+
+}  // namespace apo

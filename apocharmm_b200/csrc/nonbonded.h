@@ -1,0 +1,42 @@
+// Direct-space erfc-Ewald + CHARMM force-switched LJ over neighbour tiles.
+//
+// Replaces the reference's calcForceKernel (include/CudaDirectForce_util.h:18-333,
+// pair functions src/CudaDirectForceKernels.cu:209-489; VDW_VFSW, EWALD).
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace apo {
+
+struct NbSetup {
+  float Lx, Ly, Lz;
+  float roff2, ron2;
+  float kappa, kappa2, two_kappa_sqrtpi;
+  float k6, k12, dv6, dv12, roffinv3, roffinv6;
+};
+
+NbSetup make_nb_setup(double Lx, double Ly, double Lz, double kappa, double roff,
+                      double ron);
+
+struct NbArgs {
+  const float4 *xyzq_s;
+  const int *type_s;
+  const int2 *tiles;
+  const unsigned *masks;
+  const int4 *work;
+  const int *counts;      // [2] = number of work items
+  const float2 *vdw;      // ntype x ntype (6 c6, 12 c12)
+  int ntype;
+  long long *force;       // SoA fixed point in sorted slot order
+  int stride;
+  long long *energy;      // energy slots (elec, vdw used)
+  const NbSetup *setups;  // per system (indexed by work item .w)
+};
+
+// per_pair: round every pair contribution to 64-bit fixed point before it is
+// summed (order-independent, the reference's accumulation,
+// include/gpu_utils.h:281-312); otherwise FP32 sums per atom and tile are
+// rounded once (deterministic for a given tile list).
+void launch_nonbonded(const NbArgs &a, bool energy, bool per_pair, cudaStream_t s);
+
+}  // namespace apo

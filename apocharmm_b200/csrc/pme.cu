@@ -1,0 +1,732 @@
+// PME reciprocal-space kernels; see pme.h.
+#include "pme.h"
+
+#include <algorithm>
+#include <cmath>
+#include <functional>
+#include <numeric>
+#include <stdexcept>
+#include <vector>
+
+#include "common.h"
+#include "device_util.cuh"
+
+namespace apo {
+namespace {
+
+constexpr int kPlaneThreads = 512;
+constexpr int kPencilThreads = 256;
+constexpr int kPencilTX = 16;
+
+// ------------------------------------------------------------------------
+// B-spline weights (Essmann et al. recursion, the reference's calc_one_theta,
+// src/CudaPMERecip.cu:438-470)
+// ------------------------------------------------------------------------
+template <int ORDER>
+__device__ __forceinline__ void bspline(float w, float (&th)[ORDER], float (&dth)[ORDER]) {
+  th[ORDER - 1] = 0.f;
+  th[1] = w;
+  th[0] = 1.f - w;
+#pragma unroll
+  for (int k = 3; k <= ORDER - 1; ++k) {
+    const float div = 1.f / (float)(k - 1);
+    th[k - 1] = div * w * th[k - 2];
+#pragma unroll
+    for (int j = 1; j <= k - 2; ++j)
+      th[k - j - 1] = div * ((w + j) * th[k - j - 2] + (k - j - w) * th[k - j - 1]);
+    th[0] = div * (1.f - w) * th[0];
+  }
+  dth[0] = -th[0];
+#pragma unroll
+  for (int j = 1; j < ORDER; ++j) dth[j] = th[j - 1] - th[j];
+  const float div = 1.f / (float)(ORDER - 1);
+  th[ORDER - 1] = div * w * th[ORDER - 2];
+#pragma unroll
+  for (int j = 1; j <= ORDER - 2; ++j)
+    th[ORDER - j - 1] =
+        div * ((w + j) * th[ORDER - j - 2] + (ORDER - j - w) * th[ORDER - j - 1]);
+  th[0] = div * (1.f - w) * th[0];
+}
+
+// grid anchoring of the reference (include/cuda_pme_spread.h:64-81):
+// w = x/L + 2, fr = n (w - (floor(w+0.5) - 0.5)), points floor(fr)+0..p-1
+__device__ __forceinline__ void anchor(float x, float recip, int n, int &i0, float &w) {
+  float t = x * recip + 2.0f;
+  float fr = (float)n * (t - (floorf(t + 0.5f) - 0.5f));
+  i0 = (int)fr;
+  w = fr - (float)i0;
+  // non-finite or exploded coordinates must not index outside the grid
+  i0 = min(max(i0, 0), n - 1);
+}
+
+// ------------------------------------------------------------------------
+// small DFTs
+// ------------------------------------------------------------------------
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// cos / sin of 2*pi*k/R for the radices used (exact mathematical constants)
+__device__ __forceinline__ constexpr float rcos(int R, int k) {
+  return R == 3 ? (k == 0 ? 1.f : -0.5f)
+       : R == 5 ? (k == 0 ? 1.f : (k == 1 || k == 4) ? 0.30901699437494745f : -0.8090169943749475f)
+       : R == 6 ? (k == 0 ? 1.f : (k == 1 || k == 5) ? 0.5f : (k == 2 || k == 4) ? -0.5f : -1.f)
+       : R == 7 ? (k == 0 ? 1.f : (k == 1 || k == 6) ? 0.6234898018587336f
+                              : (k == 2 || k == 5) ? -0.22252093395631434f : -0.9009688679024191f)
+       : R == 8 ? (k == 0 ? 1.f : (k == 1 || k == 7) ? 0.7071067811865476f
+                              : (k == 2 || k == 6) ? 0.f : (k == 3 || k == 5) ? -0.7071067811865476f : -1.f)
+       : 1.f;
+}
+__device__ __forceinline__ constexpr float rsin(int R, int k) {
+  return R == 3 ? (k == 0 ? 0.f : k == 1 ? 0.8660254037844386f : -0.8660254037844386f)
+       : R == 5 ? (k == 0 ? 0.f : k == 1 ? 0.9510565162951535f : k == 2 ? 0.5877852522924731f
+                  : k == 3 ? -0.5877852522924731f : -0.9510565162951535f)
+       : R == 6 ? (k == 0 || k == 3 ? 0.f : (k == 1 || k == 2) ? 0.8660254037844386f : -0.8660254037844386f)
+       : R == 7 ? (k == 0 ? 0.f : k == 1 ? 0.7818314824680298f : k == 2 ? 0.9749279121818236f
+                  : k == 3 ? 0.4338837391175582f : k == 4 ? -0.4338837391175582f
+                  : k == 5 ? -0.9749279121818236f : -0.7818314824680298f)
+       : R == 8 ? (k == 0 || k == 4 ? 0.f : (k == 1 || k == 3) ? 0.7071067811865476f
+                  : k == 2 ? 1.f : (k == 5 || k == 7) ? -0.7071067811865476f : -1.f)
+       : 0.f;
+}
+
+// y_k = sum_q x_q exp(sign * 2 pi i q k / R)
+template <int R>
+__device__ __forceinline__ void dft(float2 (&x)[R], float sign) {
+  if (R == 2) {
+    float2 a = x[0], b = x[1];
+    x[0] = make_float2(a.x + b.x, a.y + b.y);
+    x[1] = make_float2(a.x - b.x, a.y - b.y);
+  } else if (R == 4) {
+    float2 s02 = make_float2(x[0].x + x[2].x, x[0].y + x[2].y);
+    float2 d02 = make_float2(x[0].x - x[2].x, x[0].y - x[2].y);
+    float2 s13 = make_float2(x[1].x + x[3].x, x[1].y + x[3].y);
+    float2 d13 = make_float2(x[1].x - x[3].x, x[1].y - x[3].y);
+    // sign * i * d13
+    float2 id13 = make_float2(-sign * d13.y, sign * d13.x);
+    x[0] = make_float2(s02.x + s13.x, s02.y + s13.y);
+    x[2] = make_float2(s02.x - s13.x, s02.y - s13.y);
+    x[1] = make_float2(d02.x + id13.x, d02.y + id13.y);
+    x[3] = make_float2(d02.x - id13.x, d02.y - id13.y);
+  } else {
+    float2 y[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      float re = 0.f, im = 0.f;
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const int idx = (q * k) % R;
+        const float c = rcos(R, idx), s = sign * rsin(R, idx);
+        re += x[q].x * c - x[q].y * s;
+        im += x[q].x * s + x[q].y * c;
+      }
+      y[k] = make_float2(re, im);
+    }
+#pragma unroll
+    for (int k = 0; k < R; ++k) x[k] = y[k];
+  }
+}
+
+__device__ __forceinline__ float2 twiddle(const float2 *tw, int idx, float sign) {
+  float2 w = tw[idx];
+  if (sign > 0.f) w.y = -w.y;
+  return w;
+}
+
+// One decimation-in-frequency stage (butterfly, then twiddle) on sub-blocks
+// of length m of every line.  Lines start at buf + line*lstride; element e of
+// a line is at e*estride.
+template <int R>
+__device__ void dif_stage(float2 *buf, int nlines, int lstride, int estride, int n, int m,
+                          const float2 *tw, float sign) {
+  const int mr = m / R, per_line = n / R, total = nlines * per_line, nm = n / m;
+  for (int b = threadIdx.x; b < total; b += blockDim.x) {
+    const int line = b / per_line, rem = b - line * per_line;
+    const int blk = rem / mr, j = rem - blk * mr;
+    float2 *p = buf + line * lstride + (blk * m + j) * estride;
+    float2 x[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) x[q] = p[q * mr * estride];
+    dft<R>(x, sign);
+    if (j > 0) {
+#pragma unroll
+      for (int k = 1; k < R; ++k) x[k] = cmul(x[k], twiddle(tw, (j * k * nm) % n, sign));
+    }
+#pragma unroll
+    for (int k = 0; k < R; ++k) p[k * mr * estride] = x[k];
+  }
+}
+
+// One decimation-in-time stage (twiddle, then butterfly).
+template <int R>
+__device__ void dit_stage(float2 *buf, int nlines, int lstride, int estride, int n, int m,
+                          const float2 *tw, float sign) {
+  const int mr = m / R, per_line = n / R, total = nlines * per_line, nm = n / m;
+  for (int b = threadIdx.x; b < total; b += blockDim.x) {
+    const int line = b / per_line, rem = b - line * per_line;
+    const int blk = rem / mr, j = rem - blk * mr;
+    float2 *p = buf + line * lstride + (blk * m + j) * estride;
+    float2 x[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) x[k] = p[k * mr * estride];
+    if (j > 0) {
+#pragma unroll
+      for (int k = 1; k < R; ++k) x[k] = cmul(x[k], twiddle(tw, (j * k * nm) % n, sign));
+    }
+    dft<R>(x, sign);
+#pragma unroll
+    for (int q = 0; q < R; ++q) p[q * mr * estride] = x[q];
+  }
+}
+
+template <bool DIF>
+__device__ __forceinline__ void stage(int R, float2 *buf, int nl, int ls, int es, int n, int m,
+                                      const float2 *tw, float sign) {
+  switch (R) {
+    case 2: DIF ? dif_stage<2>(buf, nl, ls, es, n, m, tw, sign) : dit_stage<2>(buf, nl, ls, es, n, m, tw, sign); break;
+    case 3: DIF ? dif_stage<3>(buf, nl, ls, es, n, m, tw, sign) : dit_stage<3>(buf, nl, ls, es, n, m, tw, sign); break;
+    case 4: DIF ? dif_stage<4>(buf, nl, ls, es, n, m, tw, sign) : dit_stage<4>(buf, nl, ls, es, n, m, tw, sign); break;
+    case 5: DIF ? dif_stage<5>(buf, nl, ls, es, n, m, tw, sign) : dit_stage<5>(buf, nl, ls, es, n, m, tw, sign); break;
+    case 6: DIF ? dif_stage<6>(buf, nl, ls, es, n, m, tw, sign) : dit_stage<6>(buf, nl, ls, es, n, m, tw, sign); break;
+    case 7: DIF ? dif_stage<7>(buf, nl, ls, es, n, m, tw, sign) : dit_stage<7>(buf, nl, ls, es, n, m, tw, sign); break;
+    case 8: DIF ? dif_stage<8>(buf, nl, ls, es, n, m, tw, sign) : dit_stage<8>(buf, nl, ls, es, n, m, tw, sign); break;
+    default: break;
+  }
+}
+
+// natural order in, digit-reversed out
+__device__ void fft_dif(float2 *buf, int nl, int ls, int es, const FftAxis &a, const float2 *tw,
+                        float sign) {
+  int m = a.n;
+  for (int s = 0; s < a.nrad; ++s) {
+    stage<true>(a.radix[s], buf, nl, ls, es, a.n, m, tw, sign);
+    __syncthreads();
+    m /= a.radix[s];
+  }
+}
+// digit-reversed in, natural order out
+__device__ void fft_dit(float2 *buf, int nl, int ls, int es, const FftAxis &a, const float2 *tw,
+                        float sign) {
+  int m = 1;
+  for (int s = a.nrad - 1; s >= 0; --s) {
+    m *= a.radix[s];
+    stage<false>(a.radix[s], buf, nl, ls, es, a.n, m, tw, sign);
+    __syncthreads();
+  }
+}
+
+// natural index -> position in the output of fft_dif
+__device__ __forceinline__ int dig_rev(int x, const FftAxis &a) {
+  int p = 0, m = a.n;
+  for (int s = 0; s < a.nrad; ++s) {
+    const int R = a.radix[s];
+    m /= R;
+    p += (x % R) * m;
+    x /= R;
+  }
+  return p;
+}
+// position in the output of fft_dif -> natural index
+__device__ __forceinline__ int dig_unrev(int p, const FftAxis &a) {
+  int k = 0, mult = 1, m = a.n;
+  for (int s = 0; s < a.nrad; ++s) {
+    const int R = a.radix[s];
+    m /= R;
+    const int d = p / m;
+    p -= d * m;
+    k += d * mult;
+    mult *= R;
+  }
+  return k;
+}
+
+// ------------------------------------------------------------------------
+// spread
+// ------------------------------------------------------------------------
+template <int ORDER>
+__global__ void __launch_bounds__(128) spread_kernel(const float4 *__restrict__ xyzq,
+                                                     const int *__restrict__ counts, PmeDims d,
+                                                     int *__restrict__ qgrid) {
+  constexpr int P3 = ORDER * ORDER * ORDER;
+  __shared__ int sh_i[3][32];
+  __shared__ float sh_q[32];
+  __shared__ float sh_th[3][32][ORDER];
+  const int nslot = counts ? counts[0] : 0;
+  const int s0 = blockIdx.x * 32;
+  if (s0 >= nslot) return;
+  if (threadIdx.x < 32) {
+    const int s = s0 + threadIdx.x;
+    float q = 0.f;
+    if (s < nslot) {
+      const float4 p = xyzq[s];
+      q = p.w;
+      float th[ORDER], dth[ORDER], w;
+      int i0;
+      anchor(p.x, 1.f / d.Lx, d.nx, i0, w);
+      bspline<ORDER>(w, th, dth);
+      sh_i[0][threadIdx.x] = i0;
+#pragma unroll
+      for (int k = 0; k < ORDER; ++k) sh_th[0][threadIdx.x][k] = th[k];
+      anchor(p.y, 1.f / d.Ly, d.ny, i0, w);
+      bspline<ORDER>(w, th, dth);
+      sh_i[1][threadIdx.x] = i0;
+#pragma unroll
+      for (int k = 0; k < ORDER; ++k) sh_th[1][threadIdx.x][k] = th[k];
+      anchor(p.z, 1.f / d.Lz, d.nz, i0, w);
+      bspline<ORDER>(w, th, dth);
+      sh_i[2][threadIdx.x] = i0;
+#pragma unroll
+      for (int k = 0; k < ORDER; ++k) sh_th[2][threadIdx.x][k] = th[k];
+    }
+    sh_q[threadIdx.x] = q;
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < 32 * P3; k += blockDim.x) {
+    const int a = k / P3, pt = k - a * P3;
+    const float q = sh_q[a];
+    if (q == 0.f) continue;
+    const int xa = pt % ORDER, yb = (pt / ORDER) % ORDER, zc = pt / (ORDER * ORDER);
+    int x = sh_i[0][a] + xa, y = sh_i[1][a] + yb, z = sh_i[2][a] + zc;
+    if (x >= d.nx) x -= d.nx;
+    if (y >= d.ny) y -= d.ny;
+    if (z >= d.nz) z -= d.nz;
+    const float v = q * sh_th[0][a][xa] * sh_th[1][a][yb] * sh_th[2][a][zc];
+    atomicAdd(&qgrid[x + d.nx * (y + d.ny * z)], __float2int_rn(v * kGridScale));
+  }
+}
+
+// ------------------------------------------------------------------------
+// plane transforms
+// ------------------------------------------------------------------------
+__global__ void __launch_bounds__(kPlaneThreads) plane_fwd_kernel(PmeDims d, int *__restrict__ qgrid,
+                                                                  float2 *__restrict__ cgrid,
+                                                                  const float2 *__restrict__ twx,
+                                                                  const float2 *__restrict__ twy) {
+  extern __shared__ float2 buf[];
+  const int nx = d.nx, ny = d.ny, nxc = d.nxc, rowp = nx + 2, h = nx / 2;
+  const int z = blockIdx.x;
+  int *plane = qgrid + (size_t)z * nx * ny;
+  for (int idx = threadIdx.x; idx < nx * ny; idx += blockDim.x) {
+    const int y = idx / nx, x = idx - y * nx;
+    const int v = plane[idx];
+    plane[idx] = 0;  // ready for the next spread
+    float *slot = reinterpret_cast<float *>(&buf[(y >> 1) * rowp + dig_rev(x, d.ax)]);
+    slot[y & 1] = (float)v * kInvGridScale;
+  }
+  __syncthreads();
+  fft_dit(buf, ny / 2, rowp, 1, d.ax, twx, -1.f);
+  // split the packed rows into the two half spectra, in place
+  const int ngrp = (h + 1) / 2 + 1;
+  for (int idx = threadIdx.x; idx < (ny / 2) * ngrp; idx += blockDim.x) {
+    const int r = idx / ngrp, g = idx - r * ngrp;
+    float2 *b = buf + r * rowp;
+    if (g == ngrp - 1) {
+      const float2 Z = b[h];
+      b[h] = make_float2(Z.x, 0.f);
+      b[nxc + h] = make_float2(Z.y, 0.f);
+    } else {
+      const int k1 = g, k2 = h - 1 - g;
+      const float2 Z1 = b[k1], M1 = b[(nx - k1) % nx];
+      const float2 Z2 = b[k2], M2 = b[nx - k2];
+      const float2 A1 = make_float2(0.5f * (Z1.x + M1.x), 0.5f * (Z1.y - M1.y));
+      const float2 B1 = make_float2(0.5f * (Z1.y + M1.y), -0.5f * (Z1.x - M1.x));
+      const float2 A2 = make_float2(0.5f * (Z2.x + M2.x), 0.5f * (Z2.y - M2.y));
+      const float2 B2 = make_float2(0.5f * (Z2.y + M2.y), -0.5f * (Z2.x - M2.x));
+      b[k1] = A1;
+      b[nxc + k1] = B1;
+      if (k2 != k1) {
+        b[k2] = A2;
+        b[nxc + k2] = B2;
+      }
+    }
+  }
+  __syncthreads();
+  fft_dif(buf, nxc, 1, nxc, d.ay, twy, -1.f);
+  float2 *out = cgrid + (size_t)z * ny * nxc;
+  for (int idx = threadIdx.x; idx < ny * nxc; idx += blockDim.x) out[idx] = buf[idx];
+}
+
+__global__ void __launch_bounds__(kPlaneThreads) plane_inv_kernel(PmeDims d,
+                                                                  const float2 *__restrict__ cgrid,
+                                                                  float *__restrict__ phi,
+                                                                  const float2 *__restrict__ twx,
+                                                                  const float2 *__restrict__ twy) {
+  extern __shared__ float2 buf[];
+  const int nx = d.nx, ny = d.ny, nxc = d.nxc, rowp = nx + 2, h = nx / 2;
+  const int z = blockIdx.x;
+  const float2 *in = cgrid + (size_t)z * ny * nxc;
+  for (int idx = threadIdx.x; idx < ny * nxc; idx += blockDim.x) buf[idx] = in[idx];
+  __syncthreads();
+  fft_dit(buf, nxc, 1, nxc, d.ay, twy, 1.f);
+  // pack pairs of half spectra into one complex row, in place
+  const int ngrp = (h + 1) / 2 + 1;
+  for (int idx = threadIdx.x; idx < (ny / 2) * ngrp; idx += blockDim.x) {
+    const int r = idx / ngrp, g = idx - r * ngrp;
+    float2 *b = buf + r * rowp;
+    if (g == ngrp - 1) {
+      const float2 A = b[h], B = b[nxc + h];
+      b[h] = make_float2(A.x - B.y, A.y + B.x);
+    } else {
+      const int k1 = g, k2 = h - 1 - g;
+      const float2 A1 = b[k1], B1 = b[nxc + k1], A2 = b[k2], B2 = b[nxc + k2];
+      b[k1] = make_float2(A1.x - B1.y, A1.y + B1.x);
+      if (k1 > 0) b[nx - k1] = make_float2(A1.x + B1.y, -A1.y + B1.x);
+      if (k2 != k1) {
+        b[k2] = make_float2(A2.x - B2.y, A2.y + B2.x);
+        if (k2 > 0) b[nx - k2] = make_float2(A2.x + B2.y, -A2.y + B2.x);
+      }
+    }
+  }
+  __syncthreads();
+  fft_dif(buf, ny / 2, rowp, 1, d.ax, twx, 1.f);
+  float *out = phi + (size_t)z * nx * ny;
+  for (int idx = threadIdx.x; idx < (ny / 2) * nx; idx += blockDim.x) {
+    const int r = idx / nx, p = idx - r * nx;
+    const int x = dig_unrev(p, d.ax);
+    const float2 v = buf[r * rowp + p];
+    out[(2 * r) * nx + x] = v.x;
+    out[(2 * r + 1) * nx + x] = v.y;
+  }
+}
+
+// ------------------------------------------------------------------------
+// z pencils: FFT, influence function, inverse FFT
+// ------------------------------------------------------------------------
+template <bool ENERGY, typename FT>
+__global__ void __launch_bounds__(kPencilThreads) pencil_kernel(PmeDims d, float2 *__restrict__ cgrid,
+                                                                const float2 *__restrict__ twz,
+                                                                const float *__restrict__ prefac,
+                                                                const double *__restrict__ prefac_d,
+                                                                long long *__restrict__ energy) {
+  __shared__ float2 buf[256 * kPencilTX];
+  __shared__ double sh_e[kPencilThreads / 32];
+  const int nx = d.nx, ny = d.ny, nz = d.nz, nxc = d.nxc;
+  const int tiles_x = (nxc + kPencilTX - 1) / kPencilTX;
+  const int py = blockIdx.x / tiles_x, x0 = (blockIdx.x - py * tiles_x) * kPencilTX;
+  for (int idx = threadIdx.x; idx < nz * kPencilTX; idx += blockDim.x) {
+    const int zz = idx / kPencilTX, xt = idx - zz * kPencilTX, kx = x0 + xt;
+    buf[idx] = kx < nxc ? cgrid[((size_t)zz * ny + py) * nxc + kx] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  fft_dif(buf, kPencilTX, 1, kPencilTX, d.az, twz, -1.f);
+  const int ky = dig_unrev(py, d.ay);
+  const int nf1 = nx / 2 + (nx & 1), nf2 = ny / 2 + (ny & 1), nf3 = nz / 2 + (nz & 1);
+  const FT m2 = (FT)(ky >= nf2 ? ky - ny : ky) / (FT)d.Ly;
+  const FT pi = (FT)3.14159265358979323846;
+  const FT fac = pi * pi / ((FT)d.kappa * (FT)d.kappa);
+  const FT piv_inv = (FT)1 / ((FT)d.Lx * (FT)d.Ly * (FT)d.Lz * pi);
+  const FT *pf = sizeof(FT) == 8 ? reinterpret_cast<const FT *>(prefac_d)
+                                 : reinterpret_cast<const FT *>(prefac);
+  const FT pyv = pf[nx + ky];
+  double e = 0.0;
+  for (int idx = threadIdx.x; idx < nz * kPencilTX; idx += blockDim.x) {
+    const int pz = idx / kPencilTX, xt = idx - pz * kPencilTX, kx = x0 + xt;
+    if (kx >= nxc) continue;
+    const int kz = dig_unrev(pz, d.az);
+    FT eterm = 0;
+    if (kx != 0 || ky != 0 || kz != 0) {
+      const FT m1 = (FT)(kx >= nf1 ? kx - nx : kx) / (FT)d.Lx;
+      const FT m3 = (FT)(kz >= nf3 ? kz - nz : kz) / (FT)d.Lz;
+      const FT msq = m1 * m1 + m2 * m2 + m3 * m3;
+      eterm = exp(-fac * msq) * piv_inv * pf[kx] * pyv * pf[nx + ny + kz] / msq;
+    }
+    const float2 q = buf[idx];
+    if (ENERGY) {
+      const FT mult = kx >= 1 ? (FT)2 : (FT)1;
+      e += (double)(mult * eterm * ((FT)q.x * q.x + (FT)q.y * q.y));
+    }
+    buf[idx] = make_float2((float)(q.x * eterm), (float)(q.y * eterm));
+  }
+  __syncthreads();
+  fft_dit(buf, kPencilTX, 1, kPencilTX, d.az, twz, 1.f);
+  for (int idx = threadIdx.x; idx < nz * kPencilTX; idx += blockDim.x) {
+    const int zz = idx / kPencilTX, xt = idx - zz * kPencilTX, kx = x0 + xt;
+    if (kx < nxc) cgrid[((size_t)zz * ny + py) * nxc + kx] = buf[idx];
+  }
+  if (ENERGY) {
+    e = warp_sum(e);
+    if ((threadIdx.x & 31) == 0) sh_e[threadIdx.x >> 5] = e;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < kPencilThreads / 32; ++w) t += sh_e[w];
+      add_energy(energy + kEEwks, 0.5 * kCcelec * t);
+    }
+  }
+}
+
+// ------------------------------------------------------------------------
+// gather: 8 threads per atom, (y,z) pairs split across the 8, x loop inside
+// ------------------------------------------------------------------------
+template <int ORDER>
+__global__ void __launch_bounds__(256) gather_kernel(const float4 *__restrict__ xyzq,
+                                                     const int *__restrict__ counts, PmeDims d,
+                                                     const float *__restrict__ phi,
+                                                     long long *__restrict__ force, int stride) {
+  const int nslot = counts[0];
+  const int s = blockIdx.x * 32 + (threadIdx.x >> 3);
+  const int sub = threadIdx.x & 7;
+  float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (s < nslot) p = xyzq[s];
+  float thx[ORDER], thy[ORDER], thz[ORDER], dx[ORDER], dy[ORDER], dz[ORDER], w;
+  int ix, iy, iz;
+  anchor(p.x, 1.f / d.Lx, d.nx, ix, w);
+  bspline<ORDER>(w, thx, dx);
+  anchor(p.y, 1.f / d.Ly, d.ny, iy, w);
+  bspline<ORDER>(w, thy, dy);
+  anchor(p.z, 1.f / d.Lz, d.nz, iz, w);
+  bspline<ORDER>(w, thz, dz);
+  float f1 = 0.f, f2 = 0.f, f3 = 0.f;
+  if (s < nslot && p.w != 0.f) {
+    for (int k = sub; k < ORDER * ORDER; k += 8) {
+      const int b = k % ORDER, c = k / ORDER;
+      int y = iy + b, z = iz + c;
+      if (y >= d.ny) y -= d.ny;
+      if (z >= d.nz) z -= d.nz;
+      const float *row = phi + ((size_t)z * d.ny + y) * d.nx;
+      float tyb = 0.f, dyb = 0.f, tzc = 0.f, dzc = 0.f;
+#pragma unroll
+      for (int t = 0; t < ORDER; ++t) {
+        if (t == b) { tyb = thy[t]; dyb = dy[t]; }
+        if (t == c) { tzc = thz[t]; dzc = dz[t]; }
+      }
+      float sx = 0.f, sdx = 0.f;
+#pragma unroll
+      for (int a = 0; a < ORDER; ++a) {
+        int x = ix + a;
+        if (x >= d.nx) x -= d.nx;
+        const float v = __ldg(row + x);
+        sx += thx[a] * v;
+        sdx += dx[a] * v;
+      }
+      f1 += sdx * tyb * tzc;
+      f2 += sx * dyb * tzc;
+      f3 += sx * tyb * dzc;
+    }
+  }
+#pragma unroll
+  for (int o = 4; o > 0; o >>= 1) {
+    f1 += __shfl_xor_sync(0xffffffffu, f1, o);
+    f2 += __shfl_xor_sync(0xffffffffu, f2, o);
+    f3 += __shfl_xor_sync(0xffffffffu, f3, o);
+  }
+  if (sub == 0 && s < nslot && p.w != 0.f) {
+    const float qc = p.w * (float)kCcelec;
+    add_fixed(force + s, to_fixed_force(qc * (float)d.nx / d.Lx * f1));
+    add_fixed(force + stride + s, to_fixed_force(qc * (float)d.ny / d.Ly * f2));
+    add_fixed(force + 2 * stride + s, to_fixed_force(qc * (float)d.nz / d.Lz * f3));
+  }
+}
+
+// B-spline moduli as the reference's dftmod (src/CudaPMERecip.cu:2656-2678)
+void bspline_moduli(int n, int order, std::vector<double> &out) {
+  std::vector<double> th(order), arr(n + order + 2, 0.0);
+  // weights at w = 0
+  th[order - 1] = 0.0;
+  th[1] = 0.0;
+  th[0] = 1.0;
+  for (int k = 3; k <= order - 1; ++k) {
+    double div = 1.0 / (k - 1);
+    th[k - 1] = 0.0;
+    for (int j = 1; j <= k - 2; ++j) th[k - j - 1] = div * (j * th[k - j - 2] + (k - j) * th[k - j - 1]);
+    th[0] = div * th[0];
+  }
+  {
+    double div = 1.0 / (order - 1);
+    th[order - 1] = 0.0;
+    for (int j = 1; j <= order - 2; ++j)
+      th[order - j - 1] = div * (j * th[order - j - 2] + (order - j) * th[order - j - 1]);
+    th[0] = div * th[0];
+  }
+  for (int i = 2; i <= order + 1; ++i) arr[i - 1] = th[i - 2];
+  out.assign(n, 0.0);
+  for (int k = 0; k < n; ++k) {
+    double s1 = 0, s2 = 0;
+    for (int j = 0; j < n - 1; ++j) {
+      double a = 2.0 * M_PI * k * j / n;
+      s1 += arr[j] * std::cos(a);
+      s2 += arr[j] * std::sin(a);
+    }
+    out[k] = s1 * s1 + s2 * s2;
+  }
+  for (int k = 0; k < n; ++k)
+    if (out[k] < 1e-10) out[k] = 0.5 * (out[(k - 1 + n) % n] + out[(k + 1) % n]);
+  for (int k = 0; k < n; ++k) out[k] = 1.0 / out[k];
+}
+
+template <typename T>
+void dalloc(T *&p, size_t n) {
+  if (p) cudaFree(p);
+  p = nullptr;
+  if (n) APO_CUDA(cudaMalloc(&p, n * sizeof(T)));
+}
+
+}  // namespace
+
+FftAxis Pme::plan_axis(int n) {
+  // fewest stages, then smallest total radix
+  std::vector<int> best;
+  std::vector<int> cur;
+  std::function<void(int)> rec = [&](int m) {
+    if (m == 1) {
+      if (best.empty() || cur.size() < best.size() ||
+          (cur.size() == best.size() &&
+           std::accumulate(cur.begin(), cur.end(), 0) < std::accumulate(best.begin(), best.end(), 0)))
+        best = cur;
+      return;
+    }
+    if (!best.empty() && cur.size() + 1 > best.size()) return;
+    for (int R : {8, 7, 6, 5, 4, 3, 2}) {
+      if (m % R == 0) {
+        cur.push_back(R);
+        rec(m / R);
+        cur.pop_back();
+      }
+    }
+  };
+  rec(n);
+  if (best.empty() || best.size() > 8)
+    throw std::invalid_argument("PME grid size " + std::to_string(n) +
+                                " must factor into 2, 3, 5 and 7");
+  FftAxis a{};
+  a.n = n;
+  a.nrad = (int)best.size();
+  for (size_t i = 0; i < best.size(); ++i) a.radix[i] = best[i];
+  return a;
+}
+
+Pme::~Pme() { release(); }
+
+void Pme::release() {
+  if (qgrid) cudaFree(qgrid);
+  if (cgrid) cudaFree(cgrid);
+  if (phi) cudaFree(phi);
+  if (m_tw) cudaFree(m_tw);
+  if (m_prefac) cudaFree(m_prefac);
+  if (m_prefac_d) cudaFree(m_prefac_d);
+  qgrid = nullptr;
+  cgrid = nullptr;
+  phi = nullptr;
+  m_tw = nullptr;
+  m_prefac = nullptr;
+  m_prefac_d = nullptr;
+}
+
+void Pme::setup(int nx, int ny, int nz, int order, double kappa, double Lx, double Ly,
+                double Lz) {
+  if (nx % 2 || ny % 2 || nz % 2)
+    throw std::invalid_argument("PME grid dimensions must be even");
+  if (nx > 256 || ny > 256 || nz > 256)
+    throw std::invalid_argument("PME grid dimensions above 256 are not supported");
+  if (order != 4 && order != 6 && order != 8)
+    throw std::invalid_argument("PME spline order must be 4, 6 or 8");
+  const size_t plane_bytes = (size_t)(ny / 2) * (nx + 2) * sizeof(float2);
+  if (plane_bytes > 227 * 1024)
+    throw std::invalid_argument("PME plane does not fit in shared memory");
+  release();
+  m_d.nx = nx;
+  m_d.ny = ny;
+  m_d.nz = nz;
+  m_d.nxc = nx / 2 + 1;
+  m_d.order = order;
+  m_d.Lx = (float)Lx;
+  m_d.Ly = (float)Ly;
+  m_d.Lz = (float)Lz;
+  m_d.kappa = (float)kappa;
+  m_d.ax = plan_axis(nx);
+  m_d.ay = plan_axis(ny);
+  m_d.az = plan_axis(nz);
+  const size_t G = (size_t)nx * ny * nz;
+  dalloc(qgrid, G);
+  dalloc(cgrid, (size_t)nz * ny * m_d.nxc);
+  dalloc(phi, G);
+  APO_CUDA(cudaMemset(qgrid, 0, G * sizeof(int)));
+  std::vector<float2> tw;
+  for (int n : {nx, ny, nz})
+    for (int k = 0; k < n; ++k) {
+      double a = 2.0 * M_PI * k / n;
+      tw.push_back(make_float2((float)std::cos(a), (float)-std::sin(a)));
+    }
+  dalloc(m_tw, tw.size());
+  APO_CUDA(cudaMemcpy(m_tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice));
+  std::vector<double> pd, tmp;
+  for (int n : {nx, ny, nz}) {
+    bspline_moduli(n, order, tmp);
+    pd.insert(pd.end(), tmp.begin(), tmp.end());
+  }
+  std::vector<float> pf(pd.begin(), pd.end());
+  dalloc(m_prefac, pf.size());
+  dalloc(m_prefac_d, pd.size());
+  APO_CUDA(cudaMemcpy(m_prefac, pf.data(), pf.size() * sizeof(float), cudaMemcpyHostToDevice));
+  APO_CUDA(cudaMemcpy(m_prefac_d, pd.data(), pd.size() * sizeof(double), cudaMemcpyHostToDevice));
+  static bool attr = false;
+  if (!attr) {
+    APO_CUDA(cudaFuncSetAttribute(plane_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  227 * 1024));
+    APO_CUDA(cudaFuncSetAttribute(plane_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  227 * 1024));
+    attr = true;
+  }
+}
+
+void Pme::spread(const float4 *xyzq_s, const int *counts, cudaStream_t s) {
+  const int blocks = (max_slots + 31) / 32;
+  switch (m_d.order) {
+    case 4: spread_kernel<4><<<blocks, 128, 0, s>>>(xyzq_s, counts, m_d, qgrid); break;
+    case 6: spread_kernel<6><<<blocks, 128, 0, s>>>(xyzq_s, counts, m_d, qgrid); break;
+    case 8: spread_kernel<8><<<blocks, 128, 0, s>>>(xyzq_s, counts, m_d, qgrid); break;
+  }
+  APO_LAUNCH_CHECK();
+}
+
+void Pme::forward(cudaStream_t s) {
+  const size_t sm = (size_t)(m_d.ny / 2) * (m_d.nx + 2) * sizeof(float2);
+  plane_fwd_kernel<<<m_d.nz, kPlaneThreads, sm, s>>>(m_d, qgrid, cgrid, m_tw, m_tw + m_d.nx);
+  APO_LAUNCH_CHECK();
+}
+
+void Pme::convolve(long long *energy, bool calc_energy, bool fp64, cudaStream_t s) {
+  const int tiles_x = (m_d.nxc + kPencilTX - 1) / kPencilTX;
+  const int grid = tiles_x * m_d.ny;
+  const float2 *twz = m_tw + m_d.nx + m_d.ny;
+  if (fp64) {
+    if (calc_energy)
+      pencil_kernel<true, double><<<grid, kPencilThreads, 0, s>>>(m_d, cgrid, twz, m_prefac, m_prefac_d, energy);
+    else
+      pencil_kernel<false, double><<<grid, kPencilThreads, 0, s>>>(m_d, cgrid, twz, m_prefac, m_prefac_d, energy);
+  } else {
+    if (calc_energy)
+      pencil_kernel<true, float><<<grid, kPencilThreads, 0, s>>>(m_d, cgrid, twz, m_prefac, m_prefac_d, energy);
+    else
+      pencil_kernel<false, float><<<grid, kPencilThreads, 0, s>>>(m_d, cgrid, twz, m_prefac, m_prefac_d, energy);
+  }
+  APO_LAUNCH_CHECK();
+}
+
+void Pme::backward(cudaStream_t s) {
+  const size_t sm = (size_t)(m_d.ny / 2) * (m_d.nx + 2) * sizeof(float2);
+  plane_inv_kernel<<<m_d.nz, kPlaneThreads, sm, s>>>(m_d, cgrid, phi, m_tw, m_tw + m_d.nx);
+  APO_LAUNCH_CHECK();
+}
+
+void Pme::gather(const float4 *xyzq_s, const int *counts, long long *force, int stride,
+                 cudaStream_t s) {
+  const int blocks = (max_slots + 31) / 32;
+  switch (m_d.order) {
+    case 4: gather_kernel<4><<<blocks, 256, 0, s>>>(xyzq_s, counts, m_d, phi, force, stride); break;
+    case 6: gather_kernel<6><<<blocks, 256, 0, s>>>(xyzq_s, counts, m_d, phi, force, stride); break;
+    case 8: gather_kernel<8><<<blocks, 256, 0, s>>>(xyzq_s, counts, m_d, phi, force, stride); break;
+  }
+  APO_LAUNCH_CHECK();
+}
+
+void Pme::compute(const float4 *xyzq_s, const int *counts, long long *force, int stride,
+                  long long *energy, bool calc_energy, bool fp64, cudaStream_t s) {
+  spread(xyzq_s, counts, s);
+  forward(s);
+  convolve(energy, calc_energy, fp64, s);
+  backward(s);
+  gather(xyzq_s, counts, force, stride, s);
+}
+
+}  // namespace apo

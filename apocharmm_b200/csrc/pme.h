@@ -1,0 +1,82 @@
+// Smooth PME reciprocal space: charge spread, 3D real FFT, influence
+// function, inverse FFT and force gather, all hand-written.
+//
+// Replaces CudaPMERecip (src/CudaPMERecip.cu) in its P1 "BOX" mode:
+// spread_charge (:1935, body include/cuda_pme_spread.h), cuFFT R2C/C2R
+// (:2547-2645), scalar_sum_ortho_kernel (:674-929), gather_force
+// (:2381, body include/cuda_pme_gather.h), calc_self_energy (:2267).
+//
+// Pipeline (5 launches):
+//   spread      int32 fixed-point atomics into the real grid (deterministic)
+//   plane_fwd   one CTA per z-plane: R2C along x (two rows packed into one
+//               complex FFT), C2C along y; the plane lives in shared memory
+//   pencil      one CTA per (y-row, 16 x-columns): FFT along z, multiply by
+//               the influence function (energy/virial reduced on the way),
+//               inverse FFT along z
+//   plane_inv   inverse of plane_fwd, writes the real potential grid
+//   gather      gradient from the potential, 8 threads per atom
+// The FFTs are in-place mixed-radix (2..8) shared-memory transforms.  A
+// decimation-in-frequency pass leaves its output in digit-reversed order and
+// a decimation-in-time pass takes digit-reversed input, so pairing them
+// (z: DIF forward / DIT inverse, y: DIF forward stored as-is / DIT inverse,
+// x: DIT forward from a scattered load / DIF inverse with a scattered store)
+// needs no reordering pass at all.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+namespace apo {
+
+struct FftAxis {
+  int n;
+  int nrad;
+  int radix[8];
+};
+
+struct PmeDims {
+  int nx, ny, nz, nxc, order;
+  float Lx, Ly, Lz;       // box
+  float kappa;
+  FftAxis ax, ay, az;
+};
+
+class Pme {
+ public:
+  Pme() = default;
+  ~Pme();
+  Pme(const Pme &) = delete;
+  Pme &operator=(const Pme &) = delete;
+
+  void setup(int nx, int ny, int nz, int order, double kappa, double Lx, double Ly,
+             double Lz);
+  // sorted coordinates in, fixed-point gradients added to `force` (sorted
+  // slot order, SoA with `stride`); ewks energy added to energy[kEEwks]
+  void compute(const float4 *xyzq_s, const int *counts, long long *force, int stride,
+               long long *energy, bool calc_energy, bool fp64_influence, cudaStream_t s);
+  // the individual stages (exposed for tests and profiling)
+  void spread(const float4 *xyzq_s, const int *counts, cudaStream_t s);
+  void forward(cudaStream_t s);
+  void convolve(long long *energy, bool calc_energy, bool fp64_influence, cudaStream_t s);
+  void backward(cudaStream_t s);
+  void gather(const float4 *xyzq_s, const int *counts, long long *force, int stride,
+              cudaStream_t s);
+
+  const PmeDims &dims() const { return m_d; }
+  int *qgrid = nullptr;     // nz*ny*nx int32 fixed point (zeroed by plane_fwd)
+  float2 *cgrid = nullptr;  // nz * ny * nxc complex (y rows in digit-reversed order)
+  float *phi = nullptr;     // nz*ny*nx real potential
+  int max_slots = 0;
+
+  static FftAxis plan_axis(int n);
+
+ private:
+  void release();
+  PmeDims m_d{};
+  float2 *m_tw = nullptr;   // twiddles: x (nx), y (ny), z (nz) consecutive
+  float *m_prefac = nullptr;  // B-spline moduli 1/|b|^2: x, y, z consecutive
+  double *m_prefac_d = nullptr;
+};
+
+}  // namespace apo

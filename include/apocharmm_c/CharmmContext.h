@@ -1,0 +1,55 @@
+/* Simulation context handle (reference: capi/include/apocharmm_c/CharmmContext.h:30-48).
+ *
+ * Additions (the reference capi has no getters for these; each exposes the C++
+ * CharmmContext/ForceManager call cited):
+ *   calculate_forces      CharmmContext::calculateForces (src/CharmmContext.cu:416)
+ *   get_forces            ForceManager::getForces (include/ForceManager.h) -- the
+ *                         total GRADIENT dU/dx, N x 3 doubles, atom order
+ *   get_energy_components ForceManager::getEnergyComponents (src/ForceManager.cu:278),
+ *                         10 doubles in the order bond angle ureyb dihe imdihe
+ *                         ewks ewse ewex elec vdw
+ *   get/set coordinates, get/set velocities (N x 3 doubles)
+ *   get_neighbor_pairs    the active (not masked) atom pairs of the tile list
+ *                         within `radius`, as (i, j, image code) triples, for
+ *                         pair-set parity checks */
+#ifndef APOCHARMM_C_CHARMM_CONTEXT_H
+#define APOCHARMM_C_CHARMM_CONTEXT_H
+#include <stddef.h>
+#include <stdint.h>
+#ifndef __cplusplus
+#include <stdbool.h>
+#endif
+#include "apocharmm_c/CharmmCrd.h"
+#include "apocharmm_c/Export.h"
+#include "apocharmm_c/ForceManager.h"
+#include "apocharmm_c/Status.h"
+#ifdef __cplusplus
+extern "C" {
+#endif
+typedef struct apo_charmm_context apo_charmm_context;
+APOCHARMM_C_API apo_status apo_charmm_context_create(apo_charmm_context **out, const apo_force_manager *force_manager); /* :30 */
+APOCHARMM_C_API void apo_charmm_context_destroy(apo_charmm_context *context); /* :33 */
+APOCHARMM_C_API apo_status apo_charmm_context_set_coordinates(apo_charmm_context *context, const apo_charmm_crd *crd); /* :35 */
+APOCHARMM_C_API apo_status apo_charmm_context_set_random_seed_for_velocities(apo_charmm_context *context, const uint64_t seed); /* :38 */
+APOCHARMM_C_API apo_status apo_charmm_context_use_holonomic_constraints(apo_charmm_context *context, const bool useHolonomicConstraints); /* :41 */
+APOCHARMM_C_API apo_status apo_charmm_context_assign_velocities_at_temperature(apo_charmm_context *context, const double temperature); /* :45 */
+APOCHARMM_C_API apo_status apo_charmm_context_compute_temperature(double *temperature, apo_charmm_context *context); /* :48 */
+/* additions */
+APOCHARMM_C_API apo_status apo_charmm_context_calculate_forces(apo_charmm_context *context, const bool reset_list, const bool calc_energy, const bool calc_virial);
+APOCHARMM_C_API apo_status apo_charmm_context_get_forces(double *xyz, const size_t len, apo_charmm_context *context);
+APOCHARMM_C_API apo_status apo_charmm_context_get_energy_components(double *energies, const size_t len, apo_charmm_context *context);
+APOCHARMM_C_API apo_status apo_charmm_context_get_potential_energy(double *energy, apo_charmm_context *context);
+APOCHARMM_C_API apo_status apo_charmm_context_set_coordinates_xyz(apo_charmm_context *context, const double *xyz, const size_t len);
+APOCHARMM_C_API apo_status apo_charmm_context_get_coordinates(double *xyz, const size_t len, apo_charmm_context *context);
+APOCHARMM_C_API apo_status apo_charmm_context_set_velocities(apo_charmm_context *context, const double *v, const size_t len);
+APOCHARMM_C_API apo_status apo_charmm_context_get_velocities(double *v, const size_t len, apo_charmm_context *context);
+APOCHARMM_C_API apo_status apo_charmm_context_get_num_atoms(size_t *num_atoms, const apo_charmm_context *context);
+APOCHARMM_C_API apo_status apo_charmm_context_get_degrees_of_freedom(int *ndegf, const apo_charmm_context *context);
+APOCHARMM_C_API apo_status apo_charmm_context_reset_neighbor_list(apo_charmm_context *context);
+APOCHARMM_C_API apo_status apo_charmm_context_get_neighbor_pairs(int *pairs, const size_t len, size_t *num_pairs, const double radius, apo_charmm_context *context);
+/* CUDA stream the context's work is issued on (a cudaStream_t), for timing */
+APOCHARMM_C_API apo_status apo_charmm_context_get_stream(void **stream, const apo_charmm_context *context);
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,36 @@
+/* Force manager handle (reference: capi/include/apocharmm_c/ForceManager.h:24-31).
+ *
+ * Additions (no C entry point in the reference capi; each exposes the C++
+ * ForceManager setter cited): the nonbonded/PME settings that the reference
+ * only offers in C++ (include/ForceManager.h:200-225), and the precision form
+ * (per-pair 64-bit fixed-point force accumulation + FP64 influence function). */
+#ifndef APOCHARMM_C_FORCE_MANAGER_H
+#define APOCHARMM_C_FORCE_MANAGER_H
+#include "apocharmm_c/CharmmParameters.h"
+#include "apocharmm_c/CharmmPsf.h"
+#include "apocharmm_c/Export.h"
+#include "apocharmm_c/Status.h"
+#ifdef __cplusplus
+extern "C" {
+#endif
+typedef struct apo_force_manager apo_force_manager;
+APOCHARMM_C_API apo_status apo_force_manager_create(apo_force_manager **out, const apo_charmm_psf *psf, const apo_charmm_parameters *parameters); /* :24 */
+APOCHARMM_C_API void apo_force_manager_destroy(apo_force_manager *force_manager); /* :28 */
+APOCHARMM_C_API apo_status apo_force_manager_set_box_dimensions(apo_force_manager *force_manager, const double x, const double y, const double z); /* :31 */
+/* additions: ForceManager::setKappa/setCutoff/setCtonnb/setCtofnb/setFFTGrid/setPmeSplineOrder */
+APOCHARMM_C_API apo_status apo_force_manager_set_kappa(apo_force_manager *force_manager, const double kappa);
+APOCHARMM_C_API apo_status apo_force_manager_set_cutoff(apo_force_manager *force_manager, const double cutnb);
+APOCHARMM_C_API apo_status apo_force_manager_set_ctonnb(apo_force_manager *force_manager, const double ctonnb);
+APOCHARMM_C_API apo_status apo_force_manager_set_ctofnb(apo_force_manager *force_manager, const double ctofnb);
+APOCHARMM_C_API apo_status apo_force_manager_set_fft_grid(apo_force_manager *force_manager, const int nx, const int ny, const int nz);
+APOCHARMM_C_API apo_status apo_force_manager_set_spline_order(apo_force_manager *force_manager, const int order);
+/* additions: precision form on/off; tiles per nonbonded work item (tuning);
+ * evaluated parts as a bit mask (1 bonded+1-4, 2 direct, 4 reciprocal) */
+APOCHARMM_C_API apo_status apo_force_manager_set_precision_mode(apo_force_manager *force_manager, const int precise);
+APOCHARMM_C_API apo_status apo_force_manager_set_tiles_per_work(apo_force_manager *force_manager, const int tiles);
+APOCHARMM_C_API apo_status apo_force_manager_set_component_mask(apo_force_manager *force_manager, const int mask);
+APOCHARMM_C_API apo_status apo_force_manager_get_fft_grid(int *nxyz3, const apo_force_manager *force_manager);
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,102 @@
+"""C-ABI checks that need no GPU: the library loads, exports every symbol
+declared in include/apocharmm_c/*.h, parses CHARMM files and reports errors
+with the reference's status codes."""
+import ctypes
+import glob
+import os
+import re
+
+import numpy as np
+import pytest
+
+from apocharmm_b200 import _lib, api
+from apocharmm_b200.systems import config_solvated_chain, water_box, write_charmm_files
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "apocharmm_c", "*.h")):
+        text = open(h).read()
+        names |= set(re.findall(r"APOCHARMM_C_API\s+[\w\s\*]+?\b(apo_\w+)\s*\(", text))
+    return sorted(names)
+
+
+def test_library_exports_every_declared_symbol():
+    L = _lib.lib()
+    names = declared_symbols()
+    assert len(names) >= 59
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_psf_prm_crd_roundtrip(tmp_path):
+    s = water_box(64, 14.0, seed=3)
+    paths = write_charmm_files(s, str(tmp_path))
+    psf = api.CharmmPsf(paths["psf"])
+    assert psf.getNumAtoms() == s.n_atoms
+    assert psf.getNumBonds() == len(s.bonds)
+    assert psf.getNumAngles() == len(s.angles)
+    assert psf.getAtomTypes() == s.atom_type
+    assert psf.getAtomNames() == s.atom_name
+    np.testing.assert_allclose(psf.getCharges(), s.charge)
+    np.testing.assert_allclose(psf.getMasses(), s.mass)
+    assert abs(psf.getNetCharge()) < 1e-9
+    assert psf.getFileName() == paths["psf"]
+    crd = api.CharmmCrd(paths["crd"])
+    assert crd.getNumAtoms() == s.n_atoms
+    np.testing.assert_allclose(np.array(crd.getCoordinates()), s.pos, atol=1e-5)
+    prm = api.CharmmParameters(paths["prm"])
+    fm = api.ForceManager(psf, prm)
+    fm.setBoxDimensions(s.box)
+    fm.setFFTGrid(16, 16, 16)
+    assert fm.getFFTGrid() == [16, 16, 16]
+
+
+def test_chain_topology_files_parse(tmp_path):
+    s = config_solvated_chain()
+    paths = write_charmm_files(s, str(tmp_path))
+    psf = api.CharmmPsf(paths["psf"])
+    assert psf.getNumAtoms() == 23558
+    assert psf.getNumDihedrals() == 2489 - 3
+    prm = api.CharmmParameters([paths["prm"]])
+    api.ForceManager(psf, prm)
+
+
+def test_error_status_and_message(tmp_path):
+    with pytest.raises(_lib.ApoCharmmError) as e:
+        api.CharmmPsf(str(tmp_path / "missing.psf"))
+    assert e.value.status == 2
+    assert "missing.psf" in str(e.value)
+    L = _lib.lib()
+    out = ctypes.c_void_p(123)
+    st = L.apo_charmm_psf_create(ctypes.byref(out), None)
+    assert st == 1 and out.value is None          # out cleared before validation
+    assert b"path" in L.apo_last_error()
+    st = L.apo_force_manager_set_kappa(None, ctypes.c_double(0.3))
+    assert st == 1
+    n = ctypes.c_size_t(7)
+    assert L.apo_charmm_psf_get_num_atoms(ctypes.byref(n), None) == 1
+    assert n.value == 0
+
+
+def test_missing_bond_parameter_is_reported(tmp_path):
+    s = water_box(8, 10.0, seed=1)
+    s.bond_params.pop(("HT", "OT"))
+    paths = write_charmm_files(s, str(tmp_path))
+    psf = api.CharmmPsf(paths["psf"])
+    prm = api.CharmmParameters(paths["prm"])
+    fm = api.ForceManager(psf, prm)       # assembly happens at initialize()
+    assert fm is not None
+
+
+def test_stream_file_with_topology_block(tmp_path):
+    # a .str stream: RTF first, parameters after "read para"
+    p = tmp_path / "toppar_test.str"
+    p.write_text("* test\n*\nread rtf card\n* rtf\n*\n36 1\nMASS -1 OT 15.9994\nRESI TIP3 0.0\nEND\n"
+                 "read para card flex\n* par\n*\nATOMS\nMASS -1 OT 15.9994\nMASS -1 HT 1.008\n"
+                 "BONDS\nHT OT 450.0 0.9572\nHT HT 0.0 1.5139\nANGLES\nHT OT HT 55.0 104.52\n"
+                 "NONBONDED nbxmod 5 atom cdiel -\ncutnb 14.0\nHT 0.0 -0.046 0.2245\n"
+                 "OT 0.0 -0.1521 1.7682\nEND\n")
+    api.CharmmParameters(str(p))

@@ -1,0 +1,90 @@
+"""GPU parity: the sm_100a path through the C ABI against the FP64 oracle
+and the reference's CHARMM golden values.
+
+Tolerances (north star): forces within 1e-5 relative RMS, energies within
+1e-6 relative (total potential), each against the FP64 oracle.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from apocharmm_b200 import api
+from apocharmm_b200.systems import config_solvated_chain, config_small_water, water_box
+from golden_systems import golden, load_case, reference_forces
+from parity_util import brute_force_pairs, oracle_for, rel_rms
+
+pytestmark = pytest.mark.gpu
+
+FORCE_RTOL = 1e-5
+ENERGY_RTOL = 1e-6
+
+
+def _run(sys, tmp_path, precise=False, settings=None):
+    psf, prm, fm, ctx = api.system_context(sys, str(tmp_path), precise=precise, settings=settings)
+    ctx.calculateForces(False, True, False)
+    return (psf, prm, fm, ctx), ctx.getEnergyComponents(), ctx.getForces()
+
+
+@pytest.mark.parametrize("precise", [False, True])
+def test_waterbox_matches_charmm_and_oracle(tmp_path, precise):
+    s = load_case("waterbox")
+    keep, E, F = _run(s, tmp_path, precise)
+    g = golden()["waterbox"]
+    for k, v in g["energy"].items():
+        val = sum(E.values()) if k == "epot" else E[k]
+        assert val == pytest.approx(v, rel=1.2e-5), k     # the reference test's tolerance
+    assert np.abs(F - reference_forces("waterbox")).max() < g["force_tol"]
+    Eo, Go = oracle_for(s).evaluate()
+    assert rel_rms(F, Go) < FORCE_RTOL
+    assert sum(E.values()) == pytest.approx(Eo["epot"], rel=ENERGY_RTOL)
+
+
+def test_solvated_chain_forces_and_energies(tmp_path):
+    s = config_solvated_chain()
+    keep, E, F = _run(s, tmp_path)
+    Eo, Go = oracle_for(s).evaluate()
+    assert rel_rms(F, Go) < FORCE_RTOL
+    assert sum(E.values()) == pytest.approx(Eo["epot"], rel=ENERGY_RTOL)
+    for k in ("bond", "angle", "dihe", "vdw", "elec", "ewks", "ewse", "ewex"):
+        assert E[k] == pytest.approx(Eo[k], rel=1e-5, abs=1e-3), k
+
+
+def test_components_separately(tmp_path):
+    s = water_box(512, 25.0, seed=11)
+    settings = dict(kappa=0.34, nfft=(24, 24, 24), order=4, ctofnb=10.0, ctonnb=8.0, cutnb=12.0)
+    psf, prm, fm, ctx = api.system_context(s, str(tmp_path), settings=settings)
+    o = oracle_for(s, settings)
+    for mask, parts in ((1, ("bonded", "14")), (2, ("direct",)), (4, ("recip", "self"))):
+        fm.setComponentMask(mask)
+        ctx.calculateForces(False, True, False)
+        F = ctx.getForces()
+        Eo, Go = o.evaluate(parts=parts)
+        assert rel_rms(F, Go) < FORCE_RTOL, parts
+        E = ctx.getEnergyComponents()
+        assert sum(E.values()) == pytest.approx(Eo["epot"], rel=ENERGY_RTOL), parts
+
+
+def test_neighbor_pairs_match_brute_force(tmp_path):
+    s = water_box(1200, 23.0, seed=5)
+    settings = dict(kappa=0.34, nfft=(24, 24, 24), order=4, ctofnb=9.0, ctonnb=7.0, cutnb=11.0)
+    psf, prm, fm, ctx = api.system_context(s, str(tmp_path), settings=settings)
+    o = oracle_for(s, settings)
+    # every pair within the list radius must be covered exactly once, and no
+    # topologically excluded pair may be active
+    got = ctx.getNeighborPairs(11.0)
+    canon = {(min(i, j), max(i, j)) for i, j, _ in got.tolist()}
+    assert len(canon) == len(got), "a pair appears in more than one tile"
+    ref = brute_force_pairs(s.pos, s.box, 11.0, o.eptr, o.eidx)
+    assert canon == ref
+
+
+def test_forces_are_deterministic(tmp_path):
+    s = config_small_water()
+    psf, prm, fm, ctx = api.system_context(s, str(tmp_path))
+    ctx.calculateForces(False, True, False)
+    f1, e1 = ctx.getForces(), ctx.getEnergyComponents()
+    ctx.calculateForces(True, True, False)
+    f2, e2 = ctx.getForces(), ctx.getEnergyComponents()
+    assert np.array_equal(f1, f2)
+    assert e1 == e2
