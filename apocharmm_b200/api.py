@@ -302,3 +302,151 @@ def system_context(sys, workdir: str, precise: bool = False, settings=None):
     ctx = CharmmContext(fm)
     ctx.setCoordinates(sys.pos)
     return psf, prm, fm, ctx
+
+
+class Subscriber(_Handle):
+    """Borrowed base view of a concrete subscriber (owned by the subclass)."""
+
+    def __init__(self):
+        super().__init__()
+        self._view = _vp()
+
+    def setReportFrequency(self, f: int):
+        call("apo_subscriber_set_report_frequency", self._view, _i(f))
+
+    def getReportFrequency(self) -> int:
+        v = _i()
+        call("apo_subscriber_get_report_frequency", ctypes.byref(v), self._view)
+        return v.value
+
+
+class DcdSubscriber(Subscriber):
+    _destroy = "apo_dcd_subscriber_destroy"
+
+    def __init__(self, path, report_frequency: int | None = None):
+        super().__init__()
+        if report_frequency is None:
+            call("apo_dcd_subscriber_create", ctypes.byref(self._h), _enc(path))
+        else:
+            call("apo_dcd_subscriber_create_with_report_frequency", ctypes.byref(self._h),
+                 _enc(path), _i(report_frequency))
+        call("apo_dcd_subscriber_as_subscriber", ctypes.byref(self._view), self._h)
+
+
+class CudaIntegrator(_Handle):
+    """Base of the integrators; `_view` is the borrowed apo_cuda_integrator."""
+
+    _as_base = ""
+
+    def __init__(self):
+        super().__init__()
+        self._view = _vp()
+        self._keep = []
+
+    def _bind_view(self):
+        call(self._as_base, ctypes.byref(self._view), self._h)
+
+    def setTimeStep(self, dt_ps: float):
+        call("apo_cuda_integrator_set_time_step", self._view, _d(dt_ps))
+
+    def setCharmmContext(self, context: CharmmContext):
+        self._keep.append(context)
+        call("apo_cuda_integrator_set_charmm_context", self._view, context.handle)
+
+    def subscribe(self, subscriber: Subscriber):
+        self._keep.append(subscriber)
+        call("apo_cuda_integrator_subscribe", self._view, subscriber._view)
+
+    def propagate(self, num_steps: int):
+        call("apo_cuda_integrator_propagate", self._view, _i(num_steps))
+
+    def initializeFromRestartFile(self, path):
+        call("apo_cuda_integrator_initialize_from_restart_file", self._view, _enc(path))
+
+    def setNonbondedListUpdateFrequency(self, f: int):
+        call("apo_cuda_integrator_set_nonbonded_list_update_frequency", self._view, _i(f))
+
+    def setUseGraphs(self, on: bool):
+        call("apo_cuda_integrator_set_use_graphs", self._view, _i(int(on)))
+
+    def getCurrentPropagatedStep(self) -> int:
+        v = ctypes.c_longlong()
+        call("apo_cuda_integrator_get_current_step", ctypes.byref(v), self._view)
+        return v.value
+
+    def getAverageTemperature(self) -> float:
+        v = _d()
+        call("apo_cuda_integrator_get_average_temperature", ctypes.byref(v), self._view)
+        return v.value
+
+    def getInstantaneousTemperature(self) -> float:
+        v = _d()
+        call("apo_cuda_integrator_get_instantaneous_temperature", ctypes.byref(v), self._view)
+        return v.value
+
+    def getKernelsPerStep(self) -> int:
+        v = _i()
+        call("apo_cuda_integrator_get_kernels_per_step", ctypes.byref(v), self._view)
+        return v.value
+
+
+class CudaNoseHooverIntegrator(CudaIntegrator):
+    _destroy = "apo_cuda_nose_hoover_integrator_destroy"
+    _as_base = "apo_cuda_nose_hoover_integrator_as_cuda_integrator"
+
+    def __init__(self, time_step: float):
+        super().__init__()
+        call("apo_cuda_nose_hoover_integrator_create", ctypes.byref(self._h), _d(time_step))
+        self._bind_view()
+
+    def setReferenceTemperature(self, t: float):
+        call("apo_cuda_nose_hoover_integrator_set_reference_temperature", self._h, _d(t))
+
+    def setNoseHooverPistonMass(self, m: float):
+        call("apo_cuda_nose_hoover_integrator_set_nose_hoover_piston_mass", self._h, _d(m))
+
+    def useOldTemperature(self, flag: bool = True):
+        call("apo_cuda_nose_hoover_integrator_use_old_temperature", self._h, ctypes.c_bool(flag))
+
+    def resetAverageTemperature(self):
+        call("apo_cuda_nose_hoover_integrator_reset_average_temperature", self._h)
+
+    def getReferenceTemperature(self) -> float:
+        v = _d()
+        call("apo_cuda_nose_hoover_integrator_get_reference_temperature", ctypes.byref(v), self._h)
+        return v.value
+
+
+class CudaLangevinThermostatIntegrator(CudaIntegrator):
+    _destroy = "apo_cuda_langevin_thermostat_integrator_destroy"
+    _as_base = "apo_cuda_langevin_thermostat_integrator_as_cuda_integrator"
+
+    def __init__(self, time_step: float):
+        super().__init__()
+        call("apo_cuda_langevin_thermostat_integrator_create", ctypes.byref(self._h), _d(time_step))
+        self._bind_view()
+
+    def setThermostatFriction(self, f: float):
+        call("apo_cuda_langevin_thermostat_integrator_set_thermostat_friction", self._h, _d(f))
+
+    def setReferenceTemperature(self, t: float):
+        call("apo_cuda_langevin_thermostat_integrator_set_reference_temperature", self._h, _d(t))
+
+    def setThermostatRngSeed(self, seed: int):
+        call("apo_cuda_langevin_thermostat_integrator_set_thermostat_rng_seed", self._h,
+             ctypes.c_uint64(seed))
+
+    def getRngSequencePos(self) -> int:
+        v = ctypes.c_ulonglong()
+        call("apo_cuda_langevin_thermostat_integrator_get_rng_sequence_pos", ctypes.byref(v), self._h)
+        return v.value
+
+
+class CudaLeapFrogIntegrator(CudaIntegrator):
+    _destroy = "apo_cuda_leap_frog_integrator_destroy"
+    _as_base = "apo_cuda_leap_frog_integrator_as_cuda_integrator"
+
+    def __init__(self, time_step: float):
+        super().__init__()
+        call("apo_cuda_leap_frog_integrator_create", ctypes.byref(self._h), _d(time_step))
+        self._bind_view()

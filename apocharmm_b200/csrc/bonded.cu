@@ -11,6 +11,13 @@ namespace {
 constexpr int kThreads = 256;
 enum Seg { kSBond = 0, kSUb, kSAngle, kSDihe, kSImp, kSIn14, kSEx14, kNumSeg };
 
+// difference of two atom positions, formed from the FP64 state coordinates
+// so that stiff terms are not limited by single-precision absolute positions
+__device__ __forceinline__ float3 diff(const BondedArgs &a, int i, int j) {
+  const double4 xi = a.coords[i], xj = a.coords[j];
+  return make_float3((float)(xi.x - xj.x), (float)(xi.y - xj.y), (float)(xi.z - xj.z));
+}
+
 __device__ __forceinline__ void push(const BondedArgs &a, int atom, float gx, float gy,
                                      float gz) {
   const int s = a.glo2loc[atom];
@@ -21,8 +28,8 @@ __device__ __forceinline__ void push(const BondedArgs &a, int atom, float gx, fl
 
 // E = k (r - r0)^2, reference src/CudaBondedForce.cu:85-120
 __device__ float bond_term(const BondedArgs &a, int i, int j, float2 p) {
-  const float4 xi = a.xyzq[i], xj = a.xyzq[j];
-  const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+  const float3 d = diff(a, i, j);
+  const float dx = d.x, dy = d.y, dz = d.z;
   const float r = sqrtf(dx * dx + dy * dy + dz * dz);
   const float db = r - p.y;
   const float f = 2.f * p.x * db / r;
@@ -34,9 +41,9 @@ __device__ float bond_term(const BondedArgs &a, int i, int j, float2 p) {
 // E = k (theta - theta0)^2 with cos(theta) clamped to +-0.999
 // (src/CudaBondedForce.cu:223-300)
 __device__ float angle_term(const BondedArgs &a, int4 t, float2 p) {
-  const float4 xi = a.xyzq[t.x], xj = a.xyzq[t.y], xk = a.xyzq[t.z];
-  const float ax = xi.x - xj.x, ay = xi.y - xj.y, az = xi.z - xj.z;
-  const float bx = xk.x - xj.x, by = xk.y - xj.y, bz = xk.z - xj.z;
+  const float3 dv1 = diff(a, t.x, t.y), dv2 = diff(a, t.z, t.y);
+  const float ax = dv1.x, ay = dv1.y, az = dv1.z;
+  const float bx = dv2.x, by = dv2.y, bz = dv2.z;
   const float rai = rsqrtf(ax * ax + ay * ay + az * az);
   const float rbi = rsqrtf(bx * bx + by * by + bz * bz);
   const float uax = ax * rai, uay = ay * rai, uaz = az * rai;
@@ -61,10 +68,10 @@ __device__ float angle_term(const BondedArgs &a, int4 t, float2 p) {
 // reference (src/CudaBondedForce.cu:517-640)
 template <bool HARM>
 __device__ float dihedral_term(const BondedArgs &a, int4 t, int2 terms, float2 hp) {
-  const float4 xi = a.xyzq[t.x], xj = a.xyzq[t.y], xk = a.xyzq[t.z], xl = a.xyzq[t.w];
-  const float fx = xi.x - xj.x, fy = xi.y - xj.y, fz = xi.z - xj.z;
-  const float gx = xj.x - xk.x, gy = xj.y - xk.y, gz = xj.z - xk.z;
-  const float hx = xl.x - xk.x, hy = xl.y - xk.y, hz = xl.z - xk.z;
+  const float3 F = diff(a, t.x, t.y), G = diff(a, t.y, t.z), H = diff(a, t.w, t.z);
+  const float fx = F.x, fy = F.y, fz = F.z;
+  const float gx = G.x, gy = G.y, gz = G.z;
+  const float hx = H.x, hy = H.y, hz = H.z;
   const float ax = fy * gz - fz * gy, ay = fz * gx - fx * gz, az = fx * gy - fy * gx;
   const float bx = hy * gz - hz * gy, by = hz * gx - hx * gz, bz = hx * gy - hy * gx;
   const float ra2 = ax * ax + ay * ay + az * az, rb2 = bx * bx + by * by + bz * bz;
@@ -113,11 +120,11 @@ __device__ float dihedral_term(const BondedArgs &a, int4 t, int2 terms, float2 h
 // (qq (erfc - 1)/r = -qq erf/r); src/CudaDirectForceKernels.cu:643-870
 template <bool INCL>
 __device__ void pair14_term(const BondedArgs &a, int2 p, float &e_el, float &e_vdw) {
-  const float4 xi = a.xyzq[p.x], xj = a.xyzq[p.y];
-  const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+  const float3 d = diff(a, p.x, p.y);
+  const float dx = d.x, dy = d.y, dz = d.z;
   const float r2 = dx * dx + dy * dy + dz * dz;
   const float rinv = rsqrtf(r2), r = r2 * rinv, rinv2 = rinv * rinv;
-  const float qq = (float)kCcelec * xi.w * xj.w;
+  const float qq = (float)kCcelec * (float)a.coords[p.x].w * (float)a.coords[p.y].w;
   const NbSetup &st = a.nb;
   const float expv = __expf(-st.kappa2 * r2);
   float fr;

@@ -17,7 +17,7 @@
 namespace apo {
 
 struct BondedArgs {
-  const float4 *xyzq;     // global atom order
+  const double4 *coords;  // global atom order: x, y, z, charge (FP64 state)
   const int *glo2loc;     // atom -> force slot
   long long *force;
   int stride;

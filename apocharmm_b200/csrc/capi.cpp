@@ -541,3 +541,24 @@ extern "C" apo_status apo_charmm_context_get_neighbor_pairs(int *pairs, const si
     return APO_STATUS_OK;
   }, fn);
 }
+
+extern "C" apo_status apo_charmm_context_set_kernel_timing(apo_charmm_context *c, const int on) {
+  const char *fn = "apo_charmm_context_set_kernel_timing";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
+    c->object->getForceManager()->setKernelTiming(on != 0);
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_charmm_context_get_kernel_time(double *ms, int *launches,
+                                                         apo_charmm_context *c) {
+  const char *fn = "apo_charmm_context_get_kernel_time";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_ptr(ms, fn, "ms"));
+    APO_RETURN_IF(require_ptr(launches, fn, "launches"));
+    APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
+    *ms = c->object->getForceManager()->kernelTimeMs(*launches);
+    return APO_STATUS_OK;
+  }, fn);
+}

@@ -1,0 +1,382 @@
+// C ABI: integrators and subscribers (same conventions as capi.cpp).
+#include "apocharmm_c/CudaIntegrator.h"
+#include "apocharmm_c/CudaLangevinThermostatIntegrator.h"
+#include "apocharmm_c/CudaNoseHooverIntegrator.h"
+#include "apocharmm_c/DcdSubscriber.h"
+#include "apocharmm_c/RestartSubscriber.h"
+#include "apocharmm_c/Subscriber.h"
+#include "capi_internal.h"
+#include "integrators.h"
+#include "subscribers.h"
+
+using namespace apocapi;
+
+struct apo_subscriber { std::shared_ptr<apo::Subscriber> object; };
+struct apo_dcd_subscriber {
+  apo_subscriber base;
+  std::shared_ptr<apo::DcdSubscriber> object;
+};
+struct apo_restart_subscriber {
+  apo_subscriber base;
+  std::shared_ptr<apo::Subscriber> object;
+};
+struct apo_cuda_integrator { std::shared_ptr<apo::CudaIntegrator> object; };
+struct apo_cuda_nose_hoover_integrator {
+  apo_cuda_integrator base;
+  std::shared_ptr<apo::CudaNoseHooverIntegrator> object;
+};
+struct apo_cuda_langevin_thermostat_integrator {
+  apo_cuda_integrator base;
+  std::shared_ptr<apo::CudaLangevinThermostatIntegrator> object;
+};
+struct apo_cuda_leap_frog_integrator {
+  apo_cuda_integrator base;
+  std::shared_ptr<apo::CudaLeapFrogIntegrator> object;
+};
+
+// ------------------------------------------------------------ base view ----
+
+extern "C" apo_status apo_cuda_integrator_set_time_step(apo_cuda_integrator *it, const double dt) {
+  const char *fn = "apo_cuda_integrator_set_time_step";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(it, fn, "CudaIntegrator"));
+    if (!(dt > 0) || !std::isfinite(dt)) return invalid(fn, "time step must be positive");
+    it->object->setTimeStep(dt);
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_cuda_integrator_set_charmm_context(apo_cuda_integrator *it,
+                                                             apo_charmm_context *ctx) {
+  const char *fn = "apo_cuda_integrator_set_charmm_context";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(it, fn, "CudaIntegrator"));
+    APO_RETURN_IF(require_handle(ctx, fn, "CharmmContext"));
+    it->object->setCharmmContext(ctx->object);
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_cuda_integrator_subscribe(apo_cuda_integrator *it, apo_subscriber *sub) {
+  const char *fn = "apo_cuda_integrator_subscribe";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(it, fn, "CudaIntegrator"));
+    APO_RETURN_IF(require_handle(sub, fn, "Subscriber"));
+    it->object->subscribe(sub->object);
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_cuda_integrator_propagate(apo_cuda_integrator *it, const int n) {
+  const char *fn = "apo_cuda_integrator_propagate";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(it, fn, "CudaIntegrator"));
+    if (n < 0) return invalid(fn, "num_steps must be >= 0");
+    it->object->propagate(n);
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_cuda_integrator_initialize_from_restart_file(apo_cuda_integrator *it,
+                                                                       const char *path) {
+  const char *fn = "apo_cuda_integrator_initialize_from_restart_file";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(it, fn, "CudaIntegrator"));
+    APO_RETURN_IF(require_string(path, fn, "path"));
+    return set_error(APO_STATUS_NOT_IMPLEMENTED,
+                     std::string(fn) + ": restart files are not implemented on this engine");
+  }, fn);
+}
+
+extern "C" apo_status apo_cuda_integrator_set_nonbonded_list_update_frequency(apo_cuda_integrator *it,
+                                                                              const int f) {
+  const char *fn = "apo_cuda_integrator_set_nonbonded_list_update_frequency";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(it, fn, "CudaIntegrator"));
+    if (f < 1) return invalid(fn, "frequency must be >= 1");
+    it->object->setNonbondedListUpdateFrequency(f);
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_cuda_integrator_set_use_graphs(apo_cuda_integrator *it, const int g) {
+  const char *fn = "apo_cuda_integrator_set_use_graphs";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(it, fn, "CudaIntegrator"));
+    it->object->setUseGraphs(g != 0);
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_cuda_integrator_get_current_step(long long *step,
+                                                           const apo_cuda_integrator *it) {
+  const char *fn = "apo_cuda_integrator_get_current_step";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_ptr(step, fn, "step"));
+    APO_RETURN_IF(require_handle(it, fn, "CudaIntegrator"));
+    *step = it->object->getCurrentPropagatedStep();
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_cuda_integrator_get_average_temperature(double *t,
+                                                                  const apo_cuda_integrator *it) {
+  const char *fn = "apo_cuda_integrator_get_average_temperature";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_ptr(t, fn, "temperature"));
+    APO_RETURN_IF(require_handle(it, fn, "CudaIntegrator"));
+    *t = it->object->getAverageTemperature();
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_cuda_integrator_get_instantaneous_temperature(double *t,
+                                                                        const apo_cuda_integrator *it) {
+  const char *fn = "apo_cuda_integrator_get_instantaneous_temperature";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_ptr(t, fn, "temperature"));
+    APO_RETURN_IF(require_handle(it, fn, "CudaIntegrator"));
+    *t = it->object->getInstantaneousTemperature();
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_cuda_integrator_get_kernels_per_step(int *k, const apo_cuda_integrator *it) {
+  const char *fn = "apo_cuda_integrator_get_kernels_per_step";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_ptr(k, fn, "kernels"));
+    APO_RETURN_IF(require_handle(it, fn, "CudaIntegrator"));
+    *k = it->object->kernelsPerStep();
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+// ---------------------------------------------------------- Nose-Hoover ----
+
+extern "C" apo_status apo_cuda_nose_hoover_integrator_create(apo_cuda_nose_hoover_integrator **out,
+                                                             const double dt) {
+  const char *fn = "apo_cuda_nose_hoover_integrator_create";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(prepare_out(out, fn));
+    if (!(dt > 0) || !std::isfinite(dt)) return invalid(fn, "time step must be positive");
+    auto h = std::make_unique<apo_cuda_nose_hoover_integrator>();
+    h->object = std::make_shared<apo::CudaNoseHooverIntegrator>(dt);
+    h->base.object = h->object;
+    *out = h.release();
+    return APO_STATUS_OK;
+  }, fn);
+}
+extern "C" void apo_cuda_nose_hoover_integrator_destroy(apo_cuda_nose_hoover_integrator *it) { delete it; }
+
+#define NH_SET(fname, type, body)                                               \
+  extern "C" apo_status fname(apo_cuda_nose_hoover_integrator *it, const type v) { \
+    return guard([&]() -> apo_status {                                          \
+      APO_RETURN_IF(require_handle(it, #fname, "CudaNoseHooverIntegrator"));    \
+      body;                                                                     \
+      return APO_STATUS_OK;                                                     \
+    }, #fname);                                                                 \
+  }
+NH_SET(apo_cuda_nose_hoover_integrator_set_reference_temperature, double,
+       if (!(v >= 0)) return invalid("set_reference_temperature", "temperature must be >= 0");
+       it->object->setReferenceTemperature(v))
+NH_SET(apo_cuda_nose_hoover_integrator_set_nose_hoover_piston_mass, double,
+       if (!(v > 0)) return invalid("set_nose_hoover_piston_mass", "mass must be positive");
+       it->object->setNoseHooverPistonMass(v))
+NH_SET(apo_cuda_nose_hoover_integrator_use_old_temperature, bool, it->object->useOldTemperature(v))
+
+extern "C" apo_status apo_cuda_nose_hoover_integrator_reset_average_temperature(
+    apo_cuda_nose_hoover_integrator *it) {
+  const char *fn = "apo_cuda_nose_hoover_integrator_reset_average_temperature";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(it, fn, "CudaNoseHooverIntegrator"));
+    if (it->object->getCharmmContext()) it->object->resetAverageTemperature();
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+#define NH_GET(fname, call)                                                                      \
+  extern "C" apo_status fname(double *t, const apo_cuda_nose_hoover_integrator *it) {            \
+    return guard([&]() -> apo_status {                                                           \
+      APO_RETURN_IF(require_ptr(t, #fname, "temperature"));                                      \
+      *t = 0.0;                                                                                  \
+      APO_RETURN_IF(require_handle(it, #fname, "CudaNoseHooverIntegrator"));                     \
+      *t = call;                                                                                 \
+      return APO_STATUS_OK;                                                                      \
+    }, #fname);                                                                                  \
+  }
+NH_GET(apo_cuda_nose_hoover_integrator_get_reference_temperature, it->object->getReferenceTemperature())
+NH_GET(apo_cuda_nose_hoover_integrator_get_average_temperature,
+       it->object->getCharmmContext() ? it->object->getAverageTemperature() : 0.0)
+NH_GET(apo_cuda_nose_hoover_integrator_get_instantaneous_temperature,
+       it->object->getCharmmContext() ? it->object->getInstantaneousTemperature() : 0.0)
+
+extern "C" apo_status apo_cuda_nose_hoover_integrator_as_cuda_integrator(
+    apo_cuda_integrator **out, apo_cuda_nose_hoover_integrator *it) {
+  const char *fn = "apo_cuda_nose_hoover_integrator_as_cuda_integrator";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(prepare_out(out, fn));
+    APO_RETURN_IF(require_handle(it, fn, "CudaNoseHooverIntegrator"));
+    *out = &it->base;
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+// ------------------------------------------------------------- Langevin ----
+
+extern "C" apo_status apo_cuda_langevin_thermostat_integrator_create(
+    apo_cuda_langevin_thermostat_integrator **out, const double dt) {
+  const char *fn = "apo_cuda_langevin_thermostat_integrator_create";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(prepare_out(out, fn));
+    if (!(dt > 0) || !std::isfinite(dt)) return invalid(fn, "time step must be positive");
+    auto h = std::make_unique<apo_cuda_langevin_thermostat_integrator>();
+    h->object = std::make_shared<apo::CudaLangevinThermostatIntegrator>(dt);
+    h->base.object = h->object;
+    *out = h.release();
+    return APO_STATUS_OK;
+  }, fn);
+}
+extern "C" void apo_cuda_langevin_thermostat_integrator_destroy(apo_cuda_langevin_thermostat_integrator *it) {
+  delete it;
+}
+
+#define LG_SET(fname, type, body)                                                        \
+  extern "C" apo_status fname(apo_cuda_langevin_thermostat_integrator *it, const type v) { \
+    return guard([&]() -> apo_status {                                                   \
+      APO_RETURN_IF(require_handle(it, #fname, "CudaLangevinThermostatIntegrator"));     \
+      body;                                                                              \
+      return APO_STATUS_OK;                                                              \
+    }, #fname);                                                                          \
+  }
+LG_SET(apo_cuda_langevin_thermostat_integrator_set_thermostat_friction, double,
+       if (!(v >= 0)) return invalid("set_thermostat_friction", "friction must be >= 0");
+       it->object->setThermostatFriction(v))
+LG_SET(apo_cuda_langevin_thermostat_integrator_set_reference_temperature, double,
+       if (!(v >= 0)) return invalid("set_reference_temperature", "temperature must be >= 0");
+       it->object->setReferenceTemperature(v))
+LG_SET(apo_cuda_langevin_thermostat_integrator_set_thermostat_rng_seed, uint64_t,
+       it->object->setThermostatRngSeed(v))
+
+extern "C" apo_status apo_cuda_langevin_thermostat_integrator_get_rng_sequence_pos(
+    unsigned long long *pos, const apo_cuda_langevin_thermostat_integrator *it) {
+  const char *fn = "apo_cuda_langevin_thermostat_integrator_get_rng_sequence_pos";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_ptr(pos, fn, "pos"));
+    APO_RETURN_IF(require_handle(it, fn, "CudaLangevinThermostatIntegrator"));
+    *pos = it->object->getCharmmContext() ? it->object->getRngSequencePos() : 0ull;
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_cuda_langevin_thermostat_integrator_as_cuda_integrator(
+    apo_cuda_integrator **out, apo_cuda_langevin_thermostat_integrator *it) {
+  const char *fn = "apo_cuda_langevin_thermostat_integrator_as_cuda_integrator";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(prepare_out(out, fn));
+    APO_RETURN_IF(require_handle(it, fn, "CudaLangevinThermostatIntegrator"));
+    *out = &it->base;
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+// ------------------------------------------------------------- leapfrog ----
+
+extern "C" apo_status apo_cuda_leap_frog_integrator_create(apo_cuda_leap_frog_integrator **out,
+                                                           const double dt) {
+  const char *fn = "apo_cuda_leap_frog_integrator_create";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(prepare_out(out, fn));
+    if (!(dt > 0) || !std::isfinite(dt)) return invalid(fn, "time step must be positive");
+    auto h = std::make_unique<apo_cuda_leap_frog_integrator>();
+    h->object = std::make_shared<apo::CudaLeapFrogIntegrator>(dt);
+    h->base.object = h->object;
+    *out = h.release();
+    return APO_STATUS_OK;
+  }, fn);
+}
+extern "C" void apo_cuda_leap_frog_integrator_destroy(apo_cuda_leap_frog_integrator *it) { delete it; }
+extern "C" apo_status apo_cuda_leap_frog_integrator_as_cuda_integrator(apo_cuda_integrator **out,
+                                                                       apo_cuda_leap_frog_integrator *it) {
+  const char *fn = "apo_cuda_leap_frog_integrator_as_cuda_integrator";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(prepare_out(out, fn));
+    APO_RETURN_IF(require_handle(it, fn, "CudaLeapFrogIntegrator"));
+    *out = &it->base;
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+// ----------------------------------------------------------- subscribers ----
+
+extern "C" apo_status apo_subscriber_set_report_frequency(apo_subscriber *s, const int f) {
+  const char *fn = "apo_subscriber_set_report_frequency";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(s, fn, "Subscriber"));
+    if (f <= 0) return invalid(fn, "report frequency must be positive");
+    s->object->setReportFrequency(f);
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_subscriber_get_report_frequency(int *f, const apo_subscriber *s) {
+  const char *fn = "apo_subscriber_get_report_frequency";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_ptr(f, fn, "report_frequency"));
+    APO_RETURN_IF(require_handle(s, fn, "Subscriber"));
+    *f = s->object->getReportFrequency();
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_dcd_subscriber_create_with_report_frequency(apo_dcd_subscriber **out,
+                                                                      const char *path, const int f) {
+  const char *fn = "apo_dcd_subscriber_create_with_report_frequency";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(prepare_out(out, fn));
+    APO_RETURN_IF(require_string(path, fn, "path"));
+    if (f <= 0) return invalid(fn, "report frequency must be positive");
+    auto h = std::make_unique<apo_dcd_subscriber>();
+    h->object = std::make_shared<apo::DcdSubscriber>(path, f);
+    h->base.object = h->object;
+    *out = h.release();
+    return APO_STATUS_OK;
+  }, fn);
+}
+extern "C" apo_status apo_dcd_subscriber_create(apo_dcd_subscriber **out, const char *path) {
+  return apo_dcd_subscriber_create_with_report_frequency(out, path, 1000);
+}
+extern "C" void apo_dcd_subscriber_destroy(apo_dcd_subscriber *s) { delete s; }
+extern "C" apo_status apo_dcd_subscriber_as_subscriber(apo_subscriber **out, apo_dcd_subscriber *s) {
+  const char *fn = "apo_dcd_subscriber_as_subscriber";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(prepare_out(out, fn));
+    APO_RETURN_IF(require_handle(s, fn, "DcdSubscriber"));
+    *out = &s->base;
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_restart_subscriber_create_with_report_frequency(apo_restart_subscriber **out,
+                                                                          const char *path, const int f) {
+  const char *fn = "apo_restart_subscriber_create_with_report_frequency";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(prepare_out(out, fn));
+    APO_RETURN_IF(require_string(path, fn, "path"));
+    (void)f;
+    return set_error(APO_STATUS_NOT_IMPLEMENTED,
+                     std::string(fn) + ": restart files are not implemented on this engine");
+  }, fn);
+}
+extern "C" apo_status apo_restart_subscriber_create(apo_restart_subscriber **out, const char *path) {
+  return apo_restart_subscriber_create_with_report_frequency(out, path, 1000);
+}
+extern "C" void apo_restart_subscriber_destroy(apo_restart_subscriber *s) { delete s; }
+extern "C" apo_status apo_restart_subscriber_as_subscriber(apo_subscriber **out, apo_restart_subscriber *s) {
+  const char *fn = "apo_restart_subscriber_as_subscriber";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(prepare_out(out, fn));
+    APO_RETURN_IF(require_handle(s, fn, "RestartSubscriber"));
+    *out = &s->base;
+    return APO_STATUS_OK;
+  }, fn);
+}

@@ -89,6 +89,10 @@ ForceManager::~ForceManager() {
     if (s) cudaStreamDestroy(s);
   for (cudaEvent_t e : {m_EvFork, m_EvNb, m_EvPme, m_EvBond})
     if (e) cudaEventDestroy(e);
+  for (auto &p : m_Timers) {
+    cudaEventDestroy(p.first);
+    cudaEventDestroy(p.second);
+  }
 }
 
 void ForceManager::setBoxDimensions(const std::array<double, 3> &box) {
@@ -223,7 +227,20 @@ void ForceManager::calcForce(const float4 *d_xyzq, bool calcEnergy, bool /*calcV
     a.stride = m_Stride;
     a.energy = m_Energy.p;
     a.setups = m_Setup.p;
+    cudaEvent_t t1 = nullptr;
+    if (m_Timing) {
+      if (m_TimerCursor >= (int)m_Timers.size()) {
+        cudaEvent_t e0, e1;
+        APO_CUDA(cudaEventCreate(&e0));
+        APO_CUDA(cudaEventCreate(&e1));
+        m_Timers.emplace_back(e0, e1);
+      }
+      APO_CUDA(cudaEventRecord(m_Timers[m_TimerCursor].first, m_SNb));
+      t1 = m_Timers[m_TimerCursor].second;
+      ++m_TimerCursor;
+    }
     launch_nonbonded(a, calcEnergy, m_Precise, m_SNb);
+    if (t1) APO_CUDA(cudaEventRecord(t1, m_SNb));
     APO_CUDA(cudaEventRecord(m_EvNb, m_SNb));
     APO_CUDA(cudaStreamWaitEvent(s, m_EvNb, 0));
   }
@@ -237,7 +254,8 @@ void ForceManager::calcForce(const float4 *d_xyzq, bool calcEnergy, bool /*calcV
   if (m_ComponentMask & 1) {
     APO_CUDA(cudaStreamWaitEvent(m_SBond, m_EvFork, 0));
     BondedArgs b;
-    b.xyzq = d_xyzq;
+    if (!m_StateCoords) throw std::runtime_error("ForceManager: no state coordinates attached");
+    b.coords = m_StateCoords;
     b.glo2loc = m_Nbl.glo2loc;
     b.force = m_Force.p;
     b.stride = m_Stride;
@@ -290,6 +308,24 @@ void ForceManager::getForces(std::vector<double> &out, cudaStream_t s) {
 
 unsigned ForceManager::readDeviceError(cudaStream_t s) { return m_Nbl.read_error(s); }
 
+void ForceManager::setKernelTiming(bool on) {
+  m_Timing = on;
+  m_TimerCursor = 0;
+}
+
+double ForceManager::kernelTimeMs(int &launches) {
+  double t = 0.0;
+  launches = 0;
+  for (int k = 0; k < m_TimerCursor && k < (int)m_Timers.size(); ++k) {
+    float ms = 0.f;
+    APO_CUDA(cudaEventSynchronize(m_Timers[k].second));
+    APO_CUDA(cudaEventElapsedTime(&ms, m_Timers[k].first, m_Timers[k].second));
+    t += ms;
+    ++launches;
+  }
+  return t;
+}
+
 // ------------------------------------------------------------ CharmmContext
 
 CharmmContext::CharmmContext(std::shared_ptr<ForceManager> fm) : m_Fm(std::move(fm)) {
@@ -311,6 +347,7 @@ CharmmContext::CharmmContext(std::shared_ptr<ForceManager> fm) : m_Fm(std::move(
   m_Coords.upload(c);
   launch_coords_to_xyzq(m_Coords.p, m_Xyzq.p, m_N, m_Stream);
   m_Groups.upload(t.groups);
+  m_Fm->setStateCoordinates(m_Coords.p);
   std::random_device rd;
   m_Seed = rd();
   useHolonomicConstraints(true);

@@ -105,6 +105,9 @@ class ForceManager {
   // clear == false); energies into the fixed-point energy slots
   void calcForce(const float4 *d_xyzq, bool calcEnergy, bool calcVirial, cudaStream_t s,
                  bool clear = true);
+  // FP64 state coordinates (x, y, z, q) in atom order, read by the bonded
+  // terms; set by the CharmmContext that owns them
+  void setStateCoordinates(const double4 *c) { m_StateCoords = c; }
 
   std::map<std::string, double> getEnergyComponents(cudaStream_t s);
   double getPotentialEnergy(cudaStream_t s);
@@ -119,6 +122,13 @@ class ForceManager {
   Pme &pme() { return m_Pme; }
   double selfEnergy() const { return m_SelfEnergy; }
   unsigned readDeviceError(cudaStream_t s);
+  // CUDA-event timing of every direct-space launch (on the stream it runs
+  // on); events of a captured graph are replayed with the graph, so the
+  // cursor is rewound at the start of every integration segment
+  void setKernelTiming(bool on);
+  void rewindKernelTimers() { m_TimerCursor = 0; }
+  // sum (ms) over the launches recorded since the last rewind
+  double kernelTimeMs(int &launches);
 
  private:
   std::shared_ptr<CharmmPSF> m_Psf;
@@ -134,6 +144,7 @@ class ForceManager {
   int m_TilesPerWork = 8;
   int m_ComponentMask = 7;
   double m_SelfEnergy = 0.0;
+  const double4 *m_StateCoords = nullptr;
   Topology m_Top;
 
   NeighborList m_Nbl;
@@ -149,6 +160,9 @@ class ForceManager {
   DeviceArray<int4> m_AngleIJK, m_DiheIJKL, m_ImpIJKL;
   DeviceArray<float4> m_DiheCoef;
   DeviceArray<double> m_Scratch;
+  bool m_Timing = false;
+  int m_TimerCursor = 0;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> m_Timers;
   cudaStream_t m_SNb = nullptr, m_SPme = nullptr, m_SBond = nullptr;
   cudaEvent_t m_EvFork = nullptr, m_EvNb = nullptr, m_EvPme = nullptr, m_EvBond = nullptr;
 };

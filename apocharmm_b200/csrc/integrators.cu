@@ -1,0 +1,913 @@
+// Integrators; see integrators.h.
+#include "integrators.h"
+
+#include <curand_kernel.h>
+
+#include <algorithm>
+#include <cmath>
+#include <random>
+#include <stdexcept>
+#include <vector>
+
+#include "device_util.cuh"
+
+namespace apo {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kMaxBlocks = 4096;
+
+// constraint group kinds
+enum GroupKind : int { kFree = 0, kSettle = 1, kShake = 2 };
+
+struct Scalars {
+  double ke[2];              // [0] average of half/on/half-step KE, [1] on-step KE
+  double avgT[2];
+  double piston_v, piston_v_prev, piston_f, piston_f_prev, piston_mass;
+  double com[4];             // mass-weighted delta sum + total mass
+  unsigned long long rngpos;
+  long long step;
+  long long window;
+  unsigned counter;
+  unsigned pad;
+};
+
+struct SettleConst {
+  double wo, wh, ra, rb, rc;
+};
+
+// TIP3 geometry and masses of SETTLE (src/CudaHolonomicConstraint.cu:18-33)
+SettleConst make_settle() {
+  const double mO = 15.99940, mH = 1.00800, mH2O = 18.0154;
+  const double rOHsq = 0.91623184, rHHsq = 2.29189321;
+  SettleConst s;
+  s.wo = mO / mH2O;
+  s.wh = mH / mH2O;
+  s.ra = s.wh * std::sqrt(4.0 * rOHsq - rHHsq);
+  s.rb = s.ra * mO / (2.0 * mH);
+  s.rc = std::sqrt(rHHsq) / 2.0;
+  return s;
+}
+
+// ------------------------------------------------------------ vector math
+struct d3 {
+  double x, y, z;
+};
+__device__ __forceinline__ d3 mk(double x, double y, double z) { return {x, y, z}; }
+__device__ __forceinline__ d3 operator+(d3 a, d3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ d3 operator-(d3 a, d3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ d3 operator*(double s, d3 a) { return {s * a.x, s * a.y, s * a.z}; }
+__device__ __forceinline__ double dot(d3 a, d3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ d3 cross(d3 a, d3 b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ d3 xyz(double4 v) { return {v.x, v.y, v.z}; }
+
+// Analytic SETTLE (Miyamoto & Kollman, J. Comput. Chem. 13, 952 (1992)):
+// moves the unconstrained positions n[0..2] (O, H, H) onto the rigid TIP3
+// geometry, keeping the centre of mass, using the constrained positions
+// o[0..2] of the previous step to fix the frame.
+__device__ void settle(const d3 o[3], d3 n[3], const SettleConst &k) {
+  const d3 com = k.wo * n[0] + k.wh * (n[1] + n[2]);
+  const d3 a1 = n[0] - com, b1 = n[1] - com, c1 = n[2] - com;
+  const d3 b0 = o[1] - o[0], c0 = o[2] - o[0];
+  d3 ez = cross(b0, c0);
+  d3 ex = cross(a1, ez);
+  d3 ey = cross(ez, ex);
+  ex = (1.0 / sqrt(dot(ex, ex))) * ex;
+  ey = (1.0 / sqrt(dot(ey, ey))) * ey;
+  ez = (1.0 / sqrt(dot(ez, ez))) * ez;
+  const double xb0 = dot(ex, b0), yb0 = dot(ey, b0), xc0 = dot(ex, c0), yc0 = dot(ey, c0);
+  const double za1 = dot(ez, a1);
+  const double xb1 = dot(ex, b1), yb1 = dot(ey, b1), zb1 = dot(ez, b1);
+  const double xc1 = dot(ex, c1), yc1 = dot(ey, c1), zc1 = dot(ez, c1);
+  const double sinphi = za1 / k.ra;
+  const double cosphi = sqrt(fmax(0.0, 1.0 - sinphi * sinphi));
+  const double sinpsi = (zb1 - zc1) / (2.0 * k.rc * cosphi);
+  const double cospsi = sqrt(fmax(0.0, 1.0 - sinpsi * sinpsi));
+  const double ya2 = k.ra * cosphi;
+  const double xb2 = -k.rc * cospsi;
+  const double yb2 = -k.rb * cosphi - k.rc * sinpsi * sinphi;
+  const double yc2 = -k.rb * cosphi + k.rc * sinpsi * sinphi;
+  const double alpha = xb2 * (xb0 - xc0) + yb0 * yb2 + yc0 * yc2;
+  const double beta = xb2 * (yc0 - yb0) + xb0 * yb2 + xc0 * yc2;
+  const double gamma = xb0 * yb1 - xb1 * yb0 + xc0 * yc1 - xc1 * yc0;
+  const double ab2 = alpha * alpha + beta * beta;
+  const double sinth = (alpha * gamma - beta * sqrt(fmax(0.0, ab2 - gamma * gamma))) / ab2;
+  const double costh = sqrt(fmax(0.0, 1.0 - sinth * sinth));
+  const d3 a3 = mk(-ya2 * sinth, ya2 * costh, za1);
+  const d3 b3 = mk(xb2 * costh - yb2 * sinth, xb2 * sinth + yb2 * costh, zb1);
+  const d3 c3 = mk(-xb2 * costh - yc2 * sinth, -xb2 * sinth + yc2 * costh, zc1);
+  n[0] = com + a3.x * ex + a3.y * ey + a3.z * ez;
+  n[1] = com + b3.x * ex + b3.y * ey + b3.z * ez;
+  n[2] = com + c3.x * ex + c3.y * ey + c3.z * ez;
+}
+
+// SHAKE for an X-H_m cluster (m = 1..3): exact for one bond, otherwise the
+// iterative bond-by-bond scheme of Ryckaert, Ciccotti & Berendsen (1977) to a
+// relative tolerance of 1e-10 (at most 200 sweeps).  o = reference
+// (constrained) positions, n = positions to correct.
+__device__ void shake(const d3 *o, d3 *n, int m, float4 p) {
+  const double ic = p.x, ih = p.w, b2 = p.z;
+  if (m == 1) {
+    const d3 r = o[0] - o[1], q = n[0] - n[1];
+    const double rr = dot(r, r), rq = dot(r, q), qq = dot(q, q);
+    const double lam = (-rq + sqrt(fmax(0.0, rq * rq + rr * (b2 - qq)))) / (rr * (ic + ih));
+    n[0] = n[0] + (ic * lam) * r;
+    n[1] = n[1] - (ih * lam) * r;
+    return;
+  }
+  for (int it = 0; it < 200; ++it) {
+    bool done = true;
+    for (int h = 1; h <= m; ++h) {
+      const d3 q = n[0] - n[h];
+      const double diff = b2 - dot(q, q);
+      if (fabs(diff) > 2e-10 * b2) {
+        done = false;
+        const d3 r = o[0] - o[h];
+        const double g = diff / (2.0 * dot(r, q) * (ic + ih));
+        n[0] = n[0] + (ic * g) * r;
+        n[h] = n[h] - (ih * g) * r;
+      }
+    }
+    if (done) break;
+  }
+}
+
+__device__ __forceinline__ void apply_constraint(int kind, int m, const d3 *o, d3 *n,
+                                                 const SettleConst &sk, const float4 *shake_p,
+                                                 int pidx) {
+  if (kind == kSettle) settle(o, n, sk);
+  else if (kind == kShake) shake(o, n, m - 1, shake_p[pidx]);
+}
+
+// gradient of an atom from the fixed-point slot buffer; the slot is cleared
+// for the next force evaluation
+__device__ __forceinline__ d3 take_grad(long long *f, int stride, int slot) {
+  const long long gx = f[slot], gy = f[stride + slot], gz = f[2 * stride + slot];
+  f[slot] = 0;
+  f[stride + slot] = 0;
+  f[2 * stride + slot] = 0;
+  return mk((double)gx * kInvForceScale, (double)gy * kInvForceScale,
+            (double)gz * kInvForceScale);
+}
+
+__device__ __forceinline__ void store_position(int a, d3 x, double4 *coords, float4 *xyzq,
+                                               const int *glo2loc, const float4 *slot_shift,
+                                               float4 *xyzq_s) {
+  const double q = coords[a].w;
+  coords[a] = make_double4(x.x, x.y, x.z, q);
+  const float4 f = make_float4((float)x.x, (float)x.y, (float)x.z, (float)q);
+  xyzq[a] = f;
+  const int s = glo2loc[a];
+  const float4 sh = slot_shift[s];
+  xyzq_s[s] = make_float4(f.x + sh.x, f.y + sh.y, f.z + sh.z, f.w);
+}
+
+// block-wide sum of two doubles; thread 0 writes partials[2*block + k]
+__device__ void block_partials(double a, double b, double *partials) {
+  __shared__ double sh[2][kThreads / 32];
+  a = warp_sum(a);
+  b = warp_sum(b);
+  if ((threadIdx.x & 31) == 0) {
+    sh[0][threadIdx.x >> 5] = a;
+    sh[1][threadIdx.x >> 5] = b;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s0 = 0, s1 = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      s0 += sh[0][w];
+      s1 += sh[1][w];
+    }
+    partials[2 * blockIdx.x] = s0;
+    partials[2 * blockIdx.x + 1] = s1;
+  }
+}
+
+// true in the block that finishes last; partials of all blocks are visible
+__device__ bool is_last_block(unsigned *counter) {
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  __syncthreads();
+  return last;
+}
+
+// sum of the partials in a fixed order (same result for every run)
+__device__ void sum_partials(const double *partials, double &s0, double &s1) {
+  double a = 0, b = 0;
+  if (threadIdx.x < 32) {
+    for (int k = threadIdx.x; k < (int)gridDim.x; k += 32) {
+      a += partials[2 * k];
+      b += partials[2 * k + 1];
+    }
+    a = warp_sum(a);
+    b = warp_sum(b);
+  }
+  s0 = a;
+  s1 = b;
+}
+
+struct Common {
+  int ngroups;
+  const int4 *groups;   // atoms (-1 unused)
+  const int2 *gmeta;    // (kind, shake parameter index)
+  const float4 *shake_p;
+  double4 *coords, *vel, *dprev, *delta, *dpred, *ref;
+  float4 *xyzq;
+  long long *force;
+  int stride;
+  const int *glo2loc;
+  const float4 *slot_shift;
+  float4 *xyzq_s;
+  Scalars *sc;
+  double *partials;
+  SettleConst sk;
+  int ndegf;
+  double dt;
+};
+
+__device__ __forceinline__ int group_atoms(const Common &c, int g, int (&at)[4]) {
+  const int4 a = c.groups[g];
+  at[0] = a.x;
+  at[1] = a.y;
+  at[2] = a.z;
+  at[3] = a.w;
+  return 1 + (a.y >= 0) + (a.z >= 0) + (a.w >= 0);
+}
+
+__device__ void finish_temperature(const Common &c, double ke0, double ke1) {
+  c.sc->ke[0] = ke0;
+  c.sc->ke[1] = ke1;
+  const double s = (double)(c.sc->window + 1);
+  for (int k = 0; k < 2; ++k) {
+    const double t = (k ? ke1 : ke0) / (0.5 * c.ndegf * kBoltz);
+    c.sc->avgT[k] += (t - c.sc->avgT[k]) / s;
+  }
+  c.sc->window += 1;
+}
+
+// ------------------------------------------------------------ Langevin step
+// Position-Verlet "delta" Langevin of src/CudaLangevinThermostatIntegrator.cu:576-640:
+//   delta = alpha*delta_prev - dt^2/m/(1+g/2) * (grad + sqrt(2 g kT m)/dt * xi)
+//   x += delta; constrain; delta = x - x_old;
+//   v = sqrt(1+g/2)/(2 dt) * (delta + delta_prev)
+__global__ void __launch_bounds__(kThreads) langevin_kernel(Common c, double gamma, double kbt,
+                                                            unsigned long long seed) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const double dt = c.dt, dt2 = dt * dt;
+  const double hg = 0.5 * gamma, denom = 1.0 / (1.0 + hg), alpha = (1.0 - hg) * denom;
+  const double vfac = 0.5 * sqrt(1.0 + hg) / dt, idt = 1.0 / dt;
+  double ke0 = 0.0, ke1 = 0.0;
+  const unsigned long long pos = c.sc->rngpos;
+  if (g < c.ngroups) {
+    int at[4];
+    const int m = group_atoms(c, g, at);
+    const int2 meta = c.gmeta[g];
+    d3 o[4], n[4], dp[4];
+    for (int k = 0; k < m; ++k) {
+      const int a = at[k];
+      const double4 x = c.coords[a];
+      const double4 v = c.vel[a];
+      o[k] = xyz(x);
+      dp[k] = xyz(c.dprev[a]);
+      const d3 gr = take_grad(c.force, c.stride, c.glo2loc[a]);
+      curandStatePhilox4_32_10_t st;
+      curand_init(seed, (unsigned long long)a, 0ull, &st);
+      skipahead(pos, &st);
+      const float4 rn = curand_normal4(&st);
+      const double rdf = sqrt(2.0 * gamma * kbt / v.w) / dt;
+      const double fact = dt2 * v.w * denom;
+      const d3 f = gr + rdf * mk(rn.x, rn.y, rn.z);
+      n[k] = o[k] + (alpha * dp[k] - fact * f);
+    }
+    apply_constraint(meta.x, m, o, n, c.sk, c.shake_p, meta.y);
+    for (int k = 0; k < m; ++k) {
+      const int a = at[k];
+      const d3 d = n[k] - o[k];
+      const d3 v = vfac * (d + dp[k]);
+      const double mass = 1.0 / c.vel[a].w;
+      const d3 u1 = idt * dp[k], u2 = idt * d;
+      const double kon = 0.5 * mass * dot(v, v);
+      ke0 += (0.5 * mass * dot(u1, u1) + kon + 0.5 * mass * dot(u2, u2)) / 3.0;
+      ke1 += kon;
+      c.vel[a] = make_double4(v.x, v.y, v.z, c.vel[a].w);
+      c.dprev[a] = make_double4(d.x, d.y, d.z, 0.0);
+      store_position(a, n[k], c.coords, c.xyzq, c.glo2loc, c.slot_shift, c.xyzq_s);
+    }
+  }
+  block_partials(ke0, ke1, c.partials);
+  if (is_last_block(&c.sc->counter)) {
+    double s0, s1;
+    sum_partials(c.partials, s0, s1);
+    if (threadIdx.x == 0) {
+      finish_temperature(c, s0, s1);
+      c.sc->rngpos += 4;  // curand_normal4 consumes four values per step
+      c.sc->step += 1;
+      c.sc->counter = 0;
+    }
+  }
+}
+
+// -------------------------------------------------------- Nose-Hoover step
+// src/CudaNoseHooverIntegrator.cu:647-1004, split at the grid-wide
+// kinetic-energy reductions:
+//   K0 half step + constraint + KE(v_old) + piston update
+//   K1..K3 predictor-corrector (K1, K2 also KE + piston)
+//   K4 constraint + on-step velocity + KE + piston + average temperature
+__device__ void piston_update(Scalars *sc, double ke_sel, double ke_ref, double dt) {
+  sc->piston_f = 2.0 * dt * (ke_sel - ke_ref) / sc->piston_mass;
+  if (sc->piston_f_prev == 0.0) sc->piston_f_prev = sc->piston_f;
+  sc->piston_v = sc->piston_v_prev + 0.5 * (sc->piston_f + sc->piston_f_prev);
+}
+
+__global__ void __launch_bounds__(kThreads) nh_half_kernel(Common c, double ke_ref, int use_old) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const double dt = c.dt, dt2 = dt * dt, idt = 1.0 / dt;
+  double ke0 = 0, ke1 = 0;
+  if (g < c.ngroups) {
+    int at[4];
+    const int m = group_atoms(c, g, at);
+    const int2 meta = c.gmeta[g];
+    d3 o[4], n[4];
+    for (int k = 0; k < m; ++k) {
+      const int a = at[k];
+      o[k] = xyz(c.coords[a]);
+      c.ref[a] = c.coords[a];
+      const d3 gr = take_grad(c.force, c.stride, c.glo2loc[a]);
+      n[k] = o[k] + (xyz(c.dprev[a]) - (dt2 * c.vel[a].w) * gr);
+    }
+    apply_constraint(meta.x, m, o, n, c.sk, c.shake_p, meta.y);
+    for (int k = 0; k < m; ++k) {
+      const int a = at[k];
+      const d3 d = n[k] - o[k];
+      c.delta[a] = make_double4(d.x, d.y, d.z, 0.0);
+      c.dpred[a] = c.delta[a];
+      c.coords[a] = make_double4(n[k].x, n[k].y, n[k].z, c.coords[a].w);
+      const double mass = 1.0 / c.vel[a].w;
+      const d3 v = xyz(c.vel[a]);
+      const d3 u1 = idt * xyz(c.dprev[a]), u2 = idt * d;
+      const double kon = 0.5 * mass * dot(v, v);
+      ke0 += (0.5 * mass * dot(u1, u1) + kon + 0.5 * mass * dot(u2, u2)) / 3.0;
+      ke1 += kon;
+    }
+  }
+  block_partials(ke0, ke1, c.partials);
+  if (is_last_block(&c.sc->counter)) {
+    double s0, s1;
+    sum_partials(c.partials, s0, s1);
+    if (threadIdx.x == 0) {
+      c.sc->piston_v_prev = c.sc->piston_v;
+      c.sc->piston_f_prev = c.sc->piston_f;
+      piston_update(c.sc, use_old ? s1 : s0, ke_ref, dt);
+      c.sc->counter = 0;
+    }
+  }
+}
+
+// predictor-corrector pass over atoms; with KE also the next piston update
+template <bool KE>
+__global__ void __launch_bounds__(kThreads) nh_pc_kernel(Common c, int natom, double ke_ref,
+                                                         int use_old) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  const double dt = c.dt, idt = 1.0 / dt, fact = 0.5 / dt;
+  const double xi = c.sc->piston_v;
+  double ke0 = 0, ke1 = 0;
+  if (a < natom) {
+    const d3 dprev = xyz(c.dprev[a]), dpred = xyz(c.dpred[a]), d = xyz(c.delta[a]);
+    const d3 v = fact * (dprev + dpred);
+    const d3 np = d - (dt * dt * xi) * v;
+    c.dpred[a] = make_double4(np.x, np.y, np.z, 0.0);
+    c.vel[a] = make_double4(v.x, v.y, v.z, c.vel[a].w);
+    const d3 r = xyz(c.ref[a]);
+    c.coords[a] = make_double4(r.x + np.x, r.y + np.y, r.z + np.z, c.coords[a].w);
+    if (KE) {
+      const double mass = 1.0 / c.vel[a].w;
+      const d3 u1 = idt * dprev, u2 = idt * d;
+      const double kon = 0.5 * mass * dot(v, v);
+      ke0 = (0.5 * mass * dot(u1, u1) + kon + 0.5 * mass * dot(u2, u2)) / 3.0;
+      ke1 = kon;
+    }
+  }
+  if (KE) {
+    block_partials(ke0, ke1, c.partials);
+    if (is_last_block(&c.sc->counter)) {
+      double s0, s1;
+      sum_partials(c.partials, s0, s1);
+      if (threadIdx.x == 0) {
+        piston_update(c.sc, use_old ? s1 : s0, ke_ref, dt);
+        c.sc->counter = 0;
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) nh_final_kernel(Common c, double ke_ref, int use_old) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const double dt = c.dt, idt = 1.0 / dt, fact = 0.5 / dt;
+  double ke0 = 0, ke1 = 0;
+  if (g < c.ngroups) {
+    int at[4];
+    const int m = group_atoms(c, g, at);
+    const int2 meta = c.gmeta[g];
+    d3 o[4], n[4];
+    for (int k = 0; k < m; ++k) {
+      o[k] = xyz(c.ref[at[k]]);
+      n[k] = xyz(c.coords[at[k]]);
+    }
+    apply_constraint(meta.x, m, o, n, c.sk, c.shake_p, meta.y);
+    for (int k = 0; k < m; ++k) {
+      const int a = at[k];
+      const d3 d = n[k] - o[k];
+      const d3 dp = xyz(c.dprev[a]);
+      const d3 v = fact * (d + dp);
+      const double mass = 1.0 / c.vel[a].w;
+      const d3 u1 = idt * dp, u2 = idt * d;
+      const double kon = 0.5 * mass * dot(v, v);
+      ke0 += (0.5 * mass * dot(u1, u1) + kon + 0.5 * mass * dot(u2, u2)) / 3.0;
+      ke1 += kon;
+      c.vel[a] = make_double4(v.x, v.y, v.z, c.vel[a].w);
+      c.dprev[a] = make_double4(d.x, d.y, d.z, 0.0);
+      store_position(a, n[k], c.coords, c.xyzq, c.glo2loc, c.slot_shift, c.xyzq_s);
+    }
+  }
+  block_partials(ke0, ke1, c.partials);
+  if (is_last_block(&c.sc->counter)) {
+    double s0, s1;
+    sum_partials(c.partials, s0, s1);
+    if (threadIdx.x == 0) {
+      piston_update(c.sc, use_old ? s1 : s0, ke_ref, dt);
+      finish_temperature(c, s0, s1);
+      c.sc->step += 1;
+      c.sc->counter = 0;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- leapfrog
+// v -= dt grad/m; x += dt v (src/CudaLeapFrogIntegrator.cu:22-41).  The
+// reference advances only the single-precision copy; here the FP64 state is
+// advanced and the single-precision copies are refreshed from it.
+__global__ void leapfrog_kernel(Common c, int natom) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  double ke1 = 0;
+  if (a < natom) {
+    const d3 gr = take_grad(c.force, c.stride, c.glo2loc[a]);
+    double4 v = c.vel[a];
+    const d3 nv = xyz(v) - (c.dt * v.w) * gr;
+    c.vel[a] = make_double4(nv.x, nv.y, nv.z, v.w);
+    const d3 x = xyz(c.coords[a]) + c.dt * nv;
+    store_position(a, x, c.coords, c.xyzq, c.glo2loc, c.slot_shift, c.xyzq_s);
+    ke1 = 0.5 * dot(nv, nv) / v.w;
+  }
+  block_partials(ke1, ke1, c.partials);
+  if (is_last_block(&c.sc->counter)) {
+    double s0, s1;
+    sum_partials(c.partials, s0, s1);
+    if (threadIdx.x == 0) {
+      finish_temperature(c, s0, s1);
+      c.sc->step += 1;
+      c.sc->counter = 0;
+    }
+  }
+}
+
+// ----------------------------------------------------- initialisation / COM
+// delta and delta_prev from velocities and the first forces
+// (src/CudaLangevinThermostatIntegrator.cu:138-165)
+__global__ void init_delta_kernel(Common c, int natom, double gamma) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= natom) return;
+  const double dt = c.dt, hg = 0.5 * gamma;
+  const double a0 = dt * sqrt(1.0 + hg), a1 = dt * (1.0 - hg) / sqrt(1.0 + hg);
+  const d3 gr = take_grad(c.force, c.stride, c.glo2loc[a]);
+  const double4 v = c.vel[a];
+  const double fact = 0.5 * dt * dt * v.w;
+  const d3 d = a0 * xyz(v) - fact * gr;
+  const d3 dp = a1 * xyz(v) + fact * gr;
+  c.delta[a] = make_double4(d.x, d.y, d.z, 0.0);
+  c.dprev[a] = make_double4(dp.x, dp.y, dp.z, 0.0);
+}
+
+// mode 0: constrain the current positions against themselves (projection
+// onto the constraint surface); mode 1: back step x - delta_prev, constrain
+// against x, then delta_prev = x - x_constrained
+__global__ void init_constrain_kernel(Common c, int mode) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= c.ngroups) return;
+  int at[4];
+  const int m = group_atoms(c, g, at);
+  const int2 meta = c.gmeta[g];
+  d3 o[4], n[4];
+  for (int k = 0; k < m; ++k) {
+    o[k] = xyz(c.coords[at[k]]);
+    n[k] = mode == 0 ? o[k] : o[k] - xyz(c.dprev[at[k]]);
+  }
+  apply_constraint(meta.x, m, o, n, c.sk, c.shake_p, meta.y);
+  for (int k = 0; k < m; ++k) {
+    const int a = at[k];
+    if (mode == 0) {
+      store_position(a, n[k], c.coords, c.xyzq, c.glo2loc, c.slot_shift, c.xyzq_s);
+    } else {
+      const d3 d = o[k] - n[k];
+      c.dprev[a] = make_double4(d.x, d.y, d.z, 0.0);
+    }
+  }
+}
+
+// centre-of-mass motion removal from delta_prev, every `freq` steps
+// (src/CudaLangevinThermostatIntegrator.cu:832-875), gated on the device
+// step counter so the same graph serves every segment
+__global__ void com_sum_kernel(Common c, int natom, int freq) {
+  if (c.sc->step % freq != 0) return;
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  __shared__ double sh[4][kThreads / 32];
+  double v[4] = {0, 0, 0, 0};
+  if (a < natom) {
+    const double mass = 1.0 / c.vel[a].w;
+    const double4 d = c.dprev[a];
+    v[0] = d.x * mass;
+    v[1] = d.y * mass;
+    v[2] = d.z * mass;
+    v[3] = mass;
+  }
+  for (int k = 0; k < 4; ++k) {
+    const double s = warp_sum(v[k]);
+    if ((threadIdx.x & 31) == 0) sh[k][threadIdx.x >> 5] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    double s = 0;
+    for (int w = 0; w < kThreads / 32; ++w) s += sh[threadIdx.x][w];
+    c.partials[4 * blockIdx.x + threadIdx.x] = s;
+  }
+  if (is_last_block(&c.sc->counter)) {
+    if (threadIdx.x < 4) {
+      double s = 0;
+      for (int b = 0; b < (int)gridDim.x; ++b) s += c.partials[4 * b + threadIdx.x];
+      c.sc->com[threadIdx.x] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) c.sc->counter = 0;
+  }
+}
+
+__global__ void com_apply_kernel(Common c, int natom, int freq) {
+  if (c.sc->step % freq != 0) return;
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= natom) return;
+  const double im = 1.0 / c.sc->com[3];
+  double4 d = c.dprev[a];
+  d.x -= c.sc->com[0] * im;
+  d.y -= c.sc->com[1] * im;
+  d.z -= c.sc->com[2] * im;
+  c.dprev[a] = d;
+}
+
+template <typename T>
+void upload(DeviceArray<T> &d, const std::vector<T> &v) {
+  d.upload(v.empty() ? std::vector<T>(1) : v);
+}
+
+}  // namespace
+
+struct IntegratorState {
+  DeviceArray<int4> groups;
+  DeviceArray<int2> gmeta;
+  DeviceArray<float4> shake_p;
+  DeviceArray<double4> dprev, delta, dpred, ref;
+  DeviceArray<Scalars> sc;
+  DeviceArray<double> partials;
+  int ngroups = 0, natom = 0;
+  Common c{};
+  int blocks_groups = 0, blocks_atoms = 0;
+};
+
+// -------------------------------------------------------------- base class
+
+CudaIntegrator::CudaIntegrator(double ps) : m_Dt(ps / kTimfac) {
+  if (!(ps > 0)) throw std::invalid_argument("time step must be positive");
+}
+
+CudaIntegrator::~CudaIntegrator() { clearGraphs(); }
+
+void CudaIntegrator::clearGraphs() {
+  for (auto &kv : m_Graphs) cudaGraphExecDestroy(kv.second);
+  m_Graphs.clear();
+}
+
+void CudaIntegrator::setTimeStep(double ps) {
+  if (!(ps > 0)) throw std::invalid_argument("time step must be positive");
+  m_Dt = ps / kTimfac;
+  clearGraphs();
+  if (m_S) m_S->c.dt = m_Dt;
+}
+
+void CudaIntegrator::setNonbondedListUpdateFrequency(int f) {
+  if (f < 1) throw std::invalid_argument("list update frequency must be >= 1");
+  m_ListFreq = f;
+  clearGraphs();
+}
+
+cudaStream_t CudaIntegrator::stream() const { return m_Ctx ? m_Ctx->stream() : nullptr; }
+
+int CudaIntegrator::kernelsPerRebuild() const { return 11; }
+
+void CudaIntegrator::setCharmmContext(std::shared_ptr<CharmmContext> ctx) {
+  if (m_Ctx) throw std::invalid_argument("A CharmmContext object was already set for this CudaIntegrator.");
+  if (!ctx) throw std::invalid_argument("null CharmmContext");
+  m_Ctx = std::move(ctx);
+  buildGroups();
+  initialize();
+  m_Initialized = true;
+}
+
+void CudaIntegrator::buildGroups() {
+  auto fm = m_Ctx->getForceManager();
+  const Topology &t = fm->topology();
+  const int n = t.natom;
+  const bool hol = m_Ctx->isUsingHolonomicConstraints();
+  std::vector<int> owner(n, -1);
+  std::vector<int4> groups;
+  std::vector<int2> meta;
+  if (hol) {
+    for (auto &w : t.waters) {
+      owner[w.x] = owner[w.y] = owner[w.z] = (int)groups.size();
+      groups.push_back({w.x, w.y, w.z, -1});
+      meta.push_back({kSettle, 0});
+    }
+    for (size_t k = 0; k < t.shake_atoms.size(); ++k) {
+      const int4 s = t.shake_atoms[k];
+      bool clash = owner[s.x] >= 0 || owner[s.y] >= 0 || (s.z >= 0 && owner[s.z] >= 0) ||
+                   (s.w >= 0 && owner[s.w] >= 0);
+      if (clash) throw std::invalid_argument("an atom belongs to two constraint groups");
+      owner[s.x] = owner[s.y] = (int)groups.size();
+      if (s.z >= 0) owner[s.z] = (int)groups.size();
+      if (s.w >= 0) owner[s.w] = (int)groups.size();
+      groups.push_back(s);
+      meta.push_back({kShake, (int)k});
+    }
+  }
+  // free atoms in runs of up to four consecutive atoms
+  for (int i = 0; i < n;) {
+    if (owner[i] >= 0) {
+      ++i;
+      continue;
+    }
+    int4 g = {i, -1, -1, -1};
+    int *slot = &g.y;
+    int k = 0;
+    int j = i + 1;
+    while (k < 3 && j < n && owner[j] < 0) {
+      slot[k++] = j;
+      ++j;
+    }
+    groups.push_back(g);
+    meta.push_back({kFree, 0});
+    i = j;
+  }
+  m_S = std::make_unique<IntegratorState>();
+  IntegratorState &S = *m_S;
+  S.natom = n;
+  S.ngroups = (int)groups.size();
+  S.groups.upload(groups);
+  S.gmeta.upload(meta);
+  upload(S.shake_p, t.shake_p);
+  S.dprev.alloc(n);
+  S.delta.alloc(n);
+  S.dpred.alloc(n);
+  S.ref.alloc(n);
+  APO_CUDA(cudaMemset(S.dprev.p, 0, n * sizeof(double4)));
+  APO_CUDA(cudaMemset(S.delta.p, 0, n * sizeof(double4)));
+  S.sc.alloc(1);
+  Scalars z{};
+  APO_CUDA(cudaMemcpy(S.sc.p, &z, sizeof(z), cudaMemcpyHostToDevice));
+  S.blocks_groups = (S.ngroups + kThreads - 1) / kThreads;
+  S.blocks_atoms = (n + kThreads - 1) / kThreads;
+  if (std::max(S.blocks_groups, S.blocks_atoms) > kMaxBlocks * 64)
+    throw std::invalid_argument("system too large for the integrator's reduction buffer");
+  S.partials.alloc((size_t)4 * std::max(S.blocks_groups, S.blocks_atoms) + 8);
+  Common &c = S.c;
+  c.ngroups = S.ngroups;
+  c.groups = S.groups.p;
+  c.gmeta = S.gmeta.p;
+  c.shake_p = S.shake_p.p;
+  c.coords = m_Ctx->coords();
+  c.vel = m_Ctx->velMass();
+  c.dprev = S.dprev.p;
+  c.delta = S.delta.p;
+  c.dpred = S.dpred.p;
+  c.ref = S.ref.p;
+  c.xyzq = m_Ctx->xyzq();
+  c.force = fm->forceFixed();
+  c.stride = fm->forceStride();
+  c.glo2loc = fm->neighborList().glo2loc;
+  c.slot_shift = fm->neighborList().slot_shift;
+  c.xyzq_s = fm->neighborList().xyzq_s;
+  c.sc = S.sc.p;
+  c.partials = S.partials.p;
+  c.sk = make_settle();
+  c.ndegf = m_Ctx->getDegreesOfFreedom();
+  c.dt = m_Dt;
+}
+
+void CudaIntegrator::forcesForStep(cudaStream_t s) {
+  m_Ctx->getForceManager()->calcForce(m_Ctx->xyzq(), false, false, s, /*clear=*/false);
+}
+
+void CudaIntegrator::segment(int nsteps, cudaStream_t s) {
+  IntegratorState &S = *m_S;
+  m_Ctx->getForceManager()->rewindKernelTimers();
+  com_sum_kernel<<<S.blocks_atoms, kThreads, 0, s>>>(S.c, S.natom, m_ComFreq);
+  com_apply_kernel<<<S.blocks_atoms, kThreads, 0, s>>>(S.c, S.natom, m_ComFreq);
+  APO_LAUNCH_CHECK();
+  m_Ctx->resetNeighborList(s);
+  for (int k = 0; k < nsteps; ++k) {
+    forcesForStep(s);
+    stepKernels(s);
+  }
+}
+
+void CudaIntegrator::subscribe(std::shared_ptr<Subscriber> sub) {
+  if (!sub) throw std::invalid_argument("null subscriber");
+  m_Subscribers.push_back(std::move(sub));
+}
+
+void CudaIntegrator::propagate(int numSteps) {
+  if (!m_Ctx)
+    throw std::invalid_argument("CudaIntegrator::propagate: no CharmmContext was set for this CudaIntegrator.");
+  if (numSteps <= 0) return;
+  cudaStream_t s = m_Ctx->stream();
+  int left = numSteps;
+  long long done = 0;
+  while (left > 0) {
+    int len = std::min(left, m_ListFreq);
+    // stop a segment at the next report of any subscriber
+    for (auto &sub : m_Subscribers) {
+      const long long f = sub->getReportFrequency();
+      const long long next = (done / f + 1) * f;
+      len = (int)std::min<long long>(len, next - done);
+    }
+    if (m_UseGraphs) {
+      auto it = m_Graphs.find(len);
+      if (it == m_Graphs.end()) {
+        cudaGraph_t graph;
+        APO_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        try {
+          segment(len, s);
+        } catch (...) {
+          cudaStreamEndCapture(s, &graph);
+          throw;
+        }
+        APO_CUDA(cudaStreamEndCapture(s, &graph));
+        cudaGraphExec_t exec;
+        APO_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+        APO_CUDA(cudaGraphDestroy(graph));
+        it = m_Graphs.emplace(len, exec).first;
+      }
+      APO_CUDA(cudaGraphLaunch(it->second, s));
+    } else {
+      segment(len, s);
+    }
+    left -= len;
+    m_Step += len;
+    done += len;
+    for (auto &sub : m_Subscribers)
+      if (done % sub->getReportFrequency() == 0) {
+        APO_CUDA(cudaStreamSynchronize(s));
+        sub->update(*m_Ctx, m_Step, getTimeStep());
+      }
+  }
+  APO_CUDA(cudaStreamSynchronize(s));
+  unsigned e = m_Ctx->getForceManager()->readDeviceError(s);
+  if (e & kErrNaN) throw std::runtime_error("non-finite coordinates during propagation");
+  if (e & (kErrTileOverflow | kErrWorkOverflow | kErrColumnOverflow))
+    throw std::runtime_error("neighbour list capacity exceeded during propagation (device error " +
+                             std::to_string(e) + ")");
+}
+
+double CudaIntegrator::getInstantaneousTemperature() {
+  Scalars h;
+  APO_CUDA(cudaStreamSynchronize(stream()));
+  APO_CUDA(cudaMemcpy(&h, m_S->sc.p, sizeof(h), cudaMemcpyDeviceToHost));
+  return h.ke[0] / (0.5 * m_Ctx->getDegreesOfFreedom() * kBoltz);
+}
+
+double CudaIntegrator::getAverageTemperature() {
+  Scalars h;
+  APO_CUDA(cudaStreamSynchronize(stream()));
+  APO_CUDA(cudaMemcpy(&h, m_S->sc.p, sizeof(h), cudaMemcpyDeviceToHost));
+  return h.avgT[0];
+}
+
+void CudaIntegrator::resetAverageTemperature() {
+  Scalars h;
+  APO_CUDA(cudaStreamSynchronize(stream()));
+  APO_CUDA(cudaMemcpy(&h, m_S->sc.p, sizeof(h), cudaMemcpyDeviceToHost));
+  h.avgT[0] = h.avgT[1] = 0.0;
+  h.window = 0;
+  APO_CUDA(cudaMemcpy(m_S->sc.p, &h, sizeof(h), cudaMemcpyHostToDevice));
+}
+
+// ---------------------------------------------------------------- Langevin
+
+CudaLangevinThermostatIntegrator::CudaLangevinThermostatIntegrator(double ps)
+    : CudaIntegrator(ps) {
+  std::random_device rd;
+  m_Seed = rd();
+  m_KernelsPerStep = 1;
+}
+
+void CudaLangevinThermostatIntegrator::setThermostatFriction(double f) {
+  if (f < 0) throw std::invalid_argument("friction must be >= 0");
+  m_Friction = f;
+  clearGraphs();
+}
+
+unsigned long long CudaLangevinThermostatIntegrator::getRngSequencePos() {
+  Scalars h;
+  APO_CUDA(cudaStreamSynchronize(stream()));
+  APO_CUDA(cudaMemcpy(&h, m_S->sc.p, sizeof(h), cudaMemcpyDeviceToHost));
+  return h.rngpos;
+}
+
+void CudaLangevinThermostatIntegrator::initialize() {
+  IntegratorState &S = *m_S;
+  cudaStream_t s = m_Ctx->stream();
+  const double gamma = m_Dt * kTimfac * m_Friction;
+  if (m_Ctx->isUsingHolonomicConstraints())
+    init_constrain_kernel<<<S.blocks_groups, kThreads, 0, s>>>(S.c, 0);
+  m_Ctx->getForceManager()->calcForce(m_Ctx->xyzq(), false, false, s, true);
+  init_delta_kernel<<<S.blocks_atoms, kThreads, 0, s>>>(S.c, S.natom, gamma);
+  if (m_Ctx->isUsingHolonomicConstraints())
+    init_constrain_kernel<<<S.blocks_groups, kThreads, 0, s>>>(S.c, 1);
+  APO_LAUNCH_CHECK();
+  APO_CUDA(cudaStreamSynchronize(s));
+}
+
+void CudaLangevinThermostatIntegrator::stepKernels(cudaStream_t s) {
+  IntegratorState &S = *m_S;
+  const double gamma = m_Dt * kTimfac * m_Friction;
+  const double kbt = kBoltz * m_RefT;
+  langevin_kernel<<<S.blocks_groups, kThreads, 0, s>>>(S.c, gamma, kbt, m_Seed);
+  APO_LAUNCH_CHECK();
+}
+
+// ------------------------------------------------------------- Nose-Hoover
+
+CudaNoseHooverIntegrator::CudaNoseHooverIntegrator(double ps) : CudaIntegrator(ps) {
+  m_KernelsPerStep = 5;
+}
+
+void CudaNoseHooverIntegrator::initialize() {
+  IntegratorState &S = *m_S;
+  cudaStream_t s = m_Ctx->stream();
+  if (m_PistonMass == -9999.9999) {
+    // 0.2 x total mass (src/CudaNoseHooverIntegrator.cu:1009-1021)
+    double tm = 0;
+    for (double mm : m_Ctx->getForceManager()->topology().mass) tm += mm;
+    m_PistonMass = 0.2 * tm;
+  }
+  Scalars h{};
+  h.piston_mass = m_PistonMass;
+  APO_CUDA(cudaMemcpy(S.sc.p, &h, sizeof(h), cudaMemcpyHostToDevice));
+  if (m_Ctx->isUsingHolonomicConstraints())
+    init_constrain_kernel<<<S.blocks_groups, kThreads, 0, s>>>(S.c, 0);
+  m_Ctx->getForceManager()->calcForce(m_Ctx->xyzq(), false, false, s, true);
+  init_delta_kernel<<<S.blocks_atoms, kThreads, 0, s>>>(S.c, S.natom, 0.0);
+  if (m_Ctx->isUsingHolonomicConstraints())
+    init_constrain_kernel<<<S.blocks_groups, kThreads, 0, s>>>(S.c, 1);
+  APO_LAUNCH_CHECK();
+  APO_CUDA(cudaStreamSynchronize(s));
+}
+
+void CudaNoseHooverIntegrator::stepKernels(cudaStream_t s) {
+  IntegratorState &S = *m_S;
+  const double ke_ref = 0.5 * m_Ctx->getDegreesOfFreedom() * kBoltz * m_RefT;
+  const int old = m_OldT ? 1 : 0;
+  nh_half_kernel<<<S.blocks_groups, kThreads, 0, s>>>(S.c, ke_ref, old);
+  nh_pc_kernel<true><<<S.blocks_atoms, kThreads, 0, s>>>(S.c, S.natom, ke_ref, old);
+  nh_pc_kernel<true><<<S.blocks_atoms, kThreads, 0, s>>>(S.c, S.natom, ke_ref, old);
+  nh_pc_kernel<false><<<S.blocks_atoms, kThreads, 0, s>>>(S.c, S.natom, ke_ref, old);
+  nh_final_kernel<<<S.blocks_groups, kThreads, 0, s>>>(S.c, ke_ref, old);
+  APO_LAUNCH_CHECK();
+}
+
+// ---------------------------------------------------------------- leapfrog
+
+CudaLeapFrogIntegrator::CudaLeapFrogIntegrator(double ps) : CudaIntegrator(ps) {
+  m_KernelsPerStep = 1;
+}
+
+void CudaLeapFrogIntegrator::initialize() {}
+
+void CudaLeapFrogIntegrator::stepKernels(cudaStream_t s) {
+  IntegratorState &S = *m_S;
+  leapfrog_kernel<<<S.blocks_atoms, kThreads, 0, s>>>(S.c, S.natom);
+  APO_LAUNCH_CHECK();
+}
+
+}  // namespace apo

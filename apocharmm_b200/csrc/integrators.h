@@ -1,0 +1,120 @@
+// Integrators: Langevin thermostat, Nose-Hoover and leapfrog, with SETTLE
+// (TIP3 water) and SHAKE (X-H clusters) in FP64.
+//
+// Mirror the reference's CudaIntegrator hierarchy (src/CudaIntegrator.cu,
+// src/CudaLangevinThermostatIntegrator.cu, src/CudaNoseHooverIntegrator.cu,
+// src/CudaLeapFrogIntegrator.cu, constraints src/CudaHolonomicConstraint.cu):
+// same position-Verlet "delta" formulation, same thermostat algebra, same
+// Philox stream per atom (curand_init(seed, atom, 0) + skipahead(4*step) +
+// curand_normal4), same 20-step list cadence and 1000-step centre-of-mass
+// removal.  Differences by design:
+//   * one thread owns a whole constraint group (a water, an X-H cluster or a
+//     run of free atoms), so the position update, the constraint, the
+//     velocity update, the kinetic-energy partial sums and the refresh of the
+//     sorted single-precision coordinates are one kernel;
+//   * reductions finish in the last block of the grid (fixed summation order,
+//     no host round trip), and the step counter and RNG position live on the
+//     device;
+//   * `propagate` runs whole list-update segments (rebuild + 20 steps) as
+//     captured CUDA graphs.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+#include "subscribers.h"
+
+namespace apo {
+
+struct IntegratorState;  // device buffers, defined in integrators.cu
+
+class CudaIntegrator : public std::enable_shared_from_this<CudaIntegrator> {
+ public:
+  explicit CudaIntegrator(double timeStepPs);
+  virtual ~CudaIntegrator();
+
+  double getTimeStep() const { return m_Dt * kTimfac; }
+  void setTimeStep(double ps);
+  void setCharmmContext(std::shared_ptr<CharmmContext> ctx);
+  std::shared_ptr<CharmmContext> getCharmmContext() const { return m_Ctx; }
+  void setNonbondedListUpdateFrequency(int f);
+  void setRemoveCenterOfMassFrequency(int f) { m_ComFreq = f; }
+  void setUseGraphs(bool g) { m_UseGraphs = g; }
+  void subscribe(std::shared_ptr<Subscriber> sub);
+  void propagate(int numSteps);
+  long long getCurrentPropagatedStep() const { return m_Step; }
+  double getInstantaneousTemperature();  // "Jung" estimate of the last step
+  double getAverageTemperature();
+  void resetAverageTemperature();
+  cudaStream_t stream() const;
+  // number of kernels one step and one list update launch (for accounting)
+  int kernelsPerStep() const { return m_KernelsPerStep; }
+  int kernelsPerRebuild() const;
+
+ protected:
+  virtual void initialize() = 0;
+  virtual void stepKernels(cudaStream_t s) = 0;  // the integration after forces
+  void segment(int nsteps, cudaStream_t s);      // rebuild + nsteps steps
+  void forcesForStep(cudaStream_t s);
+  double m_Dt;  // AKMA
+  int m_ListFreq = 20, m_ComFreq = 1000;
+  bool m_UseGraphs = true;
+  bool m_Initialized = false;
+  long long m_Step = 0;
+  int m_KernelsPerStep = 0;
+  std::shared_ptr<CharmmContext> m_Ctx;
+  std::unique_ptr<IntegratorState> m_S;
+  std::map<int, cudaGraphExec_t> m_Graphs;
+  std::vector<std::shared_ptr<Subscriber>> m_Subscribers;
+  void buildGroups();
+  void clearGraphs();
+};
+
+class CudaLangevinThermostatIntegrator : public CudaIntegrator {
+ public:
+  explicit CudaLangevinThermostatIntegrator(double timeStepPs);
+  void setThermostatFriction(double frictionPerPs);
+  double getThermostatFriction() const { return m_Friction; }
+  void setReferenceTemperature(double t) { m_RefT = t; }
+  double getReferenceTemperature() const { return m_RefT; }
+  void setThermostatRngSeed(uint64_t seed) { m_Seed = seed; }
+  uint64_t getThermostatRngSeed() const { return m_Seed; }
+  unsigned long long getRngSequencePos();
+
+ protected:
+  void initialize() override;
+  void stepKernels(cudaStream_t s) override;
+  double m_Friction = 0.0, m_RefT = 300.0;
+  uint64_t m_Seed;
+};
+
+class CudaNoseHooverIntegrator : public CudaIntegrator {
+ public:
+  explicit CudaNoseHooverIntegrator(double timeStepPs);
+  void setReferenceTemperature(double t) { m_RefT = t; }
+  double getReferenceTemperature() const { return m_RefT; }
+  void setNoseHooverPistonMass(double m) { m_PistonMass = m; }
+  void useOldTemperature(bool f) { m_OldT = f; }
+
+ protected:
+  void initialize() override;
+  void stepKernels(cudaStream_t s) override;
+  double m_RefT = 300.0, m_PistonMass = -9999.9999;
+  bool m_OldT = false;
+};
+
+class CudaLeapFrogIntegrator : public CudaIntegrator {
+ public:
+  explicit CudaLeapFrogIntegrator(double timeStepPs);
+
+ protected:
+  void initialize() override;
+  void stepKernels(cudaStream_t s) override;
+};
+
+}  // namespace apo

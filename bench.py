@@ -1,0 +1,333 @@
+"""Benchmark: MD throughput (ns/day) of the force/step path on one B200.
+
+Workload (N=1 line): the 23,558-atom solvated bead chain (62.23 A box, PME
+64^3 order 6, cutoff 12 A, force switch 10-12 A, list 14 A, Langevin 300 K,
+gamma 1/ps, dt 2 fs, SETTLE), synthetic and seeded.  One timed iteration is
+one neighbour-list segment: a list rebuild plus 20 MD steps, replayed from a
+captured CUDA graph.  L2 is flushed (a 256 MB device write) before every
+timed iteration, outside the timed interval.
+
+  value  ns/day from the sum of per-iteration CUDA-event times on the
+         integrator's stream, max over ranks
+  e2e    ns/day through the C ABI with host buffers: every iteration uploads
+         coordinates and velocities from pinned host memory, propagates the
+         segment and reads the coordinates back
+  roofline  direct-space kernel (FP32 pipe): 65 FLOP per in-cutoff pair over
+         its CUDA-event time, against the FP32 FMA peak measured on the same
+         GPU in the same run
+  cpu_baseline  the FP64 CPU oracle (all host threads) on a bounded sample
+
+--impl reference times the FP64 CPU restatement of the reference algorithm
+(the reference engine has no CPU implementation of this path) on the host
+cores and prints the same metric.  With torchrun (N>1) every rank runs its
+own replica of the system (replicas only: the path has no collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DT_PS = 0.002
+SEG = 20                       # MD steps per timed iteration (list cadence)
+FLOP_PER_PAIR = 65
+
+
+def ns_per_day(steps: float, seconds: float) -> float:
+    return 86400.0 * steps / seconds * DT_PS * 1e-3
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 8:
+                continue
+            try:
+                sm.append(float(p[0]))
+                mx = max(mx, float(p[1]))
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if p[4 + k].lower().startswith("active"):
+                    reasons.add(name)
+        busy = [v for v in sm if v > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(busy) if busy else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), \
+        int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def cpu_baseline(sys_obj, evals: int = 2):
+    """FP64 oracle: full force evaluations + position update on all threads."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle
+    st = sys_obj.settings
+    o = oracle.Oracle(sys_obj, st["kappa"], st["ctofnb"], st["ctonnb"], st["nfft"], st["order"])
+    threads = oracle.lib().or_max_threads()
+    pos = np.array(sys_obj.pos)
+    vel = np.zeros_like(pos)
+    inv_m = 1.0 / np.asarray(sys_obj.mass)[:, None]
+    o.evaluate(pos=pos, nthreads=threads)  # warm-up
+    t0 = time.perf_counter()
+    for _ in range(evals):
+        E, grad = o.evaluate(pos=pos, nthreads=threads)
+        vel -= (DT_PS / 0.0488882129) * grad * inv_m
+        pos = pos + (DT_PS / 0.0488882129) * vel
+    dt = time.perf_counter() - t0
+    return {"value": ns_per_day(evals, dt), "unit": "ns/day", "cores": threads, "kind": "port",
+            "sample": f"{evals} FP64 force evaluations (direct, 1-4, PME, bonded) + position "
+                      f"updates of the {sys_obj.n_atoms}-atom workload, {dt:.1f} s"}
+
+
+def run_reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from apocharmm_b200.systems import config_solvated_chain
+    s = config_solvated_chain()
+    cb = cpu_baseline(s, evals=max(1, min(args.steps, 3)))
+    line = {"impl": "reference", "metric": "ns/day", "value": cb["value"], "unit": "ns/day",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator)",
+            "config": {"workload": "chain23k", "atoms": s.n_atoms},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": "ns/day", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "note": "the reference engine is GPU-only; this arm times the FP64 CPU "
+                    "restatement of its force/step algorithm"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30, help="timed iterations (20 MD steps each)")
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precise", action="store_true", help="precision form")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import numpy as np
+    import torch
+    rank, world, local = dist_env()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+
+    from apocharmm_b200 import api
+    from apocharmm_b200.systems import config_solvated_chain
+    s = config_solvated_chain()
+    work = tempfile.mkdtemp(prefix=f"apo_bench_{rank}_")
+    psf, prm, fm, ctx = api.system_context(s, work, precise=args.precise)
+    ctx.setRandomSeedForVelocities(2024 + rank)
+    ctx.assignVelocitiesAtTemperature(300.0)
+
+    # force error of this configuration against the FP64 oracle (rank 0)
+    force_err = None
+    if rank == 0 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        ctx.calculateForces(False, True, False)
+        F = ctx.getForces()
+        st = s.settings
+        Eo, Go = oracle.Oracle(s, st["kappa"], st["ctofnb"], st["ctonnb"], st["nfft"],
+                               st["order"]).evaluate()
+        force_err = float(np.sqrt(((F - Go) ** 2).sum() / (Go ** 2).sum()))
+
+    n_pairs_cut = _count_pairs(ctx, s.settings["ctofnb"])
+
+    ctx.resetNeighborList()
+    api.call("apo_charmm_context_set_kernel_timing", ctx.handle, api._i(1))
+    integ = api.CudaLangevinThermostatIntegrator(DT_PS)
+    integ.setThermostatFriction(1.0)
+    integ.setReferenceTemperature(300.0)
+    integ.setThermostatRngSeed(777 + rank)
+    integ.setCharmmContext(ctx)
+
+    stream = torch.cuda.ExternalStream(ctx.getStream())
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+
+    for _ in range(args.warmup):
+        integ.propagate(SEG)
+
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    seg_ms, nb_ms, nb_launch = [], 0.0, 0
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            integ.propagate(SEG)
+            e1.record(stream)
+            e1.synchronize()
+            seg_ms.append(e0.elapsed_time(e1))
+            t = api.ctypes.c_double()
+            n = api.ctypes.c_int()
+            api.call("apo_charmm_context_get_kernel_time", api.ctypes.byref(t), api.ctypes.byref(n),
+                     ctx.handle)
+            nb_ms += t.value
+            nb_launch += n.value
+    torch.cuda.synchronize()
+    total_ms = sum(seg_ms)
+    if world > 1:
+        tt = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(tt.item())
+        torch.distributed.barrier()
+    md_steps = args.steps * SEG
+    value = ns_per_day(md_steps * world, total_ms * 1e-3)
+    n_pairs_end = _count_pairs(ctx, s.settings["ctofnb"])
+
+    # end-to-end through the C ABI with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        n = s.n_atoms
+        hx = torch.empty(3 * n, dtype=torch.float64, pin_memory=True)
+        hv = torch.empty(3 * n, dtype=torch.float64, pin_memory=True)
+        hx.numpy()[:] = ctx.getCoordinates().reshape(-1)
+        hv.numpy()[:] = ctx.getVelocities().reshape(-1)
+        lib = api.lib()
+        iters = max(3, args.steps // 2)
+        if world > 1:
+            torch.distributed.barrier()
+        t0 = time.perf_counter()
+        for _ in range(iters):
+            api.call("apo_charmm_context_set_coordinates_xyz", ctx.handle,
+                     api._vp(hx.data_ptr()), api._sz(3 * n))
+            api.call("apo_charmm_context_set_velocities", ctx.handle,
+                     api._vp(hv.data_ptr()), api._sz(3 * n))
+            integ.propagate(SEG)
+            api.call("apo_charmm_context_get_coordinates", api._vp(hx.data_ptr()), api._sz(3 * n),
+                     ctx.handle)
+            api.call("apo_charmm_context_get_velocities", api._vp(hv.data_ptr()), api._sz(3 * n),
+                     ctx.handle)
+        el = time.perf_counter() - t0
+        if world > 1:
+            tt = torch.tensor([el], device="cuda", dtype=torch.float64)
+            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+            el = float(tt.item())
+        e2e = {"value": ns_per_day(iters * SEG * world, el), "unit": "ns/day",
+               "h2d_bytes_per_step": 2 * 3 * n * 8 / SEG, "d2h_bytes_per_step": 2 * 3 * n * 8 / SEG,
+               "note": "per 20-step segment: coordinates+velocities up (pinned), propagate, "
+                       "coordinates+velocities down; bytes given per MD step"}
+
+    if rank == 0:
+        peak = api.ctypes.c_double()
+        api.call("apo_diag_fp32_peak_tflops", api.ctypes.byref(peak))
+        avg_nb_s = (nb_ms / max(1, nb_launch)) * 1e-3
+        pairs_avg = 0.5 * (n_pairs_cut + n_pairs_end)
+        achieved = pairs_avg * FLOP_PER_PAIR / avg_nb_s / 1e12 if avg_nb_s > 0 else None
+        cb = None
+        if not args.no_cpu_baseline:
+            cb = cpu_baseline(s, evals=2)
+        kps = integ.getKernelsPerStep()
+        launches = args.steps * (12 + SEG * (7 + kps))
+        line = {
+            "metric": "ns/day", "value": value, "unit": "ns/day", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 (forces), f64 (integration)", "data": "synthetic (seeded generator)",
+            "config": {"workload": "chain23k: 23,558-atom bead chain in TIP3P, 62.23 A box, "
+                                   "PME 64^3 order 6, cutoff 12 / switch 10-12 / list 14, "
+                                   "Langevin 300 K gamma 1/ps, dt 2 fs, SETTLE",
+                       "atoms": s.n_atoms, "md_steps_per_iteration": SEG,
+                       "form": "precision" if args.precise else "plain",
+                       "l2": "flushed (256 MB device write) before every timed iteration, "
+                             "outside the timed interval",
+                       "parallelism": f"replicas x{world}"},
+            "md_steps_timed": md_steps,
+            "force_rel_rms_vs_fp64": force_err,
+            "roofline": {"kernel": "direct-space tile kernel", "bound": "fp32",
+                         "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+                         "frac": (achieved / peak.value) if achieved else None,
+                         "traffic": None,
+                         "work": f"{FLOP_PER_PAIR} FLOP x {pairs_avg:.0f} in-cutoff pairs per launch",
+                         "launch_ms": avg_nb_s * 1e3, "launches_timed": nb_launch,
+                         "peak_source": "FP32 FMA probe measured on this GPU in this run"},
+            "clocks": clocks.summary(),
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "cpu_baseline": cb,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def _count_pairs(ctx, radius: float) -> int:
+    from apocharmm_b200 import api
+    n = api._sz()
+    api.call("apo_charmm_context_get_neighbor_pairs", None, api._sz(0), api.ctypes.byref(n),
+             api._d(radius), ctx.handle)
+    return int(n.value)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

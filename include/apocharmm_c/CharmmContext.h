@@ -47,6 +47,15 @@ APOCHARMM_C_API apo_status apo_charmm_context_get_num_atoms(size_t *num_atoms, c
 APOCHARMM_C_API apo_status apo_charmm_context_get_degrees_of_freedom(int *ndegf, const apo_charmm_context *context);
 APOCHARMM_C_API apo_status apo_charmm_context_reset_neighbor_list(apo_charmm_context *context);
 APOCHARMM_C_API apo_status apo_charmm_context_get_neighbor_pairs(int *pairs, const size_t len, size_t *num_pairs, const double radius, apo_charmm_context *context);
+/* CUDA-event timing of the direct-space kernel: enable (clears the
+ * integrators' captured graphs on their next propagate is NOT done; enable it
+ * before creating the integrator), then read the summed milliseconds and the
+ * number of launches recorded since the last integration segment began */
+APOCHARMM_C_API apo_status apo_charmm_context_set_kernel_timing(apo_charmm_context *context, const int on);
+APOCHARMM_C_API apo_status apo_charmm_context_get_kernel_time(double *ms, int *launches, apo_charmm_context *context);
+/* measured FP32 FMA throughput of the current device in TFLOP/s (a short
+ * probe kernel), the denominator of the direct-space roofline */
+APOCHARMM_C_API apo_status apo_diag_fp32_peak_tflops(double *tflops);
 /* CUDA stream the context's work is issued on (a cudaStream_t), for timing */
 APOCHARMM_C_API apo_status apo_charmm_context_get_stream(void **stream, const apo_charmm_context *context);
 #ifdef __cplusplus

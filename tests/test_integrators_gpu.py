@@ -1,0 +1,136 @@
+"""GPU tests of the integrators through the C ABI."""
+import os
+
+import numpy as np
+import pytest
+
+from apocharmm_b200 import api
+from apocharmm_b200.systems import config_small_water, solvated_chain, water_box
+
+pytestmark = pytest.mark.gpu
+
+SMALL = dict(kappa=0.34, nfft=(24, 24, 24), order=4, ctofnb=9.0, ctonnb=7.5, cutnb=11.0)
+
+
+def _setup(tmp_path, n=1000, L=31.0, seed=3):
+    s = water_box(n, L, seed=seed)
+    keep = api.system_context(s, str(tmp_path), settings=SMALL)
+    ctx = keep[3]
+    ctx.setRandomSeedForVelocities(314159)
+    ctx.assignVelocitiesAtTemperature(300.0)
+    return s, keep
+
+
+def _water_geometry(xyz):
+    o, h1, h2 = xyz[0::3], xyz[1::3], xyz[2::3]
+    return (np.linalg.norm(h1 - o, axis=1), np.linalg.norm(h2 - o, axis=1),
+            np.linalg.norm(h2 - h1, axis=1))
+
+
+def test_settle_keeps_tip3_geometry(tmp_path):
+    s, keep = _setup(tmp_path)
+    integ = api.CudaLangevinThermostatIntegrator(0.002)
+    integ.setThermostatFriction(5.0)
+    integ.setReferenceTemperature(300.0)
+    integ.setThermostatRngSeed(42)
+    integ.setCharmmContext(keep[3])
+    integ.propagate(100)
+    d1, d2, d3 = _water_geometry(keep[3].getCoordinates())
+    assert np.abs(d1 - 0.9572).max() < 1e-6
+    assert np.abs(d2 - 0.9572).max() < 1e-6
+    assert np.abs(d3 - np.sqrt(2.29189321)).max() < 1e-6
+    assert integ.getCurrentPropagatedStep() == 100
+
+
+def test_langevin_runs_are_bit_identical(tmp_path):
+    out = []
+    for rep in range(2):
+        s, keep = _setup(tmp_path / f"r{rep}")
+        integ = api.CudaLangevinThermostatIntegrator(0.002)
+        integ.setThermostatFriction(1.0)
+        integ.setThermostatRngSeed(7)
+        integ.setCharmmContext(keep[3])
+        integ.propagate(60)
+        out.append((keep[3].getCoordinates(), keep[3].getVelocities()))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+
+
+def test_graph_and_eager_paths_agree(tmp_path):
+    res = []
+    for graphs in (True, False):
+        s, keep = _setup(tmp_path / f"g{int(graphs)}")
+        integ = api.CudaLangevinThermostatIntegrator(0.002)
+        integ.setThermostatFriction(1.0)
+        integ.setThermostatRngSeed(11)
+        integ.setUseGraphs(graphs)
+        integ.setCharmmContext(keep[3])
+        integ.propagate(45)
+        res.append(keep[3].getCoordinates())
+    assert np.array_equal(res[0], res[1])
+
+
+def test_nve_energy_is_conserved(tmp_path):
+    s, keep = _setup(tmp_path)
+    ctx = keep[3]
+    integ = api.CudaLangevinThermostatIntegrator(0.001)
+    integ.setThermostatFriction(0.0)
+    integ.setCharmmContext(ctx)
+    def total():
+        pe = ctx.calculatePotentialEnergy(False)
+        return pe + 0.5 * ctx.getDegreesOfFreedom() * 1.987191e-3 * integ.getInstantaneousTemperature()
+    integ.propagate(20)
+    e0 = total()
+    integ.propagate(400)
+    e1 = total()
+    ke = 0.5 * ctx.getDegreesOfFreedom() * 1.987191e-3 * 300.0
+    assert abs(e1 - e0) < 0.02 * ke
+
+
+def test_langevin_thermostat_reaches_target(tmp_path):
+    s, keep = _setup(tmp_path)
+    integ = api.CudaLangevinThermostatIntegrator(0.002)
+    integ.setThermostatFriction(10.0)
+    integ.setReferenceTemperature(300.0)
+    integ.setThermostatRngSeed(3)
+    integ.setCharmmContext(keep[3])
+    integ.propagate(300)
+    t = integ.getAverageTemperature()
+    assert 240.0 < t < 360.0
+
+
+def test_nose_hoover_and_leapfrog_run(tmp_path):
+    s, keep = _setup(tmp_path)
+    nh = api.CudaNoseHooverIntegrator(0.002)
+    nh.setReferenceTemperature(300.0)
+    nh.setCharmmContext(keep[3])
+    nh.propagate(100)
+    t = nh.getInstantaneousTemperature()
+    assert 150.0 < t < 600.0
+    d1, _, _ = _water_geometry(keep[3].getCoordinates())
+    assert np.abs(d1 - 0.9572).max() < 1e-6
+    s2, keep2 = _setup(tmp_path / "lf")
+    keep2[3].useHolonomicConstraints(False)
+    lf = api.CudaLeapFrogIntegrator(0.0005)
+    lf.setCharmmContext(keep2[3])
+    lf.propagate(40)
+    assert np.isfinite(keep2[3].getCoordinates()).all()
+
+
+def test_dcd_subscriber_writes_frames(tmp_path):
+    s, keep = _setup(tmp_path)
+    integ = api.CudaLangevinThermostatIntegrator(0.002)
+    integ.setThermostatFriction(1.0)
+    integ.setCharmmContext(keep[3])
+    path = tmp_path / "traj.dcd"
+    dcd = api.DcdSubscriber(str(path), 25)
+    integ.subscribe(dcd)
+    integ.propagate(100)
+    dcd.close()
+    raw = path.read_bytes()
+    n = s.n_atoms
+    frame = 4 + 48 + 4 + 3 * (4 + 4 * n + 4)
+    header = (4 + 84 + 4) + (4 + 84 + 4) + (4 + 4 + 4)
+    assert len(raw) == header + 4 * frame
+    assert raw[4:8] == b"CORD"
+    assert int.from_bytes(raw[8:12], "little") == 4
