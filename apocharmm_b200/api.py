@@ -450,3 +450,51 @@ class CudaLeapFrogIntegrator(CudaIntegrator):
         super().__init__()
         call("apo_cuda_leap_frog_integrator_create", ctypes.byref(self._h), _d(time_step))
         self._bind_view()
+
+
+def rigid_water_fit(xyz: np.ndarray, waters: np.ndarray) -> np.ndarray:
+    """Replaces every TIP3 water (O, H1, H2 index triples) by the rigid TIP3P
+    template superposed on it (mass-weighted Kabsch fit)."""
+    from .systems import _water_template, M_H, M_O
+    t = _water_template()
+    w = np.array([M_O, M_H, M_H])
+    out = np.array(xyz, np.float64, copy=True)
+    P = out[waters]                                   # (n,3,3)
+    com = (w[None, :, None] * P).sum(1) / w.sum()
+    Q = P - com[:, None, :]
+    H = np.einsum("a,ai,naj->nij", w, t, Q)           # template^T W Q
+    U, _, Vt = np.linalg.svd(H)
+    d = np.sign(np.linalg.det(np.einsum("nij,njk->nik", U, Vt)))
+    D = np.ones((len(d), 3))
+    D[:, 2] = d
+    Rm = np.einsum("nij,nj,njk->nik", U, D, Vt)
+    out[waters] = com[:, None, :] + np.einsum("ai,nij->naj", t, Rm)
+    return out
+
+
+def relax(ctx: CharmmContext, waters=None, iterations: int = 150, max_step: float = 0.03):
+    """Deterministic steepest-descent relaxation on the GPU force path: every
+    iteration moves the atoms along -gradient, the largest move `max_step`
+    Angstrom; TIP3 waters are refitted to the rigid geometry at the end.
+    Used to remove the close contacts of freshly generated synthetic systems
+    before dynamics."""
+    x = ctx.getCoordinates()
+    for _ in range(iterations):
+        ctx.calculateForces(False, False, False)
+        g = ctx.getForces()
+        gmax = float(np.abs(g).max())
+        if not np.isfinite(gmax) or gmax == 0.0:
+            break
+        x = x - (max_step / gmax) * g
+        ctx.setCoordinates(x)
+    if waters is not None and len(waters):
+        x = rigid_water_fit(x, np.asarray(waters))
+        ctx.setCoordinates(x)
+    return x
+
+
+def water_indices(sys) -> np.ndarray:
+    """(n,3) atom indices of the OT-HT-HT waters of a System."""
+    t = sys.atom_type
+    return np.array([[i, i + 1, i + 2] for i in range(0, len(t) - 2)
+                     if t[i] == "OT" and t[i + 1] == "HT" and t[i + 2] == "HT"], np.int64).reshape(-1, 3)

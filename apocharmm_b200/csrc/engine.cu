@@ -228,6 +228,7 @@ void ForceManager::calcForce(const float4 *d_xyzq, bool calcEnergy, bool /*calcV
     a.energy = m_Energy.p;
     a.setups = m_Setup.p;
     cudaEvent_t t1 = nullptr;
+    bool timer_capture = false;
     if (m_Timing) {
       if (m_TimerCursor >= (int)m_Timers.size()) {
         cudaEvent_t e0, e1;
@@ -235,12 +236,23 @@ void ForceManager::calcForce(const float4 *d_xyzq, bool calcEnergy, bool /*calcV
         APO_CUDA(cudaEventCreate(&e1));
         m_Timers.emplace_back(e0, e1);
       }
-      APO_CUDA(cudaEventRecord(m_Timers[m_TimerCursor].first, m_SNb));
+      // while the stream is captured, external records stay real event nodes
+      cudaStreamCaptureStatus cs;
+      APO_CUDA(cudaStreamIsCapturing(m_SNb, &cs));
+      timer_capture = cs == cudaStreamCaptureStatusActive;
+      if (timer_capture)
+        APO_CUDA(cudaEventRecordWithFlags(m_Timers[m_TimerCursor].first, m_SNb,
+                                          cudaEventRecordExternal));
+      else
+        APO_CUDA(cudaEventRecord(m_Timers[m_TimerCursor].first, m_SNb));
       t1 = m_Timers[m_TimerCursor].second;
       ++m_TimerCursor;
     }
     launch_nonbonded(a, calcEnergy, m_Precise, m_SNb);
-    if (t1) APO_CUDA(cudaEventRecord(t1, m_SNb));
+    if (t1) {
+      if (timer_capture) APO_CUDA(cudaEventRecordWithFlags(t1, m_SNb, cudaEventRecordExternal));
+      else APO_CUDA(cudaEventRecord(t1, m_SNb));
+    }
     APO_CUDA(cudaEventRecord(m_EvNb, m_SNb));
     APO_CUDA(cudaStreamWaitEvent(s, m_EvNb, 0));
   }

@@ -720,7 +720,12 @@ void CudaIntegrator::forcesForStep(cudaStream_t s) {
 
 void CudaIntegrator::segment(int nsteps, cudaStream_t s) {
   IntegratorState &S = *m_S;
-  m_Ctx->getForceManager()->rewindKernelTimers();
+  auto fm = m_Ctx->getForceManager();
+  fm->rewindKernelTimers();
+  // a force evaluation requested between propagate() calls leaves gradients
+  // in the shared buffer; every segment starts from a cleared one (the step
+  // kernels clear each slot they consume afterwards)
+  APO_CUDA(cudaMemsetAsync(fm->forceFixed(), 0, (size_t)3 * fm->forceStride() * sizeof(long long), s));
   com_sum_kernel<<<S.blocks_atoms, kThreads, 0, s>>>(S.c, S.natom, m_ComFreq);
   com_apply_kernel<<<S.blocks_atoms, kThreads, 0, s>>>(S.c, S.natom, m_ComFreq);
   APO_LAUNCH_CHECK();

@@ -113,13 +113,37 @@ def _lattice_sites(L: float, n_per_edge: int) -> np.ndarray:
     return np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1)
 
 
-def _place_waters(rng, centres: np.ndarray, jitter: float, L: float) -> np.ndarray:
+def _place_waters(rng, centres: np.ndarray, jitter: float, L: float,
+                  others: np.ndarray | None = None, d_min: float = 1.5,
+                  max_rounds: int = 40) -> np.ndarray:
+    """Waters at jittered lattice centres with random orientations; the
+    orientation (and later the jitter) of any molecule with an atom closer
+    than d_min to an atom of another molecule (or of `others`) is redrawn,
+    for at most max_rounds rounds.  Contacts that remain in very dense
+    systems are removed by `relax` (api.py) before dynamics."""
+    from scipy.spatial import cKDTree
+
     n = centres.shape[0]
-    c = centres + rng.normal(0.0, jitter, size=centres.shape)
+    jit = rng.normal(0.0, jitter, size=centres.shape)
     R = _random_rotations(rng, n)
     t = _water_template()
-    pos = c[:, None, :] + np.einsum("nij,aj->nai", R, t)
-    return pos.reshape(-1, 3)
+    nother = 0 if others is None else others.shape[0]
+    for rnd in range(max_rounds):
+        c = centres + jit
+        pos = (c[:, None, :] + np.einsum("nij,aj->nai", R, t)).reshape(-1, 3)
+        allp = pos if others is None else np.concatenate([pos, others])
+        tree = cKDTree(np.mod(allp + L / 2, L) % L, boxsize=L)
+        pairs = tree.query_pairs(d_min, output_type="ndarray")
+        mol = np.where(np.arange(len(allp)) < 3 * n, np.arange(len(allp)) // 3, -1)
+        a, b = mol[pairs[:, 0]], mol[pairs[:, 1]]
+        bad = a != b
+        hit = np.unique(np.concatenate([a[bad & (a >= 0)], b[bad & (b >= 0)]]))
+        if hit.size == 0 or rnd == max_rounds - 1:
+            return pos
+        R[hit] = _random_rotations(rng, hit.size)
+        if rnd >= 10 and rnd % 2:
+            jit[hit] = rng.normal(0.0, jitter, size=(hit.size, 3))
+    return pos
 
 
 # --------------------------------------------------------------------------
@@ -299,7 +323,7 @@ def solvated_chain(n_atoms: int = 23558, L: float = 62.23, n_beads: int = 2489,
     if sites.shape[0] < n_water:
         raise RuntimeError("not enough free lattice sites for the solvent")
     sites = sites[np.sort(rng.choice(sites.shape[0], n_water, replace=False))]
-    wpos = _place_waters(rng, sites, 0.2, L)
+    wpos = _place_waters(rng, sites, 0.2, L, others=chain, d_min=1.6)
 
     wb, wa, wt, wn, wrn, wri, ws = _water_topology(n_water, first_atom=n_beads)
     cb = np.stack([np.arange(n_beads - 1), np.arange(1, n_beads)], 1)

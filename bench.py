@@ -180,6 +180,8 @@ def main():
     s = config_solvated_chain()
     work = tempfile.mkdtemp(prefix=f"apo_bench_{rank}_")
     psf, prm, fm, ctx = api.system_context(s, work, precise=args.precise)
+    # remove the close contacts of the generated structure (deterministic)
+    s.pos = api.relax(ctx, api.water_indices(s), iterations=150)
     ctx.setRandomSeedForVelocities(2024 + rank)
     ctx.assignVelocitiesAtTemperature(300.0)
 

@@ -80,7 +80,18 @@ def test_neighbor_pairs_match_brute_force(tmp_path):
     canon = {(min(i, j), max(i, j)) for i, j, _ in got.tolist()}
     assert len(canon) == len(got), "a pair appears in more than one tile"
     ref = brute_force_pairs(s.pos, s.box, 11.0, o.eptr, o.eidx)
-    assert canon == ref
+    # pairs within single-precision rounding of the radius may fall on either
+    # side; every other pair must agree exactly
+    box = np.asarray(s.box)
+
+    def dist(p):
+        d = s.pos[p[0]] - s.pos[p[1]]
+        d -= box * np.round(d / box)
+        return float(np.sqrt((d * d).sum()))
+
+    diff = [p for p in canon ^ ref if abs(dist(p) - 11.0) > 1e-4]
+    assert not diff, [(p, dist(p)) for p in diff[:10]]
+    assert len(canon ^ ref) < 10
 
 
 def test_forces_are_deterministic(tmp_path):
