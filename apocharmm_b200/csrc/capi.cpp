@@ -562,3 +562,20 @@ extern "C" apo_status apo_charmm_context_get_kernel_time(double *ms, int *launch
     return APO_STATUS_OK;
   }, fn);
 }
+
+extern "C" apo_status apo_charmm_context_get_list_counts(int *slots, int *tiles, int *work,
+                                                         apo_charmm_context *c) {
+  const char *fn = "apo_charmm_context_get_list_counts";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_ptr(slots, fn, "slots"));
+    APO_RETURN_IF(require_ptr(tiles, fn, "tiles"));
+    APO_RETURN_IF(require_ptr(work, fn, "work_items"));
+    APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
+    auto &nl = c->object->getForceManager()->neighborList();
+    nl.sync_counts(c->object->stream());
+    *slots = nl.h_counts[0];
+    *tiles = nl.h_counts[1];
+    *work = nl.h_counts[2];
+    return APO_STATUS_OK;
+  }, fn);
+}

@@ -1,6 +1,7 @@
 // ForceManager / CharmmContext; see engine.h.
 #include "engine.h"
 
+#include <algorithm>
 #include <cmath>
 #include <random>
 #include <sstream>
@@ -20,28 +21,34 @@ __global__ void fixed_to_global_kernel(int n, const long long *__restrict__ f, i
   out[3 * g + 2] = (double)f[2 * stride + s] * kInvForceScale;
 }
 
+// one warp per bonded component: centroid by a warp reduction, then the
+// whole component is shifted by one box length per axis where the centroid
+// left [-L/2, L/2] (src/CharmmContext.cu:276-372)
 __global__ void image_centering_kernel(double4 *__restrict__ c, float4 *__restrict__ xq,
                                        const int2 *__restrict__ groups, int ng, double Lx,
                                        double Ly, double Lz) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ng; i += gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < ng; i += nwarps) {
     const int2 g = groups[i];
     double gx = 0, gy = 0, gz = 0;
-    for (int j = g.x; j <= g.y; ++j) {
+    for (int j = g.x + lane; j <= g.y; j += 32) {
       gx += c[j].x;
       gy += c[j].y;
       gz += c[j].z;
     }
+    gx = warp_sum(gx);
+    gy = warp_sum(gy);
+    gz = warp_sum(gz);
     const double inv = 1.0 / (double)(g.y - g.x + 1);
     gx *= inv;
     gy *= inv;
     gz *= inv;
-    // shift by one box length when the centroid leaves [-L/2, L/2]
-    // (src/CharmmContext.cu:276-372)
     const double sx = gx < -0.5 * Lx ? Lx : (gx > 0.5 * Lx ? -Lx : 0.0);
     const double sy = gy < -0.5 * Ly ? Ly : (gy > 0.5 * Ly ? -Ly : 0.0);
     const double sz = gz < -0.5 * Lz ? Lz : (gz > 0.5 * Lz ? -Lz : 0.0);
     if (sx != 0.0 || sy != 0.0 || sz != 0.0) {
-      for (int j = g.x; j <= g.y; ++j) {
+      for (int j = g.x + lane; j <= g.y; j += 32) {
         c[j].x += sx;
         c[j].y += sy;
         c[j].z += sz;
@@ -67,8 +74,8 @@ __global__ void coords_to_xyzq_kernel(const double4 *__restrict__ c, float4 *__r
 void launch_image_centering(double4 *coords, float4 *xyzq, const int2 *groups, int ngroups,
                             double Lx, double Ly, double Lz, cudaStream_t s) {
   if (ngroups <= 0) return;
-  image_centering_kernel<<<(ngroups + 127) / 128, 128, 0, s>>>(coords, xyzq, groups, ngroups,
-                                                                Lx, Ly, Lz);
+  const int blocks = std::min((ngroups + 3) / 4, 148 * 16);
+  image_centering_kernel<<<blocks, 128, 0, s>>>(coords, xyzq, groups, ngroups, Lx, Ly, Lz);
   APO_LAUNCH_CHECK();
 }
 
@@ -216,6 +223,7 @@ void ForceManager::calcForce(const float4 *d_xyzq, bool calcEnergy, bool /*calcV
     APO_CUDA(cudaStreamWaitEvent(m_SNb, m_EvFork, 0));
     NbArgs a;
     a.xyzq_s = m_Nbl.xyzq_s;
+    a.perm = m_Nbl.perm;
     a.type_s = m_Nbl.type_s;
     a.tiles = m_Nbl.tiles;
     a.masks = m_Nbl.masks;

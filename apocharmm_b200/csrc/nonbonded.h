@@ -20,6 +20,7 @@ NbSetup make_nb_setup(double Lx, double Ly, double Lz, double kappa, double roff
 
 struct NbArgs {
   const float4 *xyzq_s;
+  const int *perm;        // slot -> atom, -1 for padding
   const int *type_s;
   const int2 *tiles;
   const unsigned *masks;

@@ -244,6 +244,9 @@ def main():
     md_steps = args.steps * SEG
     value = ns_per_day(md_steps * world, total_ms * 1e-3)
     n_pairs_end = _count_pairs(ctx, s.settings["ctofnb"])
+    lc = [api.ctypes.c_int() for _ in range(3)]
+    api.call("apo_charmm_context_get_list_counts", *[api.ctypes.byref(v) for v in lc], ctx.handle)
+    list_counts = {"slots": lc[0].value, "tiles": lc[1].value, "work_items": lc[2].value}
 
     # end-to-end through the C ABI with pinned host buffers
     e2e = None
@@ -303,6 +306,7 @@ def main():
                              "outside the timed interval",
                        "parallelism": f"replicas x{world}"},
             "md_steps_timed": md_steps,
+            "neighbor_list": list_counts,
             "force_rel_rms_vs_fp64": force_err,
             "roofline": {"kernel": "direct-space tile kernel", "bound": "fp32",
                          "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",

@@ -56,6 +56,8 @@ APOCHARMM_C_API apo_status apo_charmm_context_get_kernel_time(double *ms, int *l
 /* measured FP32 FMA throughput of the current device in TFLOP/s (a short
  * probe kernel), the denominator of the direct-space roofline */
 APOCHARMM_C_API apo_status apo_diag_fp32_peak_tflops(double *tflops);
+/* sizes of the current neighbour list: sorted slots, tiles, work items */
+APOCHARMM_C_API apo_status apo_charmm_context_get_list_counts(int *slots, int *tiles, int *work_items, apo_charmm_context *context);
 /* CUDA stream the context's work is issued on (a cudaStream_t), for timing */
 APOCHARMM_C_API apo_status apo_charmm_context_get_stream(void **stream, const apo_charmm_context *context);
 #ifdef __cplusplus
