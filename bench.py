@@ -1,26 +1,38 @@
 """Benchmark: MD throughput (ns/day) of the force/step path on one B200.
 
-Workload (N=1 line): the 23,558-atom solvated bead chain (62.23 A box, PME
-64^3 order 6, cutoff 12 A, force switch 10-12 A, list 14 A, Langevin 300 K,
-gamma 1/ps, dt 2 fs, SETTLE), synthetic and seeded.  One timed iteration is
-one neighbour-list segment: a list rebuild plus 20 MD steps, replayed from a
-captured CUDA graph.  L2 is flushed (a 256 MB device write) before every
-timed iteration, outside the timed interval.
+Workloads (--workload; the N=1 line uses chain23k):
+  chain23k  23,558-atom solvated bead chain (62.23 A box, PME 64^3 order 6,
+            cutoff 12 A, force switch 10-12 A, list 14 A, Langevin 300 K,
+            gamma 1/ps, dt 2 fs, SETTLE)
+  water12k  12,480-atom TIP3P box (50 A, PME 48^3 order 4, cutoff 10 A,
+            switch 8-10 A, list 12 A, leapfrog NVE, dt 2 fs, SETTLE)
+  water1m   999,999-atom TIP3P box (215.4 A, PME 216^3 order 4, cutoff 10 A,
+            switch 8-10 A, list 11.5 A, Nose-Hoover 300 K, dt 2 fs, SETTLE)
+All synthetic and seeded; the generated structure is relaxed by 150
+deterministic steepest-descent iterations before dynamics.  One timed
+iteration is one neighbour-list segment: a list rebuild plus 20 MD steps,
+replayed from a captured CUDA graph.  L2 is flushed (a 256 MB device write)
+before every timed iteration, outside the timed interval.
 
   value  ns/day from the sum of per-iteration CUDA-event times on the
          integrator's stream, max over ranks
   e2e    ns/day through the C ABI with host buffers: every iteration uploads
          coordinates and velocities from pinned host memory, propagates the
-         segment and reads the coordinates back
+         segment and reads coordinates and velocities back
   roofline  direct-space kernel (FP32 pipe): 65 FLOP per in-cutoff pair over
          its CUDA-event time, against the FP32 FMA peak measured on the same
          GPU in the same run
   cpu_baseline  the FP64 CPU oracle (all host threads) on a bounded sample
 
---impl reference times the FP64 CPU restatement of the reference algorithm
-(the reference engine has no CPU implementation of this path) on the host
-cores and prints the same metric.  With torchrun (N>1) every rank runs its
-own replica of the system (replicas only: the path has no collective).
+--impl reference runs the reference engine's own build (oracle/_ref, compiled
+from the reference sources for sm_100a by oracle/Makefile.ref) on the same
+workload through its C++ API: the same generator and relaxation algorithm on
+the reference's forces, then the same integrator for the same number of
+steps.  The FP64 host oracle is timed beside it as the CPU baseline.  Without
+that build (or without a GPU) the arm times the FP64 host oracle alone.
+With torchrun (N>1) every rank of this arm but rank 0 exits at once; the
+b200 arm runs one replica of the system per rank (replicas only: the path
+has no collective).
 """
 from __future__ import annotations
 
@@ -107,8 +119,30 @@ def dist_env():
         int(os.environ.get("LOCAL_RANK", "0"))
 
 
-def cpu_baseline(sys_obj, evals: int = 2):
-    """FP64 oracle: full force evaluations + position update on all threads."""
+WORKLOADS = {
+    "chain23k": dict(factory="config_solvated_chain", integrator="langevin", friction=1.0,
+                     desc="chain23k: 23,558-atom bead chain in TIP3P, 62.23 A box, PME 64^3 "
+                          "order 6, cutoff 12 / switch 10-12 / list 14, Langevin 300 K "
+                          "gamma 1/ps, dt 2 fs, SETTLE"),
+    "water12k": dict(factory="config_small_water", integrator="leapfrog", friction=0.0,
+                     desc="water12k: 12,480-atom TIP3P box, 50 A, PME 48^3 order 4, cutoff 10 "
+                          "/ switch 8-10 / list 12, leapfrog NVE, dt 2 fs, SETTLE"),
+    "water1m": dict(factory="config_large_water", integrator="nosehoover", friction=0.0,
+                    desc="water1m: 999,999-atom TIP3P box, 215.4 A, PME 216^3 order 4, cutoff "
+                         "10 / switch 8-10 / list 11.5, Nose-Hoover 300 K, dt 2 fs, SETTLE"),
+}
+RELAX_ITERATIONS = 150
+RELAX_MAX_STEP = 0.03          # Angstrom, largest move per iteration
+
+
+def make_system(name: str):
+    from apocharmm_b200 import systems
+    return getattr(systems, WORKLOADS[name]["factory"])()
+
+
+def cpu_baseline(sys_obj, target_s: float = 10.0):
+    """FP64 oracle: full force evaluations + position updates on all host
+    threads, as many as fit in about `target_s` seconds (at least 2)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
     import oracle
@@ -118,7 +152,9 @@ def cpu_baseline(sys_obj, evals: int = 2):
     pos = np.array(sys_obj.pos)
     vel = np.zeros_like(pos)
     inv_m = 1.0 / np.asarray(sys_obj.mass)[:, None]
-    o.evaluate(pos=pos, nthreads=threads)  # warm-up
+    t0 = time.perf_counter()
+    o.evaluate(pos=pos, nthreads=threads)  # warm-up, also sizes the sample
+    evals = int(min(200, max(2, round(target_s / max(1e-3, time.perf_counter() - t0)))))
     t0 = time.perf_counter()
     for _ in range(evals):
         E, grad = o.evaluate(pos=pos, nthreads=threads)
@@ -130,33 +166,94 @@ def cpu_baseline(sys_obj, evals: int = 2):
                       f"updates of the {sys_obj.n_atoms}-atom workload, {dt:.1f} s"}
 
 
+def _reference_build_run(args, s, spec, work):
+    """Relaxes and propagates the workload with the reference engine's own
+    build; returns the harness's JSON result."""
+    import numpy as np
+    from apocharmm_b200.api import rigid_water_fit, water_indices
+    from apocharmm_b200.systems import write_charmm_files, write_crd
+    harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    st = s.settings
+    paths = write_charmm_files(s, work)
+    common = [paths["psf"], paths["prm"], paths["crd"], str(s.box[0]), str(st["kappa"]),
+              str(st["cutnb"]), str(st["ctonnb"]), str(st["ctofnb"]), *map(str, st["nfft"]),
+              str(st["order"])]
+    relaxed = os.path.join(work, "relaxed.txt")
+    subprocess.run([harness, "relax", *common, str(RELAX_ITERATIONS), str(RELAX_MAX_STEP),
+                    relaxed], check=True, timeout=1800, stdout=subprocess.DEVNULL)
+    s.pos = rigid_water_fit(np.loadtxt(relaxed), water_indices(s))
+    write_crd(s, paths["crd"])
+    r = subprocess.run([harness, "md", *common, str(args.warmup * SEG), str(args.steps * SEG),
+                        "2024", str(spec["friction"]), spec["integrator"]],
+                       check=True, timeout=3600, stdout=subprocess.PIPE, text=True)
+    return json.loads([ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1])
+
+
 def run_reference_arm(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
-    from apocharmm_b200.systems import config_solvated_chain
-    s = config_solvated_chain()
-    cb = cpu_baseline(s, evals=max(1, min(args.steps, 3)))
-    line = {"impl": "reference", "metric": "ns/day", "value": cb["value"], "unit": "ns/day",
+    spec = WORKLOADS[args.workload]
+    s = make_system(args.workload)
+    harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    ref = None
+    reason = None
+    if not os.path.exists(harness):
+        reason = "reference build (oracle/_ref) not present"
+    elif subprocess.run(["nvidia-smi", "-L"], stdout=subprocess.DEVNULL,
+                        stderr=subprocess.DEVNULL).returncode != 0:
+        reason = "no GPU visible"
+    else:
+        ref = _reference_build_run(args, s, spec, tempfile.mkdtemp(prefix="apo_ref_"))
+    cb = cpu_baseline(s)
+    line = {"impl": "reference", "metric": "ns/day", "unit": "ns/day",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "data": "synthetic (seeded generator)",
-            "config": {"workload": "chain23k", "atoms": s.n_atoms},
-            "cpu_baseline": cb,
-            "e2e": {"value": cb["value"], "unit": "ns/day", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0},
-            "note": "the reference engine is GPU-only; this arm times the FP64 CPU "
-                    "restatement of its force/step algorithm"}
+            "config": {"workload": spec["desc"], "atoms": s.n_atoms,
+                       "md_steps_per_iteration": SEG}}
+    if ref is not None:
+        line.update({
+            "value": ref["ns_per_day"], "ms_per_step": 1e3 * ref["seconds"] / args.steps,
+            "dtype": "f32 (forces), f64 (integration)",
+            "reference_build": dict(ref, build="reference sources compiled for sm_100a "
+                                               "(oracle/Makefile.ref), driven through its C++ API"),
+            "note": "the reference engine is GPU-only: value is its own build on this GPU, "
+                    "timed on the host between device-wide synchronisations; cpu_baseline is "
+                    "the FP64 host restatement of the same force/step path"})
+    else:
+        line.update({"value": cb["value"], "dtype": "f64",
+                     "note": f"{reason}: value is the FP64 host restatement of the reference's "
+                             "force/step path"})
+    line["cpu_baseline"] = cb
+    line["e2e"] = {"value": line["value"], "unit": "ns/day", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def make_integrator(api, spec, rank):
+    kind = spec["integrator"]
+    if kind == "langevin":
+        integ = api.CudaLangevinThermostatIntegrator(DT_PS)
+        integ.setThermostatFriction(spec["friction"])
+        integ.setReferenceTemperature(300.0)
+        integ.setThermostatRngSeed(777 + rank)
+    elif kind == "leapfrog":
+        integ = api.CudaLeapFrogIntegrator(DT_PS)
+    else:
+        integ = api.CudaNoseHooverIntegrator(DT_PS)
+        integ.setReferenceTemperature(300.0)
+    return integ
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30, help="timed iterations (20 MD steps each)")
+    ap.add_argument("--steps", type=int, default=100, help="timed iterations (20 MD steps each)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="chain23k", choices=sorted(WORKLOADS))
     ap.add_argument("--precise", action="store_true", help="precision form")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -176,12 +273,13 @@ def main():
     torch.cuda.set_device(local)
 
     from apocharmm_b200 import api
-    from apocharmm_b200.systems import config_solvated_chain
-    s = config_solvated_chain()
+    spec = WORKLOADS[args.workload]
+    s = make_system(args.workload)
     work = tempfile.mkdtemp(prefix=f"apo_bench_{rank}_")
     psf, prm, fm, ctx = api.system_context(s, work, precise=args.precise)
     # remove the close contacts of the generated structure (deterministic)
-    s.pos = api.relax(ctx, api.water_indices(s), iterations=150)
+    s.pos = api.relax(ctx, api.water_indices(s), iterations=RELAX_ITERATIONS,
+                      max_step=RELAX_MAX_STEP)
     ctx.setRandomSeedForVelocities(2024 + rank)
     ctx.assignVelocitiesAtTemperature(300.0)
 
@@ -201,10 +299,7 @@ def main():
 
     ctx.resetNeighborList()
     api.call("apo_charmm_context_set_kernel_timing", ctx.handle, api._i(1))
-    integ = api.CudaLangevinThermostatIntegrator(DT_PS)
-    integ.setThermostatFriction(1.0)
-    integ.setReferenceTemperature(300.0)
-    integ.setThermostatRngSeed(777 + rank)
+    integ = make_integrator(api, spec, rank)
     integ.setCharmmContext(ctx)
 
     stream = torch.cuda.ExternalStream(ctx.getStream())
@@ -289,7 +384,7 @@ def main():
         achieved = pairs_avg * FLOP_PER_PAIR / avg_nb_s / 1e12 if avg_nb_s > 0 else None
         cb = None
         if not args.no_cpu_baseline:
-            cb = cpu_baseline(s, evals=2)
+            cb = cpu_baseline(s)
         kps = integ.getKernelsPerStep()
         launches = args.steps * (12 + SEG * (7 + kps))
         line = {
@@ -297,9 +392,7 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 (forces), f64 (integration)", "data": "synthetic (seeded generator)",
-            "config": {"workload": "chain23k: 23,558-atom bead chain in TIP3P, 62.23 A box, "
-                                   "PME 64^3 order 6, cutoff 12 / switch 10-12 / list 14, "
-                                   "Langevin 300 K gamma 1/ps, dt 2 fs, SETTLE",
+            "config": {"workload": spec["desc"],
                        "atoms": s.n_atoms, "md_steps_per_iteration": SEG,
                        "form": "precision" if args.precise else "plain",
                        "l2": "flushed (256 MB device write) before every timed iteration, "
