@@ -2,8 +2,10 @@
 #include "pme.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <functional>
+#include <mutex>
 #include <numeric>
 #include <stdexcept>
 #include <vector>
@@ -727,6 +729,251 @@ void Pme::compute(const float4 *xyzq_s, const int *counts, long long *force, int
   convolve(energy, calc_energy, fp64, s);
   backward(s);
   gather(xyzq_s, counts, force, stride, s);
+}
+
+}  // namespace apo
+
+// ---------------------------------------------------------------------------
+// Reciprocal space from a static scratch area (no allocation of its own)
+// ---------------------------------------------------------------------------
+//
+// The charge grid, complex grid, potential grid, twiddles, B-spline moduli,
+// atom count and energy accumulator live in g_pme_static, a file-scope
+// device array.  Its address is looked up once per device with
+// cudaGetSymbolAddress (that first call also sets the plane kernels'
+// shared-memory attribute, so it belongs before any stream capture).  What
+// must be zero when a call's spread starts: the charge grid and the energy
+// accumulator.  The array is zero at module load, every call clears both
+// with cudaMemsetAsync before its first kernel, and plane_fwd leaves the
+// charge grid zeroed again as it reads it.  The tables are recomputed on
+// the device by every call, so nothing else carries over between calls;
+// calls that overlap in time (two streams, two host threads) race on the
+// area.
+
+namespace apo {
+namespace {
+
+__device__ __align__(256) unsigned char g_pme_static[kPmeStaticScratchBytes];
+
+constexpr int kStaticMaxDevices = 64;
+std::mutex g_static_mu;
+std::atomic<unsigned char *> g_static_base[kStaticMaxDevices];
+
+inline size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+struct StaticLayout {
+  size_t energy, counts, tw, prefac, prefac_d, qgrid, cgrid, phi, total;
+};
+
+StaticLayout static_layout(int nx, int ny, int nz) {
+  StaticLayout l{};
+  const size_t n3 = (size_t)nx + ny + nz;
+  const size_t G = (size_t)nx * ny * nz;
+  const size_t Gc = (size_t)nz * ny * (nx / 2 + 1);
+  size_t o = 0;
+  l.energy = o;   o += align256(kNumEnergyTerms * sizeof(long long));
+  l.counts = o;   o += align256(4 * sizeof(int));
+  l.tw = o;       o += align256(n3 * sizeof(float2));
+  l.prefac = o;   o += align256(n3 * sizeof(float));
+  l.prefac_d = o; o += align256(n3 * sizeof(double));
+  l.qgrid = o;    o += align256(G * sizeof(int));
+  l.cgrid = o;    o += align256(Gc * sizeof(float2));
+  l.phi = o;      o += align256(G * sizeof(float));
+  l.total = o;
+  return l;
+}
+
+// The plan search of Pme::plan_axis (fewest stages, then the smallest sum
+// of radices, radices tried from 8 down to 2) on fixed arrays.
+struct FixedPlan {
+  int cur[8], best[8], ncur = 0, nbest = -1, sbest = 0;
+  void rec(int m) {
+    if (m == 1) {
+      int s = 0;
+      for (int i = 0; i < ncur; ++i) s += cur[i];
+      if (nbest < 0 || ncur < nbest || (ncur == nbest && s < sbest)) {
+        for (int i = 0; i < ncur; ++i) best[i] = cur[i];
+        nbest = ncur;
+        sbest = s;
+      }
+      return;
+    }
+    if (ncur == 8 || (nbest >= 0 && ncur + 1 > nbest)) return;
+    for (int R : {8, 7, 6, 5, 4, 3, 2}) {
+      if (m % R == 0) {
+        cur[ncur++] = R;
+        rec(m / R);
+        --ncur;
+      }
+    }
+  }
+};
+
+bool fixed_plan_axis(int n, FftAxis &a) {
+  FixedPlan p;
+  p.rec(n);
+  if (p.nbest < 0) return false;
+  a = FftAxis{};
+  a.n = n;
+  a.nrad = p.nbest;
+  for (int i = 0; i < p.nbest; ++i) a.radix[i] = p.best[i];
+  return true;
+}
+
+// |b(k)|^2 of the order-p B-spline for grid size n, as bspline_moduli
+__device__ double static_modulus(int n, int order, int k) {
+  double th[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  th[0] = 1.0;
+  for (int kk = 3; kk <= order; ++kk) {
+    const double div = 1.0 / (kk - 1);
+    th[kk - 1] = 0.0;
+    for (int j = 1; j <= kk - 2; ++j) th[kk - j - 1] = div * (j * th[kk - j - 2] + (kk - j) * th[kk - j - 1]);
+    th[0] = div * th[0];
+  }
+  // arr[i - 1] = th[i - 2] for i = 2..order+1: arr[j] = th[j - 1] for j = 1..order
+  double s1 = 0.0, s2 = 0.0;
+  for (int j = 1; j <= order && j < n - 1; ++j) {
+    double sv, cv;
+    sincospi(2.0 * (double)(((long long)k * j) % n) / n, &sv, &cv);
+    s1 += th[j - 1] * cv;
+    s2 += th[j - 1] * sv;
+  }
+  return s1 * s1 + s2 * s2;
+}
+
+__global__ void static_tables_kernel(PmeDims d, float2 *__restrict__ tw, float *__restrict__ prefac,
+                                     double *__restrict__ prefac_d, int *__restrict__ counts,
+                                     int natom) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t == 0) counts[0] = natom;
+  int n, k;
+  if (t < d.nx) { n = d.nx; k = t; }
+  else if (t < d.nx + d.ny) { n = d.ny; k = t - d.nx; }
+  else if (t < d.nx + d.ny + d.nz) { n = d.nz; k = t - d.nx - d.ny; }
+  else return;
+  double sv, cv;
+  sincospi(2.0 * k / n, &sv, &cv);
+  tw[t] = make_float2((float)cv, (float)-sv);
+  double m = static_modulus(n, d.order, k);
+  if (m < 1e-10)
+    m = 0.5 * (static_modulus(n, d.order, (k - 1 + n) % n) + static_modulus(n, d.order, (k + 1) % n));
+  prefac_d[t] = 1.0 / m;
+  prefac[t] = (float)(1.0 / m);
+}
+
+__global__ void static_finish_kernel(const long long *__restrict__ acc, double *__restrict__ energy) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) energy[0] = (double)acc[kEEwks] / kEnergyScale;
+}
+
+unsigned char *static_base() {
+  int dev = 0;
+  APO_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kStaticMaxDevices)
+    throw std::invalid_argument("pme_reciprocal_static: device ordinal out of range");
+  unsigned char *b = g_static_base[dev].load(std::memory_order_acquire);
+  if (b) return b;
+  std::lock_guard<std::mutex> lock(g_static_mu);
+  b = g_static_base[dev].load(std::memory_order_relaxed);
+  if (!b) {
+    void *p = nullptr;
+    APO_CUDA(cudaGetSymbolAddress(&p, g_pme_static));
+    APO_CUDA(cudaFuncSetAttribute(plane_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  227 * 1024));
+    APO_CUDA(cudaFuncSetAttribute(plane_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  227 * 1024));
+    b = static_cast<unsigned char *>(p);
+    g_static_base[dev].store(b, std::memory_order_release);
+  }
+  return b;
+}
+
+}  // namespace
+
+size_t pme_static_scratch_bytes(int nx, int ny, int nz) { return static_layout(nx, ny, nz).total; }
+
+void pme_reciprocal_static(const float4 *xyzq, int n, double Lx, double Ly, double Lz, int nx,
+                           int ny, int nz, int order, double kappa, long long *grad, int stride,
+                           double *energy, bool fp64, cudaStream_t s) {
+  if (n < 0) throw std::invalid_argument("pme_reciprocal_static: negative atom count");
+  if (n > 0 && (xyzq == nullptr || grad == nullptr))
+    throw std::invalid_argument("pme_reciprocal_static: coordinate or gradient pointer is NULL");
+  if (n > 0 && stride < n) throw std::invalid_argument("pme_reciprocal_static: stride < atom count");
+  if (!(Lx > 0.0 && Ly > 0.0 && Lz > 0.0 && kappa > 0.0))
+    throw std::invalid_argument("pme_reciprocal_static: box lengths and kappa must be positive");
+  if (nx <= 0 || ny <= 0 || nz <= 0 || nx % 2 || ny % 2 || nz % 2 || nx > 256 || ny > 256 ||
+      nz > 256)
+    throw std::invalid_argument("pme_reciprocal_static: grid dimensions must be even, 2..256");
+  if (order != 4 && order != 6 && order != 8)
+    throw std::invalid_argument("pme_reciprocal_static: spline order must be 4, 6 or 8");
+  if ((size_t)(ny / 2) * (nx + 2) * sizeof(float2) > 227 * 1024)
+    throw std::invalid_argument("pme_reciprocal_static: grid plane does not fit in shared memory");
+  const StaticLayout l = static_layout(nx, ny, nz);
+  if (l.total > kPmeStaticScratchBytes)
+    throw std::invalid_argument(
+        "pme_reciprocal_static: grid needs more scratch than the static area holds "
+        "(8 MiB: about 5.5e5 grid points)");
+  PmeDims d{};
+  d.nx = nx;
+  d.ny = ny;
+  d.nz = nz;
+  d.nxc = nx / 2 + 1;
+  d.order = order;
+  d.Lx = (float)Lx;
+  d.Ly = (float)Ly;
+  d.Lz = (float)Lz;
+  d.kappa = (float)kappa;
+  if (!fixed_plan_axis(nx, d.ax) || !fixed_plan_axis(ny, d.ay) || !fixed_plan_axis(nz, d.az))
+    throw std::invalid_argument("pme_reciprocal_static: grid sizes must factor into 2, 3, 5 and 7");
+
+  unsigned char *b = static_base();
+  long long *acc = reinterpret_cast<long long *>(b + l.energy);
+  int *counts = reinterpret_cast<int *>(b + l.counts);
+  float2 *tw = reinterpret_cast<float2 *>(b + l.tw);
+  float *prefac = reinterpret_cast<float *>(b + l.prefac);
+  double *prefac_d = reinterpret_cast<double *>(b + l.prefac_d);
+  int *qgrid = reinterpret_cast<int *>(b + l.qgrid);
+  float2 *cgrid = reinterpret_cast<float2 *>(b + l.cgrid);
+  float *phi = reinterpret_cast<float *>(b + l.phi);
+  const size_t G = (size_t)nx * ny * nz;
+
+  APO_CUDA(cudaMemsetAsync(acc, 0, kNumEnergyTerms * sizeof(long long), s));
+  if (n == 0) {
+    if (energy) APO_CUDA(cudaMemsetAsync(energy, 0, sizeof(double), s));
+    return;
+  }
+  APO_CUDA(cudaMemsetAsync(qgrid, 0, G * sizeof(int), s));
+  const int n3 = nx + ny + nz;
+  static_tables_kernel<<<(n3 + 127) / 128, 128, 0, s>>>(d, tw, prefac, prefac_d, counts, n);
+  APO_LAUNCH_CHECK();
+  const int blocks = (n + 31) / 32;
+  switch (order) {
+    case 4: spread_kernel<4><<<blocks, 128, 0, s>>>(xyzq, counts, d, qgrid); break;
+    case 6: spread_kernel<6><<<blocks, 128, 0, s>>>(xyzq, counts, d, qgrid); break;
+    case 8: spread_kernel<8><<<blocks, 128, 0, s>>>(xyzq, counts, d, qgrid); break;
+  }
+  APO_LAUNCH_CHECK();
+  const size_t sm = (size_t)(ny / 2) * (nx + 2) * sizeof(float2);
+  plane_fwd_kernel<<<nz, kPlaneThreads, sm, s>>>(d, qgrid, cgrid, tw, tw + nx);
+  APO_LAUNCH_CHECK();
+  const int pgrid = ((d.nxc + kPencilTX - 1) / kPencilTX) * ny;
+  const float2 *twz = tw + nx + ny;
+  if (fp64)
+    pencil_kernel<true, double><<<pgrid, kPencilThreads, 0, s>>>(d, cgrid, twz, prefac, prefac_d, acc);
+  else
+    pencil_kernel<true, float><<<pgrid, kPencilThreads, 0, s>>>(d, cgrid, twz, prefac, prefac_d, acc);
+  APO_LAUNCH_CHECK();
+  plane_inv_kernel<<<nz, kPlaneThreads, sm, s>>>(d, cgrid, phi, tw, tw + nx);
+  APO_LAUNCH_CHECK();
+  switch (order) {
+    case 4: gather_kernel<4><<<blocks, 256, 0, s>>>(xyzq, counts, d, phi, grad, stride); break;
+    case 6: gather_kernel<6><<<blocks, 256, 0, s>>>(xyzq, counts, d, phi, grad, stride); break;
+    case 8: gather_kernel<8><<<blocks, 256, 0, s>>>(xyzq, counts, d, phi, grad, stride); break;
+  }
+  APO_LAUNCH_CHECK();
+  if (energy) {
+    static_finish_kernel<<<1, 32, 0, s>>>(acc, energy);
+    APO_LAUNCH_CHECK();
+  }
 }
 
 }  // namespace apo

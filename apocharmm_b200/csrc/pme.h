@@ -80,3 +80,26 @@ class Pme {
 };
 
 }  // namespace apo
+
+namespace apo {
+
+// Size of the file-scope device scratch area used by pme_reciprocal_static.
+constexpr size_t kPmeStaticScratchBytes = size_t(8) << 20;  // 8 MiB
+
+// Bytes of that area a grid needs (tables, charge grid, complex grid,
+// potential grid, each 256-byte aligned).
+size_t pme_static_scratch_bytes(int nx, int ny, int nz);
+
+// Reciprocal-space gradient and energy of `n` charges (xyzq, device, any
+// order) with the kernels of Pme, but with every buffer of its own carved
+// from one file-scope __device__ array of kPmeStaticScratchBytes instead of
+// device allocations.  Gradients (2^40 fixed point) are added to the
+// caller's int64 SoA `grad` (x at [0, n), y at [stride, ...), z at
+// [2 stride, ...)); the energy (ewks) is written to energy[0] (device) when
+// `energy` is not null.  Calls on one device share the area and must not
+// overlap in time.
+void pme_reciprocal_static(const float4 *xyzq, int n, double Lx, double Ly, double Lz, int nx,
+                           int ny, int nz, int order, double kappa, long long *grad, int stride,
+                           double *energy, bool fp64_influence, cudaStream_t s);
+
+}  // namespace apo
