@@ -247,6 +247,12 @@ class CharmmContext(_Handle):
         call("apo_charmm_context_get_potential_energy", ctypes.byref(v), self._h)
         return v.value
 
+    def getVirial(self) -> np.ndarray:
+        """3x3 internal virial of the last evaluation made with calc_virial."""
+        a = np.zeros(9)
+        call("apo_charmm_context_get_virial", _ptr(a), _sz(9), self._h)
+        return a.reshape(3, 3)
+
     def getCoordinates(self) -> np.ndarray:
         n = self.getNumAtoms()
         a = np.zeros(3 * n)

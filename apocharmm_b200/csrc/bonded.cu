@@ -2,6 +2,7 @@
 #include "bonded.h"
 
 #include <algorithm>
+#include <stdexcept>
 
 #include "device_util.cuh"
 
@@ -26,8 +27,18 @@ __device__ __forceinline__ void push(const BondedArgs &a, int atom, float gx, fl
   add_fixed(a.force + 2 * a.stride + s, to_fixed_force(gz));
 }
 
+// w -= d (x) g  (one atom's contribution to the internal virial, d its
+// position relative to the term's reference atom)
+__device__ __forceinline__ void vir_sub(float *w, float dx, float dy, float dz, float gx, float gy,
+                                        float gz) {
+  w[0] -= dx * gx; w[1] -= dx * gy; w[2] -= dx * gz;
+  w[3] -= dy * gx; w[4] -= dy * gy; w[5] -= dy * gz;
+  w[6] -= dz * gx; w[7] -= dz * gy; w[8] -= dz * gz;
+}
+
 // E = k (r - r0)^2, reference src/CudaBondedForce.cu:85-120
-__device__ float bond_term(const BondedArgs &a, int i, int j, float2 p) {
+template <bool VIR>
+__device__ float bond_term(const BondedArgs &a, int i, int j, float2 p, float *w) {
   const float3 d = diff(a, i, j);
   const float dx = d.x, dy = d.y, dz = d.z;
   const float r = sqrtf(dx * dx + dy * dy + dz * dz);
@@ -35,12 +46,14 @@ __device__ float bond_term(const BondedArgs &a, int i, int j, float2 p) {
   const float f = 2.f * p.x * db / r;
   push(a, i, f * dx, f * dy, f * dz);
   push(a, j, -f * dx, -f * dy, -f * dz);
+  if (VIR) vir_sub(w, dx, dy, dz, f * dx, f * dy, f * dz);
   return p.x * db * db;
 }
 
 // E = k (theta - theta0)^2 with cos(theta) clamped to +-0.999
 // (src/CudaBondedForce.cu:223-300)
-__device__ float angle_term(const BondedArgs &a, int4 t, float2 p) {
+template <bool VIR>
+__device__ float angle_term(const BondedArgs &a, int4 t, float2 p, float *w) {
   const float3 dv1 = diff(a, t.x, t.y), dv2 = diff(a, t.z, t.y);
   const float ax = dv1.x, ay = dv1.y, az = dv1.z;
   const float bx = dv2.x, by = dv2.y, bz = dv2.z;
@@ -60,14 +73,18 @@ __device__ float angle_term(const BondedArgs &a, int4 t, float2 p) {
   push(a, t.x, gix, giy, giz);
   push(a, t.z, gkx, gky, gkz);
   push(a, t.y, -gix - gkx, -giy - gky, -giz - gkz);
+  if (VIR) {
+    vir_sub(w, ax, ay, az, gix, giy, giz);
+    vir_sub(w, bx, by, bz, gkx, gky, gkz);
+  }
   return p.x * da * da;
 }
 
 // proper (HARM = false: sum k (1 + cos(n phi - delta))) and improper
 // (HARM = true: k (phi - psi0)^2) dihedrals; gradient expressions of the
 // reference (src/CudaBondedForce.cu:517-640)
-template <bool HARM>
-__device__ float dihedral_term(const BondedArgs &a, int4 t, int2 terms, float2 hp) {
+template <bool HARM, bool VIR>
+__device__ float dihedral_term(const BondedArgs &a, int4 t, int2 terms, float2 hp, float *w) {
   const float3 F = diff(a, t.x, t.y), G = diff(a, t.y, t.z), H = diff(a, t.w, t.z);
   const float fx = F.x, fy = F.y, fz = F.z;
   const float gx = G.x, gy = G.y, gz = G.z;
@@ -113,13 +130,19 @@ __device__ float dihedral_term(const BondedArgs &a, int4 t, int2 terms, float2 h
   push(a, t.y, dgx - dfx, dgy - dfy, dgz - dfz);
   push(a, t.z, -dhx - dgx, -dhy - dgy, -dhz - dgz);
   push(a, t.w, dhx, dhy, dhz);
+  if (VIR) {
+    // positions relative to atom k: i - k = F + G, j - k = G, l - k = H
+    vir_sub(w, fx + gx, fy + gy, fz + gz, dfx, dfy, dfz);
+    vir_sub(w, gx, gy, gz, dgx - dfx, dgy - dfy, dgz - dfz);
+    vir_sub(w, hx, hy, hz, dhx, dhy, dhz);
+  }
   return e;
 }
 
 // 1-4 inclusion (LJ14 with VFSW + qq erfc/r) or exclusion correction
 // (qq (erfc - 1)/r = -qq erf/r); src/CudaDirectForceKernels.cu:643-870
-template <bool INCL>
-__device__ void pair14_term(const BondedArgs &a, int2 p, float &e_el, float &e_vdw) {
+template <bool INCL, bool VIR>
+__device__ void pair14_term(const BondedArgs &a, int2 p, float &e_el, float &e_vdw, float *w) {
   const float3 d = diff(a, p.x, p.y);
   const float dx = d.x, dy = d.y, dz = d.z;
   const float r2 = dx * dx + dy * dy + dz * dz;
@@ -150,45 +173,50 @@ __device__ void pair14_term(const BondedArgs &a, int2 p, float &e_el, float &e_v
   const float f = fr * rinv2;
   push(a, p.x, f * dx, f * dy, f * dz);
   push(a, p.y, -f * dx, -f * dy, -f * dz);
+  if (VIR) vir_sub(w, dx, dy, dz, f * dx, f * dy, f * dz);
 }
 
-template <bool ENERGY>
+template <bool ENERGY, bool VIRIAL>
 __global__ void __launch_bounds__(kThreads) bonded_kernel(BondedArgs a) {
   __shared__ unsigned long long sh_e[kNumEnergyTerms];
+  __shared__ unsigned long long sh_v[9];
   if (ENERGY) {
     if (threadIdx.x < kNumEnergyTerms) sh_e[threadIdx.x] = 0ull;
+    if (VIRIAL && threadIdx.x < 9) sh_v[threadIdx.x] = 0ull;
     __syncthreads();
   }
   const int b1 = a.nbond, b2 = b1 + a.nub, b3 = b2 + a.nangle, b4 = b3 + a.ndihe,
             b5 = b4 + a.nimp, b6 = b5 + a.nin14, b7 = b6 + a.nex14;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < b7; t += gridDim.x * blockDim.x) {
     float e = 0.f, e2 = 0.f;
+    float w[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     int slot = -1, slot2 = -1;
     if (t < b1) {
-      e = bond_term(a, a.bond_ij[t].x, a.bond_ij[t].y, a.bond_p[t]);
+      e = bond_term<VIRIAL>(a, a.bond_ij[t].x, a.bond_ij[t].y, a.bond_p[t], w);
       slot = kEBond;
     } else if (t < b2) {
       const int k = t - b1;
-      e = bond_term(a, a.ub_ij[k].x, a.ub_ij[k].y, a.ub_p[k]);
+      e = bond_term<VIRIAL>(a, a.ub_ij[k].x, a.ub_ij[k].y, a.ub_p[k], w);
       slot = kEUreyb;
     } else if (t < b3) {
       const int k = t - b2;
-      e = angle_term(a, a.angle_ijk[k], a.angle_p[k]);
+      e = angle_term<VIRIAL>(a, a.angle_ijk[k], a.angle_p[k], w);
       slot = kEAngle;
     } else if (t < b4) {
       const int k = t - b3;
-      e = dihedral_term<false>(a, a.dihe_ijkl[k], a.dihe_terms[k], make_float2(0.f, 0.f));
+      e = dihedral_term<false, VIRIAL>(a, a.dihe_ijkl[k], a.dihe_terms[k], make_float2(0.f, 0.f),
+                                       w);
       slot = kEDihe;
     } else if (t < b5) {
       const int k = t - b4;
-      e = dihedral_term<true>(a, a.imp_ijkl[k], make_int2(0, 0), a.imp_p[k]);
+      e = dihedral_term<true, VIRIAL>(a, a.imp_ijkl[k], make_int2(0, 0), a.imp_p[k], w);
       slot = kEImdihe;
     } else if (t < b6) {
-      pair14_term<true>(a, a.in14[t - b5], e, e2);
+      pair14_term<true, VIRIAL>(a, a.in14[t - b5], e, e2, w);
       slot = kEElec;
       slot2 = kEVdw;
     } else {
-      pair14_term<false>(a, a.ex14[t - b6], e, e2);
+      pair14_term<false, VIRIAL>(a, a.ex14[t - b6], e, e2, w);
       slot = kEEwex;
     }
     if (ENERGY) {
@@ -196,22 +224,35 @@ __global__ void __launch_bounds__(kThreads) bonded_kernel(BondedArgs a) {
       if (slot2 >= 0)
         atomicAdd(&sh_e[slot2], (unsigned long long)__double2ll_rn((double)e2 * kEnergyScale));
     }
+    if (VIRIAL) {
+#pragma unroll
+      for (int k = 0; k < 9; ++k)
+        atomicAdd(&sh_v[k], (unsigned long long)__double2ll_rn((double)w[k] * kEnergyScale));
+    }
   }
   if (ENERGY) {
     __syncthreads();
     if (threadIdx.x < kNumEnergyTerms && sh_e[threadIdx.x])
       add_fixed(a.energy + threadIdx.x, (long long)sh_e[threadIdx.x]);
+    if (VIRIAL && threadIdx.x < 9 && sh_v[threadIdx.x])
+      add_fixed(a.virial + threadIdx.x, (long long)sh_v[threadIdx.x]);
   }
 }
 
 }  // namespace
 
-void launch_bonded(const BondedArgs &a, bool energy, cudaStream_t s) {
+void launch_bonded(const BondedArgs &a, bool energy, cudaStream_t s, bool virial) {
   const long long total = (long long)a.nbond + a.nub + a.nangle + a.ndihe + a.nimp + a.nin14 + a.nex14;
   if (total == 0) return;
   int blocks = (int)std::min<long long>((total + kThreads - 1) / kThreads, 148 * 16);
-  if (energy) bonded_kernel<true><<<blocks, kThreads, 0, s>>>(a);
-  else bonded_kernel<false><<<blocks, kThreads, 0, s>>>(a);
+  if (virial) {
+    if (!a.virial) throw std::invalid_argument("bonded: virial requested without a buffer");
+    bonded_kernel<true, true><<<blocks, kThreads, 0, s>>>(a);
+  } else if (energy) {
+    bonded_kernel<true, false><<<blocks, kThreads, 0, s>>>(a);
+  } else {
+    bonded_kernel<false, false><<<blocks, kThreads, 0, s>>>(a);
+  }
   APO_LAUNCH_CHECK();
 }
 

@@ -31,8 +31,11 @@ struct BondedArgs {
   int nex14; const int2 *ex14;
   const int *vdwtype; const float2 *vdw14; int ntype;
   NbSetup nb;             // kappa and the VFSW constants for the 1-4 LJ
+  long long *virial = nullptr;  // 3x3 internal virial, 2^32 fixed point (virial launches)
 };
 
-void launch_bonded(const BondedArgs &a, bool energy, cudaStream_t s);
+// virial: also accumulate W = -sum over terms of (r_k - r_ref) (x) dU/dr_k
+// into a.virial (implies energy)
+void launch_bonded(const BondedArgs &a, bool energy, cudaStream_t s, bool virial = false);
 
 }  // namespace apo

@@ -381,6 +381,18 @@ extern "C" apo_status apo_charmm_context_get_energy_components(double *e, const 
   }, fn);
 }
 
+extern "C" apo_status apo_charmm_context_get_virial(double *v, const size_t len,
+                                                    apo_charmm_context *c) {
+  const char *fn = "apo_charmm_context_get_virial";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
+    APO_RETURN_IF(require_buffer(v, len, (size_t)9, fn, "virial buffer"));
+    auto w = c->object->getForceManager()->getVirial(c->object->stream());
+    for (int k = 0; k < 9; ++k) v[k] = w[k];
+    return APO_STATUS_OK;
+  }, fn);
+}
+
 extern "C" apo_status apo_charmm_context_get_potential_energy(double *e, apo_charmm_context *c) {
   const char *fn = "apo_charmm_context_get_potential_energy";
   return guard([&]() -> apo_status {
@@ -398,7 +410,7 @@ extern "C" apo_status apo_charmm_context_set_coordinates_xyz(apo_charmm_context 
     APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
     APO_RETURN_IF(require_ptr(xyz, fn, "xyz"));
     if (len != 3 * (size_t)c->object->getNumAtoms()) return invalid(fn, "len must be 3*N");
-    c->object->setCoordinates(std::vector<double>(xyz, xyz + len));
+    c->object->setCoordinatesXyz(xyz);
     return APO_STATUS_OK;
   }, fn);
 }
@@ -409,8 +421,7 @@ extern "C" apo_status apo_charmm_context_get_coordinates(double *xyz, const size
   return guard([&]() -> apo_status {
     APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
     APO_RETURN_IF(require_buffer(xyz, len, 3 * (size_t)c->object->getNumAtoms(), fn, "buffer"));
-    auto v = c->object->getCoordinates();
-    std::copy(v.begin(), v.end(), xyz);
+    c->object->getCoordinatesXyz(xyz);
     return APO_STATUS_OK;
   }, fn);
 }
@@ -422,7 +433,7 @@ extern "C" apo_status apo_charmm_context_set_velocities(apo_charmm_context *c, c
     APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
     APO_RETURN_IF(require_ptr(v, fn, "v"));
     if (len != 3 * (size_t)c->object->getNumAtoms()) return invalid(fn, "len must be 3*N");
-    c->object->setVelocities(std::vector<double>(v, v + len));
+    c->object->setVelocitiesXyz(v);
     return APO_STATUS_OK;
   }, fn);
 }
@@ -433,8 +444,7 @@ extern "C" apo_status apo_charmm_context_get_velocities(double *v, const size_t 
   return guard([&]() -> apo_status {
     APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
     APO_RETURN_IF(require_buffer(v, len, 3 * (size_t)c->object->getNumAtoms(), fn, "buffer"));
-    auto w = c->object->getVelocities();
-    std::copy(w.begin(), w.end(), v);
+    c->object->getVelocitiesXyz(v);
     return APO_STATUS_OK;
   }, fn);
 }

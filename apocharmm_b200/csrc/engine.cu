@@ -1,6 +1,8 @@
 // ForceManager / CharmmContext; see engine.h.
 #include "engine.h"
 
+#include <climits>
+
 #include <algorithm>
 #include <cmath>
 #include <random>
@@ -182,8 +184,9 @@ void ForceManager::initialize() {
   m_Stride = m_Nbl.dims().slot_cap;
   m_Force.alloc((size_t)3 * m_Stride);
   APO_CUDA(cudaMemset(m_Force.p, 0, (size_t)3 * m_Stride * sizeof(long long)));
-  m_Energy.alloc(kNumEnergyTerms);
-  APO_CUDA(cudaMemset(m_Energy.p, 0, kNumEnergyTerms * sizeof(long long)));
+  // energy terms, then the 3x3 virial (row major), all 2^32 fixed point
+  m_Energy.alloc(kNumEnergyTerms + 9);
+  APO_CUDA(cudaMemset(m_Energy.p, 0, (kNumEnergyTerms + 9) * sizeof(long long)));
 
   double q2 = 0.0;
   for (double q : m_Top.charge) q2 += q * q;
@@ -211,13 +214,17 @@ void ForceManager::resetNeighborList(const float4 *d_xyzq, cudaStream_t s) {
   }
 }
 
-void ForceManager::calcForce(const float4 *d_xyzq, bool calcEnergy, bool /*calcVirial*/,
+void ForceManager::calcForce(const float4 *d_xyzq, bool calcEnergy, bool calcVirial,
                              cudaStream_t s, bool clear) {
   if (!m_Initialized) throw std::runtime_error("ForceManager is not initialized");
   if (!m_ListBuilt) resetNeighborList(d_xyzq, s);
   else if (clear) m_Nbl.refresh(d_xyzq, s);
   if (clear) APO_CUDA(cudaMemsetAsync(m_Force.p, 0, (size_t)3 * m_Stride * sizeof(long long), s));
-  APO_CUDA(cudaMemsetAsync(m_Energy.p, 0, kNumEnergyTerms * sizeof(long long), s));
+  if (calcVirial) calcEnergy = true;
+  long long *virial = calcVirial ? m_Energy.p + kNumEnergyTerms : nullptr;
+  APO_CUDA(cudaMemsetAsync(m_Energy.p, 0,
+                           (kNumEnergyTerms + (calcVirial ? 9 : 0)) * sizeof(long long), s));
+  m_VirialValid = calcVirial;
   APO_CUDA(cudaEventRecord(m_EvFork, s));
   if (m_ComponentMask & 2) {
     APO_CUDA(cudaStreamWaitEvent(m_SNb, m_EvFork, 0));
@@ -235,6 +242,7 @@ void ForceManager::calcForce(const float4 *d_xyzq, bool calcEnergy, bool /*calcV
     a.stride = m_Stride;
     a.energy = m_Energy.p;
     a.setups = m_Setup.p;
+    a.virial = virial;
     cudaEvent_t t1 = nullptr;
     bool timer_capture = false;
     if (m_Timing) {
@@ -256,7 +264,7 @@ void ForceManager::calcForce(const float4 *d_xyzq, bool calcEnergy, bool /*calcV
       t1 = m_Timers[m_TimerCursor].second;
       ++m_TimerCursor;
     }
-    launch_nonbonded(a, calcEnergy, m_Precise, m_SNb);
+    launch_nonbonded(a, calcEnergy, m_Precise, m_SNb, calcVirial);
     if (t1) {
       if (timer_capture) APO_CUDA(cudaEventRecordWithFlags(t1, m_SNb, cudaEventRecordExternal));
       else APO_CUDA(cudaEventRecord(t1, m_SNb));
@@ -267,7 +275,7 @@ void ForceManager::calcForce(const float4 *d_xyzq, bool calcEnergy, bool /*calcV
   if (m_ComponentMask & 4) {
     APO_CUDA(cudaStreamWaitEvent(m_SPme, m_EvFork, 0));
     m_Pme.compute(m_Nbl.xyzq_s, m_Nbl.counts, m_Force.p, m_Stride, m_Energy.p, calcEnergy,
-                  m_Precise, m_SPme);
+                  m_Precise, m_SPme, virial);
     APO_CUDA(cudaEventRecord(m_EvPme, m_SPme));
     APO_CUDA(cudaStreamWaitEvent(s, m_EvPme, 0));
   }
@@ -292,7 +300,8 @@ void ForceManager::calcForce(const float4 *d_xyzq, bool calcEnergy, bool /*calcV
     b.vdw14 = m_Vdw14.p;
     b.ntype = (int)m_Top.types.size();
     b.nb = m_HostSetup;
-    launch_bonded(b, calcEnergy, m_SBond);
+    b.virial = virial;
+    launch_bonded(b, calcEnergy, m_SBond, calcVirial);
     APO_CUDA(cudaEventRecord(m_EvBond, m_SBond));
     APO_CUDA(cudaStreamWaitEvent(s, m_EvBond, 0));
   }
@@ -306,6 +315,18 @@ std::map<std::string, double> ForceManager::getEnergyComponents(cudaStream_t s) 
   for (int k = 0; k < kNumEnergyTerms; ++k) m[kEnergyNames[k]] = (double)e[k] * kInvEnergyScale;
   m["ewse"] = (m_ComponentMask & 4) ? m_SelfEnergy : 0.0;
   return m;
+}
+
+std::vector<double> ForceManager::getVirial(cudaStream_t s) {
+  if (!m_Initialized) throw std::runtime_error("ForceManager is not initialized");
+  if (!m_VirialValid)
+    throw std::runtime_error("getVirial: the last force evaluation did not compute the virial");
+  long long v[9];
+  APO_CUDA(cudaMemcpyAsync(v, m_Energy.p + kNumEnergyTerms, sizeof(v), cudaMemcpyDeviceToHost, s));
+  APO_CUDA(cudaStreamSynchronize(s));
+  std::vector<double> out(9);
+  for (int k = 0; k < 9; ++k) out[k] = (double)v[k] * kInvEnergyScale;
+  return out;
 }
 
 double ForceManager::getPotentialEnergy(cudaStream_t s) {
@@ -382,22 +403,69 @@ void CharmmContext::useHolonomicConstraints(bool flag) {
   m_Ndegf = m_Fm->topology().degrees_of_freedom(flag);
 }
 
+namespace {
+
+// first atom with a non-finite coordinate (atomicMin over the array)
+__global__ void check_finite_kernel(const double *__restrict__ xyz, int n, int *__restrict__ bad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (!isfinite(xyz[3 * i]) || !isfinite(xyz[3 * i + 1]) || !isfinite(xyz[3 * i + 2]))
+    atomicMin(bad, i);
+}
+
+// interleaved x,y,z -> the .x/.y/.z of double4 (w kept); skipped entirely
+// when the check above found a bad atom, so the state stays unchanged
+__global__ void pack_xyz_kernel(const double *__restrict__ xyz, int n, double4 *__restrict__ out,
+                                const int *__restrict__ bad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || (bad && *bad != INT_MAX)) return;
+  double4 v = out[i];
+  v.x = xyz[3 * i];
+  v.y = xyz[3 * i + 1];
+  v.z = xyz[3 * i + 2];
+  out[i] = v;
+}
+
+__global__ void unpack_xyz_kernel(const double4 *__restrict__ in, int n, double *__restrict__ xyz) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double4 v = in[i];
+  xyz[3 * i] = v.x;
+  xyz[3 * i + 1] = v.y;
+  xyz[3 * i + 2] = v.z;
+}
+
+}  // namespace
+
 void CharmmContext::setCoordinates(const std::vector<double> &xyz) {
   if ((int)xyz.size() != 3 * m_N) {
     std::ostringstream m;
     m << "setCoordinates: expected " << 3 * m_N << " values, got " << xyz.size();
     throw std::invalid_argument(m.str());
   }
-  const Topology &t = m_Fm->topology();
-  std::vector<double4> c(m_N);
-  for (int i = 0; i < m_N; ++i) {
-    if (!std::isfinite(xyz[3 * i]) || !std::isfinite(xyz[3 * i + 1]) || !std::isfinite(xyz[3 * i + 2]))
-      throw std::invalid_argument("setCoordinates: non-finite coordinate for atom " +
-                                  std::to_string(i));
-    c[i] = make_double4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], t.charge[i]);
+  setCoordinatesXyz(xyz.data());
+}
+
+void CharmmContext::setCoordinatesXyz(const double *xyz) {
+  if (m_Stage.n != (size_t)3 * m_N) m_Stage.alloc((size_t)3 * m_N);
+  if (m_BadAtom.n != 1) m_BadAtom.alloc(1);
+  const int ok = INT_MAX;
+  APO_CUDA(cudaMemcpyAsync(m_BadAtom.p, &ok, sizeof(int), cudaMemcpyHostToDevice, m_Stream));
+  APO_CUDA(cudaMemcpyAsync(m_Stage.p, xyz, (size_t)3 * m_N * sizeof(double),
+                           cudaMemcpyHostToDevice, m_Stream));
+  const int b = (m_N + 255) / 256;
+  if (m_N > 0) {
+    check_finite_kernel<<<b, 256, 0, m_Stream>>>(m_Stage.p, m_N, m_BadAtom.p);
+    APO_LAUNCH_CHECK();
+    pack_xyz_kernel<<<b, 256, 0, m_Stream>>>(m_Stage.p, m_N, m_Coords.p, m_BadAtom.p);
+    APO_LAUNCH_CHECK();
   }
-  APO_CUDA(cudaMemcpyAsync(m_Coords.p, c.data(), m_N * sizeof(double4), cudaMemcpyHostToDevice,
-                           m_Stream));
+  int bad = INT_MAX;
+  APO_CUDA(cudaMemcpyAsync(&bad, m_BadAtom.p, sizeof(int), cudaMemcpyDeviceToHost, m_Stream));
+  APO_CUDA(cudaStreamSynchronize(m_Stream));
+  if (bad != INT_MAX)
+    throw std::invalid_argument("setCoordinates: non-finite coordinate for atom " +
+                                std::to_string(bad));
   launch_coords_to_xyzq(m_Coords.p, m_Xyzq.p, m_N, m_Stream);
   m_HasCoords = true;
   resetNeighborList(m_Stream);
@@ -405,40 +473,53 @@ void CharmmContext::setCoordinates(const std::vector<double> &xyz) {
 }
 
 std::vector<double> CharmmContext::getCoordinates() {
-  std::vector<double4> c(m_N);
-  APO_CUDA(cudaMemcpyAsync(c.data(), m_Coords.p, m_N * sizeof(double4), cudaMemcpyDeviceToHost,
-                           m_Stream));
-  APO_CUDA(cudaStreamSynchronize(m_Stream));
   std::vector<double> out((size_t)3 * m_N);
-  for (int i = 0; i < m_N; ++i) {
-    out[3 * i] = c[i].x;
-    out[3 * i + 1] = c[i].y;
-    out[3 * i + 2] = c[i].z;
-  }
+  getCoordinatesXyz(out.data());
   return out;
+}
+
+void CharmmContext::getCoordinatesXyz(double *xyz) {
+  if (m_Stage.n != (size_t)3 * m_N) m_Stage.alloc((size_t)3 * m_N);
+  if (m_N > 0) {
+    unpack_xyz_kernel<<<(m_N + 255) / 256, 256, 0, m_Stream>>>(m_Coords.p, m_N, m_Stage.p);
+    APO_LAUNCH_CHECK();
+  }
+  APO_CUDA(cudaMemcpyAsync(xyz, m_Stage.p, (size_t)3 * m_N * sizeof(double),
+                           cudaMemcpyDeviceToHost, m_Stream));
+  APO_CUDA(cudaStreamSynchronize(m_Stream));
 }
 
 void CharmmContext::setVelocities(const std::vector<double> &v) {
   if ((int)v.size() != 3 * m_N) throw std::invalid_argument("setVelocities: wrong length");
-  std::vector<double4> vm = m_VelMass.download();
-  for (int i = 0; i < m_N; ++i) {
-    vm[i].x = v[3 * i];
-    vm[i].y = v[3 * i + 1];
-    vm[i].z = v[3 * i + 2];
+  setVelocitiesXyz(v.data());
+}
+
+void CharmmContext::setVelocitiesXyz(const double *v) {
+  if (m_Stage.n != (size_t)3 * m_N) m_Stage.alloc((size_t)3 * m_N);
+  APO_CUDA(cudaMemcpyAsync(m_Stage.p, v, (size_t)3 * m_N * sizeof(double), cudaMemcpyHostToDevice,
+                           m_Stream));
+  if (m_N > 0) {
+    pack_xyz_kernel<<<(m_N + 255) / 256, 256, 0, m_Stream>>>(m_Stage.p, m_N, m_VelMass.p, nullptr);
+    APO_LAUNCH_CHECK();
   }
-  APO_CUDA(cudaMemcpy(m_VelMass.p, vm.data(), m_N * sizeof(double4), cudaMemcpyHostToDevice));
+  APO_CUDA(cudaStreamSynchronize(m_Stream));
 }
 
 std::vector<double> CharmmContext::getVelocities() {
-  APO_CUDA(cudaStreamSynchronize(m_Stream));
-  std::vector<double4> vm = m_VelMass.download();
   std::vector<double> out((size_t)3 * m_N);
-  for (int i = 0; i < m_N; ++i) {
-    out[3 * i] = vm[i].x;
-    out[3 * i + 1] = vm[i].y;
-    out[3 * i + 2] = vm[i].z;
-  }
+  getVelocitiesXyz(out.data());
   return out;
+}
+
+void CharmmContext::getVelocitiesXyz(double *v) {
+  if (m_Stage.n != (size_t)3 * m_N) m_Stage.alloc((size_t)3 * m_N);
+  if (m_N > 0) {
+    unpack_xyz_kernel<<<(m_N + 255) / 256, 256, 0, m_Stream>>>(m_VelMass.p, m_N, m_Stage.p);
+    APO_LAUNCH_CHECK();
+  }
+  APO_CUDA(cudaMemcpyAsync(v, m_Stage.p, (size_t)3 * m_N * sizeof(double), cudaMemcpyDeviceToHost,
+                           m_Stream));
+  APO_CUDA(cudaStreamSynchronize(m_Stream));
 }
 
 // Maxwell-Boltzmann velocities with std::mt19937 and one

@@ -111,6 +111,10 @@ class ForceManager {
 
   std::map<std::string, double> getEnergyComponents(cudaStream_t s);
   double getPotentialEnergy(cudaStream_t s);
+  // internal virial of the last evaluation made with calcVirial, row-major
+  // 3x3 (kcal/mol): W = -sum r (x) dU/dr over direct, reciprocal, bonded,
+  // 1-4 and exclusion terms (ForceManager::getVirial, src/ForceManager.cu:393)
+  std::vector<double> getVirial(cudaStream_t s);
   // total gradient, global atom order, (N,3) row-major
   void getForces(std::vector<double> &out, cudaStream_t s);
 
@@ -138,6 +142,7 @@ class ForceManager {
   int m_Nfft[3] = {-1, -1, -1};
   int m_Order = 4;
   int m_VdwType = VDW_VFSW;
+  bool m_VirialValid = false;
   bool m_Precise = false;
   bool m_Initialized = false;
   bool m_ListBuilt = false;
@@ -177,6 +182,13 @@ class CharmmContext {
   std::vector<double> getCoordinates();
   void setVelocities(const std::vector<double> &v);
   std::vector<double> getVelocities();
+  // the same four transfers on a caller's x,y,z-interleaved host array of
+  // 3N doubles (pinned memory gives full-bandwidth copies): one copy
+  // through a device staging array and one pack/unpack kernel each
+  void setCoordinatesXyz(const double *xyz);
+  void getCoordinatesXyz(double *xyz);
+  void setVelocitiesXyz(const double *v);
+  void getVelocitiesXyz(double *v);
   void setRandomSeedForVelocities(uint64_t seed) { m_Seed = seed; }
   void assignVelocitiesAtTemperature(double temperature);
   void useHolonomicConstraints(bool flag);
@@ -211,6 +223,8 @@ class CharmmContext {
   cudaStream_t m_Stream = nullptr;
   DeviceArray<double4> m_Coords, m_VelMass;
   DeviceArray<float4> m_Xyzq;
+  DeviceArray<double> m_Stage;    // 3N doubles: host transfers
+  DeviceArray<int> m_BadAtom;     // first non-finite coordinate, or INT_MAX
   DeviceArray<int2> m_Groups;
 };
 

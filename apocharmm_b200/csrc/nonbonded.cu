@@ -96,7 +96,7 @@ __device__ __forceinline__ float erfc_from_exp(float x, float expv) {
   return expv * t * p;
 }
 
-template <bool ENERGY, bool PER_PAIR>
+template <bool ENERGY, bool PER_PAIR, bool VIRIAL = false>
 __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
   __shared__ float4 sh_xq[kWarps][32];
   __shared__ int sh_t[kWarps][32];
@@ -112,6 +112,7 @@ __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
   const int nwork = a.counts[2];
   const int stride = a.stride;
   double e_elec = 0.0, e_vdw = 0.0;
+  double dv[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // xx xy xz yy yz zz (VIRIAL)
   using Acc = typename std::conditional<PER_PAIR, long long, float>::type;
 
   for (int w = blockIdx.x * kWarps + wib; w < nwork; w += gridDim.x * kWarps) {
@@ -137,6 +138,7 @@ __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
       hi_z = fmaxf(hi_z, __shfl_xor_sync(0xffffffffu, hi_z, o));
     }
     Acc fix = 0, fiy = 0, fiz = 0;
+    float vw[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 
     for (int t = wk.y; t < wk.z; ++t) {
       const int2 tl = a.tiles[t];
@@ -205,6 +207,15 @@ __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
               e_vdw += (double)((1.f / 12.f) * cc.y * (A12 * t12 * t12 + C12) -
                                 (1.f / 6.f) * cc.x * (A6 * t6 * t6 + C6));
             }
+            if (VIRIAL) {
+              const float gx = fij * dx, gy = fij * dy, gz = fij * dz;
+              vw[0] -= gx * dx;
+              vw[1] -= gx * dy;
+              vw[2] -= gx * dz;
+              vw[3] -= gy * dy;
+              vw[4] -= gy * dz;
+              vw[5] -= gz * dz;
+            }
             if (PER_PAIR) {
               const long long gx = to_fixed_force(fij * dx);
               const long long gy = to_fixed_force(fij * dy);
@@ -248,6 +259,10 @@ __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
         }
       }
     }
+    if (VIRIAL) {
+#pragma unroll
+      for (int k = 0; k < 6; ++k) dv[k] += (double)vw[k];
+    }
     if (ivalid) {
       if (PER_PAIR) {
         add_fixed(a.force + islot, (long long)fix);
@@ -274,9 +289,23 @@ __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
       add_fixed(a.energy + kEVdw, iv);
     }
   }
+  if (VIRIAL) {
+    // xx xy xz yy yz zz -> row-major 3x3 (symmetric)
+    constexpr int kSlot[6][2] = {{0, 0}, {1, 3}, {2, 6}, {4, 4}, {5, 7}, {8, 8}};
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      long long iw = __double2ll_rn(dv[k] * kEnergyScale);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) iw += __shfl_xor_sync(0xffffffffu, iw, o);
+      if (lane == 0) {
+        add_fixed(a.virial + kSlot[k][0], iw);
+        if (kSlot[k][1] != kSlot[k][0]) add_fixed(a.virial + kSlot[k][1], iw);
+      }
+    }
+  }
 }
 
-template <bool E, bool P>
+template <bool E, bool P, bool V = false>
 void launch_t(const NbArgs &a, cudaStream_t s) {
   static int grid = 0;
   size_t sm = (size_t)a.ntype * a.ntype * sizeof(float2);
@@ -284,21 +313,27 @@ void launch_t(const NbArgs &a, cudaStream_t s) {
     int dev, nsm, per = 0;
     APO_CUDA(cudaGetDevice(&dev));
     APO_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    APO_CUDA(cudaFuncSetAttribute(nb_kernel<E, P>,
+    APO_CUDA(cudaFuncSetAttribute(nb_kernel<E, P, V>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
-    APO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, nb_kernel<E, P>, kThreads,
+    APO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, nb_kernel<E, P, V>, kThreads,
                                                            64 * 1024 > sm ? sm : 64 * 1024));
     grid = nsm * (per > 0 ? per : 1);
   }
-  nb_kernel<E, P><<<grid, kThreads, sm, s>>>(a);
+  nb_kernel<E, P, V><<<grid, kThreads, sm, s>>>(a);
   APO_LAUNCH_CHECK();
 }
 
 }  // namespace
 
-void launch_nonbonded(const NbArgs &a, bool energy, bool per_pair, cudaStream_t s) {
+void launch_nonbonded(const NbArgs &a, bool energy, bool per_pair, cudaStream_t s, bool virial) {
   if (a.ntype * a.ntype * sizeof(float2) > 64 * 1024)
     throw std::invalid_argument("nonbonded: too many LJ types for the shared table");
+  if (virial) {
+    if (!a.virial) throw std::invalid_argument("nonbonded: virial requested without a buffer");
+    if (per_pair) launch_t<true, true, true>(a, s);
+    else launch_t<true, false, true>(a, s);
+    return;
+  }
   if (per_pair) {
     if (energy) launch_t<true, true>(a, s);
     else launch_t<false, true>(a, s);

@@ -32,12 +32,16 @@ struct NbArgs {
   int stride;
   long long *energy;      // energy slots (elec, vdw used)
   const NbSetup *setups;  // per system (indexed by work item .w)
+  long long *virial = nullptr;  // 3x3 internal virial, 2^32 fixed point (virial launches)
 };
 
 // per_pair: round every pair contribution to 64-bit fixed point before it is
 // summed (order-independent, the reference's accumulation,
 // include/gpu_utils.h:281-312); otherwise FP32 sums per atom and tile are
 // rounded once (deterministic for a given tile list).
-void launch_nonbonded(const NbArgs &a, bool energy, bool per_pair, cudaStream_t s);
+// virial: also accumulate W = -sum over pairs of d (x) dU/dd into a.virial
+// (implies energy).
+void launch_nonbonded(const NbArgs &a, bool energy, bool per_pair, cudaStream_t s,
+                      bool virial = false);
 
 }  // namespace apo

@@ -394,14 +394,16 @@ __global__ void __launch_bounds__(kPlaneThreads) plane_inv_kernel(PmeDims d,
 // ------------------------------------------------------------------------
 // z pencils: FFT, influence function, inverse FFT
 // ------------------------------------------------------------------------
-template <bool ENERGY, typename FT>
+template <bool ENERGY, typename FT, bool VIRIAL = false>
 __global__ void __launch_bounds__(kPencilThreads) pencil_kernel(PmeDims d, float2 *__restrict__ cgrid,
                                                                 const float2 *__restrict__ twz,
                                                                 const float *__restrict__ prefac,
                                                                 const double *__restrict__ prefac_d,
-                                                                long long *__restrict__ energy) {
+                                                                long long *__restrict__ energy,
+                                                                long long *__restrict__ virial = nullptr) {
   __shared__ float2 buf[256 * kPencilTX];
   __shared__ double sh_e[kPencilThreads / 32];
+  __shared__ double sh_v[6][kPencilThreads / 32];
   const int nx = d.nx, ny = d.ny, nz = d.nz, nxc = d.nxc;
   const int tiles_x = (nxc + kPencilTX - 1) / kPencilTX;
   const int py = blockIdx.x / tiles_x, x0 = (blockIdx.x - py * tiles_x) * kPencilTX;
@@ -421,21 +423,32 @@ __global__ void __launch_bounds__(kPencilThreads) pencil_kernel(PmeDims d, float
                                  : reinterpret_cast<const FT *>(prefac);
   const FT pyv = pf[nx + ky];
   double e = 0.0;
+  double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   for (int idx = threadIdx.x; idx < nz * kPencilTX; idx += blockDim.x) {
     const int pz = idx / kPencilTX, xt = idx - pz * kPencilTX, kx = x0 + xt;
     if (kx >= nxc) continue;
     const int kz = dig_unrev(pz, d.az);
     FT eterm = 0;
-    if (kx != 0 || ky != 0 || kz != 0) {
-      const FT m1 = (FT)(kx >= nf1 ? kx - nx : kx) / (FT)d.Lx;
-      const FT m3 = (FT)(kz >= nf3 ? kz - nz : kz) / (FT)d.Lz;
-      const FT msq = m1 * m1 + m2 * m2 + m3 * m3;
+    const FT m1 = (FT)(kx >= nf1 ? kx - nx : kx) / (FT)d.Lx;
+    const FT m3 = (FT)(kz >= nf3 ? kz - nz : kz) / (FT)d.Lz;
+    const FT msq = m1 * m1 + m2 * m2 + m3 * m3;
+    if (kx != 0 || ky != 0 || kz != 0)
       eterm = exp(-fac * msq) * piv_inv * pf[kx] * pyv * pf[nx + ny + kz] / msq;
-    }
     const float2 q = buf[idx];
     if (ENERGY) {
       const FT mult = kx >= 1 ? (FT)2 : (FT)1;
-      e += (double)(mult * eterm * ((FT)q.x * q.x + (FT)q.y * q.y));
+      const FT t1 = mult * eterm * ((FT)q.x * q.x + (FT)q.y * q.y);
+      e += (double)t1;
+      if (VIRIAL && eterm != (FT)0) {
+        // reference scalar_sum (src/CudaPMERecip.cu:770-790): t1 (vterm m_a m_b - delta_ab)
+        const FT vt = (FT)2 * (fac + (FT)1 / msq);
+        v[0] += (double)(t1 * (vt * m1 * m1 - (FT)1));
+        v[1] += (double)(t1 * vt * m1 * m2);
+        v[2] += (double)(t1 * vt * m1 * m3);
+        v[3] += (double)(t1 * (vt * m2 * m2 - (FT)1));
+        v[4] += (double)(t1 * vt * m2 * m3);
+        v[5] += (double)(t1 * (vt * m3 * m3 - (FT)1));
+      }
     }
     buf[idx] = make_float2((float)(q.x * eterm), (float)(q.y * eterm));
   }
@@ -448,11 +461,27 @@ __global__ void __launch_bounds__(kPencilThreads) pencil_kernel(PmeDims d, float
   if (ENERGY) {
     e = warp_sum(e);
     if ((threadIdx.x & 31) == 0) sh_e[threadIdx.x >> 5] = e;
+    if (VIRIAL) {
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        const double t = warp_sum(v[k]);
+        if ((threadIdx.x & 31) == 0) sh_v[k][threadIdx.x >> 5] = t;
+      }
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
       double t = 0.0;
       for (int w = 0; w < kPencilThreads / 32; ++w) t += sh_e[w];
       add_energy(energy + kEEwks, 0.5 * kCcelec * t);
+    }
+    if (VIRIAL && threadIdx.x < 6) {
+      double t = 0.0;
+      for (int w = 0; w < kPencilThreads / 32; ++w) t += sh_v[threadIdx.x][w];
+      // xx xy xz yy yz zz -> row-major 3x3, W = -ccelec/2 * sum
+      constexpr int kA[6] = {0, 1, 2, 4, 5, 8}, kB[6] = {0, 3, 6, 4, 7, 8};
+      const long long iw = __double2ll_rn(-0.5 * kCcelec * t * kEnergyScale);
+      add_fixed(virial + kA[threadIdx.x], iw);
+      if (kB[threadIdx.x] != kA[threadIdx.x]) add_fixed(virial + kB[threadIdx.x], iw);
     }
   }
 }
@@ -687,10 +716,19 @@ void Pme::forward(cudaStream_t s) {
   APO_LAUNCH_CHECK();
 }
 
-void Pme::convolve(long long *energy, bool calc_energy, bool fp64, cudaStream_t s) {
+void Pme::convolve(long long *energy, bool calc_energy, bool fp64, cudaStream_t s,
+                   long long *virial) {
   const int tiles_x = (m_d.nxc + kPencilTX - 1) / kPencilTX;
   const int grid = tiles_x * m_d.ny;
   const float2 *twz = m_tw + m_d.nx + m_d.ny;
+  if (virial) {
+    if (fp64)
+      pencil_kernel<true, double, true><<<grid, kPencilThreads, 0, s>>>(m_d, cgrid, twz, m_prefac, m_prefac_d, energy, virial);
+    else
+      pencil_kernel<true, float, true><<<grid, kPencilThreads, 0, s>>>(m_d, cgrid, twz, m_prefac, m_prefac_d, energy, virial);
+    APO_LAUNCH_CHECK();
+    return;
+  }
   if (fp64) {
     if (calc_energy)
       pencil_kernel<true, double><<<grid, kPencilThreads, 0, s>>>(m_d, cgrid, twz, m_prefac, m_prefac_d, energy);
@@ -723,10 +761,11 @@ void Pme::gather(const float4 *xyzq_s, const int *counts, long long *force, int 
 }
 
 void Pme::compute(const float4 *xyzq_s, const int *counts, long long *force, int stride,
-                  long long *energy, bool calc_energy, bool fp64, cudaStream_t s) {
+                  long long *energy, bool calc_energy, bool fp64, cudaStream_t s,
+                  long long *virial) {
   spread(xyzq_s, counts, s);
   forward(s);
-  convolve(energy, calc_energy, fp64, s);
+  convolve(energy, calc_energy, fp64, s, virial);
   backward(s);
   gather(xyzq_s, counts, force, stride, s);
 }

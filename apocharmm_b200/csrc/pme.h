@@ -53,12 +53,15 @@ class Pme {
              double Lz);
   // sorted coordinates in, fixed-point gradients added to `force` (sorted
   // slot order, SoA with `stride`); ewks energy added to energy[kEEwks]
+  // virial (non-null): also add the reciprocal virial (3x3, 2^32 fixed point)
   void compute(const float4 *xyzq_s, const int *counts, long long *force, int stride,
-               long long *energy, bool calc_energy, bool fp64_influence, cudaStream_t s);
+               long long *energy, bool calc_energy, bool fp64_influence, cudaStream_t s,
+               long long *virial = nullptr);
   // the individual stages (exposed for tests and profiling)
   void spread(const float4 *xyzq_s, const int *counts, cudaStream_t s);
   void forward(cudaStream_t s);
-  void convolve(long long *energy, bool calc_energy, bool fp64_influence, cudaStream_t s);
+  void convolve(long long *energy, bool calc_energy, bool fp64_influence, cudaStream_t s,
+                long long *virial = nullptr);
   void backward(cudaStream_t s);
   void gather(const float4 *xyzq_s, const int *counts, long long *force, int stride,
               cudaStream_t s);

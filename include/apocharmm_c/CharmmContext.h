@@ -38,6 +38,10 @@ APOCHARMM_C_API apo_status apo_charmm_context_compute_temperature(double *temper
 APOCHARMM_C_API apo_status apo_charmm_context_calculate_forces(apo_charmm_context *context, const bool reset_list, const bool calc_energy, const bool calc_virial);
 APOCHARMM_C_API apo_status apo_charmm_context_get_forces(double *xyz, const size_t len, apo_charmm_context *context);
 APOCHARMM_C_API apo_status apo_charmm_context_get_energy_components(double *energies, const size_t len, apo_charmm_context *context);
+/* addition: ForceManager::getVirial (src/ForceManager.cu:393-415) -- the 3x3
+ * internal virial (row major, kcal/mol) of the last calculate_forces made
+ * with calc_virial (or of calculate_potential_energy); len >= 9 */
+APOCHARMM_C_API apo_status apo_charmm_context_get_virial(double *virial, const size_t len, apo_charmm_context *context);
 APOCHARMM_C_API apo_status apo_charmm_context_get_potential_energy(double *energy, apo_charmm_context *context);
 APOCHARMM_C_API apo_status apo_charmm_context_set_coordinates_xyz(apo_charmm_context *context, const double *xyz, const size_t len);
 APOCHARMM_C_API apo_status apo_charmm_context_get_coordinates(double *xyz, const size_t len, apo_charmm_context *context);

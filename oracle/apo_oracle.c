@@ -139,7 +139,7 @@ int or_direct(int n, const double *xyz, const double *q, const int *type,
               int ntype, const double *c6c12, const int *excl_ptr,
               const int *excl_idx, const double *box, double kappa,
               double roff, double ron, double *grad, double *e_elec,
-              double *e_vdw, int nthreads) {
+              double *e_vdw, double *vir9, int nthreads) {
   nb_setup s;
   nb_setup_init(&s, kappa, roff, ron);
   set_threads(nthreads);
@@ -170,7 +170,8 @@ int or_direct(int n, const double *xyz, const double *q, const int *type,
     head[cellof[i]] = i;
   }
   double ee = 0.0, ev = 0.0;
-#pragma omp parallel for schedule(dynamic, 64) reduction(+ : ee, ev)
+  double w0 = 0, w1 = 0, w2 = 0, w3 = 0, w4 = 0, w5 = 0, w6 = 0, w7 = 0, w8 = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : ee, ev, w0, w1, w2, w3, w4, w5, w6, w7, w8)
   for (int i = 0; i < n; i++) {
     int c = cellof[i];
     int cx = c % nc[0], cy = (c / nc[0]) % nc[1], cz = c / (nc[0] * nc[1]);
@@ -206,6 +207,11 @@ int or_direct(int n, const double *xyz, const double *q, const int *type,
             gx += f * d[0];
             gy += f * d[1];
             gz += f * d[2];
+            /* virial -sum over pairs of d (x) gradient_i; pairs visited twice */
+            double h = -0.5 * f;
+            w0 += h * d[0] * d[0]; w1 += h * d[0] * d[1]; w2 += h * d[0] * d[2];
+            w3 += h * d[1] * d[0]; w4 += h * d[1] * d[1]; w5 += h * d[1] * d[2];
+            w6 += h * d[2] * d[0]; w7 += h * d[2] * d[1]; w8 += h * d[2] * d[2];
           }
         }
     grad[3 * i + 0] += gx;
@@ -217,6 +223,11 @@ int or_direct(int n, const double *xyz, const double *q, const int *type,
   free(cellof);
   *e_elec = ee;
   *e_vdw = ev;
+  if (vir9) {
+    vir9[0] += w0; vir9[1] += w1; vir9[2] += w2;
+    vir9[3] += w3; vir9[4] += w4; vir9[5] += w5;
+    vir9[6] += w6; vir9[7] += w7; vir9[8] += w8;
+  }
   return 0;
 }
 

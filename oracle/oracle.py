@@ -228,11 +228,21 @@ class Oracle:
         self.q = np.ascontiguousarray(sys.charge, np.float64)
         self.box = np.array(sys.box, np.float64)
 
-    def evaluate(self, pos=None, nthreads: int = 0, parts=("bonded", "direct", "14", "recip", "self")):
+    def evaluate(self, pos=None, nthreads: int = 0, parts=("bonded", "direct", "14", "recip", "self"),
+                 virial: bool = False):
+        """Energies (dict) and gradient (n, 3); with virial=True also the
+        3x3 internal virial W = -sum over interactions of r (x) dU/dr, in
+        the reference's convention (src/CudaEnergyVirial.cu:91-200 for the
+        direct part, src/CudaPMERecip.cu:674-929 for the reciprocal part).
+        Bonded and 1-4 terms use raw coordinate differences (whole
+        molecules), so their virial is -sum_i x_i (x) g_i of their own
+        gradient; the direct part sums -d (x) g over minimum-image pairs."""
         L = lib()
         xyz = np.ascontiguousarray(self.sys.pos if pos is None else pos, np.float64).reshape(-1)
         n = self.n
-        grad = np.zeros(3 * n)
+        grad_all = np.zeros(3 * n)
+        vir = np.zeros(9)
+        grad = np.zeros(3 * n) if virial else grad_all
         E = dict(bond=0.0, angle=0.0, ureyb=0.0, dihe=0.0, imdihe=0.0,
                  ewks=0.0, ewse=0.0, ewex=0.0, elec=0.0, vdw=0.0)
         bt = self.bt
@@ -254,6 +264,11 @@ class Oracle:
             E["imdihe"] = L.or_dihedrals(ctypes.c_int(len(imp)), _p(imp), _p(bt["iptr"]),
                                          _p(bt["ik"]), _p(bt["in_n"]), _p(bt["idl"]),
                                          ctypes.c_int(1), _p(xyz), _p(grad))
+        if virial:
+            x3 = xyz.reshape(n, 3)
+            vir -= np.einsum("ia,ib->ab", x3, grad.reshape(n, 3)).reshape(-1)
+            grad_all += grad
+            grad = np.zeros(3 * n)
         ee, ev, ex = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         if "direct" in parts:
             tab = np.ascontiguousarray(self.tab)
@@ -261,9 +276,12 @@ class Oracle:
                         ctypes.c_int(len(self.types)), _p(tab), _p(self.eptr), _p(self.eidx),
                         _p(self.box), ctypes.c_double(self.kappa), ctypes.c_double(self.roff),
                         ctypes.c_double(self.ron), _p(grad), ctypes.byref(ee), ctypes.byref(ev),
-                        ctypes.c_int(nthreads))
+                        _p(vir) if virial else None, ctypes.c_int(nthreads))
             E["elec"] += ee.value
             E["vdw"] += ev.value
+            if virial:
+                grad_all += grad
+                grad = np.zeros(3 * n)
         if "14" in parts:
             in14 = np.ascontiguousarray(self.in14, np.int32)
             ex14 = np.ascontiguousarray(self.ex14, np.int32)
@@ -276,19 +294,29 @@ class Oracle:
             E["elec"] += ee.value
             E["vdw"] += ev.value
             E["ewex"] += ex.value
+            if virial:
+                vir -= np.einsum("ia,ib->ab", xyz.reshape(n, 3), grad.reshape(n, 3)).reshape(-1)
+                grad_all += grad
+                grad = np.zeros(3 * n)
         if "recip" in parts:
             ek = ctypes.c_double()
-            vir = np.zeros(6)
+            v6 = np.zeros(6)
             nx, ny, nz = self.nfft
             L.or_pme(ctypes.c_int(n), _p(xyz), _p(self.q), _p(self.box),
                      ctypes.c_double(self.kappa), ctypes.c_int(nx), ctypes.c_int(ny),
                      ctypes.c_int(nz), ctypes.c_int(self.order), _p(grad), ctypes.byref(ek),
-                     _p(vir), ctypes.c_int(nthreads))
+                     _p(v6), ctypes.c_int(nthreads))
             E["ewks"] = ek.value
+            if virial:
+                vir += v6[[0, 1, 2, 1, 3, 4, 2, 4, 5]]
+                grad_all += grad
+                grad = np.zeros(3 * n)
         if "self" in parts:
             E["ewse"] = L.or_self_energy(ctypes.c_int(n), _p(self.q), ctypes.c_double(self.kappa))
         E["epot"] = sum(v for k, v in E.items())
-        return E, grad.reshape(n, 3)
+        if virial:
+            return E, grad_all.reshape(n, 3), vir.reshape(3, 3)
+        return E, grad_all.reshape(n, 3)
 
     def ewald_recip_exact(self, pos=None, kmax=None, nthreads: int = 0):
         """Exact Ewald k-space sum (no mesh), for the PME error statement."""

@@ -70,3 +70,16 @@ def test_topology_lists_water():
     s, o = _oracle("waterDimer")
     assert o.in14.shape[0] == 0
     assert o.ex14.tolist() == [[0, 1], [0, 2], [1, 2], [3, 4], [3, 5], [4, 5]]
+
+
+@pytest.mark.parametrize("name,abs_tol", [("waterbox", 1e-3), ("waterDimer", 1e-8),
+                                          ("argon10", 1e-8)])
+def test_virial_matches_charmm(name, abs_tol):
+    """Internal virial (CHARMM c47b1 values asserted by the reference's
+    unittest-eneForces.cpp) from the oracle's pair, bonded and PME parts."""
+    s, o = _oracle(name)
+    E, grad, vir = o.evaluate(virial=True)
+    ref = np.array(golden()[name]["virial"]).reshape(3, 3)
+    # the reference test's own tolerance: 1e-4 relative to vir[0] (waterbox), 1e-4 / 1e-6 abs
+    assert np.abs(vir - ref).max() <= max(1e-4 * abs(ref[0, 0]), 1e-6)
+    assert np.abs(vir - ref).max() <= abs_tol

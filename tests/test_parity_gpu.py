@@ -103,3 +103,21 @@ def test_forces_are_deterministic(tmp_path):
     f2, e2 = ctx.getForces(), ctx.getEnergyComponents()
     assert np.array_equal(f1, f2)
     assert e1 == e2
+
+
+@pytest.mark.parametrize("name", ["waterDimer", "argon10"])
+def test_small_golden_cases(tmp_path, name):
+    """The reference's waterDimer (unittest-eneForces.cpp:110-206) and argon10
+    (:208-286) known answers through the GPU path."""
+    s = load_case(name)
+    keep, E, F = _run(s, tmp_path)
+    g = golden()[name]
+    if name == "waterDimer":
+        for k, v in g["energy"].items():
+            val = sum(E.values()) if k == "epot" else E[k]
+            assert abs(val - v) <= g["energy_margin"], k
+        ref = reference_forces(name)
+    else:
+        assert sum(E.values()) == pytest.approx(g["energy"]["epot"], abs=1e-5)
+        ref = np.array(g["forces"])
+    assert np.abs(F - ref).max() < g["force_tol"]
