@@ -505,13 +505,15 @@ extern "C" apo_status apo_charmm_context_get_neighbor_pairs(int *pairs, const si
     nl.sync_counts(s);
     const int S = nl.h_counts[0], T = nl.h_counts[1];
     std::vector<int> perm(S);
-    std::vector<float4> xs(S);
+    std::vector<float4> xs(S), origin((S + 31) / 32);
     std::vector<int2> tiles(T);
     std::vector<unsigned> masks((size_t)T * 32);
     std::vector<int4> work(nl.h_counts[2]);
     if (S) {
       APO_CUDA(cudaMemcpy(perm.data(), nl.perm, S * sizeof(int), cudaMemcpyDeviceToHost));
       APO_CUDA(cudaMemcpy(xs.data(), nl.xyzq_s, S * sizeof(float4), cudaMemcpyDeviceToHost));
+      APO_CUDA(cudaMemcpy(origin.data(), nl.cl_origin, origin.size() * sizeof(float4),
+                          cudaMemcpyDeviceToHost));
     }
     if (T) {
       APO_CUDA(cudaMemcpy(tiles.data(), nl.tiles, T * sizeof(int2), cudaMemcpyDeviceToHost));
@@ -533,8 +535,11 @@ extern "C" apo_status apo_charmm_context_get_neighbor_pairs(int *pairs, const si
           for (int j = 0; j < 32; ++j) {
             if ((m >> j) & 1u) continue;
             const int sj = jc * 32 + j;
-            const double dx = xs[si].x - (xs[sj].x + sx), dy = xs[si].y - (xs[sj].y + sy),
-                         dz = xs[si].z - (xs[sj].z + sz);
+            // sorted coordinates are relative to their cluster's origin
+            const float4 oi = origin[w.x], oj = origin[jc];
+            const double dx = ((double)xs[si].x + oi.x) - ((double)xs[sj].x + oj.x + sx),
+                         dy = ((double)xs[si].y + oi.y) - ((double)xs[sj].y + oj.y + sy),
+                         dz = ((double)xs[si].z + oi.z) - ((double)xs[sj].z + oj.z + sz);
             if (dx * dx + dy * dy + dz * dz >= r2max) continue;
             if (pairs && 3 * (count + 1) <= len) {
               pairs[3 * count] = perm[si];

@@ -177,7 +177,7 @@ void ForceManager::initialize() {
   m_HostSetup = make_nb_setup(m_Box[0], m_Box[1], m_Box[2], m_Kappa, m_Ctofnb, m_Ctonnb);
   m_Setup.upload(std::vector<NbSetup>{m_HostSetup});
 
-  m_Nbl.setup(n, (float)m_Box[0], (float)m_Box[1], (float)m_Box[2], (float)m_Cutoff,
+  m_Nbl.setup(n, m_Box[0], m_Box[1], m_Box[2], (float)m_Cutoff,
               m_Top.excl_ptr, m_Top.excl_idx, m_VdwTypeD.p, m_TilesPerWork);
   m_Pme.setup(m_Nfft[0], m_Nfft[1], m_Nfft[2], m_Order, m_Kappa, m_Box[0], m_Box[1], m_Box[2]);
   m_Pme.max_slots = m_Nbl.dims().slot_cap;
@@ -218,7 +218,7 @@ void ForceManager::calcForce(const float4 *d_xyzq, bool calcEnergy, bool calcVir
                              cudaStream_t s, bool clear) {
   if (!m_Initialized) throw std::runtime_error("ForceManager is not initialized");
   if (!m_ListBuilt) resetNeighborList(d_xyzq, s);
-  else if (clear) m_Nbl.refresh(d_xyzq, s);
+  else if (clear) m_Nbl.refresh(s);
   if (clear) APO_CUDA(cudaMemsetAsync(m_Force.p, 0, (size_t)3 * m_Stride * sizeof(long long), s));
   if (calcVirial) calcEnergy = true;
   long long *virial = calcVirial ? m_Energy.p + kNumEnergyTerms : nullptr;
@@ -230,6 +230,7 @@ void ForceManager::calcForce(const float4 *d_xyzq, bool calcEnergy, bool calcVir
     APO_CUDA(cudaStreamWaitEvent(m_SNb, m_EvFork, 0));
     NbArgs a;
     a.xyzq_s = m_Nbl.xyzq_s;
+    a.origin = m_Nbl.cl_origin;
     a.perm = m_Nbl.perm;
     a.type_s = m_Nbl.type_s;
     a.tiles = m_Nbl.tiles;
@@ -275,7 +276,7 @@ void ForceManager::calcForce(const float4 *d_xyzq, bool calcEnergy, bool calcVir
   if (m_ComponentMask & 4) {
     APO_CUDA(cudaStreamWaitEvent(m_SPme, m_EvFork, 0));
     m_Pme.compute(m_Nbl.xyzq_s, m_Nbl.counts, m_Force.p, m_Stride, m_Energy.p, calcEnergy,
-                  m_Precise, m_SPme, virial);
+                  m_Precise, m_SPme, virial, m_Nbl.cl_origin);
     APO_CUDA(cudaEventRecord(m_EvPme, m_SPme));
     APO_CUDA(cudaStreamWaitEvent(s, m_EvPme, 0));
   }

@@ -107,7 +107,10 @@ class ForceManager {
                  bool clear = true);
   // FP64 state coordinates (x, y, z, q) in atom order, read by the bonded
   // terms; set by the CharmmContext that owns them
-  void setStateCoordinates(const double4 *c) { m_StateCoords = c; }
+  void setStateCoordinates(const double4 *c) {
+    m_StateCoords = c;
+    m_Nbl.set_state_coordinates(c);
+  }
 
   std::map<std::string, double> getEnergyComponents(cudaStream_t s);
   double getPotentialEnergy(cudaStream_t s);

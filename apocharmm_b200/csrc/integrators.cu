@@ -153,16 +153,17 @@ __device__ __forceinline__ d3 take_grad(long long *f, int stride, int slot) {
             (double)gz * kInvForceScale);
 }
 
+// new FP64 position -> state, atom-order floats, and the sorted
+// cluster-local floats (position + image shift - cluster origin, in FP64)
 __device__ __forceinline__ void store_position(int a, d3 x, double4 *coords, float4 *xyzq,
-                                               const int *glo2loc, const float4 *slot_shift,
+                                               const int *glo2loc, const double4 *slot_off,
                                                float4 *xyzq_s) {
   const double q = coords[a].w;
   coords[a] = make_double4(x.x, x.y, x.z, q);
-  const float4 f = make_float4((float)x.x, (float)x.y, (float)x.z, (float)q);
-  xyzq[a] = f;
+  xyzq[a] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)q);
   const int s = glo2loc[a];
-  const float4 sh = slot_shift[s];
-  xyzq_s[s] = make_float4(f.x + sh.x, f.y + sh.y, f.z + sh.z, f.w);
+  const double4 o = slot_off[s];
+  xyzq_s[s] = make_float4((float)(x.x + o.x), (float)(x.y + o.y), (float)(x.z + o.z), (float)q);
 }
 
 // block-wide sum of two doubles; thread 0 writes partials[2*block + k]
@@ -221,7 +222,7 @@ struct Common {
   long long *force;
   int stride;
   const int *glo2loc;
-  const float4 *slot_shift;
+  const double4 *slot_off;
   float4 *xyzq_s;
   Scalars *sc;
   double *partials;
@@ -296,7 +297,7 @@ __global__ void __launch_bounds__(kThreads) langevin_kernel(Common c, double gam
       ke1 += kon;
       c.vel[a] = make_double4(v.x, v.y, v.z, c.vel[a].w);
       c.dprev[a] = make_double4(d.x, d.y, d.z, 0.0);
-      store_position(a, n[k], c.coords, c.xyzq, c.glo2loc, c.slot_shift, c.xyzq_s);
+      store_position(a, n[k], c.coords, c.xyzq, c.glo2loc, c.slot_off, c.xyzq_s);
     }
   }
   block_partials(ke0, ke1, c.partials);
@@ -431,7 +432,7 @@ __global__ void __launch_bounds__(kThreads) nh_final_kernel(Common c, double ke_
       ke1 += kon;
       c.vel[a] = make_double4(v.x, v.y, v.z, c.vel[a].w);
       c.dprev[a] = make_double4(d.x, d.y, d.z, 0.0);
-      store_position(a, n[k], c.coords, c.xyzq, c.glo2loc, c.slot_shift, c.xyzq_s);
+      store_position(a, n[k], c.coords, c.xyzq, c.glo2loc, c.slot_off, c.xyzq_s);
     }
   }
   block_partials(ke0, ke1, c.partials);
@@ -460,7 +461,7 @@ __global__ void leapfrog_kernel(Common c, int natom) {
     const d3 nv = xyz(v) - (c.dt * v.w) * gr;
     c.vel[a] = make_double4(nv.x, nv.y, nv.z, v.w);
     const d3 x = xyz(c.coords[a]) + c.dt * nv;
-    store_position(a, x, c.coords, c.xyzq, c.glo2loc, c.slot_shift, c.xyzq_s);
+    store_position(a, x, c.coords, c.xyzq, c.glo2loc, c.slot_off, c.xyzq_s);
     ke1 = 0.5 * dot(nv, nv) / v.w;
   }
   block_partials(ke1, ke1, c.partials);
@@ -510,7 +511,7 @@ __global__ void init_constrain_kernel(Common c, int mode) {
   for (int k = 0; k < m; ++k) {
     const int a = at[k];
     if (mode == 0) {
-      store_position(a, n[k], c.coords, c.xyzq, c.glo2loc, c.slot_shift, c.xyzq_s);
+      store_position(a, n[k], c.coords, c.xyzq, c.glo2loc, c.slot_off, c.xyzq_s);
     } else {
       const d3 d = o[k] - n[k];
       c.dprev[a] = make_double4(d.x, d.y, d.z, 0.0);
@@ -705,7 +706,7 @@ void CudaIntegrator::buildGroups() {
   c.force = fm->forceFixed();
   c.stride = fm->forceStride();
   c.glo2loc = fm->neighborList().glo2loc;
-  c.slot_shift = fm->neighborList().slot_shift;
+  c.slot_off = fm->neighborList().slot_off;
   c.xyzq_s = fm->neighborList().xyzq_s;
   c.sc = S.sc.p;
   c.partials = S.partials.p;

@@ -175,23 +175,66 @@ __global__ void col_sort_kernel(int ncol, const int *__restrict__ col_count,
   }
 }
 
-// sorted, wrapped coordinates (runs after every coordinate update)
-__global__ void refresh_kernel(const float4 *__restrict__ xyzq, const int *__restrict__ perm,
-                               const float4 *__restrict__ slot_shift,
+// (4b) cluster origins, one warp per cluster: the centre of the wrapped
+// positions rounded to a multiple of 1/64 A (exact in single precision for
+// any box below 2^17 A), and per slot the FP64 offset image shift - origin
+__global__ void origin_kernel(const float4 *__restrict__ xyzq, const int *__restrict__ perm,
+                              const float4 *__restrict__ slot_shift, NbListDims d,
+                              float4 *__restrict__ cl_origin, double4 *__restrict__ slot_off,
+                              const int *__restrict__ counts) {
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= counts[0] / kTile) return;
+  const int s = w * kTile + lane;
+  const int g = perm[s];
+  float4 p = make_float4(0.f, 0.f, 0.f, 0.f), sh = slot_shift[s];
+  if (g >= 0) p = xyzq[g];
+  const bool valid = g >= 0;
+  float mnx = valid ? p.x + sh.x : INFINITY, mny = valid ? p.y + sh.y : INFINITY,
+        mnz = valid ? p.z + sh.z : INFINITY;
+  float mxx = valid ? p.x + sh.x : -INFINITY, mxy = valid ? p.y + sh.y : -INFINITY,
+        mxz = valid ? p.z + sh.z : -INFINITY;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    mnx = fminf(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
+    mny = fminf(mny, __shfl_xor_sync(0xffffffffu, mny, o));
+    mnz = fminf(mnz, __shfl_xor_sync(0xffffffffu, mnz, o));
+    mxx = fmaxf(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
+    mxy = fmaxf(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
+    mxz = fmaxf(mxz, __shfl_xor_sync(0xffffffffu, mxz, o));
+  }
+  float ox = 0.f, oy = 0.f, oz = 0.f;
+  if (mnx <= mxx) {  // at least one atom
+    ox = rintf(0.5f * (mnx + mxx) * 64.f) * (1.f / 64.f);
+    oy = rintf(0.5f * (mny + mxy) * 64.f) * (1.f / 64.f);
+    oz = rintf(0.5f * (mnz + mxz) * 64.f) * (1.f / 64.f);
+  }
+  if (lane == 0) cl_origin[w] = make_float4(ox, oy, oz, 0.f);
+  // the wrap shift is k * L with a small integer k
+  const double kx = rint((double)sh.x / (double)d.Lx), ky = rint((double)sh.y / (double)d.Ly),
+               kz = rint((double)sh.z / (double)d.Lz);
+  slot_off[s] = make_double4(kx * d.Lxd - (double)ox, ky * d.Lyd - (double)oy,
+                             kz * d.Lzd - (double)oz, 0.0);
+}
+
+// sorted, cluster-local coordinates (runs after every coordinate update)
+__global__ void refresh_kernel(const double4 *__restrict__ coords, const int *__restrict__ perm,
+                               const double4 *__restrict__ slot_off,
                                float4 *__restrict__ xyzq_s, const int *__restrict__ counts) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= counts[0]) return;
   int g = perm[s];
   float4 out = make_float4(0.f, 0.f, 0.f, 0.f);
   if (g >= 0) {
-    float4 p = xyzq[g], sh = slot_shift[s];
-    out = make_float4(p.x + sh.x, p.y + sh.y, p.z + sh.z, p.w);
+    const double4 c = coords[g], o = slot_off[s];
+    out = make_float4((float)(c.x + o.x), (float)(c.y + o.y), (float)(c.z + o.z), (float)c.w);
   }
   xyzq_s[s] = out;
 }
 
 // (5) cluster bounding boxes, one warp per cluster
 __global__ void bbox_kernel(const float4 *__restrict__ xyzq_s, const int *__restrict__ perm,
+                            const float4 *__restrict__ cl_origin,
                             float4 *__restrict__ bb_c, float4 *__restrict__ bb_h,
                             const int *__restrict__ counts) {
   int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -214,7 +257,9 @@ __global__ void bbox_kernel(const float4 *__restrict__ xyzq_s, const int *__rest
     mxz = fmaxf(mxz, __shfl_xor_sync(0xffffffffu, mxz, o));
   }
   if (lane == 0) {
-    bb_c[w] = make_float4(0.5f * (mnx + mxx), 0.5f * (mny + mxy), 0.5f * (mnz + mxz), 0.f);
+    const float4 o = cl_origin[w];
+    bb_c[w] = make_float4(0.5f * (mnx + mxx) + o.x, 0.5f * (mny + mxy) + o.y,
+                          0.5f * (mnz + mxz) + o.z, 0.f);
     bb_h[w] = make_float4(0.5f * (mxx - mnx), 0.5f * (mxy - mny), 0.5f * (mxz - mnz), 0.f);
   }
 }
@@ -377,6 +422,7 @@ NeighborList::~NeighborList() { release(); }
 
 void NeighborList::release() {
   dfree(perm); dfree(glo2loc); dfree(slot_shift); dfree(xyzq_s); dfree(type_s);
+  dfree(slot_off); dfree(cl_origin);
   dfree(tiles); dfree(masks); dfree(work); dfree(counts); dfree(error);
   dfree(m_excl_ptr); dfree(m_excl_idx); dfree(m_col_count); dfree(m_col_start);
   dfree(m_atom_col); dfree(m_atom_rank); dfree(m_atom_shift); dfree(m_atom_z); dfree(m_tmp_key);
@@ -384,14 +430,19 @@ void NeighborList::release() {
   dfree(m_tile_count); dfree(m_tile_start); dfree(m_work_start);
 }
 
-void NeighborList::setup(int natom, float Lx, float Ly, float Lz, float rlist,
+void NeighborList::setup(int natom, double Lx, double Ly, double Lz, float rlist,
                          const std::vector<int> &excl_ptr, const std::vector<int> &excl_idx,
                          const int *d_vdwtype, int tiles_per_work) {
   if (natom <= 0) throw std::invalid_argument("NeighborList: no atoms");
+  if (!(Lx > 0.0 && Ly > 0.0 && Lz > 0.0) || Lx > 65536.0 || Ly > 65536.0 || Lz > 65536.0)
+    throw std::invalid_argument("NeighborList: box lengths must be in (0, 65536] A");
   m_d.natom = natom;
-  m_d.Lx = Lx;
-  m_d.Ly = Ly;
-  m_d.Lz = Lz;
+  m_d.Lx = (float)Lx;
+  m_d.Ly = (float)Ly;
+  m_d.Lz = (float)Lz;
+  m_d.Lxd = Lx;
+  m_d.Lyd = Ly;
+  m_d.Lzd = Lz;
   m_d.rlist = rlist;
   m_d.tiles_per_work = tiles_per_work;
   m_vdwtype = d_vdwtype;
@@ -434,6 +485,9 @@ void NeighborList::setup(int natom, float Lx, float Ly, float Lz, float rlist,
 void NeighborList::alloc() {
   const int n = m_d.natom, S = m_d.slot_cap, ncl = S / kTile;
   dalloc(perm, S); dalloc(glo2loc, n); dalloc(slot_shift, S); dalloc(xyzq_s, S);
+  dalloc(slot_off, S); dalloc(cl_origin, ncl);
+  APO_CUDA(cudaMemset(slot_off, 0, (size_t)S * sizeof(double4)));
+  APO_CUDA(cudaMemset(cl_origin, 0, (size_t)ncl * sizeof(float4)));
   dalloc(type_s, S); dalloc(tiles, m_d.tile_cap); dalloc(masks, (size_t)m_d.tile_cap * kTile);
   dalloc(work, m_d.work_cap); dalloc(counts, 8); dalloc(error, 1);
   dalloc(m_col_count, m_ncol); dalloc(m_col_start, m_ncol + 1); dalloc(m_atom_col, n);
@@ -467,8 +521,12 @@ void NeighborList::build(const float4 *d_xyzq, cudaStream_t s) {
                                           m_tmp_idx, m_atom_shift, m_vdwtype, perm, glo2loc,
                                           slot_shift, type_s, m_cl_col, counts, m_d.sort_cap);
   APO_LAUNCH_CHECK();
-  refresh(d_xyzq, s);
-  bbox_kernel<<<(ncl * 32 + 255) / 256, 256, 0, s>>>(xyzq_s, perm, m_bb_c, m_bb_h, counts);
+  origin_kernel<<<(ncl * 32 + 255) / 256, 256, 0, s>>>(d_xyzq, perm, slot_shift, m_d, cl_origin,
+                                                        slot_off, counts);
+  APO_LAUNCH_CHECK();
+  refresh(s);
+  bbox_kernel<<<(ncl * 32 + 255) / 256, 256, 0, s>>>(xyzq_s, perm, cl_origin, m_bb_c, m_bb_h,
+                                                      counts);
   APO_LAUNCH_CHECK();
   tiles_kernel<false><<<(ncl * 32 + 127) / 128, 128, 0, s>>>(
       m_d, m_cl_col, m_col_start, m_bb_c, m_bb_h, perm, glo2loc, m_excl_ptr, m_excl_idx,
@@ -484,8 +542,9 @@ void NeighborList::build(const float4 *d_xyzq, cudaStream_t s) {
   APO_LAUNCH_CHECK();
 }
 
-void NeighborList::refresh(const float4 *d_xyzq, cudaStream_t s) {
-  refresh_kernel<<<(m_d.slot_cap + 255) / 256, 256, 0, s>>>(d_xyzq, perm, slot_shift, xyzq_s,
+void NeighborList::refresh(cudaStream_t s) {
+  if (!m_coords) throw std::runtime_error("NeighborList: no state coordinates attached");
+  refresh_kernel<<<(m_d.slot_cap + 255) / 256, 256, 0, s>>>(m_coords, perm, slot_off, xyzq_s,
                                                              counts);
   APO_LAUNCH_CHECK();
 }

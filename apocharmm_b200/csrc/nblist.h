@@ -24,6 +24,7 @@ struct NbListDims {
   int natom = 0;
   int ncx = 1, ncy = 1;           // cell columns in x, y
   float Lx = 0, Ly = 0, Lz = 0;   // box
+  double Lxd = 0, Lyd = 0, Lzd = 0;  // box, full precision
   float rlist = 0;                // list radius (cutnb)
   int slot_cap = 0;               // padded sorted slots
   int tile_cap = 0, work_cap = 0;
@@ -39,13 +40,16 @@ class NeighborList {
   NeighborList &operator=(const NeighborList &) = delete;
 
   // topology-dependent set-up; box/rlist may be changed with set_box
-  void setup(int natom, float Lx, float Ly, float Lz, float rlist,
+  void setup(int natom, double Lx, double Ly, double Lz, float rlist,
              const std::vector<int> &excl_ptr, const std::vector<int> &excl_idx,
              const int *d_vdwtype, int tiles_per_work = 8);
   // full rebuild from global-order coordinates (device float4 x,y,z,q)
   void build(const float4 *d_xyzq, cudaStream_t s);
-  // refresh sorted coordinates from global-order coordinates
-  void refresh(const float4 *d_xyzq, cudaStream_t s);
+  // refresh the sorted, cluster-local coordinates from the FP64 state
+  void refresh(cudaStream_t s);
+  // FP64 state coordinates (atom order, x y z q) the sorted single-precision
+  // coordinates are formed from
+  void set_state_coordinates(const double4 *c) { m_coords = c; }
   // grow capacities if the last build used more than `fill` of them (sync)
   bool ensure_capacity(const float4 *d_xyzq, cudaStream_t s, double fill = 0.8);
 
@@ -56,7 +60,14 @@ class NeighborList {
   int *perm = nullptr;          // slot -> atom (-1 = padding)
   int *glo2loc = nullptr;       // atom -> slot
   float4 *slot_shift = nullptr; // image shift added to the atom's coordinates
-  float4 *xyzq_s = nullptr;     // sorted, wrapped coordinates + charge
+  // Sorted coordinates are stored relative to an origin per 32-atom cluster
+  // (a multiple of 1/64 A, exact in single precision): xyzq_s = FP64 state
+  // + slot_off, rounded once; the absolute wrapped position is xyzq_s +
+  // cl_origin[slot / 32].  Pair differences then carry the rounding of
+  // coordinates a few A from the origin instead of up to half a box.
+  double4 *slot_off = nullptr;  // image shift - cluster origin, FP64
+  float4 *cl_origin = nullptr;  // per cluster
+  float4 *xyzq_s = nullptr;     // sorted, cluster-local coordinates + charge
   int *type_s = nullptr;        // sorted LJ type
   int2 *tiles = nullptr;        // (j cluster, image code)
   unsigned *masks = nullptr;    // 32 words per tile
@@ -76,6 +87,7 @@ class NeighborList {
   int m_ncol = 0;
   int m_sys = 0;
   const int *m_vdwtype = nullptr;
+  const double4 *m_coords = nullptr;
   int *m_excl_ptr = nullptr, *m_excl_idx = nullptr;
   int *m_col_count = nullptr, *m_col_start = nullptr;
   int *m_atom_col = nullptr, *m_atom_rank = nullptr;

@@ -20,6 +20,9 @@ namespace apo {
 NbSetup make_nb_setup(double Lx, double Ly, double Lz, double kappa, double roff,
                       double ron) {
   NbSetup s;
+  s.Lxd = Lx;
+  s.Lyd = Ly;
+  s.Lzd = Lz;
   s.Lx = (float)Lx;
   s.Ly = (float)Ly;
   s.Lz = (float)Lz;
@@ -118,6 +121,7 @@ __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
   for (int w = blockIdx.x * kWarps + wib; w < nwork; w += gridDim.x * kWarps) {
     const int4 wk = a.work[w];
     const NbSetup st = a.setups[wk.w];
+    const float4 oi = a.origin[wk.x];
     const int islot = wk.x * kTile + lane;
     const float4 xi = a.xyzq_s[islot];
     const bool ivalid = a.perm[islot] >= 0;
@@ -142,8 +146,13 @@ __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
 
     for (int t = wk.y; t < wk.z; ++t) {
       const int2 tl = a.tiles[t];
-      float sx, sy, sz;
-      shift_code(tl.y, st.Lx, st.Ly, st.Lz, sx, sy, sz);
+      // j cluster frame -> i cluster frame: origin difference plus the
+      // periodic image, formed in FP64 and rounded once (|offset| < rlist + 2 cluster edges)
+      const float4 oj = a.origin[tl.x];
+      const int ic = tl.y / 9, ib = (tl.y - 9 * ic) / 3, ia = tl.y - 9 * ic - 3 * ib;
+      const float sx = (float)((double)oj.x - (double)oi.x + (double)(ia - 1) * st.Lxd);
+      const float sy = (float)((double)oj.y - (double)oi.y + (double)(ib - 1) * st.Lyd);
+      const float sz = (float)((double)oj.z - (double)oi.z + (double)(ic - 1) * st.Lzd);
       const int jslot = tl.x * kTile + lane;
       float4 xj = a.xyzq_s[jslot];
       xj.x += sx;

@@ -9,6 +9,7 @@
 namespace apo {
 
 struct NbSetup {
+  double Lxd, Lyd, Lzd;   // box, full precision (tile frame offsets)
   float Lx, Ly, Lz;
   float roff2, ron2;
   float kappa, kappa2, two_kappa_sqrtpi;
@@ -19,7 +20,8 @@ NbSetup make_nb_setup(double Lx, double Ly, double Lz, double kappa, double roff
                       double ron);
 
 struct NbArgs {
-  const float4 *xyzq_s;
+  const float4 *xyzq_s;   // cluster-local coordinates (NeighborList::xyzq_s)
+  const float4 *origin;   // per cluster origin (NeighborList::cl_origin)
   const int *perm;        // slot -> atom, -1 for padding
   const int *type_s;
   const int2 *tiles;

@@ -248,7 +248,8 @@ __device__ __forceinline__ int dig_unrev(int p, const FftAxis &a) {
 template <int ORDER>
 __global__ void __launch_bounds__(128) spread_kernel(const float4 *__restrict__ xyzq,
                                                      const int *__restrict__ counts, PmeDims d,
-                                                     int *__restrict__ qgrid) {
+                                                     int *__restrict__ qgrid,
+                                                     const float4 *__restrict__ origin) {
   constexpr int P3 = ORDER * ORDER * ORDER;
   __shared__ int sh_i[3][32];
   __shared__ float sh_q[32];
@@ -260,7 +261,13 @@ __global__ void __launch_bounds__(128) spread_kernel(const float4 *__restrict__ 
     const int s = s0 + threadIdx.x;
     float q = 0.f;
     if (s < nslot) {
-      const float4 p = xyzq[s];
+      float4 p = xyzq[s];
+      if (origin) {  // cluster-local coordinates: add the cluster's origin
+        const float4 o = origin[s >> 5];
+        p.x += o.x;
+        p.y += o.y;
+        p.z += o.z;
+      }
       q = p.w;
       float th[ORDER], dth[ORDER], w;
       int i0;
@@ -493,12 +500,21 @@ template <int ORDER>
 __global__ void __launch_bounds__(256) gather_kernel(const float4 *__restrict__ xyzq,
                                                      const int *__restrict__ counts, PmeDims d,
                                                      const float *__restrict__ phi,
-                                                     long long *__restrict__ force, int stride) {
+                                                     long long *__restrict__ force, int stride,
+                                                     const float4 *__restrict__ origin) {
   const int nslot = counts[0];
   const int s = blockIdx.x * 32 + (threadIdx.x >> 3);
   const int sub = threadIdx.x & 7;
   float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (s < nslot) p = xyzq[s];
+  if (s < nslot) {
+    p = xyzq[s];
+    if (origin) {  // cluster-local coordinates: add the cluster's origin
+      const float4 o = origin[s >> 5];
+      p.x += o.x;
+      p.y += o.y;
+      p.z += o.z;
+    }
+  }
   float thx[ORDER], thy[ORDER], thz[ORDER], dx[ORDER], dy[ORDER], dz[ORDER], w;
   int ix, iy, iz;
   anchor(p.x, 1.f / d.Lx, d.nx, ix, w);
@@ -700,12 +716,13 @@ void Pme::setup(int nx, int ny, int nz, int order, double kappa, double Lx, doub
   }
 }
 
-void Pme::spread(const float4 *xyzq_s, const int *counts, cudaStream_t s) {
+void Pme::spread(const float4 *xyzq_s, const int *counts, cudaStream_t s,
+                 const float4 *origin) {
   const int blocks = (max_slots + 31) / 32;
   switch (m_d.order) {
-    case 4: spread_kernel<4><<<blocks, 128, 0, s>>>(xyzq_s, counts, m_d, qgrid); break;
-    case 6: spread_kernel<6><<<blocks, 128, 0, s>>>(xyzq_s, counts, m_d, qgrid); break;
-    case 8: spread_kernel<8><<<blocks, 128, 0, s>>>(xyzq_s, counts, m_d, qgrid); break;
+    case 4: spread_kernel<4><<<blocks, 128, 0, s>>>(xyzq_s, counts, m_d, qgrid, origin); break;
+    case 6: spread_kernel<6><<<blocks, 128, 0, s>>>(xyzq_s, counts, m_d, qgrid, origin); break;
+    case 8: spread_kernel<8><<<blocks, 128, 0, s>>>(xyzq_s, counts, m_d, qgrid, origin); break;
   }
   APO_LAUNCH_CHECK();
 }
@@ -750,24 +767,24 @@ void Pme::backward(cudaStream_t s) {
 }
 
 void Pme::gather(const float4 *xyzq_s, const int *counts, long long *force, int stride,
-                 cudaStream_t s) {
+                 cudaStream_t s, const float4 *origin) {
   const int blocks = (max_slots + 31) / 32;
   switch (m_d.order) {
-    case 4: gather_kernel<4><<<blocks, 256, 0, s>>>(xyzq_s, counts, m_d, phi, force, stride); break;
-    case 6: gather_kernel<6><<<blocks, 256, 0, s>>>(xyzq_s, counts, m_d, phi, force, stride); break;
-    case 8: gather_kernel<8><<<blocks, 256, 0, s>>>(xyzq_s, counts, m_d, phi, force, stride); break;
+    case 4: gather_kernel<4><<<blocks, 256, 0, s>>>(xyzq_s, counts, m_d, phi, force, stride, origin); break;
+    case 6: gather_kernel<6><<<blocks, 256, 0, s>>>(xyzq_s, counts, m_d, phi, force, stride, origin); break;
+    case 8: gather_kernel<8><<<blocks, 256, 0, s>>>(xyzq_s, counts, m_d, phi, force, stride, origin); break;
   }
   APO_LAUNCH_CHECK();
 }
 
 void Pme::compute(const float4 *xyzq_s, const int *counts, long long *force, int stride,
                   long long *energy, bool calc_energy, bool fp64, cudaStream_t s,
-                  long long *virial) {
-  spread(xyzq_s, counts, s);
+                  long long *virial, const float4 *origin) {
+  spread(xyzq_s, counts, s, origin);
   forward(s);
   convolve(energy, calc_energy, fp64, s, virial);
   backward(s);
-  gather(xyzq_s, counts, force, stride, s);
+  gather(xyzq_s, counts, force, stride, s, origin);
 }
 
 }  // namespace apo
@@ -986,9 +1003,9 @@ void pme_reciprocal_static(const float4 *xyzq, int n, double Lx, double Ly, doub
   APO_LAUNCH_CHECK();
   const int blocks = (n + 31) / 32;
   switch (order) {
-    case 4: spread_kernel<4><<<blocks, 128, 0, s>>>(xyzq, counts, d, qgrid); break;
-    case 6: spread_kernel<6><<<blocks, 128, 0, s>>>(xyzq, counts, d, qgrid); break;
-    case 8: spread_kernel<8><<<blocks, 128, 0, s>>>(xyzq, counts, d, qgrid); break;
+    case 4: spread_kernel<4><<<blocks, 128, 0, s>>>(xyzq, counts, d, qgrid, nullptr); break;
+    case 6: spread_kernel<6><<<blocks, 128, 0, s>>>(xyzq, counts, d, qgrid, nullptr); break;
+    case 8: spread_kernel<8><<<blocks, 128, 0, s>>>(xyzq, counts, d, qgrid, nullptr); break;
   }
   APO_LAUNCH_CHECK();
   const size_t sm = (size_t)(ny / 2) * (nx + 2) * sizeof(float2);
@@ -1004,9 +1021,9 @@ void pme_reciprocal_static(const float4 *xyzq, int n, double Lx, double Ly, doub
   plane_inv_kernel<<<nz, kPlaneThreads, sm, s>>>(d, cgrid, phi, tw, tw + nx);
   APO_LAUNCH_CHECK();
   switch (order) {
-    case 4: gather_kernel<4><<<blocks, 256, 0, s>>>(xyzq, counts, d, phi, grad, stride); break;
-    case 6: gather_kernel<6><<<blocks, 256, 0, s>>>(xyzq, counts, d, phi, grad, stride); break;
-    case 8: gather_kernel<8><<<blocks, 256, 0, s>>>(xyzq, counts, d, phi, grad, stride); break;
+    case 4: gather_kernel<4><<<blocks, 256, 0, s>>>(xyzq, counts, d, phi, grad, stride, nullptr); break;
+    case 6: gather_kernel<6><<<blocks, 256, 0, s>>>(xyzq, counts, d, phi, grad, stride, nullptr); break;
+    case 8: gather_kernel<8><<<blocks, 256, 0, s>>>(xyzq, counts, d, phi, grad, stride, nullptr); break;
   }
   APO_LAUNCH_CHECK();
   if (energy) {

@@ -54,17 +54,20 @@ class Pme {
   // sorted coordinates in, fixed-point gradients added to `force` (sorted
   // slot order, SoA with `stride`); ewks energy added to energy[kEEwks]
   // virial (non-null): also add the reciprocal virial (3x3, 2^32 fixed point)
+  // origin (non-null): xyzq_s holds coordinates relative to a per-32-slot
+  // origin (NeighborList::cl_origin)
   void compute(const float4 *xyzq_s, const int *counts, long long *force, int stride,
                long long *energy, bool calc_energy, bool fp64_influence, cudaStream_t s,
-               long long *virial = nullptr);
+               long long *virial = nullptr, const float4 *origin = nullptr);
   // the individual stages (exposed for tests and profiling)
-  void spread(const float4 *xyzq_s, const int *counts, cudaStream_t s);
+  void spread(const float4 *xyzq_s, const int *counts, cudaStream_t s,
+              const float4 *origin = nullptr);
   void forward(cudaStream_t s);
   void convolve(long long *energy, bool calc_energy, bool fp64_influence, cudaStream_t s,
                 long long *virial = nullptr);
   void backward(cudaStream_t s);
   void gather(const float4 *xyzq_s, const int *counts, long long *force, int stride,
-              cudaStream_t s);
+              cudaStream_t s, const float4 *origin = nullptr);
 
   const PmeDims &dims() const { return m_d; }
   int *qgrid = nullptr;     // nz*ny*nx int32 fixed point (zeroed by plane_fwd)
