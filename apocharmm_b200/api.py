@@ -504,3 +504,150 @@ def water_indices(sys) -> np.ndarray:
     t = sys.atom_type
     return np.array([[i, i + 1, i + 2] for i in range(0, len(t) - 2)
                      if t[i] == "OT" and t[i + 1] == "HT" and t[i + 2] == "HT"], np.int64).reshape(-1, 3)
+
+
+class Batch(_Handle):
+    """Many independent systems advanced together (apo_batch_*): one launch
+    per stage of a step for all systems, one CUDA graph per list segment.
+    Each system keeps its own box, cutoffs, PME grid, LJ tables, velocity
+    seed and noise stream."""
+    _destroy = "apo_batch_destroy"
+
+    def __init__(self, spline_order: int = 4, tiles_per_work: int = 8, precise: bool = False):
+        super().__init__()
+        call("apo_batch_create", ctypes.byref(self._h), _i(spline_order), _i(tiles_per_work),
+             _i(int(precise)))
+        self._keep = []          # PSF/PRM handles must outlive the batch set-up
+        self._n = []
+
+    def addSystem(self, psf: "CharmmPsf", prm: "CharmmParameters", box, kappa: float,
+                  cutnb: float, ctonnb: float, ctofnb: float, nfft=(-1, -1, -1),
+                  seed: int = 1) -> int:
+        idx = _i()
+        call("apo_batch_add_system", self._h, psf.handle, prm.handle, _d(box[0]), _d(box[1]),
+             _d(box[2]), _d(kappa), _d(cutnb), _d(ctonnb), _d(ctofnb), _i(nfft[0]), _i(nfft[1]),
+             _i(nfft[2]), ctypes.c_ulonglong(seed), ctypes.byref(idx))
+        self._keep.append((psf, prm))
+        return idx.value
+
+    def initialize(self):
+        call("apo_batch_initialize", self._h)
+        n = _i()
+        call("apo_batch_get_num_systems", ctypes.byref(n), self._h)
+        self._n = [self.numAtoms(k) for k in range(n.value)]
+
+    def numSystems(self) -> int:
+        return len(self._n)
+
+    def numAtoms(self, system: int = -1) -> int:
+        v = _sz()
+        call("apo_batch_get_num_atoms", ctypes.byref(v), self._h, _i(system))
+        return int(v.value)
+
+    def setCoordinates(self, system: int, xyz):
+        a = np.ascontiguousarray(xyz, np.float64).reshape(-1)
+        call("apo_batch_set_coordinates", self._h, _i(system), _ptr(a), _sz(a.size))
+
+    def _count(self, system: int) -> int:
+        return sum(self._n) if system < 0 else self._n[system]
+
+    def getCoordinates(self, system: int) -> np.ndarray:
+        """system < 0: all systems' atoms, concatenated"""
+        a = np.zeros(3 * self._count(system))
+        call("apo_batch_get_coordinates", _ptr(a), _sz(a.size), self._h, _i(system))
+        return a.reshape(-1, 3)
+
+    def setVelocities(self, system: int, v):
+        a = np.ascontiguousarray(v, np.float64).reshape(-1)
+        call("apo_batch_set_velocities", self._h, _i(system), _ptr(a), _sz(a.size))
+
+    def getVelocities(self, system: int) -> np.ndarray:
+        a = np.zeros(3 * self._count(system))
+        call("apo_batch_get_velocities", _ptr(a), _sz(a.size), self._h, _i(system))
+        return a.reshape(-1, 3)
+
+    def assignVelocities(self, temperature: float):
+        call("apo_batch_assign_velocities", self._h, _d(temperature))
+
+    def setLangevin(self, dt_ps: float, friction: float, temperature: float, seed: int):
+        call("apo_batch_set_langevin", self._h, _d(dt_ps), _d(friction), _d(temperature),
+             ctypes.c_ulonglong(seed))
+
+    def propagate(self, steps: int):
+        call("apo_batch_propagate", self._h, _i(steps))
+
+    def calculateForces(self, energy: bool = True, virial: bool = False):
+        call("apo_batch_calculate_forces", self._h, _i(int(energy)), _i(int(virial)))
+
+    def getForces(self, system: int) -> np.ndarray:
+        a = np.zeros(3 * self._count(system))
+        call("apo_batch_get_forces", _ptr(a), _sz(a.size), self._h, _i(system))
+        return a.reshape(-1, 3)
+
+    def getEnergyComponents(self, system: int) -> Dict[str, float]:
+        a = np.zeros(len(ENERGY_TERMS))
+        call("apo_batch_get_energy_components", _ptr(a), _sz(a.size), self._h, _i(system))
+        return dict(zip(ENERGY_TERMS, a.tolist()))
+
+    def getTemperatures(self) -> np.ndarray:
+        a = np.zeros(len(self._n))
+        call("apo_batch_get_temperatures", _ptr(a), _sz(a.size), self._h)
+        return a
+
+    def autotune(self, steps: int = 20, candidates=None) -> int:
+        t = _i()
+        if candidates:
+            c = (ctypes.c_int * len(candidates))(*candidates)
+            call("apo_batch_autotune", ctypes.byref(t), self._h, _i(steps), c, _i(len(candidates)))
+        else:
+            call("apo_batch_autotune", ctypes.byref(t), self._h, _i(steps), None, _i(0))
+        return t.value
+
+    def getStream(self) -> int:
+        v = _vp()
+        call("apo_batch_get_stream", ctypes.byref(v), self._h)
+        return v.value or 0
+
+    def setComponentMask(self, mask: int):
+        call("apo_batch_set_component_mask", self._h, _i(mask))
+
+
+def batch_from_systems(systems, workdir: str, seeds=None, spline_order: int = 4,
+                       tiles_per_work: int = 8, precise: bool = False) -> "Batch":
+    """Writes every apocharmm_b200.systems.System as CHARMM files under
+    workdir, adds it to a new Batch with its own settings, initialises the
+    batch and loads the coordinates."""
+    from .systems import write_charmm_files
+    b = Batch(spline_order, tiles_per_work, precise)
+    for k, s in enumerate(systems):
+        paths = write_charmm_files(s, os.path.join(workdir, f"sys{k}"))
+        st = s.settings
+        b.addSystem(CharmmPsf(paths["psf"]), CharmmParameters(paths["prm"]), s.box, st["kappa"],
+                    st["cutnb"], st["ctonnb"], st["ctofnb"], st["nfft"],
+                    seed=(seeds[k] if seeds is not None else 1000 + k))
+    b.initialize()
+    b.setCoordinates(-1, np.concatenate([np.asarray(s.pos, np.float64) for s in systems]))
+    return b
+
+
+def relax_batch(b: "Batch", waters_per_system, iterations: int = 150, max_step: float = 0.03):
+    """relax() for every system of a batch at once: steepest descent with the
+    largest move per system `max_step`, then the TIP3 refit."""
+    n = b.numSystems()
+    off = np.concatenate([[0], np.cumsum(b._n)])
+    x = b.getCoordinates(-1)
+    for _ in range(iterations):
+        b.calculateForces(False, False)
+        g = b.getForces(-1)
+        for k in range(n):
+            gk = g[off[k]:off[k + 1]]
+            gmax = float(np.abs(gk).max())
+            if np.isfinite(gmax) and gmax > 0.0:
+                x[off[k]:off[k + 1]] -= (max_step / gmax) * gk
+        b.setCoordinates(-1, x)
+    for k in range(n):
+        w = waters_per_system[k]
+        if w is not None and len(w):
+            x[off[k]:off[k + 1]] = rigid_water_fit(x[off[k]:off[k + 1]], np.asarray(w))
+    b.setCoordinates(-1, x)
+    return [x[off[k]:off[k + 1]].copy() for k in range(n)]

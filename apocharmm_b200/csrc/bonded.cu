@@ -141,21 +141,22 @@ __device__ float dihedral_term(const BondedArgs &a, int4 t, int2 terms, float2 h
 
 // 1-4 inclusion (LJ14 with VFSW + qq erfc/r) or exclusion correction
 // (qq (erfc - 1)/r = -qq erf/r); src/CudaDirectForceKernels.cu:643-870
-template <bool INCL, bool VIR>
-__device__ void pair14_term(const BondedArgs &a, int2 p, float &e_el, float &e_vdw, float *w) {
+template <bool INCL, bool VIR, bool MULTI>
+__device__ void pair14_term(const BondedArgs &a, const NbSetup &st, int2 p, float &e_el,
+                            float &e_vdw, float *w) {
   const float3 d = diff(a, p.x, p.y);
   const float dx = d.x, dy = d.y, dz = d.z;
   const float r2 = dx * dx + dy * dy + dz * dz;
   const float rinv = rsqrtf(r2), r = r2 * rinv, rinv2 = rinv * rinv;
   const float qq = (float)kCcelec * (float)a.coords[p.x].w * (float)a.coords[p.y].w;
-  const NbSetup &st = a.nb;
   const float expv = __expf(-st.kappa2 * r2);
   float fr;
   if (INCL) {
     const float ev = qq * erfcf(st.kappa * r) * rinv;
     fr = -qq * st.two_kappa_sqrtpi * expv - ev;
     e_el = ev;
-    const float2 cc = a.vdw14[a.vdwtype[p.x] * a.ntype + a.vdwtype[p.y]];
+    const int T = MULTI ? st.ntype : a.ntype;
+    const float2 cc = a.vdw14[(MULTI ? st.vdw14_off : 0) + a.vdwtype[p.x] * T + a.vdwtype[p.y]];
     const float rinv3 = rinv * rinv2, rinv6 = rinv3 * rinv3;
     const bool sw = r2 > st.ron2;
     const float A6 = sw ? st.k6 : 1.f, B6 = sw ? st.roffinv3 : 0.f;
@@ -176,11 +177,11 @@ __device__ void pair14_term(const BondedArgs &a, int2 p, float &e_el, float &e_v
   if (VIR) vir_sub(w, dx, dy, dz, f * dx, f * dy, f * dz);
 }
 
-template <bool ENERGY, bool VIRIAL>
+template <bool ENERGY, bool VIRIAL, bool MULTI = false>
 __global__ void __launch_bounds__(kThreads) bonded_kernel(BondedArgs a) {
   __shared__ unsigned long long sh_e[kNumEnergyTerms];
   __shared__ unsigned long long sh_v[9];
-  if (ENERGY) {
+  if (ENERGY && !MULTI) {
     if (threadIdx.x < kNumEnergyTerms) sh_e[threadIdx.x] = 0ull;
     if (VIRIAL && threadIdx.x < 9) sh_v[threadIdx.x] = 0ull;
     __syncthreads();
@@ -212,12 +213,37 @@ __global__ void __launch_bounds__(kThreads) bonded_kernel(BondedArgs a) {
       e = dihedral_term<true, VIRIAL>(a, a.imp_ijkl[k], make_int2(0, 0), a.imp_p[k], w);
       slot = kEImdihe;
     } else if (t < b6) {
-      pair14_term<true, VIRIAL>(a, a.in14[t - b5], e, e2, w);
+      const int2 pr = a.in14[t - b5];
+      pair14_term<true, VIRIAL, MULTI>(a, MULTI ? a.setups[a.sys_of_atom[pr.x]] : a.nb, pr, e, e2,
+                                       w);
       slot = kEElec;
       slot2 = kEVdw;
     } else {
-      pair14_term<false, VIRIAL>(a, a.ex14[t - b6], e, e2, w);
+      const int2 pr = a.ex14[t - b6];
+      pair14_term<false, VIRIAL, MULTI>(a, MULTI ? a.setups[a.sys_of_atom[pr.x]] : a.nb, pr, e,
+                                        e2, w);
       slot = kEEwex;
+    }
+    if (MULTI) {
+      if (ENERGY) {  // straight to this term's system
+        int first;
+        if (t < b1) first = a.bond_ij[t].x;
+        else if (t < b2) first = a.ub_ij[t - b1].x;
+        else if (t < b3) first = a.angle_ijk[t - b2].x;
+        else if (t < b4) first = a.dihe_ijkl[t - b3].x;
+        else if (t < b5) first = a.imp_ijkl[t - b4].x;
+        else if (t < b6) first = a.in14[t - b5].x;
+        else first = a.ex14[t - b6].x;
+        long long *es = a.energy + (size_t)a.sys_of_atom[first] * a.energy_stride;
+        add_fixed(es + slot, __double2ll_rn((double)e * kEnergyScale));
+        if (slot2 >= 0) add_fixed(es + slot2, __double2ll_rn((double)e2 * kEnergyScale));
+        if (VIRIAL) {
+#pragma unroll
+          for (int k = 0; k < 9; ++k)
+            add_fixed(es + kNumEnergyTerms + k, __double2ll_rn((double)w[k] * kEnergyScale));
+        }
+      }
+      continue;
     }
     if (ENERGY) {
       atomicAdd(&sh_e[slot], (unsigned long long)__double2ll_rn((double)e * kEnergyScale));
@@ -230,7 +256,7 @@ __global__ void __launch_bounds__(kThreads) bonded_kernel(BondedArgs a) {
         atomicAdd(&sh_v[k], (unsigned long long)__double2ll_rn((double)w[k] * kEnergyScale));
     }
   }
-  if (ENERGY) {
+  if (ENERGY && !MULTI) {
     __syncthreads();
     if (threadIdx.x < kNumEnergyTerms && sh_e[threadIdx.x])
       add_fixed(a.energy + threadIdx.x, (long long)sh_e[threadIdx.x]);
@@ -253,6 +279,18 @@ void launch_bonded(const BondedArgs &a, bool energy, cudaStream_t s, bool virial
   } else {
     bonded_kernel<false, false><<<blocks, kThreads, 0, s>>>(a);
   }
+  APO_LAUNCH_CHECK();
+}
+
+void launch_bonded_multi(const BondedArgs &a, bool energy, cudaStream_t s, bool virial) {
+  const long long total = (long long)a.nbond + a.nub + a.nangle + a.ndihe + a.nimp + a.nin14 + a.nex14;
+  if (total == 0) return;
+  if (!a.sys_of_atom || !a.setups || ((energy || virial) && a.energy_stride <= 0))
+    throw std::invalid_argument("bonded: multi-system launch without system tables");
+  int blocks = (int)std::min<long long>((total + kThreads - 1) / kThreads, 148 * 16);
+  if (virial) bonded_kernel<true, true, true><<<blocks, kThreads, 0, s>>>(a);
+  else if (energy) bonded_kernel<true, false, true><<<blocks, kThreads, 0, s>>>(a);
+  else bonded_kernel<false, false, true><<<blocks, kThreads, 0, s>>>(a);
   APO_LAUNCH_CHECK();
 }
 

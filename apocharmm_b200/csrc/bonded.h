@@ -32,10 +32,17 @@ struct BondedArgs {
   const int *vdwtype; const float2 *vdw14; int ntype;
   NbSetup nb;             // kappa and the VFSW constants for the 1-4 LJ
   long long *virial = nullptr;  // 3x3 internal virial, 2^32 fixed point (virial launches)
+  // multi-system launches: atom -> system, per-system set-ups (kappa, VFSW,
+  // 1-4 table offset and type count), energies of system s at
+  // energy + s * energy_stride (virial at + kNumEnergyTerms)
+  const int *sys_of_atom = nullptr;
+  const NbSetup *setups = nullptr;
+  int energy_stride = 0;
 };
 
 // virial: also accumulate W = -sum over terms of (r_k - r_ref) (x) dU/dr_k
 // into a.virial (implies energy)
 void launch_bonded(const BondedArgs &a, bool energy, cudaStream_t s, bool virial = false);
+void launch_bonded_multi(const BondedArgs &a, bool energy, cudaStream_t s, bool virial = false);
 
 }  // namespace apo

@@ -28,11 +28,18 @@ __global__ void fixed_to_global_kernel(int n, const long long *__restrict__ f, i
 // left [-L/2, L/2] (src/CharmmContext.cu:276-372)
 __global__ void image_centering_kernel(double4 *__restrict__ c, float4 *__restrict__ xq,
                                        const int2 *__restrict__ groups, int ng, double Lx,
-                                       double Ly, double Lz) {
+                                       double Ly, double Lz, const int *__restrict__ sys_of_atom,
+                                       const double4 *__restrict__ boxes) {
   const int lane = threadIdx.x & 31;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < ng; i += nwarps) {
     const int2 g = groups[i];
+    if (sys_of_atom) {  // several systems: this component's own box
+      const double4 b = boxes[sys_of_atom[g.x]];
+      Lx = b.x;
+      Ly = b.y;
+      Lz = b.z;
+    }
     double gx = 0, gy = 0, gz = 0;
     for (int j = g.x + lane; j <= g.y; j += 32) {
       gx += c[j].x;
@@ -74,10 +81,12 @@ __global__ void coords_to_xyzq_kernel(const double4 *__restrict__ c, float4 *__r
 }  // namespace
 
 void launch_image_centering(double4 *coords, float4 *xyzq, const int2 *groups, int ngroups,
-                            double Lx, double Ly, double Lz, cudaStream_t s) {
+                            double Lx, double Ly, double Lz, cudaStream_t s,
+                            const int *sys_of_atom, const double4 *boxes) {
   if (ngroups <= 0) return;
   const int blocks = std::min((ngroups + 3) / 4, 148 * 16);
-  image_centering_kernel<<<blocks, 128, 0, s>>>(coords, xyzq, groups, ngroups, Lx, Ly, Lz);
+  image_centering_kernel<<<blocks, 128, 0, s>>>(coords, xyzq, groups, ngroups, Lx, Ly, Lz,
+                                                 sys_of_atom, boxes);
   APO_LAUNCH_CHECK();
 }
 
@@ -91,6 +100,16 @@ void launch_coords_to_xyzq(const double4 *coords, float4 *xyzq, int n, cudaStrea
 ForceManager::ForceManager(std::shared_ptr<CharmmPSF> psf, std::shared_ptr<CharmmParameters> prm)
     : m_Psf(std::move(psf)), m_Prm(std::move(prm)) {
   if (!m_Psf || !m_Prm) throw std::invalid_argument("ForceManager: null PSF or parameters");
+}
+
+ForceManager::ForceManager(const std::vector<SystemSpec> &systems, int order, int tilesPerWork,
+                           bool precise)
+    : m_Multi(true), m_Specs(systems) {
+  if (systems.empty()) throw std::invalid_argument("ForceManager: no systems");
+  m_Order = order;
+  m_TilesPerWork = tilesPerWork;
+  m_Precise = precise;
+  initializeMulti();
 }
 
 ForceManager::~ForceManager() {
@@ -141,6 +160,10 @@ std::array<int, 3> ForceManager::computeFFTGridSize() const {
 }
 
 void ForceManager::initialize() {
+  if (m_Multi) {
+    initializeMulti();
+    return;
+  }
   if (m_Box[0] == -9999.9999 || m_Box[1] == -9999.9999 || m_Box[2] == -9999.9999)
     throw std::invalid_argument("Error: Box dimension was not set");
   if (m_Cutoff <= 0.0 || m_Cutoff > m_Box[0] / 2.0)
@@ -192,6 +215,12 @@ void ForceManager::initialize() {
   for (double q : m_Top.charge) q2 += q * q;
   m_SelfEnergy = -m_Kappa * kCcelec / std::sqrt(M_PI) * q2;
 
+  createStreams();
+  m_ListBuilt = false;
+  m_Initialized = true;
+}
+
+void ForceManager::createStreams() {
   if (!m_SNb) {
     APO_CUDA(cudaStreamCreateWithFlags(&m_SNb, cudaStreamNonBlocking));
     APO_CUDA(cudaStreamCreateWithFlags(&m_SPme, cudaStreamNonBlocking));
@@ -199,6 +228,132 @@ void ForceManager::initialize() {
     for (cudaEvent_t *e : {&m_EvFork, &m_EvNb, &m_EvPme, &m_EvBond})
       APO_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
   }
+}
+
+namespace {
+
+template <typename T>
+void append(std::vector<T> &dst, const std::vector<T> &src) {
+  dst.insert(dst.end(), src.begin(), src.end());
+}
+int2 shift2(int2 v, int o) { return make_int2(v.x + o, v.y + o); }
+int4 shift4(int4 v, int o, int n) {  // first n components are atoms (-1 stays -1)
+  int *c = &v.x;
+  for (int k = 0; k < n; ++k)
+    if (c[k] >= 0) c[k] += o;
+  return v;
+}
+
+}  // namespace
+
+void ForceManager::initializeMulti() {
+  m_SysTop.clear();
+  m_AtomOff.assign(1, 0);
+  m_SelfEnergies.clear();
+  Topology T;
+  std::vector<NbSetup> setups;
+  std::vector<NbListSystem> lists;
+  std::vector<PmeSystemSpec> pmes;
+  std::vector<double4> boxes;
+  for (size_t k = 0; k < m_Specs.size(); ++k) {
+    SystemSpec &y = m_Specs[k];
+    if (!y.psf || !y.prm) throw std::invalid_argument("ForceManager: null PSF or parameters");
+    for (double b : y.box)
+      if (!(b > 0.0)) throw std::invalid_argument("ForceManager: system box must be positive");
+    if (y.cutnb <= 0.0 || y.cutnb > y.box[0] / 2.0 || y.cutnb > y.box[1] / 2.0 ||
+        y.cutnb > y.box[2] / 2.0)
+      throw std::invalid_argument("ForceManager: list cutoff exceeds half the box");
+    if (y.ctofnb > y.cutnb) throw std::invalid_argument("ctofnb must not exceed the list cutoff (cutnb)");
+    for (int d = 0; d < 3; ++d)
+      if (y.nfft[d] <= 0) y.nfft[d] = std::max(2, 2 * ((int)y.box[d] / 2));
+    Topology t = build_topology(*y.psf, *y.prm);
+    if ((int)t.types.size() > kMaxMultiTypes)
+      throw std::invalid_argument("ForceManager: a system of a multi-system manager has more than " +
+                                  std::to_string(kMaxMultiTypes) + " Lennard-Jones types");
+    const int off = T.natom;
+    NbSetup su = make_nb_setup(y.box[0], y.box[1], y.box[2], y.kappa, y.ctofnb, y.ctonnb);
+    su.vdw_off = (int)T.vdw.size();
+    su.vdw14_off = (int)T.vdw14.size();
+    su.ntype = (int)t.types.size();
+    setups.push_back(su);
+    lists.push_back(NbListSystem{t.natom, y.box[0], y.box[1], y.box[2], (float)y.cutnb});
+    pmes.push_back(PmeSystemSpec{y.nfft[0], y.nfft[1], y.nfft[2], y.kappa, y.box[0], y.box[1],
+                                 y.box[2]});
+    boxes.push_back(make_double4(y.box[0], y.box[1], y.box[2], 0.0));
+    double q2 = 0.0;
+    for (double q : t.charge) q2 += q * q;
+    m_SelfEnergies.push_back(-y.kappa * kCcelec / std::sqrt(M_PI) * q2);
+    // concatenate, atom indices shifted by the system's offset
+    append(T.charge, t.charge);
+    append(T.mass, t.mass);
+    append(T.vdwtype, t.vdwtype);
+    append(T.vdw, t.vdw);
+    append(T.vdw14, t.vdw14);
+    if (T.excl_ptr.empty()) T.excl_ptr.push_back(0);
+    const int ebase = (int)T.excl_idx.size();
+    for (int a = 1; a <= t.natom; ++a) T.excl_ptr.push_back(ebase + t.excl_ptr[a]);
+    for (int e : t.excl_idx) T.excl_idx.push_back(e + off);
+    for (auto v : t.in14) T.in14.push_back(shift2(v, off));
+    for (auto v : t.ex14) T.ex14.push_back(shift2(v, off));
+    for (auto v : t.bond_ij) T.bond_ij.push_back(shift2(v, off));
+    append(T.bond_p, t.bond_p);
+    for (auto v : t.ub_ij) T.ub_ij.push_back(shift2(v, off));
+    append(T.ub_p, t.ub_p);
+    for (auto v : t.angle_ijk) T.angle_ijk.push_back(shift4(v, off, 3));
+    append(T.angle_p, t.angle_p);
+    const int cbase = (int)T.dihe_coef.size();
+    for (auto v : t.dihe_ijkl) T.dihe_ijkl.push_back(shift4(v, off, 4));
+    for (auto v : t.dihe_terms) T.dihe_terms.push_back(make_int2(v.x + cbase, v.y));
+    append(T.dihe_coef, t.dihe_coef);
+    for (auto v : t.imp_ijkl) T.imp_ijkl.push_back(shift4(v, off, 4));
+    append(T.imp_p, t.imp_p);
+    for (auto v : t.waters) T.waters.push_back(shift4(v, off, 3));
+    for (auto v : t.shake_atoms) T.shake_atoms.push_back(shift4(v, off, 4));
+    append(T.shake_p, t.shake_p);
+    for (auto v : t.groups) T.groups.push_back(shift2(v, off));
+    T.natom += t.natom;
+    m_AtomOff.push_back(T.natom);
+    m_SysTop.push_back(std::move(t));
+  }
+  if (T.excl_ptr.empty()) T.excl_ptr.push_back(0);
+  T.types = m_SysTop[0].types;  // per-system tables are addressed through the set-ups
+  m_Top = std::move(T);
+  m_Box = m_Specs[0].box;
+  m_Kappa = m_Specs[0].kappa;
+  m_Cutoff = m_Specs[0].cutnb;
+  m_Ctonnb = m_Specs[0].ctonnb;
+  m_Ctofnb = m_Specs[0].ctofnb;
+  for (int d = 0; d < 3; ++d) m_Nfft[d] = m_Specs[0].nfft[d];
+  m_HostSetup = setups[0];
+
+  m_VdwTypeD.upload(m_Top.vdwtype);
+  m_Vdw.upload(m_Top.vdw);
+  m_Vdw14.upload(m_Top.vdw14);
+  m_BondIJ.upload(m_Top.bond_ij);
+  m_BondP.upload(m_Top.bond_p);
+  m_UbIJ.upload(m_Top.ub_ij);
+  m_UbP.upload(m_Top.ub_p);
+  m_AngleIJK.upload(m_Top.angle_ijk);
+  m_AngleP.upload(m_Top.angle_p);
+  m_DiheIJKL.upload(m_Top.dihe_ijkl);
+  m_DiheTerms.upload(m_Top.dihe_terms);
+  m_DiheCoef.upload(m_Top.dihe_coef);
+  m_ImpIJKL.upload(m_Top.imp_ijkl);
+  m_ImpP.upload(m_Top.imp_p);
+  m_In14.upload(m_Top.in14);
+  m_Ex14.upload(m_Top.ex14);
+  m_Setup.upload(setups);
+  m_Boxes.upload(boxes);
+
+  m_Nbl.setup(lists, m_Top.excl_ptr, m_Top.excl_idx, m_VdwTypeD.p, m_TilesPerWork);
+  m_Stride = m_Nbl.dims().slot_cap;
+  m_Force.alloc((size_t)3 * m_Stride);
+  APO_CUDA(cudaMemset(m_Force.p, 0, (size_t)3 * m_Stride * sizeof(long long)));
+  m_EStride = kNumEnergyTerms + 9;
+  m_Energy.alloc((size_t)m_EStride * m_Specs.size());
+  APO_CUDA(cudaMemset(m_Energy.p, 0, m_Energy.n * sizeof(long long)));
+  m_PmeMulti.setup(pmes, m_Order, m_Energy.p, m_EStride, m_Stride);
+  createStreams();
   m_ListBuilt = false;
   m_Initialized = true;
 }
@@ -222,8 +377,11 @@ void ForceManager::calcForce(const float4 *d_xyzq, bool calcEnergy, bool calcVir
   if (clear) APO_CUDA(cudaMemsetAsync(m_Force.p, 0, (size_t)3 * m_Stride * sizeof(long long), s));
   if (calcVirial) calcEnergy = true;
   long long *virial = calcVirial ? m_Energy.p + kNumEnergyTerms : nullptr;
-  APO_CUDA(cudaMemsetAsync(m_Energy.p, 0,
-                           (kNumEnergyTerms + (calcVirial ? 9 : 0)) * sizeof(long long), s));
+  if (m_Multi)
+    APO_CUDA(cudaMemsetAsync(m_Energy.p, 0, m_Energy.n * sizeof(long long), s));
+  else
+    APO_CUDA(cudaMemsetAsync(m_Energy.p, 0,
+                             (kNumEnergyTerms + (calcVirial ? 9 : 0)) * sizeof(long long), s));
   m_VirialValid = calcVirial;
   APO_CUDA(cudaEventRecord(m_EvFork, s));
   if (m_ComponentMask & 2) {
@@ -265,7 +423,12 @@ void ForceManager::calcForce(const float4 *d_xyzq, bool calcEnergy, bool calcVir
       t1 = m_Timers[m_TimerCursor].second;
       ++m_TimerCursor;
     }
-    launch_nonbonded(a, calcEnergy, m_Precise, m_SNb, calcVirial);
+    if (m_Multi) {
+      a.energy_stride = m_EStride;
+      launch_nonbonded_multi(a, calcEnergy, m_Precise, m_SNb, calcVirial);
+    } else {
+      launch_nonbonded(a, calcEnergy, m_Precise, m_SNb, calcVirial);
+    }
     if (t1) {
       if (timer_capture) APO_CUDA(cudaEventRecordWithFlags(t1, m_SNb, cudaEventRecordExternal));
       else APO_CUDA(cudaEventRecord(t1, m_SNb));
@@ -275,8 +438,12 @@ void ForceManager::calcForce(const float4 *d_xyzq, bool calcEnergy, bool calcVir
   }
   if (m_ComponentMask & 4) {
     APO_CUDA(cudaStreamWaitEvent(m_SPme, m_EvFork, 0));
-    m_Pme.compute(m_Nbl.xyzq_s, m_Nbl.counts, m_Force.p, m_Stride, m_Energy.p, calcEnergy,
-                  m_Precise, m_SPme, virial, m_Nbl.cl_origin);
+    if (m_Multi)
+      m_PmeMulti.compute(m_Nbl.xyzq_s, m_Nbl.cl_origin, m_Nbl.cl_sys, m_Nbl.counts, m_Force.p,
+                         m_Stride, calcEnergy, calcVirial, m_Precise, m_SPme);
+    else
+      m_Pme.compute(m_Nbl.xyzq_s, m_Nbl.counts, m_Force.p, m_Stride, m_Energy.p, calcEnergy,
+                    m_Precise, m_SPme, virial, m_Nbl.cl_origin);
     APO_CUDA(cudaEventRecord(m_EvPme, m_SPme));
     APO_CUDA(cudaStreamWaitEvent(s, m_EvPme, 0));
   }
@@ -302,13 +469,26 @@ void ForceManager::calcForce(const float4 *d_xyzq, bool calcEnergy, bool calcVir
     b.ntype = (int)m_Top.types.size();
     b.nb = m_HostSetup;
     b.virial = virial;
-    launch_bonded(b, calcEnergy, m_SBond, calcVirial);
+    if (m_Multi) {
+      b.sys_of_atom = m_Nbl.sys_of_atom;
+      b.setups = m_Setup.p;
+      b.energy_stride = m_EStride;
+      launch_bonded_multi(b, calcEnergy, m_SBond, calcVirial);
+    } else {
+      launch_bonded(b, calcEnergy, m_SBond, calcVirial);
+    }
     APO_CUDA(cudaEventRecord(m_EvBond, m_SBond));
     APO_CUDA(cudaStreamWaitEvent(s, m_EvBond, 0));
   }
 }
 
 std::map<std::string, double> ForceManager::getEnergyComponents(cudaStream_t s) {
+  if (m_Multi) {  // the sum over all systems
+    std::map<std::string, double> t;
+    for (int k = 0; k < (int)m_Specs.size(); ++k)
+      for (auto &kv : getEnergyComponents(k, s)) t[kv.first] += kv.second;
+    return t;
+  }
   long long e[kNumEnergyTerms];
   APO_CUDA(cudaMemcpyAsync(e, m_Energy.p, sizeof(e), cudaMemcpyDeviceToHost, s));
   APO_CUDA(cudaStreamSynchronize(s));
@@ -318,8 +498,51 @@ std::map<std::string, double> ForceManager::getEnergyComponents(cudaStream_t s) 
   return m;
 }
 
+std::map<std::string, double> ForceManager::getEnergyComponents(int sys, cudaStream_t s) {
+  if (!m_Multi) {
+    if (sys != 0) throw std::invalid_argument("getEnergyComponents: system index out of range");
+    return getEnergyComponents(s);
+  }
+  if (sys < 0 || sys >= (int)m_Specs.size())
+    throw std::invalid_argument("getEnergyComponents: system index out of range");
+  long long e[kNumEnergyTerms];
+  APO_CUDA(cudaMemcpyAsync(e, m_Energy.p + (size_t)sys * m_EStride, sizeof(e),
+                           cudaMemcpyDeviceToHost, s));
+  APO_CUDA(cudaStreamSynchronize(s));
+  std::map<std::string, double> m;
+  for (int k = 0; k < kNumEnergyTerms; ++k) m[kEnergyNames[k]] = (double)e[k] * kInvEnergyScale;
+  m["ewse"] = (m_ComponentMask & 4) ? m_SelfEnergies[sys] : 0.0;
+  return m;
+}
+
+std::vector<double> ForceManager::getVirial(int sys, cudaStream_t s) {
+  if (!m_Multi) {
+    if (sys != 0) throw std::invalid_argument("getVirial: system index out of range");
+    return getVirial(s);
+  }
+  if (sys < 0 || sys >= (int)m_Specs.size())
+    throw std::invalid_argument("getVirial: system index out of range");
+  if (!m_VirialValid)
+    throw std::runtime_error("getVirial: the last force evaluation did not compute the virial");
+  long long v[9];
+  APO_CUDA(cudaMemcpyAsync(v, m_Energy.p + (size_t)sys * m_EStride + kNumEnergyTerms, sizeof(v),
+                           cudaMemcpyDeviceToHost, s));
+  APO_CUDA(cudaStreamSynchronize(s));
+  std::vector<double> out(9);
+  for (int k = 0; k < 9; ++k) out[k] = (double)v[k] * kInvEnergyScale;
+  return out;
+}
+
 std::vector<double> ForceManager::getVirial(cudaStream_t s) {
   if (!m_Initialized) throw std::runtime_error("ForceManager is not initialized");
+  if (m_Multi) {  // the sum over all systems
+    std::vector<double> t(9, 0.0);
+    for (int k = 0; k < (int)m_Specs.size(); ++k) {
+      auto v = getVirial(k, s);
+      for (int j = 0; j < 9; ++j) t[j] += v[j];
+    }
+    return t;
+  }
   if (!m_VirialValid)
     throw std::runtime_error("getVirial: the last force evaluation did not compute the virial");
   long long v[9];
@@ -401,7 +624,17 @@ CharmmContext::~CharmmContext() {
 
 void CharmmContext::useHolonomicConstraints(bool flag) {
   m_Holonomic = flag;
-  m_Ndegf = m_Fm->topology().degrees_of_freedom(flag);
+  if (m_Fm->isMulti()) {  // every system loses its own centre of mass
+    m_Ndegf = 0;
+    m_SysNdegf.clear();
+    for (const Topology &t : m_Fm->systemTopologies()) {
+      m_SysNdegf.push_back(t.degrees_of_freedom(flag));
+      m_Ndegf += m_SysNdegf.back();
+    }
+  } else {
+    m_Ndegf = m_Fm->topology().degrees_of_freedom(flag);
+    m_SysNdegf.assign(1, m_Ndegf);
+  }
 }
 
 namespace {
@@ -447,18 +680,23 @@ void CharmmContext::setCoordinates(const std::vector<double> &xyz) {
   setCoordinatesXyz(xyz.data());
 }
 
-void CharmmContext::setCoordinatesXyz(const double *xyz) {
+void CharmmContext::setCoordinatesXyz(const double *xyz, int first, int count, bool rebuild) {
+  if (count < 0) count = m_N - first;
+  if (first < 0 || count < 0 || first + count > m_N)
+    throw std::invalid_argument("setCoordinates: atom range out of bounds");
   if (m_Stage.n != (size_t)3 * m_N) m_Stage.alloc((size_t)3 * m_N);
   if (m_BadAtom.n != 1) m_BadAtom.alloc(1);
   const int ok = INT_MAX;
   APO_CUDA(cudaMemcpyAsync(m_BadAtom.p, &ok, sizeof(int), cudaMemcpyHostToDevice, m_Stream));
-  APO_CUDA(cudaMemcpyAsync(m_Stage.p, xyz, (size_t)3 * m_N * sizeof(double),
+  APO_CUDA(cudaMemcpyAsync(m_Stage.p + 3 * (size_t)first, xyz, (size_t)3 * count * sizeof(double),
                            cudaMemcpyHostToDevice, m_Stream));
-  const int b = (m_N + 255) / 256;
-  if (m_N > 0) {
-    check_finite_kernel<<<b, 256, 0, m_Stream>>>(m_Stage.p, m_N, m_BadAtom.p);
+  const int b = (count + 255) / 256;
+  if (count > 0) {
+    check_finite_kernel<<<b, 256, 0, m_Stream>>>(m_Stage.p + 3 * (size_t)first, count,
+                                                 m_BadAtom.p);
     APO_LAUNCH_CHECK();
-    pack_xyz_kernel<<<b, 256, 0, m_Stream>>>(m_Stage.p, m_N, m_Coords.p, m_BadAtom.p);
+    pack_xyz_kernel<<<b, 256, 0, m_Stream>>>(m_Stage.p + 3 * (size_t)first, count,
+                                             m_Coords.p + first, m_BadAtom.p);
     APO_LAUNCH_CHECK();
   }
   int bad = INT_MAX;
@@ -466,10 +704,14 @@ void CharmmContext::setCoordinatesXyz(const double *xyz) {
   APO_CUDA(cudaStreamSynchronize(m_Stream));
   if (bad != INT_MAX)
     throw std::invalid_argument("setCoordinates: non-finite coordinate for atom " +
-                                std::to_string(bad));
+                                std::to_string(first + bad));
   launch_coords_to_xyzq(m_Coords.p, m_Xyzq.p, m_N, m_Stream);
   m_HasCoords = true;
-  resetNeighborList(m_Stream);
+  if (rebuild) {
+    resetNeighborList(m_Stream);
+  } else {
+    m_ListStale = true;
+  }
   APO_CUDA(cudaStreamSynchronize(m_Stream));
 }
 
@@ -479,13 +721,17 @@ std::vector<double> CharmmContext::getCoordinates() {
   return out;
 }
 
-void CharmmContext::getCoordinatesXyz(double *xyz) {
+void CharmmContext::getCoordinatesXyz(double *xyz, int first, int count) {
+  if (count < 0) count = m_N - first;
+  if (first < 0 || count < 0 || first + count > m_N)
+    throw std::invalid_argument("getCoordinates: atom range out of bounds");
   if (m_Stage.n != (size_t)3 * m_N) m_Stage.alloc((size_t)3 * m_N);
-  if (m_N > 0) {
-    unpack_xyz_kernel<<<(m_N + 255) / 256, 256, 0, m_Stream>>>(m_Coords.p, m_N, m_Stage.p);
+  if (count > 0) {
+    unpack_xyz_kernel<<<(count + 255) / 256, 256, 0, m_Stream>>>(m_Coords.p + first, count,
+                                                                 m_Stage.p + 3 * (size_t)first);
     APO_LAUNCH_CHECK();
   }
-  APO_CUDA(cudaMemcpyAsync(xyz, m_Stage.p, (size_t)3 * m_N * sizeof(double),
+  APO_CUDA(cudaMemcpyAsync(xyz, m_Stage.p + 3 * (size_t)first, (size_t)3 * count * sizeof(double),
                            cudaMemcpyDeviceToHost, m_Stream));
   APO_CUDA(cudaStreamSynchronize(m_Stream));
 }
@@ -495,12 +741,16 @@ void CharmmContext::setVelocities(const std::vector<double> &v) {
   setVelocitiesXyz(v.data());
 }
 
-void CharmmContext::setVelocitiesXyz(const double *v) {
+void CharmmContext::setVelocitiesXyz(const double *v, int first, int count) {
+  if (count < 0) count = m_N - first;
+  if (first < 0 || count < 0 || first + count > m_N)
+    throw std::invalid_argument("setVelocities: atom range out of bounds");
   if (m_Stage.n != (size_t)3 * m_N) m_Stage.alloc((size_t)3 * m_N);
-  APO_CUDA(cudaMemcpyAsync(m_Stage.p, v, (size_t)3 * m_N * sizeof(double), cudaMemcpyHostToDevice,
-                           m_Stream));
-  if (m_N > 0) {
-    pack_xyz_kernel<<<(m_N + 255) / 256, 256, 0, m_Stream>>>(m_Stage.p, m_N, m_VelMass.p, nullptr);
+  APO_CUDA(cudaMemcpyAsync(m_Stage.p + 3 * (size_t)first, v, (size_t)3 * count * sizeof(double),
+                           cudaMemcpyHostToDevice, m_Stream));
+  if (count > 0) {
+    pack_xyz_kernel<<<(count + 255) / 256, 256, 0, m_Stream>>>(m_Stage.p + 3 * (size_t)first,
+                                                               count, m_VelMass.p + first, nullptr);
     APO_LAUNCH_CHECK();
   }
   APO_CUDA(cudaStreamSynchronize(m_Stream));
@@ -512,14 +762,18 @@ std::vector<double> CharmmContext::getVelocities() {
   return out;
 }
 
-void CharmmContext::getVelocitiesXyz(double *v) {
+void CharmmContext::getVelocitiesXyz(double *v, int first, int count) {
+  if (count < 0) count = m_N - first;
+  if (first < 0 || count < 0 || first + count > m_N)
+    throw std::invalid_argument("getVelocities: atom range out of bounds");
   if (m_Stage.n != (size_t)3 * m_N) m_Stage.alloc((size_t)3 * m_N);
-  if (m_N > 0) {
-    unpack_xyz_kernel<<<(m_N + 255) / 256, 256, 0, m_Stream>>>(m_VelMass.p, m_N, m_Stage.p);
+  if (count > 0) {
+    unpack_xyz_kernel<<<(count + 255) / 256, 256, 0, m_Stream>>>(m_VelMass.p + first, count,
+                                                                 m_Stage.p + 3 * (size_t)first);
     APO_LAUNCH_CHECK();
   }
-  APO_CUDA(cudaMemcpyAsync(v, m_Stage.p, (size_t)3 * m_N * sizeof(double), cudaMemcpyDeviceToHost,
-                           m_Stream));
+  APO_CUDA(cudaMemcpyAsync(v, m_Stage.p + 3 * (size_t)first, (size_t)3 * count * sizeof(double),
+                           cudaMemcpyDeviceToHost, m_Stream));
   APO_CUDA(cudaStreamSynchronize(m_Stream));
 }
 
@@ -530,16 +784,53 @@ void CharmmContext::assignVelocitiesAtTemperature(double temperature) {
     throw std::invalid_argument("assignVelocitiesAtTemperature: coordinates not set");
   APO_CUDA(cudaStreamSynchronize(m_Stream));
   std::vector<double4> vm = m_VelMass.download();
-  std::mt19937 gen{(std::mt19937::result_type)m_Seed};
   const double boltz = kBoltz * (float)temperature;
-  for (int i = 0; i < m_N; ++i) {
-    double sd = std::sqrt(boltz * vm[i].w);
-    std::normal_distribution<> d(0, sd);
-    vm[i].x = d(gen);
-    vm[i].y = d(gen);
-    vm[i].z = d(gen);
+  // one generator per system, seeded with the system's own seed, so that a
+  // system gets the same velocities alone and among others
+  const std::vector<int> &off = m_Fm->isMulti() ? m_Fm->atomOffsets() : std::vector<int>{0, m_N};
+  for (size_t k = 0; k + 1 < off.size(); ++k) {
+    const uint64_t seed = m_Fm->isMulti() ? m_Fm->systemSpecs()[k].seed : m_Seed;
+    std::mt19937 gen{(std::mt19937::result_type)seed};
+    for (int i = off[k]; i < off[k + 1]; ++i) {
+      double sd = std::sqrt(boltz * vm[i].w);
+      std::normal_distribution<> d(0, sd);
+      vm[i].x = d(gen);
+      vm[i].y = d(gen);
+      vm[i].z = d(gen);
+    }
   }
   APO_CUDA(cudaMemcpy(m_VelMass.p, vm.data(), m_N * sizeof(double4), cudaMemcpyHostToDevice));
+}
+
+namespace {
+// kinetic energy of every system (2^32 fixed point, order-free)
+__global__ void system_ke_kernel(const double4 *__restrict__ vm, int n,
+                                 const int *__restrict__ sys_of_atom, long long *__restrict__ ke) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double4 v = vm[i];
+  const double e = 0.5 * (v.x * v.x + v.y * v.y + v.z * v.z) / v.w;
+  add_fixed(ke + (sys_of_atom ? sys_of_atom[i] : 0), __double2ll_rn(e * kEnergyScale));
+}
+}  // namespace
+
+std::vector<double> CharmmContext::systemTemperatures() {
+  const int ns = m_Fm->numSystems();
+  if (m_SysKe.n != (size_t)ns) m_SysKe.alloc(ns);
+  APO_CUDA(cudaMemsetAsync(m_SysKe.p, 0, ns * sizeof(long long), m_Stream));
+  if (m_N > 0) {
+    system_ke_kernel<<<(m_N + 255) / 256, 256, 0, m_Stream>>>(
+        m_VelMass.p, m_N, m_Fm->isMulti() ? m_Fm->sysOfAtom() : nullptr, m_SysKe.p);
+    APO_LAUNCH_CHECK();
+  }
+  std::vector<long long> ke(ns);
+  APO_CUDA(cudaMemcpyAsync(ke.data(), m_SysKe.p, ns * sizeof(long long), cudaMemcpyDeviceToHost,
+                           m_Stream));
+  APO_CUDA(cudaStreamSynchronize(m_Stream));
+  std::vector<double> t(ns);
+  for (int k = 0; k < ns; ++k)
+    t[k] = (double)ke[k] * kInvEnergyScale / (0.5 * m_SysNdegf[k] * kBoltz);
+  return t;
 }
 
 double CharmmContext::getKineticEnergy() {
@@ -556,17 +847,30 @@ double CharmmContext::computeTemperature() {
 
 void CharmmContext::imageCentering(cudaStream_t s) {
   auto b = m_Fm->getBoxDimensions();
-  launch_image_centering(m_Coords.p, m_Xyzq.p, m_Groups.p, (int)m_Groups.n, b[0], b[1], b[2], s);
+  if (m_Fm->isMulti())
+    launch_image_centering(m_Coords.p, m_Xyzq.p, m_Groups.p, (int)m_Groups.n, b[0], b[1], b[2], s,
+                           m_Fm->sysOfAtom(), m_Fm->systemBoxes());
+  else
+    launch_image_centering(m_Coords.p, m_Xyzq.p, m_Groups.p, (int)m_Groups.n, b[0], b[1], b[2], s);
 }
 
 void CharmmContext::resetNeighborList(cudaStream_t s) {
   imageCentering(s);
   m_Fm->resetNeighborList(m_Xyzq.p, s);
+  m_ListStale = false;
+}
+
+void CharmmContext::ensureNeighborList() {
+  if (!m_HasCoords) throw std::runtime_error("coordinates not set");
+  if (m_ListStale || !m_Fm->isListBuilt()) {
+    resetNeighborList(m_Stream);
+    APO_CUDA(cudaStreamSynchronize(m_Stream));
+  }
 }
 
 void CharmmContext::calculateForces(bool reset, bool calcEnergy, bool calcVirial) {
   if (!m_HasCoords) throw std::runtime_error("calculateForces: coordinates not set");
-  if (reset) resetNeighborList(m_Stream);
+  if (reset || m_ListStale) resetNeighborList(m_Stream);
   m_Fm->calcForce(m_Xyzq.p, calcEnergy, calcVirial, m_Stream);
   APO_CUDA(cudaStreamSynchronize(m_Stream));
 }

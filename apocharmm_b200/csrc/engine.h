@@ -64,10 +64,39 @@ struct DeviceArray {
   }
 };
 
+// One system of a multi-system force manager (replicas, lambda windows, or
+// unrelated molecules advanced together): its files, box and nonbonded/PME
+// settings.  All systems of one manager share the spline order, the
+// precision form and the tiles per work item.
+struct SystemSpec {
+  std::shared_ptr<CharmmPSF> psf;
+  std::shared_ptr<CharmmParameters> prm;
+  std::array<double, 3> box{{0.0, 0.0, 0.0}};
+  double kappa = 0.34, cutnb = 14.0, ctonnb = 12.0, ctofnb = 10.0;
+  std::array<int, 3> nfft{{-1, -1, -1}};  // -1: 2 floor(L/2)
+  uint64_t seed = 0;                      // velocities and Langevin noise of this system
+};
+
 class ForceManager {
  public:
   ForceManager(std::shared_ptr<CharmmPSF> psf, std::shared_ptr<CharmmParameters> prm);
+  // several independent systems, concatenated in order, evaluated with one
+  // launch per stage; initialised on construction
+  explicit ForceManager(const std::vector<SystemSpec> &systems, int order = 4,
+                        int tilesPerWork = 8, bool precise = false);
   ~ForceManager();
+  bool isMulti() const { return m_Multi; }
+  int numSystems() const { return m_Multi ? (int)m_Specs.size() : 1; }
+  const std::vector<SystemSpec> &systemSpecs() const { return m_Specs; }
+  // first atom of every system and the total (numSystems() + 1 entries)
+  const std::vector<int> &atomOffsets() const { return m_AtomOff; }
+  const std::vector<Topology> &systemTopologies() const { return m_SysTop; }
+  // device: atom -> system, per-system box (x, y, z, 0)
+  const int *sysOfAtom() { return m_Nbl.sys_of_atom; }
+  const double4 *systemBoxes() const { return m_Boxes.p; }
+  // energies of one system (multi-system managers)
+  std::map<std::string, double> getEnergyComponents(int sys, cudaStream_t s);
+  std::vector<double> getVirial(int sys, cudaStream_t s);
 
   void setBoxDimensions(const std::array<double, 3> &box);
   void setKappa(double k) { m_Kappa = k; m_Initialized = false; }
@@ -92,8 +121,9 @@ class ForceManager {
   double getCtofnb() const { return m_Ctofnb; }
   std::array<int, 3> getFFTGrid() const { return {m_Nfft[0], m_Nfft[1], m_Nfft[2]}; }
   int getPmeSplineOrder() const { return m_Order; }
-  int getNumAtoms() const { return m_Psf->getNumAtoms(); }
+  int getNumAtoms() const { return m_Multi ? m_Top.natom : m_Psf->getNumAtoms(); }
   bool isInitialized() const { return m_Initialized; }
+  bool isListBuilt() const { return m_ListBuilt; }
   std::shared_ptr<CharmmPSF> getPsf() const { return m_Psf; }
   const Topology &topology() const { return m_Top; }
   std::array<int, 3> computeFFTGridSize() const;
@@ -138,8 +168,18 @@ class ForceManager {
   double kernelTimeMs(int &launches);
 
  private:
+  void initializeMulti();
+  void createStreams();
   std::shared_ptr<CharmmPSF> m_Psf;
   std::shared_ptr<CharmmParameters> m_Prm;
+  bool m_Multi = false;
+  std::vector<SystemSpec> m_Specs;
+  std::vector<Topology> m_SysTop;
+  std::vector<int> m_AtomOff;
+  std::vector<double> m_SelfEnergies;
+  int m_EStride = 0;  // energy slots per system (energies + virial)
+  PmeMulti m_PmeMulti;
+  DeviceArray<double4> m_Boxes;
   std::array<double, 3> m_Box{{-9999.9999, -9999.9999, -9999.9999}};
   double m_Kappa = 0.34, m_Cutoff = 14.0, m_Ctonnb = 12.0, m_Ctofnb = 10.0;
   int m_Nfft[3] = {-1, -1, -1};
@@ -188,21 +228,32 @@ class CharmmContext {
   // the same four transfers on a caller's x,y,z-interleaved host array of
   // 3N doubles (pinned memory gives full-bandwidth copies): one copy
   // through a device staging array and one pack/unpack kernel each
-  void setCoordinatesXyz(const double *xyz);
-  void getCoordinatesXyz(double *xyz);
-  void setVelocitiesXyz(const double *v);
-  void getVelocitiesXyz(double *v);
+  // (first, count) restricts a transfer to an atom range (one system of a
+  // multi-system context); count < 0 means to the last atom
+  // rebuild = false: the list is marked stale and rebuilt before the next
+  // force evaluation (lets several systems be loaded before the first build)
+  void setCoordinatesXyz(const double *xyz, int first = 0, int count = -1, bool rebuild = true);
+  void getCoordinatesXyz(double *xyz, int first = 0, int count = -1);
+  void setVelocitiesXyz(const double *v, int first = 0, int count = -1);
+  void getVelocitiesXyz(double *v, int first = 0, int count = -1);
   void setRandomSeedForVelocities(uint64_t seed) { m_Seed = seed; }
   void assignVelocitiesAtTemperature(double temperature);
   void useHolonomicConstraints(bool flag);
   bool isUsingHolonomicConstraints() const { return m_Holonomic; }
   int getDegreesOfFreedom() const { return m_Ndegf; }
+  // per system (one entry for a single-system context)
+  const std::vector<int> &systemDegreesOfFreedom() const { return m_SysNdegf; }
+  // instantaneous temperature of every system from the on-step velocities
+  std::vector<double> systemTemperatures();
   int getNumAtoms() const { return m_N; }
   double computeTemperature();
   double getKineticEnergy();
 
   void imageCentering(cudaStream_t s);
   void resetNeighborList(cudaStream_t s);
+  // rebuild now (synchronously usable, outside any capture) if the list was
+  // never built or coordinates were loaded without a rebuild
+  void ensureNeighborList();
   void calculateForces(bool reset, bool calcEnergy, bool calcVirial);
   double calculatePotentialEnergy(bool reset, bool print);
 
@@ -222,7 +273,10 @@ class CharmmContext {
   uint64_t m_Seed = 0;
   bool m_Holonomic = true;
   int m_Ndegf = 0;
+  std::vector<int> m_SysNdegf;
+  DeviceArray<long long> m_SysKe;
   bool m_HasCoords = false;
+  bool m_ListStale = false;
   cudaStream_t m_Stream = nullptr;
   DeviceArray<double4> m_Coords, m_VelMass;
   DeviceArray<float4> m_Xyzq;
@@ -233,7 +287,8 @@ class CharmmContext {
 
 // device helpers shared with the integrators
 void launch_image_centering(double4 *coords, float4 *xyzq, const int2 *groups, int ngroups,
-                            double Lx, double Ly, double Lz, cudaStream_t s);
+                            double Lx, double Ly, double Lz, cudaStream_t s,
+                            const int *sys_of_atom = nullptr, const double4 *boxes = nullptr);
 void launch_coords_to_xyzq(const double4 *coords, float4 *xyzq, int n, cudaStream_t s);
 
 }  // namespace apo

@@ -213,6 +213,11 @@ __device__ void sum_partials(const double *partials, double &s0, double &s1) {
 }
 
 struct Common {
+  // several systems: atom -> system, first atom of every system, and every
+  // system's noise seed (null for one system)
+  const int *sys_of_atom;
+  const int *atom_off;
+  const unsigned long long *sys_seed;
   int ngroups;
   const int4 *groups;   // atoms (-1 unused)
   const int2 *gmeta;    // (kind, shake parameter index)
@@ -277,7 +282,12 @@ __global__ void __launch_bounds__(kThreads) langevin_kernel(Common c, double gam
       dp[k] = xyz(c.dprev[a]);
       const d3 gr = take_grad(c.force, c.stride, c.glo2loc[a]);
       curandStatePhilox4_32_10_t st;
-      curand_init(seed, (unsigned long long)a, 0ull, &st);
+      if (c.sys_seed) {  // a system's own stream, the same alone or among others
+        const int sy = c.sys_of_atom[a];
+        curand_init(seed ^ c.sys_seed[sy], (unsigned long long)(a - c.atom_off[sy]), 0ull, &st);
+      } else {
+        curand_init(seed, (unsigned long long)a, 0ull, &st);
+      }
       skipahead(pos, &st);
       const float4 rn = curand_normal4(&st);
       const double rdf = sqrt(2.0 * gamma * kbt / v.w) / dt;
@@ -576,6 +586,8 @@ void upload(DeviceArray<T> &d, const std::vector<T> &v) {
 }  // namespace
 
 struct IntegratorState {
+  DeviceArray<int> atom_off;
+  DeviceArray<unsigned long long> sys_seed;
   DeviceArray<int4> groups;
   DeviceArray<int2> gmeta;
   DeviceArray<float4> shake_p;
@@ -621,6 +633,9 @@ void CudaIntegrator::setCharmmContext(std::shared_ptr<CharmmContext> ctx) {
   if (m_Ctx) throw std::invalid_argument("A CharmmContext object was already set for this CudaIntegrator.");
   if (!ctx) throw std::invalid_argument("null CharmmContext");
   m_Ctx = std::move(ctx);
+  // centre-of-mass removal sums over all atoms: with several systems it
+  // would couple them, so it is not applied (Langevin damps the drift)
+  if (m_Ctx->getForceManager()->isMulti()) m_ComFreq = 0;
   buildGroups();
   initialize();
   m_Initialized = true;
@@ -692,6 +707,18 @@ void CudaIntegrator::buildGroups() {
     throw std::invalid_argument("system too large for the integrator's reduction buffer");
   S.partials.alloc((size_t)4 * std::max(S.blocks_groups, S.blocks_atoms) + 8);
   Common &c = S.c;
+  c.sys_of_atom = nullptr;
+  c.atom_off = nullptr;
+  c.sys_seed = nullptr;
+  if (fm->isMulti()) {
+    std::vector<unsigned long long> seeds;
+    for (auto &y : fm->systemSpecs()) seeds.push_back((unsigned long long)y.seed);
+    S.atom_off.upload(fm->atomOffsets());
+    S.sys_seed.upload(seeds);
+    c.sys_of_atom = fm->sysOfAtom();
+    c.atom_off = S.atom_off.p;
+    c.sys_seed = S.sys_seed.p;
+  }
   c.ngroups = S.ngroups;
   c.groups = S.groups.p;
   c.gmeta = S.gmeta.p;
@@ -727,9 +754,11 @@ void CudaIntegrator::segment(int nsteps, cudaStream_t s) {
   // in the shared buffer; every segment starts from a cleared one (the step
   // kernels clear each slot they consume afterwards)
   APO_CUDA(cudaMemsetAsync(fm->forceFixed(), 0, (size_t)3 * fm->forceStride() * sizeof(long long), s));
-  com_sum_kernel<<<S.blocks_atoms, kThreads, 0, s>>>(S.c, S.natom, m_ComFreq);
-  com_apply_kernel<<<S.blocks_atoms, kThreads, 0, s>>>(S.c, S.natom, m_ComFreq);
-  APO_LAUNCH_CHECK();
+  if (m_ComFreq > 0) {
+    com_sum_kernel<<<S.blocks_atoms, kThreads, 0, s>>>(S.c, S.natom, m_ComFreq);
+    com_apply_kernel<<<S.blocks_atoms, kThreads, 0, s>>>(S.c, S.natom, m_ComFreq);
+    APO_LAUNCH_CHECK();
+  }
   m_Ctx->resetNeighborList(s);
   for (int k = 0; k < nsteps; ++k) {
     forcesForStep(s);
@@ -747,6 +776,8 @@ void CudaIntegrator::propagate(int numSteps) {
     throw std::invalid_argument("CudaIntegrator::propagate: no CharmmContext was set for this CudaIntegrator.");
   if (numSteps <= 0) return;
   cudaStream_t s = m_Ctx->stream();
+  // the first list build sizes the buffers synchronously: never inside a capture
+  m_Ctx->ensureNeighborList();
   int left = numSteps;
   long long done = 0;
   while (left > 0) {
@@ -869,6 +900,9 @@ CudaNoseHooverIntegrator::CudaNoseHooverIntegrator(double ps) : CudaIntegrator(p
 }
 
 void CudaNoseHooverIntegrator::initialize() {
+  if (m_Ctx->getForceManager()->isMulti())
+    throw std::invalid_argument("Nose-Hoover couples all atoms through one piston: it is not "
+                                "available for a multi-system context");
   IntegratorState &S = *m_S;
   cudaStream_t s = m_Ctx->stream();
   if (m_PistonMass == -9999.9999) {

@@ -43,7 +43,8 @@ class CudaIntegrator : public std::enable_shared_from_this<CudaIntegrator> {
   void setCharmmContext(std::shared_ptr<CharmmContext> ctx);
   std::shared_ptr<CharmmContext> getCharmmContext() const { return m_Ctx; }
   void setNonbondedListUpdateFrequency(int f);
-  void setRemoveCenterOfMassFrequency(int f) { m_ComFreq = f; }
+  // 0 switches the removal off (always off for a multi-system context)
+  void setRemoveCenterOfMassFrequency(int f) { m_ComFreq = f < 0 ? 0 : f; clearGraphs(); }
   void setUseGraphs(bool g) { m_UseGraphs = g; }
   void subscribe(std::shared_ptr<Subscriber> sub);
   void propagate(int numSteps);

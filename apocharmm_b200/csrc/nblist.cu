@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <stdexcept>
 
 #include "device_util.cuh"
 
@@ -16,12 +17,15 @@ __device__ __forceinline__ int floor_div(int a, int b) {
 }
 
 // (1) bin atoms into x-y columns; record wrapped z key and image shift
-__global__ void bin_kernel(int n, const float4 *__restrict__ xyzq, NbListDims d,
+__global__ void bin_kernel(int n, const float4 *__restrict__ xyzq,
+                           const int *__restrict__ sys_of_atom,
+                           const NbSysDims *__restrict__ sysd,
                            int *__restrict__ col_count, int *__restrict__ atom_col,
                            int *__restrict__ atom_rank, float4 *__restrict__ atom_shift,
                            float *__restrict__ zkey, unsigned *__restrict__ err) {
   int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= n) return;
+  const NbSysDims d = sysd[sys_of_atom[g]];
   float4 p = xyzq[g];
   float sx = 0.f, sy = 0.f, sz = 0.f;
   int col = 0;
@@ -38,9 +42,10 @@ __global__ void bin_kernel(int n, const float4 *__restrict__ xyzq, NbListDims d,
     int cy = (int)((yw + 0.5f * d.Ly) * ((float)d.ncy / d.Ly));
     cx = min(max(cx, 0), d.ncx - 1);
     cy = min(max(cy, 0), d.ncy - 1);
-    col = cx + d.ncx * cy;
+    col = d.col_off + cx + d.ncx * cy;
   } else {
     atomicOr(err, (unsigned)kErrNaN);
+    col = d.col_off;
   }
   atom_col[g] = col;
   atom_rank[g] = atomicAdd(&col_count[col], 1);
@@ -116,6 +121,7 @@ __global__ void col_sort_kernel(int ncol, const int *__restrict__ col_count,
                                 const int *__restrict__ vdwtype, int *__restrict__ perm,
                                 int *__restrict__ glo2loc, float4 *__restrict__ slot_shift,
                                 int *__restrict__ type_s, int *__restrict__ cl_col,
+                                const int *__restrict__ col_sys, int *__restrict__ cl_sys,
                                 const int *__restrict__ counts, int sort_cap) {
   extern __shared__ unsigned char smem[];
   float *sk = reinterpret_cast<float *>(smem);
@@ -171,7 +177,10 @@ __global__ void col_sort_kernel(int ncol, const int *__restrict__ col_count,
       slot_shift[s] = make_float4(0.f, 0.f, 0.f, 0.f);
       type_s[s] = 0;
     }
-    if ((k & (kTile - 1)) == 0) cl_col[s / kTile] = col;
+    if ((k & (kTile - 1)) == 0) {
+      cl_col[s / kTile] = col;
+      cl_sys[s / kTile] = col_sys[col];
+    }
   }
 }
 
@@ -179,12 +188,14 @@ __global__ void col_sort_kernel(int ncol, const int *__restrict__ col_count,
 // positions rounded to a multiple of 1/64 A (exact in single precision for
 // any box below 2^17 A), and per slot the FP64 offset image shift - origin
 __global__ void origin_kernel(const float4 *__restrict__ xyzq, const int *__restrict__ perm,
-                              const float4 *__restrict__ slot_shift, NbListDims d,
+                              const float4 *__restrict__ slot_shift,
+                              const NbSysDims *__restrict__ sysd, const int *__restrict__ cl_sys,
                               float4 *__restrict__ cl_origin, double4 *__restrict__ slot_off,
                               const int *__restrict__ counts) {
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (w >= counts[0] / kTile) return;
+  const NbSysDims d = sysd[cl_sys[w]];
   const int s = w * kTile + lane;
   const int g = perm[s];
   float4 p = make_float4(0.f, 0.f, 0.f, 0.f), sh = slot_shift[s];
@@ -269,7 +280,8 @@ __global__ void bbox_kernel(const float4 *__restrict__ xyzq_s, const int *__rest
 // candidate order, so the list is deterministic.  With FILL the tiles, their
 // exclusion masks and the work items are written at the offsets of the scan.
 template <bool FILL>
-__global__ void tiles_kernel(NbListDims d, const int *__restrict__ cl_col,
+__global__ void tiles_kernel(const NbSysDims *__restrict__ sysd, const int *__restrict__ cl_sys,
+                             int tiles_per_work, const int *__restrict__ cl_col,
                              const int *__restrict__ col_start,
                              const float4 *__restrict__ bb_c, const float4 *__restrict__ bb_h,
                              const int *__restrict__ perm, const int *__restrict__ glo2loc,
@@ -277,12 +289,14 @@ __global__ void tiles_kernel(NbListDims d, const int *__restrict__ cl_col,
                              int *__restrict__ tile_count, const int *__restrict__ tile_start,
                              const int *__restrict__ work_start, int2 *__restrict__ tiles,
                              unsigned *__restrict__ masks, int4 *__restrict__ work,
-                             const int *__restrict__ counts, int sys) {
+                             const int *__restrict__ counts) {
   const int ic = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (ic >= counts[0] / kTile) return;
   if (FILL && counts[1] == 0) return;  // overflow: nothing to write
-  const int c = cl_col[ic];
+  const int sys = cl_sys[ic];
+  const NbSysDims d = sysd[sys];
+  const int c = cl_col[ic] - d.col_off;
   const int cx = c % d.ncx, cy = c / d.ncx;
   const float4 ci = bb_c[ic], hi = bb_h[ic];
   const float cwx = d.Lx / d.ncx, cwy = d.Ly / d.ncy;
@@ -309,7 +323,7 @@ __global__ void tiles_kernel(NbListDims d, const int *__restrict__ cl_col,
       int ix = floor_div(xx, d.ncx);
       if (ix < -1 || ix > 1) continue;
       int wx = xx - ix * d.ncx;
-      int col = wx + d.ncx * wy;
+      int col = d.col_off + wx + d.ncx * wy;
       int js = col_start[col] / kTile, je = col_start[col + 1] / kTile;
       int ncand = (je - js) * 3;
       for (int b0 = 0; b0 < ncand; b0 += 32) {
@@ -362,7 +376,7 @@ __global__ void tiles_kernel(NbListDims d, const int *__restrict__ cl_col,
     if (lane == 0) tile_count[ic] = count;
   } else if (lane == 0) {
     int w0 = work_start[ic];
-    int tpw = d.tiles_per_work;
+    int tpw = tiles_per_work;
     for (int k = 0; k * tpw < count; ++k)
       work[w0 + k] = make_int4(ic, base_tile + k * tpw, base_tile + min(count, (k + 1) * tpw), sys);
   }
@@ -422,30 +436,26 @@ NeighborList::~NeighborList() { release(); }
 
 void NeighborList::release() {
   dfree(perm); dfree(glo2loc); dfree(slot_shift); dfree(xyzq_s); dfree(type_s);
-  dfree(slot_off); dfree(cl_origin);
+  dfree(slot_off); dfree(cl_origin); dfree(cl_sys); dfree(sys_of_atom);
   dfree(tiles); dfree(masks); dfree(work); dfree(counts); dfree(error);
   dfree(m_excl_ptr); dfree(m_excl_idx); dfree(m_col_count); dfree(m_col_start);
   dfree(m_atom_col); dfree(m_atom_rank); dfree(m_atom_shift); dfree(m_atom_z); dfree(m_tmp_key);
   dfree(m_tmp_idx); dfree(m_cl_col); dfree(m_bb_c); dfree(m_bb_h);
   dfree(m_tile_count); dfree(m_tile_start); dfree(m_work_start);
+  dfree(m_sys); dfree(m_col_sys);
 }
 
 void NeighborList::setup(int natom, double Lx, double Ly, double Lz, float rlist,
                          const std::vector<int> &excl_ptr, const std::vector<int> &excl_idx,
                          const int *d_vdwtype, int tiles_per_work) {
-  if (natom <= 0) throw std::invalid_argument("NeighborList: no atoms");
-  if (!(Lx > 0.0 && Ly > 0.0 && Lz > 0.0) || Lx > 65536.0 || Ly > 65536.0 || Lz > 65536.0)
-    throw std::invalid_argument("NeighborList: box lengths must be in (0, 65536] A");
-  m_d.natom = natom;
-  m_d.Lx = (float)Lx;
-  m_d.Ly = (float)Ly;
-  m_d.Lz = (float)Lz;
-  m_d.Lxd = Lx;
-  m_d.Lyd = Ly;
-  m_d.Lzd = Lz;
-  m_d.rlist = rlist;
-  m_d.tiles_per_work = tiles_per_work;
-  m_vdwtype = d_vdwtype;
+  setup(std::vector<NbListSystem>{NbListSystem{natom, Lx, Ly, Lz, rlist}}, excl_ptr, excl_idx,
+        d_vdwtype, tiles_per_work);
+}
+
+void NeighborList::setup(const std::vector<NbListSystem> &systems,
+                         const std::vector<int> &excl_ptr, const std::vector<int> &excl_idx,
+                         const int *d_vdwtype, int tiles_per_work) {
+  if (systems.empty()) throw std::invalid_argument("NeighborList: no systems");
   {
     static bool attr = false;
     if (!attr) {
@@ -454,25 +464,71 @@ void NeighborList::setup(int natom, double Lx, double Ly, double Lz, float rlist
       attr = true;
     }
   }
-  // columns whose cross-section holds ~32 atoms per z-slab of equal height:
-  // clusters come out close to cubic
-  double rho = natom / ((double)Lx * Ly * Lz);
-  double edge = std::cbrt(32.0 / rho);
-  m_d.ncx = std::max(1, (int)std::floor(Lx / edge));
-  m_d.ncy = std::max(1, (int)std::floor(Ly / edge));
-  m_ncol = m_d.ncx * m_d.ncy;
-  double per_col = natom / (double)m_ncol;
+  release();
+  m_sys_h.clear();
+  m_d = NbListDims{};
+  m_d.nsys = (int)systems.size();
+  m_d.tiles_per_work = std::max(1, tiles_per_work);
   m_d.sort_cap = 1024;
-  while (m_d.sort_cap < 1.6 * per_col + 64) m_d.sort_cap *= 2;
-  m_d.slot_cap = natom + kTile * m_ncol;
-  m_d.slot_cap = (m_d.slot_cap + kTile - 1) / kTile * kTile;
-  // tile estimate: clusters within rlist + two cluster edges, half list
-  int ncl = m_d.slot_cap / kTile;
-  double reach = rlist + 2.0 * edge;
-  double per_cl = rho * 4.18879 * reach * reach * reach / 32.0 * 0.5 + 16.0;
-  m_d.tile_cap = (int)std::min<double>(ncl * per_cl, 2.0e9 / 128.0);
-  m_d.work_cap = m_d.tile_cap / std::max(1, tiles_per_work) + ncl + 16;
+  long long slots = 0;
+  double tiles = 0.0;
+  int natom = 0, ncol = 0;
+  std::vector<int> col_sys, atom_sys;
+  for (size_t k = 0; k < systems.size(); ++k) {
+    const NbListSystem &y = systems[k];
+    if (y.natom <= 0) throw std::invalid_argument("NeighborList: a system has no atoms");
+    if (!(y.Lx > 0.0 && y.Ly > 0.0 && y.Lz > 0.0) || y.Lx > 65536.0 || y.Ly > 65536.0 ||
+        y.Lz > 65536.0)
+      throw std::invalid_argument("NeighborList: box lengths must be in (0, 65536] A");
+    NbSysDims d;
+    d.Lx = (float)y.Lx;
+    d.Ly = (float)y.Ly;
+    d.Lz = (float)y.Lz;
+    d.Lxd = y.Lx;
+    d.Lyd = y.Ly;
+    d.Lzd = y.Lz;
+    d.rlist = y.rlist;
+    d.atom_off = natom;
+    d.natom = y.natom;
+    // columns whose cross-section holds ~32 atoms per z-slab of equal height:
+    // clusters come out close to cubic
+    const double rho = y.natom / (y.Lx * y.Ly * y.Lz);
+    const double edge = std::cbrt(32.0 / rho);
+    d.ncx = std::max(1, (int)std::floor(y.Lx / edge));
+    d.ncy = std::max(1, (int)std::floor(y.Ly / edge));
+    d.col_off = ncol;
+    const int nc = d.ncx * d.ncy;
+    const double per_col = y.natom / (double)nc;
+    while (m_d.sort_cap < 1.6 * per_col + 64) m_d.sort_cap *= 2;
+    slots += y.natom + (long long)kTile * nc;
+    // tile estimate: clusters within rlist + two cluster edges, half list
+    const double reach = y.rlist + 2.0 * edge;
+    const double ncl_s = (y.natom + (double)kTile * nc) / kTile;
+    tiles += ncl_s * (rho * 4.18879 * reach * reach * reach / 32.0 * 0.5 + 16.0);
+    for (int c = 0; c < nc; ++c) col_sys.push_back((int)k);
+    for (int a = 0; a < y.natom; ++a) atom_sys.push_back((int)k);
+    ncol += nc;
+    natom += y.natom;
+    m_sys_h.push_back(d);
+  }
+  m_d.natom = natom;
+  m_d.ncol = ncol;
+  m_d.slot_cap = (int)((slots + kTile - 1) / kTile * kTile);
+  const int ncl = m_d.slot_cap / kTile;
+  m_d.tile_cap = (int)std::min<double>(tiles, 2.0e9 / 128.0);
+  m_d.work_cap = m_d.tile_cap / m_d.tiles_per_work + ncl + 16;
+  if ((int)excl_ptr.size() != natom + 1)
+    throw std::invalid_argument("NeighborList: exclusion pointer array must have natom + 1 entries");
+  m_vdwtype = d_vdwtype;
   alloc();
+  dalloc(m_sys, m_sys_h.size());
+  APO_CUDA(cudaMemcpy(m_sys, m_sys_h.data(), m_sys_h.size() * sizeof(NbSysDims),
+                      cudaMemcpyHostToDevice));
+  dalloc(m_col_sys, col_sys.size());
+  APO_CUDA(cudaMemcpy(m_col_sys, col_sys.data(), col_sys.size() * sizeof(int),
+                      cudaMemcpyHostToDevice));
+  APO_CUDA(cudaMemcpy(sys_of_atom, atom_sys.data(), atom_sys.size() * sizeof(int),
+                      cudaMemcpyHostToDevice));
   dalloc(m_excl_ptr, excl_ptr.size());
   dalloc(m_excl_idx, std::max<size_t>(1, excl_idx.size()));
   APO_CUDA(cudaMemcpy(m_excl_ptr, excl_ptr.data(), excl_ptr.size() * sizeof(int),
@@ -482,15 +538,28 @@ void NeighborList::setup(int natom, double Lx, double Ly, double Lz, float rlist
                         cudaMemcpyHostToDevice));
 }
 
+void NeighborList::set_tiles_per_work(int tpw) {
+  tpw = std::max(1, tpw);
+  if (tpw == m_d.tiles_per_work) return;
+  const int ncl = m_d.slot_cap / kTile;
+  m_d.tiles_per_work = tpw;
+  const int need = m_d.tile_cap / tpw + ncl + 16;
+  if (need > m_d.work_cap) {
+    m_d.work_cap = need;
+    dalloc(work, m_d.work_cap);
+  }
+}
+
 void NeighborList::alloc() {
   const int n = m_d.natom, S = m_d.slot_cap, ncl = S / kTile;
   dalloc(perm, S); dalloc(glo2loc, n); dalloc(slot_shift, S); dalloc(xyzq_s, S);
-  dalloc(slot_off, S); dalloc(cl_origin, ncl);
+  dalloc(slot_off, S); dalloc(cl_origin, ncl); dalloc(cl_sys, ncl); dalloc(sys_of_atom, n);
   APO_CUDA(cudaMemset(slot_off, 0, (size_t)S * sizeof(double4)));
   APO_CUDA(cudaMemset(cl_origin, 0, (size_t)ncl * sizeof(float4)));
+  APO_CUDA(cudaMemset(cl_sys, 0, (size_t)ncl * sizeof(int)));
   dalloc(type_s, S); dalloc(tiles, m_d.tile_cap); dalloc(masks, (size_t)m_d.tile_cap * kTile);
   dalloc(work, m_d.work_cap); dalloc(counts, 8); dalloc(error, 1);
-  dalloc(m_col_count, m_ncol); dalloc(m_col_start, m_ncol + 1); dalloc(m_atom_col, n);
+  dalloc(m_col_count, m_d.ncol); dalloc(m_col_start, m_d.ncol + 1); dalloc(m_atom_col, n);
   dalloc(m_atom_rank, n); dalloc(m_atom_shift, n); dalloc(m_atom_z, n);
   dalloc(m_tmp_key, S); dalloc(m_tmp_idx, S);
   dalloc(m_cl_col, ncl); dalloc(m_bb_c, ncl); dalloc(m_bb_h, ncl);
@@ -506,39 +575,43 @@ void NeighborList::build(const float4 *d_xyzq, cudaStream_t s) {
   const int n = m_d.natom;
   const int S = m_d.slot_cap;
   const int ncl = S / kTile;
-  APO_CUDA(cudaMemsetAsync(m_col_count, 0, m_ncol * sizeof(int), s));
-  bin_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, d_xyzq, m_d, m_col_count, m_atom_col,
-                                              m_atom_rank, m_atom_shift, m_atom_z, error);
+  APO_CUDA(cudaMemsetAsync(m_col_count, 0, m_d.ncol * sizeof(int), s));
+  bin_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, d_xyzq, sys_of_atom, m_sys, m_col_count,
+                                              m_atom_col, m_atom_rank, m_atom_shift, m_atom_z,
+                                              error);
   APO_LAUNCH_CHECK();
-  col_scan_kernel<<<1, kScanThreads, 0, s>>>(m_ncol, m_col_count, m_col_start, counts, S,
+  col_scan_kernel<<<1, kScanThreads, 0, s>>>(m_d.ncol, m_col_count, m_col_start, counts, S,
                                              m_d.sort_cap, error);
   APO_LAUNCH_CHECK();
   scatter_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, m_atom_col, m_atom_rank, m_col_start,
                                                   m_atom_z, m_tmp_key, m_tmp_idx, counts);
   APO_LAUNCH_CHECK();
   size_t sm = (size_t)m_d.sort_cap * (sizeof(float) + sizeof(int));
-  col_sort_kernel<<<m_ncol, 512, sm, s>>>(m_ncol, m_col_count, m_col_start, m_tmp_key,
-                                          m_tmp_idx, m_atom_shift, m_vdwtype, perm, glo2loc,
-                                          slot_shift, type_s, m_cl_col, counts, m_d.sort_cap);
+  col_sort_kernel<<<m_d.ncol, 512, sm, s>>>(m_d.ncol, m_col_count, m_col_start, m_tmp_key,
+                                            m_tmp_idx, m_atom_shift, m_vdwtype, perm, glo2loc,
+                                            slot_shift, type_s, m_cl_col, m_col_sys, cl_sys,
+                                            counts, m_d.sort_cap);
   APO_LAUNCH_CHECK();
-  origin_kernel<<<(ncl * 32 + 255) / 256, 256, 0, s>>>(d_xyzq, perm, slot_shift, m_d, cl_origin,
-                                                        slot_off, counts);
+  origin_kernel<<<(ncl * 32 + 255) / 256, 256, 0, s>>>(d_xyzq, perm, slot_shift, m_sys, cl_sys,
+                                                        cl_origin, slot_off, counts);
   APO_LAUNCH_CHECK();
   refresh(s);
   bbox_kernel<<<(ncl * 32 + 255) / 256, 256, 0, s>>>(xyzq_s, perm, cl_origin, m_bb_c, m_bb_h,
                                                       counts);
   APO_LAUNCH_CHECK();
   tiles_kernel<false><<<(ncl * 32 + 127) / 128, 128, 0, s>>>(
-      m_d, m_cl_col, m_col_start, m_bb_c, m_bb_h, perm, glo2loc, m_excl_ptr, m_excl_idx,
-      m_tile_count, m_tile_start, m_work_start, tiles, masks, work, counts, 0);
+      m_sys, cl_sys, m_d.tiles_per_work, m_cl_col, m_col_start, m_bb_c, m_bb_h, perm, glo2loc,
+      m_excl_ptr, m_excl_idx, m_tile_count, m_tile_start, m_work_start, tiles, masks, work,
+      counts);
   APO_LAUNCH_CHECK();
   tile_scan_kernel<<<1, kScanThreads, 0, s>>>(m_tile_count, m_tile_start, m_work_start,
                                               counts, m_d.tile_cap, m_d.work_cap,
                                               m_d.tiles_per_work, error);
   APO_LAUNCH_CHECK();
   tiles_kernel<true><<<(ncl * 32 + 127) / 128, 128, 0, s>>>(
-      m_d, m_cl_col, m_col_start, m_bb_c, m_bb_h, perm, glo2loc, m_excl_ptr, m_excl_idx,
-      m_tile_count, m_tile_start, m_work_start, tiles, masks, work, counts, m_sys);
+      m_sys, cl_sys, m_d.tiles_per_work, m_cl_col, m_col_start, m_bb_c, m_bb_h, perm, glo2loc,
+      m_excl_ptr, m_excl_idx, m_tile_count, m_tile_start, m_work_start, tiles, masks, work,
+      counts);
   APO_LAUNCH_CHECK();
 }
 

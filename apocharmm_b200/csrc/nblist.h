@@ -20,16 +20,34 @@
 
 namespace apo {
 
-struct NbListDims {
-  int natom = 0;
-  int ncx = 1, ncy = 1;           // cell columns in x, y
-  float Lx = 0, Ly = 0, Lz = 0;   // box
+// One system of the list: its own box, list radius and x-y columns.  Several
+// independent systems share one list (one set of kernels per rebuild):
+// their columns are numbered consecutively, so clusters, tiles and work
+// items never mix systems and every work item carries its system index.
+struct NbSysDims {
+  float Lx = 0, Ly = 0, Lz = 0;      // box
+  float rlist = 0;                   // list radius (cutnb)
   double Lxd = 0, Lyd = 0, Lzd = 0;  // box, full precision
-  float rlist = 0;                // list radius (cutnb)
+  int ncx = 1, ncy = 1;              // cell columns in x, y
+  int col_off = 0;                   // first global column
+  int atom_off = 0, natom = 0;       // global atom range
+  int pad = 0;
+};
+
+struct NbListDims {
+  int natom = 0;                  // all systems
+  int nsys = 1;
+  int ncol = 0;                   // all systems
   int slot_cap = 0;               // padded sorted slots
   int tile_cap = 0, work_cap = 0;
   int tiles_per_work = 8;
   int sort_cap = 4096;            // max atoms in one column
+};
+
+struct NbListSystem {
+  int natom;
+  double Lx, Ly, Lz;
+  float rlist;
 };
 
 class NeighborList {
@@ -39,10 +57,15 @@ class NeighborList {
   NeighborList(const NeighborList &) = delete;
   NeighborList &operator=(const NeighborList &) = delete;
 
-  // topology-dependent set-up; box/rlist may be changed with set_box
+  // topology-dependent set-up of one system
   void setup(int natom, double Lx, double Ly, double Lz, float rlist,
              const std::vector<int> &excl_ptr, const std::vector<int> &excl_idx,
              const int *d_vdwtype, int tiles_per_work = 8);
+  // several systems, atoms concatenated in order; exclusion CSR and LJ types
+  // in global atom numbering
+  void setup(const std::vector<NbListSystem> &systems, const std::vector<int> &excl_ptr,
+             const std::vector<int> &excl_idx, const int *d_vdwtype, int tiles_per_work = 8);
+  void set_tiles_per_work(int tpw);
   // full rebuild from global-order coordinates (device float4 x,y,z,q)
   void build(const float4 *d_xyzq, cudaStream_t s);
   // refresh the sorted, cluster-local coordinates from the FP64 state
@@ -54,8 +77,8 @@ class NeighborList {
   bool ensure_capacity(const float4 *d_xyzq, cudaStream_t s, double fill = 0.8);
 
   const NbListDims &dims() const { return m_d; }
-  int num_columns() const { return m_ncol; }
-  void set_system_index(int sys) { m_sys = sys; }
+  const std::vector<NbSysDims> &system_dims() const { return m_sys_h; }
+  int num_columns() const { return m_d.ncol; }
   // device arrays
   int *perm = nullptr;          // slot -> atom (-1 = padding)
   int *glo2loc = nullptr;       // atom -> slot
@@ -74,6 +97,8 @@ class NeighborList {
   int4 *work = nullptr;         // (i cluster, first tile, end tile, system)
   int *counts = nullptr;        // [0] slots, [1] tiles, [2] work items
   unsigned *error = nullptr;    // DeviceError bits
+  int *cl_sys = nullptr;        // cluster -> system
+  int *sys_of_atom = nullptr;   // atom -> system
 
   // host copies of the counts (valid after sync_counts)
   int h_counts[3] = {0, 0, 0};
@@ -84,8 +109,9 @@ class NeighborList {
   void alloc();
   void release();
   NbListDims m_d;
-  int m_ncol = 0;
-  int m_sys = 0;
+  std::vector<NbSysDims> m_sys_h;
+  NbSysDims *m_sys = nullptr;   // device copy
+  int *m_col_sys = nullptr;     // column -> system
   const int *m_vdwtype = nullptr;
   const double4 *m_coords = nullptr;
   int *m_excl_ptr = nullptr, *m_excl_idx = nullptr;

@@ -23,6 +23,9 @@ NbSetup make_nb_setup(double Lx, double Ly, double Lz, double kappa, double roff
   s.Lxd = Lx;
   s.Lyd = Ly;
   s.Lzd = Lz;
+  s.Lx_lo = (float)(Lx - (double)(float)Lx);
+  s.Ly_lo = (float)(Ly - (double)(float)Ly);
+  s.Lz_lo = (float)(Lz - (double)(float)Lz);
   s.Lx = (float)Lx;
   s.Ly = (float)Ly;
   s.Lz = (float)Lz;
@@ -99,18 +102,31 @@ __device__ __forceinline__ float erfc_from_exp(float x, float expv) {
   return expv * t * p;
 }
 
-template <bool ENERGY, bool PER_PAIR, bool VIRIAL = false>
+// warp-wide sum of a double, rounded to fixed point, added to *dst by lane 0
+__device__ __forceinline__ void warp_flush(double v, long long *dst, int lane) {
+  long long iv = __double2ll_rn(v * kEnergyScale);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) iv += __shfl_xor_sync(0xffffffffu, iv, o);
+  if (lane == 0 && iv) add_fixed(dst, iv);
+}
+
+template <bool ENERGY, bool PER_PAIR, bool VIRIAL = false, bool MULTI = false>
 __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
   __shared__ float4 sh_xq[kWarps][32];
   __shared__ int sh_t[kWarps][32];
   __shared__ int sh_j[kWarps][32];
   extern __shared__ float2 sh_vdw[];
-  const int T = a.ntype;
-  for (int k = threadIdx.x; k < T * T; k += blockDim.x) sh_vdw[k] = a.vdw[k];
-  __syncthreads();
-
+  int T = a.ntype;
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
+  // one system: the whole table once per block; several systems: one
+  // ntype^2 slice per warp, reloaded when the warp's system changes
+  const int tab_off = MULTI ? wib * kMaxMultiTypes * kMaxMultiTypes : 0;
+  int cur_sys = -1;
+  if (!MULTI) {
+    for (int k = threadIdx.x; k < T * T; k += blockDim.x) sh_vdw[k] = a.vdw[k];
+    __syncthreads();
+  }
   const unsigned lt_mask = (1u << lane) - 1u;
   const int nwork = a.counts[2];
   const int stride = a.stride;
@@ -121,6 +137,13 @@ __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
   for (int w = blockIdx.x * kWarps + wib; w < nwork; w += gridDim.x * kWarps) {
     const int4 wk = a.work[w];
     const NbSetup st = a.setups[wk.w];
+    if (MULTI && wk.w != cur_sys) {  // warp-uniform
+      __syncwarp();
+      T = st.ntype;
+      for (int k = lane; k < T * T; k += 32) sh_vdw[tab_off + k] = a.vdw[st.vdw_off + k];
+      __syncwarp();
+      cur_sys = wk.w;
+    }
     const float4 oi = a.origin[wk.x];
     const int islot = wk.x * kTile + lane;
     const float4 xi = a.xyzq_s[islot];
@@ -146,13 +169,16 @@ __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
 
     for (int t = wk.y; t < wk.z; ++t) {
       const int2 tl = a.tiles[t];
-      // j cluster frame -> i cluster frame: origin difference plus the
-      // periodic image, formed in FP64 and rounded once (|offset| < rlist + 2 cluster edges)
+      // j cluster frame -> i cluster frame: origin difference (exact: both
+      // origins are multiples of 1/64 A) plus the periodic image k L with L
+      // as a two-float sum, so |offset| < rlist + 2 cluster edges carries
+      // about one rounding
       const float4 oj = a.origin[tl.x];
       const int ic = tl.y / 9, ib = (tl.y - 9 * ic) / 3, ia = tl.y - 9 * ic - 3 * ib;
-      const float sx = (float)((double)oj.x - (double)oi.x + (double)(ia - 1) * st.Lxd);
-      const float sy = (float)((double)oj.y - (double)oi.y + (double)(ib - 1) * st.Lyd);
-      const float sz = (float)((double)oj.z - (double)oi.z + (double)(ic - 1) * st.Lzd);
+      const float kx = (float)(ia - 1), ky = (float)(ib - 1), kz = (float)(ic - 1);
+      const float sx = fmaf(kx, st.Lx, oj.x - oi.x) + kx * st.Lx_lo;
+      const float sy = fmaf(ky, st.Ly, oj.y - oi.y) + ky * st.Ly_lo;
+      const float sz = fmaf(kz, st.Lz, oj.z - oi.z) + kz * st.Lz_lo;
       const int jslot = tl.x * kTile + lane;
       float4 xj = a.xyzq_s[jslot];
       xj.x += sx;
@@ -200,7 +226,7 @@ __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
             const float e_el = qq * erfc_v * rinv;
             const float fr_el = -qq * st.two_kappa_sqrtpi * exp_v - e_el;
             // VDW_VFSW (src/CudaDirectForceKernels.cu:263-286)
-            float2 cc = sh_vdw[ti + sh_t[wib][j]];
+            float2 cc = sh_vdw[tab_off + ti + sh_t[wib][j]];
             cc.x = in ? cc.x : 0.f;
             cc.y = in ? cc.y : 0.f;
             const float rinv3 = rinv * rinv2, rinv6 = rinv3 * rinv3;
@@ -272,6 +298,27 @@ __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
 #pragma unroll
       for (int k = 0; k < 6; ++k) dv[k] += (double)vw[k];
     }
+    if (MULTI && ENERGY) {  // energies (and virial) belong to this work item's system
+      long long *es = a.energy + (size_t)wk.w * a.energy_stride;
+      warp_flush(e_elec, es + kEElec, lane);
+      warp_flush(e_vdw, es + kEVdw, lane);
+      e_elec = 0.0;
+      e_vdw = 0.0;
+      if (VIRIAL) {
+        constexpr int kSlotM[6][2] = {{0, 0}, {1, 3}, {2, 6}, {4, 4}, {5, 7}, {8, 8}};
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+          long long iw = __double2ll_rn(dv[k] * kEnergyScale);
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) iw += __shfl_xor_sync(0xffffffffu, iw, o);
+          if (lane == 0 && iw) {
+            add_fixed(es + kNumEnergyTerms + kSlotM[k][0], iw);
+            if (kSlotM[k][1] != kSlotM[k][0]) add_fixed(es + kNumEnergyTerms + kSlotM[k][1], iw);
+          }
+          dv[k] = 0.0;
+        }
+      }
+    }
     if (ivalid) {
       if (PER_PAIR) {
         add_fixed(a.force + islot, (long long)fix);
@@ -284,7 +331,7 @@ __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
       }
     }
   }
-  if (ENERGY) {
+  if (ENERGY && !MULTI) {
     // per-lane sums rounded to fixed point, then integer sums: order-free
     long long ie = __double2ll_rn(e_elec * kEnergyScale);
     long long iv = __double2ll_rn(e_vdw * kEnergyScale);
@@ -298,7 +345,7 @@ __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
       add_fixed(a.energy + kEVdw, iv);
     }
   }
-  if (VIRIAL) {
+  if (VIRIAL && !MULTI) {
     // xx xy xz yy yz zz -> row-major 3x3 (symmetric)
     constexpr int kSlot[6][2] = {{0, 0}, {1, 3}, {2, 6}, {4, 4}, {5, 7}, {8, 8}};
 #pragma unroll
@@ -314,21 +361,22 @@ __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
   }
 }
 
-template <bool E, bool P, bool V = false>
+template <bool E, bool P, bool V = false, bool M = false>
 void launch_t(const NbArgs &a, cudaStream_t s) {
   static int grid = 0;
-  size_t sm = (size_t)a.ntype * a.ntype * sizeof(float2);
+  size_t sm = M ? (size_t)kWarps * kMaxMultiTypes * kMaxMultiTypes * sizeof(float2)
+                : (size_t)a.ntype * a.ntype * sizeof(float2);
   if (!grid) {
     int dev, nsm, per = 0;
     APO_CUDA(cudaGetDevice(&dev));
     APO_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    APO_CUDA(cudaFuncSetAttribute(nb_kernel<E, P, V>,
+    APO_CUDA(cudaFuncSetAttribute(nb_kernel<E, P, V, M>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
-    APO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, nb_kernel<E, P, V>, kThreads,
+    APO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, nb_kernel<E, P, V, M>, kThreads,
                                                            64 * 1024 > sm ? sm : 64 * 1024));
     grid = nsm * (per > 0 ? per : 1);
   }
-  nb_kernel<E, P, V><<<grid, kThreads, sm, s>>>(a);
+  nb_kernel<E, P, V, M><<<grid, kThreads, sm, s>>>(a);
   APO_LAUNCH_CHECK();
 }
 
@@ -349,6 +397,22 @@ void launch_nonbonded(const NbArgs &a, bool energy, bool per_pair, cudaStream_t 
   } else {
     if (energy) launch_t<true, false>(a, s);
     else launch_t<false, false>(a, s);
+  }
+}
+
+void launch_nonbonded_multi(const NbArgs &a, bool energy, bool per_pair, cudaStream_t s,
+                            bool virial) {
+  if (a.energy_stride <= 0 && (energy || virial))
+    throw std::invalid_argument("nonbonded: multi-system energies need an energy stride");
+  if (virial) {
+    if (per_pair) launch_t<true, true, true, true>(a, s);
+    else launch_t<true, false, true, true>(a, s);
+  } else if (energy) {
+    if (per_pair) launch_t<true, true, false, true>(a, s);
+    else launch_t<true, false, false, true>(a, s);
+  } else {
+    if (per_pair) launch_t<false, true, false, true>(a, s);
+    else launch_t<false, false, false, true>(a, s);
   }
 }
 

@@ -9,12 +9,20 @@
 namespace apo {
 
 struct NbSetup {
-  double Lxd, Lyd, Lzd;   // box, full precision (tile frame offsets)
+  double Lxd, Lyd, Lzd;   // box, full precision
   float Lx, Ly, Lz;
+  float Lx_lo, Ly_lo, Lz_lo;  // L - (float)L: the box as a two-float sum
   float roff2, ron2;
   float kappa, kappa2, two_kappa_sqrtpi;
   float k6, k12, dv6, dv12, roffinv3, roffinv6;
+  // LJ tables of this system (multi-system launches): ntype x ntype entries
+  // at vdw + vdw_off (and vdw14 + vdw14_off for the 1-4 pairs)
+  int vdw_off = 0, vdw14_off = 0, ntype = 0, pad = 0;
 };
+
+// largest LJ type count of one system in a multi-system launch (the
+// direct-space kernel keeps one ntype^2 table per warp in shared memory)
+constexpr int kMaxMultiTypes = 16;
 
 NbSetup make_nb_setup(double Lx, double Ly, double Lz, double kappa, double roff,
                       double ron);
@@ -35,6 +43,9 @@ struct NbArgs {
   long long *energy;      // energy slots (elec, vdw used)
   const NbSetup *setups;  // per system (indexed by work item .w)
   long long *virial = nullptr;  // 3x3 internal virial, 2^32 fixed point (virial launches)
+  // multi-system launches: energies (and virial) of system s at
+  // energy + s * energy_stride (virial at + kNumEnergyTerms); 0 = one system
+  int energy_stride = 0;
 };
 
 // per_pair: round every pair contribution to 64-bit fixed point before it is
@@ -45,5 +56,8 @@ struct NbArgs {
 // (implies energy).
 void launch_nonbonded(const NbArgs &a, bool energy, bool per_pair, cudaStream_t s,
                       bool virial = false);
+// every work item's system from its .w, with per-system LJ tables
+void launch_nonbonded_multi(const NbArgs &a, bool energy, bool per_pair, cudaStream_t s,
+                            bool virial = false);
 
 }  // namespace apo

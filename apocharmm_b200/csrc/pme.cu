@@ -249,7 +249,14 @@ template <int ORDER>
 __global__ void __launch_bounds__(128) spread_kernel(const float4 *__restrict__ xyzq,
                                                      const int *__restrict__ counts, PmeDims d,
                                                      int *__restrict__ qgrid,
-                                                     const float4 *__restrict__ origin) {
+                                                     const float4 *__restrict__ origin,
+                                                     const PmeSysArgs *__restrict__ multi = nullptr,
+                                                     const int *__restrict__ cl_sys = nullptr) {
+  if (multi) {  // one block = one 32-slot cluster of one system
+    const PmeSysArgs &A = multi[cl_sys[blockIdx.x]];
+    d = A.d;
+    qgrid = A.qgrid;
+  }
   constexpr int P3 = ORDER * ORDER * ORDER;
   __shared__ int sh_i[3][32];
   __shared__ float sh_q[32];
@@ -310,10 +317,21 @@ __global__ void __launch_bounds__(128) spread_kernel(const float4 *__restrict__ 
 __global__ void __launch_bounds__(kPlaneThreads) plane_fwd_kernel(PmeDims d, int *__restrict__ qgrid,
                                                                   float2 *__restrict__ cgrid,
                                                                   const float2 *__restrict__ twx,
-                                                                  const float2 *__restrict__ twy) {
+                                                                  const float2 *__restrict__ twy,
+                                                                  const PmeSysArgs *__restrict__ multi = nullptr,
+                                                                  const int *__restrict__ plane_sys = nullptr) {
   extern __shared__ float2 buf[];
+  int z = blockIdx.x;
+  if (multi) {
+    const PmeSysArgs &A = multi[plane_sys[blockIdx.x]];
+    d = A.d;
+    qgrid = A.qgrid;
+    cgrid = A.cgrid;
+    twx = A.tw;
+    twy = A.tw + d.nx;
+    z = blockIdx.x - A.plane0;
+  }
   const int nx = d.nx, ny = d.ny, nxc = d.nxc, rowp = nx + 2, h = nx / 2;
-  const int z = blockIdx.x;
   int *plane = qgrid + (size_t)z * nx * ny;
   for (int idx = threadIdx.x; idx < nx * ny; idx += blockDim.x) {
     const int y = idx / nx, x = idx - y * nx;
@@ -359,10 +377,21 @@ __global__ void __launch_bounds__(kPlaneThreads) plane_inv_kernel(PmeDims d,
                                                                   const float2 *__restrict__ cgrid,
                                                                   float *__restrict__ phi,
                                                                   const float2 *__restrict__ twx,
-                                                                  const float2 *__restrict__ twy) {
+                                                                  const float2 *__restrict__ twy,
+                                                                  const PmeSysArgs *__restrict__ multi = nullptr,
+                                                                  const int *__restrict__ plane_sys = nullptr) {
   extern __shared__ float2 buf[];
+  int z = blockIdx.x;
+  if (multi) {
+    const PmeSysArgs &A = multi[plane_sys[blockIdx.x]];
+    d = A.d;
+    cgrid = A.cgrid;
+    phi = A.phi;
+    twx = A.tw;
+    twy = A.tw + d.nx;
+    z = blockIdx.x - A.plane0;
+  }
   const int nx = d.nx, ny = d.ny, nxc = d.nxc, rowp = nx + 2, h = nx / 2;
-  const int z = blockIdx.x;
   const float2 *in = cgrid + (size_t)z * ny * nxc;
   for (int idx = threadIdx.x; idx < ny * nxc; idx += blockDim.x) buf[idx] = in[idx];
   __syncthreads();
@@ -407,13 +436,27 @@ __global__ void __launch_bounds__(kPencilThreads) pencil_kernel(PmeDims d, float
                                                                 const float *__restrict__ prefac,
                                                                 const double *__restrict__ prefac_d,
                                                                 long long *__restrict__ energy,
-                                                                long long *__restrict__ virial = nullptr) {
+                                                                long long *__restrict__ virial = nullptr,
+                                                                const PmeSysArgs *__restrict__ multi = nullptr,
+                                                                const int *__restrict__ pencil_sys = nullptr) {
   __shared__ float2 buf[256 * kPencilTX];
   __shared__ double sh_e[kPencilThreads / 32];
   __shared__ double sh_v[6][kPencilThreads / 32];
+  int blk = blockIdx.x;
+  if (multi) {
+    const PmeSysArgs &A = multi[pencil_sys[blockIdx.x]];
+    d = A.d;
+    cgrid = A.cgrid;
+    twz = A.tw + d.nx + d.ny;
+    prefac = A.prefac;
+    prefac_d = A.prefac_d;
+    energy = A.energy;
+    virial = A.virial;
+    blk = blockIdx.x - A.pencil0;
+  }
   const int nx = d.nx, ny = d.ny, nz = d.nz, nxc = d.nxc;
   const int tiles_x = (nxc + kPencilTX - 1) / kPencilTX;
-  const int py = blockIdx.x / tiles_x, x0 = (blockIdx.x - py * tiles_x) * kPencilTX;
+  const int py = blk / tiles_x, x0 = (blk - py * tiles_x) * kPencilTX;
   for (int idx = threadIdx.x; idx < nz * kPencilTX; idx += blockDim.x) {
     const int zz = idx / kPencilTX, xt = idx - zz * kPencilTX, kx = x0 + xt;
     buf[idx] = kx < nxc ? cgrid[((size_t)zz * ny + py) * nxc + kx] : make_float2(0.f, 0.f);
@@ -501,7 +544,14 @@ __global__ void __launch_bounds__(256) gather_kernel(const float4 *__restrict__ 
                                                      const int *__restrict__ counts, PmeDims d,
                                                      const float *__restrict__ phi,
                                                      long long *__restrict__ force, int stride,
-                                                     const float4 *__restrict__ origin) {
+                                                     const float4 *__restrict__ origin,
+                                                     const PmeSysArgs *__restrict__ multi = nullptr,
+                                                     const int *__restrict__ cl_sys = nullptr) {
+  if (multi) {  // one block = one 32-slot cluster of one system
+    const PmeSysArgs &A = multi[cl_sys[blockIdx.x]];
+    d = A.d;
+    phi = A.phi;
+  }
   const int nslot = counts[0];
   const int s = blockIdx.x * 32 + (threadIdx.x >> 3);
   const int sub = threadIdx.x & 7;
@@ -785,6 +835,175 @@ void Pme::compute(const float4 *xyzq_s, const int *counts, long long *force, int
   convolve(energy, calc_energy, fp64, s, virial);
   backward(s);
   gather(xyzq_s, counts, force, stride, s, origin);
+}
+
+}  // namespace apo
+
+// ---------------------------------------------------------------------------
+// Many systems
+// ---------------------------------------------------------------------------
+
+namespace apo {
+
+PmeMulti::~PmeMulti() { release(); }
+
+void PmeMulti::release() {
+  for (void *p : {(void *)m_args, (void *)m_plane_sys, (void *)m_pencil_sys, (void *)m_q,
+                  (void *)m_c, (void *)m_phi, (void *)m_tw, (void *)m_pf, (void *)m_pfd})
+    if (p) cudaFree(p);
+  m_args = nullptr;
+  m_plane_sys = m_pencil_sys = nullptr;
+  m_q = nullptr;
+  m_c = nullptr;
+  m_phi = nullptr;
+  m_tw = nullptr;
+  m_pf = nullptr;
+  m_pfd = nullptr;
+}
+
+void PmeMulti::setup(const std::vector<PmeSystemSpec> &systems, int order, long long *energy,
+                     int energy_stride, int max_slots) {
+  if (systems.empty()) throw std::invalid_argument("PmeMulti: no systems");
+  if (order != 4 && order != 6 && order != 8)
+    throw std::invalid_argument("PME spline order must be 4, 6 or 8");
+  release();
+  m_host.clear();
+  m_order = order;
+  m_max_slots = max_slots;
+  size_t q = 0, c = 0, t = 0;
+  std::vector<int> plane_sys, pencil_sys;
+  std::vector<float2> tw;
+  std::vector<double> pd;
+  m_plane_smem = 0;
+  for (size_t k = 0; k < systems.size(); ++k) {
+    const PmeSystemSpec &y = systems[k];
+    if (y.nx % 2 || y.ny % 2 || y.nz % 2 || y.nx <= 0 || y.ny <= 0 || y.nz <= 0)
+      throw std::invalid_argument("PME grid dimensions must be even");
+    if (y.nx > 256 || y.ny > 256 || y.nz > 256)
+      throw std::invalid_argument("PME grid dimensions above 256 are not supported");
+    const size_t plane_bytes = (size_t)(y.ny / 2) * (y.nx + 2) * sizeof(float2);
+    if (plane_bytes > 227 * 1024) throw std::invalid_argument("PME plane does not fit in shared memory");
+    m_plane_smem = std::max(m_plane_smem, plane_bytes);
+    PmeSysArgs A{};
+    A.d.nx = y.nx;
+    A.d.ny = y.ny;
+    A.d.nz = y.nz;
+    A.d.nxc = y.nx / 2 + 1;
+    A.d.order = order;
+    A.d.Lx = (float)y.Lx;
+    A.d.Ly = (float)y.Ly;
+    A.d.Lz = (float)y.Lz;
+    A.d.kappa = (float)y.kappa;
+    A.d.ax = Pme::plan_axis(y.nx);
+    A.d.ay = Pme::plan_axis(y.ny);
+    A.d.az = Pme::plan_axis(y.nz);
+    // offsets for now; turned into pointers once the buffers exist
+    A.qgrid = reinterpret_cast<int *>(q);
+    A.phi = reinterpret_cast<float *>(q);
+    A.cgrid = reinterpret_cast<float2 *>(c);
+    A.tw = reinterpret_cast<const float2 *>(t);
+    A.prefac = reinterpret_cast<const float *>(t);
+    A.prefac_d = reinterpret_cast<const double *>(t);
+    A.energy = energy + k * (size_t)energy_stride;
+    A.virial = A.energy + kNumEnergyTerms;
+    A.plane0 = m_planes;
+    A.pencil0 = m_pencils;
+    const int tiles_x = (A.d.nxc + kPencilTX - 1) / kPencilTX;
+    for (int z = 0; z < y.nz; ++z) plane_sys.push_back((int)k);
+    for (int b = 0; b < tiles_x * y.ny; ++b) pencil_sys.push_back((int)k);
+    m_planes += y.nz;
+    m_pencils += tiles_x * y.ny;
+    q += (size_t)y.nx * y.ny * y.nz;
+    c += (size_t)y.nz * y.ny * A.d.nxc;
+    t += (size_t)y.nx + y.ny + y.nz;
+    for (int n : {y.nx, y.ny, y.nz})
+      for (int j = 0; j < n; ++j) {
+        const double a = 2.0 * M_PI * j / n;
+        tw.push_back(make_float2((float)std::cos(a), (float)-std::sin(a)));
+      }
+    std::vector<double> tmp;
+    for (int n : {y.nx, y.ny, y.nz}) {
+      bspline_moduli(n, order, tmp);
+      pd.insert(pd.end(), tmp.begin(), tmp.end());
+    }
+    m_host.push_back(A);
+  }
+  APO_CUDA(cudaMalloc(&m_q, q * sizeof(int)));
+  APO_CUDA(cudaMalloc(&m_phi, q * sizeof(float)));
+  APO_CUDA(cudaMalloc(&m_c, c * sizeof(float2)));
+  APO_CUDA(cudaMalloc(&m_tw, t * sizeof(float2)));
+  APO_CUDA(cudaMalloc(&m_pf, t * sizeof(float)));
+  APO_CUDA(cudaMalloc(&m_pfd, t * sizeof(double)));
+  APO_CUDA(cudaMemset(m_q, 0, q * sizeof(int)));
+  std::vector<float> pf(pd.begin(), pd.end());
+  APO_CUDA(cudaMemcpy(m_tw, tw.data(), t * sizeof(float2), cudaMemcpyHostToDevice));
+  APO_CUDA(cudaMemcpy(m_pf, pf.data(), t * sizeof(float), cudaMemcpyHostToDevice));
+  APO_CUDA(cudaMemcpy(m_pfd, pd.data(), t * sizeof(double), cudaMemcpyHostToDevice));
+  for (PmeSysArgs &A : m_host) {
+    const size_t qo = reinterpret_cast<size_t>(A.qgrid), co = reinterpret_cast<size_t>(A.cgrid),
+                 to = reinterpret_cast<size_t>(A.tw);
+    A.qgrid = m_q + qo;
+    A.phi = m_phi + qo;
+    A.cgrid = m_c + co;
+    A.tw = m_tw + to;
+    A.prefac = m_pf + to;
+    A.prefac_d = m_pfd + to;
+  }
+  APO_CUDA(cudaMalloc(&m_args, m_host.size() * sizeof(PmeSysArgs)));
+  APO_CUDA(cudaMemcpy(m_args, m_host.data(), m_host.size() * sizeof(PmeSysArgs),
+                      cudaMemcpyHostToDevice));
+  APO_CUDA(cudaMalloc(&m_plane_sys, plane_sys.size() * sizeof(int)));
+  APO_CUDA(cudaMemcpy(m_plane_sys, plane_sys.data(), plane_sys.size() * sizeof(int),
+                      cudaMemcpyHostToDevice));
+  APO_CUDA(cudaMalloc(&m_pencil_sys, pencil_sys.size() * sizeof(int)));
+  APO_CUDA(cudaMemcpy(m_pencil_sys, pencil_sys.data(), pencil_sys.size() * sizeof(int),
+                      cudaMemcpyHostToDevice));
+  APO_CUDA(cudaFuncSetAttribute(plane_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                227 * 1024));
+  APO_CUDA(cudaFuncSetAttribute(plane_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                227 * 1024));
+}
+
+void PmeMulti::compute(const float4 *xyzq_s, const float4 *origin, const int *cl_sys,
+                       const int *counts, long long *force, int stride, bool calc_energy,
+                       bool calc_virial, bool fp64, cudaStream_t s) {
+  const PmeDims &d0 = m_host[0].d;
+  const int blocks = (m_max_slots + 31) / 32;
+  switch (m_order) {
+    case 4: spread_kernel<4><<<blocks, 128, 0, s>>>(xyzq_s, counts, d0, nullptr, origin, m_args, cl_sys); break;
+    case 6: spread_kernel<6><<<blocks, 128, 0, s>>>(xyzq_s, counts, d0, nullptr, origin, m_args, cl_sys); break;
+    case 8: spread_kernel<8><<<blocks, 128, 0, s>>>(xyzq_s, counts, d0, nullptr, origin, m_args, cl_sys); break;
+  }
+  APO_LAUNCH_CHECK();
+  plane_fwd_kernel<<<m_planes, kPlaneThreads, m_plane_smem, s>>>(d0, nullptr, nullptr, nullptr,
+                                                                  nullptr, m_args, m_plane_sys);
+  APO_LAUNCH_CHECK();
+  if (calc_virial) {
+    if (fp64)
+      pencil_kernel<true, double, true><<<m_pencils, kPencilThreads, 0, s>>>(d0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, m_args, m_pencil_sys);
+    else
+      pencil_kernel<true, float, true><<<m_pencils, kPencilThreads, 0, s>>>(d0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, m_args, m_pencil_sys);
+  } else if (calc_energy) {
+    if (fp64)
+      pencil_kernel<true, double><<<m_pencils, kPencilThreads, 0, s>>>(d0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, m_args, m_pencil_sys);
+    else
+      pencil_kernel<true, float><<<m_pencils, kPencilThreads, 0, s>>>(d0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, m_args, m_pencil_sys);
+  } else {
+    if (fp64)
+      pencil_kernel<false, double><<<m_pencils, kPencilThreads, 0, s>>>(d0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, m_args, m_pencil_sys);
+    else
+      pencil_kernel<false, float><<<m_pencils, kPencilThreads, 0, s>>>(d0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, m_args, m_pencil_sys);
+  }
+  APO_LAUNCH_CHECK();
+  plane_inv_kernel<<<m_planes, kPlaneThreads, m_plane_smem, s>>>(d0, nullptr, nullptr, nullptr,
+                                                                  nullptr, m_args, m_plane_sys);
+  APO_LAUNCH_CHECK();
+  switch (m_order) {
+    case 4: gather_kernel<4><<<blocks, 256, 0, s>>>(xyzq_s, counts, d0, nullptr, force, stride, origin, m_args, cl_sys); break;
+    case 6: gather_kernel<6><<<blocks, 256, 0, s>>>(xyzq_s, counts, d0, nullptr, force, stride, origin, m_args, cl_sys); break;
+    case 8: gather_kernel<8><<<blocks, 256, 0, s>>>(xyzq_s, counts, d0, nullptr, force, stride, origin, m_args, cl_sys); break;
+  }
+  APO_LAUNCH_CHECK();
 }
 
 }  // namespace apo

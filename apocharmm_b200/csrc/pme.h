@@ -42,6 +42,21 @@ struct PmeDims {
   FftAxis ax, ay, az;
 };
 
+// One system of a multi-system PME: its grid dimensions and its slices of
+// the concatenated buffers.
+struct PmeSysArgs {
+  PmeDims d;
+  int *qgrid;
+  float2 *cgrid;
+  float *phi;
+  const float2 *tw;          // twiddles: x (nx), y (ny), z (nz)
+  const float *prefac;       // B-spline moduli 1/|b|^2: x, y, z
+  const double *prefac_d;
+  long long *energy;         // this system's energy slots
+  long long *virial;         // this system's virial slots
+  int plane0, pencil0;       // first plane / pencil block of this system
+};
+
 class Pme {
  public:
   Pme() = default;
@@ -83,6 +98,44 @@ class Pme {
   float2 *m_tw = nullptr;   // twiddles: x (nx), y (ny), z (nz) consecutive
   float *m_prefac = nullptr;  // B-spline moduli 1/|b|^2: x, y, z consecutive
   double *m_prefac_d = nullptr;
+};
+
+// Reciprocal space of many independent systems (one spline order) with one
+// launch per stage: blocks map to (system, plane) or (system, pencil)
+// through tables, and spread/gather blocks (one 32-slot cluster each) take
+// the cluster's system from the neighbour list.
+struct PmeSystemSpec {
+  int nx, ny, nz;
+  double kappa, Lx, Ly, Lz;
+};
+
+class PmeMulti {
+ public:
+  PmeMulti() = default;
+  ~PmeMulti();
+  PmeMulti(const PmeMulti &) = delete;
+  PmeMulti &operator=(const PmeMulti &) = delete;
+  // energy (+ virial) slots of system s start at energy + s * energy_stride
+  void setup(const std::vector<PmeSystemSpec> &systems, int order, long long *energy,
+             int energy_stride, int max_slots);
+  void compute(const float4 *xyzq_s, const float4 *origin, const int *cl_sys, const int *counts,
+               long long *force, int stride, bool calc_energy, bool calc_virial,
+               bool fp64_influence, cudaStream_t s);
+  int num_systems() const { return (int)m_host.size(); }
+
+ private:
+  void release();
+  std::vector<PmeSysArgs> m_host;
+  PmeSysArgs *m_args = nullptr;
+  int *m_plane_sys = nullptr, *m_pencil_sys = nullptr;
+  int m_planes = 0, m_pencils = 0, m_order = 4, m_max_slots = 0;
+  size_t m_plane_smem = 0;
+  int *m_q = nullptr;
+  float2 *m_c = nullptr;
+  float *m_phi = nullptr;
+  float2 *m_tw = nullptr;
+  float *m_pf = nullptr;
+  double *m_pfd = nullptr;
 };
 
 }  // namespace apo

@@ -293,6 +293,121 @@ def solvated_chain(n_atoms: int = 23558, L: float = 62.23, n_beads: int = 2489,
     # waters: candidate lattice sites away from the chain
     n_edge = int(math.ceil((n_water * 1.6) ** (1.0 / 3.0)))
     sites = _lattice_sites(L, n_edge)
+    # distance to the nearest bead (minimum image) via a periodic KD-tree
+    from scipy.spatial import cKDTree
+
+    def _wrap(p):
+        w = np.mod(p + L / 2, L)
+        return np.where(w >= L, w - L, w)
+    dist, _ = cKDTree(_wrap(chain), boxsize=L).query(_wrap(sites), k=1)
+    keep = dist >= 3.0
+    sites = sites[keep]
+    pos = _place_waters(rng, sites, jitter, L)
+    bonds, angles, types, names, resn, resi, segs = _water_topology(n_molecules)
+    p = _water_params()
+    n = 3 * n_molecules
+    return System(
+        name=name, box=(L, L, L), pos=pos,
+        charge=np.tile([Q_O, Q_H, Q_H], n_molecules).astype(np.float64),
+        mass=np.tile([M_O, M_H, M_H], n_molecules).astype(np.float64),
+        atom_type=types, atom_name=names, res_name=resn, res_id=resi, seg_id=segs,
+        bonds=bonds.astype(np.int64), angles=angles.astype(np.int64),
+        dihedrals=np.zeros((0, 4), np.int64), impropers=np.zeros((0, 4), np.int64),
+        masses_by_type=p["masses_by_type"], bond_params=p["bond_params"],
+        angle_params=p["angle_params"], dihedral_params={}, improper_params={},
+        lj_params=p["lj"], lj14_params={},
+    )
+
+
+def _self_avoiding_chain(rng, n_beads: int, L: float, bond: float = 1.53,
+                         theta0: float = 111.0, min_dist: float = 2.6,
+                         margin: float = 1.5) -> np.ndarray:
+    """Confined self-avoiding walk with fixed bond length and angle.
+
+    Beads stay inside [-L/2+margin, L/2-margin]^3 so the molecule never crosses
+    the periodic boundary; non-neighbour beads (|i-j|>3) keep min_dist apart.
+    """
+    half = L / 2 - margin
+    cell = min_dist
+    ncell = max(1, int(L // cell))
+    grid: Dict[Tuple[int, int, int], List[int]] = {}
+
+    def key(p):
+        return tuple(((p + L / 2) // cell).astype(int) % ncell)
+
+    def clash(p, upto):
+        k = key(p)
+        for dx in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dz in (-1, 0, 1):
+                    kk = ((k[0] + dx) % ncell, (k[1] + dy) % ncell, (k[2] + dz) % ncell)
+                    for j in grid.get(kk, ()):
+                        if j < upto - 3 and np.sum((pos[j] - p) ** 2) < min_dist ** 2:
+                            return True
+        return False
+
+    pos = np.zeros((n_beads, 3))
+    pos[0] = rng.uniform(-half / 2, half / 2, 3)
+    d = rng.normal(size=3)
+    pos[1] = pos[0] + bond * d / np.linalg.norm(d)
+    for b in (0, 1):
+        grid.setdefault(key(pos[b]), []).append(b)
+    ct = math.cos(math.radians(180.0 - theta0))
+    st = math.sin(math.radians(180.0 - theta0))
+    i = 2
+    fails = 0
+    while i < n_beads:
+        u = pos[i - 1] - pos[i - 2]
+        u /= np.linalg.norm(u)
+        a = np.cross(u, [1.0, 0.0, 0.0])
+        if np.linalg.norm(a) < 1e-3:
+            a = np.cross(u, [0.0, 1.0, 0.0])
+        a /= np.linalg.norm(a)
+        b2 = np.cross(u, a)
+        ok = False
+        for _ in range(40):
+            phi = rng.uniform(0, 2 * np.pi)
+            d = ct * u + st * (math.cos(phi) * a + math.sin(phi) * b2)
+            p = pos[i - 1] + bond * d
+            if np.all(np.abs(p) < half) and not clash(p, i):
+                ok = True
+                break
+        if ok:
+            pos[i] = p
+            grid.setdefault(key(p), []).append(i)
+            i += 1
+            fails = 0
+        else:
+            # back-track a few beads
+            fails += 1
+            nb = min(i - 2, 2 + fails)
+            for j in range(i - nb, i):
+                grid[key(pos[j])].remove(j)
+            i -= nb
+    return pos
+
+
+def solvated_chain(n_atoms: int = 23558, L: float = 62.23, n_beads: int = 2489,
+                   seed: int = 1234, n_types: int = 8, name: str = "chain") -> System:
+    """Seeded bead chain (bonds, angles, n=3 dihedrals, 1-4 scaled LJ) in TIP3P."""
+    rng = np.random.default_rng(seed)
+    n_water = (n_atoms - n_beads) // 3
+    if n_beads + 3 * n_water != n_atoms:
+        raise ValueError("n_atoms - n_beads must be a multiple of 3")
+    chain = _self_avoiding_chain(rng, n_beads, L)
+    # LJ types: eps in [0.05, 0.2], rmin/2 in [1.3, 2.1]; 1-4 values scaled
+    types = [f"CB{k + 1}" for k in range(n_types)]
+    eps = np.linspace(0.05, 0.2, n_types)
+    rmh = np.linspace(1.3, 2.1, n_types)
+    perm = rng.permutation(n_types)
+    lj = {types[k]: (-float(eps[perm[k]]), float(rmh[k])) for k in range(n_types)}
+    lj14 = {t: (0.5 * lj[t][0], lj[t][1] - 0.1) for t in types}
+    bead_type = [types[k] for k in rng.integers(0, n_types, n_beads)]
+    q = rng.uniform(-0.5, 0.5, n_beads)
+    q -= q.mean()
+    # waters: candidate lattice sites away from the chain
+    n_edge = int(math.ceil((n_water * 1.6) ** (1.0 / 3.0)))
+    sites = _lattice_sites(L, n_edge)
     # distance to nearest bead (minimum image) via a coarse cell search
     keep = np.ones(sites.shape[0], bool)
     cell = 3.0
@@ -393,6 +508,29 @@ def config_large_water(seed: int = 77) -> System:
     s.settings = dict(kappa=0.34, nfft=(216, 216, 216), order=4, ctofnb=10.0,
                       ctonnb=8.0, cutnb=11.5, dt_ps=0.002)
     return s
+
+
+def batch_system(seed: int, n_atoms: int) -> System:
+    """One system of the many-system workload: a bead chain of ~10 % of the
+    atoms in TIP3P, the cubic box sized to 0.997 g/cm^3, PME grid spacing at
+    most 1 A rounded up to an FFT-friendly size, spline order 4, cutoff 10 A
+    (switch 8-10 A, list 12 A)."""
+    n_beads = max(30, int(round(0.1 * n_atoms)))
+    n_beads += (n_atoms - n_beads) % 3          # the rest is whole waters
+    masses = n_beads * 12.011 + (n_atoms - n_beads) // 3 * (15.9994 + 2 * 1.008)
+    L = (masses / (0.997 / 1.66053906660)) ** (1.0 / 3.0)
+    s = solvated_chain(n_atoms=n_atoms, L=L, n_beads=n_beads, seed=seed,
+                       name=f"batch{seed}")
+    n = fft_friendly(int(math.ceil(L)))
+    s.settings = dict(kappa=0.34, nfft=(n, n, n), order=4, ctofnb=10.0, ctonnb=8.0,
+                      cutnb=12.0, dt_ps=0.002)
+    return s
+
+
+def batch_sizes(n_systems: int = 256, lo: int = 3000, hi: int = 30000, seed: int = 99):
+    """Atom counts log-uniform in [lo, hi], seeded."""
+    rng = np.random.default_rng(seed)
+    return [int(v) for v in np.exp(rng.uniform(math.log(lo), math.log(hi), n_systems))]
 
 
 def fft_friendly(n: int) -> int:

@@ -100,3 +100,19 @@ def test_stream_file_with_topology_block(tmp_path):
                  "NONBONDED nbxmod 5 atom cdiel -\ncutnb 14.0\nHT 0.0 -0.046 0.2245\n"
                  "OT 0.0 -0.1521 1.7682\nEND\n")
     api.CharmmParameters(str(p))
+
+
+def test_batch_handle_errors_without_gpu():
+    """Batch creation and argument checks need no device."""
+    import ctypes
+    from apocharmm_b200._lib import lib
+    L = lib()
+    h = ctypes.c_void_p()
+    assert L.apo_batch_create(ctypes.byref(h), 5, 8, 0) == 1           # bad spline order
+    assert not h.value
+    assert L.apo_batch_create(ctypes.byref(h), 4, 8, 0) == 0
+    n = ctypes.c_int(-1)
+    assert L.apo_batch_get_num_systems(ctypes.byref(n), h) == 0 and n.value == 0
+    assert L.apo_batch_propagate(h, 10) == 4                             # not initialised
+    assert L.apo_batch_initialize(h) == 1                                # no systems
+    L.apo_batch_destroy(h)
