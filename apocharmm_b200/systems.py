@@ -216,32 +216,47 @@ def _self_avoiding_chain(rng, n_beads: int, L: float, bond: float = 1.53,
     cell = min_dist
     ncell = max(1, int(L // cell))
     grid: Dict[Tuple[int, int, int], List[int]] = {}
+    md2 = min_dist ** 2
+    hl = L / 2
 
     def key(p):
-        return tuple(((p + L / 2) // cell).astype(int) % ncell)
+        return (int((p[0] + hl) // cell) % ncell, int((p[1] + hl) // cell) % ncell,
+                int((p[2] + hl) // cell) % ncell)
 
     def clash(p, upto):
         k = key(p)
+        px, py, pz = float(p[0]), float(p[1]), float(p[2])
         for dx in (-1, 0, 1):
             for dy in (-1, 0, 1):
                 for dz in (-1, 0, 1):
                     kk = ((k[0] + dx) % ncell, (k[1] + dy) % ncell, (k[2] + dz) % ncell)
                     for j in grid.get(kk, ()):
-                        if j < upto - 3 and np.sum((pos[j] - p) ** 2) < min_dist ** 2:
-                            return True
+                        if j < upto - 3:
+                            q = posl[j]
+                            ex, ey, ez = q[0] - px, q[1] - py, q[2] - pz
+                            if ex * ex + ey * ey + ez * ez < md2:
+                                return True
         return False
 
     pos = np.zeros((n_beads, 3))
+    posl = [None] * n_beads             # the same positions as Python floats
+    # a walk that keeps back-tracking in a dead end is started afresh
+    limit = 20 * n_beads + 10000
+    iters = 0
     pos[0] = rng.uniform(-half / 2, half / 2, 3)
     d = rng.normal(size=3)
     pos[1] = pos[0] + bond * d / np.linalg.norm(d)
     for b in (0, 1):
+        posl[b] = (float(pos[b][0]), float(pos[b][1]), float(pos[b][2]))
         grid.setdefault(key(pos[b]), []).append(b)
     ct = math.cos(math.radians(180.0 - theta0))
     st = math.sin(math.radians(180.0 - theta0))
     i = 2
     fails = 0
     while i < n_beads:
+        iters += 1
+        if iters > limit:
+            return _self_avoiding_chain(rng, n_beads, L, bond, theta0, min_dist, margin)
         u = pos[i - 1] - pos[i - 2]
         u /= np.linalg.norm(u)
         a = np.cross(u, [1.0, 0.0, 0.0])
@@ -259,6 +274,7 @@ def _self_avoiding_chain(rng, n_beads: int, L: float, bond: float = 1.53,
                 break
         if ok:
             pos[i] = p
+            posl[i] = (float(p[0]), float(p[1]), float(p[2]))
             grid.setdefault(key(p), []).append(i)
             i += 1
             fails = 0
@@ -331,32 +347,47 @@ def _self_avoiding_chain(rng, n_beads: int, L: float, bond: float = 1.53,
     cell = min_dist
     ncell = max(1, int(L // cell))
     grid: Dict[Tuple[int, int, int], List[int]] = {}
+    md2 = min_dist ** 2
+    hl = L / 2
 
     def key(p):
-        return tuple(((p + L / 2) // cell).astype(int) % ncell)
+        return (int((p[0] + hl) // cell) % ncell, int((p[1] + hl) // cell) % ncell,
+                int((p[2] + hl) // cell) % ncell)
 
     def clash(p, upto):
         k = key(p)
+        px, py, pz = float(p[0]), float(p[1]), float(p[2])
         for dx in (-1, 0, 1):
             for dy in (-1, 0, 1):
                 for dz in (-1, 0, 1):
                     kk = ((k[0] + dx) % ncell, (k[1] + dy) % ncell, (k[2] + dz) % ncell)
                     for j in grid.get(kk, ()):
-                        if j < upto - 3 and np.sum((pos[j] - p) ** 2) < min_dist ** 2:
-                            return True
+                        if j < upto - 3:
+                            q = posl[j]
+                            ex, ey, ez = q[0] - px, q[1] - py, q[2] - pz
+                            if ex * ex + ey * ey + ez * ez < md2:
+                                return True
         return False
 
     pos = np.zeros((n_beads, 3))
+    posl = [None] * n_beads             # the same positions as Python floats
+    # a walk that keeps back-tracking in a dead end is started afresh
+    limit = 20 * n_beads + 10000
+    iters = 0
     pos[0] = rng.uniform(-half / 2, half / 2, 3)
     d = rng.normal(size=3)
     pos[1] = pos[0] + bond * d / np.linalg.norm(d)
     for b in (0, 1):
+        posl[b] = (float(pos[b][0]), float(pos[b][1]), float(pos[b][2]))
         grid.setdefault(key(pos[b]), []).append(b)
     ct = math.cos(math.radians(180.0 - theta0))
     st = math.sin(math.radians(180.0 - theta0))
     i = 2
     fails = 0
     while i < n_beads:
+        iters += 1
+        if iters > limit:
+            return _self_avoiding_chain(rng, n_beads, L, bond, theta0, min_dist, margin)
         u = pos[i - 1] - pos[i - 2]
         u /= np.linalg.norm(u)
         a = np.cross(u, [1.0, 0.0, 0.0])
@@ -374,6 +405,7 @@ def _self_avoiding_chain(rng, n_beads: int, L: float, bond: float = 1.53,
                 break
         if ok:
             pos[i] = p
+            posl[i] = (float(p[0]), float(p[1]), float(p[2]))
             grid.setdefault(key(p), []).append(i)
             i += 1
             fails = 0

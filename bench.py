@@ -235,6 +235,184 @@ def run_reference_arm(args):
     return 0
 
 
+def _gen_batch_system(arg):
+    """Process-pool worker: one system of the many-system workload."""
+    seed, n_atoms = arg
+    sys.path.insert(0, ROOT)
+    from apocharmm_b200.systems import batch_system
+    return batch_system(seed, n_atoms)
+
+
+def run_batch(args):
+    """Many-system workload: seeded systems (bead chain + TIP3P, atom counts
+    log-uniform in 3,000-30,000, boxes at 0.997 g/cm^3, PME spacing <= 1 A,
+    order 4, cutoff 10 A, Langevin 300 K, dt 2 fs, SETTLE) advanced together
+    by the batch engine, against the same systems stepped one at a time in
+    the plain form on the same GPU.  Both are timed with CUDA events over
+    list-update segments; aggregate ns/day = simulated time of all systems
+    per wall day."""
+    import multiprocessing as mp
+
+    import numpy as np
+    rank, world, local = dist_env()
+    t_start = time.perf_counter()
+
+    def log(msg):
+        print(f"[batch {time.perf_counter() - t_start:7.1f} s] {msg}", file=sys.stderr, flush=True)
+
+    from apocharmm_b200.systems import batch_sizes
+    sizes = batch_sizes(args.systems)
+    with mp.get_context("spawn").Pool(min(len(sizes), os.cpu_count() or 1)) as pool:
+        systems = pool.map(_gen_batch_system, [(1000 + k, n) for k, n in enumerate(sizes)],
+                           chunksize=1)
+    t_gen = time.perf_counter() - t_start
+    log(f"generated {len(systems)} systems, {sum(s.n_atoms for s in systems)} atoms")
+    import torch
+    torch.cuda.set_device(local)
+    from apocharmm_b200 import api
+    work = tempfile.mkdtemp(prefix="apo_batch_")
+    seeds = [5000 + k for k in range(len(systems))]
+    b = api.batch_from_systems(systems, work, seeds=seeds, tiles_per_work=8,
+                               precise=args.precise)
+    log("batch initialised")
+    waters = [api.water_indices(s) for s in systems]
+    xs = api.relax_batch(b, waters, iterations=RELAX_ITERATIONS, max_step=RELAX_MAX_STEP)
+    log("relaxed")
+    b.assignVelocities(300.0)
+    b.setLangevin(DT_PS, 1.0, 300.0, 777)
+    tpw = b.autotune(SEG, [4, 8, 12, 16])
+    log(f"autotuned: {tpw} tiles per work item")
+    stream = torch.cuda.ExternalStream(b.getStream())
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    for _ in range(args.warmup):
+        b.propagate(SEG)
+    torch.cuda.synchronize()
+    seg_ms = []
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            b.propagate(SEG)
+            e1.record(stream)
+            e1.synchronize()
+            seg_ms.append(e0.elapsed_time(e1))
+    n_sys = len(systems)
+    value = ns_per_day(args.steps * SEG * n_sys, sum(seg_ms) * 1e-3)
+    log(f"timed: {sum(seg_ms) / args.steps:.2f} ms per segment, {value:.1f} ns/day")
+    # end to end through the C ABI: all coordinates and velocities up and down per segment
+    ntot = sum(s.n_atoms for s in systems)
+    hx = torch.empty((ntot, 3), dtype=torch.float64, pin_memory=True)
+    hv = torch.empty((ntot, 3), dtype=torch.float64, pin_memory=True)
+    hx.numpy()[:] = b.getCoordinates(-1)
+    hv.numpy()[:] = b.getVelocities(-1)
+    iters = max(3, args.steps // 2)
+    t0 = time.perf_counter()
+    for _ in range(iters):
+        api.call("apo_batch_set_coordinates", b.handle, api._i(-1), api._vp(hx.data_ptr()),
+                 api._sz(3 * ntot))
+        api.call("apo_batch_set_velocities", b.handle, api._i(-1), api._vp(hv.data_ptr()),
+                 api._sz(3 * ntot))
+        b.propagate(SEG)
+        api.call("apo_batch_get_coordinates", api._vp(hx.data_ptr()), api._sz(3 * ntot), b.handle,
+                 api._i(-1))
+        api.call("apo_batch_get_velocities", api._vp(hv.data_ptr()), api._sz(3 * ntot), b.handle,
+                 api._i(-1))
+    e2e_s = time.perf_counter() - t0
+    log("end to end done")
+    # force error against FP64 on a sample of systems, batch and single engine
+    sample = sorted({0, n_sys // 3, 2 * n_sys // 3, n_sys - 1})
+    b.calculateForces(False, False)
+    errs, one_errs = [], []
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        for k in sample:
+            s = systems[k]
+            st = s.settings
+            Eo, Go = oracle.Oracle(s, st["kappa"], st["ctofnb"], st["ctonnb"], st["nfft"],
+                                   st["order"]).evaluate(pos=b.getCoordinates(k))
+            F = b.getForces(k)
+            errs.append(float(np.sqrt(((F - Go) ** 2).sum() / (Go ** 2).sum())))
+            s.oracle_grad = Go
+        log("force errors done")
+    # the same systems one at a time in the plain (single-system) engine,
+    # from the files and relaxed coordinates the batch used
+    one_ms = 0.0
+    for k, s in enumerate(systems):
+        st = s.settings
+        d = os.path.join(work, f"sys{k}")
+        psf = api.CharmmPsf(os.path.join(d, f"{s.name}.psf"))
+        prm = api.CharmmParameters(os.path.join(d, f"{s.name}.prm"))
+        fm = api.ForceManager(psf, prm)
+        fm.setBoxDimensions(s.box)
+        fm.setKappa(st["kappa"])
+        fm.setCutoff(st["cutnb"])
+        fm.setCtonnb(st["ctonnb"])
+        fm.setCtofnb(st["ctofnb"])
+        fm.setFFTGrid(*st["nfft"])
+        fm.setPmeSplineOrder(st["order"])
+        fm.setPrecisionMode(args.precise)
+        ctx = api.CharmmContext(fm)
+        ctx.setCoordinates(xs[k])
+        ctx.setRandomSeedForVelocities(seeds[k])
+        ctx.assignVelocitiesAtTemperature(300.0)
+        if k in sample and errs:
+            ctx.calculateForces(False, False, False)
+            F = ctx.getForces()
+            Go = s.oracle_grad
+            one_errs.append(float(np.sqrt(((F - Go) ** 2).sum() / (Go ** 2).sum())))
+        integ = api.CudaLangevinThermostatIntegrator(DT_PS)
+        integ.setThermostatFriction(1.0)
+        integ.setReferenceTemperature(300.0)
+        integ.setThermostatRngSeed(777)
+        integ.setCharmmContext(ctx)
+        integ.propagate(SEG)                       # capture + first replay
+        st1 = torch.cuda.ExternalStream(ctx.getStream())
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st1)
+        for _ in range(args.one_steps):
+            integ.propagate(SEG)
+        e1.record(st1)
+        e1.synchronize()
+        one_ms += e0.elapsed_time(e1)
+        del integ, ctx, fm, prm, psf
+        if k % 32 == 31:
+            log(f"one by one: {k + 1} systems")
+    one_value = ns_per_day(args.one_steps * SEG * n_sys, one_ms * 1e-3)
+    line = {
+        "metric": "aggregate ns/day (many independent systems)", "value": value,
+        "unit": "ns/day", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": sum(seg_ms) / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (forces), f64 (integration)",
+        "data": "synthetic (seeded generator)",
+        "config": {"workload": f"batch{n_sys}: {n_sys} systems, bead chain (~10 %) in TIP3P, "
+                               "atoms log-uniform 3,000-30,000, 0.997 g/cm^3, PME spacing "
+                               "<= 1 A, order 4, cutoff 10 / switch 8-10 / list 12, Langevin "
+                               "300 K gamma 1/ps, dt 2 fs, SETTLE",
+                   "systems": n_sys, "atoms": ntot, "md_steps_per_iteration": SEG,
+                   "form": "precision" if args.precise else "plain",
+                   "tiles_per_work_autotuned": tpw,
+                   "l2": "flushed (256 MB device write) before every timed iteration"},
+        "one_by_one": {"value": one_value, "unit": "ns/day",
+                       "note": f"the same systems, one single-system context at a time, "
+                               f"{args.one_steps} timed segments each after one warm-up segment",
+                       "force_rel_rms_vs_fp64": one_errs},
+        "batched_over_one_by_one": value / one_value if one_value else None,
+        "force_rel_rms_vs_fp64": errs, "force_error_sample_systems": sample,
+        "e2e": {"value": ns_per_day(iters * SEG * n_sys, e2e_s), "unit": "ns/day",
+                "h2d_bytes_per_step": 2 * 3 * ntot * 8 / SEG,
+                "d2h_bytes_per_step": 2 * 3 * ntot * 8 / SEG},
+        "clocks": clocks.summary(), "generation_s": t_gen,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def make_integrator(api, spec, rank):
     kind = spec["integrator"]
     if kind == "langevin":
@@ -256,12 +434,21 @@ def main():
     ap.add_argument("--steps", type=int, default=100, help="timed iterations (20 MD steps each)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="chain23k", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="chain23k", choices=sorted(WORKLOADS) + ["batch"])
+    ap.add_argument("--systems", type=int, default=256, help="batch workload: number of systems")
+    ap.add_argument("--one-steps", type=int, default=2,
+                    help="batch workload: timed segments per system in the one-by-one baseline")
     ap.add_argument("--precise", action="store_true", help="precision form")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    if args.workload == "batch":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no "
+                              "many-system engine; the one-by-one baseline is in the b200 line"}))
+            return 0
+        return run_batch(args)
     if args.impl == "reference":
         return run_reference_arm(args)
 
