@@ -276,8 +276,26 @@ def run_batch(args):
                                precise=args.precise)
     log("batch initialised")
     waters = [api.water_indices(s) for s in systems]
+    n_sys_all = len(systems)
     xs = api.relax_batch(b, waters, iterations=RELAX_ITERATIONS, max_step=RELAX_MAX_STEP)
     log("relaxed")
+    # force error against FP64 on a sample of systems at the relaxed
+    # coordinates; the one-by-one engine is checked at the same coordinates
+    sample = sorted({0, n_sys_all // 3, 2 * n_sys_all // 3, n_sys_all - 1})
+    b.calculateForces(False, False)
+    errs, one_errs, grads = [], [], {}
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        for k in sample:
+            s = systems[k]
+            st = s.settings
+            Eo, Go = oracle.Oracle(s, st["kappa"], st["ctofnb"], st["ctonnb"], st["nfft"],
+                                   st["order"]).evaluate(pos=xs[k])
+            F = b.getForces(k)
+            errs.append(float(np.sqrt(((F - Go) ** 2).sum() / (Go ** 2).sum())))
+            grads[k] = Go
+        log("force errors done")
     b.assignVelocities(300.0)
     b.setLangevin(DT_PS, 1.0, 300.0, 777)
     tpw = b.autotune(SEG, [4, 8, 12, 16])
@@ -322,22 +340,6 @@ def run_batch(args):
                  api._i(-1))
     e2e_s = time.perf_counter() - t0
     log("end to end done")
-    # force error against FP64 on a sample of systems, batch and single engine
-    sample = sorted({0, n_sys // 3, 2 * n_sys // 3, n_sys - 1})
-    b.calculateForces(False, False)
-    errs, one_errs = [], []
-    if not args.no_cpu_baseline:
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import oracle
-        for k in sample:
-            s = systems[k]
-            st = s.settings
-            Eo, Go = oracle.Oracle(s, st["kappa"], st["ctofnb"], st["ctonnb"], st["nfft"],
-                                   st["order"]).evaluate(pos=b.getCoordinates(k))
-            F = b.getForces(k)
-            errs.append(float(np.sqrt(((F - Go) ** 2).sum() / (Go ** 2).sum())))
-            s.oracle_grad = Go
-        log("force errors done")
     # the same systems one at a time in the plain (single-system) engine,
     # from the files and relaxed coordinates the batch used
     one_ms = 0.0
@@ -359,10 +361,10 @@ def run_batch(args):
         ctx.setCoordinates(xs[k])
         ctx.setRandomSeedForVelocities(seeds[k])
         ctx.assignVelocitiesAtTemperature(300.0)
-        if k in sample and errs:
+        if k in grads:
             ctx.calculateForces(False, False, False)
             F = ctx.getForces()
-            Go = s.oracle_grad
+            Go = grads[k]
             one_errs.append(float(np.sqrt(((F - Go) ** 2).sum() / (Go ** 2).sum())))
         integ = api.CudaLangevinThermostatIntegrator(DT_PS)
         integ.setThermostatFriction(1.0)
