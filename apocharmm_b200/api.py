@@ -176,6 +176,7 @@ class ForceManager(_Handle):
     def setPrecisionMode(self, on: bool): call("apo_force_manager_set_precision_mode", self._h, _i(int(on)))
     def setTilesPerWork(self, t: int): call("apo_force_manager_set_tiles_per_work", self._h, _i(t))
     def setComponentMask(self, m: int): call("apo_force_manager_set_component_mask", self._h, _i(m))
+    def setDirectKernel(self, form: int): call("apo_force_manager_set_direct_kernel", self._h, _i(form))
 
     def getFFTGrid(self):
         a = (ctypes.c_int * 3)()
@@ -610,6 +611,11 @@ class Batch(_Handle):
 
     def setComponentMask(self, mask: int):
         call("apo_batch_set_component_mask", self._h, _i(mask))
+
+    def getDirectKernel(self) -> int:
+        v = _i()
+        call("apo_batch_get_direct_kernel", ctypes.byref(v), self._h)
+        return v.value
 
 
 def batch_from_systems(systems, workdir: str, seeds=None, spline_order: int = 4,

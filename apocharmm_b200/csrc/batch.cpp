@@ -138,27 +138,32 @@ int Batch::autotune(int steps, const std::vector<int> &candidates) {
   APO_CUDA(cudaEventCreate(&e0));
   APO_CUDA(cudaEventCreate(&e1));
   float best = 1e30f;
-  int best_t = m_Tpw;
-  for (int t : candidates) {
-    if (t < 1) continue;
-    m_Fm->neighborList().set_tiles_per_work(t);
-    m_Integ.reset();            // graphs hold the old launch arguments
-    propagate(steps);           // warm-up: graph capture, first replay
-    APO_CUDA(cudaEventRecord(e0, s));
-    propagate(steps);
-    APO_CUDA(cudaEventRecord(e1, s));
-    APO_CUDA(cudaEventSynchronize(e1));
-    float ms = 0.f;
-    APO_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    if (ms < best) {
-      best = ms;
-      best_t = t;
+  int best_t = m_Tpw, best_f = m_Form;
+  for (int form : {kNbTileBatches, kNbGroupedQueues})
+    for (int t : candidates) {
+      if (t < 1) continue;
+      m_Fm->setDirectKernel(form);
+      m_Fm->neighborList().set_tiles_per_work(t);
+      m_Integ.reset();            // graphs hold the old launch arguments
+      propagate(steps);           // warm-up: graph capture, first replay
+      APO_CUDA(cudaEventRecord(e0, s));
+      propagate(steps);
+      APO_CUDA(cudaEventRecord(e1, s));
+      APO_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      APO_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (ms < best) {
+        best = ms;
+        best_t = t;
+        best_f = form;
+      }
     }
-  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  m_Fm->setDirectKernel(best_f);
   m_Fm->neighborList().set_tiles_per_work(best_t);
   m_Tpw = best_t;
+  m_Form = best_f;
   m_Integ.reset();
   m_Ctx->setCoordinatesXyz(x.data());
   m_Ctx->setVelocitiesXyz(v.data());

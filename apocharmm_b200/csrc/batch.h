@@ -42,10 +42,12 @@ class Batch {
   std::map<std::string, double> energyComponents(int sys);
   void getForces(int sys, double *xyz);
   std::vector<double> temperatures();
-  // time `steps` steps for each candidate tiles-per-work-item value and keep
-  // the fastest; returns it (the list is rebuilt, coordinates are restored)
+  // time `steps` steps for each direct-space kernel form and each candidate
+  // tiles-per-work-item value and keep the fastest pair; returns the tiles
+  // per work item (the state is restored afterwards)
   int autotune(int steps, const std::vector<int> &candidates);
   int tilesPerWork() const { return m_Tpw; }
+  int directKernel() const { return m_Form; }
   std::shared_ptr<CharmmContext> context() const { return m_Ctx; }
   std::shared_ptr<ForceManager> forceManager() const { return m_Fm; }
   std::shared_ptr<CudaLangevinThermostatIntegrator> integrator() const { return m_Integ; }
@@ -53,7 +55,7 @@ class Batch {
  private:
   void requireInit() const;
   void requireSys(int sys) const;
-  int m_Order, m_Tpw;
+  int m_Order, m_Tpw, m_Form = kNbTileBatches;
   bool m_Precise;
   std::vector<SystemSpec> m_Specs;
   std::shared_ptr<ForceManager> m_Fm;

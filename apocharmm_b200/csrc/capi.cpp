@@ -248,6 +248,7 @@ FM_SETTER(apo_force_manager_set_spline_order, int, setPmeSplineOrder(v), v == 4 
 FM_SETTER(apo_force_manager_set_precision_mode, int, setPrecisionMode(v != 0), true)
 FM_SETTER(apo_force_manager_set_tiles_per_work, int, setTilesPerWork(v), v >= 1 && v <= 1024)
 FM_SETTER(apo_force_manager_set_component_mask, int, setComponentMask(v), v >= 0 && v <= 7)
+FM_SETTER(apo_force_manager_set_direct_kernel, int, setDirectKernel(v), v == 0 || v == 1)
 
 extern "C" apo_status apo_force_manager_set_fft_grid(apo_force_manager *fm, const int nx,
                                                      const int ny, const int nz) {

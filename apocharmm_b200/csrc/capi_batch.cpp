@@ -239,3 +239,13 @@ extern "C" apo_status apo_batch_set_component_mask(apo_batch *b, const int mask)
     return APO_STATUS_OK;
   }, fn);
 }
+
+extern "C" apo_status apo_batch_get_direct_kernel(int *form, const apo_batch *b) {
+  const char *fn = "apo_batch_get_direct_kernel";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF_B(require_ptr(form, fn, "form"));
+    APO_RETURN_IF_B(require_batch(b, fn, false));
+    *form = b->object->directKernel();
+    return APO_STATUS_OK;
+  }, fn);
+}

@@ -140,6 +140,13 @@ void ForceManager::setFFTGrid(int nx, int ny, int nz) {
   m_Initialized = false;
 }
 
+void ForceManager::setDirectKernel(int v) {
+  if (v != kNbTileBatches && v != kNbGroupedQueues)
+    throw std::invalid_argument("direct-space kernel form must be 0 (tile batches) or 1 "
+                                "(grouped queues)");
+  m_NbVariant = v;
+}
+
 void ForceManager::setVdwType(int type) {
   if (type != VDW_VFSW)
     throw std::invalid_argument("only the VDW_VFSW (force switch) Lennard-Jones model is "
@@ -402,6 +409,7 @@ void ForceManager::calcForce(const float4 *d_xyzq, bool calcEnergy, bool calcVir
     a.energy = m_Energy.p;
     a.setups = m_Setup.p;
     a.virial = virial;
+    a.variant = m_NbVariant;
     cudaEvent_t t1 = nullptr;
     bool timer_capture = false;
     if (m_Timing) {

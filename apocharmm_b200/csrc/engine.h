@@ -111,6 +111,9 @@ class ForceManager {
   void setPrecisionMode(bool precise) { m_Precise = precise; }
   bool getPrecisionMode() const { return m_Precise; }
   void setTilesPerWork(int t) { m_TilesPerWork = t; m_Initialized = false; }
+  // direct-space kernel form (kNbTileBatches or kNbGroupedQueues, nonbonded.h)
+  void setDirectKernel(int v);
+  int getDirectKernel() const { return m_NbVariant; }
   // bit mask of the parts evaluated: 1 bonded+1-4, 2 direct, 4 reciprocal
   void setComponentMask(int mask) { m_ComponentMask = mask; }
 
@@ -190,6 +193,7 @@ class ForceManager {
   bool m_Initialized = false;
   bool m_ListBuilt = false;
   int m_TilesPerWork = 8;
+  int m_NbVariant = kNbTileBatches;
   int m_ComponentMask = 7;
   double m_SelfEnergy = 0.0;
   const double4 *m_StateCoords = nullptr;

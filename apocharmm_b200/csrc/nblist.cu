@@ -122,10 +122,12 @@ __global__ void col_sort_kernel(int ncol, const int *__restrict__ col_count,
                                 int *__restrict__ glo2loc, float4 *__restrict__ slot_shift,
                                 int *__restrict__ type_s, int *__restrict__ cl_col,
                                 const int *__restrict__ col_sys, int *__restrict__ cl_sys,
-                                const int *__restrict__ counts, int sort_cap) {
+                                const int *__restrict__ counts, int sort_cap,
+                                const float4 *__restrict__ xyzq) {
   extern __shared__ unsigned char smem[];
   float *sk = reinterpret_cast<float *>(smem);
   int *si = reinterpret_cast<int *>(smem + sizeof(float) * sort_cap);
+  int *so = si + sort_cap;
   int col = blockIdx.x;
   if (col >= ncol || counts[0] == 0) return;
   int cnt = col_count[col];
@@ -164,10 +166,30 @@ __global__ void col_sort_kernel(int ncol, const int *__restrict__ col_count,
       __syncthreads();
     }
   }
+  // inside every 32-atom cluster: the lower and the upper z-half, each
+  // ordered by x, so that slots 8m..8m+7 form compact 8-atom blocks (the
+  // direct-space kernel's i-groups); ties by atom index
+  for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+    const int g = si[k];
+    sk[k] = xyzq[g].x + atom_shift[g].x;
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+    const int c0 = k & ~15, n16 = min(16, cnt - c0);
+    const float xk = sk[k];
+    const int gk = si[k];
+    int rank = 0;
+    for (int m = c0; m < c0 + n16; ++m) {
+      const float xm = sk[m];
+      rank += (xm < xk || (xm == xk && si[m] < gk)) ? 1 : 0;
+    }
+    so[c0 + rank] = gk;
+  }
+  __syncthreads();
   for (int k = threadIdx.x; k < padded; k += blockDim.x) {
     int s = start + k;
     if (k < cnt) {
-      int g = si[k];
+      int g = so[k];
       perm[s] = g;
       glo2loc[g] = s;
       slot_shift[s] = atom_shift[g];
@@ -511,6 +533,9 @@ void NeighborList::setup(const std::vector<NbListSystem> &systems,
     natom += y.natom;
     m_sys_h.push_back(d);
   }
+  if ((size_t)m_d.sort_cap * (sizeof(float) + 2 * sizeof(int)) > 96 * 1024)
+    throw std::invalid_argument("NeighborList: a cell column would hold more atoms than the "
+                                "column sort supports (box too elongated for its density)");
   m_d.natom = natom;
   m_d.ncol = ncol;
   m_d.slot_cap = (int)((slots + kTile - 1) / kTile * kTile);
@@ -586,11 +611,11 @@ void NeighborList::build(const float4 *d_xyzq, cudaStream_t s) {
   scatter_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, m_atom_col, m_atom_rank, m_col_start,
                                                   m_atom_z, m_tmp_key, m_tmp_idx, counts);
   APO_LAUNCH_CHECK();
-  size_t sm = (size_t)m_d.sort_cap * (sizeof(float) + sizeof(int));
+  size_t sm = (size_t)m_d.sort_cap * (sizeof(float) + 2 * sizeof(int));
   col_sort_kernel<<<m_d.ncol, 512, sm, s>>>(m_d.ncol, m_col_count, m_col_start, m_tmp_key,
                                             m_tmp_idx, m_atom_shift, m_vdwtype, perm, glo2loc,
                                             slot_shift, type_s, m_cl_col, m_col_sys, cl_sys,
-                                            counts, m_d.sort_cap);
+                                            counts, m_d.sort_cap, d_xyzq);
   APO_LAUNCH_CHECK();
   origin_kernel<<<(ncl * 32 + 255) / 256, 256, 0, s>>>(d_xyzq, perm, slot_shift, m_sys, cl_sys,
                                                         cl_origin, slot_off, counts);

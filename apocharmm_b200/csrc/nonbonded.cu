@@ -361,6 +361,382 @@ __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Grouped-queue variant.  The i-cluster is split into four 8-atom groups
+// (the neighbour list orders each cluster as two z-halves of two x-halves,
+// so a group is a compact 3.5 x 3.5 x 7 A block).  Every j-atom of a tile
+// is tested against each group's live box and appended to that group's
+// queue in shared memory (a 64-entry ring per group) with its position
+// already in the i-cluster frame; the queues are consumed in batches of 8
+// entries per group across tile boundaries.  Lane (g, l) computes the pairs
+// of its i-atom with 8 entries of queue g, and the j-forces are combined
+// over the group's 8 lanes (3 shuffle levels) before one atomic add per j.
+// Fewer wasted pairs than testing all 32 i-atoms against a j that is only
+// near part of the cluster, and no padding to 8 pairs per tile.
+// ---------------------------------------------------------------------------
+
+constexpr int kQ = 64;  // ring entries per group
+
+__device__ __forceinline__ int sel4(int g, int a0, int a1, int a2, int a3) {
+  return g == 0 ? a0 : g == 1 ? a1 : g == 2 ? a2 : a3;
+}
+
+// bits [start, start + n) of a 64-bit ring (n <= 64)
+__device__ __forceinline__ unsigned long long ring_mask(int start, int n) {
+  if (n <= 0) return 0ull;
+  const unsigned long long m = n >= 64 ? ~0ull : ((1ull << n) - 1ull);
+  const int s = start & 63;
+  return s == 0 ? m : ((m << s) | (m >> (64 - s)));
+}
+
+// sum of v[k] over the 8 lanes of a group; lane l of the group returns the
+// total of entry l
+template <typename T>
+__device__ __forceinline__ T group_reduce8(T (&v)[8], int lane) {
+  const bool b4 = lane & 4, b2 = lane & 2, b1 = lane & 1;
+  T u[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const T send = b4 ? v[k] : v[k + 4];
+    const T keep = b4 ? v[k + 4] : v[k];
+    u[k] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+  }
+  T w[2];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const T send = b2 ? u[k] : u[k + 2];
+    const T keep = b2 ? u[k + 2] : u[k];
+    w[k] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+  }
+  const T send = b1 ? w[0] : w[1];
+  return (b1 ? w[1] : w[0]) + __shfl_xor_sync(0xffffffffu, send, 1);
+}
+
+template <bool ENERGY, bool PER_PAIR, bool VIRIAL, bool MULTI>
+__global__ void __launch_bounds__(kThreads, 5) nbq_kernel(NbArgs a) {
+  __shared__ float4 q_pos[kWarps][4][kQ];   // j position in the i frame, charge
+  __shared__ int2 q_inf[kWarps][4][kQ];     // j slot, LJ type
+  __shared__ float sh_box[kWarps][4][6];    // group boxes: lo xyz, hi xyz
+  extern __shared__ float2 sh_vdw[];
+  int T = a.ntype;
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const int g = lane >> 3;
+  const int tab_off = MULTI ? wib * kMaxMultiTypes * kMaxMultiTypes : 0;
+  int cur_sys = -1;
+  if (!MULTI) {
+    for (int k = threadIdx.x; k < T * T; k += blockDim.x) sh_vdw[k] = a.vdw[k];
+    __syncthreads();
+  }
+  const unsigned lt_mask = (1u << lane) - 1u;
+  const int nwork = a.counts[2];
+  const int stride = a.stride;
+  double e_elec = 0.0, e_vdw = 0.0;
+  double dv[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  using Acc = typename std::conditional<PER_PAIR, long long, float>::type;
+
+  for (int w = blockIdx.x * kWarps + wib; w < nwork; w += gridDim.x * kWarps) {
+    const int4 wk = a.work[w];
+    const NbSetup st = a.setups[wk.w];
+    if (MULTI && wk.w != cur_sys) {  // warp-uniform
+      __syncwarp();
+      T = st.ntype;
+      for (int k = lane; k < T * T; k += 32) sh_vdw[tab_off + k] = a.vdw[st.vdw_off + k];
+      __syncwarp();
+      cur_sys = wk.w;
+    }
+    const float4 oi = a.origin[wk.x];
+    const int islot = wk.x * kTile + lane;
+    const float4 xi = a.xyzq_s[islot];
+    const bool ivalid = a.perm[islot] >= 0;
+    const float qi = xi.w * (float)kCcelec;
+    const int ti = a.type_s[islot] * T;
+    // live box of this lane's group
+    float lo_x = ivalid ? xi.x : INFINITY, lo_y = ivalid ? xi.y : INFINITY,
+          lo_z = ivalid ? xi.z : INFINITY;
+    float hi_x = ivalid ? xi.x : -INFINITY, hi_y = ivalid ? xi.y : -INFINITY,
+          hi_z = ivalid ? xi.z : -INFINITY;
+#pragma unroll
+    for (int o = 4; o > 0; o >>= 1) {
+      lo_x = fminf(lo_x, __shfl_xor_sync(0xffffffffu, lo_x, o));
+      lo_y = fminf(lo_y, __shfl_xor_sync(0xffffffffu, lo_y, o));
+      lo_z = fminf(lo_z, __shfl_xor_sync(0xffffffffu, lo_z, o));
+      hi_x = fmaxf(hi_x, __shfl_xor_sync(0xffffffffu, hi_x, o));
+      hi_y = fmaxf(hi_y, __shfl_xor_sync(0xffffffffu, hi_y, o));
+      hi_z = fmaxf(hi_z, __shfl_xor_sync(0xffffffffu, hi_z, o));
+    }
+    __syncwarp();
+    if ((lane & 7) == 0) {
+      sh_box[wib][g][0] = lo_x;
+      sh_box[wib][g][1] = lo_y;
+      sh_box[wib][g][2] = lo_z;
+      sh_box[wib][g][3] = hi_x;
+      sh_box[wib][g][4] = hi_y;
+      sh_box[wib][g][5] = hi_z;
+    }
+    __syncwarp();
+    Acc fix = 0, fiy = 0, fiz = 0;
+    float vw[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    int h0 = 0, h1 = 0, h2 = 0, h3 = 0;   // ring heads (uniform)
+    int t0 = 0, t1 = 0, t2 = 0, t3 = 0;   // ring tails (uniform)
+    unsigned long long xmask = 0ull;      // excluded entries of my group, by ring position
+
+    // consume up to 8 entries of every group
+    auto batch = [&]() {
+      const int head = sel4(g, h0, h1, h2, h3);
+      const int cnt = min(8, sel4(g, t0, t1, t2, t3) - head);
+      Acc fx[8], fy[8], fz[8];
+#pragma unroll
+      for (int jj = 0; jj < 8; ++jj) {
+        const int pos = (head + jj) & (kQ - 1);
+        // entries past this group's count are stale ring contents (possibly
+        // not even finite): they are masked and their differences zeroed
+        const float4 pj = q_pos[wib][g][pos];
+        const int tj = q_inf[wib][g][pos].y;
+        float dx = xi.x - pj.x, dy = xi.y - pj.y, dz = xi.z - pj.z;
+        const float r2raw = dx * dx + dy * dy + dz * dz;
+        const bool in = jj < cnt && ivalid && !((xmask >> pos) & 1ull) && r2raw < st.roff2;
+        dx = in ? dx : 0.f;
+        dy = in ? dy : 0.f;
+        dz = in ? dz : 0.f;
+        const float r2 = in ? r2raw : 1.f;
+        const float rinv = rsqrtf(r2);
+        const float rr = r2 * rinv;
+        const float rinv2 = rinv * rinv;
+        // erfc-Ewald (src/CudaDirectForceKernels.cu:479-489)
+        const float qq = in ? qi * pj.w : 0.f;
+        const float exp_v = __expf(-st.kappa2 * r2);
+        const float erfc_v = erfc_from_exp(st.kappa * rr, exp_v);
+        const float e_el = qq * erfc_v * rinv;
+        const float fr_el = -qq * st.two_kappa_sqrtpi * exp_v - e_el;
+        // VDW_VFSW (src/CudaDirectForceKernels.cu:263-286)
+        float2 cc = sh_vdw[tab_off + ti + (in ? tj : 0)];
+        cc.x = in ? cc.x : 0.f;
+        cc.y = in ? cc.y : 0.f;
+        const float rinv3 = rinv * rinv2, rinv6 = rinv3 * rinv3;
+        const bool sw = r2 > st.ron2;
+        const float A6 = sw ? st.k6 : 1.f, B6 = sw ? st.roffinv3 : 0.f;
+        const float A12 = sw ? st.k12 : 1.f, B12 = sw ? st.roffinv6 : 0.f;
+        const float t6 = rinv3 - B6, t12 = rinv6 - B12;
+        const float fr_vdw = cc.x * A6 * t6 * rinv3 - cc.y * A12 * t12 * rinv6;
+        const float fij = (fr_vdw + fr_el) * rinv2;
+        if (ENERGY) {
+          const float C6 = sw ? 0.f : st.dv6, C12 = sw ? 0.f : st.dv12;
+          e_elec += (double)e_el;
+          e_vdw += (double)((1.f / 12.f) * cc.y * (A12 * t12 * t12 + C12) -
+                            (1.f / 6.f) * cc.x * (A6 * t6 * t6 + C6));
+        }
+        if (VIRIAL) {
+          const float gx = fij * dx, gy = fij * dy, gz = fij * dz;
+          vw[0] -= gx * dx;
+          vw[1] -= gx * dy;
+          vw[2] -= gx * dz;
+          vw[3] -= gy * dy;
+          vw[4] -= gy * dz;
+          vw[5] -= gz * dz;
+        }
+        if (PER_PAIR) {
+          const long long gx = to_fixed_force(fij * dx);
+          const long long gy = to_fixed_force(fij * dy);
+          const long long gz = to_fixed_force(fij * dz);
+          fix += gx;
+          fiy += gy;
+          fiz += gz;
+          fx[jj] = -gx;
+          fy[jj] = -gy;
+          fz[jj] = -gz;
+        } else {
+          fix += fij * dx;
+          fiy += fij * dy;
+          fiz += fij * dz;
+          fx[jj] = -fij * dx;
+          fy[jj] = -fij * dy;
+          fz[jj] = -fij * dz;
+        }
+      }
+      const Acc rx = group_reduce8(fx, lane);
+      const Acc ry = group_reduce8(fy, lane);
+      const Acc rz = group_reduce8(fz, lane);
+      const int own = lane & 7;
+      if (own < cnt) {
+        const int js = q_inf[wib][g][(head + own) & (kQ - 1)].x;
+        if (PER_PAIR) {
+          add_fixed(a.force + js, (long long)rx);
+          add_fixed(a.force + stride + js, (long long)ry);
+          add_fixed(a.force + 2 * stride + js, (long long)rz);
+        } else {
+          add_fixed(a.force + js, to_fixed_force((float)rx));
+          add_fixed(a.force + stride + js, to_fixed_force((float)ry));
+          add_fixed(a.force + 2 * stride + js, to_fixed_force((float)rz));
+        }
+      }
+      xmask &= ~ring_mask(head, cnt > 0 ? cnt : 0);
+      h0 += min(8, t0 - h0);
+      h1 += min(8, t1 - h1);
+      h2 += min(8, t2 - h2);
+      h3 += min(8, t3 - h3);
+      __syncwarp();
+    };
+
+    // one call site for the batch and one for the enqueue (code size: the
+    // batch is an unrolled 8-pair loop): full batches while every group has
+    // 8 waiting; before a tile, at most 32 waiting per group so that the tile
+    // fits the rings; after the last tile, until the rings are empty
+    int t = wk.y;
+    for (;;) {
+      const int fmin = min(min(t0 - h0, t1 - h1), min(t2 - h2, t3 - h3));
+      const int fmax = max(max(t0 - h0, t1 - h1), max(t2 - h2, t3 - h3));
+      if (fmin >= 8 || fmax > kQ - 32 || (t >= wk.z && fmax > 0)) {
+        batch();
+        continue;
+      }
+      if (t >= wk.z) break;
+      const int2 tl = a.tiles[t];
+      const float4 oj = a.origin[tl.x];
+      const int ic = tl.y / 9, ib = (tl.y - 9 * ic) / 3, ia = tl.y - 9 * ic - 3 * ib;
+      const float kx = (float)(ia - 1), ky = (float)(ib - 1), kz = (float)(ic - 1);
+      const float sx = fmaf(kx, st.Lx, oj.x - oi.x) + kx * st.Lx_lo;
+      const float sy = fmaf(ky, st.Ly, oj.y - oi.y) + ky * st.Ly_lo;
+      const float sz = fmaf(kz, st.Lz, oj.z - oi.z) + kz * st.Lz_lo;
+      const int jslot = tl.x * kTile + lane;
+      float4 xj = a.xyzq_s[jslot];
+      xj.x += sx;
+      xj.y += sy;
+      xj.z += sz;
+      const bool jvalid = a.perm[jslot] >= 0;
+      const int tj = a.type_s[jslot];
+      const unsigned excl = a.masks[(size_t)t * kTile + lane];
+      const bool any_excl = __any_sync(0xffffffffu, ivalid && excl != 0u);
+#pragma unroll
+      for (int h = 0; h < 4; ++h) {
+        const float *bb = sh_box[wib][h];
+        const float bx = fmaxf(0.f, fmaxf(bb[0] - xj.x, xj.x - bb[3]));
+        const float by = fmaxf(0.f, fmaxf(bb[1] - xj.y, xj.y - bb[4]));
+        const float bz = fmaxf(0.f, fmaxf(bb[2] - xj.z, xj.z - bb[5]));
+        const bool near = jvalid && bx * bx + by * by + bz * bz < st.roff2;
+        const unsigned m = __ballot_sync(0xffffffffu, near);
+        const int tail = h == 0 ? t0 : h == 1 ? t1 : h == 2 ? t2 : t3;
+        if (near) {
+          const int pos = (tail + __popc(m & lt_mask)) & (kQ - 1);
+          q_pos[wib][h][pos] = xj;
+          q_inf[wib][h][pos] = make_int2(jslot, tj);
+        }
+        if (any_excl && g == h && ivalid && excl != 0u) {
+          unsigned mm = m & excl;   // excluded among the new entries, in order
+          while (mm) {
+            const int k = __ffs(mm) - 1;
+            mm &= mm - 1u;
+            xmask |= 1ull << ((tail + __popc(m & ((1u << k) - 1u))) & (kQ - 1));
+          }
+        }
+        const int n = __popc(m);
+        if (h == 0) t0 += n;
+        else if (h == 1) t1 += n;
+        else if (h == 2) t2 += n;
+        else t3 += n;
+      }
+      __syncwarp();
+      ++t;
+    }
+
+    if (VIRIAL) {
+#pragma unroll
+      for (int k = 0; k < 6; ++k) dv[k] += (double)vw[k];
+    }
+    if (MULTI && ENERGY) {
+      long long *es = a.energy + (size_t)wk.w * a.energy_stride;
+      warp_flush(e_elec, es + kEElec, lane);
+      warp_flush(e_vdw, es + kEVdw, lane);
+      e_elec = 0.0;
+      e_vdw = 0.0;
+      if (VIRIAL) {
+        constexpr int kSlotM[6][2] = {{0, 0}, {1, 3}, {2, 6}, {4, 4}, {5, 7}, {8, 8}};
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+          long long iw = __double2ll_rn(dv[k] * kEnergyScale);
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) iw += __shfl_xor_sync(0xffffffffu, iw, o);
+          if (lane == 0 && iw) {
+            add_fixed(es + kNumEnergyTerms + kSlotM[k][0], iw);
+            if (kSlotM[k][1] != kSlotM[k][0]) add_fixed(es + kNumEnergyTerms + kSlotM[k][1], iw);
+          }
+          dv[k] = 0.0;
+        }
+      }
+    }
+    if (ivalid) {
+      if (PER_PAIR) {
+        add_fixed(a.force + islot, (long long)fix);
+        add_fixed(a.force + stride + islot, (long long)fiy);
+        add_fixed(a.force + 2 * stride + islot, (long long)fiz);
+      } else {
+        add_fixed(a.force + islot, to_fixed_force((float)fix));
+        add_fixed(a.force + stride + islot, to_fixed_force((float)fiy));
+        add_fixed(a.force + 2 * stride + islot, to_fixed_force((float)fiz));
+      }
+    }
+  }
+  if (ENERGY && !MULTI) {
+    long long ie = __double2ll_rn(e_elec * kEnergyScale);
+    long long iv = __double2ll_rn(e_vdw * kEnergyScale);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      ie += __shfl_xor_sync(0xffffffffu, ie, o);
+      iv += __shfl_xor_sync(0xffffffffu, iv, o);
+    }
+    if (lane == 0) {
+      add_fixed(a.energy + kEElec, ie);
+      add_fixed(a.energy + kEVdw, iv);
+    }
+  }
+  if (VIRIAL && !MULTI) {
+    constexpr int kSlot[6][2] = {{0, 0}, {1, 3}, {2, 6}, {4, 4}, {5, 7}, {8, 8}};
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      long long iw = __double2ll_rn(dv[k] * kEnergyScale);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) iw += __shfl_xor_sync(0xffffffffu, iw, o);
+      if (lane == 0) {
+        add_fixed(a.virial + kSlot[k][0], iw);
+        if (kSlot[k][1] != kSlot[k][0]) add_fixed(a.virial + kSlot[k][1], iw);
+      }
+    }
+  }
+}
+
+template <bool E, bool P, bool V, bool M>
+void launch_q(const NbArgs &a, cudaStream_t s) {
+  static int grid = 0;
+  size_t sm = M ? (size_t)kWarps * kMaxMultiTypes * kMaxMultiTypes * sizeof(float2)
+                : (size_t)a.ntype * a.ntype * sizeof(float2);
+  if (!grid) {
+    int dev, nsm, per = 0;
+    APO_CUDA(cudaGetDevice(&dev));
+    APO_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    APO_CUDA(cudaFuncSetAttribute(nbq_kernel<E, P, V, M>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+    APO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, nbq_kernel<E, P, V, M>, kThreads,
+                                                           64 * 1024 > sm ? sm : 64 * 1024));
+    grid = nsm * (per > 0 ? per : 1);
+  }
+  nbq_kernel<E, P, V, M><<<grid, kThreads, sm, s>>>(a);
+  APO_LAUNCH_CHECK();
+}
+
+template <bool M>
+void dispatch_q(const NbArgs &a, bool energy, bool per_pair, bool virial, cudaStream_t s) {
+  if (virial) {
+    if (per_pair) launch_q<true, true, true, M>(a, s);
+    else launch_q<true, false, true, M>(a, s);
+  } else if (energy) {
+    if (per_pair) launch_q<true, true, false, M>(a, s);
+    else launch_q<true, false, false, M>(a, s);
+  } else {
+    if (per_pair) launch_q<false, true, false, M>(a, s);
+    else launch_q<false, false, false, M>(a, s);
+  }
+}
+
 template <bool E, bool P, bool V = false, bool M = false>
 void launch_t(const NbArgs &a, cudaStream_t s) {
   static int grid = 0;
@@ -385,6 +761,8 @@ void launch_t(const NbArgs &a, cudaStream_t s) {
 void launch_nonbonded(const NbArgs &a, bool energy, bool per_pair, cudaStream_t s, bool virial) {
   if (a.ntype * a.ntype * sizeof(float2) > 64 * 1024)
     throw std::invalid_argument("nonbonded: too many LJ types for the shared table");
+  if (virial && !a.virial) throw std::invalid_argument("nonbonded: virial requested without a buffer");
+  if (a.variant == kNbGroupedQueues) return dispatch_q<false>(a, energy, per_pair, virial, s);
   if (virial) {
     if (!a.virial) throw std::invalid_argument("nonbonded: virial requested without a buffer");
     if (per_pair) launch_t<true, true, true>(a, s);
@@ -404,6 +782,7 @@ void launch_nonbonded_multi(const NbArgs &a, bool energy, bool per_pair, cudaStr
                             bool virial) {
   if (a.energy_stride <= 0 && (energy || virial))
     throw std::invalid_argument("nonbonded: multi-system energies need an energy stride");
+  if (a.variant == kNbGroupedQueues) return dispatch_q<true>(a, energy, per_pair, virial, s);
   if (virial) {
     if (per_pair) launch_t<true, true, true, true>(a, s);
     else launch_t<true, false, true, true>(a, s);

@@ -46,7 +46,13 @@ struct NbArgs {
   // multi-system launches: energies (and virial) of system s at
   // energy + s * energy_stride (virial at + kNumEnergyTerms); 0 = one system
   int energy_stride = 0;
+  int variant = 0;        // kernel form, below
 };
+
+// direct-space kernel forms: one j-list per tile for all 32 i-atoms, or one
+// queue per 8-atom i-group carried across tiles
+constexpr int kNbTileBatches = 0;
+constexpr int kNbGroupedQueues = 1;
 
 // per_pair: round every pair contribution to 64-bit fixed point before it is
 // summed (order-independent, the reference's accumulation,

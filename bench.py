@@ -298,8 +298,9 @@ def run_batch(args):
         log("force errors done")
     b.assignVelocities(300.0)
     b.setLangevin(DT_PS, 1.0, 300.0, 777)
-    tpw = b.autotune(SEG, [4, 8, 12, 16])
-    log(f"autotuned: {tpw} tiles per work item")
+    tpw = b.autotune(SEG, [4, 8, 16, 32])
+    form = b.getDirectKernel()
+    log(f"autotuned: {tpw} tiles per work item, kernel form {form}")
     stream = torch.cuda.ExternalStream(b.getStream())
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
     for _ in range(args.warmup):
@@ -343,7 +344,7 @@ def run_batch(args):
     # the same systems one at a time in the plain (single-system) engine,
     # from the files and relaxed coordinates the batch used
     one_ms = 0.0
-    for k, s in enumerate(systems):
+    for k, s in enumerate(systems if args.one_steps > 0 else []):
         st = s.settings
         d = os.path.join(work, f"sys{k}")
         psf = api.CharmmPsf(os.path.join(d, f"{s.name}.psf"))
@@ -384,7 +385,7 @@ def run_batch(args):
         del integ, ctx, fm, prm, psf
         if k % 32 == 31:
             log(f"one by one: {k + 1} systems")
-    one_value = ns_per_day(args.one_steps * SEG * n_sys, one_ms * 1e-3)
+    one_value = ns_per_day(args.one_steps * SEG * n_sys, one_ms * 1e-3) if one_ms > 0 else None
     line = {
         "metric": "aggregate ns/day (many independent systems)", "value": value,
         "unit": "ns/day", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
@@ -398,6 +399,7 @@ def run_batch(args):
                    "systems": n_sys, "atoms": ntot, "md_steps_per_iteration": SEG,
                    "form": "precision" if args.precise else "plain",
                    "tiles_per_work_autotuned": tpw,
+                   "direct_kernel_autotuned": ["tile batches", "grouped queues"][form],
                    "l2": "flushed (256 MB device write) before every timed iteration"},
         "one_by_one": {"value": one_value, "unit": "ns/day",
                        "note": f"the same systems, one single-system context at a time, "
@@ -439,10 +441,13 @@ def main():
     ap.add_argument("--workload", default="chain23k", choices=sorted(WORKLOADS) + ["batch"])
     ap.add_argument("--systems", type=int, default=256, help="batch workload: number of systems")
     ap.add_argument("--one-steps", type=int, default=2,
-                    help="batch workload: timed segments per system in the one-by-one baseline")
+                    help="batch workload: timed segments per system in the one-by-one baseline "
+                         "(0: skip the baseline)")
     ap.add_argument("--precise", action="store_true", help="precision form")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--direct-kernel", type=int, default=0, choices=[0, 1],
+                    help="direct-space kernel form: 0 tile batches, 1 grouped queues")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.workload == "batch":
@@ -469,6 +474,7 @@ def main():
     s = make_system(args.workload)
     work = tempfile.mkdtemp(prefix=f"apo_bench_{rank}_")
     psf, prm, fm, ctx = api.system_context(s, work, precise=args.precise)
+    fm.setDirectKernel(args.direct_kernel)
     # remove the close contacts of the generated structure (deterministic)
     s.pos = api.relax(ctx, api.water_indices(s), iterations=RELAX_ITERATIONS,
                       max_step=RELAX_MAX_STEP)
@@ -587,6 +593,7 @@ def main():
             "config": {"workload": spec["desc"],
                        "atoms": s.n_atoms, "md_steps_per_iteration": SEG,
                        "form": "precision" if args.precise else "plain",
+                       "direct_kernel": ["tile batches", "grouped queues"][args.direct_kernel],
                        "l2": "flushed (256 MB device write) before every timed iteration, "
                              "outside the timed interval",
                        "parallelism": f"replicas x{world}"},

@@ -40,9 +40,12 @@ APOCHARMM_C_API apo_status apo_batch_get_forces(double *xyz, const size_t len, a
 APOCHARMM_C_API apo_status apo_batch_get_energy_components(double *energies, const size_t len, apo_batch *batch, const int system);
 /* instantaneous temperature of every system from its on-step velocities */
 APOCHARMM_C_API apo_status apo_batch_get_temperatures(double *temperatures, const size_t len, apo_batch *batch);
-/* measured sweep over the candidate tiles per work item (NULL: 2 4 6 8 12 16);
- * keeps and returns the fastest; the batch state is restored */
+/* measured sweep over both direct-space kernel forms and the candidate tiles
+ * per work item (NULL: 2 4 6 8 12 16); keeps the fastest pair and returns
+ * its tiles per work item; the batch state is restored */
 APOCHARMM_C_API apo_status apo_batch_autotune(int *tiles_per_work, apo_batch *batch, const int steps, const int *candidates, const int num_candidates);
+/* the direct-space kernel form in use (0 tile batches, 1 grouped queues) */
+APOCHARMM_C_API apo_status apo_batch_get_direct_kernel(int *form, const apo_batch *batch);
 APOCHARMM_C_API apo_status apo_batch_get_stream(void **stream, const apo_batch *batch);
 /* evaluated parts as a bit mask (1 bonded+1-4, 2 direct, 4 reciprocal), as
  * apo_force_manager_set_component_mask */

@@ -30,6 +30,9 @@ APOCHARMM_C_API apo_status apo_force_manager_set_precision_mode(apo_force_manage
 APOCHARMM_C_API apo_status apo_force_manager_set_tiles_per_work(apo_force_manager *force_manager, const int tiles);
 APOCHARMM_C_API apo_status apo_force_manager_set_component_mask(apo_force_manager *force_manager, const int mask);
 APOCHARMM_C_API apo_status apo_force_manager_get_fft_grid(int *nxyz3, const apo_force_manager *force_manager);
+/* addition: direct-space kernel form, 0 = one j-list per tile for the whole
+ * i-cluster (default), 1 = one queue per 8-atom i-group across tiles */
+APOCHARMM_C_API apo_status apo_force_manager_set_direct_kernel(apo_force_manager *force_manager, const int form);
 #ifdef __cplusplus
 }
 #endif
