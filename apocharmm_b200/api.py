@@ -657,3 +657,81 @@ def relax_batch(b: "Batch", waters_per_system, iterations: int = 150, max_step: 
             x[off[k]:off[k + 1]] = rigid_water_fit(x[off[k]:off[k + 1]], np.asarray(w))
     b.setCoordinates(-1, x)
     return [x[off[k]:off[k + 1]].copy() for k in range(n)]
+
+
+class Server(_Handle):
+    """Request server with continuous batching (apo_server_*): MD-segment and
+    energy/force requests admitted by free HBM, advanced together 20 steps at
+    a time and re-batched as they arrive and finish; every request's result
+    is the same alone and among others."""
+    _destroy = "apo_server_destroy"
+    PENDING, DONE, FAILED = 0, 1, 2
+
+    def __init__(self, hbm_fraction: float = 0.5, spline_order: int = 4, precise: bool = False,
+                 dt_ps: float = 0.002, friction: float = 1.0, temperature: float = 300.0,
+                 seed: int = 1):
+        super().__init__()
+        call("apo_server_create", ctypes.byref(self._h), _d(hbm_fraction), _i(spline_order),
+             _i(int(precise)), _d(dt_ps), _d(friction), _d(temperature), ctypes.c_ulonglong(seed))
+        self._n = {}
+        self._keep = {}
+
+    def submit(self, kind: int, psf: "CharmmPsf", prm: "CharmmParameters", box, settings,
+               xyz, seed: int, steps: int = 0) -> int:
+        """kind 0: MD segment of `steps` steps, 1: energies and forces.
+        settings: kappa, cutnb, ctonnb, ctofnb and nfft (as System.settings)."""
+        a = np.ascontiguousarray(xyz, np.float64).reshape(-1)
+        rid = _i()
+        nf = settings.get("nfft", (-1, -1, -1))
+        call("apo_server_submit", ctypes.byref(rid), self._h, _i(kind), psf.handle, prm.handle,
+             _d(box[0]), _d(box[1]), _d(box[2]), _d(settings["kappa"]), _d(settings["cutnb"]),
+             _d(settings["ctonnb"]), _d(settings["ctofnb"]), _i(nf[0]), _i(nf[1]), _i(nf[2]),
+             ctypes.c_ulonglong(seed), _ptr(a), _sz(a.size), ctypes.c_longlong(steps))
+        self._n[rid.value] = a.size // 3
+        self._keep[rid.value] = (psf, prm)
+        return rid.value
+
+    def poll(self, rid: int) -> int:
+        st = _i()
+        call("apo_server_poll", ctypes.byref(st), self._h, _i(rid))
+        return st.value
+
+    def wait(self, rid: int, timeout_s: float = -1.0) -> int:
+        st = _i()
+        call("apo_server_wait", ctypes.byref(st), self._h, _i(rid), _d(timeout_s))
+        return st.value
+
+    def _vec(self, name: str, rid: int) -> np.ndarray:
+        a = np.zeros(3 * self._n[rid])
+        call(name, _ptr(a), _sz(a.size), self._h, _i(rid))
+        return a.reshape(-1, 3)
+
+    def coordinates(self, rid: int) -> np.ndarray:
+        return self._vec("apo_server_get_coordinates", rid)
+
+    def velocities(self, rid: int) -> np.ndarray:
+        return self._vec("apo_server_get_velocities", rid)
+
+    def forces(self, rid: int) -> np.ndarray:
+        return self._vec("apo_server_get_forces", rid)
+
+    def energies(self, rid: int) -> Dict[str, float]:
+        a = np.zeros(len(ENERGY_TERMS))
+        call("apo_server_get_energy_components", _ptr(a), _sz(a.size), self._h, _i(rid))
+        return dict(zip(ENERGY_TERMS, a.tolist()))
+
+    def latency(self, rid: int) -> float:
+        v = _d()
+        call("apo_server_get_latency", ctypes.byref(v), self._h, _i(rid))
+        return v.value
+
+    def release(self, rid: int):
+        call("apo_server_release", self._h, _i(rid))
+        self._n.pop(rid, None)
+        self._keep.pop(rid, None)
+
+    def stats(self) -> Dict[str, float]:
+        a = np.zeros(6)
+        call("apo_server_get_stats", _ptr(a), _sz(6), self._h)
+        return dict(zip(("system_steps", "simulated_ps", "rebuilds", "segments", "max_batch",
+                         "busy_s"), a.tolist()))

@@ -87,15 +87,20 @@ void Batch::setLangevin(double dtPs, double frictionPerPs, double temperature, u
   m_Integ.reset();
 }
 
+void Batch::createIntegrator() {
+  requireInit();
+  m_Ctx->ensureNeighborList();
+  m_Integ = std::make_shared<CudaLangevinThermostatIntegrator>(m_Dt);
+  m_Integ->setThermostatFriction(m_Friction);
+  m_Integ->setReferenceTemperature(m_Temp);
+  m_Integ->setThermostatRngSeed(m_Seed);
+  m_Integ->setCharmmContext(m_Ctx);
+  m_Fm->setDirectKernel(m_Form);
+}
+
 void Batch::propagate(int steps) {
   requireInit();
-  if (!m_Integ) {
-    m_Integ = std::make_shared<CudaLangevinThermostatIntegrator>(m_Dt);
-    m_Integ->setThermostatFriction(m_Friction);
-    m_Integ->setReferenceTemperature(m_Temp);
-    m_Integ->setThermostatRngSeed(m_Seed);
-    m_Integ->setCharmmContext(m_Ctx);
-  }
+  if (!m_Integ) createIntegrator();
   m_Integ->propagate(steps);
 }
 
@@ -142,6 +147,7 @@ int Batch::autotune(int steps, const std::vector<int> &candidates) {
   for (int form : {kNbTileBatches, kNbGroupedQueues})
     for (int t : candidates) {
       if (t < 1) continue;
+      m_Form = form;
       m_Fm->setDirectKernel(form);
       m_Fm->neighborList().set_tiles_per_work(t);
       m_Integ.reset();            // graphs hold the old launch arguments

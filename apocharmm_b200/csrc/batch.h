@@ -37,6 +37,9 @@ class Batch {
   void getVelocities(int sys, double *v);
   void assignVelocities(double temperature);
   void setLangevin(double dtPs, double frictionPerPs, double temperature, uint64_t seed);
+  // create the Langevin integrator now (it is otherwise created by the first
+  // propagate); it initialises every system's delta state from its velocities
+  void createIntegrator();
   void propagate(int steps);
   void calculateForces(bool energy, bool virial);
   std::map<std::string, double> energyComponents(int sys);

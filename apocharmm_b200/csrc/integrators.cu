@@ -15,7 +15,7 @@ namespace apo {
 
 namespace {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 64;  // small blocks: a step spreads over all SMs even for small systems
 constexpr int kMaxBlocks = 4096;
 
 // constraint group kinds
@@ -218,6 +218,11 @@ struct Common {
   const int *sys_of_atom;
   const int *atom_off;
   const unsigned long long *sys_seed;
+  // several systems: noise position of every system when this integrator
+  // started, and the number of steps each system may take from then on
+  // (groups of a system past its limit are left as they are); null = none
+  const unsigned long long *sys_rng0;
+  const long long *sys_stop;
   int ngroups;
   const int4 *groups;   // atoms (-1 unused)
   const int2 *gmeta;    // (kind, shake parameter index)
@@ -269,7 +274,20 @@ __global__ void __launch_bounds__(kThreads) langevin_kernel(Common c, double gam
   const double vfac = 0.5 * sqrt(1.0 + hg) / dt, idt = 1.0 / dt;
   double ke0 = 0.0, ke1 = 0.0;
   const unsigned long long pos = c.sc->rngpos;
-  if (g < c.ngroups) {
+  bool run = g < c.ngroups;
+  if (run && c.sys_stop) {  // a group never spans two systems
+    int at0[4];
+    group_atoms(c, g, at0);
+    const int sy = c.sys_of_atom[at0[0]];
+    if (c.sc->step >= c.sys_stop[sy]) {
+      run = false;
+      // the gradient slots are consumed all the same
+      int at[4];
+      const int m = group_atoms(c, g, at);
+      for (int k = 0; k < m; ++k) take_grad(c.force, c.stride, c.glo2loc[at[k]]);
+    }
+  }
+  if (run) {
     int at[4];
     const int m = group_atoms(c, g, at);
     const int2 meta = c.gmeta[g];
@@ -282,13 +300,15 @@ __global__ void __launch_bounds__(kThreads) langevin_kernel(Common c, double gam
       dp[k] = xyz(c.dprev[a]);
       const d3 gr = take_grad(c.force, c.stride, c.glo2loc[a]);
       curandStatePhilox4_32_10_t st;
+      unsigned long long p = pos;
       if (c.sys_seed) {  // a system's own stream, the same alone or among others
         const int sy = c.sys_of_atom[a];
         curand_init(seed ^ c.sys_seed[sy], (unsigned long long)(a - c.atom_off[sy]), 0ull, &st);
+        if (c.sys_rng0) p += c.sys_rng0[sy];
       } else {
         curand_init(seed, (unsigned long long)a, 0ull, &st);
       }
-      skipahead(pos, &st);
+      skipahead(p, &st);
       const float4 rn = curand_normal4(&st);
       const double rdf = sqrt(2.0 * gamma * kbt / v.w) / dt;
       const double fact = dt2 * v.w * denom;
@@ -587,7 +607,8 @@ void upload(DeviceArray<T> &d, const std::vector<T> &v) {
 
 struct IntegratorState {
   DeviceArray<int> atom_off;
-  DeviceArray<unsigned long long> sys_seed;
+  DeviceArray<unsigned long long> sys_seed, sys_rng0;
+  DeviceArray<long long> sys_stop;
   DeviceArray<int4> groups;
   DeviceArray<int2> gmeta;
   DeviceArray<float4> shake_p;
@@ -667,7 +688,13 @@ void CudaIntegrator::buildGroups() {
       meta.push_back({kShake, (int)k});
     }
   }
-  // free atoms in runs of up to four consecutive atoms
+  // free atoms in runs of up to four consecutive atoms of one system
+  std::vector<int> sys_end(n, n);
+  if (fm->isMulti()) {
+    const auto &off = fm->atomOffsets();
+    for (size_t k = 0; k + 1 < off.size(); ++k)
+      for (int a = off[k]; a < off[k + 1]; ++a) sys_end[a] = off[k + 1];
+  }
   for (int i = 0; i < n;) {
     if (owner[i] >= 0) {
       ++i;
@@ -677,7 +704,7 @@ void CudaIntegrator::buildGroups() {
     int *slot = &g.y;
     int k = 0;
     int j = i + 1;
-    while (k < 3 && j < n && owner[j] < 0) {
+    while (k < 3 && j < sys_end[i] && owner[j] < 0) {
       slot[k++] = j;
       ++j;
     }
@@ -710,6 +737,8 @@ void CudaIntegrator::buildGroups() {
   c.sys_of_atom = nullptr;
   c.atom_off = nullptr;
   c.sys_seed = nullptr;
+  c.sys_rng0 = nullptr;
+  c.sys_stop = nullptr;
   if (fm->isMulti()) {
     std::vector<unsigned long long> seeds;
     for (auto &y : fm->systemSpecs()) seeds.push_back((unsigned long long)y.seed);
@@ -862,6 +891,29 @@ void CudaLangevinThermostatIntegrator::setThermostatFriction(double f) {
   if (f < 0) throw std::invalid_argument("friction must be >= 0");
   m_Friction = f;
   clearGraphs();
+}
+
+double4 *CudaIntegrator::deltaState() const { return m_S ? m_S->dprev.p : nullptr; }
+
+void CudaIntegrator::setSystemLimits(const std::vector<unsigned long long> &rng0,
+                                     const std::vector<long long> &stop) {
+  if (!m_S || !m_Ctx) throw std::runtime_error("setSystemLimits: no context set");
+  auto fm = m_Ctx->getForceManager();
+  if (!fm->isMulti()) throw std::invalid_argument("setSystemLimits: not a multi-system context");
+  if ((int)rng0.size() != fm->numSystems() || (int)stop.size() != fm->numSystems())
+    throw std::invalid_argument("setSystemLimits: one entry per system expected");
+  m_S->sys_rng0.upload(rng0);
+  m_S->sys_stop.upload(stop);
+  m_S->c.sys_rng0 = m_S->sys_rng0.p;
+  m_S->c.sys_stop = m_S->sys_stop.p;
+  clearGraphs();  // the graphs hold the launch arguments
+}
+
+long long CudaIntegrator::deviceStep() {
+  Scalars h;
+  APO_CUDA(cudaStreamSynchronize(stream()));
+  APO_CUDA(cudaMemcpy(&h, m_S->sc.p, sizeof(h), cudaMemcpyDeviceToHost));
+  return h.step;
 }
 
 unsigned long long CudaLangevinThermostatIntegrator::getRngSequencePos() {

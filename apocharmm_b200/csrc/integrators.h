@@ -56,6 +56,15 @@ class CudaIntegrator : public std::enable_shared_from_this<CudaIntegrator> {
   // number of kernels one step and one list update launch (for accounting)
   int kernelsPerStep() const { return m_KernelsPerStep; }
   int kernelsPerRebuild() const;
+  // position-Verlet state: the last displacement of every atom (device)
+  double4 *deltaState() const;
+  // several systems (Langevin): every system's noise position at the start
+  // of this integrator and its step limit from then on; a system past its
+  // limit is not advanced (its forces are still evaluated)
+  void setSystemLimits(const std::vector<unsigned long long> &rng0,
+                       const std::vector<long long> &stop);
+  // steps taken by this integrator, read from the device counter
+  long long deviceStep();
 
  protected:
   virtual void initialize() = 0;

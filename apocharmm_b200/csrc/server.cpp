@@ -1,0 +1,269 @@
+// Request server with continuous batching; see server.h.
+#include "server.h"
+
+#include <algorithm>
+#include <stdexcept>
+
+namespace apo {
+
+namespace {
+constexpr int kSegment = 20;  // MD steps per list-update segment
+double seconds_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+}  // namespace
+
+Server::Server(double fraction, int order, bool precise, double dt, double friction,
+               double temperature, uint64_t seed)
+    : m_Fraction(fraction), m_Order(order), m_Precise(precise), m_Dt(dt),
+      m_Friction(friction), m_Temp(temperature), m_Seed(seed) {
+  if (!(fraction > 0.0 && fraction <= 1.0))
+    throw std::invalid_argument("Server: HBM fraction must be in (0, 1]");
+  if (order != 4 && order != 6 && order != 8)
+    throw std::invalid_argument("Server: spline order must be 4, 6 or 8");
+  if (!(dt > 0.0)) throw std::invalid_argument("Server: time step must be positive");
+  APO_CUDA(cudaGetDevice(&m_Device));
+  size_t free_b = 0, total_b = 0;
+  APO_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  m_Budget = (size_t)(fraction * (double)free_b);
+  m_Thread = std::thread([this] { loop(); });
+}
+
+Server::~Server() { stop(); }
+
+void Server::stop() {
+  {
+    std::lock_guard<std::mutex> lk(m_Mu);
+    m_Stop = true;
+  }
+  m_Cv.notify_all();
+  if (m_Thread.joinable()) m_Thread.join();
+}
+
+int Server::submit(ServeRequest r) {
+  if (!r.spec.psf || !r.spec.prm) throw std::invalid_argument("Server: null PSF or parameters");
+  const int n = r.spec.psf->getNumAtoms();
+  if ((int)r.xyz.size() != 3 * n) throw std::invalid_argument("Server: coordinates must be 3 N");
+  if (r.kind == 0 && r.steps <= 0) throw std::invalid_argument("Server: MD steps must be positive");
+  if (r.kind != 0 && r.kind != 1) throw std::invalid_argument("Server: unknown request kind");
+  auto j = std::make_shared<Job>();
+  j->req = std::move(r);
+  j->natom = n;
+  j->t0 = std::chrono::steady_clock::now();
+  std::lock_guard<std::mutex> lk(m_Mu);
+  if (m_Stop) throw std::runtime_error("Server: stopped");
+  if (!m_Fatal.empty()) throw std::runtime_error("Server: failed earlier: " + m_Fatal);
+  j->id = m_NextId++;
+  m_Results[j->id] = ServeResult{};
+  m_Results[j->id].kind = j->req.kind;
+  m_Queue.push_back(j);
+  m_Cv.notify_all();
+  return j->id;
+}
+
+bool Server::poll(int id, ServeResult *out) {
+  std::lock_guard<std::mutex> lk(m_Mu);
+  auto it = m_Results.find(id);
+  if (it == m_Results.end()) throw std::invalid_argument("Server: unknown request id");
+  if (it->second.status == 0) return false;
+  if (out) *out = it->second;
+  return true;
+}
+
+bool Server::wait(int id, double timeout_s, ServeResult *out) {
+  std::unique_lock<std::mutex> lk(m_Mu);
+  auto ready = [&] {
+    auto it = m_Results.find(id);
+    return it == m_Results.end() || it->second.status != 0;
+  };
+  if (timeout_s < 0) m_Cv.wait(lk, ready);
+  else m_Cv.wait_for(lk, std::chrono::duration<double>(timeout_s), ready);
+  auto it = m_Results.find(id);
+  if (it == m_Results.end()) throw std::invalid_argument("Server: unknown request id");
+  if (it->second.status == 0) return false;
+  if (out) *out = it->second;
+  return true;
+}
+
+void Server::release(int id) {
+  std::lock_guard<std::mutex> lk(m_Mu);
+  m_Results.erase(id);
+}
+
+ServerStats Server::stats() {
+  std::lock_guard<std::mutex> lk(m_Mu);
+  return m_Stats;
+}
+
+void Server::finish(const std::shared_ptr<Job> &j, ServeResult &&r) {
+  r.latency_s = seconds_since(j->t0);
+  std::lock_guard<std::mutex> lk(m_Mu);
+  auto it = m_Results.find(j->id);
+  if (it != m_Results.end()) it->second = std::move(r);
+  m_Cv.notify_all();
+}
+
+void Server::evaluateEnergies(std::vector<std::shared_ptr<Job>> &jobs) {
+  Batch b(m_Order, 8, m_Precise);
+  std::vector<double> all;
+  for (auto &j : jobs) {
+    b.addSystem(j->req.spec);
+    all.insert(all.end(), j->req.xyz.begin(), j->req.xyz.end());
+  }
+  b.initialize();
+  b.setCoordinates(-1, all.data());
+  b.calculateForces(true, false);
+  for (size_t k = 0; k < jobs.size(); ++k) {
+    ServeResult r;
+    r.kind = 1;
+    r.status = 1;
+    r.forces.resize((size_t)3 * jobs[k]->natom);
+    b.getForces((int)k, r.forces.data());
+    auto e = b.energyComponents((int)k);
+    for (int t = 0; t < kNumEnergyTerms; ++t) r.energy[t] = e[kEnergyNames[t]];
+    r.xyz = jobs[k]->req.xyz;
+    finish(jobs[k], std::move(r));
+  }
+}
+
+// re-form the MD batch around m_Active, carrying every continuing system's
+// state over exactly
+void Server::reform() {
+  if (m_Batch) {  // save the state of the systems that continue
+    double4 *delta = m_Batch->integrator() ? m_Batch->integrator()->deltaState() : nullptr;
+    for (size_t k = 0; k < m_BatchJobs.size(); ++k) {
+      auto &j = m_BatchJobs[k];
+      if (j->done >= j->req.steps || !delta) continue;
+      j->xyz.resize((size_t)3 * j->natom);
+      j->vel.resize((size_t)3 * j->natom);
+      m_Batch->getCoordinates((int)k, j->xyz.data());
+      m_Batch->getVelocities((int)k, j->vel.data());
+      j->delta.resize(j->natom);
+      APO_CUDA(cudaMemcpy(j->delta.data(), delta + m_Batch->atomOffset((int)k),
+                          j->delta.size() * sizeof(double4), cudaMemcpyDeviceToHost));
+    }
+    m_Batch.reset();
+  }
+  m_BatchJobs = m_Active;
+  m_Batch.reset(new Batch(m_Order, 8, m_Precise));
+  std::vector<double> all;
+  for (auto &j : m_Active) {
+    m_Batch->addSystem(j->req.spec);
+    const std::vector<double> &x = j->started ? j->xyz : j->req.xyz;
+    all.insert(all.end(), x.begin(), x.end());
+  }
+  m_Batch->initialize();
+  m_Batch->setCoordinates(-1, all.data());
+  m_Batch->setLangevin(m_Dt, m_Friction, m_Temp, m_Seed);
+  m_Batch->assignVelocities(m_Temp);   // every system from its own seed
+  for (size_t k = 0; k < m_Active.size(); ++k)
+    if (m_Active[k]->started) m_Batch->setVelocities((int)k, m_Active[k]->vel.data());
+  m_Batch->createIntegrator();         // new systems: constraint + delta from velocities
+  std::vector<unsigned long long> rng0;
+  std::vector<long long> stop;
+  double4 *delta = m_Batch->integrator()->deltaState();
+  for (size_t k = 0; k < m_Active.size(); ++k) {
+    auto &j = m_Active[k];
+    if (j->started) {  // overwrite whatever the initialisation did
+      m_Batch->setCoordinates((int)k, j->xyz.data());
+      m_Batch->setVelocities((int)k, j->vel.data());
+      APO_CUDA(cudaMemcpy(delta + m_Batch->atomOffset((int)k), j->delta.data(),
+                          j->delta.size() * sizeof(double4), cudaMemcpyHostToDevice));
+    }
+    j->started = true;
+    rng0.push_back(j->rng);
+    stop.push_back(j->req.steps - j->done);
+  }
+  m_Batch->integrator()->setSystemLimits(rng0, stop);
+  m_Dirty = false;
+  std::lock_guard<std::mutex> lk(m_Mu);
+  ++m_Stats.rebuilds;
+}
+
+void Server::loop() {
+  try {
+    APO_CUDA(cudaSetDevice(m_Device));
+    for (;;) {
+      std::vector<std::shared_ptr<Job>> admit, energy;
+      {
+        std::unique_lock<std::mutex> lk(m_Mu);
+        if (m_Queue.empty() && m_Active.empty())
+          m_Cv.wait_for(lk, std::chrono::milliseconds(2),
+                        [&] { return m_Stop || !m_Queue.empty(); });
+        if (m_Stop) break;
+        // admission by the estimated device memory of the running set
+        double used = 0.0;
+        for (auto &j : m_Active) used += j->natom * bytesPerAtom();
+        while (!m_Queue.empty()) {
+          auto &j = m_Queue.front();
+          const double need = j->natom * bytesPerAtom();
+          const bool nothing_running = m_Active.empty() && admit.empty() && energy.empty();
+          if (used + need > (double)m_Budget && !nothing_running) break;
+          (j->req.kind == 1 ? energy : admit).push_back(j);
+          used += need;
+          m_Queue.pop_front();
+        }
+      }
+      const auto t0 = std::chrono::steady_clock::now();
+      if (!energy.empty()) evaluateEnergies(energy);
+      if (!admit.empty()) {
+        m_Active.insert(m_Active.end(), admit.begin(), admit.end());
+        m_Dirty = true;
+      }
+      if (m_Active.empty()) {
+        if (m_Batch) {  // nothing left to run: free the device memory
+          m_Batch.reset();
+          m_BatchJobs.clear();
+        }
+        std::lock_guard<std::mutex> lk(m_Mu);
+        m_Stats.busy_s += seconds_since(t0);
+        continue;
+      }
+      if (m_Dirty) reform();
+      m_Batch->propagate(kSegment);
+      long long advanced = 0;
+      const int nactive = (int)m_BatchJobs.size();
+      std::vector<std::shared_ptr<Job>> keep;
+      for (size_t k = 0; k < m_BatchJobs.size(); ++k) {
+        auto &j = m_BatchJobs[k];
+        if (j->done >= j->req.steps) continue;  // finished earlier, held still
+        const long long take = std::min<long long>(kSegment, j->req.steps - j->done);
+        j->done += take;
+        j->rng += 4ull * (unsigned long long)take;
+        advanced += take;
+        if (j->done >= j->req.steps) {
+          ServeResult r;
+          r.kind = 0;
+          r.status = 1;
+          r.xyz.resize((size_t)3 * j->natom);
+          r.vel.resize((size_t)3 * j->natom);
+          m_Batch->getCoordinates((int)k, r.xyz.data());
+          m_Batch->getVelocities((int)k, r.vel.data());
+          finish(j, std::move(r));
+          m_Dirty = true;
+        } else {
+          keep.push_back(j);
+        }
+      }
+      m_Active.swap(keep);
+      std::lock_guard<std::mutex> lk(m_Mu);
+      ++m_Stats.segments;
+      m_Stats.md_steps += advanced;
+      m_Stats.sim_ps += advanced * m_Dt;
+      m_Stats.max_active = std::max(m_Stats.max_active, nactive);
+      m_Stats.busy_s += seconds_since(t0);
+    }
+  } catch (const std::exception &e) {
+    std::lock_guard<std::mutex> lk(m_Mu);
+    m_Fatal = e.what();
+    for (auto &kv : m_Results)
+      if (kv.second.status == 0) {
+        kv.second.status = 2;
+        kv.second.error = m_Fatal;
+      }
+    m_Cv.notify_all();
+  }
+  m_Batch.reset();
+}
+
+}  // namespace apo
