@@ -417,6 +417,119 @@ def run_batch(args):
     return 0
 
 
+def run_serve(args):
+    """Serving workload: a seeded Poisson request stream (mean 50 requests/s),
+    70 % MD segments (U[100, 5000] steps) and 30 % single energy/force
+    evaluations, each on its own system (bead chain + TIP3P, atoms
+    log-uniform in 2,000-100,000, 0.997 g/cm^3, PME spacing <= 1 A, order 4,
+    cutoff 10 A), Langevin 300 K, dt 2 fs.  Requests are submitted to the
+    server at their arrival times; latency is arrival -> result.  Aggregate
+    ns/day = simulated time of all MD requests over the wall time from the
+    first arrival to the last result."""
+    import multiprocessing as mp
+
+    import numpy as np
+    rank, world, local = dist_env()
+    t_start = time.perf_counter()
+
+    def log(msg):
+        print(f"[serve {time.perf_counter() - t_start:7.1f} s] {msg}", file=sys.stderr, flush=True)
+
+    rng = np.random.default_rng(4242)
+    nreq = args.requests
+    sizes = [int(v) for v in np.exp(rng.uniform(np.log(2000), np.log(100000), nreq))]
+    kinds = (rng.uniform(size=nreq) >= 0.7).astype(int)          # 1 = energy/force
+    steps = rng.integers(100, 5001, nreq)
+    arrivals = np.cumsum(rng.exponential(1.0 / 50.0, nreq))
+    with mp.get_context("spawn").Pool(min(nreq, os.cpu_count() or 1)) as pool:
+        systems = pool.map(_gen_batch_system, [(2000 + k, n) for k, n in enumerate(sizes)],
+                           chunksize=1)
+    log(f"generated {nreq} systems, {sum(s.n_atoms for s in systems)} atoms")
+    import torch
+    torch.cuda.set_device(local)
+    from apocharmm_b200 import api
+    from apocharmm_b200.systems import write_charmm_files
+    work = tempfile.mkdtemp(prefix="apo_serve_")
+    b = api.batch_from_systems(systems, os.path.join(work, "relax"))
+    xs = api.relax_batch(b, [api.water_indices(s) for s in systems],
+                         iterations=RELAX_ITERATIONS, max_step=RELAX_MAX_STEP)
+    b.close()
+    del b
+    handles = []
+    for k, s in enumerate(systems):
+        p = write_charmm_files(s, os.path.join(work, f"r{k}"))
+        handles.append((api.CharmmPsf(p["psf"]), api.CharmmParameters(p["prm"])))
+    log("relaxed, files written")
+    srv = api.Server(hbm_fraction=0.8, spline_order=4, precise=args.precise, dt_ps=DT_PS,
+                     friction=1.0, temperature=300.0, seed=31)
+    ids = []
+    t0 = time.perf_counter()
+    with ClockSampler(local) as clocks:
+        for k in range(nreq):
+            delay = arrivals[k] - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+            s = systems[k]
+            ids.append(srv.submit(int(kinds[k]), handles[k][0], handles[k][1], s.box, s.settings,
+                                  xs[k], 7000 + k, int(steps[k])))
+        for rid in ids:
+            if srv.wait(rid, 3600.0) != api.Server.DONE:
+                raise RuntimeError(f"request {rid} failed")
+    wall = time.perf_counter() - t0
+    lat = np.array([srv.latency(r) for r in ids])
+    md = kinds == 0
+    st = srv.stats()
+    sim_ns = float(sum(int(steps[k]) for k in range(nreq) if md[k])) * DT_PS * 1e-3
+    value = sim_ns / (wall / 86400.0)
+    log(f"served: wall {wall:.1f} s, p50 {np.percentile(lat, 50):.3f} s, "
+        f"p99 {np.percentile(lat, 99):.3f} s")
+    # force error against FP64 for the smallest energy/force requests
+    errs = []
+    same = None
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        ek = sorted([k for k in range(nreq) if not md[k]], key=lambda k: sizes[k])[:2]
+        for k in ek:
+            s = systems[k]
+            stt = s.settings
+            Eo, Go = oracle.Oracle(s, stt["kappa"], stt["ctofnb"], stt["ctonnb"], stt["nfft"],
+                                   stt["order"]).evaluate(pos=xs[k])
+            F = srv.forces(ids[k])
+            errs.append(float(np.sqrt(((F - Go) ** 2).sum() / (Go ** 2).sum())))
+        # the smallest MD request again, alone on a fresh server
+        k = min([k for k in range(nreq) if md[k]], key=lambda k: sizes[k])
+        alone = api.Server(hbm_fraction=0.8, spline_order=4, precise=args.precise, dt_ps=DT_PS,
+                           friction=1.0, temperature=300.0, seed=31)
+        s = systems[k]
+        rid = alone.submit(0, handles[k][0], handles[k][1], s.box, s.settings, xs[k], 7000 + k,
+                           int(steps[k]))
+        alone.wait(rid, 3600.0)
+        same = bool(np.array_equal(alone.coordinates(rid), srv.coordinates(ids[k])))
+        alone.close()
+    line = {
+        "metric": "serving: aggregate ns/day with p50/p99 latency", "value": value,
+        "unit": "ns/day", "n_gpus": 1, "steps": nreq, "warmup": 0,
+        "ms_per_step": 1e3 * wall / max(1, nreq), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (forces), f64 (integration)",
+        "data": "synthetic (seeded generator and request stream)",
+        "config": {"workload": f"serve{nreq}: Poisson 50 req/s, 70 % MD U[100, 5000] steps, 30 % "
+                               "energy/force, atoms log-uniform 2,000-100,000, bead chain in "
+                               "TIP3P, PME spacing <= 1 A, order 4, cutoff 10 A, Langevin 300 K, "
+                               "dt 2 fs", "requests": nreq, "md_requests": int(md.sum()),
+                   "atoms": int(sum(sizes)), "hbm_fraction": 0.8},
+        "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                      "p50_md": float(np.percentile(lat[md], 50)) if md.any() else None,
+                      "p50_energy": float(np.percentile(lat[~md], 50)) if (~md).any() else None},
+        "wall_s": wall, "server": st, "force_rel_rms_vs_fp64": errs,
+        "smallest_md_request_same_alone": same, "clocks": clocks.summary(),
+    }
+    srv.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def make_integrator(api, spec, rank):
     kind = spec["integrator"]
     if kind == "langevin":
@@ -438,7 +551,9 @@ def main():
     ap.add_argument("--steps", type=int, default=100, help="timed iterations (20 MD steps each)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="chain23k", choices=sorted(WORKLOADS) + ["batch"])
+    ap.add_argument("--workload", default="chain23k",
+                    choices=sorted(WORKLOADS) + ["batch", "serve"])
+    ap.add_argument("--requests", type=int, default=40, help="serve workload: requests")
     ap.add_argument("--systems", type=int, default=256, help="batch workload: number of systems")
     ap.add_argument("--one-steps", type=int, default=2,
                     help="batch workload: timed segments per system in the one-by-one baseline "
@@ -450,6 +565,12 @@ def main():
                     help="direct-space kernel form: 0 tile batches, 1 grouped queues")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    if args.workload == "serve":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no "
+                              "serving layer"}))
+            return 0
+        return run_serve(args)
     if args.workload == "batch":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no "
