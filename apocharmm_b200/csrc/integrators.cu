@@ -15,7 +15,7 @@ namespace apo {
 
 namespace {
 
-constexpr int kThreads = 64;  // small blocks: a step spreads over all SMs even for small systems
+constexpr int kThreads = 256;
 constexpr int kMaxBlocks = 4096;
 
 // constraint group kinds
@@ -288,46 +288,87 @@ __global__ void __launch_bounds__(kThreads) langevin_kernel(Common c, double gam
     }
   }
   if (run) {
+    // all loads of the group first (every level of the chain atom -> slot ->
+    // gradient is issued for the whole group at once), then the arithmetic,
+    // then the stores: the kernel is bound by memory latency, not by math
     int at[4];
     const int m = group_atoms(c, g, at);
     const int2 meta = c.gmeta[g];
-    d3 o[4], n[4], dp[4];
-    for (int k = 0; k < m; ++k) {
-      const int a = at[k];
-      const double4 x = c.coords[a];
-      const double4 v = c.vel[a];
-      o[k] = xyz(x);
-      dp[k] = xyz(c.dprev[a]);
-      const d3 gr = take_grad(c.force, c.stride, c.glo2loc[a]);
-      curandStatePhilox4_32_10_t st;
-      unsigned long long p = pos;
-      if (c.sys_seed) {  // a system's own stream, the same alone or among others
-        const int sy = c.sys_of_atom[a];
-        curand_init(seed ^ c.sys_seed[sy], (unsigned long long)(a - c.atom_off[sy]), 0ull, &st);
-        if (c.sys_rng0) p += c.sys_rng0[sy];
-      } else {
-        curand_init(seed, (unsigned long long)a, 0ull, &st);
+    d3 o[4], n[4], dp[4], gr[4];
+    double im[4], qa[4];
+    int slot[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (k < m) {
+        const int a = at[k];
+        const double4 x = c.coords[a];
+        o[k] = xyz(x);
+        qa[k] = x.w;
+        im[k] = c.vel[a].w;
+        dp[k] = xyz(c.dprev[a]);
+        slot[k] = c.glo2loc[a];
       }
-      skipahead(p, &st);
-      const float4 rn = curand_normal4(&st);
-      const double rdf = sqrt(2.0 * gamma * kbt / v.w) / dt;
-      const double fact = dt2 * v.w * denom;
-      const d3 f = gr + rdf * mk(rn.x, rn.y, rn.z);
-      n[k] = o[k] + (alpha * dp[k] - fact * f);
+    }
+    long long gi[4][3];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (k < m) {
+        gi[k][0] = c.force[slot[k]];
+        gi[k][1] = c.force[c.stride + slot[k]];
+        gi[k][2] = c.force[2 * c.stride + slot[k]];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (k < m) {  // cleared for the next force evaluation
+        c.force[slot[k]] = 0;
+        c.force[c.stride + slot[k]] = 0;
+        c.force[2 * c.stride + slot[k]] = 0;
+        gr[k] = mk((double)gi[k][0] * kInvForceScale, (double)gi[k][1] * kInvForceScale,
+                   (double)gi[k][2] * kInvForceScale);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (k < m) {
+        const int a = at[k];
+        curandStatePhilox4_32_10_t st;
+        unsigned long long p = pos;
+        if (c.sys_seed) {  // a system's own stream, the same alone or among others
+          const int sy = c.sys_of_atom[a];
+          curand_init(seed ^ c.sys_seed[sy], (unsigned long long)(a - c.atom_off[sy]), 0ull, &st);
+          if (c.sys_rng0) p += c.sys_rng0[sy];
+        } else {
+          curand_init(seed, (unsigned long long)a, 0ull, &st);
+        }
+        skipahead(p, &st);
+        const float4 rn = curand_normal4(&st);
+        const double rdf = sqrt(2.0 * gamma * kbt / im[k]) / dt;
+        const double fact = dt2 * im[k] * denom;
+        const d3 f = gr[k] + rdf * mk(rn.x, rn.y, rn.z);
+        n[k] = o[k] + (alpha * dp[k] - fact * f);
+      }
     }
     apply_constraint(meta.x, m, o, n, c.sk, c.shake_p, meta.y);
-    for (int k = 0; k < m; ++k) {
-      const int a = at[k];
-      const d3 d = n[k] - o[k];
-      const d3 v = vfac * (d + dp[k]);
-      const double mass = 1.0 / c.vel[a].w;
-      const d3 u1 = idt * dp[k], u2 = idt * d;
-      const double kon = 0.5 * mass * dot(v, v);
-      ke0 += (0.5 * mass * dot(u1, u1) + kon + 0.5 * mass * dot(u2, u2)) / 3.0;
-      ke1 += kon;
-      c.vel[a] = make_double4(v.x, v.y, v.z, c.vel[a].w);
-      c.dprev[a] = make_double4(d.x, d.y, d.z, 0.0);
-      store_position(a, n[k], c.coords, c.xyzq, c.glo2loc, c.slot_off, c.xyzq_s);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (k < m) {
+        const int a = at[k];
+        const d3 d = n[k] - o[k];
+        const d3 v = vfac * (d + dp[k]);
+        const double mass = 1.0 / im[k];
+        const d3 u1 = idt * dp[k], u2 = idt * d;
+        const double kon = 0.5 * mass * dot(v, v);
+        ke0 += (0.5 * mass * dot(u1, u1) + kon + 0.5 * mass * dot(u2, u2)) / 3.0;
+        ke1 += kon;
+        c.vel[a] = make_double4(v.x, v.y, v.z, im[k]);
+        c.dprev[a] = make_double4(d.x, d.y, d.z, 0.0);
+        c.coords[a] = make_double4(n[k].x, n[k].y, n[k].z, qa[k]);
+        c.xyzq[a] = make_float4((float)n[k].x, (float)n[k].y, (float)n[k].z, (float)qa[k]);
+        const double4 so = c.slot_off[slot[k]];
+        c.xyzq_s[slot[k]] = make_float4((float)(n[k].x + so.x), (float)(n[k].y + so.y),
+                                        (float)(n[k].z + so.z), (float)qa[k]);
+      }
     }
   }
   block_partials(ke0, ke1, c.partials);

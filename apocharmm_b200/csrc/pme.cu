@@ -333,12 +333,25 @@ __global__ void __launch_bounds__(kPlaneThreads) plane_fwd_kernel(PmeDims d, int
   }
   const int nx = d.nx, ny = d.ny, nxc = d.nxc, rowp = nx + 2, h = nx / 2;
   int *plane = qgrid + (size_t)z * nx * ny;
-  for (int idx = threadIdx.x; idx < nx * ny; idx += blockDim.x) {
-    const int y = idx / nx, x = idx - y * nx;
-    const int v = plane[idx];
-    plane[idx] = 0;  // ready for the next spread
-    float *slot = reinterpret_cast<float *>(&buf[(y >> 1) * rowp + dig_rev(x, d.ax)]);
-    slot[y & 1] = (float)v * kInvGridScale;
+  // four loads in flight per thread before any store (latency-bound loop)
+  const int total = nx * ny;
+  for (int base = threadIdx.x; base < total; base += 4 * blockDim.x) {
+    int v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int idx = base + u * blockDim.x;
+      v[u] = idx < total ? plane[idx] : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int idx = base + u * blockDim.x;
+      if (idx < total) {
+        plane[idx] = 0;  // ready for the next spread
+        const int y = idx / nx, x = idx - y * nx;
+        float *slot = reinterpret_cast<float *>(&buf[(y >> 1) * rowp + dig_rev(x, d.ax)]);
+        slot[y & 1] = (float)v[u] * kInvGridScale;
+      }
+    }
   }
   __syncthreads();
   fft_dit(buf, ny / 2, rowp, 1, d.ax, twx, -1.f);
