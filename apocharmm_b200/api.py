@@ -287,7 +287,8 @@ class CharmmContext(_Handle):
         return p.value or 0
 
 
-def system_context(sys, workdir: str, precise: bool = False, settings=None):
+def system_context(sys, workdir: str, precise: bool = False, settings=None,
+                   tiles_per_work: int = None):
     """Writes `sys` (apocharmm_b200.systems.System) as CHARMM files, loads it
     through the C ABI and returns (psf, prm, fm, ctx).  `settings` overrides
     sys.settings (kappa, nfft, order, ctofnb, ctonnb, cutnb)."""
@@ -306,6 +307,8 @@ def system_context(sys, workdir: str, precise: bool = False, settings=None):
     fm.setFFTGrid(*st["nfft"])
     fm.setPmeSplineOrder(st["order"])
     fm.setPrecisionMode(precise)
+    if tiles_per_work is not None:
+        fm.setTilesPerWork(tiles_per_work)
     ctx = CharmmContext(fm)
     ctx.setCoordinates(sys.pos)
     return psf, prm, fm, ctx

@@ -561,6 +561,8 @@ def main():
     ap.add_argument("--precise", action="store_true", help="precision form")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--tiles-per-work", type=int, default=8,
+                    help="j-tiles per direct-space work item")
     ap.add_argument("--direct-kernel", type=int, default=0, choices=[0, 1],
                     help="direct-space kernel form: 0 tile batches, 1 grouped queues")
     args = ap.parse_args()
@@ -594,7 +596,8 @@ def main():
     spec = WORKLOADS[args.workload]
     s = make_system(args.workload)
     work = tempfile.mkdtemp(prefix=f"apo_bench_{rank}_")
-    psf, prm, fm, ctx = api.system_context(s, work, precise=args.precise)
+    psf, prm, fm, ctx = api.system_context(s, work, precise=args.precise,
+                                           tiles_per_work=args.tiles_per_work)
     fm.setDirectKernel(args.direct_kernel)
     # remove the close contacts of the generated structure (deterministic)
     s.pos = api.relax(ctx, api.water_indices(s), iterations=RELAX_ITERATIONS,
@@ -715,6 +718,7 @@ def main():
                        "atoms": s.n_atoms, "md_steps_per_iteration": SEG,
                        "form": "precision" if args.precise else "plain",
                        "direct_kernel": ["tile batches", "grouped queues"][args.direct_kernel],
+                       "tiles_per_work": args.tiles_per_work,
                        "l2": "flushed (256 MB device write) before every timed iteration, "
                              "outside the timed interval",
                        "parallelism": f"replicas x{world}"},
