@@ -343,6 +343,55 @@ class DcdSubscriber(Subscriber):
         call("apo_dcd_subscriber_as_subscriber", ctypes.byref(self._view), self._h)
 
 
+class RestartSubscriber(Subscriber):
+    """Rewrites a CHARMM-layout restart file every `report_frequency` steps
+    (Langevin thermostat and Nose-Hoover integrators)."""
+
+    _destroy = "apo_restart_subscriber_destroy"
+
+    def __init__(self, path, report_frequency: int | None = None):
+        super().__init__()
+        if report_frequency is None:
+            call("apo_restart_subscriber_create", ctypes.byref(self._h), _enc(path))
+        else:
+            call("apo_restart_subscriber_create_with_report_frequency", ctypes.byref(self._h),
+                 _enc(path), _i(report_frequency))
+        call("apo_restart_subscriber_as_subscriber", ctypes.byref(self._view), self._h)
+
+
+def read_restart_file(path) -> dict:
+    """Scalars and per-atom sections of a restart file (no device needed)."""
+    natom, ndegf, has_rng = _i(), _i(), _i()
+    npriv = ctypes.c_longlong()
+    seed, rngpos = ctypes.c_ulonglong(), ctypes.c_ulonglong()
+    box = np.zeros(3)
+    pnhv, pnhf = _d(), _d()
+    call("apo_restart_file_read_header", _enc(path), ctypes.byref(natom), ctypes.byref(npriv),
+         ctypes.byref(ndegf), ctypes.byref(seed), ctypes.byref(rngpos), ctypes.byref(has_rng),
+         _ptr(box), ctypes.byref(pnhv), ctypes.byref(pnhf))
+    n = natom.value
+    xold, vel, delta = (np.zeros((max(n, 1), 3)) for _ in range(3))
+    call("apo_restart_file_read", _enc(path), _i(n), _ptr(xold), _ptr(vel), _ptr(delta))
+    return {"natom": n, "npriv": npriv.value, "ndegf": ndegf.value, "seed": seed.value,
+            "rngpos": rngpos.value if has_rng.value else None, "box": box,
+            "pnhv": pnhv.value, "pnhf": pnhf.value,
+            "xold": xold[:n], "vel": vel[:n], "delta": delta[:n]}
+
+
+def write_restart_file(path, xold, vel, delta, box, npriv: int = 0, ndegf: int = 0,
+                       seed: int = 0, rngpos: int | None = None, pnhv: float = 0.0,
+                       pnhf: float = 0.0):
+    """Writes a restart file from host arrays (natom x 3 each)."""
+    arrs = [np.ascontiguousarray(a, dtype=np.float64).reshape(-1, 3) for a in (xold, vel, delta)]
+    n = arrs[0].shape[0]
+    if any(a.shape[0] != n for a in arrs):
+        raise ValueError("xold, vel and delta must have the same number of atoms")
+    b = np.ascontiguousarray(box, dtype=np.float64).reshape(3)
+    call("apo_restart_file_write", _enc(path), _i(n), ctypes.c_longlong(npriv), _i(ndegf),
+         ctypes.c_ulonglong(seed), ctypes.c_ulonglong(rngpos or 0), _i(rngpos is not None),
+         _ptr(b), _d(pnhv), _d(pnhf), _ptr(arrs[0]), _ptr(arrs[1]), _ptr(arrs[2]))
+
+
 class CudaIntegrator(_Handle):
     """Base of the integrators; `_view` is the borrowed apo_cuda_integrator."""
 

@@ -3,8 +3,11 @@
 #include "apocharmm_c/CudaLangevinThermostatIntegrator.h"
 #include "apocharmm_c/CudaNoseHooverIntegrator.h"
 #include "apocharmm_c/DcdSubscriber.h"
+#include "apocharmm_c/RestartFile.h"
 #include "apocharmm_c/RestartSubscriber.h"
 #include "apocharmm_c/Subscriber.h"
+#include <algorithm>
+
 #include "capi_internal.h"
 #include "integrators.h"
 #include "subscribers.h"
@@ -18,7 +21,7 @@ struct apo_dcd_subscriber {
 };
 struct apo_restart_subscriber {
   apo_subscriber base;
-  std::shared_ptr<apo::Subscriber> object;
+  std::shared_ptr<apo::RestartSubscriber> object;
 };
 struct apo_cuda_integrator { std::shared_ptr<apo::CudaIntegrator> object; };
 struct apo_cuda_nose_hoover_integrator {
@@ -83,8 +86,8 @@ extern "C" apo_status apo_cuda_integrator_initialize_from_restart_file(apo_cuda_
   return guard([&]() -> apo_status {
     APO_RETURN_IF(require_handle(it, fn, "CudaIntegrator"));
     APO_RETURN_IF(require_string(path, fn, "path"));
-    return set_error(APO_STATUS_NOT_IMPLEMENTED,
-                     std::string(fn) + ": restart files are not implemented on this engine");
+    it->object->initializeFromRestartFile(path);
+    return APO_STATUS_OK;
   }, fn);
 }
 
@@ -362,9 +365,12 @@ extern "C" apo_status apo_restart_subscriber_create_with_report_frequency(apo_re
   return guard([&]() -> apo_status {
     APO_RETURN_IF(prepare_out(out, fn));
     APO_RETURN_IF(require_string(path, fn, "path"));
-    (void)f;
-    return set_error(APO_STATUS_NOT_IMPLEMENTED,
-                     std::string(fn) + ": restart files are not implemented on this engine");
+    if (f <= 0) return invalid(fn, "report frequency must be positive");
+    auto h = std::make_unique<apo_restart_subscriber>();
+    h->object = std::make_shared<apo::RestartSubscriber>(path, f);
+    h->base.object = h->object;
+    *out = h.release();
+    return APO_STATUS_OK;
   }, fn);
 }
 extern "C" apo_status apo_restart_subscriber_create(apo_restart_subscriber **out, const char *path) {
@@ -377,6 +383,76 @@ extern "C" apo_status apo_restart_subscriber_as_subscriber(apo_subscriber **out,
     APO_RETURN_IF(prepare_out(out, fn));
     APO_RETURN_IF(require_handle(s, fn, "RestartSubscriber"));
     *out = &s->base;
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+// ---------------------------------------------------------- restart files ----
+
+extern "C" apo_status apo_restart_file_read_header(const char *path, int *natom, long long *npriv,
+                                                   int *ndegf, unsigned long long *seed,
+                                                   unsigned long long *rngpos, int *has_rng,
+                                                   double *box3, double *pnhv, double *pnhf) {
+  const char *fn = "apo_restart_file_read_header";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_string(path, fn, "path"));
+    if (!natom || !npriv || !ndegf || !seed || !rngpos || !has_rng || !box3 || !pnhv || !pnhf)
+      return invalid(fn, "null output pointer");
+    const apo::RestartRecord r = apo::readRestartFile(path);
+    *natom = r.natom;
+    *npriv = r.npriv;
+    *ndegf = r.ndegf;
+    *seed = r.seed;
+    *rngpos = r.rngpos;
+    *has_rng = r.has_rng ? 1 : 0;
+    for (int d = 0; d < 3; ++d) box3[d] = r.box[d];
+    *pnhv = r.pnhv;
+    *pnhf = r.pnhf;
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_restart_file_read(const char *path, const int natom, double *xold,
+                                            double *vel, double *delta) {
+  const char *fn = "apo_restart_file_read";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_string(path, fn, "path"));
+    if (!xold || !vel || !delta) return invalid(fn, "null output array");
+    const apo::RestartRecord r = apo::readRestartFile(path);
+    if (r.natom != natom) return invalid(fn, "natom does not match the file");
+    std::copy(r.xold.begin(), r.xold.end(), xold);
+    std::copy(r.vel.begin(), r.vel.end(), vel);
+    std::copy(r.delta.begin(), r.delta.end(), delta);
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_restart_file_write(const char *path, const int natom, const long long npriv,
+                                             const int ndegf, const unsigned long long seed,
+                                             const unsigned long long rngpos, const int has_rng,
+                                             const double *box3, const double pnhv, const double pnhf,
+                                             const double *xold, const double *vel,
+                                             const double *delta) {
+  const char *fn = "apo_restart_file_write";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_string(path, fn, "path"));
+    if (natom < 0 || npriv < 0) return invalid(fn, "natom and npriv must be >= 0");
+    if (!box3 || (natom > 0 && (!xold || !vel || !delta))) return invalid(fn, "null input array");
+    apo::RestartRecord r;
+    r.natom = natom;
+    r.npriv = r.nstep = npriv;
+    r.ndegf = ndegf;
+    r.seed = seed;
+    r.rngpos = rngpos;
+    r.has_rng = has_rng != 0;
+    for (int d = 0; d < 3; ++d) r.box[d] = box3[d];
+    r.pnhv = pnhv;
+    r.pnhf = pnhf;
+    const size_t n3 = (size_t)3 * natom;
+    r.xold.assign(xold, xold + n3);
+    r.vel.assign(vel, vel + n3);
+    r.delta.assign(delta, delta + n3);
+    apo::writeRestartFile(path, r);
     return APO_STATUS_OK;
   }, fn);
 }

@@ -838,6 +838,7 @@ void CudaIntegrator::segment(int nsteps, cudaStream_t s) {
 
 void CudaIntegrator::subscribe(std::shared_ptr<Subscriber> sub) {
   if (!sub) throw std::invalid_argument("null subscriber");
+  sub->attach(this);
   m_Subscribers.push_back(std::move(sub));
 }
 
@@ -955,6 +956,93 @@ long long CudaIntegrator::deviceStep() {
   APO_CUDA(cudaStreamSynchronize(stream()));
   APO_CUDA(cudaMemcpy(&h, m_S->sc.p, sizeof(h), cudaMemcpyDeviceToHost));
   return h.step;
+}
+
+RestartRecord CudaIntegrator::restartRecord() {
+  if (!m_S || !m_Ctx) throw std::runtime_error("restart: no CharmmContext was set for this integrator");
+  auto *lt = dynamic_cast<CudaLangevinThermostatIntegrator *>(this);
+  auto *nh = dynamic_cast<CudaNoseHooverIntegrator *>(this);
+  if (!lt && !nh)
+    throw std::runtime_error("Attempted to write a restart file for an unsupported integrator type. "
+                             "The supported integrators are CudaLangevinThermostatIntegrator and "
+                             "CudaNoseHooverIntegrator.");
+  if (m_Ctx->getForceManager()->isMulti())
+    throw std::runtime_error("restart files describe one system: not available for a "
+                             "multi-system context");
+  cudaStream_t s = stream();
+  Scalars h;
+  APO_CUDA(cudaStreamSynchronize(s));
+  APO_CUDA(cudaMemcpy(&h, m_S->sc.p, sizeof(h), cudaMemcpyDeviceToHost));
+  RestartRecord r;
+  r.box = m_Ctx->getForceManager()->getBoxDimensions();
+  r.natom = m_S->natom;
+  r.npriv = m_Step;
+  r.nstep = m_Step;
+  r.ndegf = m_Ctx->getDegreesOfFreedom();
+  r.avetem = h.avgT[0];
+  if (lt) {
+    r.seed = lt->getThermostatRngSeed();
+    r.has_rng = true;
+    r.rngpos = h.rngpos;
+  } else {
+    r.pnhv = h.piston_v;
+    r.pnhf = h.piston_f;
+  }
+  r.xold = m_Ctx->getCoordinates();
+  r.vel = m_Ctx->getVelocities();
+  std::vector<double4> d(m_S->natom);
+  APO_CUDA(cudaMemcpy(d.data(), m_S->dprev.p, d.size() * sizeof(double4), cudaMemcpyDeviceToHost));
+  r.delta.resize((size_t)3 * m_S->natom);
+  for (int i = 0; i < m_S->natom; ++i) {
+    r.delta[3 * (size_t)i] = d[i].x;
+    r.delta[3 * (size_t)i + 1] = d[i].y;
+    r.delta[3 * (size_t)i + 2] = d[i].z;
+  }
+  return r;
+}
+
+void CudaIntegrator::initializeFromRestartFile(const std::string &path) {
+  if (path.empty()) throw std::invalid_argument("initializeFromRestartFile: empty file name");
+  if (!m_S || !m_Ctx)
+    throw std::runtime_error("CharmmContext must be set before initializing from a restart file");
+  auto *lt = dynamic_cast<CudaLangevinThermostatIntegrator *>(this);
+  auto *nh = dynamic_cast<CudaNoseHooverIntegrator *>(this);
+  if (!lt && !nh)
+    throw std::runtime_error("initializeFromRestartFile: only the Langevin thermostat and "
+                             "Nose-Hoover integrators read restart files");
+  auto fm = m_Ctx->getForceManager();
+  if (fm->isMulti())
+    throw std::runtime_error("restart files describe one system: not available for a "
+                             "multi-system context");
+  const RestartRecord r = readRestartFile(path);
+  if (r.natom != m_Ctx->getNumAtoms())
+    throw std::invalid_argument("NATOM mismatch in restart file \"" + path + "\"");
+  if (r.ndegf != m_Ctx->getDegreesOfFreedom())
+    throw std::invalid_argument("NDEGF mismatch in restart file \"" + path + "\"");
+  if (r.box != fm->getBoxDimensions())
+    throw std::invalid_argument("restart file \"" + path + "\" holds another box: set it on the "
+                                "ForceManager before the integrator is created");
+  m_Ctx->setCoordinates(r.xold);
+  m_Ctx->setVelocities(r.vel);
+  std::vector<double4> d(r.natom);
+  for (int i = 0; i < r.natom; ++i)
+    d[i] = make_double4(r.delta[3 * (size_t)i], r.delta[3 * (size_t)i + 1],
+                        r.delta[3 * (size_t)i + 2], 0.0);
+  APO_CUDA(cudaMemcpy(m_S->dprev.p, d.data(), d.size() * sizeof(double4), cudaMemcpyHostToDevice));
+  Scalars h;
+  APO_CUDA(cudaMemcpy(&h, m_S->sc.p, sizeof(h), cudaMemcpyDeviceToHost));
+  h.step = r.npriv;
+  if (lt) {
+    lt->setThermostatRngSeed(r.seed);
+    // a file without the APO tag carries no RNG position (as the reference reads it)
+    h.rngpos = (r.apo && r.has_rng) ? r.rngpos : 0ull;
+  } else {
+    h.piston_v = r.pnhv;
+    h.piston_f = r.pnhf;
+  }
+  APO_CUDA(cudaMemcpy(m_S->sc.p, &h, sizeof(h), cudaMemcpyHostToDevice));
+  m_Step = r.npriv;
+  clearGraphs();  // the captured launches hold the seed
 }
 
 unsigned long long CudaLangevinThermostatIntegrator::getRngSequencePos() {

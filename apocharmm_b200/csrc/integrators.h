@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "restart.h"
 #include "subscribers.h"
 
 namespace apo {
@@ -65,6 +66,16 @@ class CudaIntegrator : public std::enable_shared_from_this<CudaIntegrator> {
                        const std::vector<long long> &stop);
   // steps taken by this integrator, read from the device counter
   long long deviceStep();
+  // the state a restart file carries (Langevin thermostat and Nose-Hoover
+  // only, as in src/RestartSubscriber.cu:53-68; one system)
+  RestartRecord restartRecord();
+  // continue the run a restart file describes: coordinates, velocities,
+  // the position-Verlet delta, the step counters and the thermostat seed
+  // and RNG position (Langevin) or piston velocity and force (Nose-Hoover)
+  // (src/CudaLangevinThermostatIntegrator.cu:264-545,
+  // src/CudaNoseHooverIntegrator.cu:337-615).  The context must already
+  // hold the box of the file.
+  void initializeFromRestartFile(const std::string &path);
 
  protected:
   virtual void initialize() = 0;

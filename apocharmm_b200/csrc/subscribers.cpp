@@ -8,6 +8,8 @@
 
 #include "common.h"
 #include "engine.h"
+#include "integrators.h"
+#include "restart.h"
 
 namespace apo {
 
@@ -77,6 +79,22 @@ void DcdSubscriber::update(CharmmContext &ctx, long long step, double dtPs) {
   ++m_Frames;
   writeHeader(n, step - (long long)(m_Frames - 1) * m_Freq, dtPs);
   std::fflush(m_File);
+}
+
+RestartSubscriber::RestartSubscriber(const std::string &path, int f)
+    : Subscriber(f), m_Path(path) {
+  // fail at creation, not at the first report, when the path is unusable
+  std::FILE *t = std::fopen(path.c_str(), "a");
+  if (!t) throw std::invalid_argument("Cannot open restart file " + path);
+  std::fclose(t);
+}
+
+void RestartSubscriber::update(CharmmContext &, long long, double) {
+  if (!m_Integrator) throw std::runtime_error("RestartSubscriber: not subscribed to an integrator");
+  RestartRecord r = m_Integrator->restartRecord();
+  r.nsavc = m_Freq;
+  writeRestartFile(m_Path, r);
+  ++m_Writes;
 }
 
 }  // namespace apo
