@@ -183,6 +183,49 @@ class ForceManager(_Handle):
         call("apo_force_manager_get_fft_grid", a, self._h)
         return list(a)
 
+    def subscribe(self, force: "HarmonicRestraintForce", tag: str):
+        """Adds a plug-in force to every evaluation; its energy is reported as `tag`."""
+        self._plugins = getattr(self, "_plugins", {})
+        call("apo_force_manager_subscribe_harmonic_restraint", self._h, force.handle, _enc(tag))
+        self._plugins[tag] = force
+
+    def unsubscribe(self, tag: str) -> bool:
+        removed = _i()
+        call("apo_force_manager_unsubscribe", ctypes.byref(removed), self._h, _enc(tag))
+        getattr(self, "_plugins", {}).pop(tag, None)
+        return bool(removed.value)
+
+
+class HarmonicRestraintForce(_Handle):
+    """E = sum k_i m_i |r_i - r0_i|^2 over the selected atoms (masses 1 unless set)."""
+
+    _destroy = "apo_harmonic_restraint_force_destroy"
+
+    def __init__(self, num_atoms: int):
+        super().__init__()
+        self._n = int(num_atoms)
+        call("apo_harmonic_restraint_force_create", ctypes.byref(self._h), _i(self._n))
+
+    def setSelection(self, atoms):
+        a = np.ascontiguousarray(atoms, dtype=np.int32).reshape(-1)
+        call("apo_harmonic_restraint_force_set_selection", self._h, _ptr(a), _sz(a.size))
+
+    def setForceConstant(self, k: float):
+        call("apo_harmonic_restraint_force_set_force_constant", self._h, _d(k))
+
+    def _per_atom(self, fn, v, per):
+        a = np.ascontiguousarray(v, dtype=np.float64).reshape(-1)
+        call(fn, self._h, _ptr(a), _sz(a.size))
+
+    def setForceConstants(self, k):
+        self._per_atom("apo_harmonic_restraint_force_set_force_constants", k, 1)
+
+    def setReferenceCoordinates(self, xyz):
+        self._per_atom("apo_harmonic_restraint_force_set_reference_coordinates", xyz, 3)
+
+    def setMasses(self, m):
+        self._per_atom("apo_harmonic_restraint_force_set_masses", m, 1)
+
 
 class CharmmContext(_Handle):
     _destroy = "apo_charmm_context_destroy"
@@ -246,6 +289,12 @@ class CharmmContext(_Handle):
     def getPotentialEnergy(self) -> float:
         v = _d()
         call("apo_charmm_context_get_potential_energy", ctypes.byref(v), self._h)
+        return v.value
+
+    def getEnergyComponent(self, name: str) -> float:
+        """A built-in energy term or a plug-in force's energy, by name."""
+        v = _d()
+        call("apo_charmm_context_get_energy_component", ctypes.byref(v), self._h, _enc(name))
         return v.value
 
     def getVirial(self) -> np.ndarray:

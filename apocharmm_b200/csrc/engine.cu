@@ -225,6 +225,7 @@ void ForceManager::initialize() {
   createStreams();
   m_ListBuilt = false;
   m_Initialized = true;
+  for (auto &p : m_Plugins) p.second->initialize(m_Top.natom, m_Box);
 }
 
 void ForceManager::createStreams() {
@@ -488,6 +489,66 @@ void ForceManager::calcForce(const float4 *d_xyzq, bool calcEnergy, bool calcVir
     APO_CUDA(cudaEventRecord(m_EvBond, m_SBond));
     APO_CUDA(cudaStreamWaitEvent(s, m_EvBond, 0));
   }
+  if (!m_Plugins.empty()) {
+    if (!m_StateCoords) throw std::runtime_error("ForceManager: no state coordinates attached");
+    if (calcEnergy)
+      APO_CUDA(cudaMemsetAsync(m_PluginEnergy.p, 0, kMaxPlugins * sizeof(long long), s));
+    for (size_t k = 0; k < m_Plugins.size(); ++k) {
+      ForcePluginArgs pa;
+      pa.natom = m_Top.natom;
+      pa.coords = m_StateCoords;
+      pa.xyzq = d_xyzq;
+      pa.glo2loc = m_Nbl.glo2loc;
+      pa.force = m_Force.p;
+      pa.stride = m_Stride;
+      pa.energy = m_PluginEnergy.p + k;
+      for (int d = 0; d < 3; ++d) pa.box[d] = m_Box[d];
+      m_Plugins[k].second->calcForce(pa, calcEnergy, calcVirial, s);
+    }
+  }
+}
+
+void ForceManager::subscribe(std::shared_ptr<ForcePlugin> force, const std::string &tag) {
+  if (!force) throw std::invalid_argument("ForceManager::subscribe: null force");
+  if (m_Multi)
+    throw std::invalid_argument("ForceManager::subscribe: plug-in forces need a single-system "
+                                "force manager");
+  if (tag.empty()) throw std::invalid_argument("ForceManager::subscribe: empty tag");
+  for (int k = 0; k < kNumEnergyTerms; ++k)
+    if (tag == kEnergyNames[k])
+      throw std::invalid_argument("ForceManager::subscribe: tag '" + tag + "' names a built-in term");
+  for (auto &p : m_Plugins)
+    if (p.first == tag)
+      throw std::invalid_argument("ForceManager::subscribe: tag '" + tag + "' is already in use");
+  if ((int)m_Plugins.size() >= kMaxPlugins)
+    throw std::invalid_argument("ForceManager::subscribe: at most 16 plug-in forces");
+  if (!m_PluginEnergy.p) {
+    m_PluginEnergy.alloc(kMaxPlugins);
+    APO_CUDA(cudaMemset(m_PluginEnergy.p, 0, kMaxPlugins * sizeof(long long)));
+  }
+  if (m_Initialized) force->initialize(m_Top.natom, m_Box);
+  m_Plugins.emplace_back(tag, std::move(force));
+  ++m_PluginGen;
+}
+
+bool ForceManager::unsubscribe(const std::string &tag) {
+  for (size_t k = 0; k < m_Plugins.size(); ++k)
+    if (m_Plugins[k].first == tag) {
+      m_Plugins.erase(m_Plugins.begin() + k);
+      ++m_PluginGen;
+      return true;
+    }
+  return false;
+}
+
+bool ForceManager::unsubscribe(const ForcePlugin *force) {
+  for (size_t k = 0; k < m_Plugins.size(); ++k)
+    if (m_Plugins[k].second.get() == force) {
+      m_Plugins.erase(m_Plugins.begin() + k);
+      ++m_PluginGen;
+      return true;
+    }
+  return false;
 }
 
 std::map<std::string, double> ForceManager::getEnergyComponents(cudaStream_t s) {
@@ -503,6 +564,13 @@ std::map<std::string, double> ForceManager::getEnergyComponents(cudaStream_t s) 
   std::map<std::string, double> m;
   for (int k = 0; k < kNumEnergyTerms; ++k) m[kEnergyNames[k]] = (double)e[k] * kInvEnergyScale;
   m["ewse"] = (m_ComponentMask & 4) ? m_SelfEnergy : 0.0;
+  if (!m_Plugins.empty()) {
+    long long pe[kMaxPlugins];
+    APO_CUDA(cudaMemcpyAsync(pe, m_PluginEnergy.p, sizeof(pe), cudaMemcpyDeviceToHost, s));
+    APO_CUDA(cudaStreamSynchronize(s));
+    for (size_t k = 0; k < m_Plugins.size(); ++k)
+      m[m_Plugins[k].first] = (double)pe[k] * kInvEnergyScale;
+  }
   return m;
 }
 

@@ -24,6 +24,7 @@
 #include "bonded.h"
 #include "charmm_io.h"
 #include "common.h"
+#include "force_plugins.h"
 #include "nblist.h"
 #include "nonbonded.h"
 #include "pme.h"
@@ -116,6 +117,15 @@ class ForceManager {
   int getDirectKernel() const { return m_NbVariant; }
   // bit mask of the parts evaluated: 1 bonded+1-4, 2 direct, 4 reciprocal
   void setComponentMask(int mask) { m_ComponentMask = mask; }
+  // extra force terms evaluated with every force call, their energies
+  // reported under `tag` (ForceManager::subscribe/unsubscribe,
+  // include/ForceManager.h:420-475); one system only
+  void subscribe(std::shared_ptr<ForcePlugin> force, const std::string &tag);
+  bool unsubscribe(const std::string &tag);
+  bool unsubscribe(const ForcePlugin *force);
+  // changes whenever the set of plug-ins changes (captured graphs are stale)
+  int pluginGeneration() const { return m_PluginGen; }
+  static constexpr int kMaxPlugins = 16;
 
   const std::array<double, 3> &getBoxDimensions() const { return m_Box; }
   double getKappa() const { return m_Kappa; }
@@ -197,6 +207,9 @@ class ForceManager {
   int m_ComponentMask = 7;
   double m_SelfEnergy = 0.0;
   const double4 *m_StateCoords = nullptr;
+  std::vector<std::pair<std::string, std::shared_ptr<ForcePlugin>>> m_Plugins;
+  DeviceArray<long long> m_PluginEnergy;  // kMaxPlugins fixed-point slots
+  int m_PluginGen = 0;
   Topology m_Top;
 
   NeighborList m_Nbl;

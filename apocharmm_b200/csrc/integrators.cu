@@ -849,6 +849,11 @@ void CudaIntegrator::propagate(int numSteps) {
   cudaStream_t s = m_Ctx->stream();
   // the first list build sizes the buffers synchronously: never inside a capture
   m_Ctx->ensureNeighborList();
+  const int gen = m_Ctx->getForceManager()->pluginGeneration();
+  if (gen != m_PluginGen) {  // a plug-in force joined or left: capture again
+    clearGraphs();
+    m_PluginGen = gen;
+  }
   int left = numSteps;
   long long done = 0;
   while (left > 0) {

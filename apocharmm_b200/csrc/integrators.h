@@ -88,6 +88,7 @@ class CudaIntegrator : public std::enable_shared_from_this<CudaIntegrator> {
   bool m_Initialized = false;
   long long m_Step = 0;
   int m_KernelsPerStep = 0;
+  int m_PluginGen = -1;  // plug-in set the graphs were captured with
   std::shared_ptr<CharmmContext> m_Ctx;
   std::unique_ptr<IntegratorState> m_S;
   std::map<int, cudaGraphExec_t> m_Graphs;
