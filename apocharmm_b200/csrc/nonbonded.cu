@@ -34,6 +34,7 @@ NbSetup make_nb_setup(double Lx, double Ly, double Lz, double kappa, double roff
   s.kappa = (float)kappa;
   s.kappa2 = (float)(kappa * kappa);
   s.two_kappa_sqrtpi = (float)(2.0 * kappa / std::sqrt(M_PI));
+  s.ewald_e2 = (float)(-kappa * kappa / std::log(2.0));
   // VDW_VFSW constants (src/CudaPMEDirectForce.cu:318-330)
   double roff3 = roff * roff * roff, ron3 = ron * ron * ron;
   double roff6 = roff3 * roff3, ron6 = ron3 * ron3;
@@ -88,8 +89,19 @@ __device__ __forceinline__ T transpose_reduce8(T (&v)[8], int lane) {
 // coefficients fitted for relative accuracy on 0 <= x <= 6 (max relative
 // error 1.3e-7 in single precision; fit_erfc.py in this directory).  The
 // exponential is the one the Ewald force needs anyway.
+__device__ __forceinline__ float rcp_approx(float v) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(v));
+  return r;
+}
+__device__ __forceinline__ float ex2_approx(float v) {
+  float r;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(v));
+  return r;
+}
+
 __device__ __forceinline__ float erfc_from_exp(float x, float expv) {
-  const float t = __frcp_rn(fmaf(0.365f, x, 1.f));
+  const float t = rcp_approx(fmaf(0.365f, x, 1.f));
   float p = 6.816177070e-02f;
   p = fmaf(p, t, -3.500733972e-01f);
   p = fmaf(p, t, 6.125112772e-01f);
@@ -110,11 +122,44 @@ __device__ __forceinline__ void warp_flush(double v, long long *dst, int lane) {
   if (lane == 0 && iv) add_fixed(dst, iv);
 }
 
+// One pair: erfc-Ewald (src/CudaDirectForceKernels.cu:479-489) plus VDW_VFSW
+// (src/CudaDirectForceKernels.cu:263-286).  Returns f with gradient on i =
+// f (x_i - x_j); `in` = inside the cutoff and not excluded, anything else
+// gives 0 (r2raw may then be anything finite, including 0).  With ENERGY the
+// two energies of the pair are added to e_el / e_vdw.
+template <bool ENERGY>
+__device__ __forceinline__ float pair_force(const NbSetup &st, float r2raw, bool in, float qi,
+                                            float qj, float2 cc, double &e_el, double &e_vdw) {
+  const float r2 = in ? r2raw : 1.f;
+  const float rinv = rsqrtf(r2);
+  const float rr = r2 * rinv;
+  const float rinv2 = rinv * rinv;
+  const float qq = qi * qj;
+  const float exp_v = ex2_approx(st.ewald_e2 * r2);
+  const float erfc_v = erfc_from_exp(st.kappa * rr, exp_v);
+  const float el = qq * erfc_v * rinv;
+  const float fr_el = fmaf(-qq * st.two_kappa_sqrtpi, exp_v, -el);
+  const float rinv3 = rinv * rinv2, rinv6 = rinv3 * rinv3;
+  const bool sw = r2 > st.ron2;
+  const float A6 = sw ? st.k6 : 1.f, B6 = sw ? st.roffinv3 : 0.f;
+  const float A12 = sw ? st.k12 : 1.f, B12 = sw ? st.roffinv6 : 0.f;
+  const float t6 = rinv3 - B6, t12 = rinv6 - B12;
+  const float fr_vdw = (cc.x * A6) * t6 * rinv3 - (cc.y * A12) * t12 * rinv6;
+  if (ENERGY && in) {
+    const float C6 = sw ? 0.f : st.dv6, C12 = sw ? 0.f : st.dv12;
+    e_el += (double)el;
+    e_vdw += (double)((1.f / 12.f) * cc.y * (A12 * t12 * t12 + C12) -
+                      (1.f / 6.f) * cc.x * (A6 * t6 * t6 + C6));
+  }
+  return in ? (fr_vdw + fr_el) * rinv2 : 0.f;
+}
+
 template <bool ENERGY, bool PER_PAIR, bool VIRIAL = false, bool MULTI = false>
 __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
+  // the j-atoms of a tile that pass the box test, compacted: position and
+  // charge, and (LJ type | tile lane << 16)
   __shared__ float4 sh_xq[kWarps][32];
-  __shared__ int sh_t[kWarps][32];
-  __shared__ int sh_j[kWarps][32];
+  __shared__ int sh_tj[kWarps][32];
   extern __shared__ float2 sh_vdw[];
   int T = a.ntype;
   const int lane = threadIdx.x & 31;
@@ -193,10 +238,13 @@ __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
       if (jmask == 0u) continue;
       const unsigned excl = a.masks[(size_t)t * kTile + lane];
       const int nj = __popc(jmask);
+      const int tj_own = a.type_s[jslot] | (lane << 16);
       __syncwarp();
-      sh_xq[wib][lane] = xj;
-      sh_t[wib][lane] = a.type_s[jslot];
-      if (jnear) sh_j[wib][__popc(jmask & lt_mask)] = lane;
+      if (jnear) {
+        const int pos = __popc(jmask & lt_mask);
+        sh_xq[wib][pos] = xj;
+        sh_tj[wib][pos] = tj_own;
+      }
       __syncwarp();
 
       Acc fjx = 0, fjy = 0, fjz = 0;  // force of compacted j (lane&3)*8 + (lane>>2)
@@ -210,38 +258,13 @@ __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
           fy[jj] = 0;
           fz[jj] = 0;
           if (r < nj) {  // uniform across the warp
-            const int j = sh_j[wib][r];
-            const float4 pj = sh_xq[wib][j];
+            const float4 pj = sh_xq[wib][r];
+            const int tj = sh_tj[wib][r];
             const float dx = xi.x - pj.x, dy = xi.y - pj.y, dz = xi.z - pj.z;
             const float r2raw = dx * dx + dy * dy + dz * dz;
-            const bool in = !((excl >> j) & 1u) && r2raw < st.roff2;
-            const float r2 = in ? r2raw : 1.f;
-            const float rinv = rsqrtf(r2);
-            const float rr = r2 * rinv;
-            const float rinv2 = rinv * rinv;
-            // erfc-Ewald (src/CudaDirectForceKernels.cu:479-489)
-            const float qq = in ? qi * pj.w : 0.f;
-            const float exp_v = __expf(-st.kappa2 * r2);
-            const float erfc_v = erfc_from_exp(st.kappa * rr, exp_v);
-            const float e_el = qq * erfc_v * rinv;
-            const float fr_el = -qq * st.two_kappa_sqrtpi * exp_v - e_el;
-            // VDW_VFSW (src/CudaDirectForceKernels.cu:263-286)
-            float2 cc = sh_vdw[tab_off + ti + sh_t[wib][j]];
-            cc.x = in ? cc.x : 0.f;
-            cc.y = in ? cc.y : 0.f;
-            const float rinv3 = rinv * rinv2, rinv6 = rinv3 * rinv3;
-            const bool sw = r2 > st.ron2;
-            const float A6 = sw ? st.k6 : 1.f, B6 = sw ? st.roffinv3 : 0.f;
-            const float A12 = sw ? st.k12 : 1.f, B12 = sw ? st.roffinv6 : 0.f;
-            const float t6 = rinv3 - B6, t12 = rinv6 - B12;
-            const float fr_vdw = cc.x * A6 * t6 * rinv3 - cc.y * A12 * t12 * rinv6;
-            const float fij = (fr_vdw + fr_el) * rinv2;
-            if (ENERGY) {
-              const float C6 = sw ? 0.f : st.dv6, C12 = sw ? 0.f : st.dv12;
-              e_elec += (double)e_el;
-              e_vdw += (double)((1.f / 12.f) * cc.y * (A12 * t12 * t12 + C12) -
-                                (1.f / 6.f) * cc.x * (A6 * t6 * t6 + C6));
-            }
+            const bool in = !((excl >> (tj >> 16)) & 1u) && r2raw < st.roff2;
+            const float2 cc = sh_vdw[tab_off + ti + (tj & 0xffff)];
+            const float fij = pair_force<ENERGY>(st, r2raw, in, qi, pj.w, cc, e_elec, e_vdw);
             if (VIRIAL) {
               const float gx = fij * dx, gy = fij * dy, gz = fij * dz;
               vw[0] -= gx * dx;
@@ -282,7 +305,7 @@ __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
       }
       const int rown = (lane & 3) * 8 + (lane >> 2);
       if (rown < nj) {
-        const int jown = tl.x * kTile + sh_j[wib][rown];
+        const int jown = tl.x * kTile + (sh_tj[wib][rown] >> 16);
         if (PER_PAIR) {
           add_fixed(a.force + jown, (long long)fjx);
           add_fixed(a.force + stride + jown, (long long)fjy);
@@ -499,33 +522,9 @@ __global__ void __launch_bounds__(kThreads, 5) nbq_kernel(NbArgs a) {
         dx = in ? dx : 0.f;
         dy = in ? dy : 0.f;
         dz = in ? dz : 0.f;
-        const float r2 = in ? r2raw : 1.f;
-        const float rinv = rsqrtf(r2);
-        const float rr = r2 * rinv;
-        const float rinv2 = rinv * rinv;
-        // erfc-Ewald (src/CudaDirectForceKernels.cu:479-489)
-        const float qq = in ? qi * pj.w : 0.f;
-        const float exp_v = __expf(-st.kappa2 * r2);
-        const float erfc_v = erfc_from_exp(st.kappa * rr, exp_v);
-        const float e_el = qq * erfc_v * rinv;
-        const float fr_el = -qq * st.two_kappa_sqrtpi * exp_v - e_el;
-        // VDW_VFSW (src/CudaDirectForceKernels.cu:263-286)
-        float2 cc = sh_vdw[tab_off + ti + (in ? tj : 0)];
-        cc.x = in ? cc.x : 0.f;
-        cc.y = in ? cc.y : 0.f;
-        const float rinv3 = rinv * rinv2, rinv6 = rinv3 * rinv3;
-        const bool sw = r2 > st.ron2;
-        const float A6 = sw ? st.k6 : 1.f, B6 = sw ? st.roffinv3 : 0.f;
-        const float A12 = sw ? st.k12 : 1.f, B12 = sw ? st.roffinv6 : 0.f;
-        const float t6 = rinv3 - B6, t12 = rinv6 - B12;
-        const float fr_vdw = cc.x * A6 * t6 * rinv3 - cc.y * A12 * t12 * rinv6;
-        const float fij = (fr_vdw + fr_el) * rinv2;
-        if (ENERGY) {
-          const float C6 = sw ? 0.f : st.dv6, C12 = sw ? 0.f : st.dv12;
-          e_elec += (double)e_el;
-          e_vdw += (double)((1.f / 12.f) * cc.y * (A12 * t12 * t12 + C12) -
-                            (1.f / 6.f) * cc.x * (A6 * t6 * t6 + C6));
-        }
+        // stale entries: an in-range table index and a finite charge
+        const float2 cc = sh_vdw[tab_off + ti + (in ? tj : 0)];
+        const float fij = pair_force<ENERGY>(st, r2raw, in, qi, in ? pj.w : 0.f, cc, e_elec, e_vdw);
         if (VIRIAL) {
           const float gx = fij * dx, gy = fij * dy, gz = fij * dz;
           vw[0] -= gx * dx;

@@ -14,10 +14,11 @@ struct NbSetup {
   float Lx_lo, Ly_lo, Lz_lo;  // L - (float)L: the box as a two-float sum
   float roff2, ron2;
   float kappa, kappa2, two_kappa_sqrtpi;
+  float ewald_e2;             // -kappa^2 log2(e): exp(-kappa^2 r^2) = 2^(ewald_e2 r^2)
   float k6, k12, dv6, dv12, roffinv3, roffinv6;
   // LJ tables of this system (multi-system launches): ntype x ntype entries
   // at vdw + vdw_off (and vdw14 + vdw14_off for the 1-4 pairs)
-  int vdw_off = 0, vdw14_off = 0, ntype = 0, pad = 0;
+  int vdw_off = 0, vdw14_off = 0, ntype = 0;
 };
 
 // largest LJ type count of one system in a multi-system launch (the
