@@ -411,6 +411,7 @@ void ForceManager::calcForce(const float4 *d_xyzq, bool calcEnergy, bool calcVir
     a.setups = m_Setup.p;
     a.virial = virial;
     a.variant = m_NbVariant;
+    a.sched = m_Nbl.counts + 6;  // counts[6..7]: zero between launches
     cudaEvent_t t1 = nullptr;
     bool timer_capture = false;
     if (m_Timing) {

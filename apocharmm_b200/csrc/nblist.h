@@ -95,7 +95,8 @@ class NeighborList {
   int2 *tiles = nullptr;        // (j cluster, image code)
   unsigned *masks = nullptr;    // 32 words per tile
   int4 *work = nullptr;         // (i cluster, first tile, end tile, system)
-  int *counts = nullptr;        // [0] slots, [1] tiles, [2] work items
+  int *counts = nullptr;        // [0] slots, [1] tiles, [2] work items, [3..4] scan
+                                // carries, [6..7] direct-space schedule counters
   unsigned *error = nullptr;    // DeviceError bits
   int *cl_sys = nullptr;        // cluster -> system
   int *sys_of_atom = nullptr;   // atom -> system

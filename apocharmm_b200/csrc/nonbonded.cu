@@ -122,6 +122,21 @@ __device__ __forceinline__ void warp_flush(double v, long long *dst, int lane) {
   if (lane == 0 && iv) add_fixed(dst, iv);
 }
 
+// Work items are handed out one at a time from a counter, so warps that
+// start late (SMs still busy with the reciprocal-space kernels of the other
+// stream) or draw cheap items simply take more of them.
+__device__ __forceinline__ int next_work(int *sched, int lane) {
+  int v = 0;
+  if (lane == 0) v = atomicAdd(sched, 1);
+  return __shfl_sync(0xffffffffu, v, 0);
+}
+__device__ __forceinline__ void retire_warp(int *sched, int lane) {
+  if (lane == 0 && atomicAdd(sched + 1, 1) == (int)(gridDim.x * (blockDim.x >> 5)) - 1) {
+    sched[0] = 0;
+    sched[1] = 0;
+  }
+}
+
 // One pair: erfc-Ewald (src/CudaDirectForceKernels.cu:479-489) plus VDW_VFSW
 // (src/CudaDirectForceKernels.cu:263-286).  Returns f with gradient on i =
 // f (x_i - x_j); `in` = inside the cutoff and not excluded, anything else
@@ -176,10 +191,15 @@ __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
   const int nwork = a.counts[2];
   const int stride = a.stride;
   double e_elec = 0.0, e_vdw = 0.0;
-  double dv[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // xx xy xz yy yz zz (VIRIAL)
+  double dv[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  // one system: per-lane fixed-point sums of every work item's energies and
+  // virial (integer sums: the total does not depend on which warp took
+  // which item)
+  long long ie_el = 0, ie_vdw = 0;
+  long long ivir[6] = {0, 0, 0, 0, 0, 0};  // xx xy xz yy yz zz (VIRIAL)
   using Acc = typename std::conditional<PER_PAIR, long long, float>::type;
 
-  for (int w = blockIdx.x * kWarps + wib; w < nwork; w += gridDim.x * kWarps) {
+  for (int w = next_work(a.sched, lane); w < nwork; w = next_work(a.sched, lane)) {
     const int4 wk = a.work[w];
     const NbSetup st = a.setups[wk.w];
     if (MULTI && wk.w != cur_sys) {  // warp-uniform
@@ -342,6 +362,19 @@ __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
         }
       }
     }
+    if (ENERGY && !MULTI) {
+      ie_el += __double2ll_rn(e_elec * kEnergyScale);
+      ie_vdw += __double2ll_rn(e_vdw * kEnergyScale);
+      e_elec = 0.0;
+      e_vdw = 0.0;
+      if (VIRIAL) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+          ivir[k] += __double2ll_rn(dv[k] * kEnergyScale);
+          dv[k] = 0.0;
+        }
+      }
+    }
     if (ivalid) {
       if (PER_PAIR) {
         add_fixed(a.force + islot, (long long)fix);
@@ -354,10 +387,9 @@ __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
       }
     }
   }
+  retire_warp(a.sched, lane);
   if (ENERGY && !MULTI) {
-    // per-lane sums rounded to fixed point, then integer sums: order-free
-    long long ie = __double2ll_rn(e_elec * kEnergyScale);
-    long long iv = __double2ll_rn(e_vdw * kEnergyScale);
+    long long ie = ie_el, iv = ie_vdw;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       ie += __shfl_xor_sync(0xffffffffu, ie, o);
@@ -373,7 +405,7 @@ __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
     constexpr int kSlot[6][2] = {{0, 0}, {1, 3}, {2, 6}, {4, 4}, {5, 7}, {8, 8}};
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
-      long long iw = __double2ll_rn(dv[k] * kEnergyScale);
+      long long iw = ivir[k];
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) iw += __shfl_xor_sync(0xffffffffu, iw, o);
       if (lane == 0) {
@@ -456,9 +488,14 @@ __global__ void __launch_bounds__(kThreads, 5) nbq_kernel(NbArgs a) {
   const int stride = a.stride;
   double e_elec = 0.0, e_vdw = 0.0;
   double dv[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  // one system: per-lane fixed-point sums of every work item's energies and
+  // virial (integer sums: the total does not depend on which warp took
+  // which item)
+  long long ie_el = 0, ie_vdw = 0;
+  long long ivir[6] = {0, 0, 0, 0, 0, 0};
   using Acc = typename std::conditional<PER_PAIR, long long, float>::type;
 
-  for (int w = blockIdx.x * kWarps + wib; w < nwork; w += gridDim.x * kWarps) {
+  for (int w = next_work(a.sched, lane); w < nwork; w = next_work(a.sched, lane)) {
     const int4 wk = a.work[w];
     const NbSetup st = a.setups[wk.w];
     if (MULTI && wk.w != cur_sys) {  // warp-uniform
@@ -663,6 +700,19 @@ __global__ void __launch_bounds__(kThreads, 5) nbq_kernel(NbArgs a) {
         }
       }
     }
+    if (ENERGY && !MULTI) {
+      ie_el += __double2ll_rn(e_elec * kEnergyScale);
+      ie_vdw += __double2ll_rn(e_vdw * kEnergyScale);
+      e_elec = 0.0;
+      e_vdw = 0.0;
+      if (VIRIAL) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+          ivir[k] += __double2ll_rn(dv[k] * kEnergyScale);
+          dv[k] = 0.0;
+        }
+      }
+    }
     if (ivalid) {
       if (PER_PAIR) {
         add_fixed(a.force + islot, (long long)fix);
@@ -675,9 +725,9 @@ __global__ void __launch_bounds__(kThreads, 5) nbq_kernel(NbArgs a) {
       }
     }
   }
+  retire_warp(a.sched, lane);
   if (ENERGY && !MULTI) {
-    long long ie = __double2ll_rn(e_elec * kEnergyScale);
-    long long iv = __double2ll_rn(e_vdw * kEnergyScale);
+    long long ie = ie_el, iv = ie_vdw;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       ie += __shfl_xor_sync(0xffffffffu, ie, o);
@@ -692,7 +742,7 @@ __global__ void __launch_bounds__(kThreads, 5) nbq_kernel(NbArgs a) {
     constexpr int kSlot[6][2] = {{0, 0}, {1, 3}, {2, 6}, {4, 4}, {5, 7}, {8, 8}};
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
-      long long iw = __double2ll_rn(dv[k] * kEnergyScale);
+      long long iw = ivir[k];
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) iw += __shfl_xor_sync(0xffffffffu, iw, o);
       if (lane == 0) {
@@ -758,6 +808,7 @@ void launch_t(const NbArgs &a, cudaStream_t s) {
 }  // namespace
 
 void launch_nonbonded(const NbArgs &a, bool energy, bool per_pair, cudaStream_t s, bool virial) {
+  if (!a.sched) throw std::invalid_argument("nonbonded: no schedule counters");
   if (a.ntype * a.ntype * sizeof(float2) > 64 * 1024)
     throw std::invalid_argument("nonbonded: too many LJ types for the shared table");
   if (virial && !a.virial) throw std::invalid_argument("nonbonded: virial requested without a buffer");
@@ -779,6 +830,7 @@ void launch_nonbonded(const NbArgs &a, bool energy, bool per_pair, cudaStream_t 
 
 void launch_nonbonded_multi(const NbArgs &a, bool energy, bool per_pair, cudaStream_t s,
                             bool virial) {
+  if (!a.sched) throw std::invalid_argument("nonbonded: no schedule counters");
   if (a.energy_stride <= 0 && (energy || virial))
     throw std::invalid_argument("nonbonded: multi-system energies need an energy stride");
   if (a.variant == kNbGroupedQueues) return dispatch_q<true>(a, energy, per_pair, virial, s);

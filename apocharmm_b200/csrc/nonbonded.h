@@ -48,6 +48,9 @@ struct NbArgs {
   // energy + s * energy_stride (virial at + kNumEnergyTerms); 0 = one system
   int energy_stride = 0;
   int variant = 0;        // kernel form, below
+  // dynamic schedule: [0] work items handed out, [1] warps retired; both
+  // zero between launches (the last warp to retire resets them)
+  int *sched = nullptr;
 };
 
 // direct-space kernel forms: one j-list per tile for all 32 i-atoms, or one
