@@ -175,6 +175,7 @@ class ForceManager(_Handle):
     def setFFTGrid(self, nx, ny, nz): call("apo_force_manager_set_fft_grid", self._h, _i(nx), _i(ny), _i(nz))
     def setPrecisionMode(self, on: bool): call("apo_force_manager_set_precision_mode", self._h, _i(int(on)))
     def setTilesPerWork(self, t: int): call("apo_force_manager_set_tiles_per_work", self._h, _i(t))
+    def setWorkItemsPerWarp(self, k: int): call("apo_force_manager_set_work_items_per_warp", self._h, _i(k))
     def setComponentMask(self, m: int): call("apo_force_manager_set_component_mask", self._h, _i(m))
     def setDirectKernel(self, form: int): call("apo_force_manager_set_direct_kernel", self._h, _i(form))
 
@@ -337,7 +338,7 @@ class CharmmContext(_Handle):
 
 
 def system_context(sys, workdir: str, precise: bool = False, settings=None,
-                   tiles_per_work: int = None):
+                   tiles_per_work: int = None, items_per_warp: int = None):
     """Writes `sys` (apocharmm_b200.systems.System) as CHARMM files, loads it
     through the C ABI and returns (psf, prm, fm, ctx).  `settings` overrides
     sys.settings (kappa, nfft, order, ctofnb, ctonnb, cutnb)."""
@@ -358,6 +359,8 @@ def system_context(sys, workdir: str, precise: bool = False, settings=None,
     fm.setPrecisionMode(precise)
     if tiles_per_work is not None:
         fm.setTilesPerWork(tiles_per_work)
+    if items_per_warp is not None:
+        fm.setWorkItemsPerWarp(items_per_warp)
     ctx = CharmmContext(fm)
     ctx.setCoordinates(sys.pos)
     return psf, prm, fm, ctx

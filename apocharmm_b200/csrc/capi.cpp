@@ -247,6 +247,7 @@ FM_SETTER(apo_force_manager_set_ctofnb, double, setCtofnb(v), v > 0 && std::isfi
 FM_SETTER(apo_force_manager_set_spline_order, int, setPmeSplineOrder(v), v == 4 || v == 6 || v == 8)
 FM_SETTER(apo_force_manager_set_precision_mode, int, setPrecisionMode(v != 0), true)
 FM_SETTER(apo_force_manager_set_tiles_per_work, int, setTilesPerWork(v), v >= 1 && v <= 1024)
+FM_SETTER(apo_force_manager_set_work_items_per_warp, int, setWorkItemsPerWarp(v), v >= 0 && v <= 1 << 20)
 FM_SETTER(apo_force_manager_set_component_mask, int, setComponentMask(v), v >= 0 && v <= 7)
 FM_SETTER(apo_force_manager_set_direct_kernel, int, setDirectKernel(v), v == 0 || v == 1)
 

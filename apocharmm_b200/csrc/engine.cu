@@ -230,9 +230,14 @@ void ForceManager::initialize() {
 
 void ForceManager::createStreams() {
   if (!m_SNb) {
-    APO_CUDA(cudaStreamCreateWithFlags(&m_SNb, cudaStreamNonBlocking));
-    APO_CUDA(cudaStreamCreateWithFlags(&m_SPme, cudaStreamNonBlocking));
-    APO_CUDA(cudaStreamCreateWithFlags(&m_SBond, cudaStreamNonBlocking));
+    // the reciprocal-space chain (five dependent, latency-bound kernels) and
+    // the bonded kernel get the higher priority: their blocks go first
+    // whenever direct-space blocks retire
+    int lo = 0, hi = 0;
+    APO_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    APO_CUDA(cudaStreamCreateWithPriority(&m_SNb, cudaStreamNonBlocking, lo));
+    APO_CUDA(cudaStreamCreateWithPriority(&m_SPme, cudaStreamNonBlocking, hi));
+    APO_CUDA(cudaStreamCreateWithPriority(&m_SBond, cudaStreamNonBlocking, hi));
     for (cudaEvent_t *e : {&m_EvFork, &m_EvNb, &m_EvPme, &m_EvBond})
       APO_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
   }
@@ -412,6 +417,8 @@ void ForceManager::calcForce(const float4 *d_xyzq, bool calcEnergy, bool calcVir
     a.virial = virial;
     a.variant = m_NbVariant;
     a.sched = m_Nbl.counts + 6;  // counts[6..7]: zero between launches
+    a.items_per_warp = m_ItemsPerWarp;
+    a.work_cap = m_Nbl.dims().work_cap;
     cudaEvent_t t1 = nullptr;
     bool timer_capture = false;
     if (m_Timing) {

@@ -112,6 +112,10 @@ class ForceManager {
   void setPrecisionMode(bool precise) { m_Precise = precise; }
   bool getPrecisionMode() const { return m_Precise; }
   void setTilesPerWork(int t) { m_TilesPerWork = t; m_Initialized = false; }
+  // work items a warp of the direct-space kernel takes before it retires
+  // (0: persistent grid, every warp until the list is done)
+  void setWorkItemsPerWarp(int k) { m_ItemsPerWarp = k < 0 ? 0 : k; }
+  int getWorkItemsPerWarp() const { return m_ItemsPerWarp; }
   // direct-space kernel form (kNbTileBatches or kNbGroupedQueues, nonbonded.h)
   void setDirectKernel(int v);
   int getDirectKernel() const { return m_NbVariant; }
@@ -203,6 +207,7 @@ class ForceManager {
   bool m_Initialized = false;
   bool m_ListBuilt = false;
   int m_TilesPerWork = 8;
+  int m_ItemsPerWarp = 0;
   int m_NbVariant = kNbTileBatches;
   int m_ComponentMask = 7;
   double m_SelfEnergy = 0.0;

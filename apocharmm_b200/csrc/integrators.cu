@@ -877,7 +877,8 @@ void CudaIntegrator::propagate(int numSteps) {
         }
         APO_CUDA(cudaStreamEndCapture(s, &graph));
         cudaGraphExec_t exec;
-        APO_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+        // keep the stream priorities of the captured launches
+        APO_CUDA(cudaGraphInstantiate(&exec, graph, cudaGraphInstantiateFlagUseNodePriority));
         APO_CUDA(cudaGraphDestroy(graph));
         it = m_Graphs.emplace(len, exec).first;
       }

@@ -10,6 +10,7 @@
 // which lane L holds the full force of j-atom (L&3)*8 + (L>>2).
 #include "nonbonded.h"
 
+#include <algorithm>
 #include <cmath>
 #include <type_traits>
 
@@ -199,7 +200,13 @@ __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
   long long ivir[6] = {0, 0, 0, 0, 0, 0};  // xx xy xz yy yz zz (VIRIAL)
   using Acc = typename std::conditional<PER_PAIR, long long, float>::type;
 
-  for (int w = next_work(a.sched, lane); w < nwork; w = next_work(a.sched, lane)) {
+  int taken = 0;  // warp-uniform
+  auto next = [&]() -> int {
+    if (a.items_per_warp > 0 && taken >= a.items_per_warp) return nwork;
+    ++taken;
+    return next_work(a.sched, lane);
+  };
+  for (int w = next(); w < nwork; w = next()) {
     const int4 wk = a.work[w];
     const NbSetup st = a.setups[wk.w];
     if (MULTI && wk.w != cur_sys) {  // warp-uniform
@@ -495,7 +502,13 @@ __global__ void __launch_bounds__(kThreads, 5) nbq_kernel(NbArgs a) {
   long long ivir[6] = {0, 0, 0, 0, 0, 0};
   using Acc = typename std::conditional<PER_PAIR, long long, float>::type;
 
-  for (int w = next_work(a.sched, lane); w < nwork; w = next_work(a.sched, lane)) {
+  int taken = 0;  // warp-uniform
+  auto next = [&]() -> int {
+    if (a.items_per_warp > 0 && taken >= a.items_per_warp) return nwork;
+    ++taken;
+    return next_work(a.sched, lane);
+  };
+  for (int w = next(); w < nwork; w = next()) {
     const int4 wk = a.work[w];
     const NbSetup st = a.setups[wk.w];
     if (MULTI && wk.w != cur_sys) {  // warp-uniform
@@ -753,6 +766,15 @@ __global__ void __launch_bounds__(kThreads, 5) nbq_kernel(NbArgs a) {
   }
 }
 
+// persistent grid (resident blocks) or, with a bound on the items per warp,
+// enough blocks for every work item the list can hold
+int launch_grid(int resident, const NbArgs &a) {
+  if (a.items_per_warp <= 0) return resident;
+  const long long per_block = (long long)kWarps * a.items_per_warp;
+  const long long need = ((long long)a.work_cap + per_block - 1) / per_block;
+  return (int)std::max<long long>(resident, std::min<long long>(need, 1ll << 30));
+}
+
 template <bool E, bool P, bool V, bool M>
 void launch_q(const NbArgs &a, cudaStream_t s) {
   static int grid = 0;
@@ -768,7 +790,7 @@ void launch_q(const NbArgs &a, cudaStream_t s) {
                                                            64 * 1024 > sm ? sm : 64 * 1024));
     grid = nsm * (per > 0 ? per : 1);
   }
-  nbq_kernel<E, P, V, M><<<grid, kThreads, sm, s>>>(a);
+  nbq_kernel<E, P, V, M><<<launch_grid(grid, a), kThreads, sm, s>>>(a);
   APO_LAUNCH_CHECK();
 }
 
@@ -801,7 +823,7 @@ void launch_t(const NbArgs &a, cudaStream_t s) {
                                                            64 * 1024 > sm ? sm : 64 * 1024));
     grid = nsm * (per > 0 ? per : 1);
   }
-  nb_kernel<E, P, V, M><<<grid, kThreads, sm, s>>>(a);
+  nb_kernel<E, P, V, M><<<launch_grid(grid, a), kThreads, sm, s>>>(a);
   APO_LAUNCH_CHECK();
 }
 

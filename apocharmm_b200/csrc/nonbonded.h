@@ -51,6 +51,11 @@ struct NbArgs {
   // dynamic schedule: [0] work items handed out, [1] warps retired; both
   // zero between launches (the last warp to retire resets them)
   int *sched = nullptr;
+  // at most this many work items per warp (0: no bound, a persistent grid);
+  // with a bound the grid covers work_cap items, so blocks retire while the
+  // reciprocal-space kernels of the other stream wait for SMs
+  int items_per_warp = 0;
+  int work_cap = 0;
 };
 
 // direct-space kernel forms: one j-list per tile for all 32 i-atoms, or one

@@ -563,6 +563,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--tiles-per-work", type=int, default=8,
                     help="j-tiles per direct-space work item")
+    ap.add_argument("--items-per-warp", type=int, default=None,
+                    help="direct-space work items per warp before it retires (0: persistent "
+                         "grid; default: the library's)")
     ap.add_argument("--direct-kernel", type=int, default=0, choices=[0, 1],
                     help="direct-space kernel form: 0 tile batches, 1 grouped queues")
     args = ap.parse_args()
@@ -597,7 +600,8 @@ def main():
     s = make_system(args.workload)
     work = tempfile.mkdtemp(prefix=f"apo_bench_{rank}_")
     psf, prm, fm, ctx = api.system_context(s, work, precise=args.precise,
-                                           tiles_per_work=args.tiles_per_work)
+                                           tiles_per_work=args.tiles_per_work,
+                                           items_per_warp=args.items_per_warp)
     fm.setDirectKernel(args.direct_kernel)
     # remove the close contacts of the generated structure (deterministic)
     s.pos = api.relax(ctx, api.water_indices(s), iterations=RELAX_ITERATIONS,
@@ -719,6 +723,7 @@ def main():
                        "form": "precision" if args.precise else "plain",
                        "direct_kernel": ["tile batches", "grouped queues"][args.direct_kernel],
                        "tiles_per_work": args.tiles_per_work,
+                       "items_per_warp": args.items_per_warp,
                        "l2": "flushed (256 MB device write) before every timed iteration, "
                              "outside the timed interval",
                        "parallelism": f"replicas x{world}"},

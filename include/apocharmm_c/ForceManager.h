@@ -28,6 +28,9 @@ APOCHARMM_C_API apo_status apo_force_manager_set_spline_order(apo_force_manager 
  * evaluated parts as a bit mask (1 bonded+1-4, 2 direct, 4 reciprocal) */
 APOCHARMM_C_API apo_status apo_force_manager_set_precision_mode(apo_force_manager *force_manager, const int precise);
 APOCHARMM_C_API apo_status apo_force_manager_set_tiles_per_work(apo_force_manager *force_manager, const int tiles);
+/* addition: work items one warp of the direct-space kernel takes before it
+ * retires (0 = persistent grid, the default) */
+APOCHARMM_C_API apo_status apo_force_manager_set_work_items_per_warp(apo_force_manager *force_manager, const int items);
 APOCHARMM_C_API apo_status apo_force_manager_set_component_mask(apo_force_manager *force_manager, const int mask);
 APOCHARMM_C_API apo_status apo_force_manager_get_fft_grid(int *nxyz3, const apo_force_manager *force_manager);
 /* addition: direct-space kernel form, 0 = one j-list per tile for the whole
