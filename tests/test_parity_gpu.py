@@ -105,6 +105,26 @@ def test_forces_are_deterministic(tmp_path):
     assert e1 == e2
 
 
+def test_direct_space_schedule_does_not_change_results(tmp_path):
+    """Work items are handed out dynamically; with a persistent grid or with
+    1, 2 or 4 items per warp, forces, energies and the virial are the same
+    bit for bit (every item's forces and energies are rounded to fixed
+    point on their own)."""
+    s = config_solvated_chain()
+    out = {}
+    for k in (0, 1, 2, 4):
+        psf, prm, fm, ctx = api.system_context(s, str(tmp_path / f"k{k}"), items_per_warp=k)
+        ctx.calculateForces(False, True, True)
+        out[k] = (ctx.getForces(), ctx.getEnergyComponents(), ctx.getVirial())
+        # a second evaluation on the same context: the counters were reset
+        ctx.calculateForces(False, True, True)
+        assert np.array_equal(ctx.getForces(), out[k][0])
+    for k in (1, 2, 4):
+        assert np.array_equal(out[0][0], out[k][0])
+        assert out[0][1] == out[k][1]
+        assert np.array_equal(out[0][2], out[k][2])
+
+
 @pytest.mark.parametrize("name", ["waterDimer", "argon10"])
 def test_small_golden_cases(tmp_path, name):
     """The reference's waterDimer (unittest-eneForces.cpp:110-206) and argon10
