@@ -119,6 +119,23 @@ def dist_env():
         int(os.environ.get("LOCAL_RANK", "0"))
 
 
+def max_over_ranks(value: float, world: int, device: str = "cuda") -> float:
+    """The largest of every rank's value (each rank passes its own): a
+    multi-GPU time is the slowest rank's.  Every rank must call it."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_seed(rank: int) -> int:
+    """Velocity seed of one replica: replicas differ, runs repeat."""
+    return 2024 + rank
+
+
 WORKLOADS = {
     "chain23k": dict(factory="config_solvated_chain", integrator="langevin", friction=1.0,
                      desc="chain23k: 23,558-atom bead chain in TIP3P, 62.23 A box, PME 64^3 "
@@ -606,7 +623,7 @@ def main():
     # remove the close contacts of the generated structure (deterministic)
     s.pos = api.relax(ctx, api.water_indices(s), iterations=RELAX_ITERATIONS,
                       max_step=RELAX_MAX_STEP)
-    ctx.setRandomSeedForVelocities(2024 + rank)
+    ctx.setRandomSeedForVelocities(replica_seed(rank))
     ctx.assignVelocitiesAtTemperature(300.0)
 
     # force error of this configuration against the FP64 oracle (rank 0)
@@ -656,11 +673,8 @@ def main():
             nb_ms += t.value
             nb_launch += n.value
     torch.cuda.synchronize()
-    total_ms = sum(seg_ms)
+    total_ms = max_over_ranks(sum(seg_ms), world)
     if world > 1:
-        tt = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(tt.item())
         torch.distributed.barrier()
     md_steps = args.steps * SEG
     value = ns_per_day(md_steps * world, total_ms * 1e-3)
@@ -692,11 +706,7 @@ def main():
                      ctx.handle)
             api.call("apo_charmm_context_get_velocities", api._vp(hv.data_ptr()), api._sz(3 * n),
                      ctx.handle)
-        el = time.perf_counter() - t0
-        if world > 1:
-            tt = torch.tensor([el], device="cuda", dtype=torch.float64)
-            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-            el = float(tt.item())
+        el = max_over_ranks(time.perf_counter() - t0, world)
         e2e = {"value": ns_per_day(iters * SEG * world, el), "unit": "ns/day",
                "h2d_bytes_per_step": 2 * 3 * n * 8 / SEG, "d2h_bytes_per_step": 2 * 3 * n * 8 / SEG,
                "note": "per 20-step segment: coordinates+velocities up (pinned), propagate, "
