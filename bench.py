@@ -52,6 +52,12 @@ sys.path.insert(0, ROOT)
 DT_PS = 0.002
 SEG = 20                       # MD steps per timed iteration (list cadence)
 FLOP_PER_PAIR = 65
+# DRAM bytes per launch of the direct-space kernel (dram__bytes_read.sum +
+# dram__bytes_write.sum) from one ncu capture of the same kernel on the same
+# workload (the inputs and the fixed-point force buffer stay in L2)
+NB_TRAFFIC = {
+    "chain23k": (7423488, "ncu --set full capture, profiles/nb_kernel_chain23k.md"),
+}
 
 
 def ns_per_day(steps: float, seconds: float) -> float:
@@ -743,7 +749,8 @@ def main():
             "roofline": {"kernel": "direct-space tile kernel", "bound": "fp32",
                          "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
                          "frac": (achieved / peak.value) if achieved else None,
-                         "traffic": None,
+                         "traffic": NB_TRAFFIC.get(args.workload, (None, None))[0],
+                         "traffic_source": NB_TRAFFIC.get(args.workload, (None, None))[1],
                          "work": f"{FLOP_PER_PAIR} FLOP x {pairs_avg:.0f} in-cutoff pairs per launch",
                          "launch_ms": avg_nb_s * 1e3, "launches_timed": nb_launch,
                          "peak_source": "FP32 FMA probe measured on this GPU in this run"},
