@@ -15,7 +15,7 @@ namespace apo {
 
 namespace {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 128;
 constexpr int kMaxBlocks = 4096;
 
 // constraint group kinds
