@@ -1025,9 +1025,13 @@ void CudaIntegrator::initializeFromRestartFile(const std::string &path) {
     throw std::invalid_argument("NATOM mismatch in restart file \"" + path + "\"");
   if (r.ndegf != m_Ctx->getDegreesOfFreedom())
     throw std::invalid_argument("NDEGF mismatch in restart file \"" + path + "\"");
-  if (r.box != fm->getBoxDimensions())
-    throw std::invalid_argument("restart file \"" + path + "\" holds another box: set it on the "
-                                "ForceManager before the integrator is created");
+  // a file written with 16 significant digits (the reference's form) need
+  // not give back the last bit of the box
+  const auto &box = fm->getBoxDimensions();
+  for (int k = 0; k < 3; ++k)
+    if (std::fabs(r.box[k] - box[k]) > 1e-12 * std::fabs(box[k]))
+      throw std::invalid_argument("restart file \"" + path + "\" holds another box: set it on "
+                                  "the ForceManager before the integrator is created");
   m_Ctx->setCoordinates(r.xold);
   m_Ctx->setVelocities(r.vel);
   std::vector<double4> d(r.natom);
