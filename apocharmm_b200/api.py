@@ -468,6 +468,11 @@ class CudaIntegrator(_Handle):
         self._keep.append(subscriber)
         call("apo_cuda_integrator_subscribe", self._view, subscriber._view)
 
+    def unsubscribe(self, subscriber: Subscriber) -> bool:
+        removed = _i()
+        call("apo_cuda_integrator_unsubscribe", ctypes.byref(removed), self._view, subscriber._view)
+        return bool(removed.value)
+
     def propagate(self, num_steps: int):
         call("apo_cuda_integrator_propagate", self._view, _i(num_steps))
 

@@ -70,6 +70,18 @@ extern "C" apo_status apo_cuda_integrator_subscribe(apo_cuda_integrator *it, apo
   }, fn);
 }
 
+extern "C" apo_status apo_cuda_integrator_unsubscribe(int *removed, apo_cuda_integrator *it,
+                                                      apo_subscriber *sub) {
+  const char *fn = "apo_cuda_integrator_unsubscribe";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_ptr(removed, fn, "removed"));
+    APO_RETURN_IF(require_handle(it, fn, "CudaIntegrator"));
+    APO_RETURN_IF(require_handle(sub, fn, "Subscriber"));
+    *removed = it->object->unsubscribe(sub->object) ? 1 : 0;
+    return APO_STATUS_OK;
+  }, fn);
+}
+
 extern "C" apo_status apo_cuda_integrator_propagate(apo_cuda_integrator *it, const int n) {
   const char *fn = "apo_cuda_integrator_propagate";
   return guard([&]() -> apo_status {

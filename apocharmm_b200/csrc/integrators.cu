@@ -842,6 +842,16 @@ void CudaIntegrator::subscribe(std::shared_ptr<Subscriber> sub) {
   m_Subscribers.push_back(std::move(sub));
 }
 
+bool CudaIntegrator::unsubscribe(const std::shared_ptr<Subscriber> &sub) {
+  for (size_t k = 0; k < m_Subscribers.size(); ++k)
+    if (m_Subscribers[k] == sub) {
+      m_Subscribers[k]->attach(nullptr);
+      m_Subscribers.erase(m_Subscribers.begin() + k);
+      return true;
+    }
+  return false;
+}
+
 void CudaIntegrator::propagate(int numSteps) {
   if (!m_Ctx)
     throw std::invalid_argument("CudaIntegrator::propagate: no CharmmContext was set for this CudaIntegrator.");

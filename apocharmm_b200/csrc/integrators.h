@@ -48,6 +48,9 @@ class CudaIntegrator : public std::enable_shared_from_this<CudaIntegrator> {
   void setRemoveCenterOfMassFrequency(int f) { m_ComFreq = f < 0 ? 0 : f; clearGraphs(); }
   void setUseGraphs(bool g) { m_UseGraphs = g; }
   void subscribe(std::shared_ptr<Subscriber> sub);
+  // stops the reports of one subscriber (src/CudaIntegrator.cu unsubscribe);
+  // true when it was subscribed
+  bool unsubscribe(const std::shared_ptr<Subscriber> &sub);
   void propagate(int numSteps);
   long long getCurrentPropagatedStep() const { return m_Step; }
   double getInstantaneousTemperature();  // "Jung" estimate of the last step

@@ -14,6 +14,9 @@ typedef struct apo_cuda_integrator apo_cuda_integrator;
 APOCHARMM_C_API apo_status apo_cuda_integrator_set_time_step(apo_cuda_integrator *integrator, const double time_step); /* :24 */
 APOCHARMM_C_API apo_status apo_cuda_integrator_set_charmm_context(apo_cuda_integrator *integrator, apo_charmm_context *context); /* :27 */
 APOCHARMM_C_API apo_status apo_cuda_integrator_subscribe(apo_cuda_integrator *integrator, apo_subscriber *subscriber); /* :30 */
+/* addition: CudaIntegrator::unsubscribe (include/CudaIntegrator.h:139, C++ only in the
+ * reference); *removed = 1 when the subscriber was subscribed */
+APOCHARMM_C_API apo_status apo_cuda_integrator_unsubscribe(int *removed, apo_cuda_integrator *integrator, apo_subscriber *subscriber);
 APOCHARMM_C_API apo_status apo_cuda_integrator_propagate(apo_cuda_integrator *integrator, const int num_steps); /* :33 */
 APOCHARMM_C_API apo_status apo_cuda_integrator_initialize_from_restart_file(apo_cuda_integrator *integrator, const char *path); /* :36 */
 /* additions: list-update cadence (CudaIntegrator::setNonbondedListUpdateFrequency,

@@ -92,6 +92,23 @@ def test_restart_holds_the_state_of_the_report_step(tmp_path):
     np.testing.assert_array_equal(r["box"], s.box)
 
 
+def test_unsubscribed_restart_stops_reporting(tmp_path):
+    # the reference test's pattern (unittest-restartSubscriber.cpp:70-83):
+    # report, unsubscribe, propagate on
+    s, keep = _context(tmp_path)
+    it = _langevin(8)
+    it.setCharmmContext(keep[3])
+    rst = tmp_path / "u.rst"
+    sub = api.RestartSubscriber(str(rst), 20)
+    it.subscribe(sub)
+    it.propagate(20)
+    assert it.unsubscribe(sub)
+    assert not it.unsubscribe(sub)
+    it.propagate(20)
+    assert api.read_restart_file(rst)["npriv"] == 20
+    assert it.getCurrentPropagatedStep() == 40
+
+
 def test_restart_errors(tmp_path):
     s, keep = _context(tmp_path, relax=False)
     keep[3].useHolonomicConstraints(False)
