@@ -2,7 +2,7 @@
 // compiled by oracle/Makefile.ref) through its public C++ API.
 //
 // TEST / MEASUREMENT INFRASTRUCTURE ONLY: used by the parity tests and the
-// reference arm of the benchmark on a GPU box, never by the product.
+// reference arm of the benchmark on a machine with a GPU, never by the product.
 //
 //   ref_harness forces <psf> <prm> <crd> <L> <kappa> <cutnb> <ctonnb> <ctofnb>
 //               <nx> <ny> <nz> <order> <out>
