@@ -116,3 +116,44 @@ def test_batch_handle_errors_without_gpu():
     assert L.apo_batch_propagate(h, 10) == 4                             # not initialised
     assert L.apo_batch_initialize(h) == 1                                # no systems
     L.apo_batch_destroy(h)
+
+
+def test_null_handles_are_reported_without_gpu():
+    """Every entry point added for plug-ins, restart files, unsubscribe and
+    the direct-space knobs rejects NULL handles and outputs with
+    APO_STATUS_INVALID_ARGUMENT (1) and a message, without touching a device."""
+    import ctypes
+    from apocharmm_b200._lib import lib
+    L = lib()
+    L.apo_last_error.restype = ctypes.c_char_p
+    i = ctypes.c_int()
+    calls = [
+        lambda: L.apo_cuda_integrator_unsubscribe(ctypes.byref(i), None, None),
+        lambda: L.apo_cuda_integrator_unsubscribe(None, None, None),
+        lambda: L.apo_force_manager_unsubscribe(ctypes.byref(i), None, b"harm"),
+        lambda: L.apo_force_manager_subscribe_harmonic_restraint(None, None, b"harm"),
+        lambda: L.apo_force_manager_set_work_items_per_warp(None, ctypes.c_int(2)),
+        lambda: L.apo_harmonic_restraint_force_set_force_constant(None, ctypes.c_double(1.0)),
+        lambda: L.apo_charmm_context_get_energy_component(None, None, b"vdw"),
+        lambda: L.apo_restart_file_read(b"", 0, None, None, None),
+    ]
+    for k, c in enumerate(calls):
+        assert c() == 1, k
+        assert L.apo_last_error(), k
+
+
+def test_restraint_handle_subscribes_only_matching_sizes_without_gpu(tmp_path):
+    """A force manager built from files (no device work) refuses a restraint
+    for another number of atoms, and an empty tag."""
+    import ctypes
+    from apocharmm_b200._lib import lib
+    from apocharmm_b200.systems import water_box, write_charmm_files
+    s = water_box(10, 12.0, seed=1)
+    p = write_charmm_files(s, str(tmp_path))
+    psf, prm = api.CharmmPsf(p["psf"]), api.CharmmParameters(p["prm"])
+    fm = api.ForceManager(psf, prm)
+    L = lib()
+    h = api.HarmonicRestraintForce(31)
+    assert L.apo_force_manager_subscribe_harmonic_restraint(fm.handle, h.handle, b"harm") == 1
+    h30 = api.HarmonicRestraintForce(30)
+    assert L.apo_force_manager_subscribe_harmonic_restraint(fm.handle, h30.handle, b"") == 1
