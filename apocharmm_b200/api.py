@@ -178,6 +178,12 @@ class ForceManager(_Handle):
     def setWorkItemsPerWarp(self, k: int): call("apo_force_manager_set_work_items_per_warp", self._h, _i(k))
     def setComponentMask(self, m: int): call("apo_force_manager_set_component_mask", self._h, _i(m))
     def setDirectKernel(self, form: int): call("apo_force_manager_set_direct_kernel", self._h, _i(form))
+    def setListCapacity(self, tiles: int): call("apo_force_manager_set_list_capacity", self._h, _i(tiles))
+
+    def getListCapacity(self) -> int:
+        v = _i()
+        call("apo_force_manager_get_list_capacity", ctypes.byref(v), self._h)
+        return v.value
 
     def getFFTGrid(self):
         a = (ctypes.c_int * 3)()
@@ -328,6 +334,15 @@ class CharmmContext(_Handle):
         call("apo_charmm_context_get_neighbor_pairs", None, _sz(0), ctypes.byref(n), _d(radius), self._h)
         a = np.zeros(3 * max(1, n.value), np.int32)
         call("apo_charmm_context_get_neighbor_pairs", _ptr(a), _sz(a.size), ctypes.byref(n),
+             _d(radius), self._h)
+        return a[:3 * n.value].reshape(-1, 3)
+
+    def getListPairs(self, radius: float) -> np.ndarray:
+        """Every pair of the tile list within `radius`: (i, j, excluded) rows."""
+        n = _sz()
+        call("apo_charmm_context_get_list_pairs", None, _sz(0), ctypes.byref(n), _d(radius), self._h)
+        a = np.zeros(3 * max(1, n.value), np.int32)
+        call("apo_charmm_context_get_list_pairs", _ptr(a), _sz(a.size), ctypes.byref(n),
              _d(radius), self._h)
         return a[:3 * n.value].reshape(-1, 3)
 

@@ -250,6 +250,17 @@ FM_SETTER(apo_force_manager_set_tiles_per_work, int, setTilesPerWork(v), v >= 1 
 FM_SETTER(apo_force_manager_set_work_items_per_warp, int, setWorkItemsPerWarp(v), v >= 0 && v <= 1 << 20)
 FM_SETTER(apo_force_manager_set_component_mask, int, setComponentMask(v), v >= 0 && v <= 7)
 FM_SETTER(apo_force_manager_set_direct_kernel, int, setDirectKernel(v), v == 0 || v == 1)
+FM_SETTER(apo_force_manager_set_list_capacity, int, setListCapacity(v), v >= 1)
+
+extern "C" apo_status apo_force_manager_get_list_capacity(int *tiles, const apo_force_manager *fm) {
+  const char *fn = "apo_force_manager_get_list_capacity";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_ptr(tiles, fn, "tiles"));
+    APO_RETURN_IF(require_handle(fm, fn, "ForceManager"));
+    *tiles = fm->object->getListCapacity();
+    return APO_STATUS_OK;
+  }, fn);
+}
 
 extern "C" apo_status apo_force_manager_set_fft_grid(apo_force_manager *fm, const int nx,
                                                      const int ny, const int nz) {
@@ -488,6 +499,77 @@ extern "C" apo_status apo_charmm_context_get_stream(void **stream, const apo_cha
     APO_RETURN_IF(require_ptr(stream, fn, "stream"));
     APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
     *stream = (void *)c->object->stream();
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+// Every tile-list pair within `radius`, with its exclusion bit:
+// (atom i, atom j, excluded).  The self tile of a cluster holds each pair
+// twice (the mask drops j <= i); only its upper triangle is reported.
+extern "C" apo_status apo_charmm_context_get_list_pairs(int *pairs, const size_t len,
+                                                        size_t *num_pairs, const double radius,
+                                                        apo_charmm_context *c) {
+  const char *fn = "apo_charmm_context_get_list_pairs";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_ptr(num_pairs, fn, "num_pairs"));
+    APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
+    if (!(radius > 0.0)) return invalid(fn, "radius must be positive");
+    auto fm = c->object->getForceManager();
+    auto &nl = fm->neighborList();
+    cudaStream_t s = c->object->stream();
+    APO_CUDA(cudaStreamSynchronize(s));
+    nl.sync_counts(s);
+    const int S = nl.h_counts[0], T = nl.h_counts[1];
+    std::vector<int> perm(S);
+    std::vector<float4> xs(S), origin((S + 31) / 32);
+    std::vector<int2> tiles(T);
+    std::vector<unsigned> masks((size_t)T * 32);
+    std::vector<int4> work(nl.h_counts[2]);
+    if (S) {
+      APO_CUDA(cudaMemcpy(perm.data(), nl.perm, S * sizeof(int), cudaMemcpyDeviceToHost));
+      APO_CUDA(cudaMemcpy(xs.data(), nl.xyzq_s, S * sizeof(float4), cudaMemcpyDeviceToHost));
+      APO_CUDA(cudaMemcpy(origin.data(), nl.cl_origin, origin.size() * sizeof(float4),
+                          cudaMemcpyDeviceToHost));
+    }
+    if (T) {
+      APO_CUDA(cudaMemcpy(tiles.data(), nl.tiles, T * sizeof(int2), cudaMemcpyDeviceToHost));
+      APO_CUDA(cudaMemcpy(masks.data(), nl.masks, masks.size() * sizeof(unsigned), cudaMemcpyDeviceToHost));
+    }
+    if (!work.empty())
+      APO_CUDA(cudaMemcpy(work.data(), nl.work, work.size() * sizeof(int4), cudaMemcpyDeviceToHost));
+    auto box = fm->getBoxDimensions();
+    const double r2max = radius * radius;
+    size_t count = 0;
+    for (auto &w : work) {
+      for (int t = w.y; t < w.z; ++t) {
+        const int jc = tiles[t].x, sc = tiles[t].y;
+        const bool self = jc == w.x && sc == 13;
+        const double sx = (sc % 3 - 1) * box[0], sy = ((sc / 3) % 3 - 1) * box[1],
+                     sz = (sc / 9 - 1) * box[2];
+        const float4 oi = origin[w.x], oj = origin[jc];
+        for (int i = 0; i < 32; ++i) {
+          const int si = w.x * 32 + i;
+          if (perm[si] < 0) continue;
+          const unsigned m = masks[(size_t)t * 32 + i];
+          for (int j = self ? i + 1 : 0; j < 32; ++j) {
+            const int sj = jc * 32 + j;
+            if (perm[sj] < 0) continue;
+            const double dx = ((double)xs[si].x + oi.x) - ((double)xs[sj].x + oj.x + sx),
+                         dy = ((double)xs[si].y + oi.y) - ((double)xs[sj].y + oj.y + sy),
+                         dz = ((double)xs[si].z + oi.z) - ((double)xs[sj].z + oj.z + sz);
+            if (dx * dx + dy * dy + dz * dz >= r2max) continue;
+            if (pairs && 3 * (count + 1) <= len) {
+              pairs[3 * count] = perm[si];
+              pairs[3 * count + 1] = perm[sj];
+              pairs[3 * count + 2] = (int)((m >> j) & 1u);
+            }
+            ++count;
+          }
+        }
+      }
+    }
+    *num_pairs = count;
+    if (pairs && 3 * count > len) return invalid(fn, "pair buffer too small");
     return APO_STATUS_OK;
   }, fn);
 }

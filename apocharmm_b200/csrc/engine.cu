@@ -380,12 +380,49 @@ void ForceManager::resetNeighborList(const float4 *d_xyzq, cudaStream_t s) {
   } else {
     m_Nbl.build(d_xyzq, s);
   }
+  m_ListDirty = false;
+}
+
+void ForceManager::setListCapacity(int tiles) {
+  if (!m_Initialized) throw std::runtime_error("ForceManager is not initialized");
+  if (tiles < 1) throw std::invalid_argument("ForceManager::setListCapacity: capacity must be positive");
+  const int ncl = m_Nbl.dims().slot_cap / kTile;
+  m_Nbl.set_capacity(tiles, tiles / std::max(1, m_Nbl.dims().tiles_per_work) + ncl + 16);
+  // no tile or work item is published until the next build fills the new
+  // buffers
+  APO_CUDA(cudaMemset(m_Nbl.counts + 1, 0, 4 * sizeof(int)));
+  m_ListDirty = true;
+  ++m_PluginGen;  // the captured graphs hold the old buffers
+}
+
+void ForceManager::calcForceChecked(const float4 *d_xyzq, bool calcEnergy, bool calcVirial,
+                                    cudaStream_t s) {
+  calcForce(d_xyzq, calcEnergy, calcVirial, s, true);
+  APO_CUDA(cudaStreamSynchronize(s));
+  const unsigned e = readDeviceError(s);
+  if (e & (kErrTileOverflow | kErrWorkOverflow)) {
+    growNeighborList(d_xyzq, s);
+    calcForce(d_xyzq, calcEnergy, calcVirial, s, true);
+    APO_CUDA(cudaStreamSynchronize(s));
+  }
+}
+
+bool ForceManager::growNeighborList(const float4 *d_xyzq, cudaStream_t s) {
+  APO_CUDA(cudaStreamSynchronize(s));
+  const int t0 = m_Nbl.dims().tile_cap, w0 = m_Nbl.dims().work_cap;
+  m_Nbl.clear_error(s);
+  m_Nbl.ensure_capacity(d_xyzq, s);
+  m_Nbl.clear_error(s);
+  APO_CUDA(cudaStreamSynchronize(s));
+  const bool moved = m_Nbl.dims().tile_cap != t0 || m_Nbl.dims().work_cap != w0;
+  if (moved) ++m_PluginGen;
+  return moved;
 }
 
 void ForceManager::calcForce(const float4 *d_xyzq, bool calcEnergy, bool calcVirial,
                              cudaStream_t s, bool clear) {
   if (!m_Initialized) throw std::runtime_error("ForceManager is not initialized");
-  if (!m_ListBuilt) resetNeighborList(d_xyzq, s);
+  if (!m_ListBuilt || m_ListDirty) resetNeighborList(d_xyzq, s);
   else if (clear) m_Nbl.refresh(s);
   if (clear) APO_CUDA(cudaMemsetAsync(m_Force.p, 0, (size_t)3 * m_Stride * sizeof(long long), s));
   if (calcVirial) calcEnergy = true;
@@ -955,8 +992,7 @@ void CharmmContext::ensureNeighborList() {
 void CharmmContext::calculateForces(bool reset, bool calcEnergy, bool calcVirial) {
   if (!m_HasCoords) throw std::runtime_error("calculateForces: coordinates not set");
   if (reset || m_ListStale) resetNeighborList(m_Stream);
-  m_Fm->calcForce(m_Xyzq.p, calcEnergy, calcVirial, m_Stream);
-  APO_CUDA(cudaStreamSynchronize(m_Stream));
+  m_Fm->calcForceChecked(m_Xyzq.p, calcEnergy, calcVirial, m_Stream);
 }
 
 double CharmmContext::calculatePotentialEnergy(bool reset, bool /*print*/) {

@@ -127,8 +127,20 @@ class ForceManager {
   void subscribe(std::shared_ptr<ForcePlugin> force, const std::string &tag);
   bool unsubscribe(const std::string &tag);
   bool unsubscribe(const ForcePlugin *force);
-  // changes whenever the set of plug-ins changes (captured graphs are stale)
+  // changes whenever the set of plug-ins or a device buffer the force path
+  // reads changes (captured graphs are then stale)
   int pluginGeneration() const { return m_PluginGen; }
+  // tile capacity of the neighbour list (work items follow); a list that
+  // outgrows it during propagate() is grown and the segment run again
+  void setListCapacity(int tiles);
+  int getListCapacity() const { return m_Nbl.dims().tile_cap; }
+  // after a device-side list overflow: rebuild the list at the current
+  // coordinates with capacities that hold it, clear the error word (sync);
+  // true when the buffers moved
+  bool growNeighborList(const float4 *d_xyzq, cudaStream_t s);
+  // calcForce with clear = true, then a synchronisation; a list that
+  // overflowed on the way is grown and the forces evaluated again
+  void calcForceChecked(const float4 *d_xyzq, bool calcEnergy, bool calcVirial, cudaStream_t s);
   static constexpr int kMaxPlugins = 16;
 
   const std::array<double, 3> &getBoxDimensions() const { return m_Box; }
@@ -206,6 +218,7 @@ class ForceManager {
   bool m_Precise = false;
   bool m_Initialized = false;
   bool m_ListBuilt = false;
+  bool m_ListDirty = false;  // buffers replaced: rebuild before the next use
   int m_TilesPerWork = 8;
   int m_ItemsPerWarp = 0;
   int m_NbVariant = kNbTileBatches;

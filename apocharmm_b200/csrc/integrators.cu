@@ -236,6 +236,9 @@ struct Common {
   float4 *xyzq_s;
   Scalars *sc;
   double *partials;
+  // the neighbour list's error word: once a list build has overflowed or
+  // met non-finite coordinates, every step kernel leaves the state as it is
+  const unsigned *err;
   SettleConst sk;
   int ndegf;
   double dt;
@@ -268,6 +271,7 @@ __device__ void finish_temperature(const Common &c, double ke0, double ke1) {
 //   v = sqrt(1+g/2)/(2 dt) * (delta + delta_prev)
 __global__ void __launch_bounds__(kThreads) langevin_kernel(Common c, double gamma, double kbt,
                                                             unsigned long long seed) {
+  if (*c.err) return;  // the same word for every block: the whole grid returns
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   const double dt = c.dt, dt2 = dt * dt;
   const double hg = 0.5 * gamma, denom = 1.0 / (1.0 + hg), alpha = (1.0 - hg) * denom;
@@ -397,6 +401,7 @@ __device__ void piston_update(Scalars *sc, double ke_sel, double ke_ref, double 
 }
 
 __global__ void __launch_bounds__(kThreads) nh_half_kernel(Common c, double ke_ref, int use_old) {
+  if (*c.err) return;
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   const double dt = c.dt, dt2 = dt * dt, idt = 1.0 / dt;
   double ke0 = 0, ke1 = 0;
@@ -404,13 +409,14 @@ __global__ void __launch_bounds__(kThreads) nh_half_kernel(Common c, double ke_r
     int at[4];
     const int m = group_atoms(c, g, at);
     const int2 meta = c.gmeta[g];
-    d3 o[4], n[4];
+    d3 o[4], n[4], n0[4];
     for (int k = 0; k < m; ++k) {
       const int a = at[k];
       o[k] = xyz(c.coords[a]);
       c.ref[a] = c.coords[a];
       const d3 gr = take_grad(c.force, c.stride, c.glo2loc[a]);
       n[k] = o[k] + (xyz(c.dprev[a]) - (dt2 * c.vel[a].w) * gr);
+      n0[k] = n[k];
     }
     apply_constraint(meta.x, m, o, n, c.sk, c.shake_p, meta.y);
     for (int k = 0; k < m; ++k) {
@@ -420,7 +426,11 @@ __global__ void __launch_bounds__(kThreads) nh_half_kernel(Common c, double ke_r
       c.dpred[a] = c.delta[a];
       c.coords[a] = make_double4(n[k].x, n[k].y, n[k].z, c.coords[a].w);
       const double mass = 1.0 / c.vel[a].w;
-      const d3 v = xyz(c.vel[a]);
+      // the on-step velocity of the first predictor-corrector pass carries
+      // the constraint's displacement over dt, as the reference's constraint
+      // pass adds it to the velocities (src/CudaHolonomicConstraint.cu:94-106,
+      // src/CudaNoseHooverIntegrator.cu:905-930)
+      const d3 v = xyz(c.vel[a]) + idt * (n[k] - n0[k]);
       const d3 u1 = idt * xyz(c.dprev[a]), u2 = idt * d;
       const double kon = 0.5 * mass * dot(v, v);
       ke0 += (0.5 * mass * dot(u1, u1) + kon + 0.5 * mass * dot(u2, u2)) / 3.0;
@@ -444,6 +454,7 @@ __global__ void __launch_bounds__(kThreads) nh_half_kernel(Common c, double ke_r
 template <bool KE>
 __global__ void __launch_bounds__(kThreads) nh_pc_kernel(Common c, int natom, double ke_ref,
                                                          int use_old) {
+  if (*c.err) return;
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   const double dt = c.dt, idt = 1.0 / dt, fact = 0.5 / dt;
   const double xi = c.sc->piston_v;
@@ -478,6 +489,7 @@ __global__ void __launch_bounds__(kThreads) nh_pc_kernel(Common c, int natom, do
 }
 
 __global__ void __launch_bounds__(kThreads) nh_final_kernel(Common c, double ke_ref, int use_old) {
+  if (*c.err) return;
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   const double dt = c.dt, idt = 1.0 / dt, fact = 0.5 / dt;
   double ke0 = 0, ke1 = 0;
@@ -524,6 +536,7 @@ __global__ void __launch_bounds__(kThreads) nh_final_kernel(Common c, double ke_
 // reference advances only the single-precision copy; here the FP64 state is
 // advanced and the single-precision copies are refreshed from it.
 __global__ void leapfrog_kernel(Common c, int natom) {
+  if (*c.err) return;
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   double ke1 = 0;
   if (a < natom) {
@@ -566,21 +579,29 @@ __global__ void init_delta_kernel(Common c, int natom, double gamma) {
 
 // mode 0: constrain the current positions against themselves (projection
 // onto the constraint surface); mode 1: back step x - delta_prev, constrain
-// against x, then delta_prev = x - x_constrained
+// against x, then delta_prev = x - x_constrained.  As the reference's
+// handleHolonomicConstraints (src/CudaHolonomicConstraint.cu:94-106), every
+// constraint pass also adds its displacement over dt to the velocities; in
+// mode 0 that correction reaches the initial position-Verlet delta.
 __global__ void init_constrain_kernel(Common c, int mode) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= c.ngroups) return;
   int at[4];
   const int m = group_atoms(c, g, at);
   const int2 meta = c.gmeta[g];
-  d3 o[4], n[4];
+  d3 o[4], n[4], n0[4];
   for (int k = 0; k < m; ++k) {
     o[k] = xyz(c.coords[at[k]]);
     n[k] = mode == 0 ? o[k] : o[k] - xyz(c.dprev[at[k]]);
+    n0[k] = n[k];
   }
   apply_constraint(meta.x, m, o, n, c.sk, c.shake_p, meta.y);
+  const double idt = 1.0 / c.dt;
   for (int k = 0; k < m; ++k) {
     const int a = at[k];
+    const double4 v = c.vel[a];
+    const d3 dv = idt * (n[k] - n0[k]);
+    c.vel[a] = make_double4(v.x + dv.x, v.y + dv.y, v.z + dv.z, v.w);
     if (mode == 0) {
       store_position(a, n[k], c.coords, c.xyzq, c.glo2loc, c.slot_off, c.xyzq_s);
     } else {
@@ -594,7 +615,7 @@ __global__ void init_constrain_kernel(Common c, int mode) {
 // (src/CudaLangevinThermostatIntegrator.cu:832-875), gated on the device
 // step counter so the same graph serves every segment
 __global__ void com_sum_kernel(Common c, int natom, int freq) {
-  if (c.sc->step % freq != 0) return;
+  if (*c.err || c.sc->step % freq != 0) return;
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   __shared__ double sh[4][kThreads / 32];
   double v[4] = {0, 0, 0, 0};
@@ -628,7 +649,7 @@ __global__ void com_sum_kernel(Common c, int natom, int freq) {
 }
 
 __global__ void com_apply_kernel(Common c, int natom, int freq) {
-  if (c.sc->step % freq != 0) return;
+  if (*c.err || c.sc->step % freq != 0) return;
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= natom) return;
   const double im = 1.0 / c.sc->com[3];
@@ -659,6 +680,21 @@ struct IntegratorState {
   int ngroups = 0, natom = 0;
   Common c{};
   int blocks_groups = 0, blocks_atoms = 0;
+  // the error word after each of the last two segments, copied to pinned
+  // host memory behind the segment, and the events that say it has landed
+  unsigned *h_err = nullptr;
+  cudaEvent_t seg_done[2] = {nullptr, nullptr};
+  IntegratorState() {
+    APO_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&h_err), 2 * sizeof(unsigned),
+                           cudaHostAllocDefault));
+    h_err[0] = h_err[1] = 0;
+    for (auto &e : seg_done) APO_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  ~IntegratorState() {
+    for (auto &e : seg_done)
+      if (e) cudaEventDestroy(e);
+    if (h_err) cudaFreeHost(h_err);
+  }
 };
 
 // -------------------------------------------------------------- base class
@@ -807,6 +843,7 @@ void CudaIntegrator::buildGroups() {
   c.xyzq_s = fm->neighborList().xyzq_s;
   c.sc = S.sc.p;
   c.partials = S.partials.p;
+  c.err = fm->neighborList().error;
   c.sk = make_settle();
   c.ndegf = m_Ctx->getDegreesOfFreedom();
   c.dt = m_Dt;
@@ -852,65 +889,117 @@ bool CudaIntegrator::unsubscribe(const std::shared_ptr<Subscriber> &sub) {
   return false;
 }
 
+void CudaIntegrator::launchSegment(int len, cudaStream_t s) {
+  if (m_UseGraphs) {
+    auto it = m_Graphs.find(len);
+    if (it == m_Graphs.end()) {
+      cudaGraph_t graph;
+      APO_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      try {
+        segment(len, s);
+      } catch (...) {
+        cudaStreamEndCapture(s, &graph);
+        throw;
+      }
+      APO_CUDA(cudaStreamEndCapture(s, &graph));
+      cudaGraphExec_t exec;
+      // keep the stream priorities of the captured launches
+      APO_CUDA(cudaGraphInstantiate(&exec, graph, cudaGraphInstantiateFlagUseNodePriority));
+      APO_CUDA(cudaGraphDestroy(graph));
+      it = m_Graphs.emplace(len, exec).first;
+    }
+    APO_CUDA(cudaGraphLaunch(it->second, s));
+  } else {
+    segment(len, s);
+  }
+}
+
+// Segments are launched without waiting.  A neighbour-list build that
+// overflows its buffers (or meets non-finite coordinates) sets the list's
+// error word, and from then on every step kernel leaves the state alone, so
+// the state stays at the start of the failed segment.  The word is copied
+// to pinned memory behind every segment and looked at, without waiting,
+// two launches later; at the end (and before every subscriber report) it is
+// read after a synchronisation.  On an overflow the list is grown at the
+// frozen coordinates and the run continues from the device's step counter:
+// the segments after it start at the same steps as in an uninterrupted run,
+// so the trajectory is the same.  Non-finite coordinates end the call with
+// an exception and the state frozen at the failed segment
+// (the reference checks its energies at the report frequency,
+// src/CudaIntegrator.cu:357-369).
 void CudaIntegrator::propagate(int numSteps) {
   if (!m_Ctx)
     throw std::invalid_argument("CudaIntegrator::propagate: no CharmmContext was set for this CudaIntegrator.");
   if (numSteps <= 0) return;
   cudaStream_t s = m_Ctx->stream();
+  IntegratorState &S = *m_S;
+  auto fm = m_Ctx->getForceManager();
   // the first list build sizes the buffers synchronously: never inside a capture
   m_Ctx->ensureNeighborList();
-  const int gen = m_Ctx->getForceManager()->pluginGeneration();
-  if (gen != m_PluginGen) {  // a plug-in force joined or left: capture again
-    clearGraphs();
-    m_PluginGen = gen;
-  }
-  int left = numSteps;
+  const long long step0 = m_Step;
+  const long long dev0 = deviceStep();
   long long done = 0;
-  while (left > 0) {
-    int len = std::min(left, m_ListFreq);
-    // stop a segment at the next report of any subscriber
-    for (auto &sub : m_Subscribers) {
-      const long long f = sub->getReportFrequency();
-      const long long next = (done / f + 1) * f;
-      len = (int)std::min<long long>(len, next - done);
+  int regrowths = 0;
+  for (;;) {
+    const int gen = fm->pluginGeneration();
+    if (gen != m_PluginGen) {  // a plug-in force or a list buffer changed: capture again
+      clearGraphs();
+      m_PluginGen = gen;
     }
-    if (m_UseGraphs) {
-      auto it = m_Graphs.find(len);
-      if (it == m_Graphs.end()) {
-        cudaGraph_t graph;
-        APO_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        try {
-          segment(len, s);
-        } catch (...) {
-          cudaStreamEndCapture(s, &graph);
-          throw;
-        }
-        APO_CUDA(cudaStreamEndCapture(s, &graph));
-        cudaGraphExec_t exec;
-        // keep the stream priorities of the captured launches
-        APO_CUDA(cudaGraphInstantiate(&exec, graph, cudaGraphInstantiateFlagUseNodePriority));
-        APO_CUDA(cudaGraphDestroy(graph));
-        it = m_Graphs.emplace(len, exec).first;
+    long long launched = done;
+    int k = 0;
+    bool seen = false;
+    while (launched < numSteps && !seen) {
+      int len = (int)std::min<long long>(numSteps - launched, m_ListFreq);
+      // stop a segment at the next report of any subscriber
+      for (auto &sub : m_Subscribers) {
+        const long long f = sub->getReportFrequency();
+        const long long next = (launched / f + 1) * f;
+        len = (int)std::min<long long>(len, next - launched);
       }
-      APO_CUDA(cudaGraphLaunch(it->second, s));
-    } else {
-      segment(len, s);
-    }
-    left -= len;
-    m_Step += len;
-    done += len;
-    for (auto &sub : m_Subscribers)
-      if (done % sub->getReportFrequency() == 0) {
+      const int slot = k & 1;
+      if (k >= 2 && cudaEventQuery(S.seg_done[slot]) == cudaSuccess && S.h_err[slot]) {
+        seen = true;
+        break;
+      }
+      launchSegment(len, s);
+      APO_CUDA(cudaMemcpyAsync(&S.h_err[slot], S.c.err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+      APO_CUDA(cudaEventRecord(S.seg_done[slot], s));
+      launched += len;
+      ++k;
+      bool report = false;
+      for (auto &sub : m_Subscribers) report |= launched % sub->getReportFrequency() == 0;
+      if (report) {
         APO_CUDA(cudaStreamSynchronize(s));
-        sub->update(*m_Ctx, m_Step, getTimeStep());
+        if (S.h_err[slot]) {
+          seen = true;
+          break;
+        }
+        m_Step = step0 + launched;
+        for (auto &sub : m_Subscribers)
+          if (launched % sub->getReportFrequency() == 0) sub->update(*m_Ctx, m_Step, getTimeStep());
       }
+    }
+    APO_CUDA(cudaStreamSynchronize(s));
+    const unsigned e = fm->readDeviceError(s);
+    done = deviceStep() - dev0;
+    m_Step = step0 + done;
+    if (!e) {
+      if (done >= numSteps) return;
+      throw std::runtime_error("CudaIntegrator::propagate: the device step counter stopped at " +
+                               std::to_string(done) + " of " + std::to_string(numSteps) + " steps");
+    }
+    if (e & kErrNaN)
+      throw std::runtime_error("non-finite coordinates during propagation (state kept at step " +
+                               std::to_string(m_Step) + ")");
+    if (e & kErrColumnOverflow)
+      throw std::runtime_error("neighbour list: a cell column outgrew the column sort during "
+                               "propagation (state kept at step " + std::to_string(m_Step) + ")");
+    if (++regrowths > 8)
+      throw std::runtime_error("neighbour list capacity exceeded repeatedly during propagation "
+                               "(device error " + std::to_string(e) + ")");
+    fm->growNeighborList(m_Ctx->xyzq(), s);
   }
-  APO_CUDA(cudaStreamSynchronize(s));
-  unsigned e = m_Ctx->getForceManager()->readDeviceError(s);
-  if (e & kErrNaN) throw std::runtime_error("non-finite coordinates during propagation");
-  if (e & (kErrTileOverflow | kErrWorkOverflow | kErrColumnOverflow))
-    throw std::runtime_error("neighbour list capacity exceeded during propagation (device error " +
-                             std::to_string(e) + ")");
 }
 
 double CudaIntegrator::getInstantaneousTemperature() {
@@ -1078,7 +1167,7 @@ void CudaLangevinThermostatIntegrator::initialize() {
   const double gamma = m_Dt * kTimfac * m_Friction;
   if (m_Ctx->isUsingHolonomicConstraints())
     init_constrain_kernel<<<S.blocks_groups, kThreads, 0, s>>>(S.c, 0);
-  m_Ctx->getForceManager()->calcForce(m_Ctx->xyzq(), false, false, s, true);
+  m_Ctx->getForceManager()->calcForceChecked(m_Ctx->xyzq(), false, false, s);
   init_delta_kernel<<<S.blocks_atoms, kThreads, 0, s>>>(S.c, S.natom, gamma);
   if (m_Ctx->isUsingHolonomicConstraints())
     init_constrain_kernel<<<S.blocks_groups, kThreads, 0, s>>>(S.c, 1);
@@ -1117,7 +1206,7 @@ void CudaNoseHooverIntegrator::initialize() {
   APO_CUDA(cudaMemcpy(S.sc.p, &h, sizeof(h), cudaMemcpyHostToDevice));
   if (m_Ctx->isUsingHolonomicConstraints())
     init_constrain_kernel<<<S.blocks_groups, kThreads, 0, s>>>(S.c, 0);
-  m_Ctx->getForceManager()->calcForce(m_Ctx->xyzq(), false, false, s, true);
+  m_Ctx->getForceManager()->calcForceChecked(m_Ctx->xyzq(), false, false, s);
   init_delta_kernel<<<S.blocks_atoms, kThreads, 0, s>>>(S.c, S.natom, 0.0);
   if (m_Ctx->isUsingHolonomicConstraints())
     init_constrain_kernel<<<S.blocks_groups, kThreads, 0, s>>>(S.c, 1);

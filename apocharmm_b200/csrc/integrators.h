@@ -84,6 +84,7 @@ class CudaIntegrator : public std::enable_shared_from_this<CudaIntegrator> {
   virtual void initialize() = 0;
   virtual void stepKernels(cudaStream_t s) = 0;  // the integration after forces
   void segment(int nsteps, cudaStream_t s);      // rebuild + nsteps steps
+  void launchSegment(int nsteps, cudaStream_t s);  // as a captured graph (cached) or eagerly
   void forcesForStep(cudaStream_t s);
   double m_Dt;  // AKMA
   int m_ListFreq = 20, m_ComFreq = 1000;

@@ -647,6 +647,19 @@ void NeighborList::refresh(cudaStream_t s) {
   APO_LAUNCH_CHECK();
 }
 
+void NeighborList::set_capacity(int tile_cap, int work_cap) {
+  if (tile_cap < 1 || work_cap < 1) throw std::invalid_argument("NeighborList: capacities must be positive");
+  m_d.tile_cap = tile_cap;
+  m_d.work_cap = work_cap;
+  dalloc(tiles, m_d.tile_cap);
+  dalloc(masks, (size_t)m_d.tile_cap * kTile);
+  dalloc(work, m_d.work_cap);
+}
+
+void NeighborList::clear_error(cudaStream_t s) {
+  APO_CUDA(cudaMemsetAsync(error, 0, sizeof(unsigned), s));
+}
+
 void NeighborList::sync_counts(cudaStream_t s) {
   int c[8];
   APO_CUDA(cudaMemcpyAsync(c, counts, sizeof(c), cudaMemcpyDeviceToHost, s));

@@ -75,6 +75,9 @@ class NeighborList {
   void set_state_coordinates(const double4 *c) { m_coords = c; }
   // grow capacities if the last build used more than `fill` of them (sync)
   bool ensure_capacity(const float4 *d_xyzq, cudaStream_t s, double fill = 0.8);
+  // tile and work-item capacity set by hand (the buffers are reallocated)
+  void set_capacity(int tile_cap, int work_cap);
+  void clear_error(cudaStream_t s);
 
   const NbListDims &dims() const { return m_d; }
   const std::vector<NbSysDims> &system_dims() const { return m_sys_h; }

@@ -51,14 +51,33 @@ __device__ __forceinline__ void bspline(float w, float (&th)[ORDER], float (&dth
 }
 
 // grid anchoring of the reference (include/cuda_pme_spread.h:64-81):
-// w = x/L + 2, fr = n (w - (floor(w+0.5) - 0.5)), points floor(fr)+0..p-1
-__device__ __forceinline__ void anchor(float x, float recip, int n, int &i0, float &w) {
-  float t = x * recip + 2.0f;
-  float fr = (float)n * (t - (floorf(t + 0.5f) - 0.5f));
-  i0 = (int)fr;
-  w = fr - (float)i0;
+// w = x/L + 2, fr = n (w - (floor(w+0.5) - 0.5)), points floor(fr)+0..p-1.
+// Evaluated in FP64 from the exact global position (cluster origin + local
+// offset): in FP32 the rounding of w near 2 (1.2e-7) times n shifts the
+// B-spline fraction by up to n * 1.2e-7 grid units, which at a 216-point
+// axis is the largest error of the reciprocal force.  The fraction itself
+// is returned in FP32 for the spline recursion.
+__device__ __forceinline__ void anchor(double x, double recip, int n, int &i0, float &w) {
+  const double t = x * recip + 2.0;
+  const double fr = (double)n * (t - (floor(t + 0.5) - 0.5));
   // non-finite or exploded coordinates must not index outside the grid
-  i0 = min(max(i0, 0), n - 1);
+  if (!(fr >= 0.0 && fr < (double)n)) {
+    i0 = fr >= (double)n ? n - 1 : 0;
+    w = 0.f;
+    return;
+  }
+  i0 = (int)fr;
+  w = (float)(fr - (double)i0);
+  if (i0 > n - 1) i0 = n - 1;
+}
+
+// global position of a sorted slot: the cluster origin (a multiple of
+// 1/64 A, exact in FP32) plus the local offset, summed without rounding
+__device__ __forceinline__ double3 global_pos(const float4 &p, const float4 *origin, int s) {
+  if (!origin) return make_double3(p.x, p.y, p.z);
+  const float4 o = origin[s >> 5];
+  return make_double3((double)o.x + (double)p.x, (double)o.y + (double)p.y,
+                      (double)o.z + (double)p.z);
 }
 
 // ------------------------------------------------------------------------
@@ -268,27 +287,22 @@ __global__ void __launch_bounds__(128) spread_kernel(const float4 *__restrict__ 
     const int s = s0 + threadIdx.x;
     float q = 0.f;
     if (s < nslot) {
-      float4 p = xyzq[s];
-      if (origin) {  // cluster-local coordinates: add the cluster's origin
-        const float4 o = origin[s >> 5];
-        p.x += o.x;
-        p.y += o.y;
-        p.z += o.z;
-      }
+      const float4 p = xyzq[s];
+      const double3 g = global_pos(p, origin, s);
       q = p.w;
       float th[ORDER], dth[ORDER], w;
       int i0;
-      anchor(p.x, 1.f / d.Lx, d.nx, i0, w);
+      anchor(g.x, d.rLx, d.nx, i0, w);
       bspline<ORDER>(w, th, dth);
       sh_i[0][threadIdx.x] = i0;
 #pragma unroll
       for (int k = 0; k < ORDER; ++k) sh_th[0][threadIdx.x][k] = th[k];
-      anchor(p.y, 1.f / d.Ly, d.ny, i0, w);
+      anchor(g.y, d.rLy, d.ny, i0, w);
       bspline<ORDER>(w, th, dth);
       sh_i[1][threadIdx.x] = i0;
 #pragma unroll
       for (int k = 0; k < ORDER; ++k) sh_th[1][threadIdx.x][k] = th[k];
-      anchor(p.z, 1.f / d.Lz, d.nz, i0, w);
+      anchor(g.z, d.rLz, d.nz, i0, w);
       bspline<ORDER>(w, th, dth);
       sh_i[2][threadIdx.x] = i0;
 #pragma unroll
@@ -569,22 +583,18 @@ __global__ void __launch_bounds__(256) gather_kernel(const float4 *__restrict__ 
   const int s = blockIdx.x * 32 + (threadIdx.x >> 3);
   const int sub = threadIdx.x & 7;
   float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
+  double3 g = make_double3(0.0, 0.0, 0.0);
   if (s < nslot) {
     p = xyzq[s];
-    if (origin) {  // cluster-local coordinates: add the cluster's origin
-      const float4 o = origin[s >> 5];
-      p.x += o.x;
-      p.y += o.y;
-      p.z += o.z;
-    }
+    g = global_pos(p, origin, s);
   }
   float thx[ORDER], thy[ORDER], thz[ORDER], dx[ORDER], dy[ORDER], dz[ORDER], w;
   int ix, iy, iz;
-  anchor(p.x, 1.f / d.Lx, d.nx, ix, w);
+  anchor(g.x, d.rLx, d.nx, ix, w);
   bspline<ORDER>(w, thx, dx);
-  anchor(p.y, 1.f / d.Ly, d.ny, iy, w);
+  anchor(g.y, d.rLy, d.ny, iy, w);
   bspline<ORDER>(w, thy, dy);
-  anchor(p.z, 1.f / d.Lz, d.nz, iz, w);
+  anchor(g.z, d.rLz, d.nz, iz, w);
   bspline<ORDER>(w, thz, dz);
   float f1 = 0.f, f2 = 0.f, f3 = 0.f;
   if (s < nslot && p.w != 0.f) {
@@ -730,6 +740,9 @@ void Pme::setup(int nx, int ny, int nz, int order, double kappa, double Lx, doub
     throw std::invalid_argument("PME grid dimensions above 256 are not supported");
   if (order != 4 && order != 6 && order != 8)
     throw std::invalid_argument("PME spline order must be 4, 6 or 8");
+  // a spline's p points wrap the grid at most once only when n >= p
+  if (nx < order || ny < order || nz < order)
+    throw std::invalid_argument("PME grid dimensions must be at least the spline order");
   const size_t plane_bytes = (size_t)(ny / 2) * (nx + 2) * sizeof(float2);
   if (plane_bytes > 227 * 1024)
     throw std::invalid_argument("PME plane does not fit in shared memory");
@@ -742,6 +755,9 @@ void Pme::setup(int nx, int ny, int nz, int order, double kappa, double Lx, doub
   m_d.Lx = (float)Lx;
   m_d.Ly = (float)Ly;
   m_d.Lz = (float)Lz;
+  m_d.rLx = 1.0 / Lx;
+  m_d.rLy = 1.0 / Ly;
+  m_d.rLz = 1.0 / Lz;
   m_d.kappa = (float)kappa;
   m_d.ax = plan_axis(nx);
   m_d.ay = plan_axis(ny);
@@ -894,6 +910,8 @@ void PmeMulti::setup(const std::vector<PmeSystemSpec> &systems, int order, long 
       throw std::invalid_argument("PME grid dimensions must be even");
     if (y.nx > 256 || y.ny > 256 || y.nz > 256)
       throw std::invalid_argument("PME grid dimensions above 256 are not supported");
+    if (y.nx < order || y.ny < order || y.nz < order)
+      throw std::invalid_argument("PME grid dimensions must be at least the spline order");
     const size_t plane_bytes = (size_t)(y.ny / 2) * (y.nx + 2) * sizeof(float2);
     if (plane_bytes > 227 * 1024) throw std::invalid_argument("PME plane does not fit in shared memory");
     m_plane_smem = std::max(m_plane_smem, plane_bytes);
@@ -906,6 +924,9 @@ void PmeMulti::setup(const std::vector<PmeSystemSpec> &systems, int order, long 
     A.d.Lx = (float)y.Lx;
     A.d.Ly = (float)y.Ly;
     A.d.Lz = (float)y.Lz;
+    A.d.rLx = 1.0 / y.Lx;
+    A.d.rLy = 1.0 / y.Ly;
+    A.d.rLz = 1.0 / y.Lz;
     A.d.kappa = (float)y.kappa;
     A.d.ax = Pme::plan_axis(y.nx);
     A.d.ay = Pme::plan_axis(y.ny);
@@ -1193,6 +1214,9 @@ void pme_reciprocal_static(const float4 *xyzq, int n, double Lx, double Ly, doub
     throw std::invalid_argument("pme_reciprocal_static: grid dimensions must be even, 2..256");
   if (order != 4 && order != 6 && order != 8)
     throw std::invalid_argument("pme_reciprocal_static: spline order must be 4, 6 or 8");
+  if (nx < order || ny < order || nz < order)
+    throw std::invalid_argument(
+        "pme_reciprocal_static: grid dimensions must be at least the spline order");
   if ((size_t)(ny / 2) * (nx + 2) * sizeof(float2) > 227 * 1024)
     throw std::invalid_argument("pme_reciprocal_static: grid plane does not fit in shared memory");
   const StaticLayout l = static_layout(nx, ny, nz);
@@ -1209,6 +1233,9 @@ void pme_reciprocal_static(const float4 *xyzq, int n, double Lx, double Ly, doub
   d.Lx = (float)Lx;
   d.Ly = (float)Ly;
   d.Lz = (float)Lz;
+  d.rLx = 1.0 / Lx;
+  d.rLy = 1.0 / Ly;
+  d.rLz = 1.0 / Lz;
   d.kappa = (float)kappa;
   if (!fixed_plan_axis(nx, d.ax) || !fixed_plan_axis(ny, d.ay) || !fixed_plan_axis(nz, d.az))
     throw std::invalid_argument("pme_reciprocal_static: grid sizes must factor into 2, 3, 5 and 7");

@@ -38,6 +38,7 @@ struct FftAxis {
 struct PmeDims {
   int nx, ny, nz, nxc, order;
   float Lx, Ly, Lz;       // box
+  double rLx, rLy, rLz;   // 1 / box, for the FP64 grid anchoring
   float kappa;
   FftAxis ax, ay, az;
 };

@@ -237,8 +237,9 @@ Topology build_topology(const CharmmPSF &psf, const CharmmParameters &prm) {
         if (f != prm.bonds.end()) b0 = f->second.b0;
       }
       t.shake_atoms.push_back(g);
-      t.shake_p.push_back(make_float4((float)(1.0 / t.mass[i]), 0.f, b0 * b0,
-                                      (float)(1.0 / t.mass[hyd[i].back()])));
+      // inverse masses rounded as the reference rounds them (1.0f / (float)m)
+      t.shake_p.push_back(make_float4(1.0f / (float)t.mass[i], 0.f, b0 * b0,
+                                      1.0f / (float)t.mass[hyd[i].back()]));
     }
   }
   for (auto &g : psf.getConnectedComponents()) t.groups.push_back({g[0], g[1]});

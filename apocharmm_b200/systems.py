@@ -309,137 +309,6 @@ def solvated_chain(n_atoms: int = 23558, L: float = 62.23, n_beads: int = 2489,
     # waters: candidate lattice sites away from the chain
     n_edge = int(math.ceil((n_water * 1.6) ** (1.0 / 3.0)))
     sites = _lattice_sites(L, n_edge)
-    # distance to the nearest bead (minimum image) via a periodic KD-tree
-    from scipy.spatial import cKDTree
-
-    def _wrap(p):
-        w = np.mod(p + L / 2, L)
-        return np.where(w >= L, w - L, w)
-    dist, _ = cKDTree(_wrap(chain), boxsize=L).query(_wrap(sites), k=1)
-    keep = dist >= 3.0
-    sites = sites[keep]
-    pos = _place_waters(rng, sites, jitter, L)
-    bonds, angles, types, names, resn, resi, segs = _water_topology(n_molecules)
-    p = _water_params()
-    n = 3 * n_molecules
-    return System(
-        name=name, box=(L, L, L), pos=pos,
-        charge=np.tile([Q_O, Q_H, Q_H], n_molecules).astype(np.float64),
-        mass=np.tile([M_O, M_H, M_H], n_molecules).astype(np.float64),
-        atom_type=types, atom_name=names, res_name=resn, res_id=resi, seg_id=segs,
-        bonds=bonds.astype(np.int64), angles=angles.astype(np.int64),
-        dihedrals=np.zeros((0, 4), np.int64), impropers=np.zeros((0, 4), np.int64),
-        masses_by_type=p["masses_by_type"], bond_params=p["bond_params"],
-        angle_params=p["angle_params"], dihedral_params={}, improper_params={},
-        lj_params=p["lj"], lj14_params={},
-    )
-
-
-def _self_avoiding_chain(rng, n_beads: int, L: float, bond: float = 1.53,
-                         theta0: float = 111.0, min_dist: float = 2.6,
-                         margin: float = 1.5) -> np.ndarray:
-    """Confined self-avoiding walk with fixed bond length and angle.
-
-    Beads stay inside [-L/2+margin, L/2-margin]^3 so the molecule never crosses
-    the periodic boundary; non-neighbour beads (|i-j|>3) keep min_dist apart.
-    """
-    half = L / 2 - margin
-    cell = min_dist
-    ncell = max(1, int(L // cell))
-    grid: Dict[Tuple[int, int, int], List[int]] = {}
-    md2 = min_dist ** 2
-    hl = L / 2
-
-    def key(p):
-        return (int((p[0] + hl) // cell) % ncell, int((p[1] + hl) // cell) % ncell,
-                int((p[2] + hl) // cell) % ncell)
-
-    def clash(p, upto):
-        k = key(p)
-        px, py, pz = float(p[0]), float(p[1]), float(p[2])
-        for dx in (-1, 0, 1):
-            for dy in (-1, 0, 1):
-                for dz in (-1, 0, 1):
-                    kk = ((k[0] + dx) % ncell, (k[1] + dy) % ncell, (k[2] + dz) % ncell)
-                    for j in grid.get(kk, ()):
-                        if j < upto - 3:
-                            q = posl[j]
-                            ex, ey, ez = q[0] - px, q[1] - py, q[2] - pz
-                            if ex * ex + ey * ey + ez * ez < md2:
-                                return True
-        return False
-
-    pos = np.zeros((n_beads, 3))
-    posl = [None] * n_beads             # the same positions as Python floats
-    # a walk that keeps back-tracking in a dead end is started afresh
-    limit = 20 * n_beads + 10000
-    iters = 0
-    pos[0] = rng.uniform(-half / 2, half / 2, 3)
-    d = rng.normal(size=3)
-    pos[1] = pos[0] + bond * d / np.linalg.norm(d)
-    for b in (0, 1):
-        posl[b] = (float(pos[b][0]), float(pos[b][1]), float(pos[b][2]))
-        grid.setdefault(key(pos[b]), []).append(b)
-    ct = math.cos(math.radians(180.0 - theta0))
-    st = math.sin(math.radians(180.0 - theta0))
-    i = 2
-    fails = 0
-    while i < n_beads:
-        iters += 1
-        if iters > limit:
-            return _self_avoiding_chain(rng, n_beads, L, bond, theta0, min_dist, margin)
-        u = pos[i - 1] - pos[i - 2]
-        u /= np.linalg.norm(u)
-        a = np.cross(u, [1.0, 0.0, 0.0])
-        if np.linalg.norm(a) < 1e-3:
-            a = np.cross(u, [0.0, 1.0, 0.0])
-        a /= np.linalg.norm(a)
-        b2 = np.cross(u, a)
-        ok = False
-        for _ in range(40):
-            phi = rng.uniform(0, 2 * np.pi)
-            d = ct * u + st * (math.cos(phi) * a + math.sin(phi) * b2)
-            p = pos[i - 1] + bond * d
-            if np.all(np.abs(p) < half) and not clash(p, i):
-                ok = True
-                break
-        if ok:
-            pos[i] = p
-            posl[i] = (float(p[0]), float(p[1]), float(p[2]))
-            grid.setdefault(key(p), []).append(i)
-            i += 1
-            fails = 0
-        else:
-            # back-track a few beads
-            fails += 1
-            nb = min(i - 2, 2 + fails)
-            for j in range(i - nb, i):
-                grid[key(pos[j])].remove(j)
-            i -= nb
-    return pos
-
-
-def solvated_chain(n_atoms: int = 23558, L: float = 62.23, n_beads: int = 2489,
-                   seed: int = 1234, n_types: int = 8, name: str = "chain") -> System:
-    """Seeded bead chain (bonds, angles, n=3 dihedrals, 1-4 scaled LJ) in TIP3P."""
-    rng = np.random.default_rng(seed)
-    n_water = (n_atoms - n_beads) // 3
-    if n_beads + 3 * n_water != n_atoms:
-        raise ValueError("n_atoms - n_beads must be a multiple of 3")
-    chain = _self_avoiding_chain(rng, n_beads, L)
-    # LJ types: eps in [0.05, 0.2], rmin/2 in [1.3, 2.1]; 1-4 values scaled
-    types = [f"CB{k + 1}" for k in range(n_types)]
-    eps = np.linspace(0.05, 0.2, n_types)
-    rmh = np.linspace(1.3, 2.1, n_types)
-    perm = rng.permutation(n_types)
-    lj = {types[k]: (-float(eps[perm[k]]), float(rmh[k])) for k in range(n_types)}
-    lj14 = {t: (0.5 * lj[t][0], lj[t][1] - 0.1) for t in types}
-    bead_type = [types[k] for k in rng.integers(0, n_types, n_beads)]
-    q = rng.uniform(-0.5, 0.5, n_beads)
-    q -= q.mean()
-    # waters: candidate lattice sites away from the chain
-    n_edge = int(math.ceil((n_water * 1.6) ** (1.0 / 3.0)))
-    sites = _lattice_sites(L, n_edge)
     # distance to nearest bead (minimum image) via a coarse cell search
     keep = np.ones(sites.shape[0], bool)
     cell = 3.0
@@ -513,6 +382,141 @@ def solvated_chain(n_atoms: int = 23558, L: float = 62.23, n_beads: int = 2489,
     )
 
 
+def _dir(axis, refv, theta, phi):
+    """Unit vector at angle theta (degrees) from `axis`, turned by phi
+    (degrees) about it out of the plane of `axis` and `refv`."""
+    u = axis / np.linalg.norm(axis)
+    r = refv - (refv @ u) * u
+    r /= np.linalg.norm(r)
+    w = np.cross(u, r)
+    t, f = math.radians(theta), math.radians(phi)
+    return math.cos(t) * u + math.sin(t) * (math.cos(f) * r + math.sin(f) * w)
+
+
+def _ethanol():
+    """CH3-CH2-OH: SHAKE clusters of 4 (CH3), 3 (CH2) and 2 (OH) atoms."""
+    c1 = np.array([0.0, 0.0, 0.0])
+    c2 = np.array([1.528, 0.0, 0.0])
+    o1 = c2 + 1.42 * _dir(c1 - c2, np.array([0.0, 1.0, 0.0]), 110.1, 0.0)
+    h_c1 = [c1 + 1.111 * _dir(c2 - c1, o1 - c2, 110.1, 180.0 + k * 120.0) for k in range(3)]
+    h_c2 = [c2 + 1.111 * _dir(c1 - c2, o1 - c2, 110.1, k) for k in (120.0, 240.0)]
+    ho = o1 + 0.96 * _dir(c2 - o1, c1 - c2, 106.0, 180.0)
+    return dict(
+        xyz=np.stack([c1, *h_c1, c2, *h_c2, o1, ho]),
+        types=["CT3", "HA", "HA", "HA", "CT2", "HA", "HA", "OH1", "H"],
+        names=["C1", "H11", "H12", "H13", "C2", "H21", "H22", "O1", "HO1"],
+        charges=[-0.27, 0.09, 0.09, 0.09, 0.05, 0.09, 0.09, -0.66, 0.43],
+        bonds=[(0, 1), (0, 2), (0, 3), (0, 4), (4, 5), (4, 6), (4, 7), (7, 8)],
+        resname="ETOH")
+
+
+def _glycol():
+    """HO-CH2-CH2-OH: SHAKE clusters of 3 (CH2) and 2 (OH) atoms only."""
+    c1 = np.array([0.0, 0.0, 0.0])
+    c2 = np.array([1.53, 0.0, 0.0])
+    o1 = c1 + 1.42 * _dir(c2 - c1, np.array([0.0, 1.0, 0.0]), 110.1, 0.0)
+    o2 = c2 + 1.42 * _dir(c1 - c2, o1 - c1, 110.1, 180.0)
+    h_c1 = [c1 + 1.111 * _dir(c2 - c1, o1 - c1, 110.1, k) for k in (120.0, 240.0)]
+    h_c2 = [c2 + 1.111 * _dir(c1 - c2, o2 - c2, 110.1, k) for k in (120.0, 240.0)]
+    ho1 = o1 + 0.96 * _dir(c1 - o1, c2 - c1, 106.0, 180.0)
+    ho2 = o2 + 0.96 * _dir(c2 - o2, c1 - c2, 106.0, 180.0)
+    return dict(
+        xyz=np.stack([o1, ho1, c1, *h_c1, c2, *h_c2, o2, ho2]),
+        types=["OH1", "H", "CT2", "HA", "HA", "CT2", "HA", "HA", "OH1", "H"],
+        names=["O1", "HO1", "C1", "H11", "H12", "C2", "H21", "H22", "O2", "HO2"],
+        charges=[-0.66, 0.43, 0.05, 0.09, 0.09, 0.05, 0.09, 0.09, -0.66, 0.43],
+        bonds=[(0, 1), (0, 2), (2, 3), (2, 4), (2, 5), (5, 6), (5, 7), (5, 8), (8, 9)],
+        resname="EGLY")
+
+
+def _angles_dihedrals(bonds, n):
+    """All angles i-j-k and proper dihedrals i-j-k-l of a bond graph."""
+    nb = [set() for _ in range(n)]
+    for a, b in bonds:
+        nb[a].add(b)
+        nb[b].add(a)
+    angles = sorted({(min(i, k), j, max(i, k)) for j in range(n) for i in nb[j] for k in nb[j] if i != k})
+    dih = set()
+    for j, k in bonds:
+        for i in nb[j] - {k}:
+            for l in nb[k] - {j}:
+                if i != l:
+                    dih.add((i, j, k, l) if (i, j) < (l, k) else (l, k, j, i))
+    return angles, sorted(dih)
+
+
+# CHARMM-like parameters of the small solutes (types CT3, CT2, HA, OH1, H)
+_SOLUTE_BONDS = {("CT3", "HA"): (322.0, 1.111), ("CT2", "HA"): (309.0, 1.111),
+                 ("CT2", "CT3"): (222.5, 1.528), ("CT2", "CT2"): (222.5, 1.53),
+                 ("CT2", "OH1"): (428.0, 1.42), ("H", "OH1"): (545.0, 0.96)}
+_SOLUTE_ANGLES = {("HA", "CT3", "HA"): (35.5, 108.4), ("CT2", "CT3", "HA"): (34.6, 110.1),
+                  ("CT3", "CT2", "HA"): (34.6, 110.1), ("HA", "CT2", "HA"): (35.5, 109.0),
+                  ("CT3", "CT2", "OH1"): (75.7, 110.1), ("HA", "CT2", "OH1"): (45.9, 108.89),
+                  ("CT2", "OH1", "H"): (57.5, 106.0), ("CT2", "CT2", "HA"): (26.5, 110.1),
+                  ("CT2", "CT2", "OH1"): (75.7, 110.1)}
+_SOLUTE_DIHEDRALS = {("X", "CT2", "CT3", "X"): [(0.16, 3, 0.0)],
+                     ("X", "CT2", "OH1", "X"): [(0.14, 3, 0.0)],
+                     ("X", "CT2", "CT2", "X"): [(0.19, 3, 0.0)]}
+_SOLUTE_LJ = {"CT3": (-0.078, 2.04), "CT2": (-0.055, 2.175), "HA": (-0.022, 1.32),
+              "OH1": (-0.1521, 1.77), "H": (-0.046, 0.2245)}
+_SOLUTE_MASSES = {"CT3": 12.011, "CT2": 12.011, "HA": 1.008, "OH1": 15.999, "H": 1.008}
+
+
+def solvated_solute(mol: dict, n_mol: int, L: float, seed: int, name: str) -> System:
+    """n_mol copies of a small molecule at seeded random positions (at least
+    6.5 A apart) and orientations in a TIP3P box of edge L, waters on a
+    jittered lattice away from the solutes."""
+    from scipy.spatial import cKDTree
+
+    rng = np.random.default_rng(seed)
+    t = mol["xyz"] - mol["xyz"].mean(axis=0)
+    na = t.shape[0]
+    R = _random_rotations(rng, n_mol)
+    centres = []
+    while len(centres) < n_mol:
+        c = rng.uniform(-L / 2, L / 2, 3)
+        if all(np.linalg.norm((c - q) - L * np.round((c - q) / L)) > 6.5 for q in centres):
+            centres.append(c)
+    spos = (np.asarray(centres)[:, None, :] + np.einsum("nij,aj->nai", R, t)).reshape(-1, 3)
+
+    def _wrap(p):
+        w = np.mod(p + L / 2, L)
+        return np.where(w >= L, w - L, w)
+    sites = _lattice_sites(L, int(round(L / 3.0)))
+    dist, _ = cKDTree(_wrap(spos), boxsize=L).query(_wrap(sites), k=1)
+    sites = sites[dist >= 2.7]
+    n_water = sites.shape[0]
+    wpos = _place_waters(rng, sites, 0.2, L, others=spos, d_min=1.6)
+    ns = na * n_mol
+    wb, wa, wt, wn, wrn, wri, ws = _water_topology(n_water, first_atom=ns, first_res=n_mol + 1)
+    ang1, dih1 = _angles_dihedrals(mol["bonds"], na)
+    off = (na * np.arange(n_mol))[:, None, None]
+    b = (np.asarray(mol["bonds"])[None] + off).reshape(-1, 2)
+    a = (np.asarray(ang1)[None] + off).reshape(-1, 3)
+    d = (np.asarray(dih1)[None] + off).reshape(-1, 4)
+    wp = _water_params()
+    bond_params = {**wp["bond_params"], **_SOLUTE_BONDS}
+    angle_params = {**wp["angle_params"], **_SOLUTE_ANGLES}
+    masses = {**wp["masses_by_type"], **_SOLUTE_MASSES}
+    lj = {**wp["lj"], **_SOLUTE_LJ}
+    types = mol["types"] * n_mol + wt
+    return System(
+        name=name, box=(L, L, L), pos=np.concatenate([spos, wpos]),
+        charge=np.concatenate([np.tile(mol["charges"], n_mol), np.tile([Q_O, Q_H, Q_H], n_water)]),
+        mass=np.array([masses[x] for x in types]),
+        atom_type=types, atom_name=mol["names"] * n_mol + wn,
+        res_name=[mol["resname"]] * ns + wrn,
+        res_id=[1 + k // na for k in range(ns)] + wri,
+        seg_id=["SOL"] * ns + ws,
+        bonds=np.concatenate([b, wb]).astype(np.int64),
+        angles=np.concatenate([a, wa]).astype(np.int64),
+        dihedrals=d.astype(np.int64), impropers=np.zeros((0, 4), np.int64),
+        masses_by_type=masses, bond_params=bond_params, angle_params=angle_params,
+        dihedral_params=dict(_SOLUTE_DIHEDRALS), improper_params={}, lj_params=lj,
+        lj14_params={},
+    )
+
+
 # --------------------------------------------------------------------------
 # named workloads
 # --------------------------------------------------------------------------
@@ -539,6 +543,24 @@ def config_large_water(seed: int = 77) -> System:
     s = water_box(333333, L, seed=seed, name="water1m")
     s.settings = dict(kappa=0.34, nfft=(216, 216, 216), order=4, ctofnb=10.0,
                       ctonnb=8.0, cutnb=11.5, dt_ps=0.002)
+    return s
+
+
+def config_ethanol(seed: int = 31) -> System:
+    """40 ethanols in TIP3P (32 A box): SHAKE clusters of 2, 3 and 4 atoms
+    beside SETTLE waters; PME 32^3 order 4, roff 10, ron 8, list 12."""
+    s = solvated_solute(_ethanol(), 40, 32.0, seed, "ethanol3k")
+    s.settings = dict(kappa=0.34, nfft=(32, 32, 32), order=4, ctofnb=10.0,
+                      ctonnb=8.0, cutnb=12.0, dt_ps=0.002)
+    return s
+
+
+def config_glycol(seed: int = 37) -> System:
+    """40 ethylene glycols in TIP3P (32 A box): SHAKE clusters of 2 and 3
+    atoms beside SETTLE waters; PME 32^3 order 4, roff 10, ron 8, list 12."""
+    s = solvated_solute(_glycol(), 40, 32.0, seed, "glycol3k")
+    s.settings = dict(kappa=0.34, nfft=(32, 32, 32), order=4, ctofnb=10.0,
+                      ctonnb=8.0, cutnb=12.0, dt_ps=0.002)
     return s
 
 

@@ -51,6 +51,14 @@ APOCHARMM_C_API apo_status apo_charmm_context_get_num_atoms(size_t *num_atoms, c
 APOCHARMM_C_API apo_status apo_charmm_context_get_degrees_of_freedom(int *ndegf, const apo_charmm_context *context);
 APOCHARMM_C_API apo_status apo_charmm_context_reset_neighbor_list(apo_charmm_context *context);
 APOCHARMM_C_API apo_status apo_charmm_context_get_neighbor_pairs(int *pairs, const size_t len, size_t *num_pairs, const double radius, apo_charmm_context *context);
+/* addition: every atom pair the tile list holds (the ForceManager's cluster
+ * pairs; the reference's list is ientry/tile_indj/tile_excl,
+ * src/CudaNeighborListBuild.cu:727,902-912) whose distance, in FP64 from the
+ * sorted coordinates and the tile's image shift, is below `radius`, masked
+ * or not, as (global i, global j, excluded) triples: excluded = 1 when the
+ * tile's exclusion mask drops the pair.  Each unordered pair appears once.
+ * With pairs == NULL only *num_pairs is set; len counts ints. */
+APOCHARMM_C_API apo_status apo_charmm_context_get_list_pairs(int *pairs, const size_t len, size_t *num_pairs, const double radius, apo_charmm_context *context);
 /* CUDA-event timing of the direct-space kernel: enable (clears the
  * integrators' captured graphs on their next propagate is NOT done; enable it
  * before creating the integrator), then read the summed milliseconds and the

@@ -36,6 +36,13 @@ APOCHARMM_C_API apo_status apo_force_manager_get_fft_grid(int *nxyz3, const apo_
 /* addition: direct-space kernel form, 0 = one j-list per tile for the whole
  * i-cluster (default), 1 = one queue per 8-atom i-group across tiles */
 APOCHARMM_C_API apo_status apo_force_manager_set_direct_kernel(apo_force_manager *force_manager, const int form);
+/* addition: tile capacity of the neighbour list (the work-item capacity
+ * follows); needs an initialised manager.  The list is rebuilt before its
+ * next use; a list that outgrows the capacity is grown (during propagate,
+ * the segment whose build overflowed is run again from the unchanged state,
+ * so the trajectory is the same).  Capacity of the last build: get_list_capacity. */
+APOCHARMM_C_API apo_status apo_force_manager_set_list_capacity(apo_force_manager *force_manager, const int tiles);
+APOCHARMM_C_API apo_status apo_force_manager_get_list_capacity(int *tiles, const apo_force_manager *force_manager);
 #ifdef __cplusplus
 }
 #endif

@@ -19,6 +19,20 @@
 //     deterministic steepest descent on the reference's forces: each
 //     iteration moves every atom along -gradient, the largest move
 //     `max_step` Angstrom; writes the final x y z per line.
+//   ref_harness traj <psf> <prm> <crd> <L> <kappa> <cutnb> <ctonnb> <ctofnb>
+//               <nx> <ny> <nz> <order> <langevin|leapfrog|nosehoover> <steps>
+//               <seed> <friction> <velocities> <out>
+//     takes the velocities (3N values, A per AKMA time unit) from a text file
+//     (CharmmContext::assignVelocities), runs `steps` steps of the named
+//     integrator at 300 K with dt 2 fs and writes per atom the FP64 state
+//     x y z, the single-precision x y z (the only copy the reference's
+//     leapfrog advances) and vx vy vz.
+//   ref_harness nblist <psf> <prm> <crd> <L> <kappa> <cutnb> <ctonnb> <ctofnb>
+//               <nx> <ny> <nz> <order> <radius> <out>
+//     builds the neighbour list (CharmmContext::resetNeighborList) and writes
+//     every atom pair of its tiles whose distance (FP64, from the sorted
+//     coordinates and the tile's image shift) is below `radius` as int32
+//     triples (global i, global j, exclusion bit) to a binary file.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -37,10 +51,36 @@
 #include "CharmmParameters.h"
 #include "CudaLangevinThermostatIntegrator.h"
 #include "CudaLeapFrogIntegrator.h"
+#include "CudaNeighborList.h"
 #include "CudaNoseHooverIntegrator.h"
+#include "CudaPMEDirectForce.h"
 #include "ForceManager.h"
 
 namespace {
+
+// White-box access to the list the reference's direct-space force builds:
+// pointers to protected members, formed in a class derived from the owner,
+// applied to the owner's object (no change to the reference's classes).
+struct FmPeek : ForceManager {
+  static CudaPMEDirectForce<long long int, float> *direct(ForceManager &f) {
+    return (f.*(&FmPeek::m_DirectForcePtr)).get();
+  }
+};
+struct DirectPeek : CudaPMEDirectForce<long long int, float> {
+  using D = CudaPMEDirectForce<long long int, float>;
+  static CudaNeighborList<32> &list(D &d) { return *(d.*(&DirectPeek::neighborList)); }
+  static const float4 *sorted(D &d) {
+    return (d.*(&DirectPeek::xyzq_sorted)).getDeviceArray().data();
+  }
+  static const int *l2g(D &d) { return d.*(&DirectPeek::loc2glo); }
+};
+
+template <typename T>
+std::vector<T> from_device(const T *p, size_t n) {
+  std::vector<T> h(n);
+  if (n) cudaMemcpy(h.data(), p, n * sizeof(T), cudaMemcpyDeviceToHost);
+  return h;
+}
 
 struct Setup {
   std::vector<double4> xyz;
@@ -169,6 +209,113 @@ int main(int argc, char **argv) {
     std::printf("{\"steps\": %d, \"seconds\": %.6f, \"ns_per_day\": %.4f, "
                 "\"integrator\": \"%s\", \"temperature_end\": %.3f}\n",
                 steps, sec, 86400.0 * steps / sec * 0.002 * 1e-3, kind.c_str(), temp);
+    return 0;
+  }
+  if (mode == "traj" && argc == 20) {
+    Setup s = make(argv + 2);
+    const std::string kind = argv[14];
+    const int steps = std::atoi(argv[15]);
+    const unsigned long long seed = std::strtoull(argv[16], nullptr, 10);
+    const double friction = std::atof(argv[17]);
+    const int n = s.ctx->getNumAtoms();
+    std::vector<double> vel;
+    {
+      FILE *in = std::fopen(argv[18], "r");
+      if (!in) return 3;
+      double v;
+      while (std::fscanf(in, "%lf", &v) == 1) vel.push_back(v);
+      std::fclose(in);
+    }
+    if ((int)vel.size() != 3 * n) {
+      std::fprintf(stderr, "velocity file holds %zu values, expected %d\n", vel.size(), 3 * n);
+      return 2;
+    }
+    s.ctx->assignVelocities(vel);
+    std::shared_ptr<CudaIntegrator> integ;
+    if (kind == "langevin") {
+      auto lg = std::make_shared<CudaLangevinThermostatIntegrator>(0.002);
+      lg->setThermostatFriction(friction);
+      lg->setReferenceTemperature(300.0);
+      lg->setThermostatRngSeed(seed);
+      integ = lg;
+    } else if (kind == "leapfrog") {
+      integ = std::make_shared<CudaLeapFrogIntegrator>(0.002);
+    } else if (kind == "nosehoover") {
+      auto nh = std::make_shared<CudaNoseHooverIntegrator>(0.002);
+      nh->setReferenceTemperature(300.0);
+      integ = nh;
+    } else {
+      std::fprintf(stderr, "unknown integrator %s\n", kind.c_str());
+      return 2;
+    }
+    integ->setCharmmContext(s.ctx);
+    if (steps > 0) integ->propagate(steps);
+    cudaDeviceSynchronize();
+    auto x = from_device(s.ctx->getCoordinatesCharges().getDeviceArray().data(), n);
+    auto xf = from_device(s.ctx->getXYZQ().getDeviceArray().data(), n);
+    auto v = from_device(s.ctx->getVelocityMass().getDeviceArray().data(), n);
+    FILE *out = std::fopen(argv[19], "w");
+    if (!out) return 3;
+    for (int i = 0; i < n; ++i)
+      std::fprintf(out, "%.17g %.17g %.17g %.9g %.9g %.9g %.17g %.17g %.17g\n", x[i].x, x[i].y,
+                   x[i].z, xf[i].x, xf[i].y, xf[i].z, v[i].x, v[i].y, v[i].z);
+    std::fclose(out);
+    return 0;
+  }
+  if (mode == "nblist" && argc == 16) {
+    Setup s = make(argv + 2);
+    const double radius = std::atof(argv[14]);
+    s.ctx->resetNeighborList();
+    s.ctx->calculatePotentialEnergy(true, false);
+    cudaDeviceSynchronize();
+    auto *direct = FmPeek::direct(*s.fm);
+    if (!direct) {
+      std::fprintf(stderr, "no direct-space force\n");
+      return 2;
+    }
+    auto &nl = DirectPeek::list(*direct);
+    auto &b = nl.getBuilder(0);
+    const int n = s.ctx->getNumAtoms();
+    const int ne = b.get_n_ientry(), nt = b.get_n_tile();
+    auto ientry = from_device(b.get_ientry(), ne);
+    auto indj = from_device(b.get_tile_indj(), nt);
+    auto excl = from_device(b.get_tile_excl(), nt);
+    auto xs = from_device(DirectPeek::sorted(*direct), n);
+    auto l2g = from_device(DirectPeek::l2g(*direct), n);
+    const double L = std::atof(argv[5]);
+    const double r2 = radius * radius;
+    std::vector<int> out3;
+    for (const ientry_t &e : ientry) {
+      int ish = e.ish;
+      const double shz = (ish / 9 - 1) * L;
+      ish -= (ish / 9) * 9;
+      const double shy = (ish / 3 - 1) * L;
+      ish -= (ish / 3) * 3;
+      const double shx = (ish - 1) * L;
+      for (int t = e.tileStart; t <= e.tileEnd; ++t) {
+        for (int wid = 0; wid < 32; ++wid) {
+          const int j = indj[t] + wid;
+          if (j >= n) continue;
+          const unsigned word = excl[t].excl[wid];
+          for (int k = 0; k < 32; ++k) {
+            const int i = e.iatomStart + (wid + k) % 32;
+            if (i >= n) continue;
+            const double dx = (double)xs[i].x + shx - (double)xs[j].x;
+            const double dy = (double)xs[i].y + shy - (double)xs[j].y;
+            const double dz = (double)xs[i].z + shz - (double)xs[j].z;
+            if (dx * dx + dy * dy + dz * dz >= r2) continue;
+            out3.push_back(l2g[i]);
+            out3.push_back(l2g[j]);
+            out3.push_back((int)((word >> k) & 1u));
+          }
+        }
+      }
+    }
+    FILE *out = std::fopen(argv[15], "wb");
+    if (!out) return 3;
+    std::fwrite(out3.data(), sizeof(int), out3.size(), out);
+    std::fclose(out);
+    std::printf("{\"ientries\": %d, \"tiles\": %d, \"pairs\": %zu}\n", ne, nt, out3.size() / 3);
     return 0;
   }
   std::fprintf(stderr, "bad arguments\n");

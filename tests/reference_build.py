@@ -38,3 +38,25 @@ def md(paths, box, st, warmup, steps, seed=1, friction=1.0, timeout=1800):
         if line.startswith("{"):
             return json.loads(line)
     raise RuntimeError("reference harness printed no result: " + r.stdout[-2000:])
+
+
+def traj(paths, box, st, kind, steps, seed, friction, velocities, workdir, timeout=900):
+    """Runs `steps` steps of the reference's integrator `kind` from the CRD
+    coordinates and the given (N,3) velocities; returns (x FP64, x FP32, v)."""
+    vpath = os.path.join(workdir, f"v_{kind}.txt")
+    np.savetxt(vpath, np.asarray(velocities, np.float64).reshape(-1), fmt="%.17g")
+    out = os.path.join(workdir, f"traj_{kind}.txt")
+    cmd = [HARNESS, "traj", paths["psf"], paths["prm"], paths["crd"]] + settings_args(box, st) + \
+        [kind, str(steps), str(seed), str(friction), vpath, out]
+    subprocess.run(cmd, check=True, timeout=timeout, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)
+    a = np.loadtxt(out)
+    return a[:, 0:3], a[:, 3:6], a[:, 6:9]
+
+
+def nblist(paths, box, st, radius, workdir, timeout=900):
+    """The reference's tile-list pairs within `radius`: (i, j, excluded) rows."""
+    out = os.path.join(workdir, "ref_pairs.bin")
+    cmd = [HARNESS, "nblist", paths["psf"], paths["prm"], paths["crd"]] + settings_args(box, st) + \
+        [str(radius), out]
+    subprocess.run(cmd, check=True, timeout=timeout, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)
+    return np.fromfile(out, dtype=np.int32).reshape(-1, 3)

@@ -157,3 +157,23 @@ def test_restraint_handle_subscribes_only_matching_sizes_without_gpu(tmp_path):
     assert L.apo_force_manager_subscribe_harmonic_restraint(fm.handle, h.handle, b"harm") == 1
     h30 = api.HarmonicRestraintForce(30)
     assert L.apo_force_manager_subscribe_harmonic_restraint(fm.handle, h30.handle, b"") == 1
+
+
+def test_static_reciprocal_argument_checks_without_gpu():
+    """apo_pme_reciprocal_static validates its arguments before it touches a
+    device: a grid axis shorter than the spline order, an odd axis or an
+    unknown order is refused.  The pointers are never dereferenced."""
+    fn = _lib.lib().apo_pme_reciprocal_static
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                   ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                   ctypes.c_double, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                   ctypes.c_int, ctypes.c_void_p]
+    fake = ctypes.c_void_p(4096)
+    for nfft, order in (((4, 4, 4), 6), ((6, 6, 6), 8), ((2, 8, 8), 4), ((8, 8, 7), 4), ((8, 8, 8), 5)):
+        st = fn(fake, 8, 30.0, 30.0, 30.0, nfft[0], nfft[1], nfft[2], order, 0.34, fake, 8,
+                None, 0, None)
+        assert st == 1, (nfft, order)
+    msg = _lib.lib().apo_last_error()
+    msg = msg.decode() if isinstance(msg, bytes) else str(msg)
+    assert "order" in msg

@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 from apocharmm_b200 import api
-from apocharmm_b200.systems import config_small_water, solvated_chain, water_box
+from apocharmm_b200.systems import config_ethanol, config_small_water, solvated_chain, water_box
 
 pytestmark = pytest.mark.gpu
 
@@ -96,6 +96,116 @@ def test_nve_energy_is_conserved(tmp_path):
     drift = abs(series[-10:].mean() - series[:10].mean())
     assert drift < 0.01 * ke, (drift, series)
     assert series.std() < 0.01 * ke, series
+
+
+def test_leapfrog_conserves_energy(tmp_path):
+    """NVE with the leapfrog integrator (SETTLE on): total energy, with the
+    on-step kinetic energy taken as the mean of the two half-step values
+    around x(n), stays within 1 % of the kinetic energy over 400 steps."""
+    s = water_box(1000, 31.0, seed=3)
+    st = dict(kappa=0.34, nfft=(32, 32, 32), order=4, ctofnb=10.0, ctonnb=8.0, cutnb=12.0)
+    keep = api.system_context(s, str(tmp_path), settings=st)
+    ctx = keep[3]
+    api.relax(ctx, api.water_indices(s), iterations=100)
+    ctx.setRandomSeedForVelocities(27)
+    ctx.assignVelocitiesAtTemperature(300.0)
+    lf = api.CudaLeapFrogIntegrator(0.001)
+    lf.setCharmmContext(ctx)
+    m = s.mass[:, None]
+
+    def total():
+        pe = ctx.calculatePotentialEnergy(False)
+        k1 = 0.5 * (m * ctx.getVelocities() ** 2).sum()
+        lf.propagate(1)
+        k2 = 0.5 * (m * ctx.getVelocities() ** 2).sum()
+        return pe + 0.5 * (k1 + k2)
+
+    lf.propagate(40)
+    series = []
+    for _ in range(40):
+        series.append(total())
+        lf.propagate(9)
+    series = np.array(series)
+    ke = 0.5 * ctx.getDegreesOfFreedom() * 1.987191e-3 * 300.0
+    drift = abs(series[-10:].mean() - series[:10].mean())
+    print(f"leapfrog NVE: drift {drift:.3f} kcal/mol, std {series.std():.3f}, KE {ke:.1f}")
+    assert drift < 0.01 * ke, (drift, series)
+    assert series.std() < 0.01 * ke, series
+
+
+def test_shake_holds_x_h_bonds(tmp_path):
+    """SHAKE clusters of 2 (O-H), 3 (CH2) and 4 (CH3) atoms keep their bond
+    lengths through 200 Langevin steps; SETTLE keeps the waters rigid."""
+    s = config_ethanol()
+    keep = api.system_context(s, str(tmp_path))
+    ctx = keep[3]
+    api.relax(ctx, api.water_indices(s), iterations=150, max_step=0.02)
+    ctx.setRandomSeedForVelocities(8)
+    ctx.assignVelocitiesAtTemperature(300.0)
+    it = api.CudaLangevinThermostatIntegrator(0.002)
+    it.setThermostatFriction(5.0)
+    it.setThermostatRngSeed(9)
+    it.setCharmmContext(ctx)
+    it.propagate(200)
+    x = ctx.getCoordinates()
+    box = np.asarray(s.box)
+
+    def dist(i, j):
+        d = x[i] - x[j]
+        return np.linalg.norm(d - box * np.round(d / box), axis=-1)
+    b0 = {("CT3", "HA"): 1.111, ("CT2", "HA"): 1.111, ("H", "OH1"): 0.96}
+    worst, count = 0.0, 0
+    for i, j in s.bonds:
+        key = tuple(sorted((s.atom_type[i], s.atom_type[j])))
+        if key in b0:
+            worst = max(worst, abs(dist(i, j) - b0[key]))
+            count += 1
+    print(f"{count} X-H bonds, largest deviation {worst:.2e} A")
+    assert count == 40 * 6
+    assert worst < 1e-5
+    w = api.water_indices(s)
+    assert np.abs(dist(w[:, 1], w[:, 0]) - 0.9572).max() < 1e-6
+
+
+def test_list_overflow_during_propagate_is_grown_and_replayed(tmp_path):
+    """A neighbour list that outgrows its buffers during propagate() freezes
+    the state at the start of that segment; the list is grown and the
+    segment run again, so the trajectory is bit for bit the one of a run
+    that never overflowed (the reference checks at report frequency,
+    src/CudaIntegrator.cu:357-369)."""
+    runs = []
+    for small in (False, True):
+        s, keep = _setup(tmp_path / f"o{int(small)}")
+        fm, ctx = keep[2], keep[3]
+        it = api.CudaLangevinThermostatIntegrator(0.002)
+        it.setThermostatFriction(1.0)
+        it.setThermostatRngSeed(5)
+        it.setCharmmContext(ctx)
+        it.propagate(20)
+        before = fm.getListCapacity()
+        if small:
+            fm.setListCapacity(64)      # far below the ~1e4 tiles this box needs
+        it.propagate(45)
+        assert it.getCurrentPropagatedStep() == 65
+        if small:
+            assert fm.getListCapacity() > 64
+        runs.append((ctx.getCoordinates(), ctx.getVelocities(), before))
+    assert np.array_equal(runs[0][0], runs[1][0])
+    assert np.array_equal(runs[0][1], runs[1][1])
+
+
+def test_non_finite_coordinates_are_refused(tmp_path):
+    """Non-finite coordinates never reach the device: setCoordinates refuses
+    them and the state is unchanged (inside propagate the list build flags
+    them and every step kernel then leaves the state alone)."""
+    s, keep = _setup(tmp_path)
+    ctx = keep[3]
+    x = ctx.getCoordinates()
+    bad = x.copy()
+    bad[7, 1] = np.nan
+    with pytest.raises(RuntimeError, match="non-finite"):
+        ctx.setCoordinates(bad)
+    assert np.array_equal(ctx.getCoordinates(), x)
 
 
 def test_langevin_thermostat_reaches_target(tmp_path):

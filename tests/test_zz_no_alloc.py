@@ -60,10 +60,16 @@ def test_static_reciprocal_matches_context(tmp_path, order, nfft, precise):
     for call in range(2):                # two calls in a row reuse the static area
         grad = torch.zeros(3 * stride, dtype=torch.int64, device="cuda")
         energy = torch.full((1,), float("nan"), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
         st = _static_call(torch, xyzq.data_ptr(), n, s.box, nfft, order, 0.34,
                           grad.data_ptr(), stride, energy.data_ptr(), precise)
         assert st == 0, lib().apo_last_error()
         torch.cuda.synchronize()
+        if call == 1:
+            # the first call may load the kernels' code onto the device; the
+            # second allocates nothing: the device's free memory is unchanged
+            assert torch.cuda.mem_get_info()[0] == free_before
         G = grad.view(3, stride)[:, :n].t().cpu().numpy().astype(np.float64) / FORCE_SCALE
         rel = np.sqrt(((G - G_ref) ** 2).sum() / (G_ref ** 2).sum())
         assert rel < FORCE_RTOL, (call, rel)
@@ -90,5 +96,9 @@ def test_static_reciprocal_rejects_oversize_and_bad_arguments():
                       grad.data_ptr(), 8, None, False)
     assert st == 1
     st = _static_call(torch, xyzq.data_ptr(), 8, (30.0, 30.0, 30.0), (24, 24, 24), 5, 0.34,
+                      grad.data_ptr(), 8, None, False)
+    assert st == 1
+    # a grid axis shorter than the spline order would wrap a spline twice
+    st = _static_call(torch, xyzq.data_ptr(), 8, (30.0, 30.0, 30.0), (4, 4, 4), 6, 0.34,
                       grad.data_ptr(), 8, None, False)
     assert st == 1
