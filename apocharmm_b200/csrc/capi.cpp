@@ -503,9 +503,68 @@ extern "C" apo_status apo_charmm_context_get_stream(void **stream, const apo_cha
   }, fn);
 }
 
+namespace {
+
+// Walks the pairs of the current tile list whose distance (FP64, from the
+// sorted cluster-local coordinates, the cluster origins and the tile's
+// image shift) is below `radius`: fn(atom i, atom j, image code, excluded).
+// Padding slots and the lower triangle of a cluster's tile with itself are
+// not pairs; `excluded` is the tile's topological exclusion bit.
+template <typename Fn>
+void for_each_list_pair(apo::CharmmContext &ctx, double radius, Fn fn) {
+  auto fm = ctx.getForceManager();
+  auto &nl = fm->neighborList();
+  cudaStream_t s = ctx.stream();
+  APO_CUDA(cudaStreamSynchronize(s));
+  int counts[8];
+  APO_CUDA(cudaMemcpy(counts, nl.counts, sizeof(counts), cudaMemcpyDeviceToHost));
+  const int S = counts[0], T = counts[1], W = counts[2];
+  const int M = std::min(counts[5], nl.dims().mask_cap);
+  std::vector<int> perm(S);
+  std::vector<float4> xs(S), origin((S + 31) / 32);
+  std::vector<int2> tiles(T);
+  std::vector<unsigned> masks((size_t)M * 32);
+  std::vector<int4> work(W);
+  if (S) {
+    APO_CUDA(cudaMemcpy(perm.data(), nl.perm, S * sizeof(int), cudaMemcpyDeviceToHost));
+    APO_CUDA(cudaMemcpy(xs.data(), nl.xyzq_s, S * sizeof(float4), cudaMemcpyDeviceToHost));
+    APO_CUDA(cudaMemcpy(origin.data(), nl.cl_origin, origin.size() * sizeof(float4),
+                        cudaMemcpyDeviceToHost));
+  }
+  if (T) APO_CUDA(cudaMemcpy(tiles.data(), nl.tiles, T * sizeof(int2), cudaMemcpyDeviceToHost));
+  if (M) APO_CUDA(cudaMemcpy(masks.data(), nl.masks, masks.size() * sizeof(unsigned), cudaMemcpyDeviceToHost));
+  if (W) APO_CUDA(cudaMemcpy(work.data(), nl.work, W * sizeof(int4), cudaMemcpyDeviceToHost));
+  auto box = fm->getBoxDimensions();
+  const double r2max = radius * radius;
+  for (auto &w : work) {
+    for (int t = w.y; t < w.z; ++t) {
+      const int jc = tiles[t].x, sc = apo::tile_image(tiles[t].y), mi = apo::tile_mask(tiles[t].y);
+      const bool self = jc == w.x && sc == 13;
+      const double sx = (sc % 3 - 1) * box[0], sy = ((sc / 3) % 3 - 1) * box[1],
+                   sz = (sc / 9 - 1) * box[2];
+      const float4 oi = origin[w.x], oj = origin[jc];
+      for (int i = 0; i < 32; ++i) {
+        const int si = w.x * 32 + i;
+        if (perm[si] < 0) continue;
+        const unsigned m = (mi >= 0 && mi < M) ? masks[(size_t)mi * 32 + i] : 0u;
+        for (int j = self ? i + 1 : 0; j < 32; ++j) {
+          const int sj = jc * 32 + j;
+          if (perm[sj] < 0) continue;
+          const double dx = ((double)xs[si].x + oi.x) - ((double)xs[sj].x + oj.x + sx),
+                       dy = ((double)xs[si].y + oi.y) - ((double)xs[sj].y + oj.y + sy),
+                       dz = ((double)xs[si].z + oi.z) - ((double)xs[sj].z + oj.z + sz);
+          if (dx * dx + dy * dy + dz * dz >= r2max) continue;
+          fn(perm[si], perm[sj], sc, ((m >> j) & 1u) != 0u);
+        }
+      }
+    }
+  }
+}
+
+}  // namespace
+
 // Every tile-list pair within `radius`, with its exclusion bit:
-// (atom i, atom j, excluded).  The self tile of a cluster holds each pair
-// twice (the mask drops j <= i); only its upper triangle is reported.
+// (atom i, atom j, excluded); each unordered pair once.
 extern "C" apo_status apo_charmm_context_get_list_pairs(int *pairs, const size_t len,
                                                         size_t *num_pairs, const double radius,
                                                         apo_charmm_context *c) {
@@ -514,60 +573,15 @@ extern "C" apo_status apo_charmm_context_get_list_pairs(int *pairs, const size_t
     APO_RETURN_IF(require_ptr(num_pairs, fn, "num_pairs"));
     APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
     if (!(radius > 0.0)) return invalid(fn, "radius must be positive");
-    auto fm = c->object->getForceManager();
-    auto &nl = fm->neighborList();
-    cudaStream_t s = c->object->stream();
-    APO_CUDA(cudaStreamSynchronize(s));
-    nl.sync_counts(s);
-    const int S = nl.h_counts[0], T = nl.h_counts[1];
-    std::vector<int> perm(S);
-    std::vector<float4> xs(S), origin((S + 31) / 32);
-    std::vector<int2> tiles(T);
-    std::vector<unsigned> masks((size_t)T * 32);
-    std::vector<int4> work(nl.h_counts[2]);
-    if (S) {
-      APO_CUDA(cudaMemcpy(perm.data(), nl.perm, S * sizeof(int), cudaMemcpyDeviceToHost));
-      APO_CUDA(cudaMemcpy(xs.data(), nl.xyzq_s, S * sizeof(float4), cudaMemcpyDeviceToHost));
-      APO_CUDA(cudaMemcpy(origin.data(), nl.cl_origin, origin.size() * sizeof(float4),
-                          cudaMemcpyDeviceToHost));
-    }
-    if (T) {
-      APO_CUDA(cudaMemcpy(tiles.data(), nl.tiles, T * sizeof(int2), cudaMemcpyDeviceToHost));
-      APO_CUDA(cudaMemcpy(masks.data(), nl.masks, masks.size() * sizeof(unsigned), cudaMemcpyDeviceToHost));
-    }
-    if (!work.empty())
-      APO_CUDA(cudaMemcpy(work.data(), nl.work, work.size() * sizeof(int4), cudaMemcpyDeviceToHost));
-    auto box = fm->getBoxDimensions();
-    const double r2max = radius * radius;
     size_t count = 0;
-    for (auto &w : work) {
-      for (int t = w.y; t < w.z; ++t) {
-        const int jc = tiles[t].x, sc = tiles[t].y;
-        const bool self = jc == w.x && sc == 13;
-        const double sx = (sc % 3 - 1) * box[0], sy = ((sc / 3) % 3 - 1) * box[1],
-                     sz = (sc / 9 - 1) * box[2];
-        const float4 oi = origin[w.x], oj = origin[jc];
-        for (int i = 0; i < 32; ++i) {
-          const int si = w.x * 32 + i;
-          if (perm[si] < 0) continue;
-          const unsigned m = masks[(size_t)t * 32 + i];
-          for (int j = self ? i + 1 : 0; j < 32; ++j) {
-            const int sj = jc * 32 + j;
-            if (perm[sj] < 0) continue;
-            const double dx = ((double)xs[si].x + oi.x) - ((double)xs[sj].x + oj.x + sx),
-                         dy = ((double)xs[si].y + oi.y) - ((double)xs[sj].y + oj.y + sy),
-                         dz = ((double)xs[si].z + oi.z) - ((double)xs[sj].z + oj.z + sz);
-            if (dx * dx + dy * dy + dz * dz >= r2max) continue;
-            if (pairs && 3 * (count + 1) <= len) {
-              pairs[3 * count] = perm[si];
-              pairs[3 * count + 1] = perm[sj];
-              pairs[3 * count + 2] = (int)((m >> j) & 1u);
-            }
-            ++count;
-          }
-        }
+    for_each_list_pair(*c->object, radius, [&](int i, int j, int, bool excluded) {
+      if (pairs && 3 * (count + 1) <= len) {
+        pairs[3 * count] = i;
+        pairs[3 * count + 1] = j;
+        pairs[3 * count + 2] = excluded ? 1 : 0;
       }
-    }
+      ++count;
+    });
     *num_pairs = count;
     if (pairs && 3 * count > len) return invalid(fn, "pair buffer too small");
     return APO_STATUS_OK;
@@ -582,59 +596,16 @@ extern "C" apo_status apo_charmm_context_get_neighbor_pairs(int *pairs, const si
   return guard([&]() -> apo_status {
     APO_RETURN_IF(require_ptr(num_pairs, fn, "num_pairs"));
     APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
-    auto fm = c->object->getForceManager();
-    auto &nl = fm->neighborList();
-    cudaStream_t s = c->object->stream();
-    APO_CUDA(cudaStreamSynchronize(s));
-    nl.sync_counts(s);
-    const int S = nl.h_counts[0], T = nl.h_counts[1];
-    std::vector<int> perm(S);
-    std::vector<float4> xs(S), origin((S + 31) / 32);
-    std::vector<int2> tiles(T);
-    std::vector<unsigned> masks((size_t)T * 32);
-    std::vector<int4> work(nl.h_counts[2]);
-    if (S) {
-      APO_CUDA(cudaMemcpy(perm.data(), nl.perm, S * sizeof(int), cudaMemcpyDeviceToHost));
-      APO_CUDA(cudaMemcpy(xs.data(), nl.xyzq_s, S * sizeof(float4), cudaMemcpyDeviceToHost));
-      APO_CUDA(cudaMemcpy(origin.data(), nl.cl_origin, origin.size() * sizeof(float4),
-                          cudaMemcpyDeviceToHost));
-    }
-    if (T) {
-      APO_CUDA(cudaMemcpy(tiles.data(), nl.tiles, T * sizeof(int2), cudaMemcpyDeviceToHost));
-      APO_CUDA(cudaMemcpy(masks.data(), nl.masks, masks.size() * sizeof(unsigned), cudaMemcpyDeviceToHost));
-    }
-    if (!work.empty())
-      APO_CUDA(cudaMemcpy(work.data(), nl.work, work.size() * sizeof(int4), cudaMemcpyDeviceToHost));
-    auto box = fm->getBoxDimensions();
-    const double r2max = radius * radius;
     size_t count = 0;
-    for (auto &w : work) {
-      for (int t = w.y; t < w.z; ++t) {
-        const int jc = tiles[t].x, sc = tiles[t].y;
-        const double sx = (sc % 3 - 1) * box[0], sy = ((sc / 3) % 3 - 1) * box[1],
-                     sz = (sc / 9 - 1) * box[2];
-        for (int i = 0; i < 32; ++i) {
-          const unsigned m = masks[(size_t)t * 32 + i];
-          const int si = w.x * 32 + i;
-          for (int j = 0; j < 32; ++j) {
-            if ((m >> j) & 1u) continue;
-            const int sj = jc * 32 + j;
-            // sorted coordinates are relative to their cluster's origin
-            const float4 oi = origin[w.x], oj = origin[jc];
-            const double dx = ((double)xs[si].x + oi.x) - ((double)xs[sj].x + oj.x + sx),
-                         dy = ((double)xs[si].y + oi.y) - ((double)xs[sj].y + oj.y + sy),
-                         dz = ((double)xs[si].z + oi.z) - ((double)xs[sj].z + oj.z + sz);
-            if (dx * dx + dy * dy + dz * dz >= r2max) continue;
-            if (pairs && 3 * (count + 1) <= len) {
-              pairs[3 * count] = perm[si];
-              pairs[3 * count + 1] = perm[sj];
-              pairs[3 * count + 2] = sc;
-            }
-            ++count;
-          }
-        }
+    for_each_list_pair(*c->object, radius, [&](int i, int j, int sc, bool excluded) {
+      if (excluded) return;
+      if (pairs && 3 * (count + 1) <= len) {
+        pairs[3 * count] = i;
+        pairs[3 * count + 1] = j;
+        pairs[3 * count + 2] = sc;
       }
-    }
+      ++count;
+    });
     *num_pairs = count;
     if (pairs && 3 * count > len) return invalid(fn, "pair buffer too small");
     return APO_STATUS_OK;

@@ -311,7 +311,8 @@ __global__ void tiles_kernel(const NbSysDims *__restrict__ sysd, const int *__re
                              int *__restrict__ tile_count, const int *__restrict__ tile_start,
                              const int *__restrict__ work_start, int2 *__restrict__ tiles,
                              unsigned *__restrict__ masks, int4 *__restrict__ work,
-                             const int *__restrict__ counts) {
+                             int *__restrict__ counts, int mask_cap,
+                             unsigned *__restrict__ err) {
   const int ic = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (ic >= counts[0] / kTile) return;
@@ -373,20 +374,26 @@ __global__ void tiles_kernel(const NbSysDims *__restrict__ sysd, const int *__re
             int tsc = __shfl_sync(0xffffffffu, sc, src);
             int t = base_tile + count;
             ++count;
-            int pj = perm[tjc * kTile + lane];
-            unsigned word = __ballot_sync(0xffffffffu, pj < 0);
-            if (gi < 0) {
-              word = 0xffffffffu;
-            } else {
-              if (tjc == ic && tsc == 13)
-                word |= (lane == 31) ? 0xffffffffu : ((2u << lane) - 1u);
+            // topological exclusions of i-lane `lane` against this j-cluster
+            unsigned word = 0u;
+            if (gi >= 0) {
               for (int e = nexcl_begin; e < nexcl_end; ++e) {
                 int lp = glo2loc[excl_idx[e]];
                 if ((lp >> 5) == tjc) word |= 1u << (lp & 31);
               }
             }
-            if (lane == 0) tiles[t] = make_int2(tjc, tsc);
-            masks[(size_t)t * kTile + lane] = word;
+            int midx = -1;
+            if (__any_sync(0xffffffffu, word != 0u)) {
+              if (lane == 0) midx = atomicAdd(&counts[5], 1);
+              midx = __shfl_sync(0xffffffffu, midx, 0);
+              if (midx < mask_cap) {
+                masks[(size_t)midx * kTile + lane] = word;
+              } else {  // more masked tiles than allocated: the build is void
+                if (lane == 0) atomicOr(err, (unsigned)kErrTileOverflow);
+                midx = -1;
+              }
+            }
+            if (lane == 0) tiles[t] = make_int2(tjc, tsc | ((midx + 1) << 5));
           }
         } else {
           count += __popc(hits);
@@ -437,6 +444,7 @@ __global__ void tile_scan_kernel(const int *__restrict__ tile_count, int *__rest
     }
     counts[1] = carry_t;
     counts[2] = carry_w;
+    counts[5] = 0;  // masked tiles, counted by the fill pass
   }
 }
 
@@ -542,6 +550,9 @@ void NeighborList::setup(const std::vector<NbListSystem> &systems,
   const int ncl = m_d.slot_cap / kTile;
   m_d.tile_cap = (int)std::min<double>(tiles, 2.0e9 / 128.0);
   m_d.work_cap = m_d.tile_cap / m_d.tiles_per_work + ncl + 16;
+  // masked tiles: a cluster's tile with itself and with its neighbours along
+  // the column usually hold its molecules' exclusions
+  m_d.mask_cap = 4 * ncl + 1024;
   if ((int)excl_ptr.size() != natom + 1)
     throw std::invalid_argument("NeighborList: exclusion pointer array must have natom + 1 entries");
   m_vdwtype = d_vdwtype;
@@ -582,7 +593,7 @@ void NeighborList::alloc() {
   APO_CUDA(cudaMemset(slot_off, 0, (size_t)S * sizeof(double4)));
   APO_CUDA(cudaMemset(cl_origin, 0, (size_t)ncl * sizeof(float4)));
   APO_CUDA(cudaMemset(cl_sys, 0, (size_t)ncl * sizeof(int)));
-  dalloc(type_s, S); dalloc(tiles, m_d.tile_cap); dalloc(masks, (size_t)m_d.tile_cap * kTile);
+  dalloc(type_s, S); dalloc(tiles, m_d.tile_cap); dalloc(masks, (size_t)m_d.mask_cap * kTile);
   dalloc(work, m_d.work_cap); dalloc(counts, 8); dalloc(error, 1);
   dalloc(m_col_count, m_d.ncol); dalloc(m_col_start, m_d.ncol + 1); dalloc(m_atom_col, n);
   dalloc(m_atom_rank, n); dalloc(m_atom_shift, n); dalloc(m_atom_z, n);
@@ -627,7 +638,7 @@ void NeighborList::build(const float4 *d_xyzq, cudaStream_t s) {
   tiles_kernel<false><<<(ncl * 32 + 127) / 128, 128, 0, s>>>(
       m_sys, cl_sys, m_d.tiles_per_work, m_cl_col, m_col_start, m_bb_c, m_bb_h, perm, glo2loc,
       m_excl_ptr, m_excl_idx, m_tile_count, m_tile_start, m_work_start, tiles, masks, work,
-      counts);
+      counts, m_d.mask_cap, error);
   APO_LAUNCH_CHECK();
   tile_scan_kernel<<<1, kScanThreads, 0, s>>>(m_tile_count, m_tile_start, m_work_start,
                                               counts, m_d.tile_cap, m_d.work_cap,
@@ -636,7 +647,7 @@ void NeighborList::build(const float4 *d_xyzq, cudaStream_t s) {
   tiles_kernel<true><<<(ncl * 32 + 127) / 128, 128, 0, s>>>(
       m_sys, cl_sys, m_d.tiles_per_work, m_cl_col, m_col_start, m_bb_c, m_bb_h, perm, glo2loc,
       m_excl_ptr, m_excl_idx, m_tile_count, m_tile_start, m_work_start, tiles, masks, work,
-      counts);
+      counts, m_d.mask_cap, error);
   APO_LAUNCH_CHECK();
 }
 
@@ -652,7 +663,6 @@ void NeighborList::set_capacity(int tile_cap, int work_cap) {
   m_d.tile_cap = tile_cap;
   m_d.work_cap = work_cap;
   dalloc(tiles, m_d.tile_cap);
-  dalloc(masks, (size_t)m_d.tile_cap * kTile);
   dalloc(work, m_d.work_cap);
 }
 
@@ -685,12 +695,19 @@ bool NeighborList::ensure_capacity(const float4 *d_xyzq, cudaStream_t s, double 
   if (e & (kErrColumnOverflow | kErrNaN))
     throw std::runtime_error("neighbour list: column overflow or non-finite coordinates");
   bool grew = false;
-  if (c[3] > fill * m_d.tile_cap || c[4] > fill * m_d.work_cap) {
-    m_d.tile_cap = (int)(std::max<double>(c[3], 1) / fill * 1.25) + 1024;
-    m_d.work_cap = (int)(std::max<double>(c[4], 1) / fill * 1.25) + 1024;
-    dalloc(tiles, m_d.tile_cap);
-    dalloc(masks, (size_t)m_d.tile_cap * kTile);
-    dalloc(work, m_d.work_cap);
+  const bool tiles_short = c[3] > fill * m_d.tile_cap || c[4] > fill * m_d.work_cap;
+  const bool masks_short = c[5] > fill * m_d.mask_cap;
+  if (tiles_short || masks_short) {
+    if (tiles_short) {
+      m_d.tile_cap = (int)(std::max<double>(c[3], 1) / fill * 1.25) + 1024;
+      m_d.work_cap = (int)(std::max<double>(c[4], 1) / fill * 1.25) + 1024;
+      dalloc(tiles, m_d.tile_cap);
+      dalloc(work, m_d.work_cap);
+    }
+    if (masks_short) {
+      m_d.mask_cap = (int)(std::max<double>(c[5], 1) / fill * 1.25) + 1024;
+      dalloc(masks, (size_t)m_d.mask_cap * kTile);
+    }
     APO_CUDA(cudaMemsetAsync(error, 0, sizeof(unsigned), s));
     build(d_xyzq, s);
     APO_CUDA(cudaStreamSynchronize(s));

@@ -7,9 +7,11 @@
 //    can sit inside a CUDA graph;
 //  * the atom order inside a column is fully determined by (z, atom index),
 //    so the sorted order, the tile list and the masks are deterministic;
-//  * a tile carries its own periodic image code and its own mask word per
-//    i-lane: bit j of word i set = pair (i, j) is skipped (padding, the lower
-//    triangle of a self tile, or a topological 1-2/1-3/1-4 exclusion).
+//  * a tile carries its own periodic image code and, only when one of its
+//    pairs is a topological 1-2/1-3/1-4 exclusion, the index of its mask (32
+//    words, bit j of word i set = pair (i, j) excluded) in a compact mask
+//    array; padding slots and the lower triangle of a cluster's tile with
+//    itself are skipped by the kernels, so most tiles need no mask.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -40,9 +42,18 @@ struct NbListDims {
   int ncol = 0;                   // all systems
   int slot_cap = 0;               // padded sorted slots
   int tile_cap = 0, work_cap = 0;
+  int mask_cap = 0;               // tiles with an exclusion mask
   int tiles_per_work = 8;
   int sort_cap = 4096;            // max atoms in one column
 };
+
+// A tile's image code and mask index, packed in its second int.
+__host__ __device__ inline int tile_image(int packed) { return packed & 31; }
+__host__ __device__ inline int tile_mask(int packed) { return (packed >> 5) - 1; }  // -1: none
+// the pairs a cluster's tile with itself skips: j <= i, as a mask word of lane i
+__host__ __device__ inline unsigned self_tile_word(int i) {
+  return i == 31 ? 0xffffffffu : ((2u << i) - 1u);
+}
 
 struct NbListSystem {
   int natom;
@@ -95,11 +106,12 @@ class NeighborList {
   float4 *cl_origin = nullptr;  // per cluster
   float4 *xyzq_s = nullptr;     // sorted, cluster-local coordinates + charge
   int *type_s = nullptr;        // sorted LJ type
-  int2 *tiles = nullptr;        // (j cluster, image code)
-  unsigned *masks = nullptr;    // 32 words per tile
+  int2 *tiles = nullptr;        // (j cluster, image code | (mask index + 1) << 5)
+  unsigned *masks = nullptr;    // 32 words per masked tile
   int4 *work = nullptr;         // (i cluster, first tile, end tile, system)
   int *counts = nullptr;        // [0] slots, [1] tiles, [2] work items, [3..4] scan
-                                // carries, [6..7] direct-space schedule counters
+                                // carries, [5] masked tiles, [6..7] direct-space
+                                // schedule counters
   unsigned *error = nullptr;    // DeviceError bits
   int *cl_sys = nullptr;        // cluster -> system
   int *sys_of_atom = nullptr;   // atom -> system

@@ -15,6 +15,7 @@
 #include <type_traits>
 
 #include "device_util.cuh"
+#include "nblist.h"
 
 namespace apo {
 
@@ -86,10 +87,13 @@ __device__ __forceinline__ T transpose_reduce8(T (&v)[8], int lane) {
   return z;
 }
 
-// erfc(x) = exp(-x^2) t P(t), t = 1/(1 + p x): Hastings' form with
-// coefficients fitted for relative accuracy on 0 <= x <= 6 (max relative
-// error 1.3e-7 in single precision; fit_erfc.py in this directory).  The
-// exponential is the one the Ewald force needs anyway.
+// erfc(x) = exp(-x^2) t P(t), t = 1/(1 + p x): the form of Hastings'
+// approximation (Abramowitz & Stegun 7.1.26) with p = 0.365 and the nine
+// coefficients of P refitted here by linear least squares on the relative
+// error of erfc over 0 <= x <= 6 (the range kappa r takes inside the
+// cutoff); max relative error 1.3e-8 in FP64, 1.3e-7 with the coefficients
+// rounded to single precision.  The exponential is the one the Ewald force
+// needs anyway.
 __device__ __forceinline__ float rcp_approx(float v) {
   float r;
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(v));
@@ -121,6 +125,17 @@ __device__ __forceinline__ void warp_flush(double v, long long *dst, int lane) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) iv += __shfl_xor_sync(0xffffffffu, iv, o);
   if (lane == 0 && iv) add_fixed(dst, iv);
+}
+
+// The pairs of i-lane `lane` that a tile skips, as a bit per j-lane: its
+// topological exclusions (only tiles that hold one carry a mask) and, for a
+// cluster's tile with itself, the pairs j <= i.
+__device__ __forceinline__ unsigned tile_excl_word(const NbArgs &a, int2 tl, int code, int icl,
+                                                   int lane) {
+  const int midx = tile_mask(tl.y);
+  unsigned w = midx >= 0 ? a.masks[(size_t)midx * kTile + lane] : 0u;
+  if (tl.x == icl && code == 13) w |= self_tile_word(lane);
+  return w;
 }
 
 // Work items are handed out one at a time from a counter, so warps that
@@ -241,12 +256,13 @@ __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
 
     for (int t = wk.y; t < wk.z; ++t) {
       const int2 tl = a.tiles[t];
+      const int code = tile_image(tl.y);
       // j cluster frame -> i cluster frame: origin difference (exact: both
       // origins are multiples of 1/64 A) plus the periodic image k L with L
       // as a two-float sum, so |offset| < rlist + 2 cluster edges carries
       // about one rounding
       const float4 oj = a.origin[tl.x];
-      const int ic = tl.y / 9, ib = (tl.y - 9 * ic) / 3, ia = tl.y - 9 * ic - 3 * ib;
+      const int ic = code / 9, ib = (code - 9 * ic) / 3, ia = code - 9 * ic - 3 * ib;
       const float kx = (float)(ia - 1), ky = (float)(ib - 1), kz = (float)(ic - 1);
       const float sx = fmaf(kx, st.Lx, oj.x - oi.x) + kx * st.Lx_lo;
       const float sy = fmaf(ky, st.Ly, oj.y - oi.y) + ky * st.Ly_lo;
@@ -263,7 +279,7 @@ __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
       const bool jnear = a.perm[jslot] >= 0 && bx * bx + by * by + bz * bz < st.roff2;
       const unsigned jmask = __ballot_sync(0xffffffffu, jnear);
       if (jmask == 0u) continue;
-      const unsigned excl = a.masks[(size_t)t * kTile + lane];
+      const unsigned excl = tile_excl_word(a, tl, code, wk.x, lane);
       const int nj = __popc(jmask);
       const int tj_own = a.type_s[jslot] | (lane << 16);
       __syncwarp();
@@ -289,7 +305,7 @@ __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
             const int tj = sh_tj[wib][r];
             const float dx = xi.x - pj.x, dy = xi.y - pj.y, dz = xi.z - pj.z;
             const float r2raw = dx * dx + dy * dy + dz * dz;
-            const bool in = !((excl >> (tj >> 16)) & 1u) && r2raw < st.roff2;
+            const bool in = ivalid && !((excl >> (tj >> 16)) & 1u) && r2raw < st.roff2;
             const float2 cc = sh_vdw[tab_off + ti + (tj & 0xffff)];
             const float fij = pair_force<ENERGY>(st, r2raw, in, qi, pj.w, cc, e_elec, e_vdw);
             if (VIRIAL) {
@@ -641,8 +657,9 @@ __global__ void __launch_bounds__(kThreads, 5) nbq_kernel(NbArgs a) {
       }
       if (t >= wk.z) break;
       const int2 tl = a.tiles[t];
+      const int code = tile_image(tl.y);
       const float4 oj = a.origin[tl.x];
-      const int ic = tl.y / 9, ib = (tl.y - 9 * ic) / 3, ia = tl.y - 9 * ic - 3 * ib;
+      const int ic = code / 9, ib = (code - 9 * ic) / 3, ia = code - 9 * ic - 3 * ib;
       const float kx = (float)(ia - 1), ky = (float)(ib - 1), kz = (float)(ic - 1);
       const float sx = fmaf(kx, st.Lx, oj.x - oi.x) + kx * st.Lx_lo;
       const float sy = fmaf(ky, st.Ly, oj.y - oi.y) + ky * st.Ly_lo;
@@ -654,7 +671,7 @@ __global__ void __launch_bounds__(kThreads, 5) nbq_kernel(NbArgs a) {
       xj.z += sz;
       const bool jvalid = a.perm[jslot] >= 0;
       const int tj = a.type_s[jslot];
-      const unsigned excl = a.masks[(size_t)t * kTile + lane];
+      const unsigned excl = tile_excl_word(a, tl, code, wk.x, lane);
       const bool any_excl = __any_sync(0xffffffffu, ivalid && excl != 0u);
 #pragma unroll
       for (int h = 0; h < 4; ++h) {

@@ -20,8 +20,8 @@ before every timed iteration, outside the timed interval.
          coordinates and velocities from pinned host memory, propagates the
          segment and reads coordinates and velocities back
   roofline  direct-space kernel (FP32 pipe): 65 FLOP per in-cutoff pair over
-         its CUDA-event time, against the FP32 FMA peak measured on the same
-         GPU in the same run
+         its CUDA-event time, against the FP32 FMA peak of the GPU at the SM
+         clock sampled during the timed region (SMs x 128 lanes x 2 x clock)
   cpu_baseline  the FP64 CPU oracle (all host threads) on a bounded sample
 
 --impl reference runs the reference engine's own build (oracle/_ref, compiled
@@ -32,7 +32,8 @@ steps.  The FP64 host oracle is timed beside it as the CPU baseline.  Without
 that build (or without a GPU) the arm times the FP64 host oracle alone.
 With torchrun (N>1) every rank of this arm but rank 0 exits at once; the
 b200 arm runs one replica of the system per rank (replicas only: the path
-has no collective).
+has no collective).  `--gpus N` with N > 1 outside torchrun starts itself
+under torchrun with N ranks; inside torchrun, N must equal WORLD_SIZE.
 """
 from __future__ import annotations
 
@@ -56,7 +57,8 @@ FLOP_PER_PAIR = 65
 # dram__bytes_write.sum) from one ncu capture of the same kernel on the same
 # workload (the inputs and the fixed-point force buffer stay in L2)
 NB_TRAFFIC = {
-    "chain23k": (7423488, "ncu --set full capture, profiles/nb_kernel_chain23k.md"),
+    "chain23k": (7423488, "ncu capture of this kernel on this workload "
+                          "(dram__bytes_read.sum + dram__bytes_write.sum)"),
 }
 
 
@@ -142,6 +144,28 @@ def replica_seed(rank: int) -> int:
     return 2024 + rank
 
 
+def bench_config(spec: dict, atoms: int) -> dict:
+    """The `config` of a bench line: the same keys and values in both arms."""
+    return {"workload": spec["desc"], "atoms": atoms, "md_steps_per_iteration": SEG,
+            "dt_fs": DT_PS * 1e3}
+
+
+def fp32_peak_tflops(sm_mhz: float, n_sm: int) -> float:
+    """FP32 FMA peak: every SM issues 128 FMA lanes (2 FLOP) per clock."""
+    return n_sm * 128 * 2 * sm_mhz * 1e6 / 1e12
+
+
+def relaunch_under_torchrun(n: int, argv) -> int:
+    """Runs this script again under torchrun with one rank per GPU."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr=127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + list(argv)
+    return subprocess.run(cmd).returncode
+
+
 WORKLOADS = {
     "chain23k": dict(factory="config_solvated_chain", integrator="langevin", friction=1.0,
                      desc="chain23k: 23,558-atom bead chain in TIP3P, 62.23 A box, PME 64^3 "
@@ -215,6 +239,14 @@ def _reference_build_run(args, s, spec, work):
     return json.loads([ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1])
 
 
+def _gpu_visible() -> bool:
+    try:
+        return subprocess.run(["nvidia-smi", "-L"], stdout=subprocess.DEVNULL,
+                              stderr=subprocess.DEVNULL).returncode == 0
+    except OSError:
+        return False
+
+
 def run_reference_arm(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -226,8 +258,7 @@ def run_reference_arm(args):
     reason = None
     if not os.path.exists(harness):
         reason = "reference build (oracle/_ref) not present"
-    elif subprocess.run(["nvidia-smi", "-L"], stdout=subprocess.DEVNULL,
-                        stderr=subprocess.DEVNULL).returncode != 0:
+    elif not _gpu_visible():
         reason = "no GPU visible"
     else:
         ref = _reference_build_run(args, s, spec, tempfile.mkdtemp(prefix="apo_ref_"))
@@ -236,8 +267,7 @@ def run_reference_arm(args):
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "data": "synthetic (seeded generator)",
-            "config": {"workload": spec["desc"], "atoms": s.n_atoms,
-                       "md_steps_per_iteration": SEG}}
+            "config": bench_config(spec, s.n_atoms)}
     if ref is not None:
         line.update({
             "value": ref["ns_per_day"], "ms_per_step": 1e3 * ref["seconds"] / args.steps,
@@ -593,6 +623,13 @@ def main():
                     help="direct-space kernel form: 0 tile batches, 1 grouped queues")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    if "WORLD_SIZE" in os.environ:
+        if int(os.environ["WORLD_SIZE"]) != args.gpus:
+            print(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={os.environ['WORLD_SIZE']}",
+                  file=sys.stderr)
+            return 2
+    elif args.gpus > 1:
+        return relaunch_under_torchrun(args.gpus, sys.argv[1:])
     if args.workload == "serve":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no "
@@ -719,8 +756,9 @@ def main():
                        "coordinates+velocities down; bytes given per MD step"}
 
     if rank == 0:
-        peak = api.ctypes.c_double()
-        api.call("apo_diag_fp32_peak_tflops", api.ctypes.byref(peak))
+        clk = clocks.summary()
+        n_sm = torch.cuda.get_device_properties(local).multi_processor_count
+        peak = fp32_peak_tflops(clk["sm_mhz"] or 1965.0, n_sm)
         avg_nb_s = (nb_ms / max(1, nb_launch)) * 1e-3
         pairs_avg = 0.5 * (n_pairs_cut + n_pairs_end)
         achieved = pairs_avg * FLOP_PER_PAIR / avg_nb_s / 1e12 if avg_nb_s > 0 else None
@@ -734,27 +772,27 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 (forces), f64 (integration)", "data": "synthetic (seeded generator)",
-            "config": {"workload": spec["desc"],
-                       "atoms": s.n_atoms, "md_steps_per_iteration": SEG,
-                       "form": "precision" if args.precise else "plain",
+            "config": bench_config(spec, s.n_atoms),
+            "engine": {"form": "precision" if args.precise else "plain",
                        "direct_kernel": ["tile batches", "grouped queues"][args.direct_kernel],
                        "tiles_per_work": args.tiles_per_work,
-                       "items_per_warp": args.items_per_warp,
-                       "l2": "flushed (256 MB device write) before every timed iteration, "
-                             "outside the timed interval",
-                       "parallelism": f"replicas x{world}"},
+                       "items_per_warp": args.items_per_warp},
+            "l2": "flushed (256 MB device write) before every timed iteration, outside the "
+                  "timed interval",
+            "parallelism": f"replicas x{world}",
             "md_steps_timed": md_steps,
             "neighbor_list": list_counts,
             "force_rel_rms_vs_fp64": force_err,
             "roofline": {"kernel": "direct-space tile kernel", "bound": "fp32",
-                         "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
-                         "frac": (achieved / peak.value) if achieved else None,
+                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": (achieved / peak) if achieved else None,
                          "traffic": NB_TRAFFIC.get(args.workload, (None, None))[0],
                          "traffic_source": NB_TRAFFIC.get(args.workload, (None, None))[1],
                          "work": f"{FLOP_PER_PAIR} FLOP x {pairs_avg:.0f} in-cutoff pairs per launch",
                          "launch_ms": avg_nb_s * 1e3, "launches_timed": nb_launch,
-                         "peak_source": "FP32 FMA probe measured on this GPU in this run"},
-            "clocks": clocks.summary(),
+                         "peak_source": f"{n_sm} SMs x 128 FP32 lanes x 2 FLOP x the median SM "
+                                        f"clock sampled in the timed region ({clk['sm_mhz']} MHz)"},
+            "clocks": clk,
             "e2e": e2e,
             "gpu_launches": launches,
             "cpu_baseline": cb,

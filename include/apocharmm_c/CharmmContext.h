@@ -65,9 +65,6 @@ APOCHARMM_C_API apo_status apo_charmm_context_get_list_pairs(int *pairs, const s
  * number of launches recorded since the last integration segment began */
 APOCHARMM_C_API apo_status apo_charmm_context_set_kernel_timing(apo_charmm_context *context, const int on);
 APOCHARMM_C_API apo_status apo_charmm_context_get_kernel_time(double *ms, int *launches, apo_charmm_context *context);
-/* measured FP32 FMA throughput of the current device in TFLOP/s (a short
- * probe kernel), the denominator of the direct-space roofline */
-APOCHARMM_C_API apo_status apo_diag_fp32_peak_tflops(double *tflops);
 /* sizes of the current neighbour list: sorted slots, tiles, work items */
 APOCHARMM_C_API apo_status apo_charmm_context_get_list_counts(int *slots, int *tiles, int *work_items, apo_charmm_context *context);
 /* CUDA stream the context's work is issued on (a cudaStream_t), for timing */

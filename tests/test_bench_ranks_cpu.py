@@ -69,3 +69,32 @@ def test_reference_arm_runs_on_rank_zero_only(monkeypatch):
     monkeypatch.setattr(bench, "cpu_baseline", no_work)
     args = types.SimpleNamespace(workload="chain23k", gpus=2, steps=1, warmup=3)
     assert bench.run_reference_arm(args) == 0
+
+
+def test_gpus_flag_relaunches_under_torchrun():
+    """`bench.py --gpus 2` outside torchrun starts itself under torchrun with
+    two ranks; the reference arm then runs on rank 0 alone (here, without a
+    GPU, it times the FP64 host restatement) and prints one line."""
+    env = dict(os.environ)
+    for k in ("RANK", "WORLD_SIZE", "LOCAL_RANK", "MASTER_ADDR", "MASTER_PORT"):
+        env.pop(k, None)
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                        "--gpus", "2", "--steps", "1", "--warmup", "3", "--workload", "water12k"],
+                       env=env, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, r.stdout
+    import json
+    line = json.loads(lines[0])
+    assert line["impl"] == "reference" and line["n_gpus"] == 2
+    assert line["config"] == bench.bench_config(bench.WORKLOADS["water12k"], 12480)
+
+
+def test_gpus_flag_must_match_world_size():
+    env = dict(os.environ, RANK="0", WORLD_SIZE="2", LOCAL_RANK="0")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--gpus", "1"],
+                       env=env, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True,
+                       timeout=120)
+    assert r.returncode == 2
+    assert "WORLD_SIZE" in r.stderr
