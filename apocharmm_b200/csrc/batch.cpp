@@ -144,7 +144,7 @@ int Batch::autotune(int steps, const std::vector<int> &candidates) {
   APO_CUDA(cudaEventCreate(&e1));
   float best = 1e30f;
   int best_t = m_Tpw, best_f = m_Form;
-  for (int form : {kNbTileBatches, kNbGroupedQueues})
+  for (int form : {kNbTileBatches, kNbGroupedQueues, kNbOctetLists})
     for (int t : candidates) {
       if (t < 1) continue;
       m_Form = form;

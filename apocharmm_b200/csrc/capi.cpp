@@ -249,7 +249,7 @@ FM_SETTER(apo_force_manager_set_precision_mode, int, setPrecisionMode(v != 0), t
 FM_SETTER(apo_force_manager_set_tiles_per_work, int, setTilesPerWork(v), v >= 1 && v <= 1024)
 FM_SETTER(apo_force_manager_set_work_items_per_warp, int, setWorkItemsPerWarp(v), v >= 0 && v <= 1 << 20)
 FM_SETTER(apo_force_manager_set_component_mask, int, setComponentMask(v), v >= 0 && v <= 7)
-FM_SETTER(apo_force_manager_set_direct_kernel, int, setDirectKernel(v), v == 0 || v == 1)
+FM_SETTER(apo_force_manager_set_direct_kernel, int, setDirectKernel(v), v >= 0 && v <= 2)
 FM_SETTER(apo_force_manager_set_list_capacity, int, setListCapacity(v), v >= 1)
 
 extern "C" apo_status apo_force_manager_get_list_capacity(int *tiles, const apo_force_manager *fm) {

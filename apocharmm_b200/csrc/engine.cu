@@ -141,9 +141,9 @@ void ForceManager::setFFTGrid(int nx, int ny, int nz) {
 }
 
 void ForceManager::setDirectKernel(int v) {
-  if (v != kNbTileBatches && v != kNbGroupedQueues)
-    throw std::invalid_argument("direct-space kernel form must be 0 (tile batches) or 1 "
-                                "(grouped queues)");
+  if (v != kNbTileBatches && v != kNbGroupedQueues && v != kNbOctetLists)
+    throw std::invalid_argument("direct-space kernel form must be 0 (tile batches), 1 "
+                                "(grouped queues) or 2 (octet lists)");
   m_NbVariant = v;
 }
 

@@ -62,6 +62,7 @@ struct NbArgs {
 // queue per 8-atom i-group carried across tiles
 constexpr int kNbTileBatches = 0;
 constexpr int kNbGroupedQueues = 1;
+constexpr int kNbOctetLists = 2;
 
 // per_pair: round every pair contribution to 64-bit fixed point before it is
 // summed (order-independent, the reference's accumulation,
@@ -74,5 +75,9 @@ void launch_nonbonded(const NbArgs &a, bool energy, bool per_pair, cudaStream_t 
 // every work item's system from its .w, with per-system LJ tables
 void launch_nonbonded_multi(const NbArgs &a, bool energy, bool per_pair, cudaStream_t s,
                             bool virial = false);
+
+// the octet-list form (nonbonded_lists.cu)
+void launch_nonbonded_octets(const NbArgs &a, bool energy, bool per_pair, bool virial, bool multi,
+                             cudaStream_t s);
 
 }  // namespace apo

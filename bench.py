@@ -619,8 +619,8 @@ def main():
     ap.add_argument("--items-per-warp", type=int, default=None,
                     help="direct-space work items per warp before it retires (0: persistent "
                          "grid; default: the library's)")
-    ap.add_argument("--direct-kernel", type=int, default=0, choices=[0, 1],
-                    help="direct-space kernel form: 0 tile batches, 1 grouped queues")
+    ap.add_argument("--direct-kernel", type=int, default=0, choices=[0, 1, 2],
+                    help="direct-space kernel form: 0 tile batches, 1 grouped queues, 2 octet lists")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if "WORLD_SIZE" in os.environ:
@@ -774,7 +774,7 @@ def main():
             "dtype": "f32 (forces), f64 (integration)", "data": "synthetic (seeded generator)",
             "config": bench_config(spec, s.n_atoms),
             "engine": {"form": "precision" if args.precise else "plain",
-                       "direct_kernel": ["tile batches", "grouped queues"][args.direct_kernel],
+                       "direct_kernel": ["tile batches", "grouped queues", "octet lists"][args.direct_kernel],
                        "tiles_per_work": args.tiles_per_work,
                        "items_per_warp": args.items_per_warp},
             "l2": "flushed (256 MB device write) before every timed iteration, outside the "

@@ -105,15 +105,17 @@ def test_forces_are_deterministic(tmp_path):
     assert e1 == e2
 
 
-def test_direct_space_schedule_does_not_change_results(tmp_path):
+@pytest.mark.parametrize("form", [0, 2])
+def test_direct_space_schedule_does_not_change_results(tmp_path, form):
     """Work items are handed out dynamically; with a persistent grid or with
     1, 2 or 4 items per warp, forces, energies and the virial are the same
     bit for bit (every item's forces and energies are rounded to fixed
-    point on their own)."""
+    point on their own), for the tile-batch and the octet-list forms."""
     s = config_solvated_chain()
     out = {}
     for k in (0, 1, 2, 4):
         psf, prm, fm, ctx = api.system_context(s, str(tmp_path / f"k{k}"), items_per_warp=k)
+        fm.setDirectKernel(form)
         ctx.calculateForces(False, True, True)
         out[k] = (ctx.getForces(), ctx.getEnergyComponents(), ctx.getVirial())
         # a second evaluation on the same context: the counters were reset
@@ -145,20 +147,22 @@ def test_small_golden_cases(tmp_path, name):
 
 @pytest.mark.parametrize("precise", [False, True])
 def test_direct_kernel_forms_agree(tmp_path, precise):
-    """Both direct-space kernel forms (tile batches, grouped queues) against
-    the FP64 oracle and against each other on the solvated chain."""
+    """The three direct-space kernel forms (tile batches, grouped queues,
+    octet lists) against the FP64 oracle and against each other on the
+    solvated chain."""
     s = config_solvated_chain()
     psf, prm, fm, ctx = api.system_context(s, str(tmp_path), precise=precise)
     fm.setComponentMask(2)
     Eo, Go = oracle_for(s).evaluate(pos=ctx.getCoordinates(), parts=("direct",))
     out = {}
-    for form in (0, 1):
+    for form in (0, 1, 2):
         fm.setDirectKernel(form)
         ctx.calculateForces(False, True, False)
         F, E = ctx.getForces(), ctx.getEnergyComponents()
         assert rel_rms(F, Go) < FORCE_RTOL, form
         assert E["elec"] + E["vdw"] == pytest.approx(Eo["elec"] + Eo["vdw"], rel=ENERGY_RTOL)
         out[form] = (F, E)
-    assert rel_rms(out[0][0], out[1][0]) < 2e-6
-    if precise:   # per-pair fixed point: the same pairs give the same sums in any order
-        assert np.array_equal(out[0][0], out[1][0])
+    for form in (1, 2):
+        assert rel_rms(out[0][0], out[form][0]) < 2e-6, form
+        if precise:   # per-pair fixed point: the same pairs give the same sums in any order
+            assert np.array_equal(out[0][0], out[form][0]), form
