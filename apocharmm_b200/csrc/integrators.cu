@@ -409,32 +409,65 @@ __global__ void __launch_bounds__(kThreads) nh_half_kernel(Common c, double ke_r
     int at[4];
     const int m = group_atoms(c, g, at);
     const int2 meta = c.gmeta[g];
+    // every load of the group first (each level of the chain atom -> slot ->
+    // gradient for all atoms at once), then the arithmetic, then the stores:
+    // at a million atoms the kernel is bound by memory latency
+    double4 x[4], vm[4], dp[4];
+    int slot[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (k < m) {
+        const int a = at[k];
+        x[k] = c.coords[a];
+        vm[k] = c.vel[a];
+        dp[k] = c.dprev[a];
+        slot[k] = c.glo2loc[a];
+      }
+    }
+    long long gi[4][3];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (k < m) {
+        gi[k][0] = c.force[slot[k]];
+        gi[k][1] = c.force[c.stride + slot[k]];
+        gi[k][2] = c.force[2 * c.stride + slot[k]];
+      }
+    }
     d3 o[4], n[4], n0[4];
-    for (int k = 0; k < m; ++k) {
-      const int a = at[k];
-      o[k] = xyz(c.coords[a]);
-      c.ref[a] = c.coords[a];
-      const d3 gr = take_grad(c.force, c.stride, c.glo2loc[a]);
-      n[k] = o[k] + (xyz(c.dprev[a]) - (dt2 * c.vel[a].w) * gr);
-      n0[k] = n[k];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (k < m) {  // the slots are cleared for the next force evaluation
+        c.force[slot[k]] = 0;
+        c.force[c.stride + slot[k]] = 0;
+        c.force[2 * c.stride + slot[k]] = 0;
+        const d3 gr = mk((double)gi[k][0] * kInvForceScale, (double)gi[k][1] * kInvForceScale,
+                         (double)gi[k][2] * kInvForceScale);
+        o[k] = xyz(x[k]);
+        n[k] = o[k] + (xyz(dp[k]) - (dt2 * vm[k].w) * gr);
+        n0[k] = n[k];
+      }
     }
     apply_constraint(meta.x, m, o, n, c.sk, c.shake_p, meta.y);
-    for (int k = 0; k < m; ++k) {
-      const int a = at[k];
-      const d3 d = n[k] - o[k];
-      c.delta[a] = make_double4(d.x, d.y, d.z, 0.0);
-      c.dpred[a] = c.delta[a];
-      c.coords[a] = make_double4(n[k].x, n[k].y, n[k].z, c.coords[a].w);
-      const double mass = 1.0 / c.vel[a].w;
-      // the on-step velocity of the first predictor-corrector pass carries
-      // the constraint's displacement over dt, as the reference's constraint
-      // pass adds it to the velocities (src/CudaHolonomicConstraint.cu:94-106,
-      // src/CudaNoseHooverIntegrator.cu:905-930)
-      const d3 v = xyz(c.vel[a]) + idt * (n[k] - n0[k]);
-      const d3 u1 = idt * xyz(c.dprev[a]), u2 = idt * d;
-      const double kon = 0.5 * mass * dot(v, v);
-      ke0 += (0.5 * mass * dot(u1, u1) + kon + 0.5 * mass * dot(u2, u2)) / 3.0;
-      ke1 += kon;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (k < m) {
+        const int a = at[k];
+        const d3 d = n[k] - o[k];
+        c.ref[a] = x[k];
+        c.delta[a] = make_double4(d.x, d.y, d.z, 0.0);
+        c.dpred[a] = make_double4(d.x, d.y, d.z, 0.0);
+        c.coords[a] = make_double4(n[k].x, n[k].y, n[k].z, x[k].w);
+        const double mass = 1.0 / vm[k].w;
+        // the on-step velocity of the first predictor-corrector pass carries
+        // the constraint's displacement over dt, as the reference's constraint
+        // pass adds it to the velocities (src/CudaHolonomicConstraint.cu:94-106,
+        // src/CudaNoseHooverIntegrator.cu:905-930)
+        const d3 v = xyz(vm[k]) + idt * (n[k] - n0[k]);
+        const d3 u1 = idt * xyz(dp[k]), u2 = idt * d;
+        const double kon = 0.5 * mass * dot(v, v);
+        ke0 += (0.5 * mass * dot(u1, u1) + kon + 0.5 * mass * dot(u2, u2)) / 3.0;
+        ke1 += kon;
+      }
     }
   }
   block_partials(ke0, ke1, c.partials);
@@ -497,25 +530,46 @@ __global__ void __launch_bounds__(kThreads) nh_final_kernel(Common c, double ke_
     int at[4];
     const int m = group_atoms(c, g, at);
     const int2 meta = c.gmeta[g];
-    d3 o[4], n[4];
-    for (int k = 0; k < m; ++k) {
-      o[k] = xyz(c.ref[at[k]]);
-      n[k] = xyz(c.coords[at[k]]);
+    // loads first (as nh_half_kernel), then the constraint, then the stores
+    d3 o[4], n[4], dp[4];
+    double q[4], im[4];
+    int slot[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (k < m) {
+        const int a = at[k];
+        o[k] = xyz(c.ref[a]);
+        const double4 x = c.coords[a];
+        n[k] = xyz(x);
+        q[k] = x.w;
+        dp[k] = xyz(c.dprev[a]);
+        im[k] = c.vel[a].w;
+        slot[k] = c.glo2loc[a];
+      }
     }
+    double4 so[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (k < m) so[k] = c.slot_off[slot[k]];
     apply_constraint(meta.x, m, o, n, c.sk, c.shake_p, meta.y);
-    for (int k = 0; k < m; ++k) {
-      const int a = at[k];
-      const d3 d = n[k] - o[k];
-      const d3 dp = xyz(c.dprev[a]);
-      const d3 v = fact * (d + dp);
-      const double mass = 1.0 / c.vel[a].w;
-      const d3 u1 = idt * dp, u2 = idt * d;
-      const double kon = 0.5 * mass * dot(v, v);
-      ke0 += (0.5 * mass * dot(u1, u1) + kon + 0.5 * mass * dot(u2, u2)) / 3.0;
-      ke1 += kon;
-      c.vel[a] = make_double4(v.x, v.y, v.z, c.vel[a].w);
-      c.dprev[a] = make_double4(d.x, d.y, d.z, 0.0);
-      store_position(a, n[k], c.coords, c.xyzq, c.glo2loc, c.slot_off, c.xyzq_s);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (k < m) {
+        const int a = at[k];
+        const d3 d = n[k] - o[k];
+        const d3 v = fact * (d + dp[k]);
+        const double mass = 1.0 / im[k];
+        const d3 u1 = idt * dp[k], u2 = idt * d;
+        const double kon = 0.5 * mass * dot(v, v);
+        ke0 += (0.5 * mass * dot(u1, u1) + kon + 0.5 * mass * dot(u2, u2)) / 3.0;
+        ke1 += kon;
+        c.vel[a] = make_double4(v.x, v.y, v.z, im[k]);
+        c.dprev[a] = make_double4(d.x, d.y, d.z, 0.0);
+        c.coords[a] = make_double4(n[k].x, n[k].y, n[k].z, q[k]);
+        c.xyzq[a] = make_float4((float)n[k].x, (float)n[k].y, (float)n[k].z, (float)q[k]);
+        c.xyzq_s[slot[k]] = make_float4((float)(n[k].x + so[k].x), (float)(n[k].y + so[k].y),
+                                        (float)(n[k].z + so[k].z), (float)q[k]);
+      }
     }
   }
   block_partials(ke0, ke1, c.partials);

@@ -115,7 +115,8 @@ __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
     const float4 xi = a.xyzq_s[islot];
     const bool ivalid = a.perm[islot] >= 0;
     const float qi = xi.w * (float)kCcelec;
-    const int ti = a.type_s[islot] * T;
+    // this lane's row of the LJ table
+    const float2 *vrow = sh_vdw + tab_off + a.type_s[islot] * T;
     // box around the current positions of the i-cluster
     float lo_x = ivalid ? xi.x : INFINITY, lo_y = ivalid ? xi.y : INFINITY,
           lo_z = ivalid ? xi.z : INFINITY;
@@ -185,7 +186,7 @@ __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
             const float dx = xi.x - pj.x, dy = xi.y - pj.y, dz = xi.z - pj.z;
             const float r2raw = dx * dx + dy * dy + dz * dz;
             const bool in = ivalid && !((excl >> (tj >> 16)) & 1u) && r2raw < st.roff2;
-            const float2 cc = sh_vdw[tab_off + ti + (tj & 0xffff)];
+            const float2 cc = vrow[tj & 0xffff];
             const float fij = pair_force<ENERGY>(st, r2raw, in, qi, pj.w, cc, e_elec, e_vdw);
             if (VIRIAL) {
               const float gx = fij * dx, gy = fij * dy, gz = fij * dz;

@@ -51,6 +51,11 @@ __device__ __forceinline__ float rcp_approx(float v) {
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(v));
   return r;
 }
+__device__ __forceinline__ float rsqrt_approx(float v) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(v));
+  return r;
+}
 __device__ __forceinline__ float ex2_approx(float v) {
   float r;
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(v));
@@ -114,7 +119,7 @@ template <bool ENERGY>
 __device__ __forceinline__ float pair_force(const NbSetup &st, float r2raw, bool in, float qi,
                                             float qj, float2 cc, double &e_el, double &e_vdw) {
   const float r2 = in ? r2raw : 1.f;
-  const float rinv = rsqrtf(r2);
+  const float rinv = rsqrt_approx(r2);  // r2 >= 1e-2 inside the cutoff: never denormal
   const float rr = r2 * rinv;
   const float rinv2 = rinv * rinv;
   const float qq = qi * qj;

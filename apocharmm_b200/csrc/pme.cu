@@ -17,6 +17,9 @@ namespace apo {
 namespace {
 
 constexpr int kPlaneThreads = 512;
+// dynamic shared memory a plane transform may use: the SM's 227 KB per
+// block less the kernels' static digit-reversal table
+constexpr size_t kPlaneSmemMax = 227 * 1024 - 1024;
 constexpr int kPencilThreads = 256;
 constexpr int kPencilTX = 16;
 
@@ -156,14 +159,14 @@ __device__ __forceinline__ float2 twiddle(const float2 *tw, int idx, float sign)
 
 // One decimation-in-frequency stage (butterfly, then twiddle) on sub-blocks
 // of length m of every line.  Lines start at buf + line*lstride; element e of
-// a line is at e*estride.
+// a line is at e*estride.  The twiddle index j k n/m stays below n.
 template <int R>
 __device__ void dif_stage(float2 *buf, int nlines, int lstride, int estride, int n, int m,
-                          const float2 *tw, float sign) {
+                          FastDiv fpl, FastDiv fmr, const float2 *tw, float sign) {
   const int mr = m / R, per_line = n / R, total = nlines * per_line, nm = n / m;
   for (int b = threadIdx.x; b < total; b += blockDim.x) {
-    const int line = b / per_line, rem = b - line * per_line;
-    const int blk = rem / mr, j = rem - blk * mr;
+    const int line = (int)fdiv((unsigned)b, fpl), rem = b - line * per_line;
+    const int blk = (int)fdiv((unsigned)rem, fmr), j = rem - blk * mr;
     float2 *p = buf + line * lstride + (blk * m + j) * estride;
     float2 x[R];
 #pragma unroll
@@ -171,7 +174,7 @@ __device__ void dif_stage(float2 *buf, int nlines, int lstride, int estride, int
     dft<R>(x, sign);
     if (j > 0) {
 #pragma unroll
-      for (int k = 1; k < R; ++k) x[k] = cmul(x[k], twiddle(tw, (j * k * nm) % n, sign));
+      for (int k = 1; k < R; ++k) x[k] = cmul(x[k], twiddle(tw, j * k * nm, sign));
     }
 #pragma unroll
     for (int k = 0; k < R; ++k) p[k * mr * estride] = x[k];
@@ -181,18 +184,18 @@ __device__ void dif_stage(float2 *buf, int nlines, int lstride, int estride, int
 // One decimation-in-time stage (twiddle, then butterfly).
 template <int R>
 __device__ void dit_stage(float2 *buf, int nlines, int lstride, int estride, int n, int m,
-                          const float2 *tw, float sign) {
+                          FastDiv fpl, FastDiv fmr, const float2 *tw, float sign) {
   const int mr = m / R, per_line = n / R, total = nlines * per_line, nm = n / m;
   for (int b = threadIdx.x; b < total; b += blockDim.x) {
-    const int line = b / per_line, rem = b - line * per_line;
-    const int blk = rem / mr, j = rem - blk * mr;
+    const int line = (int)fdiv((unsigned)b, fpl), rem = b - line * per_line;
+    const int blk = (int)fdiv((unsigned)rem, fmr), j = rem - blk * mr;
     float2 *p = buf + line * lstride + (blk * m + j) * estride;
     float2 x[R];
 #pragma unroll
     for (int k = 0; k < R; ++k) x[k] = p[k * mr * estride];
     if (j > 0) {
 #pragma unroll
-      for (int k = 1; k < R; ++k) x[k] = cmul(x[k], twiddle(tw, (j * k * nm) % n, sign));
+      for (int k = 1; k < R; ++k) x[k] = cmul(x[k], twiddle(tw, j * k * nm, sign));
     }
     dft<R>(x, sign);
 #pragma unroll
@@ -202,15 +205,15 @@ __device__ void dit_stage(float2 *buf, int nlines, int lstride, int estride, int
 
 template <bool DIF>
 __device__ __forceinline__ void stage(int R, float2 *buf, int nl, int ls, int es, int n, int m,
-                                      const float2 *tw, float sign) {
+                                      FastDiv fpl, FastDiv fmr, const float2 *tw, float sign) {
   switch (R) {
-    case 2: DIF ? dif_stage<2>(buf, nl, ls, es, n, m, tw, sign) : dit_stage<2>(buf, nl, ls, es, n, m, tw, sign); break;
-    case 3: DIF ? dif_stage<3>(buf, nl, ls, es, n, m, tw, sign) : dit_stage<3>(buf, nl, ls, es, n, m, tw, sign); break;
-    case 4: DIF ? dif_stage<4>(buf, nl, ls, es, n, m, tw, sign) : dit_stage<4>(buf, nl, ls, es, n, m, tw, sign); break;
-    case 5: DIF ? dif_stage<5>(buf, nl, ls, es, n, m, tw, sign) : dit_stage<5>(buf, nl, ls, es, n, m, tw, sign); break;
-    case 6: DIF ? dif_stage<6>(buf, nl, ls, es, n, m, tw, sign) : dit_stage<6>(buf, nl, ls, es, n, m, tw, sign); break;
-    case 7: DIF ? dif_stage<7>(buf, nl, ls, es, n, m, tw, sign) : dit_stage<7>(buf, nl, ls, es, n, m, tw, sign); break;
-    case 8: DIF ? dif_stage<8>(buf, nl, ls, es, n, m, tw, sign) : dit_stage<8>(buf, nl, ls, es, n, m, tw, sign); break;
+    case 2: DIF ? dif_stage<2>(buf, nl, ls, es, n, m, fpl, fmr, tw, sign) : dit_stage<2>(buf, nl, ls, es, n, m, fpl, fmr, tw, sign); break;
+    case 3: DIF ? dif_stage<3>(buf, nl, ls, es, n, m, fpl, fmr, tw, sign) : dit_stage<3>(buf, nl, ls, es, n, m, fpl, fmr, tw, sign); break;
+    case 4: DIF ? dif_stage<4>(buf, nl, ls, es, n, m, fpl, fmr, tw, sign) : dit_stage<4>(buf, nl, ls, es, n, m, fpl, fmr, tw, sign); break;
+    case 5: DIF ? dif_stage<5>(buf, nl, ls, es, n, m, fpl, fmr, tw, sign) : dit_stage<5>(buf, nl, ls, es, n, m, fpl, fmr, tw, sign); break;
+    case 6: DIF ? dif_stage<6>(buf, nl, ls, es, n, m, fpl, fmr, tw, sign) : dit_stage<6>(buf, nl, ls, es, n, m, fpl, fmr, tw, sign); break;
+    case 7: DIF ? dif_stage<7>(buf, nl, ls, es, n, m, fpl, fmr, tw, sign) : dit_stage<7>(buf, nl, ls, es, n, m, fpl, fmr, tw, sign); break;
+    case 8: DIF ? dif_stage<8>(buf, nl, ls, es, n, m, fpl, fmr, tw, sign) : dit_stage<8>(buf, nl, ls, es, n, m, fpl, fmr, tw, sign); break;
     default: break;
   }
 }
@@ -220,7 +223,7 @@ __device__ void fft_dif(float2 *buf, int nl, int ls, int es, const FftAxis &a, c
                         float sign) {
   int m = a.n;
   for (int s = 0; s < a.nrad; ++s) {
-    stage<true>(a.radix[s], buf, nl, ls, es, a.n, m, tw, sign);
+    stage<true>(a.radix[s], buf, nl, ls, es, a.n, m, a.per_line[s], a.dif_mr[s], tw, sign);
     __syncthreads();
     m /= a.radix[s];
   }
@@ -231,10 +234,14 @@ __device__ void fft_dit(float2 *buf, int nl, int ls, int es, const FftAxis &a, c
   int m = 1;
   for (int s = a.nrad - 1; s >= 0; --s) {
     m *= a.radix[s];
-    stage<false>(a.radix[s], buf, nl, ls, es, a.n, m, tw, sign);
+    stage<false>(a.radix[s], buf, nl, ls, es, a.n, m, a.per_line[s], a.dit_mr[s], tw, sign);
     __syncthreads();
   }
 }
+
+// digit-reversal table of an axis (positions of fft_dif's output, or their
+// inverse) in shared memory, built by the whole block
+__device__ __forceinline__ void fill_rev_table(short *tab, const FftAxis &a, bool inverse);
 
 // natural index -> position in the output of fft_dif
 __device__ __forceinline__ int dig_rev(int x, const FftAxis &a) {
@@ -259,6 +266,11 @@ __device__ __forceinline__ int dig_unrev(int p, const FftAxis &a) {
     mult *= R;
   }
   return k;
+}
+
+__device__ __forceinline__ void fill_rev_table(short *tab, const FftAxis &a, bool inverse) {
+  for (int x = threadIdx.x; x < a.n; x += blockDim.x)
+    tab[x] = (short)(inverse ? dig_unrev(x, a) : dig_rev(x, a));
 }
 
 // ------------------------------------------------------------------------
@@ -328,7 +340,10 @@ __global__ void __launch_bounds__(128) spread_kernel(const float4 *__restrict__ 
 // ------------------------------------------------------------------------
 // plane transforms
 // ------------------------------------------------------------------------
-__global__ void __launch_bounds__(kPlaneThreads) plane_fwd_kernel(PmeDims d, int *__restrict__ qgrid,
+// The grid dimensions are read through a pointer (to the kernel parameter or
+// to the system's entry of the multi-system table), never copied: the FFT
+// stages index their per-stage divisors at run time.
+__global__ void __launch_bounds__(kPlaneThreads) plane_fwd_kernel(const __grid_constant__ PmeDims d0, int *__restrict__ qgrid,
                                                                   float2 *__restrict__ cgrid,
                                                                   const float2 *__restrict__ twx,
                                                                   const float2 *__restrict__ twy,
@@ -336,17 +351,22 @@ __global__ void __launch_bounds__(kPlaneThreads) plane_fwd_kernel(PmeDims d, int
                                                                   const int *__restrict__ plane_sys = nullptr) {
   extern __shared__ float2 buf[];
   int z = blockIdx.x;
+  const PmeDims *dp = &d0;
   if (multi) {
     const PmeSysArgs &A = multi[plane_sys[blockIdx.x]];
-    d = A.d;
+    dp = &A.d;
     qgrid = A.qgrid;
     cgrid = A.cgrid;
     twx = A.tw;
-    twy = A.tw + d.nx;
+    twy = A.tw + A.d.nx;
     z = blockIdx.x - A.plane0;
   }
+  const PmeDims &d = *dp;
+  __shared__ short s_rev[256];  // x -> position in the digit-reversed row
   const int nx = d.nx, ny = d.ny, nxc = d.nxc, rowp = nx + 2, h = nx / 2;
   int *plane = qgrid + (size_t)z * nx * ny;
+  fill_rev_table(s_rev, d.ax, false);
+  __syncthreads();
   // four loads in flight per thread before any store (latency-bound loop)
   const int total = nx * ny;
   for (int base = threadIdx.x; base < total; base += 4 * blockDim.x) {
@@ -361,8 +381,8 @@ __global__ void __launch_bounds__(kPlaneThreads) plane_fwd_kernel(PmeDims d, int
       const int idx = base + u * blockDim.x;
       if (idx < total) {
         plane[idx] = 0;  // ready for the next spread
-        const int y = idx / nx, x = idx - y * nx;
-        float *slot = reinterpret_cast<float *>(&buf[(y >> 1) * rowp + dig_rev(x, d.ax)]);
+        const int y = (int)fdiv((unsigned)idx, d.ax.by_n), x = idx - y * nx;
+        float *slot = reinterpret_cast<float *>(&buf[(y >> 1) * rowp + s_rev[x]]);
         slot[y & 1] = (float)v[u] * kInvGridScale;
       }
     }
@@ -372,7 +392,7 @@ __global__ void __launch_bounds__(kPlaneThreads) plane_fwd_kernel(PmeDims d, int
   // split the packed rows into the two half spectra, in place
   const int ngrp = (h + 1) / 2 + 1;
   for (int idx = threadIdx.x; idx < (ny / 2) * ngrp; idx += blockDim.x) {
-    const int r = idx / ngrp, g = idx - r * ngrp;
+    const int r = (int)fdiv((unsigned)idx, d.ax.by_ngrp), g = idx - r * ngrp;
     float2 *b = buf + r * rowp;
     if (g == ngrp - 1) {
       const float2 Z = b[h];
@@ -400,7 +420,7 @@ __global__ void __launch_bounds__(kPlaneThreads) plane_fwd_kernel(PmeDims d, int
   for (int idx = threadIdx.x; idx < ny * nxc; idx += blockDim.x) out[idx] = buf[idx];
 }
 
-__global__ void __launch_bounds__(kPlaneThreads) plane_inv_kernel(PmeDims d,
+__global__ void __launch_bounds__(kPlaneThreads) plane_inv_kernel(const __grid_constant__ PmeDims d0,
                                                                   const float2 *__restrict__ cgrid,
                                                                   float *__restrict__ phi,
                                                                   const float2 *__restrict__ twx,
@@ -409,24 +429,28 @@ __global__ void __launch_bounds__(kPlaneThreads) plane_inv_kernel(PmeDims d,
                                                                   const int *__restrict__ plane_sys = nullptr) {
   extern __shared__ float2 buf[];
   int z = blockIdx.x;
+  const PmeDims *dp = &d0;
   if (multi) {
     const PmeSysArgs &A = multi[plane_sys[blockIdx.x]];
-    d = A.d;
+    dp = &A.d;
     cgrid = A.cgrid;
     phi = A.phi;
     twx = A.tw;
-    twy = A.tw + d.nx;
+    twy = A.tw + A.d.nx;
     z = blockIdx.x - A.plane0;
   }
+  const PmeDims &d = *dp;
+  __shared__ short s_unrev[256];  // position in the digit-reversed row -> x
   const int nx = d.nx, ny = d.ny, nxc = d.nxc, rowp = nx + 2, h = nx / 2;
   const float2 *in = cgrid + (size_t)z * ny * nxc;
+  fill_rev_table(s_unrev, d.ax, true);
   for (int idx = threadIdx.x; idx < ny * nxc; idx += blockDim.x) buf[idx] = in[idx];
   __syncthreads();
   fft_dit(buf, nxc, 1, nxc, d.ay, twy, 1.f);
   // pack pairs of half spectra into one complex row, in place
   const int ngrp = (h + 1) / 2 + 1;
   for (int idx = threadIdx.x; idx < (ny / 2) * ngrp; idx += blockDim.x) {
-    const int r = idx / ngrp, g = idx - r * ngrp;
+    const int r = (int)fdiv((unsigned)idx, d.ax.by_ngrp), g = idx - r * ngrp;
     float2 *b = buf + r * rowp;
     if (g == ngrp - 1) {
       const float2 A = b[h], B = b[nxc + h];
@@ -446,8 +470,8 @@ __global__ void __launch_bounds__(kPlaneThreads) plane_inv_kernel(PmeDims d,
   fft_dif(buf, ny / 2, rowp, 1, d.ax, twx, 1.f);
   float *out = phi + (size_t)z * nx * ny;
   for (int idx = threadIdx.x; idx < (ny / 2) * nx; idx += blockDim.x) {
-    const int r = idx / nx, p = idx - r * nx;
-    const int x = dig_unrev(p, d.ax);
+    const int r = (int)fdiv((unsigned)idx, d.ax.by_n), p = idx - r * nx;
+    const int x = s_unrev[p];
     const float2 v = buf[r * rowp + p];
     out[(2 * r) * nx + x] = v.x;
     out[(2 * r + 1) * nx + x] = v.y;
@@ -458,7 +482,7 @@ __global__ void __launch_bounds__(kPlaneThreads) plane_inv_kernel(PmeDims d,
 // z pencils: FFT, influence function, inverse FFT
 // ------------------------------------------------------------------------
 template <bool ENERGY, typename FT, bool VIRIAL = false>
-__global__ void __launch_bounds__(kPencilThreads) pencil_kernel(PmeDims d, float2 *__restrict__ cgrid,
+__global__ void __launch_bounds__(kPencilThreads) pencil_kernel(const __grid_constant__ PmeDims d0, float2 *__restrict__ cgrid,
                                                                 const float2 *__restrict__ twz,
                                                                 const float *__restrict__ prefac,
                                                                 const double *__restrict__ prefac_d,
@@ -467,23 +491,27 @@ __global__ void __launch_bounds__(kPencilThreads) pencil_kernel(PmeDims d, float
                                                                 const PmeSysArgs *__restrict__ multi = nullptr,
                                                                 const int *__restrict__ pencil_sys = nullptr) {
   __shared__ float2 buf[256 * kPencilTX];
+  __shared__ short s_unrev_z[256];
   __shared__ double sh_e[kPencilThreads / 32];
   __shared__ double sh_v[6][kPencilThreads / 32];
   int blk = blockIdx.x;
+  const PmeDims *dp = &d0;
   if (multi) {
     const PmeSysArgs &A = multi[pencil_sys[blockIdx.x]];
-    d = A.d;
+    dp = &A.d;
     cgrid = A.cgrid;
-    twz = A.tw + d.nx + d.ny;
+    twz = A.tw + A.d.nx + A.d.ny;
     prefac = A.prefac;
     prefac_d = A.prefac_d;
     energy = A.energy;
     virial = A.virial;
     blk = blockIdx.x - A.pencil0;
   }
+  const PmeDims &d = *dp;
   const int nx = d.nx, ny = d.ny, nz = d.nz, nxc = d.nxc;
   const int tiles_x = (nxc + kPencilTX - 1) / kPencilTX;
   const int py = blk / tiles_x, x0 = (blk - py * tiles_x) * kPencilTX;
+  fill_rev_table(s_unrev_z, d.az, true);
   for (int idx = threadIdx.x; idx < nz * kPencilTX; idx += blockDim.x) {
     const int zz = idx / kPencilTX, xt = idx - zz * kPencilTX, kx = x0 + xt;
     buf[idx] = kx < nxc ? cgrid[((size_t)zz * ny + py) * nxc + kx] : make_float2(0.f, 0.f);
@@ -504,7 +532,7 @@ __global__ void __launch_bounds__(kPencilThreads) pencil_kernel(PmeDims d, float
   for (int idx = threadIdx.x; idx < nz * kPencilTX; idx += blockDim.x) {
     const int pz = idx / kPencilTX, xt = idx - pz * kPencilTX, kx = x0 + xt;
     if (kx >= nxc) continue;
-    const int kz = dig_unrev(pz, d.az);
+    const int kz = s_unrev_z[pz];
     FT eterm = 0;
     const FT m1 = (FT)(kx >= nf1 ? kx - nx : kx) / (FT)d.Lx;
     const FT m3 = (FT)(kz >= nf3 ? kz - nz : kz) / (FT)d.Lz;
@@ -683,6 +711,32 @@ void dalloc(T *&p, size_t n) {
 
 }  // namespace
 
+FastDiv make_fastdiv(unsigned d) {
+  FastDiv f{0u, 0u};
+  if (d <= 1) return f;
+  unsigned l = 0;  // ceil(log2 d)
+  while ((1u << l) < d) ++l;
+  f.mul = (unsigned)(((1ull << (31 + l)) + d - 1) / d);
+  f.shift = l - 1;
+  return f;
+}
+
+void fill_axis_divisors(FftAxis &a) {
+  int prod = 1;
+  for (int s = 0; s < a.nrad; ++s) {
+    prod *= a.radix[s];
+    a.per_line[s] = make_fastdiv((unsigned)(a.n / a.radix[s]));
+    a.dif_mr[s] = make_fastdiv((unsigned)(a.n / prod));
+  }
+  int tail = 1;
+  for (int s = a.nrad - 1; s >= 0; --s) {
+    a.dit_mr[s] = make_fastdiv((unsigned)tail);
+    tail *= a.radix[s];
+  }
+  a.by_n = make_fastdiv((unsigned)a.n);
+  a.by_ngrp = make_fastdiv((unsigned)((a.n / 2 + 1) / 2 + 1));
+}
+
 FftAxis Pme::plan_axis(int n) {
   // fewest stages, then smallest total radix
   std::vector<int> best;
@@ -712,6 +766,7 @@ FftAxis Pme::plan_axis(int n) {
   a.n = n;
   a.nrad = (int)best.size();
   for (size_t i = 0; i < best.size(); ++i) a.radix[i] = best[i];
+  fill_axis_divisors(a);
   return a;
 }
 
@@ -744,7 +799,7 @@ void Pme::setup(int nx, int ny, int nz, int order, double kappa, double Lx, doub
   if (nx < order || ny < order || nz < order)
     throw std::invalid_argument("PME grid dimensions must be at least the spline order");
   const size_t plane_bytes = (size_t)(ny / 2) * (nx + 2) * sizeof(float2);
-  if (plane_bytes > 227 * 1024)
+  if (plane_bytes > kPlaneSmemMax)
     throw std::invalid_argument("PME plane does not fit in shared memory");
   release();
   m_d.nx = nx;
@@ -788,9 +843,9 @@ void Pme::setup(int nx, int ny, int nz, int order, double kappa, double Lx, doub
   static bool attr = false;
   if (!attr) {
     APO_CUDA(cudaFuncSetAttribute(plane_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  227 * 1024));
+                                  kPlaneSmemMax));
     APO_CUDA(cudaFuncSetAttribute(plane_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  227 * 1024));
+                                  kPlaneSmemMax));
     attr = true;
   }
 }
@@ -913,7 +968,7 @@ void PmeMulti::setup(const std::vector<PmeSystemSpec> &systems, int order, long 
     if (y.nx < order || y.ny < order || y.nz < order)
       throw std::invalid_argument("PME grid dimensions must be at least the spline order");
     const size_t plane_bytes = (size_t)(y.ny / 2) * (y.nx + 2) * sizeof(float2);
-    if (plane_bytes > 227 * 1024) throw std::invalid_argument("PME plane does not fit in shared memory");
+    if (plane_bytes > kPlaneSmemMax) throw std::invalid_argument("PME plane does not fit in shared memory");
     m_plane_smem = std::max(m_plane_smem, plane_bytes);
     PmeSysArgs A{};
     A.d.nx = y.nx;
@@ -993,9 +1048,9 @@ void PmeMulti::setup(const std::vector<PmeSystemSpec> &systems, int order, long 
   APO_CUDA(cudaMemcpy(m_pencil_sys, pencil_sys.data(), pencil_sys.size() * sizeof(int),
                       cudaMemcpyHostToDevice));
   APO_CUDA(cudaFuncSetAttribute(plane_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                227 * 1024));
+                                kPlaneSmemMax));
   APO_CUDA(cudaFuncSetAttribute(plane_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                227 * 1024));
+                                kPlaneSmemMax));
 }
 
 void PmeMulti::compute(const float4 *xyzq_s, const float4 *origin, const int *cl_sys,
@@ -1126,6 +1181,7 @@ bool fixed_plan_axis(int n, FftAxis &a) {
   a.n = n;
   a.nrad = p.nbest;
   for (int i = 0; i < p.nbest; ++i) a.radix[i] = p.best[i];
+  fill_axis_divisors(a);
   return true;
 }
 
@@ -1187,9 +1243,9 @@ unsigned char *static_base() {
     void *p = nullptr;
     APO_CUDA(cudaGetSymbolAddress(&p, g_pme_static));
     APO_CUDA(cudaFuncSetAttribute(plane_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  227 * 1024));
+                                  kPlaneSmemMax));
     APO_CUDA(cudaFuncSetAttribute(plane_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  227 * 1024));
+                                  kPlaneSmemMax));
     b = static_cast<unsigned char *>(p);
     g_static_base[dev].store(b, std::memory_order_release);
   }
@@ -1217,7 +1273,7 @@ void pme_reciprocal_static(const float4 *xyzq, int n, double Lx, double Ly, doub
   if (nx < order || ny < order || nz < order)
     throw std::invalid_argument(
         "pme_reciprocal_static: grid dimensions must be at least the spline order");
-  if ((size_t)(ny / 2) * (nx + 2) * sizeof(float2) > 227 * 1024)
+  if ((size_t)(ny / 2) * (nx + 2) * sizeof(float2) > kPlaneSmemMax)
     throw std::invalid_argument("pme_reciprocal_static: grid plane does not fit in shared memory");
   const StaticLayout l = static_layout(nx, ny, nz);
   if (l.total > kPmeStaticScratchBytes)

@@ -29,11 +29,33 @@
 
 namespace apo {
 
+// x / d for 0 <= x < 2^31 as a multiply-high and a shift (division by an
+// invariant integer, Granlund & Montgomery 1994); mul == 0 means d == 1
+struct FastDiv {
+  unsigned mul, shift;
+};
+FastDiv make_fastdiv(unsigned d);
+__host__ __device__ inline unsigned fdiv(unsigned x, FastDiv f) {
+#ifdef __CUDA_ARCH__
+  return f.mul ? (__umulhi(x, f.mul) >> f.shift) : x;
+#else
+  return f.mul ? (unsigned)(((unsigned long long)x * f.mul >> 32) >> f.shift) : x;
+#endif
+}
+
 struct FftAxis {
   int n;
   int nrad;
   int radix[8];
+  // per stage s: n / radix[s], and the sub-block length over the radix of
+  // the decimation-in-frequency (n / radix[0..s]) and the decimation-in-time
+  // (radix[s+1..]) passes
+  FastDiv per_line[8], dif_mr[8], dit_mr[8];
+  FastDiv by_n;      // x / n
+  FastDiv by_ngrp;   // x / ((n/2 + 1)/2 + 1): the real-to-complex split groups
 };
+// fills the fast divisors of an axis whose n, nrad and radix are set
+void fill_axis_divisors(FftAxis &a);
 
 struct PmeDims {
   int nx, ny, nz, nxc, order;
