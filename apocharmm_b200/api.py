@@ -179,6 +179,12 @@ class ForceManager(_Handle):
     def setComponentMask(self, m: int): call("apo_force_manager_set_component_mask", self._h, _i(m))
     def setDirectKernel(self, form: int): call("apo_force_manager_set_direct_kernel", self._h, _i(form))
     def setListCapacity(self, tiles: int): call("apo_force_manager_set_list_capacity", self._h, _i(tiles))
+    def setPmeTensorCopies(self, on: bool): call("apo_force_manager_set_pme_tensor_copies", self._h, _i(int(on)))
+
+    def getPmeTensorCopies(self) -> bool:
+        v = _i()
+        call("apo_force_manager_get_pme_tensor_copies", ctypes.byref(v), self._h)
+        return bool(v.value)
 
     def getListCapacity(self) -> int:
         v = _i()

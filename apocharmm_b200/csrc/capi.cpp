@@ -251,6 +251,17 @@ FM_SETTER(apo_force_manager_set_work_items_per_warp, int, setWorkItemsPerWarp(v)
 FM_SETTER(apo_force_manager_set_component_mask, int, setComponentMask(v), v >= 0 && v <= 7)
 FM_SETTER(apo_force_manager_set_direct_kernel, int, setDirectKernel(v), v >= 0 && v <= 2)
 FM_SETTER(apo_force_manager_set_list_capacity, int, setListCapacity(v), v >= 1)
+FM_SETTER(apo_force_manager_set_pme_tensor_copies, int, setPmeTensorCopies(v != 0), v == 0 || v == 1)
+
+extern "C" apo_status apo_force_manager_get_pme_tensor_copies(int *on, const apo_force_manager *fm) {
+  const char *fn = "apo_force_manager_get_pme_tensor_copies";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_ptr(on, fn, "on"));
+    APO_RETURN_IF(require_handle(fm, fn, "ForceManager"));
+    *on = fm->object->getPmeTensorCopies() ? 1 : 0;
+    return APO_STATUS_OK;
+  }, fn);
+}
 
 extern "C" apo_status apo_force_manager_get_list_capacity(int *tiles, const apo_force_manager *fm) {
   const char *fn = "apo_force_manager_get_list_capacity";

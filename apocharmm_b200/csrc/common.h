@@ -45,6 +45,7 @@ enum DeviceError : unsigned {
   kErrColumnOverflow = 1u << 1,   // a cell column exceeded the sort capacity
   kErrWorkOverflow = 1u << 2,     // nonbonded work list larger than allocated
   kErrNaN = 1u << 3,              // non-finite coordinates
+  kErrCopyTimeout = 1u << 4,      // an asynchronous tensor copy did not complete in time
 };
 
 struct CudaError : public std::runtime_error {

@@ -211,6 +211,8 @@ void ForceManager::initialize() {
               m_Top.excl_ptr, m_Top.excl_idx, m_VdwTypeD.p, m_TilesPerWork);
   m_Pme.setup(m_Nfft[0], m_Nfft[1], m_Nfft[2], m_Order, m_Kappa, m_Box[0], m_Box[1], m_Box[2]);
   m_Pme.max_slots = m_Nbl.dims().slot_cap;
+  m_Pme.set_error_word(m_Nbl.error);
+  m_Pme.set_tensor_copies(m_PmeTensorCopies);
   m_Stride = m_Nbl.dims().slot_cap;
   m_Force.alloc((size_t)3 * m_Stride);
   APO_CUDA(cudaMemset(m_Force.p, 0, (size_t)3 * m_Stride * sizeof(long long)));
@@ -395,11 +397,19 @@ void ForceManager::setListCapacity(int tiles) {
   ++m_PluginGen;  // the captured graphs hold the old buffers
 }
 
+void ForceManager::setPmeTensorCopies(bool on) {
+  m_PmeTensorCopies = on;
+  m_Pme.set_tensor_copies(on);
+  ++m_PluginGen;  // captured graphs hold the other kernel form
+}
+
 void ForceManager::calcForceChecked(const float4 *d_xyzq, bool calcEnergy, bool calcVirial,
                                     cudaStream_t s) {
   calcForce(d_xyzq, calcEnergy, calcVirial, s, true);
   APO_CUDA(cudaStreamSynchronize(s));
   const unsigned e = readDeviceError(s);
+  if (e & kErrCopyTimeout)
+    throw std::runtime_error("a tensor copy of the reciprocal-space grid did not complete");
   if (e & (kErrTileOverflow | kErrWorkOverflow)) {
     growNeighborList(d_xyzq, s);
     calcForce(d_xyzq, calcEnergy, calcVirial, s, true);

@@ -138,6 +138,9 @@ class ForceManager {
   // coordinates with capacities that hold it, clear the error word (sync);
   // true when the buffers moved
   bool growNeighborList(const float4 *d_xyzq, cudaStream_t s);
+  // z-pencil slabs moved by tiled tensor copies (default) or by plain loads
+  void setPmeTensorCopies(bool on);
+  bool getPmeTensorCopies() const { return m_Pme.tensor_copies(); }
   // calcForce with clear = true, then a synchronisation; a list that
   // overflowed on the way is grown and the forces evaluated again
   void calcForceChecked(const float4 *d_xyzq, bool calcEnergy, bool calcVirial, cudaStream_t s);
@@ -219,6 +222,7 @@ class ForceManager {
   bool m_Initialized = false;
   bool m_ListBuilt = false;
   bool m_ListDirty = false;  // buffers replaced: rebuild before the next use
+  bool m_PmeTensorCopies = true;
   int m_TilesPerWork = 8;
   int m_ItemsPerWarp = 0;
   int m_NbVariant = kNbTileBatches;

@@ -1046,6 +1046,9 @@ void CudaIntegrator::propagate(int numSteps) {
     if (e & kErrNaN)
       throw std::runtime_error("non-finite coordinates during propagation (state kept at step " +
                                std::to_string(m_Step) + ")");
+    if (e & kErrCopyTimeout)
+      throw std::runtime_error("a tensor copy of the reciprocal-space grid did not complete "
+                               "(state kept at step " + std::to_string(m_Step) + ")");
     if (e & kErrColumnOverflow)
       throw std::runtime_error("neighbour list: a cell column outgrew the column sort during "
                                "propagation (state kept at step " + std::to_string(m_Step) + ")");

@@ -1,6 +1,8 @@
 // PME reciprocal-space kernels; see pme.h.
 #include "pme.h"
 
+#include <cuda.h>  // CUtensorMap (the encoder is fetched through the runtime)
+
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -20,6 +22,8 @@ constexpr int kPlaneThreads = 512;
 // dynamic shared memory a plane transform may use: the SM's 227 KB per
 // block less the kernels' static digit-reversal table
 constexpr size_t kPlaneSmemMax = 227 * 1024 - 1024;
+// the tensor-map argument of launches that move their slabs with plain loads
+const CUtensorMap kNoTensorMap{};
 constexpr int kPencilThreads = 256;
 constexpr int kPencilTX = 16;
 
@@ -274,6 +278,64 @@ __device__ __forceinline__ void fill_rev_table(short *tab, const FftAxis &a, boo
 }
 
 // ------------------------------------------------------------------------
+// tensor-memory-access (TMA) copies of pencil slabs: one thread issues a
+// tiled bulk copy between global memory and shared memory; the load's
+// completion is counted on an mbarrier (transaction bytes), waited for with
+// a bounded number of polls
+// ------------------------------------------------------------------------
+constexpr int kTmaPollLimit = 1 << 22;
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// true once the phase `parity` has completed; false after kTmaPollLimit polls
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity) {
+  for (int i = 0; i < kTmaPollLimit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z,
+                                            unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap *map, int x, int y, int z,
+                                             const void *src) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(
+          reinterpret_cast<unsigned long long>(map)),
+      "r"(x), "r"(y), "r"(z), "r"(smem_u32(src))
+      : "memory");
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+// shared-memory writes of this thread become visible to the async proxy
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// ------------------------------------------------------------------------
 // spread
 // ------------------------------------------------------------------------
 template <int ORDER>
@@ -363,7 +425,7 @@ __global__ void __launch_bounds__(kPlaneThreads) plane_fwd_kernel(const __grid_c
   }
   const PmeDims &d = *dp;
   __shared__ short s_rev[256];  // x -> position in the digit-reversed row
-  const int nx = d.nx, ny = d.ny, nxc = d.nxc, rowp = nx + 2, h = nx / 2;
+  const int nx = d.nx, ny = d.ny, nxc = d.nxc, nxcp = d.nxcp, rowp = nx + 2, h = nx / 2;
   int *plane = qgrid + (size_t)z * nx * ny;
   fill_rev_table(s_rev, d.ax, false);
   __syncthreads();
@@ -415,9 +477,14 @@ __global__ void __launch_bounds__(kPlaneThreads) plane_fwd_kernel(const __grid_c
     }
   }
   __syncthreads();
+  // the in-place split leaves row y at y*nxc (rowp = 2 nxc: row 2r+1 starts
+  // right after row 2r); in global memory rows have the even pitch nxcp
   fft_dif(buf, nxc, 1, nxc, d.ay, twy, -1.f);
-  float2 *out = cgrid + (size_t)z * ny * nxc;
-  for (int idx = threadIdx.x; idx < ny * nxc; idx += blockDim.x) out[idx] = buf[idx];
+  float2 *out = cgrid + (size_t)z * ny * nxcp;
+  for (int idx = threadIdx.x; idx < ny * nxcp; idx += blockDim.x) {
+    const int y = (int)fdiv((unsigned)idx, d.ax.by_nxcp), kx = idx - y * nxcp;
+    out[idx] = kx < nxc ? buf[y * nxc + kx] : make_float2(0.f, 0.f);
+  }
 }
 
 __global__ void __launch_bounds__(kPlaneThreads) plane_inv_kernel(const __grid_constant__ PmeDims d0,
@@ -441,10 +508,13 @@ __global__ void __launch_bounds__(kPlaneThreads) plane_inv_kernel(const __grid_c
   }
   const PmeDims &d = *dp;
   __shared__ short s_unrev[256];  // position in the digit-reversed row -> x
-  const int nx = d.nx, ny = d.ny, nxc = d.nxc, rowp = nx + 2, h = nx / 2;
-  const float2 *in = cgrid + (size_t)z * ny * nxc;
+  const int nx = d.nx, ny = d.ny, nxc = d.nxc, nxcp = d.nxcp, rowp = nx + 2, h = nx / 2;
+  const float2 *in = cgrid + (size_t)z * ny * nxcp;
   fill_rev_table(s_unrev, d.ax, true);
-  for (int idx = threadIdx.x; idx < ny * nxc; idx += blockDim.x) buf[idx] = in[idx];
+  for (int idx = threadIdx.x; idx < ny * nxc; idx += blockDim.x) {
+    const int y = (int)fdiv((unsigned)idx, d.ax.by_nxc), kx = idx - y * nxc;
+    buf[idx] = in[y * nxcp + kx];
+  }
   __syncthreads();
   fft_dit(buf, nxc, 1, nxc, d.ay, twy, 1.f);
   // pack pairs of half spectra into one complex row, in place
@@ -481,16 +551,21 @@ __global__ void __launch_bounds__(kPlaneThreads) plane_inv_kernel(const __grid_c
 // ------------------------------------------------------------------------
 // z pencils: FFT, influence function, inverse FFT
 // ------------------------------------------------------------------------
-template <bool ENERGY, typename FT, bool VIRIAL = false>
+template <bool ENERGY, typename FT, bool VIRIAL = false, bool TMA = false>
 __global__ void __launch_bounds__(kPencilThreads) pencil_kernel(const __grid_constant__ PmeDims d0, float2 *__restrict__ cgrid,
                                                                 const float2 *__restrict__ twz,
                                                                 const float *__restrict__ prefac,
                                                                 const double *__restrict__ prefac_d,
                                                                 long long *__restrict__ energy,
-                                                                long long *__restrict__ virial = nullptr,
-                                                                const PmeSysArgs *__restrict__ multi = nullptr,
-                                                                const int *__restrict__ pencil_sys = nullptr) {
-  __shared__ float2 buf[256 * kPencilTX];
+                                                                long long *__restrict__ virial,
+                                                                const PmeSysArgs *__restrict__ multi,
+                                                                const int *__restrict__ pencil_sys,
+                                                                const __grid_constant__ CUtensorMap tmap,
+                                                                unsigned *__restrict__ err) {
+  // TMA: the slab of 16 complex columns x nz arrives in (and leaves from)
+  // buf as one tiled copy of the padded complex grid
+  __shared__ __align__(128) float2 buf[256 * kPencilTX];
+  __shared__ __align__(8) unsigned long long s_bar;
   __shared__ short s_unrev_z[256];
   __shared__ double sh_e[kPencilThreads / 32];
   __shared__ double sh_v[6][kPencilThreads / 32];
@@ -511,10 +586,28 @@ __global__ void __launch_bounds__(kPencilThreads) pencil_kernel(const __grid_con
   const int nx = d.nx, ny = d.ny, nz = d.nz, nxc = d.nxc;
   const int tiles_x = (nxc + kPencilTX - 1) / kPencilTX;
   const int py = blk / tiles_x, x0 = (blk - py * tiles_x) * kPencilTX;
-  fill_rev_table(s_unrev_z, d.az, true);
-  for (int idx = threadIdx.x; idx < nz * kPencilTX; idx += blockDim.x) {
-    const int zz = idx / kPencilTX, xt = idx - zz * kPencilTX, kx = x0 + xt;
-    buf[idx] = kx < nxc ? cgrid[((size_t)zz * ny + py) * nxc + kx] : make_float2(0.f, 0.f);
+  if (TMA) {
+    if (threadIdx.x == 0) mbar_init(&s_bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      mbar_expect_tx(&s_bar, (unsigned)(nz * kPencilTX * sizeof(float2)));
+      tma_load_3d(buf, &tmap, 2 * x0, py, 0, &s_bar);
+    }
+    fill_rev_table(s_unrev_z, d.az, true);
+    if (!mbar_wait(&s_bar, 0u)) {
+      // the copy did not land: report it, give it a second bounded wait so
+      // no write into this block's shared memory is left in flight, and leave
+      // the slab untouched
+      if (threadIdx.x == 0) atomicOr(err, (unsigned)kErrCopyTimeout);
+      mbar_wait(&s_bar, 0u);
+      return;
+    }
+  } else {
+    fill_rev_table(s_unrev_z, d.az, true);
+    for (int idx = threadIdx.x; idx < nz * kPencilTX; idx += blockDim.x) {
+      const int zz = idx / kPencilTX, xt = idx - zz * kPencilTX, kx = x0 + xt;
+      buf[idx] = kx < nxc ? cgrid[((size_t)zz * ny + py) * d.nxcp + kx] : make_float2(0.f, 0.f);
+    }
   }
   __syncthreads();
   fft_dif(buf, kPencilTX, 1, kPencilTX, d.az, twz, -1.f);
@@ -559,9 +652,16 @@ __global__ void __launch_bounds__(kPencilThreads) pencil_kernel(const __grid_con
   }
   __syncthreads();
   fft_dit(buf, kPencilTX, 1, kPencilTX, d.az, twz, 1.f);
-  for (int idx = threadIdx.x; idx < nz * kPencilTX; idx += blockDim.x) {
-    const int zz = idx / kPencilTX, xt = idx - zz * kPencilTX, kx = x0 + xt;
-    if (kx < nxc) cgrid[((size_t)zz * ny + py) * nxc + kx] = buf[idx];
+  if (TMA) {
+    // columns past the grid's padded width are clipped by the copy
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0) tma_store_3d(&tmap, 2 * x0, py, 0, buf);
+  } else {
+    for (int idx = threadIdx.x; idx < nz * kPencilTX; idx += blockDim.x) {
+      const int zz = idx / kPencilTX, xt = idx - zz * kPencilTX, kx = x0 + xt;
+      if (kx < nxc) cgrid[((size_t)zz * ny + py) * d.nxcp + kx] = buf[idx];
+    }
   }
   if (ENERGY) {
     e = warp_sum(e);
@@ -711,6 +811,45 @@ void dalloc(T *&p, size_t n) {
 
 }  // namespace
 
+// The tensor map of the pencil slabs: the padded complex grid viewed as
+// floats [nz][ny][2 nxcp], a box of 16 complex columns x 1 row x nz planes.
+// The encoder is the driver's, fetched through the runtime (no link to the
+// driver library).
+bool encode_pencil_map(CUtensorMap *map, float2 *cgrid, const PmeDims &d) {
+  using Encode = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                              const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                              const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                              CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static Encode fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<Encode>(p);
+    else
+      cudaGetLastError();
+  }
+  // a row at least one box wide, at most 256 planes, rows of 16-byte multiples
+  if (!fn || d.nz > 256 || (d.nxcp & 1) || 2 * d.nxcp < 2 * kPencilTX) return false;
+  const cuuint64_t dims[3] = {2ull * d.nxcp, (cuuint64_t)d.ny, (cuuint64_t)d.nz};
+  const cuuint64_t strides[2] = {2ull * d.nxcp * sizeof(float),
+                                 2ull * d.nxcp * d.ny * sizeof(float)};
+  const cuuint32_t box[3] = {2u * kPencilTX, 1u, (cuuint32_t)d.nz};
+  const cuuint32_t es[3] = {1u, 1u, 1u};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, cgrid, dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// shared memory of one plane transform: ny/2 packed rows of nx + 2 complex
+static size_t plane_smem_bytes(int nx, int ny) {
+  return (size_t)(ny / 2) * (nx + 2) * sizeof(float2);
+}
+
 FastDiv make_fastdiv(unsigned d) {
   FastDiv f{0u, 0u};
   if (d <= 1) return f;
@@ -734,6 +873,8 @@ void fill_axis_divisors(FftAxis &a) {
     tail *= a.radix[s];
   }
   a.by_n = make_fastdiv((unsigned)a.n);
+  a.by_nxc = make_fastdiv((unsigned)(a.n / 2 + 1));
+  a.by_nxcp = make_fastdiv((unsigned)((a.n / 2 + 2) & ~1));
   a.by_ngrp = make_fastdiv((unsigned)((a.n / 2 + 1) / 2 + 1));
 }
 
@@ -798,7 +939,7 @@ void Pme::setup(int nx, int ny, int nz, int order, double kappa, double Lx, doub
   // a spline's p points wrap the grid at most once only when n >= p
   if (nx < order || ny < order || nz < order)
     throw std::invalid_argument("PME grid dimensions must be at least the spline order");
-  const size_t plane_bytes = (size_t)(ny / 2) * (nx + 2) * sizeof(float2);
+  const size_t plane_bytes = plane_smem_bytes(nx, ny);
   if (plane_bytes > kPlaneSmemMax)
     throw std::invalid_argument("PME plane does not fit in shared memory");
   release();
@@ -806,6 +947,7 @@ void Pme::setup(int nx, int ny, int nz, int order, double kappa, double Lx, doub
   m_d.ny = ny;
   m_d.nz = nz;
   m_d.nxc = nx / 2 + 1;
+  m_d.nxcp = (m_d.nxc + 1) & ~1;
   m_d.order = order;
   m_d.Lx = (float)Lx;
   m_d.Ly = (float)Ly;
@@ -819,7 +961,9 @@ void Pme::setup(int nx, int ny, int nz, int order, double kappa, double Lx, doub
   m_d.az = plan_axis(nz);
   const size_t G = (size_t)nx * ny * nz;
   dalloc(qgrid, G);
-  dalloc(cgrid, (size_t)nz * ny * m_d.nxc);
+  dalloc(cgrid, (size_t)nz * ny * m_d.nxcp);
+  APO_CUDA(cudaMemset(cgrid, 0, (size_t)nz * ny * m_d.nxcp * sizeof(float2)));
+  m_tma = encode_pencil_map(&m_tmap, cgrid, m_d);
   dalloc(phi, G);
   APO_CUDA(cudaMemset(qgrid, 0, G * sizeof(int)));
   std::vector<float2> tw;
@@ -862,7 +1006,7 @@ void Pme::spread(const float4 *xyzq_s, const int *counts, cudaStream_t s,
 }
 
 void Pme::forward(cudaStream_t s) {
-  const size_t sm = (size_t)(m_d.ny / 2) * (m_d.nx + 2) * sizeof(float2);
+  const size_t sm = plane_smem_bytes(m_d.nx, m_d.ny);
   plane_fwd_kernel<<<m_d.nz, kPlaneThreads, sm, s>>>(m_d, qgrid, cgrid, m_tw, m_tw + m_d.nx);
   APO_LAUNCH_CHECK();
 }
@@ -872,30 +1016,32 @@ void Pme::convolve(long long *energy, bool calc_energy, bool fp64, cudaStream_t 
   const int tiles_x = (m_d.nxc + kPencilTX - 1) / kPencilTX;
   const int grid = tiles_x * m_d.ny;
   const float2 *twz = m_tw + m_d.nx + m_d.ny;
+  const bool tma = tensor_copies() && m_err;
+#define APO_PENCIL(E, FT, V)                                                                   \
+  do {                                                                                         \
+    if (tma)                                                                                   \
+      pencil_kernel<E, FT, V, true><<<grid, kPencilThreads, 0, s>>>(                           \
+          m_d, cgrid, twz, m_prefac, m_prefac_d, energy, virial, nullptr, nullptr, m_tmap, m_err); \
+    else                                                                                       \
+      pencil_kernel<E, FT, V, false><<<grid, kPencilThreads, 0, s>>>(                          \
+          m_d, cgrid, twz, m_prefac, m_prefac_d, energy, virial, nullptr, nullptr, m_tmap, m_err); \
+  } while (0)
   if (virial) {
-    if (fp64)
-      pencil_kernel<true, double, true><<<grid, kPencilThreads, 0, s>>>(m_d, cgrid, twz, m_prefac, m_prefac_d, energy, virial);
-    else
-      pencil_kernel<true, float, true><<<grid, kPencilThreads, 0, s>>>(m_d, cgrid, twz, m_prefac, m_prefac_d, energy, virial);
-    APO_LAUNCH_CHECK();
-    return;
-  }
-  if (fp64) {
-    if (calc_energy)
-      pencil_kernel<true, double><<<grid, kPencilThreads, 0, s>>>(m_d, cgrid, twz, m_prefac, m_prefac_d, energy);
-    else
-      pencil_kernel<false, double><<<grid, kPencilThreads, 0, s>>>(m_d, cgrid, twz, m_prefac, m_prefac_d, energy);
+    if (fp64) APO_PENCIL(true, double, true);
+    else APO_PENCIL(true, float, true);
+  } else if (fp64) {
+    if (calc_energy) APO_PENCIL(true, double, false);
+    else APO_PENCIL(false, double, false);
   } else {
-    if (calc_energy)
-      pencil_kernel<true, float><<<grid, kPencilThreads, 0, s>>>(m_d, cgrid, twz, m_prefac, m_prefac_d, energy);
-    else
-      pencil_kernel<false, float><<<grid, kPencilThreads, 0, s>>>(m_d, cgrid, twz, m_prefac, m_prefac_d, energy);
+    if (calc_energy) APO_PENCIL(true, float, false);
+    else APO_PENCIL(false, float, false);
   }
+#undef APO_PENCIL
   APO_LAUNCH_CHECK();
 }
 
 void Pme::backward(cudaStream_t s) {
-  const size_t sm = (size_t)(m_d.ny / 2) * (m_d.nx + 2) * sizeof(float2);
+  const size_t sm = plane_smem_bytes(m_d.nx, m_d.ny);
   plane_inv_kernel<<<m_d.nz, kPlaneThreads, sm, s>>>(m_d, cgrid, phi, m_tw, m_tw + m_d.nx);
   APO_LAUNCH_CHECK();
 }
@@ -967,7 +1113,7 @@ void PmeMulti::setup(const std::vector<PmeSystemSpec> &systems, int order, long 
       throw std::invalid_argument("PME grid dimensions above 256 are not supported");
     if (y.nx < order || y.ny < order || y.nz < order)
       throw std::invalid_argument("PME grid dimensions must be at least the spline order");
-    const size_t plane_bytes = (size_t)(y.ny / 2) * (y.nx + 2) * sizeof(float2);
+    const size_t plane_bytes = plane_smem_bytes(y.nx, y.ny);
     if (plane_bytes > kPlaneSmemMax) throw std::invalid_argument("PME plane does not fit in shared memory");
     m_plane_smem = std::max(m_plane_smem, plane_bytes);
     PmeSysArgs A{};
@@ -975,6 +1121,7 @@ void PmeMulti::setup(const std::vector<PmeSystemSpec> &systems, int order, long 
     A.d.ny = y.ny;
     A.d.nz = y.nz;
     A.d.nxc = y.nx / 2 + 1;
+    A.d.nxcp = (A.d.nxc + 1) & ~1;
     A.d.order = order;
     A.d.Lx = (float)y.Lx;
     A.d.Ly = (float)y.Ly;
@@ -1003,7 +1150,7 @@ void PmeMulti::setup(const std::vector<PmeSystemSpec> &systems, int order, long 
     m_planes += y.nz;
     m_pencils += tiles_x * y.ny;
     q += (size_t)y.nx * y.ny * y.nz;
-    c += (size_t)y.nz * y.ny * A.d.nxc;
+    c += (size_t)y.nz * y.ny * A.d.nxcp;
     t += (size_t)y.nx + y.ny + y.nz;
     for (int n : {y.nx, y.ny, y.nz})
       for (int j = 0; j < n; ++j) {
@@ -1069,19 +1216,19 @@ void PmeMulti::compute(const float4 *xyzq_s, const float4 *origin, const int *cl
   APO_LAUNCH_CHECK();
   if (calc_virial) {
     if (fp64)
-      pencil_kernel<true, double, true><<<m_pencils, kPencilThreads, 0, s>>>(d0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, m_args, m_pencil_sys);
+      pencil_kernel<true, double, true><<<m_pencils, kPencilThreads, 0, s>>>(d0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, m_args, m_pencil_sys, kNoTensorMap, nullptr);
     else
-      pencil_kernel<true, float, true><<<m_pencils, kPencilThreads, 0, s>>>(d0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, m_args, m_pencil_sys);
+      pencil_kernel<true, float, true><<<m_pencils, kPencilThreads, 0, s>>>(d0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, m_args, m_pencil_sys, kNoTensorMap, nullptr);
   } else if (calc_energy) {
     if (fp64)
-      pencil_kernel<true, double><<<m_pencils, kPencilThreads, 0, s>>>(d0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, m_args, m_pencil_sys);
+      pencil_kernel<true, double><<<m_pencils, kPencilThreads, 0, s>>>(d0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, m_args, m_pencil_sys, kNoTensorMap, nullptr);
     else
-      pencil_kernel<true, float><<<m_pencils, kPencilThreads, 0, s>>>(d0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, m_args, m_pencil_sys);
+      pencil_kernel<true, float><<<m_pencils, kPencilThreads, 0, s>>>(d0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, m_args, m_pencil_sys, kNoTensorMap, nullptr);
   } else {
     if (fp64)
-      pencil_kernel<false, double><<<m_pencils, kPencilThreads, 0, s>>>(d0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, m_args, m_pencil_sys);
+      pencil_kernel<false, double><<<m_pencils, kPencilThreads, 0, s>>>(d0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, m_args, m_pencil_sys, kNoTensorMap, nullptr);
     else
-      pencil_kernel<false, float><<<m_pencils, kPencilThreads, 0, s>>>(d0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, m_args, m_pencil_sys);
+      pencil_kernel<false, float><<<m_pencils, kPencilThreads, 0, s>>>(d0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, m_args, m_pencil_sys, kNoTensorMap, nullptr);
   }
   APO_LAUNCH_CHECK();
   plane_inv_kernel<<<m_planes, kPlaneThreads, m_plane_smem, s>>>(d0, nullptr, nullptr, nullptr,
@@ -1133,7 +1280,7 @@ StaticLayout static_layout(int nx, int ny, int nz) {
   StaticLayout l{};
   const size_t n3 = (size_t)nx + ny + nz;
   const size_t G = (size_t)nx * ny * nz;
-  const size_t Gc = (size_t)nz * ny * (nx / 2 + 1);
+  const size_t Gc = (size_t)nz * ny * ((nx / 2 + 2) & ~1);  // padded rows
   size_t o = 0;
   l.energy = o;   o += align256(kNumEnergyTerms * sizeof(long long));
   l.counts = o;   o += align256(4 * sizeof(int));
@@ -1273,7 +1420,7 @@ void pme_reciprocal_static(const float4 *xyzq, int n, double Lx, double Ly, doub
   if (nx < order || ny < order || nz < order)
     throw std::invalid_argument(
         "pme_reciprocal_static: grid dimensions must be at least the spline order");
-  if ((size_t)(ny / 2) * (nx + 2) * sizeof(float2) > kPlaneSmemMax)
+  if (plane_smem_bytes(nx, ny) > kPlaneSmemMax)
     throw std::invalid_argument("pme_reciprocal_static: grid plane does not fit in shared memory");
   const StaticLayout l = static_layout(nx, ny, nz);
   if (l.total > kPmeStaticScratchBytes)
@@ -1285,6 +1432,7 @@ void pme_reciprocal_static(const float4 *xyzq, int n, double Lx, double Ly, doub
   d.ny = ny;
   d.nz = nz;
   d.nxc = nx / 2 + 1;
+  d.nxcp = (d.nxc + 1) & ~1;
   d.order = order;
   d.Lx = (float)Lx;
   d.Ly = (float)Ly;
@@ -1323,15 +1471,15 @@ void pme_reciprocal_static(const float4 *xyzq, int n, double Lx, double Ly, doub
     case 8: spread_kernel<8><<<blocks, 128, 0, s>>>(xyzq, counts, d, qgrid, nullptr); break;
   }
   APO_LAUNCH_CHECK();
-  const size_t sm = (size_t)(ny / 2) * (nx + 2) * sizeof(float2);
+  const size_t sm = plane_smem_bytes(nx, ny);
   plane_fwd_kernel<<<nz, kPlaneThreads, sm, s>>>(d, qgrid, cgrid, tw, tw + nx);
   APO_LAUNCH_CHECK();
   const int pgrid = ((d.nxc + kPencilTX - 1) / kPencilTX) * ny;
   const float2 *twz = tw + nx + ny;
   if (fp64)
-    pencil_kernel<true, double><<<pgrid, kPencilThreads, 0, s>>>(d, cgrid, twz, prefac, prefac_d, acc);
+    pencil_kernel<true, double><<<pgrid, kPencilThreads, 0, s>>>(d, cgrid, twz, prefac, prefac_d, acc, nullptr, nullptr, nullptr, kNoTensorMap, nullptr);
   else
-    pencil_kernel<true, float><<<pgrid, kPencilThreads, 0, s>>>(d, cgrid, twz, prefac, prefac_d, acc);
+    pencil_kernel<true, float><<<pgrid, kPencilThreads, 0, s>>>(d, cgrid, twz, prefac, prefac_d, acc, nullptr, nullptr, nullptr, kNoTensorMap, nullptr);
   APO_LAUNCH_CHECK();
   plane_inv_kernel<<<nz, kPlaneThreads, sm, s>>>(d, cgrid, phi, tw, tw + nx);
   APO_LAUNCH_CHECK();

@@ -23,6 +23,7 @@
 // needs no reordering pass at all.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <vector>
@@ -52,13 +53,18 @@ struct FftAxis {
   // (radix[s+1..]) passes
   FastDiv per_line[8], dif_mr[8], dit_mr[8];
   FastDiv by_n;      // x / n
+  FastDiv by_nxc;    // x / (n/2 + 1)
+  FastDiv by_nxcp;   // x / the even pitch of n/2 + 1
   FastDiv by_ngrp;   // x / ((n/2 + 1)/2 + 1): the real-to-complex split groups
 };
 // fills the fast divisors of an axis whose n, nrad and radix are set
 void fill_axis_divisors(FftAxis &a);
 
 struct PmeDims {
-  int nx, ny, nz, nxc, order;
+  // nxc = nx/2 + 1 complex values per half-spectrum row, stored with an
+  // even pitch nxcp (rows of a multiple of 16 bytes, as a tensor-memory
+  // copy needs)
+  int nx, ny, nz, nxc, nxcp, order;
   float Lx, Ly, Lz;       // box
   double rLx, rLy, rLz;   // 1 / box, for the FP64 grid anchoring
   float kappa;
@@ -108,6 +114,12 @@ class Pme {
               cudaStream_t s, const float4 *origin = nullptr);
 
   const PmeDims &dims() const { return m_d; }
+  // the z pencils move their slabs with tiled tensor copies (on by default
+  // where the driver offers the encoder); a copy that does not complete sets
+  // kErrCopyTimeout in `err`
+  void set_tensor_copies(bool on) { m_tma_on = on; }
+  bool tensor_copies() const { return m_tma_on && m_tma; }
+  void set_error_word(unsigned *err) { m_err = err; }
   int *qgrid = nullptr;     // nz*ny*nx int32 fixed point (zeroed by plane_fwd)
   float2 *cgrid = nullptr;  // nz * ny * nxc complex (y rows in digit-reversed order)
   float *phi = nullptr;     // nz*ny*nx real potential
@@ -118,6 +130,9 @@ class Pme {
  private:
   void release();
   PmeDims m_d{};
+  CUtensorMap m_tmap{};     // the padded complex grid as floats [nz][ny][2 nxcp]
+  bool m_tma = false, m_tma_on = true;
+  unsigned *m_err = nullptr;
   float2 *m_tw = nullptr;   // twiddles: x (nx), y (ny), z (nz) consecutive
   float *m_prefac = nullptr;  // B-spline moduli 1/|b|^2: x, y, z consecutive
   double *m_prefac_d = nullptr;

@@ -612,6 +612,8 @@ def main():
                     help="batch workload: timed segments per system in the one-by-one baseline "
                          "(0: skip the baseline)")
     ap.add_argument("--precise", action="store_true", help="precision form")
+    ap.add_argument("--pme-tensor-copies", type=int, default=1, choices=[0, 1],
+                    help="z-pencil slabs by tiled tensor copies (1) or plain loads (0)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--tiles-per-work", type=int, default=8,
@@ -663,6 +665,7 @@ def main():
                                            tiles_per_work=args.tiles_per_work,
                                            items_per_warp=args.items_per_warp)
     fm.setDirectKernel(args.direct_kernel)
+    fm.setPmeTensorCopies(bool(args.pme_tensor_copies))
     # remove the close contacts of the generated structure (deterministic)
     s.pos = api.relax(ctx, api.water_indices(s), iterations=RELAX_ITERATIONS,
                       max_step=RELAX_MAX_STEP)
@@ -776,7 +779,8 @@ def main():
             "engine": {"form": "precision" if args.precise else "plain",
                        "direct_kernel": ["tile batches", "grouped queues", "octet lists"][args.direct_kernel],
                        "tiles_per_work": args.tiles_per_work,
-                       "items_per_warp": args.items_per_warp},
+                       "items_per_warp": args.items_per_warp,
+                       "pme_tensor_copies": fm.getPmeTensorCopies()},
             "l2": "flushed (256 MB device write) before every timed iteration, outside the "
                   "timed interval",
             "parallelism": f"replicas x{world}",

@@ -43,6 +43,12 @@ APOCHARMM_C_API apo_status apo_force_manager_set_direct_kernel(apo_force_manager
  * so the trajectory is the same).  Capacity of the last build: get_list_capacity. */
 APOCHARMM_C_API apo_status apo_force_manager_set_list_capacity(apo_force_manager *force_manager, const int tiles);
 APOCHARMM_C_API apo_status apo_force_manager_get_list_capacity(int *tiles, const apo_force_manager *force_manager);
+/* addition: 1 (default) moves the reciprocal-space z-pencil slabs between the
+ * complex grid and shared memory with tiled tensor copies (TMA), 0 with plain
+ * loads and stores; the results are the same. */
+APOCHARMM_C_API apo_status apo_force_manager_set_pme_tensor_copies(apo_force_manager *force_manager, const int on);
+/* 1 when an initialised manager moves its pencil slabs by tensor copies */
+APOCHARMM_C_API apo_status apo_force_manager_get_pme_tensor_copies(int *on, const apo_force_manager *force_manager);
 #ifdef __cplusplus
 }
 #endif

@@ -166,3 +166,25 @@ def test_direct_kernel_forms_agree(tmp_path, precise):
         assert rel_rms(out[0][0], out[form][0]) < 2e-6, form
         if precise:   # per-pair fixed point: the same pairs give the same sums in any order
             assert np.array_equal(out[0][0], out[form][0]), form
+
+
+@pytest.mark.parametrize("nfft", [(48, 48, 48), (64, 60, 50), (40, 48, 56)])
+def test_pme_tensor_copies_give_the_same_results(tmp_path, nfft):
+    """The z-pencil slabs moved by tiled tensor copies (TMA) or by plain
+    loads and stores: the same arithmetic on the same values, so forces,
+    energies and the virial are bit for bit the same (grids whose
+    half-spectrum rows are odd (48: 25) and even (40: 21 -> padded, 64: 33))."""
+    s = water_box(1500, 36.0, seed=4)
+    settings = dict(kappa=0.34, nfft=nfft, order=4, ctofnb=10.0, ctonnb=8.0, cutnb=12.0)
+    out = []
+    for on in (True, False):
+        psf, prm, fm, ctx = api.system_context(s, str(tmp_path / f"t{int(on)}"), settings=settings)
+        fm.setPmeTensorCopies(on)
+        ctx.calculateForces(False, True, True)
+        assert fm.getPmeTensorCopies() == on
+        out.append((ctx.getForces(), ctx.getEnergyComponents(), ctx.getVirial()))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert out[0][1] == out[1][1]
+    assert np.array_equal(out[0][2], out[1][2])
+    Eo, Go = oracle_for(s, settings).evaluate(parts=("recip",))
+    assert out[0][1]["ewks"] == pytest.approx(Eo["ewks"], rel=1e-5)
