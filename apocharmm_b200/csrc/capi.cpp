@@ -6,6 +6,7 @@
 // C++ exceptions become APO_STATUS_RUNTIME_ERROR with the message in a
 // thread-local string read by apo_last_error() (ErrorInternal.h:27-41).
 // CUDA failures are reported as APO_STATUS_CUDA_ERROR.
+#include "apocharmm_c/ForceView.h"
 #include "capi_internal.h"
 
 #include <cstring>
@@ -248,7 +249,7 @@ FM_SETTER(apo_force_manager_set_spline_order, int, setPmeSplineOrder(v), v == 4 
 FM_SETTER(apo_force_manager_set_precision_mode, int, setPrecisionMode(v != 0), true)
 FM_SETTER(apo_force_manager_set_tiles_per_work, int, setTilesPerWork(v), v >= 1 && v <= 1024)
 FM_SETTER(apo_force_manager_set_work_items_per_warp, int, setWorkItemsPerWarp(v), v >= 0 && v <= 1 << 20)
-FM_SETTER(apo_force_manager_set_component_mask, int, setComponentMask(v), v >= 0 && v <= 7)
+FM_SETTER(apo_force_manager_set_component_mask, int, setComponentMask(v), v >= 0 && v <= 15)
 FM_SETTER(apo_force_manager_set_direct_kernel, int, setDirectKernel(v), v >= 0 && v <= 2)
 FM_SETTER(apo_force_manager_set_list_capacity, int, setListCapacity(v), v >= 1)
 FM_SETTER(apo_force_manager_set_pme_tensor_copies, int, setPmeTensorCopies(v != 0), v == 0 || v == 1)
@@ -522,10 +523,9 @@ namespace {
 // Padding slots and the lower triangle of a cluster's tile with itself are
 // not pairs; `excluded` is the tile's topological exclusion bit.
 template <typename Fn>
-void for_each_list_pair(apo::CharmmContext &ctx, double radius, Fn fn) {
-  auto fm = ctx.getForceManager();
+void for_each_list_pair(apo::ForceManager &fmr, cudaStream_t s, double radius, Fn fn) {
+  apo::ForceManager *fm = &fmr;
   auto &nl = fm->neighborList();
-  cudaStream_t s = ctx.stream();
   APO_CUDA(cudaStreamSynchronize(s));
   int counts[8];
   APO_CUDA(cudaMemcpy(counts, nl.counts, sizeof(counts), cudaMemcpyDeviceToHost));
@@ -585,7 +585,7 @@ extern "C" apo_status apo_charmm_context_get_list_pairs(int *pairs, const size_t
     APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
     if (!(radius > 0.0)) return invalid(fn, "radius must be positive");
     size_t count = 0;
-    for_each_list_pair(*c->object, radius, [&](int i, int j, int, bool excluded) {
+    for_each_list_pair(*c->object->getForceManager(), c->object->stream(), radius, [&](int i, int j, int, bool excluded) {
       if (pairs && 3 * (count + 1) <= len) {
         pairs[3 * count] = i;
         pairs[3 * count + 1] = j;
@@ -608,7 +608,7 @@ extern "C" apo_status apo_charmm_context_get_neighbor_pairs(int *pairs, const si
     APO_RETURN_IF(require_ptr(num_pairs, fn, "num_pairs"));
     APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
     size_t count = 0;
-    for_each_list_pair(*c->object, radius, [&](int i, int j, int sc, bool excluded) {
+    for_each_list_pair(*c->object->getForceManager(), c->object->stream(), radius, [&](int i, int j, int sc, bool excluded) {
       if (excluded) return;
       if (pairs && 3 * (count + 1) <= len) {
         pairs[3 * count] = i;
@@ -619,6 +619,66 @@ extern "C" apo_status apo_charmm_context_get_neighbor_pairs(int *pairs, const si
     });
     *num_pairs = count;
     if (pairs && 3 * count > len) return invalid(fn, "pair buffer too small");
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+// The same walk over a force manager's own list (the C++ CudaNeighborList
+// view): every pair within `radius` as (atom i, atom j, excluded).
+extern "C" apo_status apo_force_manager_get_list_pairs(int *pairs, const size_t len,
+                                                       size_t *num_pairs, const double radius,
+                                                       apo_force_manager *fm, void *stream) {
+  const char *fn = "apo_force_manager_get_list_pairs";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_ptr(num_pairs, fn, "num_pairs"));
+    APO_RETURN_IF(require_handle(fm, fn, "ForceManager"));
+    if (fm->object->isMulti()) return invalid(fn, "needs a single-system force manager");
+    if (!fm->object->isListBuilt()) return invalid(fn, "no neighbour list has been built");
+    if (!(radius > 0.0)) return invalid(fn, "radius must be positive");
+    size_t count = 0;
+    for_each_list_pair(*fm->object, reinterpret_cast<cudaStream_t>(stream), radius,
+                       [&](int i, int j, int, bool excluded) {
+      if (pairs && 3 * (count + 1) <= len) {
+        pairs[3 * count] = i;
+        pairs[3 * count + 1] = j;
+        pairs[3 * count + 2] = excluded ? 1 : 0;
+      }
+      ++count;
+    });
+    *num_pairs = count;
+    if (pairs && 3 * count > len) return invalid(fn, "pair buffer too small");
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_force_manager_get_list_counts(int *slots, int *tiles, int *work,
+                                                        apo_force_manager *fm, void *stream) {
+  const char *fn = "apo_force_manager_get_list_counts";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_ptr(slots, fn, "slots"));
+    APO_RETURN_IF(require_ptr(tiles, fn, "tiles"));
+    APO_RETURN_IF(require_ptr(work, fn, "work_items"));
+    APO_RETURN_IF(require_handle(fm, fn, "ForceManager"));
+    if (!fm->object->isListBuilt()) return invalid(fn, "no neighbour list has been built");
+    auto &nl = fm->object->neighborList();
+    nl.sync_counts(reinterpret_cast<cudaStream_t>(stream));
+    *slots = nl.h_counts[0];
+    *tiles = nl.h_counts[1];
+    *work = nl.h_counts[2];
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_force_manager_get_list_arrays(const int **glo2loc, const int **ind_sorted,
+                                                        apo_force_manager *fm) {
+  const char *fn = "apo_force_manager_get_list_arrays";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_ptr(glo2loc, fn, "glo2loc"));
+    APO_RETURN_IF(require_ptr(ind_sorted, fn, "ind_sorted"));
+    APO_RETURN_IF(require_handle(fm, fn, "ForceManager"));
+    if (!fm->object->isInitialized()) return invalid(fn, "the force manager is not initialized");
+    *glo2loc = fm->object->neighborList().glo2loc;
+    *ind_sorted = fm->object->neighborList().perm;
     return APO_STATUS_OK;
   }, fn);
 }

@@ -2,6 +2,7 @@
 #include "engine.h"
 
 #include <climits>
+#include <type_traits>
 
 #include <algorithm>
 #include <cmath>
@@ -21,6 +22,33 @@ __global__ void fixed_to_global_kernel(int n, const long long *__restrict__ f, i
   out[3 * g + 0] = (double)f[s] * kInvForceScale;
   out[3 * g + 1] = (double)f[stride + s] * kInvForceScale;
   out[3 * g + 2] = (double)f[2 * stride + s] * kInvForceScale;
+}
+
+// slot-order fixed-point gradient -> atom-order planes `ostride` apart
+template <typename T>
+__global__ void fixed_to_planes_kernel(int n, const long long *__restrict__ f, int stride,
+                                       const int *__restrict__ glo2loc, T *__restrict__ out,
+                                       int ostride) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n) return;
+  int s = glo2loc[g];
+  if constexpr (std::is_integral<T>::value) {
+    out[g] = f[s];
+    out[ostride + g] = f[stride + s];
+    out[2 * ostride + g] = f[2 * stride + s];
+  } else {
+    out[g] = (T)f[s] * (T)kInvForceScale;
+    out[ostride + g] = (T)f[stride + s] * (T)kInvForceScale;
+    out[2 * ostride + g] = (T)f[2 * stride + s] * (T)kInvForceScale;
+  }
+}
+
+__global__ void xyzq_to_state_kernel(int n, const float4 *__restrict__ xq,
+                                     double4 *__restrict__ c) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n) return;
+  const float4 p = xq[g];
+  c[g] = make_double4(p.x, p.y, p.z, p.w);
 }
 
 // one warp per bonded component: centroid by a warp reduction, then the
@@ -443,6 +471,7 @@ void ForceManager::calcForce(const float4 *d_xyzq, bool calcEnergy, bool calcVir
     APO_CUDA(cudaMemsetAsync(m_Energy.p, 0,
                              (kNumEnergyTerms + (calcVirial ? 9 : 0)) * sizeof(long long), s));
   m_VirialValid = calcVirial;
+  m_EvalMask = m_ComponentMask;
   APO_CUDA(cudaEventRecord(m_EvFork, s));
   if (m_ComponentMask & 2) {
     APO_CUDA(cudaStreamWaitEvent(m_SNb, m_EvFork, 0));
@@ -511,7 +540,12 @@ void ForceManager::calcForce(const float4 *d_xyzq, bool calcEnergy, bool calcVir
     APO_CUDA(cudaEventRecord(m_EvPme, m_SPme));
     APO_CUDA(cudaStreamWaitEvent(s, m_EvPme, 0));
   }
-  if (m_ComponentMask & 1) {
+  // bonded terms proper; the 1-4 pairs and exclusion corrections go with
+  // them or, under kComponent14WithDirect, with the direct space
+  const bool bonded_proper = m_ComponentMask & 1;
+  const bool pairs14 = (m_ComponentMask & kComponent14WithDirect) ? (m_ComponentMask & 2)
+                                                                   : (m_ComponentMask & 1);
+  if (bonded_proper || pairs14) {
     APO_CUDA(cudaStreamWaitEvent(m_SBond, m_EvFork, 0));
     BondedArgs b;
     if (!m_StateCoords) throw std::runtime_error("ForceManager: no state coordinates attached");
@@ -528,6 +562,8 @@ void ForceManager::calcForce(const float4 *d_xyzq, bool calcEnergy, bool calcVir
     b.nimp = (int)m_ImpIJKL.n; b.imp_ijkl = m_ImpIJKL.p; b.imp_p = m_ImpP.p;
     b.nin14 = (int)m_In14.n; b.in14 = m_In14.p;
     b.nex14 = (int)m_Ex14.n; b.ex14 = m_Ex14.p;
+    if (!bonded_proper) b.nbond = b.nub = b.nangle = b.ndihe = b.nimp = 0;
+    if (!pairs14) b.nin14 = b.nex14 = 0;
     b.vdwtype = m_VdwTypeD.p;
     b.vdw14 = m_Vdw14.p;
     b.ntype = (int)m_Top.types.size();
@@ -618,7 +654,7 @@ std::map<std::string, double> ForceManager::getEnergyComponents(cudaStream_t s) 
   APO_CUDA(cudaStreamSynchronize(s));
   std::map<std::string, double> m;
   for (int k = 0; k < kNumEnergyTerms; ++k) m[kEnergyNames[k]] = (double)e[k] * kInvEnergyScale;
-  m["ewse"] = (m_ComponentMask & 4) ? m_SelfEnergy : 0.0;
+  m["ewse"] = (m_EvalMask & 4) ? m_SelfEnergy : 0.0;
   if (!m_Plugins.empty()) {
     long long pe[kMaxPlugins];
     APO_CUDA(cudaMemcpyAsync(pe, m_PluginEnergy.p, sizeof(pe), cudaMemcpyDeviceToHost, s));
@@ -642,7 +678,7 @@ std::map<std::string, double> ForceManager::getEnergyComponents(int sys, cudaStr
   APO_CUDA(cudaStreamSynchronize(s));
   std::map<std::string, double> m;
   for (int k = 0; k < kNumEnergyTerms; ++k) m[kEnergyNames[k]] = (double)e[k] * kInvEnergyScale;
-  m["ewse"] = (m_ComponentMask & 4) ? m_SelfEnergies[sys] : 0.0;
+  m["ewse"] = (m_EvalMask & 4) ? m_SelfEnergies[sys] : 0.0;
   return m;
 }
 
@@ -700,6 +736,56 @@ void ForceManager::getForces(std::vector<double> &out, cudaStream_t s) {
   APO_CUDA(cudaMemcpyAsync(out.data(), m_Scratch.p, (size_t)3 * n * sizeof(double),
                            cudaMemcpyDeviceToHost, s));
   APO_CUDA(cudaStreamSynchronize(s));
+}
+
+void ForceManager::getForcesDevice(double *d_out, int stride, cudaStream_t s) {
+  const int n = m_Top.natom;
+  if (!m_Initialized) throw std::runtime_error("ForceManager is not initialized");
+  if (!d_out || stride < n) throw std::invalid_argument("getForcesDevice: buffer or stride too small");
+  fixed_to_planes_kernel<double><<<(n + 255) / 256, 256, 0, s>>>(n, m_Force.p, m_Stride,
+                                                                 m_Nbl.glo2loc, d_out, stride);
+  APO_LAUNCH_CHECK();
+}
+
+void ForceManager::getForceFixedDevice(long long *d_out, int stride, cudaStream_t s) {
+  const int n = m_Top.natom;
+  if (!m_Initialized) throw std::runtime_error("ForceManager is not initialized");
+  if (!d_out || stride < n)
+    throw std::invalid_argument("getForceFixedDevice: buffer or stride too small");
+  fixed_to_planes_kernel<long long><<<(n + 255) / 256, 256, 0, s>>>(n, m_Force.p, m_Stride,
+                                                                    m_Nbl.glo2loc, d_out, stride);
+  APO_LAUNCH_CHECK();
+}
+
+void ForceManager::calcForceXyzq(const float4 *d_xyzq, bool reset, bool calcEnergy,
+                                 bool calcVirial, int components, cudaStream_t s) {
+  if (m_Multi) throw std::invalid_argument("calcForceXyzq: needs a single-system force manager");
+  if (!d_xyzq) throw std::invalid_argument("calcForceXyzq: xyzq is NULL");
+  if (components < 0 || components > 15)
+    throw std::invalid_argument("calcForceXyzq: components must be a mask of 1, 2, 4 and 8");
+  if (!m_Initialized) initialize();
+  const int n = m_Top.natom;
+  if (m_XyzqState.n != (size_t)n) m_XyzqState.alloc(n);
+  xyzq_to_state_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, d_xyzq, m_XyzqState.p);
+  APO_LAUNCH_CHECK();
+  // the state of an attached context comes back afterwards; the sorted
+  // coordinates it refreshes next are then its own again, and a list built
+  // here from other coordinates is rebuilt before its next use
+  const double4 *attached = m_StateCoords;
+  const int mask = m_ComponentMask;
+  setStateCoordinates(m_XyzqState.p);
+  m_ComponentMask = components;
+  try {
+    if (reset || !m_ListBuilt || m_ListDirty) resetNeighborList(d_xyzq, s);
+    calcForceChecked(d_xyzq, calcEnergy, calcVirial, s);
+  } catch (...) {
+    m_ComponentMask = mask;
+    setStateCoordinates(attached);
+    throw;
+  }
+  m_ComponentMask = mask;
+  setStateCoordinates(attached);
+  if (reset && attached) m_ListDirty = true;
 }
 
 unsigned ForceManager::readDeviceError(cudaStream_t s) { return m_Nbl.read_error(s); }

@@ -119,8 +119,13 @@ class ForceManager {
   // direct-space kernel form (kNbTileBatches or kNbGroupedQueues, nonbonded.h)
   void setDirectKernel(int v);
   int getDirectKernel() const { return m_NbVariant; }
-  // bit mask of the parts evaluated: 1 bonded+1-4, 2 direct, 4 reciprocal
+  // evaluated parts: 1 bonded (with the 1-4 pairs and exclusion corrections
+  // unless kComponent14WithDirect is set), 2 direct space, 4 reciprocal space
   void setComponentMask(int mask) { m_ComponentMask = mask; }
+  int getComponentMask() const { return m_ComponentMask; }
+  // the 1-4 pairs and the exclusion corrections go with the direct space, as
+  // the reference splits CudaBondedForce and CudaPMEDirectForce
+  static constexpr int kComponent14WithDirect = 8;
   // extra force terms evaluated with every force call, their energies
   // reported under `tag` (ForceManager::subscribe/unsubscribe,
   // include/ForceManager.h:420-475); one system only
@@ -173,6 +178,14 @@ class ForceManager {
     m_StateCoords = c;
     m_Nbl.set_state_coordinates(c);
   }
+  // The reference's ForceManager::calcForce(xyzq, reset, calcEnergy,
+  // calcVirial) (include/ForceManager.h:424, src/ForceManager.cu:821) on
+  // caller-owned single-precision coordinates and charges (device float4,
+  // atom order): the FP64 state the kernels read is formed from them, the
+  // list is rebuilt when `reset` (or when none exists yet), and `components`
+  // selects the parts as setComponentMask does, for this call only.
+  void calcForceXyzq(const float4 *d_xyzq, bool reset, bool calcEnergy, bool calcVirial,
+                     int components, cudaStream_t s);
 
   std::map<std::string, double> getEnergyComponents(cudaStream_t s);
   double getPotentialEnergy(cudaStream_t s);
@@ -182,6 +195,10 @@ class ForceManager {
   std::vector<double> getVirial(cudaStream_t s);
   // total gradient, global atom order, (N,3) row-major
   void getForces(std::vector<double> &out, cudaStream_t s);
+  // the same into a caller's device buffer of x/y/z planes `stride` apart,
+  // in FP64 or in the 2^40 fixed point it is summed in (stream-ordered on s)
+  void getForcesDevice(double *d_out, int stride, cudaStream_t s);
+  void getForceFixedDevice(long long *d_out, int stride, cudaStream_t s);
 
   // device state used by the integrators
   long long *forceFixed() const { return m_Force.p; }
@@ -227,8 +244,10 @@ class ForceManager {
   int m_ItemsPerWarp = 0;
   int m_NbVariant = kNbTileBatches;
   int m_ComponentMask = 7;
+  int m_EvalMask = 7;  // parts of the last evaluation
   double m_SelfEnergy = 0.0;
   const double4 *m_StateCoords = nullptr;
+  DeviceArray<double4> m_XyzqState;  // FP64 state formed by calcForceXyzq
   std::vector<std::pair<std::string, std::shared_ptr<ForcePlugin>>> m_Plugins;
   DeviceArray<long long> m_PluginEnergy;  // kMaxPlugins fixed-point slots
   int m_PluginGen = 0;

@@ -46,7 +46,69 @@ __global__ void harmonic_restraint_kernel(const int *__restrict__ count,
   }
 }
 
+// atom-order fixed-point gradient of an external force into the slot-order
+// buffer; thread 0 adds the FP64 energies as one fixed-point value
+__global__ void add_external_kernel(int n, const long long *__restrict__ f, int fstride,
+                                    const int *__restrict__ glo2loc,
+                                    long long *__restrict__ force, int stride,
+                                    const double *__restrict__ e, int ne,
+                                    long long *__restrict__ energy) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < n) {
+    const int s = glo2loc[g];
+    force[s] += f[g];
+    force[stride + s] += f[fstride + g];
+    force[2 * stride + s] += f[2 * fstride + g];
+  }
+  if (g == 0 && e) {
+    double t = 0.0;
+    for (int k = 0; k < ne; ++k) t += e[k];
+    add_energy(energy, t);
+  }
+}
+
 }  // namespace
+
+ExternalForce::ExternalForce(const ExternalForceOps &ops) : m_Ops(ops) {
+  if (!ops.calc_force || !ops.get_force)
+    throw std::invalid_argument("external force: calc_force and get_force are required");
+  if (!ops.stream) throw std::invalid_argument("external force: a stream is required");
+  APO_CUDA(cudaEventCreateWithFlags(&m_Fork, cudaEventDisableTiming));
+  APO_CUDA(cudaEventCreateWithFlags(&m_Join, cudaEventDisableTiming));
+}
+
+ExternalForce::~ExternalForce() {
+  if (m_Fork) cudaEventDestroy(m_Fork);
+  if (m_Join) cudaEventDestroy(m_Join);
+}
+
+void ExternalForce::initialize(int natom, const std::array<double, 3> &box) {
+  if (m_Ops.initialize) m_Ops.initialize(m_Ops.object, natom, box.data());
+}
+
+void ExternalForce::calcForce(const ForcePluginArgs &a, bool calcEnergy, bool calcVirial,
+                              cudaStream_t s) {
+  // the manager's gradient slots are only written on s before and after
+  // this call, so the additions below need no atomics (glo2loc is one to one)
+  APO_CUDA(cudaEventRecord(m_Fork, s));
+  APO_CUDA(cudaStreamWaitEvent(m_Ops.stream, m_Fork, 0));
+  if (m_Ops.clear) m_Ops.clear(m_Ops.object);
+  m_Ops.calc_force(m_Ops.object, reinterpret_cast<const float *>(a.xyzq), calcEnergy ? 1 : 0,
+                   calcVirial ? 1 : 0);
+  int fstride = 0;
+  const long long *f = m_Ops.get_force(m_Ops.object, &fstride);
+  int ne = 0;
+  const double *e = (calcEnergy && m_Ops.get_energies) ? m_Ops.get_energies(m_Ops.object, &ne)
+                                                        : nullptr;
+  APO_CUDA(cudaEventRecord(m_Join, m_Ops.stream));
+  APO_CUDA(cudaStreamWaitEvent(s, m_Join, 0));
+  if (!f || fstride < a.natom)
+    throw std::runtime_error("external force: no force buffer, or its stride is below the atom count");
+  if (e && ne < 0) throw std::runtime_error("external force: negative energy count");
+  add_external_kernel<<<(a.natom + kThreads - 1) / kThreads, kThreads, 0, s>>>(
+      a.natom, f, fstride, a.glo2loc, a.force, a.stride, e, ne, a.energy);
+  APO_LAUNCH_CHECK();
+}
 
 HarmonicRestraintForce::HarmonicRestraintForce(int natom) : m_N(natom) {
   if (natom <= 0) throw std::invalid_argument("HarmonicRestraintForce: number of atoms must be > 0");

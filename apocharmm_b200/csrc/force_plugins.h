@@ -88,4 +88,38 @@ class HarmonicRestraintForce : public ForcePlugin {
   double4 *m_Target = nullptr; // device: (x0, y0, z0, k m) per restrained atom
 };
 
+// A force term evaluated by the caller's own code, reached through a table
+// of plain functions: the reference's ForceView type erasure
+// (include/ForceManager.h:37-105) across the C ABI.  Each call forks the
+// caller's stream from the manager's, lets the caller clear and evaluate
+// its term there, joins back, and adds the caller's atom-order fixed-point
+// gradient (2^40, x/y/z planes) and the sum of its FP64 energies into the
+// manager's buffers (src/ForceManager.cu:596-620 and 678-690 do the same
+// through per-force streams and a host-side total).  The caller's virial is
+// not added: the reference computes it from the force buffers only for the
+// pressure, which no integrator here reads from plug-ins.
+struct ExternalForceOps {
+  void *object = nullptr;
+  void (*initialize)(void *object, int num_atoms, const double *box3) = nullptr;
+  void (*clear)(void *object) = nullptr;
+  void (*calc_force)(void *object, const float *d_xyzq, int calc_energy, int calc_virial) = nullptr;
+  const long long *(*get_force)(void *object, int *stride) = nullptr;
+  const double *(*get_energies)(void *object, int *count) = nullptr;
+  cudaStream_t stream = nullptr;
+};
+
+class ExternalForce : public ForcePlugin {
+ public:
+  explicit ExternalForce(const ExternalForceOps &ops);
+  ~ExternalForce() override;
+  void initialize(int natom, const std::array<double, 3> &box) override;
+  void calcForce(const ForcePluginArgs &a, bool calcEnergy, bool calcVirial,
+                 cudaStream_t s) override;
+  const void *object() const { return m_Ops.object; }
+
+ private:
+  ExternalForceOps m_Ops;
+  cudaEvent_t m_Fork = nullptr, m_Join = nullptr;
+};
+
 }  // namespace apo

@@ -25,7 +25,8 @@ APOCHARMM_C_API apo_status apo_force_manager_set_ctofnb(apo_force_manager *force
 APOCHARMM_C_API apo_status apo_force_manager_set_fft_grid(apo_force_manager *force_manager, const int nx, const int ny, const int nz);
 APOCHARMM_C_API apo_status apo_force_manager_set_spline_order(apo_force_manager *force_manager, const int order);
 /* additions: precision form on/off; tiles per nonbonded work item (tuning);
- * evaluated parts as a bit mask (1 bonded+1-4, 2 direct, 4 reciprocal) */
+ * evaluated parts as a bit mask (1 bonded+1-4, 2 direct, 4 reciprocal; + 8
+ * moves the 1-4 pairs and exclusion corrections to the direct part) */
 APOCHARMM_C_API apo_status apo_force_manager_set_precision_mode(apo_force_manager *force_manager, const int precise);
 APOCHARMM_C_API apo_status apo_force_manager_set_tiles_per_work(apo_force_manager *force_manager, const int tiles);
 /* addition: work items one warp of the direct-space kernel takes before it
