@@ -861,7 +861,7 @@ class Server(_Handle):
         self._keep.pop(rid, None)
 
     def stats(self) -> Dict[str, float]:
-        a = np.zeros(6)
-        call("apo_server_get_stats", _ptr(a), _sz(6), self._h)
+        a = np.zeros(8)
+        call("apo_server_get_stats", _ptr(a), _sz(8), self._h)
         return dict(zip(("system_steps", "simulated_ps", "rebuilds", "segments", "max_batch",
-                         "busy_s"), a.tolist()))
+                         "busy_s", "reform_s", "energy_evals"), a.tolist()))

@@ -73,6 +73,30 @@ void Batch::getVelocities(int sys, double *v) {
   m_Ctx->getVelocitiesXyz(v, atomOffset(sys), numAtoms(sys));
 }
 
+void Batch::saveState(int sys, double4 *dst) {
+  requireSys(sys);
+  const int o = atomOffset(sys), n = numAtoms(sys);
+  cudaStream_t s = m_Ctx->stream();
+  m_Ctx->saveStateDevice(dst, o, n);
+  if (m_Integ && m_Integ->deltaState())
+    APO_CUDA(cudaMemcpyAsync(dst + 2 * (size_t)n, m_Integ->deltaState() + o, n * sizeof(double4),
+                             cudaMemcpyDeviceToDevice, s));
+  else
+    APO_CUDA(cudaMemsetAsync(dst + 2 * (size_t)n, 0, n * sizeof(double4), s));
+  APO_CUDA(cudaStreamSynchronize(s));
+}
+
+void Batch::loadState(int sys, const double4 *src) {
+  requireSys(sys);
+  const int o = atomOffset(sys), n = numAtoms(sys);
+  cudaStream_t s = m_Ctx->stream();
+  m_Ctx->loadStateDevice(src, o, n);
+  if (m_Integ && m_Integ->deltaState())
+    APO_CUDA(cudaMemcpyAsync(m_Integ->deltaState() + o, src + 2 * (size_t)n, n * sizeof(double4),
+                             cudaMemcpyDeviceToDevice, s));
+  APO_CUDA(cudaStreamSynchronize(s));
+}
+
 void Batch::assignVelocities(double temperature) {
   requireInit();
   m_Ctx->assignVelocitiesAtTemperature(temperature);

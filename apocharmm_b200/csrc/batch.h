@@ -35,6 +35,12 @@ class Batch {
   void getCoordinates(int sys, double *xyz);
   void setVelocities(int sys, const double *v);
   void getVelocities(int sys, double *v);
+  // a system's state kept on the device: coordinates, velocities and the
+  // integrator's position-Verlet delta, 3 x numAtoms(sys) double4 at dst
+  // (the delta part is zero while no integrator exists); loadState puts all
+  // three back (the delta only when an integrator exists).  Synchronous.
+  void saveState(int sys, double4 *dst);
+  void loadState(int sys, const double4 *src);
   void assignVelocities(double temperature);
   void setLangevin(double dtPs, double frictionPerPs, double temperature, uint64_t seed);
   // create the Langevin integrator now (it is otherwise created by the first

@@ -193,6 +193,10 @@ extern "C" apo_status apo_server_get_stats(double *stats, const size_t len, apo_
     stats[3] = (double)st.segments;
     stats[4] = (double)st.max_active;
     stats[5] = st.busy_s;
+    if (len >= 8) {
+      stats[6] = st.reform_s;
+      stats[7] = (double)st.energy_evals;
+    }
     return APO_STATUS_OK;
   }, fn);
 }

@@ -309,7 +309,9 @@ void ForceManager::initializeMulti() {
     if (y.ctofnb > y.cutnb) throw std::invalid_argument("ctofnb must not exceed the list cutoff (cutnb)");
     for (int d = 0; d < 3; ++d)
       if (y.nfft[d] <= 0) y.nfft[d] = std::max(2, 2 * ((int)y.box[d] / 2));
-    Topology t = build_topology(*y.psf, *y.prm);
+    Topology t = y.topology ? *y.topology : build_topology(*y.psf, *y.prm);
+    if (t.natom != y.psf->getNumAtoms())
+      throw std::invalid_argument("ForceManager: a system's topology does not match its PSF");
     if ((int)t.types.size() > kMaxMultiTypes)
       throw std::invalid_argument("ForceManager: a system of a multi-system manager has more than " +
                                   std::to_string(kMaxMultiTypes) + " Lennard-Jones types");
@@ -930,6 +932,29 @@ void CharmmContext::setCoordinatesXyz(const double *xyz, int first, int count, b
     m_ListStale = true;
   }
   APO_CUDA(cudaStreamSynchronize(m_Stream));
+}
+
+void CharmmContext::saveStateDevice(double4 *dst, int first, int count) {
+  if (first < 0 || count < 0 || first + count > m_N)
+    throw std::invalid_argument("saveStateDevice: atom range out of bounds");
+  if (!count) return;
+  APO_CUDA(cudaMemcpyAsync(dst, m_Coords.p + first, count * sizeof(double4),
+                           cudaMemcpyDeviceToDevice, m_Stream));
+  APO_CUDA(cudaMemcpyAsync(dst + count, m_VelMass.p + first, count * sizeof(double4),
+                           cudaMemcpyDeviceToDevice, m_Stream));
+}
+
+void CharmmContext::loadStateDevice(const double4 *src, int first, int count) {
+  if (first < 0 || count < 0 || first + count > m_N)
+    throw std::invalid_argument("loadStateDevice: atom range out of bounds");
+  if (!count) return;
+  APO_CUDA(cudaMemcpyAsync(m_Coords.p + first, src, count * sizeof(double4),
+                           cudaMemcpyDeviceToDevice, m_Stream));
+  APO_CUDA(cudaMemcpyAsync(m_VelMass.p + first, src + count, count * sizeof(double4),
+                           cudaMemcpyDeviceToDevice, m_Stream));
+  launch_coords_to_xyzq(m_Coords.p + first, m_Xyzq.p + first, count, m_Stream);
+  m_HasCoords = true;
+  m_ListStale = true;
 }
 
 std::vector<double> CharmmContext::getCoordinates() {

@@ -76,6 +76,9 @@ struct SystemSpec {
   double kappa = 0.34, cutnb = 14.0, ctonnb = 12.0, ctofnb = 10.0;
   std::array<int, 3> nfft{{-1, -1, -1}};  // -1: 2 floor(L/2)
   uint64_t seed = 0;                      // velocities and Langevin noise of this system
+  // the system's topology built beforehand from psf and prm (build_topology),
+  // or null to build it during initialisation
+  std::shared_ptr<const Topology> topology;
 };
 
 class ForceManager {
@@ -294,6 +297,12 @@ class CharmmContext {
   void getCoordinatesXyz(double *xyz, int first = 0, int count = -1);
   void setVelocitiesXyz(const double *v, int first = 0, int count = -1);
   void getVelocitiesXyz(double *v, int first = 0, int count = -1);
+  // device-resident copy of an atom range's state: coordinates (x, y, z,
+  // charge) then velocities (with the mass term), 2 x count double4 at dst,
+  // and back; stream-ordered on the context's stream (a load marks the list
+  // stale and refreshes the single-precision coordinates)
+  void saveStateDevice(double4 *dst, int first, int count);
+  void loadStateDevice(const double4 *src, int first, int count);
   void setRandomSeedForVelocities(uint64_t seed) { m_Seed = seed; }
   void assignVelocitiesAtTemperature(double temperature);
   void useHolonomicConstraints(bool flag);

@@ -26,6 +26,7 @@ Server::Server(double fraction, int order, bool precise, double dt, double frict
   size_t free_b = 0, total_b = 0;
   APO_CUDA(cudaMemGetInfo(&free_b, &total_b));
   m_Budget = (size_t)(fraction * (double)free_b);
+  m_PrepThread = std::thread([this] { prepareLoop(); });
   m_Thread = std::thread([this] { loop(); });
 }
 
@@ -37,6 +38,7 @@ void Server::stop() {
     m_Stop = true;
   }
   m_Cv.notify_all();
+  if (m_PrepThread.joinable()) m_PrepThread.join();
   if (m_Thread.joinable()) m_Thread.join();
 }
 
@@ -56,9 +58,38 @@ int Server::submit(ServeRequest r) {
   j->id = m_NextId++;
   m_Results[j->id] = ServeResult{};
   m_Results[j->id].kind = j->req.kind;
-  m_Queue.push_back(j);
+  m_Prepare.push_back(j);
   m_Cv.notify_all();
   return j->id;
+}
+
+// builds each submitted request's topology off the worker thread, in
+// submission order, and hands it on to admission
+void Server::prepareLoop() {
+  for (;;) {
+    std::shared_ptr<Job> j;
+    {
+      std::unique_lock<std::mutex> lk(m_Mu);
+      m_Cv.wait(lk, [&] { return m_Stop || !m_Prepare.empty(); });
+      if (m_Stop) return;
+      j = m_Prepare.front();
+      m_Prepare.pop_front();
+    }
+    try {
+      j->req.spec.topology =
+          std::make_shared<const Topology>(build_topology(*j->req.spec.psf, *j->req.spec.prm));
+    } catch (const std::exception &e) {
+      ServeResult r;
+      r.kind = j->req.kind;
+      r.status = 2;
+      r.error = std::string("Server: topology: ") + e.what();
+      finish(j, std::move(r));
+      continue;
+    }
+    std::lock_guard<std::mutex> lk(m_Mu);
+    m_Queue.push_back(j);
+    m_Cv.notify_all();
+  }
 }
 
 bool Server::poll(int id, ServeResult *out) {
@@ -103,88 +134,95 @@ void Server::finish(const std::shared_ptr<Job> &j, ServeResult &&r) {
   m_Cv.notify_all();
 }
 
-void Server::evaluateEnergies(std::vector<std::shared_ptr<Job>> &jobs) {
-  Batch b(m_Order, 8, m_Precise);
-  std::vector<double> all;
-  for (auto &j : jobs) {
-    b.addSystem(j->req.spec);
-    all.insert(all.end(), j->req.xyz.begin(), j->req.xyz.end());
-  }
-  b.initialize();
-  b.setCoordinates(-1, all.data());
-  b.calculateForces(true, false);
-  for (size_t k = 0; k < jobs.size(); ++k) {
+// answers the energy/force requests of the current batch: one force call
+// of the whole batch (every member at its current coordinates; the MD
+// members' trajectories are untouched, their forces are recomputed by the
+// next step), then they leave at the next re-formation
+void Server::evaluateEnergies() {
+  bool any = false;
+  for (auto &j : m_BatchJobs) any |= j->req.kind == 1 && !j->evaluated;
+  if (!any) return;
+  m_Batch->calculateForces(true, false);
+  for (size_t k = 0; k < m_BatchJobs.size(); ++k) {
+    auto &j = m_BatchJobs[k];
+    if (j->req.kind != 1 || j->evaluated) continue;
     ServeResult r;
     r.kind = 1;
     r.status = 1;
-    r.forces.resize((size_t)3 * jobs[k]->natom);
-    b.getForces((int)k, r.forces.data());
-    auto e = b.energyComponents((int)k);
+    r.forces.resize((size_t)3 * j->natom);
+    m_Batch->getForces((int)k, r.forces.data());
+    auto e = m_Batch->energyComponents((int)k);
     for (int t = 0; t < kNumEnergyTerms; ++t) r.energy[t] = e[kEnergyNames[t]];
-    r.xyz = jobs[k]->req.xyz;
-    finish(jobs[k], std::move(r));
+    r.xyz = j->req.xyz;
+    j->evaluated = true;
+    finish(j, std::move(r));
   }
+  std::vector<std::shared_ptr<Job>> keep;
+  for (auto &j : m_Active)
+    if (!(j->req.kind == 1 && j->evaluated)) keep.push_back(j);
+  m_Active.swap(keep);
+  m_Dirty = true;
+  std::lock_guard<std::mutex> lk(m_Mu);
+  ++m_Stats.energy_evals;
 }
 
-// re-form the MD batch around m_Active, carrying every continuing system's
-// state over exactly
+// re-form the batch around m_Active; every continuing system's state moves
+// device to device through m_Carry and comes back bit for bit
 void Server::reform() {
-  if (m_Batch) {  // save the state of the systems that continue
-    double4 *delta = m_Batch->integrator() ? m_Batch->integrator()->deltaState() : nullptr;
-    for (size_t k = 0; k < m_BatchJobs.size(); ++k) {
-      auto &j = m_BatchJobs[k];
-      if (j->done >= j->req.steps || !delta) continue;
-      j->xyz.resize((size_t)3 * j->natom);
-      j->vel.resize((size_t)3 * j->natom);
-      m_Batch->getCoordinates((int)k, j->xyz.data());
-      m_Batch->getVelocities((int)k, j->vel.data());
-      j->delta.resize(j->natom);
-      APO_CUDA(cudaMemcpy(j->delta.data(), delta + m_Batch->atomOffset((int)k),
-                          j->delta.size() * sizeof(double4), cudaMemcpyDeviceToHost));
-    }
-    m_Batch.reset();
+  const auto t0 = std::chrono::steady_clock::now();
+  std::map<int, size_t> carried;  // job id -> offset in m_Carry (double4)
+  if (m_Batch) {
+    std::map<int, int> in_old;
+    for (size_t k = 0; k < m_BatchJobs.size(); ++k) in_old[m_BatchJobs[k]->id] = (int)k;
+    size_t total = 0;
+    for (auto &j : m_Active)
+      if (j->started && j->req.kind == 0 && in_old.count(j->id)) {
+        carried[j->id] = total;
+        total += 3 * (size_t)j->natom;
+      }
+    if (m_Carry.n < total) m_Carry.alloc(total);
+    for (auto &kv : carried) m_Batch->saveState(in_old[kv.first], m_Carry.p + kv.second);
+    m_Batch.reset();  // the old batch's memory is free before the new one is built
   }
   m_BatchJobs = m_Active;
   m_Batch.reset(new Batch(m_Order, 8, m_Precise));
-  std::vector<double> all;
-  for (auto &j : m_Active) {
-    m_Batch->addSystem(j->req.spec);
-    const std::vector<double> &x = j->started ? j->xyz : j->req.xyz;
-    all.insert(all.end(), x.begin(), x.end());
-  }
+  for (auto &j : m_Active) m_Batch->addSystem(j->req.spec);
   m_Batch->initialize();
-  m_Batch->setCoordinates(-1, all.data());
+  for (size_t k = 0; k < m_Active.size(); ++k) {
+    auto &j = m_Active[k];
+    auto it = carried.find(j->id);
+    if (it != carried.end()) m_Batch->loadState((int)k, m_Carry.p + it->second);
+    else m_Batch->setCoordinates((int)k, j->req.xyz.data());
+  }
   m_Batch->setLangevin(m_Dt, m_Friction, m_Temp, m_Seed);
   m_Batch->assignVelocities(m_Temp);   // every system from its own seed
-  for (size_t k = 0; k < m_Active.size(); ++k)
-    if (m_Active[k]->started) m_Batch->setVelocities((int)k, m_Active[k]->vel.data());
   m_Batch->createIntegrator();         // new systems: constraint + delta from velocities
   std::vector<unsigned long long> rng0;
   std::vector<long long> stop;
-  double4 *delta = m_Batch->integrator()->deltaState();
   for (size_t k = 0; k < m_Active.size(); ++k) {
     auto &j = m_Active[k];
-    if (j->started) {  // overwrite whatever the initialisation did
-      m_Batch->setCoordinates((int)k, j->xyz.data());
-      m_Batch->setVelocities((int)k, j->vel.data());
-      APO_CUDA(cudaMemcpy(delta + m_Batch->atomOffset((int)k), j->delta.data(),
-                          j->delta.size() * sizeof(double4), cudaMemcpyHostToDevice));
-    }
+    auto it = carried.find(j->id);
+    // continuing systems: coordinates, velocities and delta as they were;
+    // energy requests: their own coordinates (the integrator's constraint
+    // set-up may have moved them)
+    if (it != carried.end()) m_Batch->loadState((int)k, m_Carry.p + it->second);
+    else if (j->req.kind == 1) m_Batch->setCoordinates((int)k, j->req.xyz.data());
     j->started = true;
     rng0.push_back(j->rng);
-    stop.push_back(j->req.steps - j->done);
+    stop.push_back(j->req.kind == 1 ? 0 : j->req.steps - j->done);
   }
   m_Batch->integrator()->setSystemLimits(rng0, stop);
   m_Dirty = false;
   std::lock_guard<std::mutex> lk(m_Mu);
   ++m_Stats.rebuilds;
+  m_Stats.reform_s += seconds_since(t0);
 }
 
 void Server::loop() {
   try {
     APO_CUDA(cudaSetDevice(m_Device));
     for (;;) {
-      std::vector<std::shared_ptr<Job>> admit, energy;
+      std::vector<std::shared_ptr<Job>> admit;
       {
         std::unique_lock<std::mutex> lk(m_Mu);
         if (m_Queue.empty() && m_Active.empty())
@@ -197,15 +235,14 @@ void Server::loop() {
         while (!m_Queue.empty()) {
           auto &j = m_Queue.front();
           const double need = j->natom * bytesPerAtom();
-          const bool nothing_running = m_Active.empty() && admit.empty() && energy.empty();
+          const bool nothing_running = m_Active.empty() && admit.empty();
           if (used + need > (double)m_Budget && !nothing_running) break;
-          (j->req.kind == 1 ? energy : admit).push_back(j);
+          admit.push_back(j);
           used += need;
           m_Queue.pop_front();
         }
       }
       const auto t0 = std::chrono::steady_clock::now();
-      if (!energy.empty()) evaluateEnergies(energy);
       if (!admit.empty()) {
         m_Active.insert(m_Active.end(), admit.begin(), admit.end());
         m_Dirty = true;
@@ -220,12 +257,21 @@ void Server::loop() {
         continue;
       }
       if (m_Dirty) reform();
+      evaluateEnergies();
+      bool md = false;
+      for (auto &j : m_Active) md |= j->req.kind == 0;
+      if (!md) {  // only energy requests were waiting
+        std::lock_guard<std::mutex> lk(m_Mu);
+        m_Stats.busy_s += seconds_since(t0);
+        continue;
+      }
       m_Batch->propagate(kSegment);
       long long advanced = 0;
       const int nactive = (int)m_BatchJobs.size();
       std::vector<std::shared_ptr<Job>> keep;
       for (size_t k = 0; k < m_BatchJobs.size(); ++k) {
         auto &j = m_BatchJobs[k];
+        if (j->req.kind == 1) continue;         // energy request, held still
         if (j->done >= j->req.steps) continue;  // finished earlier, held still
         const long long take = std::min<long long>(kSegment, j->req.steps - j->done);
         j->done += take;

@@ -1,18 +1,24 @@
 // Request server with continuous batching.
 //
 // Clients submit MD-segment requests (a system, its coordinates, a step
-// count and a seed) and energy/force requests; a worker thread owns the GPU
-// and advances every admitted MD request together in one batch (batch.h),
-// 20 steps (one list-update segment, one CUDA graph) at a time.  Between
-// segments it admits waiting requests while their estimated device memory
-// fits a fraction of the free HBM measured at start, and drops finished
-// ones; when the set changes the batch is re-formed and every continuing
-// system carries over its coordinates, velocities, position-Verlet delta
-// and noise position exactly.  A system therefore follows the same
-// trajectory alone and among any others: its segments always start at its
-// own steps 0, 20, 40, ..., and a system whose step count ends inside a
-// segment is held still (not advanced) for the rest of it.  Energy/force
-// requests are evaluated together in a batch of their own.
+// count and a seed) and energy/force requests.  A preparation thread builds
+// each request's topology from its PSF and parameters as it arrives; a
+// worker thread owns the GPU and advances every admitted MD request
+// together in one batch (batch.h), 20 steps (one list-update segment, one
+// CUDA graph) at a time.  Between segments it admits prepared requests
+// while their estimated device memory fits a fraction of the free HBM
+// measured at start, and drops finished ones; when the set changes the
+// batch is re-formed from the prepared topologies, and every continuing
+// system carries its coordinates, velocities and position-Verlet delta
+// over device to device (through a compact device buffer, so the old and
+// the new batch never coexist) together with its noise position.  A system
+// therefore follows the same trajectory alone and among any others: its
+// segments always start at its own steps 0, 20, 40, ..., and a system whose
+// step count ends inside a segment is held still (not advanced) for the
+// rest of it.  Energy/force requests join the batch at its next
+// re-formation, are evaluated by one force call of the whole batch at
+// their own coordinates, and leave at the following one (held still for at
+// most one segment in between).
 //
 // No counterpart in the reference (it has no serving layer); the physics
 // is the reference's per-system force/step path.
@@ -56,6 +62,8 @@ struct ServerStats {
   long long segments = 0;
   int max_active = 0;
   double busy_s = 0.0;          // time the worker spent on GPU work
+  double reform_s = 0.0;        // of which re-forming the batch
+  long long energy_evals = 0;   // force calls made for energy/force requests
 };
 
 class Server {
@@ -82,12 +90,12 @@ class Server {
     int natom = 0;
     long long done = 0;                  // steps taken
     unsigned long long rng = 0;          // noise position
-    bool started = false;
-    std::vector<double> xyz, vel;        // state between batches (host)
-    std::vector<double4> delta;          // position-Verlet delta (host)
+    bool started = false;                // has been a member of a batch
+    bool evaluated = false;              // energy/force request answered
   };
   void loop();
-  void evaluateEnergies(std::vector<std::shared_ptr<Job>> &jobs);
+  void prepareLoop();
+  void evaluateEnergies();
   void reform();
   void finish(const std::shared_ptr<Job> &j, ServeResult &&r);
 
@@ -103,7 +111,8 @@ class Server {
   std::condition_variable m_Cv;
   bool m_Stop = false;
   int m_NextId = 1;
-  std::deque<std::shared_ptr<Job>> m_Queue;      // submitted, not admitted
+  std::deque<std::shared_ptr<Job>> m_Prepare;    // submitted, topology not built yet
+  std::deque<std::shared_ptr<Job>> m_Queue;      // prepared, not admitted
   std::map<int, ServeResult> m_Results;
   ServerStats m_Stats;
   std::string m_Fatal;
@@ -112,8 +121,9 @@ class Server {
   std::vector<std::shared_ptr<Job>> m_Active;    // MD jobs running
   std::vector<std::shared_ptr<Job>> m_BatchJobs; // the jobs of m_Batch, in its order
   std::unique_ptr<Batch> m_Batch;
+  DeviceArray<double4> m_Carry;                  // continuing systems' state during a re-formation
   bool m_Dirty = false;
-  std::thread m_Thread;
+  std::thread m_Thread, m_PrepThread;
 };
 
 }  // namespace apo

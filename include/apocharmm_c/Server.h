@@ -44,7 +44,8 @@ APOCHARMM_C_API apo_status apo_server_get_latency(double *seconds, apo_server *s
 APOCHARMM_C_API apo_status apo_server_release(apo_server *server, const int id);
 /* stats[0] system-steps advanced, [1] simulated ps over all requests,
  * [2] batch re-formations, [3] segments, [4] most systems in one batch,
- * [5] seconds the worker spent on device work */
+ * [5] seconds the worker spent on device work; with len >= 8 also [6] of
+ * which re-forming the batch, [7] force calls made for energy requests */
 APOCHARMM_C_API apo_status apo_server_get_stats(double *stats, const size_t len, apo_server *server);
 #ifdef __cplusplus
 }
