@@ -8,6 +8,7 @@ namespace apo {
 
 namespace {
 constexpr int kSegment = 20;  // MD steps per list-update segment
+constexpr double kIdleShare = 0.3;  // idle atoms in a batch that trigger a re-formation
 double seconds_since(std::chrono::steady_clock::time_point t0) {
   return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
@@ -161,9 +162,24 @@ void Server::evaluateEnergies() {
   for (auto &j : m_Active)
     if (!(j->req.kind == 1 && j->evaluated)) keep.push_back(j);
   m_Active.swap(keep);
-  m_Dirty = true;
+  markIdle();
   std::lock_guard<std::mutex> lk(m_Mu);
   ++m_Stats.energy_evals;
+}
+
+// Members that are done (finished MD requests, answered energy requests)
+// stay in the batch, held still, until they hold more than kIdleShare of
+// its atoms or the batch is re-formed for a new member anyway: a
+// re-formation costs more than carrying a few idle systems for a while.
+void Server::markIdle() {
+  double idle = 0.0, all = 0.0;
+  std::map<int, bool> active;
+  for (auto &j : m_Active) active[j->id] = true;
+  for (auto &j : m_BatchJobs) {
+    all += j->natom;
+    if (!active.count(j->id)) idle += j->natom;
+  }
+  if (all > 0.0 && idle > kIdleShare * all) m_Dirty = true;
 }
 
 // re-form the batch around m_Active; every continuing system's state moves
@@ -286,12 +302,12 @@ void Server::loop() {
           m_Batch->getCoordinates((int)k, r.xyz.data());
           m_Batch->getVelocities((int)k, r.vel.data());
           finish(j, std::move(r));
-          m_Dirty = true;
         } else {
           keep.push_back(j);
         }
       }
       m_Active.swap(keep);
+      markIdle();
       std::lock_guard<std::mutex> lk(m_Mu);
       ++m_Stats.segments;
       m_Stats.md_steps += advanced;

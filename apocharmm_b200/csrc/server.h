@@ -15,10 +15,12 @@
 // therefore follows the same trajectory alone and among any others: its
 // segments always start at its own steps 0, 20, 40, ..., and a system whose
 // step count ends inside a segment is held still (not advanced) for the
-// rest of it.  Energy/force requests join the batch at its next
-// re-formation, are evaluated by one force call of the whole batch at
-// their own coordinates, and leave at the following one (held still for at
-// most one segment in between).
+// rest of it, and for as long afterwards as it stays in the batch: done
+// members leave at the next re-formation, which comes with the next
+// admission or once they hold 30 % of the batch's atoms.  Energy/force
+// requests join the batch at its next re-formation, are evaluated by one
+// force call of the whole batch at their own coordinates, and are then done
+// members like finished MD requests.
 //
 // No counterpart in the reference (it has no serving layer); the physics
 // is the reference's per-system force/step path.
@@ -96,6 +98,7 @@ class Server {
   void loop();
   void prepareLoop();
   void evaluateEnergies();
+  void markIdle();
   void reform();
   void finish(const std::shared_ptr<Job> &j, ServeResult &&r);
 
