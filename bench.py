@@ -57,7 +57,7 @@ FLOP_PER_PAIR = 65
 # dram__bytes_write.sum) from one ncu capture of the same kernel on the same
 # workload (the inputs and the fixed-point force buffer stay in L2)
 NB_TRAFFIC = {
-    "chain23k": (7423488, "ncu capture of this kernel on this workload "
+    "chain23k": (2193920, "ncu capture of this kernel on this workload "
                           "(dram__bytes_read.sum + dram__bytes_write.sum)"),
 }
 
