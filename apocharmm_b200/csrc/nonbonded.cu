@@ -135,8 +135,11 @@ __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
     }
     Acc fix = 0, fiy = 0, fiz = 0;
     float vw[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    // packed form: i-atom values in both halves, two partial sums per sum
-    const F2 xi2x = f2(xi.x), xi2y = f2(xi.y), xi2z = f2(xi.z), qi2 = f2(qi);
+    // packed form: i-atom values in both halves, two partial sums per sum;
+    // a padding slot sits 1e18 A away, so none of its pairs is inside the
+    // cutoff (its differences stay finite: their force factor is exactly 0)
+    const F2 xi2x = f2(ivalid ? xi.x : 1e18f), xi2y = f2(ivalid ? xi.y : 1e18f),
+             xi2z = f2(ivalid ? xi.z : 1e18f), qi2 = f2(qi);
     F2 fi2x = f2(0.f), fi2y = f2(0.f), fi2z = f2(0.f);
     F2 vw2[6] = {f2(0.f), f2(0.f), f2(0.f), f2(0.f), f2(0.f), f2(0.f)};
 
@@ -196,57 +199,67 @@ __global__ void __launch_bounds__(kThreads) nb_kernel(NbArgs a) {
       Acc fjx = 0, fjy = 0, fjz = 0;  // force of compacted j (lane&3)*8 + (lane>>2)
       const int nbatch = (nj + 7) >> 3;
       if constexpr (!PER_PAIR) {
-        for (int b = 0; b < nbatch; ++b) {
-          float fx[8], fy[8], fz[8];
+        // tiles without a topological exclusion and other than a cluster's
+        // tile with itself (most of them) skip the exclusion test
+        auto batches = [&](auto with_excl) {
+          constexpr bool EXCL = decltype(with_excl)::value;
+          for (int b = 0; b < nbatch; ++b) {
+            float fx[8], fy[8], fz[8];
 #pragma unroll
-          for (int pp = 0; pp < 4; ++pp) {
-            const int r = b * 8 + 2 * pp;
-            fx[2 * pp] = fx[2 * pp + 1] = 0.f;
-            fy[2 * pp] = fy[2 * pp + 1] = 0.f;
-            fz[2 * pp] = fz[2 * pp + 1] = 0.f;
-            if (r < nj) {  // uniform across the warp
-              const float4 A = sh_xq[wib][r];      // x0 x1 y0 y1
-              const float4 B = sh_xq[wib][r + 1];  // z0 z1 q0 q1
-              const int2 tj = *reinterpret_cast<const int2 *>(&sh_tj[wib][r]);
-              const F2 dx = xi2x - f2(A.x, A.y), dy = xi2y - f2(A.z, A.w),
-                       dz = xi2z - f2(B.x, B.y);
-              const F2 r2raw = fma2(dz, dz, fma2(dy, dy, dx * dx));
-              const bool in0 = ivalid && !((excl >> (tj.x >> 16)) & 1u) && f2lo(r2raw) < st.roff2;
-              const bool in1 = ivalid && r + 1 < nj && !((excl >> (tj.y >> 16)) & 1u) &&
-                               f2hi(r2raw) < st.roff2;
-              const float2 cc0 = vrow[tj.x & 0xffff], cc1 = vrow[tj.y & 0xffff];
-              const F2 f = pair_force2<ENERGY>(st, r2raw, in0, in1, qi2 * f2(B.z, B.w), cc0, cc1,
-                                               e_elec, e_vdw);
-              const F2 gx = f * dx, gy = f * dy, gz = f * dz;
-              if (VIRIAL) {
-                vw2[0] = fma2(gx, dx, vw2[0]);
-                vw2[1] = fma2(gx, dy, vw2[1]);
-                vw2[2] = fma2(gx, dz, vw2[2]);
-                vw2[3] = fma2(gy, dy, vw2[3]);
-                vw2[4] = fma2(gy, dz, vw2[4]);
-                vw2[5] = fma2(gz, dz, vw2[5]);
+            for (int pp = 0; pp < 4; ++pp) {
+              const int r = b * 8 + 2 * pp;
+              fx[2 * pp] = fx[2 * pp + 1] = 0.f;
+              fy[2 * pp] = fy[2 * pp + 1] = 0.f;
+              fz[2 * pp] = fz[2 * pp + 1] = 0.f;
+              if (r < nj) {  // uniform across the warp
+                const float4 A = sh_xq[wib][r];      // x0 x1 y0 y1
+                const float4 B = sh_xq[wib][r + 1];  // z0 z1 q0 q1
+                const int2 tj = *reinterpret_cast<const int2 *>(&sh_tj[wib][r]);
+                const F2 dx = xi2x - f2(A.x, A.y), dy = xi2y - f2(A.z, A.w),
+                         dz = xi2z - f2(B.x, B.y);
+                const F2 r2raw = fma2(dz, dz, fma2(dy, dy, dx * dx));
+                bool in0 = f2lo(r2raw) < st.roff2;
+                bool in1 = r + 1 < nj && f2hi(r2raw) < st.roff2;
+                if (EXCL) {
+                  in0 = in0 && !((excl >> (tj.x >> 16)) & 1u);
+                  in1 = in1 && !((excl >> (tj.y >> 16)) & 1u);
+                }
+                const float2 cc0 = vrow[tj.x & 0xffff], cc1 = vrow[tj.y & 0xffff];
+                const F2 f = pair_force2<ENERGY>(st, r2raw, in0, in1, qi2 * f2(B.z, B.w), cc0,
+                                                 cc1, e_elec, e_vdw);
+                const F2 gx = f * dx, gy = f * dy, gz = f * dz;
+                if (VIRIAL) {
+                  vw2[0] = fma2(gx, dx, vw2[0]);
+                  vw2[1] = fma2(gx, dy, vw2[1]);
+                  vw2[2] = fma2(gx, dz, vw2[2]);
+                  vw2[3] = fma2(gy, dy, vw2[3]);
+                  vw2[4] = fma2(gy, dz, vw2[4]);
+                  vw2[5] = fma2(gz, dz, vw2[5]);
+                }
+                fi2x = fi2x + gx;
+                fi2y = fi2y + gy;
+                fi2z = fi2z + gz;
+                fx[2 * pp] = f2lo(gx);
+                fx[2 * pp + 1] = f2hi(gx);
+                fy[2 * pp] = f2lo(gy);
+                fy[2 * pp + 1] = f2hi(gy);
+                fz[2 * pp] = f2lo(gz);
+                fz[2 * pp + 1] = f2hi(gz);
               }
-              fi2x = fi2x + gx;
-              fi2y = fi2y + gy;
-              fi2z = fi2z + gz;
-              fx[2 * pp] = f2lo(gx);
-              fx[2 * pp + 1] = f2hi(gx);
-              fy[2 * pp] = f2lo(gy);
-              fy[2 * pp + 1] = f2hi(gy);
-              fz[2 * pp] = f2lo(gz);
-              fz[2 * pp + 1] = f2hi(gz);
+            }
+            // the sums hold the gradient on i of each pair: the j-atom's is minus it
+            const float rx = transpose_reduce8(fx, lane);
+            const float ry = transpose_reduce8(fy, lane);
+            const float rz = transpose_reduce8(fz, lane);
+            if ((lane & 3) == b) {
+              fjx = -rx;
+              fjy = -ry;
+              fjz = -rz;
             }
           }
-          // the sums hold the gradient on i of each pair: the j-atom's is minus it
-          const float rx = transpose_reduce8(fx, lane);
-          const float ry = transpose_reduce8(fy, lane);
-          const float rz = transpose_reduce8(fz, lane);
-          if ((lane & 3) == b) {
-            fjx = -rx;
-            fjy = -ry;
-            fjz = -rz;
-          }
-        }
+        };
+        if (__any_sync(0xffffffffu, excl != 0u)) batches(std::true_type{});
+        else batches(std::false_type{});
       } else for (int b = 0; b < nbatch; ++b) {
         Acc fx[8], fy[8], fz[8];
 #pragma unroll
