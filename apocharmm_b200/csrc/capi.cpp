@@ -435,7 +435,8 @@ extern "C" apo_status apo_charmm_context_set_coordinates_xyz(apo_charmm_context 
     APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
     APO_RETURN_IF(require_ptr(xyz, fn, "xyz"));
     if (len != 3 * (size_t)c->object->getNumAtoms()) return invalid(fn, "len must be 3*N");
-    c->object->setCoordinatesXyz(xyz);
+    // the list is rebuilt before the next force evaluation or MD segment
+    c->object->setCoordinatesXyz(xyz, 0, -1, /*rebuild=*/false);
     return APO_STATUS_OK;
   }, fn);
 }
@@ -585,6 +586,7 @@ extern "C" apo_status apo_charmm_context_get_list_pairs(int *pairs, const size_t
     APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
     if (!(radius > 0.0)) return invalid(fn, "radius must be positive");
     size_t count = 0;
+    c->object->ensureNeighborList();  // coordinates set since the last build
     for_each_list_pair(*c->object->getForceManager(), c->object->stream(), radius, [&](int i, int j, int, bool excluded) {
       if (pairs && 3 * (count + 1) <= len) {
         pairs[3 * count] = i;
@@ -608,6 +610,7 @@ extern "C" apo_status apo_charmm_context_get_neighbor_pairs(int *pairs, const si
     APO_RETURN_IF(require_ptr(num_pairs, fn, "num_pairs"));
     APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
     size_t count = 0;
+    c->object->ensureNeighborList();  // coordinates set since the last build
     for_each_list_pair(*c->object->getForceManager(), c->object->stream(), radius, [&](int i, int j, int sc, bool excluded) {
       if (excluded) return;
       if (pairs && 3 * (count + 1) <= len) {
@@ -712,6 +715,7 @@ extern "C" apo_status apo_charmm_context_get_list_counts(int *slots, int *tiles,
     APO_RETURN_IF(require_ptr(tiles, fn, "tiles"));
     APO_RETURN_IF(require_ptr(work, fn, "work_items"));
     APO_RETURN_IF(require_handle(c, fn, "CharmmContext"));
+    c->object->ensureNeighborList();
     auto &nl = c->object->getForceManager()->neighborList();
     nl.sync_counts(c->object->stream());
     *slots = nl.h_counts[0];

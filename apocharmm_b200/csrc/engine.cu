@@ -1110,6 +1110,14 @@ void CharmmContext::ensureNeighborList() {
   }
 }
 
+void CharmmContext::ensureListBuffers() {
+  if (!m_HasCoords) throw std::runtime_error("coordinates not set");
+  if (!m_Fm->isListBuilt()) {
+    resetNeighborList(m_Stream);
+    APO_CUDA(cudaStreamSynchronize(m_Stream));
+  }
+}
+
 void CharmmContext::calculateForces(bool reset, bool calcEnergy, bool calcVirial) {
   if (!m_HasCoords) throw std::runtime_error("calculateForces: coordinates not set");
   if (reset || m_ListStale) resetNeighborList(m_Stream);

@@ -321,6 +321,9 @@ class CharmmContext {
   // rebuild now (synchronously usable, outside any capture) if the list was
   // never built or coordinates were loaded without a rebuild
   void ensureNeighborList();
+  // the list's buffers exist (the first build sizes them, synchronously); a
+  // list that is merely stale is left for the caller's next rebuild
+  void ensureListBuffers();
   void calculateForces(bool reset, bool calcEnergy, bool calcVirial);
   double calculatePotentialEnergy(bool reset, bool print);
 

@@ -988,8 +988,11 @@ void CudaIntegrator::propagate(int numSteps) {
   cudaStream_t s = m_Ctx->stream();
   IntegratorState &S = *m_S;
   auto fm = m_Ctx->getForceManager();
-  // the first list build sizes the buffers synchronously: never inside a capture
-  m_Ctx->ensureNeighborList();
+  // the first list build sizes the buffers synchronously: never inside a
+  // capture; a list made stale by new coordinates is rebuilt by the first
+  // segment, which starts with a rebuild (an overflow there is grown and
+  // the segment run again, below)
+  m_Ctx->ensureListBuffers();
   const long long step0 = m_Step;
   const long long dev0 = deviceStep();
   long long done = 0;

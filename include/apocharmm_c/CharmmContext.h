@@ -43,6 +43,8 @@ APOCHARMM_C_API apo_status apo_charmm_context_get_energy_components(double *ener
  * with calc_virial (or of calculate_potential_energy); len >= 9 */
 APOCHARMM_C_API apo_status apo_charmm_context_get_virial(double *virial, const size_t len, apo_charmm_context *context);
 APOCHARMM_C_API apo_status apo_charmm_context_get_potential_energy(double *energy, apo_charmm_context *context);
+/* N x 3 doubles; the neighbour list is rebuilt before the next force
+ * evaluation, list query or MD segment (an MD segment starts with one) */
 APOCHARMM_C_API apo_status apo_charmm_context_set_coordinates_xyz(apo_charmm_context *context, const double *xyz, const size_t len);
 APOCHARMM_C_API apo_status apo_charmm_context_get_coordinates(double *xyz, const size_t len, apo_charmm_context *context);
 APOCHARMM_C_API apo_status apo_charmm_context_set_velocities(apo_charmm_context *context, const double *v, const size_t len);
