@@ -200,6 +200,46 @@ void Server::reform() {
     for (auto &kv : carried) m_Batch->saveState(in_old[kv.first], m_Carry.p + kv.second);
     m_Batch.reset();  // the old batch's memory is free before the new one is built
   }
+  // members that have never run: if the new batch cannot be built (a
+  // request whose system is invalid or does not fit in memory), they are
+  // answered with the error and the batch is built again without them
+  std::map<int, bool> fresh;
+  for (auto &j : m_Active)
+    if (!j->started) fresh[j->id] = true;
+  for (;;) {
+    try {
+      build(carried);
+      break;
+    } catch (const std::exception &e) {
+      m_Batch.reset();
+      std::vector<std::shared_ptr<Job>> keep, bad;
+      for (auto &j : m_Active) (fresh.count(j->id) ? bad : keep).push_back(j);
+      if (bad.empty()) throw;  // not a new request's doing: the server stops
+      for (auto &j : bad) {
+        ServeResult r;
+        r.kind = j->req.kind;
+        r.status = 2;
+        r.error = std::string("Server: the batch could not take this request: ") + e.what();
+        finish(j, std::move(r));
+      }
+      fresh.clear();
+      m_Active.swap(keep);
+      cudaGetLastError();  // a failed allocation leaves no sticky error; clear the last one
+      if (m_Active.empty()) {
+        m_BatchJobs.clear();
+        m_Dirty = false;
+        return;
+      }
+    }
+  }
+  m_Dirty = false;
+  std::lock_guard<std::mutex> lk(m_Mu);
+  ++m_Stats.rebuilds;
+  m_Stats.reform_s += seconds_since(t0);
+}
+
+// builds the batch around m_Active, continuing systems from m_Carry
+void Server::build(const std::map<int, size_t> &carried) {
   m_BatchJobs = m_Active;
   m_Batch.reset(new Batch(m_Order, 8, m_Precise));
   for (auto &j : m_Active) m_Batch->addSystem(j->req.spec);
@@ -228,10 +268,6 @@ void Server::reform() {
     stop.push_back(j->req.kind == 1 ? 0 : j->req.steps - j->done);
   }
   m_Batch->integrator()->setSystemLimits(rng0, stop);
-  m_Dirty = false;
-  std::lock_guard<std::mutex> lk(m_Mu);
-  ++m_Stats.rebuilds;
-  m_Stats.reform_s += seconds_since(t0);
 }
 
 void Server::loop() {

@@ -100,6 +100,7 @@ class Server {
   void evaluateEnergies();
   void markIdle();
   void reform();
+  void build(const std::map<int, size_t> &carried);
   void finish(const std::shared_ptr<Job> &j, ServeResult &&r);
 
   double m_Fraction;

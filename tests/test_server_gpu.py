@@ -92,3 +92,28 @@ def test_md_result_moves_and_stays_bound(tmp_path):
     with pytest.raises(Exception):
         srv.poll(rid)
     srv.close()
+
+
+def test_a_request_that_cannot_join_fails_alone(tmp_path):
+    """A request whose coordinates are not finite cannot join the batch: it
+    is answered with an error, while the request already running goes on
+    and ends as it does alone."""
+    systems, xs, handles = _systems(tmp_path)
+    good_req = (1, 0, 20000, 12)
+    alone = api.Server(hbm_fraction=0.5, seed=99)
+    ref = _result(alone, _submit(alone, systems, xs, handles, good_req), 0)
+    alone.close()
+    srv = api.Server(hbm_fraction=0.5, seed=99)
+    good = _submit(srv, systems, xs, handles, good_req)
+    time.sleep(0.3)  # the good request is running by now
+    bad_x = np.array(xs[0], copy=True)
+    bad_x[5, 1] = np.nan
+    s = systems[0]
+    bad = srv.submit(0, handles[0][0], handles[0][1], s.box, s.settings, bad_x, 11, 60)
+    assert srv.wait(bad, 300.0) == api.Server.FAILED
+    got = _result(srv, good, 0)
+    assert np.array_equal(got[0], ref[0]) and np.array_equal(got[1], ref[1])
+    # the server still takes requests
+    again = _submit(srv, systems, xs, handles, (0, 0, 60, 11))
+    assert srv.wait(again, 300.0) == api.Server.DONE
+    srv.close()
