@@ -357,32 +357,26 @@ __global__ void __launch_bounds__(128) spread_kernel(const float4 *__restrict__ 
   const int nslot = counts ? counts[0] : 0;
   const int s0 = blockIdx.x * 32;
   if (s0 >= nslot) return;
-  if (threadIdx.x < 32) {
-    const int s = s0 + threadIdx.x;
-    float q = 0.f;
+  // the splines of the 32 atoms, one thread per (dimension, atom)
+  if (threadIdx.x < 96) {
+    const int dim = threadIdx.x >> 5, a = threadIdx.x & 31;
+    const int s = s0 + a;
+    float q = 0.f, w = 0.f;
+    int i0 = 0;
     if (s < nslot) {
       const float4 p = xyzq[s];
       const double3 g = global_pos(p, origin, s);
       q = p.w;
-      float th[ORDER], dth[ORDER], w;
-      int i0;
-      anchor(g.x, d.rLx, d.nx, i0, w);
-      bspline<ORDER>(w, th, dth);
-      sh_i[0][threadIdx.x] = i0;
-#pragma unroll
-      for (int k = 0; k < ORDER; ++k) sh_th[0][threadIdx.x][k] = th[k];
-      anchor(g.y, d.rLy, d.ny, i0, w);
-      bspline<ORDER>(w, th, dth);
-      sh_i[1][threadIdx.x] = i0;
-#pragma unroll
-      for (int k = 0; k < ORDER; ++k) sh_th[1][threadIdx.x][k] = th[k];
-      anchor(g.z, d.rLz, d.nz, i0, w);
-      bspline<ORDER>(w, th, dth);
-      sh_i[2][threadIdx.x] = i0;
-#pragma unroll
-      for (int k = 0; k < ORDER; ++k) sh_th[2][threadIdx.x][k] = th[k];
+      if (dim == 0) anchor(g.x, d.rLx, d.nx, i0, w);
+      else if (dim == 1) anchor(g.y, d.rLy, d.ny, i0, w);
+      else anchor(g.z, d.rLz, d.nz, i0, w);
     }
-    sh_q[threadIdx.x] = q;
+    float th[ORDER], dth[ORDER];
+    bspline<ORDER>(w, th, dth);
+    sh_i[dim][a] = i0;
+#pragma unroll
+    for (int k = 0; k < ORDER; ++k) sh_th[dim][a][k] = th[k];
+    if (dim == 0) sh_q[a] = q;
   }
   __syncthreads();
   for (int k = threadIdx.x; k < 32 * P3; k += blockDim.x) {
