@@ -269,111 +269,111 @@ __device__ void finish_temperature(const Common &c, double ke0, double ke1) {
 //   delta = alpha*delta_prev - dt^2/m/(1+g/2) * (grad + sqrt(2 g kT m)/dt * xi)
 //   x += delta; constrain; delta = x - x_old;
 //   v = sqrt(1+g/2)/(2 dt) * (delta + delta_prev)
+// Four lanes per constraint group (a water, an X-H cluster, a run of free
+// atoms): each lane loads, draws the noise for and moves one atom, the
+// lanes exchange the group's old and new positions by shuffles and each
+// applies the group's constraint to the whole group (the same arithmetic,
+// in the same order, as one thread per group), then keeps and stores its own
+// atom.  Four times the threads of one per group: the step is bound by the
+// latency of its dependent loads and arithmetic, not by throughput.
+__device__ __forceinline__ d3 pick(const d3 (&v)[4], int k) {
+  return k == 0 ? v[0] : (k == 1 ? v[1] : (k == 2 ? v[2] : v[3]));
+}
+
 __global__ void __launch_bounds__(kThreads) langevin_kernel(Common c, double gamma, double kbt,
                                                             unsigned long long seed) {
-  if (*c.err) return;  // the same word for every block: the whole grid returns
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  // the error word is the same for every block; it is looked at before the
+  // first store, after the loads are under way
+  const unsigned err = *c.err;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int g = t >> 2, k = t & 3;
+  const int base = (threadIdx.x & 31) & ~3;
   const double dt = c.dt, dt2 = dt * dt;
   const double hg = 0.5 * gamma, denom = 1.0 / (1.0 + hg), alpha = (1.0 - hg) * denom;
   const double vfac = 0.5 * sqrt(1.0 + hg) / dt, idt = 1.0 / dt;
   double ke0 = 0.0, ke1 = 0.0;
   const unsigned long long pos = c.sc->rngpos;
-  bool run = g < c.ngroups;
-  if (run && c.sys_stop) {  // a group never spans two systems
-    int at0[4];
-    group_atoms(c, g, at0);
-    const int sy = c.sys_of_atom[at0[0]];
-    if (c.sc->step >= c.sys_stop[sy]) {
-      run = false;
-      // the gradient slots are consumed all the same
-      int at[4];
-      const int m = group_atoms(c, g, at);
-      for (int k = 0; k < m; ++k) take_grad(c.force, c.stride, c.glo2loc[at[k]]);
+  const bool gvalid = g < c.ngroups;
+  int at[4] = {0, 0, 0, 0};
+  int m = 0;
+  int2 meta = make_int2(0, 0);
+  if (gvalid) {
+    m = group_atoms(c, g, at);
+    meta = c.gmeta[g];
+  }
+  const bool mine = gvalid && k < m;
+  const int a = k == 0 ? at[0] : (k == 1 ? at[1] : (k == 2 ? at[2] : at[3]));
+  bool run = gvalid;
+  if (run && c.sys_stop && c.sc->step >= c.sys_stop[c.sys_of_atom[at[0]]])
+    run = false;  // a system past its step limit: its gradient slots are consumed all the same
+  double4 x = make_double4(0.0, 0.0, 0.0, 0.0), vm = x, dpv = x, so = x;
+  int slot = 0;
+  if (mine) {
+    x = c.coords[a];
+    vm = c.vel[a];
+    dpv = c.dprev[a];
+    slot = c.glo2loc[a];
+  }
+  long long gi0 = 0, gi1 = 0, gi2 = 0;
+  if (mine) {
+    gi0 = c.force[slot];
+    gi1 = c.force[c.stride + slot];
+    gi2 = c.force[2 * c.stride + slot];
+    so = c.slot_off[slot];
+  }
+  if (err) return;
+  const d3 o = xyz(x), dp = xyz(dpv);
+  const double im = vm.w;
+  d3 n = o;
+  if (mine) {  // cleared for the next force evaluation
+    c.force[slot] = 0;
+    c.force[c.stride + slot] = 0;
+    c.force[2 * c.stride + slot] = 0;
+    if (run) {
+      const d3 gr = mk((double)gi0 * kInvForceScale, (double)gi1 * kInvForceScale,
+                       (double)gi2 * kInvForceScale);
+      curandStatePhilox4_32_10_t st;
+      unsigned long long p = pos;
+      if (c.sys_seed) {  // a system's own stream, the same alone or among others
+        const int sy = c.sys_of_atom[a];
+        curand_init(seed ^ c.sys_seed[sy], (unsigned long long)(a - c.atom_off[sy]), 0ull, &st);
+        if (c.sys_rng0) p += c.sys_rng0[sy];
+      } else {
+        curand_init(seed, (unsigned long long)a, 0ull, &st);
+      }
+      skipahead(p, &st);
+      const float4 rn = curand_normal4(&st);
+      const double rdf = sqrt(2.0 * gamma * kbt / im) / dt;
+      const double fact = dt2 * im * denom;
+      const d3 f = gr + rdf * mk(rn.x, rn.y, rn.z);
+      n = o + (alpha * dp - fact * f);
     }
   }
-  if (run) {
-    // all loads of the group first (every level of the chain atom -> slot ->
-    // gradient is issued for the whole group at once), then the arithmetic,
-    // then the stores: the kernel is bound by memory latency, not by math
-    int at[4];
-    const int m = group_atoms(c, g, at);
-    const int2 meta = c.gmeta[g];
-    d3 o[4], n[4], dp[4], gr[4];
-    double im[4], qa[4];
-    int slot[4];
+  // the group's old and new positions in every lane of the group
+  d3 og[4], ng[4];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      if (k < m) {
-        const int a = at[k];
-        const double4 x = c.coords[a];
-        o[k] = xyz(x);
-        qa[k] = x.w;
-        im[k] = c.vel[a].w;
-        dp[k] = xyz(c.dprev[a]);
-        slot[k] = c.glo2loc[a];
-      }
-    }
-    long long gi[4][3];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      if (k < m) {
-        gi[k][0] = c.force[slot[k]];
-        gi[k][1] = c.force[c.stride + slot[k]];
-        gi[k][2] = c.force[2 * c.stride + slot[k]];
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      if (k < m) {  // cleared for the next force evaluation
-        c.force[slot[k]] = 0;
-        c.force[c.stride + slot[k]] = 0;
-        c.force[2 * c.stride + slot[k]] = 0;
-        gr[k] = mk((double)gi[k][0] * kInvForceScale, (double)gi[k][1] * kInvForceScale,
-                   (double)gi[k][2] * kInvForceScale);
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      if (k < m) {
-        const int a = at[k];
-        curandStatePhilox4_32_10_t st;
-        unsigned long long p = pos;
-        if (c.sys_seed) {  // a system's own stream, the same alone or among others
-          const int sy = c.sys_of_atom[a];
-          curand_init(seed ^ c.sys_seed[sy], (unsigned long long)(a - c.atom_off[sy]), 0ull, &st);
-          if (c.sys_rng0) p += c.sys_rng0[sy];
-        } else {
-          curand_init(seed, (unsigned long long)a, 0ull, &st);
-        }
-        skipahead(p, &st);
-        const float4 rn = curand_normal4(&st);
-        const double rdf = sqrt(2.0 * gamma * kbt / im[k]) / dt;
-        const double fact = dt2 * im[k] * denom;
-        const d3 f = gr[k] + rdf * mk(rn.x, rn.y, rn.z);
-        n[k] = o[k] + (alpha * dp[k] - fact * f);
-      }
-    }
-    apply_constraint(meta.x, m, o, n, c.sk, c.shake_p, meta.y);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      if (k < m) {
-        const int a = at[k];
-        const d3 d = n[k] - o[k];
-        const d3 v = vfac * (d + dp[k]);
-        const double mass = 1.0 / im[k];
-        const d3 u1 = idt * dp[k], u2 = idt * d;
-        const double kon = 0.5 * mass * dot(v, v);
-        ke0 += (0.5 * mass * dot(u1, u1) + kon + 0.5 * mass * dot(u2, u2)) / 3.0;
-        ke1 += kon;
-        c.vel[a] = make_double4(v.x, v.y, v.z, im[k]);
-        c.dprev[a] = make_double4(d.x, d.y, d.z, 0.0);
-        c.coords[a] = make_double4(n[k].x, n[k].y, n[k].z, qa[k]);
-        c.xyzq[a] = make_float4((float)n[k].x, (float)n[k].y, (float)n[k].z, (float)qa[k]);
-        const double4 so = c.slot_off[slot[k]];
-        c.xyzq_s[slot[k]] = make_float4((float)(n[k].x + so.x), (float)(n[k].y + so.y),
-                                        (float)(n[k].z + so.z), (float)qa[k]);
-      }
-    }
+  for (int q = 0; q < 4; ++q) {
+    og[q] = mk(__shfl_sync(0xffffffffu, o.x, base + q), __shfl_sync(0xffffffffu, o.y, base + q),
+               __shfl_sync(0xffffffffu, o.z, base + q));
+    ng[q] = mk(__shfl_sync(0xffffffffu, n.x, base + q), __shfl_sync(0xffffffffu, n.y, base + q),
+               __shfl_sync(0xffffffffu, n.z, base + q));
+  }
+  if (run) apply_constraint(meta.x, m, og, ng, c.sk, c.shake_p, meta.y);
+  if (mine && run) {
+    const d3 nk = pick(ng, k);
+    const d3 d = nk - o;
+    const d3 v = vfac * (d + dp);
+    const double mass = 1.0 / im;
+    const d3 u1 = idt * dp, u2 = idt * d;
+    const double kon = 0.5 * mass * dot(v, v);
+    ke0 = (0.5 * mass * dot(u1, u1) + kon + 0.5 * mass * dot(u2, u2)) / 3.0;
+    ke1 = kon;
+    c.vel[a] = make_double4(v.x, v.y, v.z, im);
+    c.dprev[a] = make_double4(d.x, d.y, d.z, 0.0);
+    c.coords[a] = make_double4(nk.x, nk.y, nk.z, x.w);
+    c.xyzq[a] = make_float4((float)nk.x, (float)nk.y, (float)nk.z, (float)x.w);
+    c.xyzq_s[slot] = make_float4((float)(nk.x + so.x), (float)(nk.y + so.y),
+                                 (float)(nk.z + so.z), (float)x.w);
   }
   block_partials(ke0, ke1, c.partials);
   if (is_last_block(&c.sc->counter)) {
@@ -733,7 +733,7 @@ struct IntegratorState {
   DeviceArray<double> partials;
   int ngroups = 0, natom = 0;
   Common c{};
-  int blocks_groups = 0, blocks_atoms = 0;
+  int blocks_groups = 0, blocks_atoms = 0, blocks_lanes = 0;  // lanes: 4 per group
   // the error word after each of the last two segments, copied to pinned
   // host memory behind the segment, and the events that say it has landed
   unsigned *h_err = nullptr;
@@ -861,9 +861,10 @@ void CudaIntegrator::buildGroups() {
   APO_CUDA(cudaMemcpy(S.sc.p, &z, sizeof(z), cudaMemcpyHostToDevice));
   S.blocks_groups = (S.ngroups + kThreads - 1) / kThreads;
   S.blocks_atoms = (n + kThreads - 1) / kThreads;
-  if (std::max(S.blocks_groups, S.blocks_atoms) > kMaxBlocks * 64)
+  S.blocks_lanes = (4 * S.ngroups + kThreads - 1) / kThreads;
+  if (std::max(S.blocks_lanes, S.blocks_atoms) > kMaxBlocks * 64)
     throw std::invalid_argument("system too large for the integrator's reduction buffer");
-  S.partials.alloc((size_t)4 * std::max(S.blocks_groups, S.blocks_atoms) + 8);
+  S.partials.alloc((size_t)4 * std::max(S.blocks_lanes, S.blocks_atoms) + 8);
   Common &c = S.c;
   c.sys_of_atom = nullptr;
   c.atom_off = nullptr;
@@ -1239,7 +1240,7 @@ void CudaLangevinThermostatIntegrator::stepKernels(cudaStream_t s) {
   IntegratorState &S = *m_S;
   const double gamma = m_Dt * kTimfac * m_Friction;
   const double kbt = kBoltz * m_RefT;
-  langevin_kernel<<<S.blocks_groups, kThreads, 0, s>>>(S.c, gamma, kbt, m_Seed);
+  langevin_kernel<<<S.blocks_lanes, kThreads, 0, s>>>(S.c, gamma, kbt, m_Seed);
   APO_LAUNCH_CHECK();
 }
 
