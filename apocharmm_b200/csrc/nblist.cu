@@ -327,12 +327,25 @@ __global__ void tiles_kernel(const NbSysDims *__restrict__ sysd, const int *__re
   const float rl2 = d.rlist * d.rlist;
   int gi = 0;
   int nexcl_begin = 0, nexcl_end = 0;
+  // the slots of this lane's first kExclSlots exclusion partners, loaded once
+  // for all tiles (the rest, if any, are read again for every tile)
+  constexpr int kExclSlots = 16;
+  int ex_slot[kExclSlots];
+#pragma unroll
+  for (int q = 0; q < kExclSlots; ++q) ex_slot[q] = -1;
   if (FILL) {
     gi = perm[ic * kTile + lane];
     if (gi >= 0) {
       nexcl_begin = excl_ptr[gi];
       nexcl_end = excl_ptr[gi + 1];
     }
+    int eidx[kExclSlots];
+#pragma unroll
+    for (int q = 0; q < kExclSlots; ++q)
+      eidx[q] = nexcl_begin + q < nexcl_end ? excl_idx[nexcl_begin + q] : -1;
+#pragma unroll
+    for (int q = 0; q < kExclSlots; ++q)
+      if (eidx[q] >= 0) ex_slot[q] = glo2loc[eidx[q]];
   }
   int count = 0;
   const int base_tile = FILL ? tile_start[ic] : 0;
@@ -376,11 +389,12 @@ __global__ void tiles_kernel(const NbSysDims *__restrict__ sysd, const int *__re
             ++count;
             // topological exclusions of i-lane `lane` against this j-cluster
             unsigned word = 0u;
-            if (gi >= 0) {
-              for (int e = nexcl_begin; e < nexcl_end; ++e) {
-                int lp = glo2loc[excl_idx[e]];
-                if ((lp >> 5) == tjc) word |= 1u << (lp & 31);
-              }
+#pragma unroll
+            for (int q = 0; q < kExclSlots; ++q)
+              if (ex_slot[q] >= 0 && (ex_slot[q] >> 5) == tjc) word |= 1u << (ex_slot[q] & 31);
+            for (int e = nexcl_begin + kExclSlots; e < nexcl_end; ++e) {
+              int lp = glo2loc[excl_idx[e]];
+              if ((lp >> 5) == tjc) word |= 1u << (lp & 31);
             }
             int midx = -1;
             if (__any_sync(0xffffffffu, word != 0u)) {
