@@ -51,23 +51,40 @@ __global__ void xyzq_to_state_kernel(int n, const float4 *__restrict__ xq,
   c[g] = make_double4(p.x, p.y, p.z, p.w);
 }
 
-// one warp per bonded component: centroid by a warp reduction, then the
-// whole component is shifted by one box length per axis where the centroid
-// left [-L/2, L/2] (src/CharmmContext.cu:276-372)
+// one bonded component moved back into the box: its centroid, and a shift
+// of one box length per axis where the centroid left [-L/2, L/2]
+// (src/CharmmContext.cu:276-372).  Components of more than
+// kSmallComponent atoms come first and take a warp each (centroid by a warp
+// reduction); the rest take one thread each.
+constexpr int kSmallComponent = 8;
+
+__device__ __forceinline__ void component_box(const int2 g, const int *sys_of_atom,
+                                              const double4 *boxes, double &Lx, double &Ly,
+                                              double &Lz) {
+  if (sys_of_atom) {  // several systems: this component's own box
+    const double4 b = boxes[sys_of_atom[g.x]];
+    Lx = b.x;
+    Ly = b.y;
+    Lz = b.z;
+  }
+}
+
+__device__ __forceinline__ double image_shift(double gc, double L) {
+  return gc < -0.5 * L ? L : (gc > 0.5 * L ? -L : 0.0);
+}
+
 __global__ void image_centering_kernel(double4 *__restrict__ c, float4 *__restrict__ xq,
-                                       const int2 *__restrict__ groups, int ng, double Lx,
-                                       double Ly, double Lz, const int *__restrict__ sys_of_atom,
+                                       const int2 *__restrict__ groups, int ng, int nbig,
+                                       int big_blocks, double Lx0, double Ly0, double Lz0,
+                                       const int *__restrict__ sys_of_atom,
                                        const double4 *__restrict__ boxes) {
-  const int lane = threadIdx.x & 31;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < ng; i += nwarps) {
+  double Lx = Lx0, Ly = Ly0, Lz = Lz0;
+  if ((int)blockIdx.x < big_blocks) {  // a warp per large component
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= nbig) return;
     const int2 g = groups[i];
-    if (sys_of_atom) {  // several systems: this component's own box
-      const double4 b = boxes[sys_of_atom[g.x]];
-      Lx = b.x;
-      Ly = b.y;
-      Lz = b.z;
-    }
+    component_box(g, sys_of_atom, boxes, Lx, Ly, Lz);
     double gx = 0, gy = 0, gz = 0;
     for (int j = g.x + lane; j <= g.y; j += 32) {
       gx += c[j].x;
@@ -78,12 +95,8 @@ __global__ void image_centering_kernel(double4 *__restrict__ c, float4 *__restri
     gy = warp_sum(gy);
     gz = warp_sum(gz);
     const double inv = 1.0 / (double)(g.y - g.x + 1);
-    gx *= inv;
-    gy *= inv;
-    gz *= inv;
-    const double sx = gx < -0.5 * Lx ? Lx : (gx > 0.5 * Lx ? -Lx : 0.0);
-    const double sy = gy < -0.5 * Ly ? Ly : (gy > 0.5 * Ly ? -Ly : 0.0);
-    const double sz = gz < -0.5 * Lz ? Lz : (gz > 0.5 * Lz ? -Lz : 0.0);
+    const double sx = image_shift(gx * inv, Lx), sy = image_shift(gy * inv, Ly),
+                 sz = image_shift(gz * inv, Lz);
     if (sx != 0.0 || sy != 0.0 || sz != 0.0) {
       for (int j = g.x + lane; j <= g.y; j += 32) {
         c[j].x += sx;
@@ -92,6 +105,40 @@ __global__ void image_centering_kernel(double4 *__restrict__ c, float4 *__restri
         xq[j].x += (float)sx;
         xq[j].y += (float)sy;
         xq[j].z += (float)sz;
+      }
+    }
+    return;
+  }
+  const int i = nbig + ((int)blockIdx.x - big_blocks) * blockDim.x + threadIdx.x;
+  if (i >= ng) return;  // a thread per small component
+  const int2 g = groups[i];
+  component_box(g, sys_of_atom, boxes, Lx, Ly, Lz);
+  double4 a[kSmallComponent];
+  const int m = g.y - g.x + 1;
+  double gx = 0, gy = 0, gz = 0;
+#pragma unroll
+  for (int k = 0; k < kSmallComponent; ++k) {
+    if (k < m) {
+      a[k] = c[g.x + k];
+      gx += a[k].x;
+      gy += a[k].y;
+      gz += a[k].z;
+    }
+  }
+  const double inv = 1.0 / (double)m;
+  const double sx = image_shift(gx * inv, Lx), sy = image_shift(gy * inv, Ly),
+               sz = image_shift(gz * inv, Lz);
+  if (sx != 0.0 || sy != 0.0 || sz != 0.0) {
+#pragma unroll
+    for (int k = 0; k < kSmallComponent; ++k) {
+      if (k < m) {
+        const int j = g.x + k;
+        c[j] = make_double4(a[k].x + sx, a[k].y + sy, a[k].z + sz, a[k].w);
+        float4 f = xq[j];
+        f.x += (float)sx;
+        f.y += (float)sy;
+        f.z += (float)sz;
+        xq[j] = f;
       }
     }
   }
@@ -109,13 +156,22 @@ __global__ void coords_to_xyzq_kernel(const double4 *__restrict__ c, float4 *__r
 }  // namespace
 
 void launch_image_centering(double4 *coords, float4 *xyzq, const int2 *groups, int ngroups,
-                            double Lx, double Ly, double Lz, cudaStream_t s,
+                            int nbig, double Lx, double Ly, double Lz, cudaStream_t s,
                             const int *sys_of_atom, const double4 *boxes) {
   if (ngroups <= 0) return;
-  const int blocks = std::min((ngroups + 3) / 4, 148 * 16);
-  image_centering_kernel<<<blocks, 128, 0, s>>>(coords, xyzq, groups, ngroups, Lx, Ly, Lz,
-                                                 sys_of_atom, boxes);
+  const int big_blocks = (nbig + 3) / 4;  // 4 warps a block
+  const int small_blocks = (ngroups - nbig + 127) / 128;
+  image_centering_kernel<<<big_blocks + small_blocks, 128, 0, s>>>(
+      coords, xyzq, groups, ngroups, nbig, big_blocks, Lx, Ly, Lz, sys_of_atom, boxes);
   APO_LAUNCH_CHECK();
+}
+
+int order_components(std::vector<int2> &groups, int small) {
+  std::stable_partition(groups.begin(), groups.end(),
+                        [small](const int2 &g) { return g.y - g.x + 1 > small; });
+  int nbig = 0;
+  for (const int2 &g : groups) nbig += g.y - g.x + 1 > small ? 1 : 0;
+  return nbig;
 }
 
 void launch_coords_to_xyzq(const double4 *coords, float4 *xyzq, int n, cudaStream_t s) {
@@ -830,7 +886,11 @@ CharmmContext::CharmmContext(std::shared_ptr<ForceManager> fm) : m_Fm(std::move(
   m_VelMass.upload(vm);
   m_Coords.upload(c);
   launch_coords_to_xyzq(m_Coords.p, m_Xyzq.p, m_N, m_Stream);
-  m_Groups.upload(t.groups);
+  {  // large components first (a warp each), then the small ones (a thread each)
+    std::vector<int2> groups = t.groups;
+    m_NumBigGroups = order_components(groups, kSmallComponent);
+    m_Groups.upload(groups);
+  }
   m_Fm->setStateCoordinates(m_Coords.p);
   std::random_device rd;
   m_Seed = rd();
@@ -1090,10 +1150,11 @@ double CharmmContext::computeTemperature() {
 void CharmmContext::imageCentering(cudaStream_t s) {
   auto b = m_Fm->getBoxDimensions();
   if (m_Fm->isMulti())
-    launch_image_centering(m_Coords.p, m_Xyzq.p, m_Groups.p, (int)m_Groups.n, b[0], b[1], b[2], s,
-                           m_Fm->sysOfAtom(), m_Fm->systemBoxes());
+    launch_image_centering(m_Coords.p, m_Xyzq.p, m_Groups.p, (int)m_Groups.n, m_NumBigGroups,
+                           b[0], b[1], b[2], s, m_Fm->sysOfAtom(), m_Fm->systemBoxes());
   else
-    launch_image_centering(m_Coords.p, m_Xyzq.p, m_Groups.p, (int)m_Groups.n, b[0], b[1], b[2], s);
+    launch_image_centering(m_Coords.p, m_Xyzq.p, m_Groups.p, (int)m_Groups.n, m_NumBigGroups,
+                           b[0], b[1], b[2], s);
 }
 
 void CharmmContext::resetNeighborList(cudaStream_t s) {

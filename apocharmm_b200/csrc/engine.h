@@ -353,12 +353,17 @@ class CharmmContext {
   DeviceArray<double> m_Stage;    // 3N doubles: host transfers
   DeviceArray<int> m_BadAtom;     // first non-finite coordinate, or INT_MAX
   DeviceArray<int2> m_Groups;
+  int m_NumBigGroups = 0;  // leading components taken by a warp each
 };
 
 // device helpers shared with the integrators
+// groups: bonded components (first, last atom), the nbig components of more
+// than kSmallComponent atoms first (order_components sorts them so)
 void launch_image_centering(double4 *coords, float4 *xyzq, const int2 *groups, int ngroups,
-                            double Lx, double Ly, double Lz, cudaStream_t s,
+                            int nbig, double Lx, double Ly, double Lz, cudaStream_t s,
                             const int *sys_of_atom = nullptr, const double4 *boxes = nullptr);
+// stable reorder: components of more than `small` atoms first; returns their count
+int order_components(std::vector<int2> &groups, int small);
 void launch_coords_to_xyzq(const double4 *coords, float4 *xyzq, int n, cudaStream_t s);
 
 }  // namespace apo
