@@ -349,6 +349,27 @@ __global__ void tiles_kernel(const NbSysDims *__restrict__ sysd, const int *__re
   }
   int count = 0;
   const int base_tile = FILL ? tile_start[ic] : 0;
+  // the cluster ranges of the columns in reach, loaded at once by the lanes
+  // (column q of the (2 Rx + 1) x (2 Ry + 1) window by lane q mod 32) and
+  // handed out by shuffles in the loop below; wider windows read them there
+  const int wxn = 2 * Rx + 1, ncols = wxn * (2 * Ry + 1);
+  const bool pre = ncols <= 64;
+  int pre_js[2] = {0, 0}, pre_je[2] = {0, 0};
+  if (pre) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int q = lane + 32 * h;
+      if (q < ncols) {
+        const int yy = cy + q / wxn - Ry, xx = cx + q % wxn - Rx;
+        const int iy = floor_div(yy, d.ncy), ix = floor_div(xx, d.ncx);
+        if (iy >= -1 && iy <= 1 && ix >= -1 && ix <= 1) {
+          const int col = d.col_off + (xx - ix * d.ncx) + d.ncx * (yy - iy * d.ncy);
+          pre_js[h] = col_start[col] / kTile;
+          pre_je[h] = col_start[col + 1] / kTile;
+        }
+      }
+    }
+  }
   for (int dy = -Ry; dy <= Ry; ++dy) {
     int yy = cy + dy;
     int iy = floor_div(yy, d.ncy);
@@ -360,7 +381,15 @@ __global__ void tiles_kernel(const NbSysDims *__restrict__ sysd, const int *__re
       if (ix < -1 || ix > 1) continue;
       int wx = xx - ix * d.ncx;
       int col = d.col_off + wx + d.ncx * wy;
-      int js = col_start[col] / kTile, je = col_start[col + 1] / kTile;
+      int js, je;
+      if (pre) {
+        const int q = (dy + Ry) * wxn + (dx + Rx);
+        js = __shfl_sync(0xffffffffu, q < 32 ? pre_js[0] : pre_js[1], q & 31);
+        je = __shfl_sync(0xffffffffu, q < 32 ? pre_je[0] : pre_je[1], q & 31);
+      } else {
+        js = col_start[col] / kTile;
+        je = col_start[col + 1] / kTile;
+      }
       int ncand = (je - js) * 3;
       for (int b0 = 0; b0 < ncand; b0 += 32) {
         int cand = b0 + lane;
