@@ -8,8 +8,11 @@
  * steps at a time, and re-batched as requests arrive and finish; a system's
  * coordinates, velocities and integrator state stay on the device between
  * segments and carry over exactly when the batch changes, so its result is
- * the same alone and among others.  Energy/force requests are evaluated
- * together in batches of their own.  Results are kept until released.
+ * the same alone and among others.  Topologies are built on a second host
+ * thread as requests arrive.  Energy/force requests join the running batch
+ * and are answered by one force call of it.  A request that cannot join
+ * (invalid coordinates, no device memory) fails alone with the error; the
+ * server goes on.  Results are kept until released.
  * Langevin settings (time step, friction, temperature, noise seed) are the
  * server's; each system's velocities and noise stream come from its seed. */
 #ifndef APOCHARMM_C_SERVER_H
