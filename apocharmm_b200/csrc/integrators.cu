@@ -1185,13 +1185,23 @@ void CudaIntegrator::initializeFromRestartFile(const std::string &path) {
     throw std::invalid_argument("NATOM mismatch in restart file \"" + path + "\"");
   if (r.ndegf != m_Ctx->getDegreesOfFreedom())
     throw std::invalid_argument("NDEGF mismatch in restart file \"" + path + "\"");
-  // a file written with 16 significant digits (the reference's form) need
-  // not give back the last bit of the box
-  const auto &box = fm->getBoxDimensions();
-  for (int k = 0; k < 3; ++k)
-    if (std::fabs(r.box[k] - box[k]) > 1e-12 * std::fabs(box[k]))
-      throw std::invalid_argument("restart file \"" + path + "\" holds another box: set it on "
-                                  "the ForceManager before the integrator is created");
+  // The file's box becomes the context's, as in the reference
+  // (src/CudaLangevinThermostatIntegrator.cu:394): the force manager is set
+  // up again for it (spline order and FFT grid unchanged) and this
+  // integrator's state is built again over the manager's new buffers.  A
+  // file written with 16 significant digits (the reference's form) need not
+  // give back the last bit of a box that is already the same.
+  const auto box = fm->getBoxDimensions();
+  bool other_box = false;
+  for (int k = 0; k < 3; ++k) other_box |= std::fabs(r.box[k] - box[k]) > 1e-12 * std::fabs(box[k]);
+  if (other_box) {
+    fm->setBoxDimensions({r.box[0], r.box[1], r.box[2]});
+    fm->initialize();
+    fm->setStateCoordinates(m_Ctx->coords());
+    clearGraphs();
+    buildGroups();
+    initialize();
+  }
   m_Ctx->setCoordinates(r.xold);
   m_Ctx->setVelocities(r.vel);
   std::vector<double4> d(r.natom);

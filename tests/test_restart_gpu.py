@@ -76,6 +76,36 @@ def test_resumed_run_matches_uninterrupted_run(tmp_path, kind):
     assert it2.getCurrentPropagatedStep() == 100
 
 
+def test_restart_brings_its_box(tmp_path):
+    """A context set up with another box takes the restart file's box, as
+    the reference's initializeFromRestartFile does
+    (src/CudaLangevinThermostatIntegrator.cu:394); with the same FFT grid the
+    resumed run then follows the uninterrupted one bit for bit."""
+    s, keep1 = _context(tmp_path / "a")
+    start = keep1[3].getCoordinates()
+    it1 = _langevin(1234)
+    it1.setCharmmContext(keep1[3])
+    rst = tmp_path / "run.rst"
+    it1.subscribe(api.RestartSubscriber(str(rst), 40))
+    it1.propagate(40)
+    saved = tmp_path / "at40.rst"
+    shutil.copy(rst, saved)
+    it1.propagate(60)
+    x1, v1 = keep1[3].getCoordinates(), keep1[3].getVelocities()
+
+    s2 = water_box(1000, 31.0, seed=3)
+    s2.box = (32.5, 32.5, 32.5)  # a placeholder box
+    keep2 = api.system_context(s2, str(tmp_path / "b"), settings=SMALL)
+    keep2[3].setCoordinates(start)
+    it2 = _langevin(99)
+    it2.setCharmmContext(keep2[3])
+    it2.initializeFromRestartFile(str(saved))
+    it2.propagate(60)
+    x2, v2 = keep2[3].getCoordinates(), keep2[3].getVelocities()
+    assert np.array_equal(x1, x2), np.abs(x1 - x2).max()
+    assert np.array_equal(v1, v2), np.abs(v1 - v2).max()
+
+
 def test_restart_holds_the_state_of_the_report_step(tmp_path):
     s, keep = _context(tmp_path)
     it = _langevin(5)
