@@ -1,15 +1,17 @@
 """The C++ class surface (include/apocharmm/: ForceManager with
 calcForce(xyzq, reset, calcEnergy, calcVirial) / getForces, ForceView
 subscriptions, CudaBondedForce, CudaPMEDirectForce, CudaPMEReciprocalForce,
-CudaNeighborList<32>) compiled into a user program (tests/cpp/force_classes.cu)
-and linked against the library.
+CudaNeighborList<32>, CharmmCrd, CharmmContext, the integrators and the
+subscribers) compiled into user programs (tests/cpp/force_classes.cu,
+tests/cpp/md_classes.cu) and linked against the library.
 
-CPU: every header compiles on its own and the program links.  GPU: the
-program runs on the ethylene-glycol box; the whole field and each part
+CPU: every header compiles on its own and the programs link.  GPU: the
+force program runs on the ethylene-glycol box; the whole field and each part
 match the FP64 oracle at the program's single-precision coordinates, the
 parts add up to the whole in fixed point, a user force subscribed through
 ForceView adds exactly its gradient and energy, and the list's index arrays
-and pairs are consistent."""
+and pairs are consistent.  The MD program's Langevin run ends in the same
+state, bit for bit, as the same run made through the Python API."""
 import glob
 import os
 import shutil
@@ -25,6 +27,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 INC = os.path.join(ROOT, "include")
 LIBDIR = os.path.join(ROOT, "apocharmm_b200")
 SRC = os.path.join(ROOT, "tests", "cpp", "force_classes.cu")
+MD_SRC = os.path.join(ROOT, "tests", "cpp", "md_classes.cu")
 NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 CUDA_INC = os.path.join(os.path.dirname(os.path.dirname(os.path.realpath(NVCC))), "include")
 
@@ -32,10 +35,10 @@ FORCE_RTOL = 1e-5
 ENERGY_RTOL = 1e-6
 
 
-def build_program(out_dir):
-    exe = os.path.join(out_dir, "force_classes")
+def build_program(out_dir, src=SRC):
+    exe = os.path.join(out_dir, os.path.splitext(os.path.basename(src))[0])
     cmd = [NVCC, "-std=c++17", "-O1", "-gencode", "arch=compute_100a,code=sm_100a", "-I", INC,
-           SRC, "-L", LIBDIR, "-lapocharmm_c", "-Xlinker", "-rpath," + LIBDIR, "-o", exe]
+           src, "-L", LIBDIR, "-lapocharmm_c", "-Xlinker", "-rpath," + LIBDIR, "-o", exe]
     r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True, timeout=300)
     assert r.returncode == 0, r.stdout[-4000:]
     return exe
@@ -56,6 +59,7 @@ def test_headers_compile_alone(tmp_path):
 def test_program_links(tmp_path):
     assert os.path.exists(os.path.join(LIBDIR, "libapocharmm_c.so"))
     build_program(str(tmp_path))
+    build_program(str(tmp_path), MD_SRC)
 
 
 def _results(path):
@@ -144,3 +148,97 @@ def test_force_classes_against_oracle(tmp_path):
     np.testing.assert_array_equal(grad("after_unsubscribe"), G)
     assert res["after_unsubscribe_has_well"] == [0.0]
     assert res["bad_cutoff_exception"] == [1.0]
+
+
+MD_SETTINGS = dict(kappa=0.34, nfft=(24, 24, 24), order=4, ctofnb=9.0, ctonnb=7.5, cutnb=11.0)
+
+
+@pytest.mark.gpu
+def test_md_classes_match_python_api(tmp_path):
+    """CharmmContext + CudaLangevinThermostatIntegrator + Dcd/Restart
+    subscribers in C++ against the same calls through the Python API: the
+    same library underneath, so positions, velocities, forces, energies and
+    the restart file agree exactly."""
+    from apocharmm_b200 import api
+    from apocharmm_b200.systems import water_box, write_crd
+
+    exe = build_program(str(tmp_path), MD_SRC)
+    s = water_box(1000, 31.0, seed=3)
+    keep = api.system_context(s, str(tmp_path / "relax"), settings=MD_SETTINGS)
+    api.relax(keep[3], api.water_indices(s), iterations=100)
+    relaxed = keep[3].getCoordinates()
+    del keep
+    paths = write_charmm_files(s, str(tmp_path / "files"))
+    write_crd(s, paths["crd"], pos=relaxed)
+    st = MD_SETTINGS
+    nsteps = 40
+    out = tmp_path / "cpp"
+    out.mkdir()
+    args = [exe, paths["psf"], paths["prm"], paths["crd"], repr(s.box[0]), repr(st["kappa"]),
+            repr(st["cutnb"]), repr(st["ctonnb"]), repr(st["ctofnb"]), str(st["nfft"][0]),
+            str(st["nfft"][1]), str(st["nfft"][2]), str(st["order"]), str(nsteps), str(out)]
+    r = subprocess.run(args, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-4000:]
+    res = {}
+    energies = {}
+    for line in open(out / "results.txt"):
+        f = line.split()
+        if f and f[0] == "energy":
+            energies[f[1]] = float(f[2])
+        elif f:
+            res[f[0]] = f[1:]
+    assert "done" in res
+
+    # the same sequence through the Python API
+    psf = api.CharmmPsf(paths["psf"])
+    prm = api.CharmmParameters(paths["prm"])
+    fm = api.ForceManager(psf, prm)
+    fm.setBoxDimensions(s.box)
+    fm.setKappa(st["kappa"])
+    fm.setCutoff(st["cutnb"])
+    fm.setCtonnb(st["ctonnb"])
+    fm.setCtofnb(st["ctofnb"])
+    fm.setFFTGrid(*st["nfft"])
+    fm.setPmeSplineOrder(st["order"])
+    ctx = api.CharmmContext(fm)
+    ctx.setCoordinates(api.CharmmCrd(paths["crd"]))
+    ctx.setRandomSeedForVelocities(314159)
+    ctx.assignVelocitiesAtTemperature(300.0)
+    it = api.CudaLangevinThermostatIntegrator(0.002)
+    it.setThermostatFriction(5.0)
+    it.setReferenceTemperature(300.0)
+    it.setThermostatRngSeed(1234)
+    it.setCharmmContext(ctx)
+    py = tmp_path / "py"
+    py.mkdir()
+    dcd = api.DcdSubscriber(str(py / "traj.dcd"), 10)
+    rst = api.RestartSubscriber(str(py / "run.rst"), nsteps)
+    it.subscribe(dcd)
+    it.subscribe(rst)
+    it.propagate(nsteps)
+
+    n = s.n_atoms
+    assert res["crd_atoms"] == [str(n), str(n)]
+    assert int(res["ndegf"][0]) == ctx.getDegreesOfFreedom()
+    assert res["report_frequency"] == ["10", str(nsteps), "5"]
+    assert res["subscribers"] == ["2"]
+    assert int(res["step"][0]) == nsteps == it.getCurrentPropagatedStep()
+    assert int(res["rngpos"][0]) == it.getRngSequencePos()
+    x_cpp = np.fromfile(out / "coords.bin", np.float64).reshape(-1, 3)
+    v_cpp = np.fromfile(out / "velocities.bin", np.float64).reshape(-1, 3)
+    np.testing.assert_array_equal(x_cpp, ctx.getCoordinates())
+    np.testing.assert_array_equal(v_cpp, np.asarray(ctx.getVelocities()).reshape(-1, 3))
+    assert float(res["temperature"][0]) == pytest.approx(ctx.computeTemperature(), rel=1e-6)
+
+    ctx.calculateForces(True, True, True)
+    e_py = ctx.getEnergyComponents()
+    for k, v in energies.items():
+        assert v == e_py[k], k
+    np.testing.assert_array_equal(np.fromfile(out / "forces.bin", np.float64).reshape(-1, 3),
+                                  ctx.getForces())
+    a, b = api.read_restart_file(out / "run.rst"), api.read_restart_file(py / "run.rst")
+    assert a["npriv"] == b["npriv"] == nsteps and a["rngpos"] == b["rngpos"]
+    for key in ("xold", "vel", "delta", "box"):
+        np.testing.assert_array_equal(a[key], b[key])
+    assert os.path.getsize(out / "traj.dcd") == os.path.getsize(py / "traj.dcd") > 0
+    assert res["leapfrog_step"] == ["5"]
