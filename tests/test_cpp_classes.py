@@ -189,15 +189,17 @@ def test_md_classes_match_python_api(tmp_path):
             res[f[0]] = f[1:]
     assert "done" in res
 
-    # the same sequence through the Python API
+    # the same sequence through the Python API; the C++ setters take float,
+    # as the reference's do, so the Python side is given the same float values
+    f32 = lambda x: float(np.float32(x))  # noqa: E731
     psf = api.CharmmPsf(paths["psf"])
     prm = api.CharmmParameters(paths["prm"])
     fm = api.ForceManager(psf, prm)
     fm.setBoxDimensions(s.box)
-    fm.setKappa(st["kappa"])
-    fm.setCutoff(st["cutnb"])
-    fm.setCtonnb(st["ctonnb"])
-    fm.setCtofnb(st["ctofnb"])
+    fm.setKappa(f32(st["kappa"]))
+    fm.setCutoff(f32(st["cutnb"]))
+    fm.setCtonnb(f32(st["ctonnb"]))
+    fm.setCtofnb(f32(st["ctofnb"]))
     fm.setFFTGrid(*st["nfft"])
     fm.setPmeSplineOrder(st["order"])
     ctx = api.CharmmContext(fm)
