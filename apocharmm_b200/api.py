@@ -167,6 +167,12 @@ class ForceManager(_Handle):
     def setBoxDimensions(self, box: Sequence[float]):
         call("apo_force_manager_set_box_dimensions", self._h, _d(box[0]), _d(box[1]), _d(box[2]))
 
+    def getBoxDimensions(self) -> np.ndarray:
+        """The box in force (A); the Langevin piston changes it every step."""
+        a = np.zeros(3)
+        call("apo_force_manager_get_box_dimensions", _ptr(a), _sz(3), self._h)
+        return a
+
     def setKappa(self, v): call("apo_force_manager_set_kappa", self._h, _d(v))
     def setCutoff(self, v): call("apo_force_manager_set_cutoff", self._h, _d(v))
     def setCtonnb(self, v): call("apo_force_manager_set_ctonnb", self._h, _d(v))
@@ -587,6 +593,109 @@ class CudaLeapFrogIntegrator(CudaIntegrator):
         super().__init__()
         call("apo_cuda_leap_frog_integrator_create", ctypes.byref(self._h), _d(time_step))
         self._bind_view()
+
+
+class CudaLangevinPistonIntegrator(CudaIntegrator):
+    """Constant pressure (Langevin piston on the box edges, optional
+    Nose-Hoover thermostat): include/CudaLangevinPistonIntegrator.h.
+    Crystal types 1 cubic, 2 orthorhombic, 3 tetragonal (enum CRYSTAL);
+    pressures in atm, 3x3 row major."""
+
+    _destroy = "apo_cuda_langevin_piston_integrator_destroy"
+    _as_base = "apo_cuda_langevin_piston_integrator_as_cuda_integrator"
+    CUBIC, ORTHORHOMBIC, TETRAGONAL = 1, 2, 3
+
+    def __init__(self, time_step: float):
+        super().__init__()
+        call("apo_cuda_langevin_piston_integrator_create", ctypes.byref(self._h), _d(time_step))
+        self._bind_view()
+
+    def setCrystalType(self, crystal: int):
+        call("apo_cuda_langevin_piston_integrator_set_crystal_type", self._h, _i(crystal))
+
+    def setPressure(self, p):
+        a = np.ascontiguousarray(p, np.float64).reshape(-1)
+        call("apo_cuda_langevin_piston_integrator_set_pressure", self._h, _ptr(a), _sz(a.size))
+
+    def setLangevinPistonMass(self, m):
+        a = np.ascontiguousarray(m, np.float64).reshape(-1)
+        call("apo_cuda_langevin_piston_integrator_set_langevin_piston_mass", self._h, _ptr(a),
+             _sz(a.size))
+
+    def getLangevinPistonMass(self) -> np.ndarray:
+        a, n = np.zeros(3), _sz()
+        call("apo_cuda_langevin_piston_integrator_get_langevin_piston_mass", _ptr(a), _sz(3),
+             ctypes.byref(n), self._h)
+        return a[:n.value]
+
+    def setLangevinPistonFriction(self, g: float):
+        call("apo_cuda_langevin_piston_integrator_set_langevin_piston_friction", self._h, _d(g))
+
+    def setLangevinPistonFrictionSeed(self, seed: int):
+        call("apo_cuda_langevin_piston_integrator_set_langevin_piston_friction_seed", self._h,
+             ctypes.c_uint64(seed))
+
+    def setRngSequencePos(self, pos: int):
+        call("apo_cuda_langevin_piston_integrator_set_rng_sequence_pos", self._h,
+             ctypes.c_ulonglong(pos))
+
+    def getRngSequencePos(self) -> int:
+        v = ctypes.c_ulonglong()
+        call("apo_cuda_langevin_piston_integrator_get_rng_sequence_pos", ctypes.byref(v), self._h)
+        return v.value
+
+    def setReferenceTemperature(self, t: float):
+        call("apo_cuda_langevin_piston_integrator_set_reference_temperature", self._h, _d(t))
+
+    def useNoseHooverThermostat(self, flag: bool = True):
+        call("apo_cuda_langevin_piston_integrator_use_nose_hoover_thermostat", self._h,
+             ctypes.c_bool(flag))
+
+    def setNoseHooverPistonMass(self, m: float):
+        call("apo_cuda_langevin_piston_integrator_set_nose_hoover_piston_mass", self._h, _d(m))
+
+    def useOldTemperature(self, flag: bool = True):
+        call("apo_cuda_langevin_piston_integrator_use_old_temperature", self._h, ctypes.c_bool(flag))
+
+    def setMaxPredictorCorrectorIterations(self, n: int):
+        call("apo_cuda_langevin_piston_integrator_set_max_predictor_corrector_iterations", self._h,
+             _i(n))
+
+    def setConstantSurfaceTension(self, flag: bool, tension: float = 0.0):
+        call("apo_cuda_langevin_piston_integrator_set_constant_surface_tension", self._h,
+             ctypes.c_bool(flag), _d(tension))
+
+    def resetAverages(self):
+        call("apo_cuda_langevin_piston_integrator_reset_averages", self._h)
+
+    def _tensor(self, name) -> np.ndarray:
+        a = np.zeros(9)
+        call(name, _ptr(a), _sz(9), self._h)
+        return a.reshape(3, 3)
+
+    def getInstantaneousPressureTensor(self) -> np.ndarray:
+        return self._tensor("apo_cuda_langevin_piston_integrator_get_instantaneous_pressure_tensor")
+
+    def getAveragePressureTensor(self) -> np.ndarray:
+        return self._tensor("apo_cuda_langevin_piston_integrator_get_average_pressure_tensor")
+
+    def getInstantaneousPressureScalar(self) -> float:
+        v = _d()
+        call("apo_cuda_langevin_piston_integrator_get_instantaneous_pressure_scalar",
+             ctypes.byref(v), self._h)
+        return v.value
+
+    def getAveragePressureScalar(self) -> float:
+        v = _d()
+        call("apo_cuda_langevin_piston_integrator_get_average_pressure_scalar", ctypes.byref(v),
+             self._h)
+        return v.value
+
+    def getLangevinPistonOnStepPosition(self) -> np.ndarray:
+        a, n = np.zeros(3), _sz()
+        call("apo_cuda_langevin_piston_integrator_get_langevin_piston_on_step_position", _ptr(a),
+             _sz(3), ctypes.byref(n), self._h)
+        return a[:n.value]
 
 
 def rigid_water_fit(xyz: np.ndarray, waters: np.ndarray) -> np.ndarray:

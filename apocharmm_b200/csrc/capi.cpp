@@ -232,6 +232,18 @@ extern "C" apo_status apo_force_manager_set_box_dimensions(apo_force_manager *fm
   }, fn);
 }
 
+extern "C" apo_status apo_force_manager_get_box_dimensions(double *box, const size_t len,
+                                                           const apo_force_manager *fm) {
+  const char *fn = "apo_force_manager_get_box_dimensions";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_buffer(box, len, 3, fn, "box"));
+    APO_RETURN_IF(require_handle(fm, fn, "ForceManager"));
+    const auto &b = fm->object->getBoxDimensions();
+    for (int d = 0; d < 3; ++d) box[d] = b[d];
+    return APO_STATUS_OK;
+  }, fn);
+}
+
 #define FM_SETTER(fname, type, call, check)                                        \
   extern "C" apo_status fname(apo_force_manager *fm, const type v) {               \
     return guard([&]() -> apo_status {                                             \

@@ -1,5 +1,6 @@
 // C ABI: integrators and subscribers (same conventions as capi.cpp).
 #include "apocharmm_c/CudaIntegrator.h"
+#include "apocharmm_c/CudaLangevinPistonIntegrator.h"
 #include "apocharmm_c/CudaLangevinThermostatIntegrator.h"
 #include "apocharmm_c/CudaNoseHooverIntegrator.h"
 #include "apocharmm_c/DcdSubscriber.h"
@@ -465,6 +466,206 @@ extern "C" apo_status apo_restart_file_write(const char *path, const int natom, 
     r.vel.assign(vel, vel + n3);
     r.delta.assign(delta, delta + n3);
     apo::writeRestartFile(path, r);
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+// ------------------------------------------------------ Langevin piston ----
+
+struct apo_cuda_langevin_piston_integrator {
+  apo_cuda_integrator base;
+  std::shared_ptr<apo::CudaLangevinPistonIntegrator> object;
+};
+
+extern "C" apo_status apo_cuda_langevin_piston_integrator_create(
+    apo_cuda_langevin_piston_integrator **out, const double dt) {
+  const char *fn = "apo_cuda_langevin_piston_integrator_create";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(prepare_out(out, fn));
+    if (!(dt > 0) || !std::isfinite(dt)) return invalid(fn, "time step must be positive");
+    auto h = std::make_unique<apo_cuda_langevin_piston_integrator>();
+    h->object = std::make_shared<apo::CudaLangevinPistonIntegrator>(dt);
+    h->base.object = h->object;
+    *out = h.release();
+    return APO_STATUS_OK;
+  }, fn);
+}
+extern "C" void apo_cuda_langevin_piston_integrator_destroy(apo_cuda_langevin_piston_integrator *it) {
+  delete it;
+}
+
+extern "C" apo_status apo_cuda_langevin_piston_integrator_as_cuda_integrator(
+    apo_cuda_integrator **out, apo_cuda_langevin_piston_integrator *it) {
+  const char *fn = "apo_cuda_langevin_piston_integrator_as_cuda_integrator";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(prepare_out(out, fn));
+    APO_RETURN_IF(require_handle(it, fn, "CudaLangevinPistonIntegrator"));
+    *out = &it->base;
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+#define LP_SET(fname, type, body)                                                   \
+  extern "C" apo_status fname(apo_cuda_langevin_piston_integrator *it, const type v) { \
+    return guard([&]() -> apo_status {                                              \
+      APO_RETURN_IF(require_handle(it, #fname, "CudaLangevinPistonIntegrator"));    \
+      body;                                                                         \
+      return APO_STATUS_OK;                                                         \
+    }, #fname);                                                                     \
+  }
+LP_SET(apo_cuda_langevin_piston_integrator_set_crystal_type, int,
+       if (v < 1 || v > 3) return invalid("set_crystal_type",
+                                          "crystal type must be 1 (cubic), 2 (orthorhombic) or 3 (tetragonal)");
+       it->object->setCrystalType((apo::Crystal)v))
+LP_SET(apo_cuda_langevin_piston_integrator_set_langevin_piston_friction, double,
+       if (!(v >= 0) || !std::isfinite(v)) return invalid("set_langevin_piston_friction", "friction must be >= 0");
+       it->object->setLangevinPistonFriction(v))
+LP_SET(apo_cuda_langevin_piston_integrator_set_langevin_piston_friction_seed, uint64_t,
+       it->object->setLangevinPistonFrictionSeed(v))
+LP_SET(apo_cuda_langevin_piston_integrator_set_rng_sequence_pos, unsigned long long,
+       it->object->setRngSequencePos(v))
+LP_SET(apo_cuda_langevin_piston_integrator_set_reference_temperature, double,
+       if (!(v >= 0) || !std::isfinite(v)) return invalid("set_reference_temperature", "temperature must be >= 0");
+       it->object->setReferenceTemperature(v))
+LP_SET(apo_cuda_langevin_piston_integrator_use_nose_hoover_thermostat, bool,
+       it->object->useNoseHooverThermostat(v))
+LP_SET(apo_cuda_langevin_piston_integrator_set_nose_hoover_piston_mass, double,
+       if (!(v > 0) || !std::isfinite(v)) return invalid("set_nose_hoover_piston_mass", "mass must be positive");
+       it->object->setNoseHooverPistonMass(v))
+LP_SET(apo_cuda_langevin_piston_integrator_use_old_temperature, bool, it->object->useOldTemperature(v))
+LP_SET(apo_cuda_langevin_piston_integrator_set_max_predictor_corrector_iterations, int,
+       it->object->setMaxPredictorCorrectorIterations(v))
+
+extern "C" apo_status apo_cuda_langevin_piston_integrator_set_constant_surface_tension(
+    apo_cuda_langevin_piston_integrator *it, const bool flag, const double tension) {
+  const char *fn = "apo_cuda_langevin_piston_integrator_set_constant_surface_tension";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(it, fn, "CudaLangevinPistonIntegrator"));
+    if (!std::isfinite(tension)) return invalid(fn, "surface tension must be finite");
+    it->object->setConstantSurfaceTension(flag);
+    it->object->setSurfaceTension(tension);
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_cuda_langevin_piston_integrator_set_pressure(
+    apo_cuda_langevin_piston_integrator *it, const double *p, const size_t len) {
+  const char *fn = "apo_cuda_langevin_piston_integrator_set_pressure";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(it, fn, "CudaLangevinPistonIntegrator"));
+    APO_RETURN_IF(require_ptr(p, fn, "pressure"));
+    it->object->setPressure(std::vector<double>(p, p + len));
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_cuda_langevin_piston_integrator_set_langevin_piston_mass(
+    apo_cuda_langevin_piston_integrator *it, const double *m, const size_t len) {
+  const char *fn = "apo_cuda_langevin_piston_integrator_set_langevin_piston_mass";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(it, fn, "CudaLangevinPistonIntegrator"));
+    APO_RETURN_IF(require_ptr(m, fn, "mass"));
+    for (size_t k = 0; k < len; ++k)
+      if (!(m[k] >= 0) || !std::isfinite(m[k])) return invalid(fn, "masses must be >= 0");
+    it->object->setLangevinPistonMass(std::vector<double>(m, m + len));
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_cuda_langevin_piston_integrator_reset_averages(
+    apo_cuda_langevin_piston_integrator *it) {
+  const char *fn = "apo_cuda_langevin_piston_integrator_reset_averages";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(it, fn, "CudaLangevinPistonIntegrator"));
+    it->object->resetAverages();
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_cuda_langevin_piston_integrator_get_rng_sequence_pos(
+    unsigned long long *pos, const apo_cuda_langevin_piston_integrator *it) {
+  const char *fn = "apo_cuda_langevin_piston_integrator_get_rng_sequence_pos";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_ptr(pos, fn, "pos"));
+    APO_RETURN_IF(require_handle(it, fn, "CudaLangevinPistonIntegrator"));
+    *pos = it->object->getRngSequencePos();
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+namespace {
+apo_status lp_tensor(double *out, size_t len, apo_cuda_langevin_piston_integrator *it,
+                     const char *fn, bool average) {
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_buffer(out, len, 9, fn, "pressure"));
+    APO_RETURN_IF(require_handle(it, fn, "CudaLangevinPistonIntegrator"));
+    if (!it->object->getCharmmContext())
+      return set_error(APO_STATUS_NOT_INITIALIZED, std::string(fn) + ": no CharmmContext was set");
+    const auto v = average ? it->object->getAveragePressureTensor()
+                           : it->object->getInstantaneousPressureTensor();
+    std::copy(v.begin(), v.end(), out);
+    return APO_STATUS_OK;
+  }, fn);
+}
+apo_status lp_scalar(double *out, apo_cuda_langevin_piston_integrator *it, const char *fn,
+                     bool average) {
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_ptr(out, fn, "pressure"));
+    APO_RETURN_IF(require_handle(it, fn, "CudaLangevinPistonIntegrator"));
+    if (!it->object->getCharmmContext())
+      return set_error(APO_STATUS_NOT_INITIALIZED, std::string(fn) + ": no CharmmContext was set");
+    *out = average ? it->object->getAveragePressureScalar()
+                   : it->object->getInstantaneousPressureScalar();
+    return APO_STATUS_OK;
+  }, fn);
+}
+}  // namespace
+
+extern "C" apo_status apo_cuda_langevin_piston_integrator_get_instantaneous_pressure_tensor(
+    double *p, const size_t len, apo_cuda_langevin_piston_integrator *it) {
+  return lp_tensor(p, len, it, "apo_cuda_langevin_piston_integrator_get_instantaneous_pressure_tensor",
+                   false);
+}
+extern "C" apo_status apo_cuda_langevin_piston_integrator_get_average_pressure_tensor(
+    double *p, const size_t len, apo_cuda_langevin_piston_integrator *it) {
+  return lp_tensor(p, len, it, "apo_cuda_langevin_piston_integrator_get_average_pressure_tensor", true);
+}
+extern "C" apo_status apo_cuda_langevin_piston_integrator_get_instantaneous_pressure_scalar(
+    double *p, apo_cuda_langevin_piston_integrator *it) {
+  return lp_scalar(p, it, "apo_cuda_langevin_piston_integrator_get_instantaneous_pressure_scalar",
+                   false);
+}
+extern "C" apo_status apo_cuda_langevin_piston_integrator_get_average_pressure_scalar(
+    double *p, apo_cuda_langevin_piston_integrator *it) {
+  return lp_scalar(p, it, "apo_cuda_langevin_piston_integrator_get_average_pressure_scalar", true);
+}
+
+extern "C" apo_status apo_cuda_langevin_piston_integrator_get_langevin_piston_mass(
+    double *m, const size_t len, size_t *num, const apo_cuda_langevin_piston_integrator *it) {
+  const char *fn = "apo_cuda_langevin_piston_integrator_get_langevin_piston_mass";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_ptr(num, fn, "num"));
+    APO_RETURN_IF(require_handle(it, fn, "CudaLangevinPistonIntegrator"));
+    const auto v = it->object->getLangevinPistonMass();
+    *num = v.size();
+    APO_RETURN_IF(require_buffer(m, len, v.size(), fn, "mass"));
+    std::copy(v.begin(), v.end(), m);
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_cuda_langevin_piston_integrator_get_langevin_piston_on_step_position(
+    double *x, const size_t len, size_t *num, apo_cuda_langevin_piston_integrator *it) {
+  const char *fn = "apo_cuda_langevin_piston_integrator_get_langevin_piston_on_step_position";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_ptr(num, fn, "num"));
+    APO_RETURN_IF(require_handle(it, fn, "CudaLangevinPistonIntegrator"));
+    if (!it->object->getCharmmContext())
+      return set_error(APO_STATUS_NOT_INITIALIZED, std::string(fn) + ": no CharmmContext was set");
+    const auto v = it->object->getLangevinPistonOnStepPosition();
+    *num = v.size();
+    APO_RETURN_IF(require_buffer(x, len, v.size(), fn, "position"));
+    std::copy(v.begin(), v.end(), x);
     return APO_STATUS_OK;
   }, fn);
 }

@@ -217,6 +217,28 @@ void ForceManager::setBoxDimensions(const std::array<double, 3> &box) {
   m_Initialized = false;
 }
 
+void ForceManager::updateBoxDimensions(const std::array<double, 3> &box) {
+  if (!m_Initialized) throw std::runtime_error("ForceManager is not initialized");
+  if (m_Multi)
+    throw std::invalid_argument("updateBoxDimensions: a multi-system force manager keeps its boxes");
+  for (double b : box)
+    if (!(b > 0.0) || !std::isfinite(b))
+      throw std::invalid_argument("Box dimensions: " + std::to_string(box[0]) + " x " +
+                                  std::to_string(box[1]) + " x " + std::to_string(box[2]) +
+                                  " are NOT valid");
+  for (double b : box)
+    if (m_Cutoff > b / 2.0)
+      throw std::runtime_error("the box shrank below twice the cutoff (" + std::to_string(b) +
+                               " A edge, cutoff " + std::to_string(m_Cutoff) + " A)");
+  m_Box = box;
+  m_HostSetup = make_nb_setup(m_Box[0], m_Box[1], m_Box[2], m_Kappa, m_Ctofnb, m_Ctonnb);
+  APO_CUDA(cudaMemcpy(m_Setup.p, &m_HostSetup, sizeof(NbSetup), cudaMemcpyHostToDevice));
+  m_Nbl.set_box(0, m_Box[0], m_Box[1], m_Box[2]);
+  m_Pme.set_box(m_Box[0], m_Box[1], m_Box[2]);
+  m_ListDirty = true;
+  ++m_PluginGen;  // captured graphs hold the old box
+}
+
 void ForceManager::setFFTGrid(int nx, int ny, int nz) {
   m_Nfft[0] = nx;
   m_Nfft[1] = ny;

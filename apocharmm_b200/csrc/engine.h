@@ -103,6 +103,12 @@ class ForceManager {
   std::vector<double> getVirial(int sys, cudaStream_t s);
 
   void setBoxDimensions(const std::array<double, 3> &box);
+  // a box that changes every step (pressure control, one system): the
+  // direct-space set-up, the list's box and the reciprocal box follow it
+  // without a new initialisation; the list is rebuilt at the next
+  // evaluation and graphs captured with the old box are dropped.  The
+  // caller has synchronised the context's stream.
+  void updateBoxDimensions(const std::array<double, 3> &box);
   void setKappa(double k) { m_Kappa = k; m_Initialized = false; }
   void setCutoff(double c) { m_Cutoff = c; m_Initialized = false; }
   void setCtonnb(double c) { m_Ctonnb = c; m_Initialized = false; }
@@ -209,6 +215,9 @@ class ForceManager {
   long long *energyFixed() const { return m_Energy.p; }
   NeighborList &neighborList() { return m_Nbl; }
   Pme &pme() { return m_Pme; }
+  // the virial slots of the last evaluation made with calcVirial (3x3 row
+  // major, 2^32 fixed point; one system)
+  const long long *deviceVirial() const { return m_Energy.p + kNumEnergyTerms; }
   double selfEnergy() const { return m_SelfEnergy; }
   unsigned readDeviceError(cudaStream_t s);
   // CUDA-event timing of every direct-space launch (on the stream it runs

@@ -4,6 +4,7 @@
 #include <curand_kernel.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <cmath>
 #include <random>
 #include <stdexcept>
@@ -714,6 +715,419 @@ __global__ void com_apply_kernel(Common c, int natom, int freq) {
   c.dprev[a] = d;
 }
 
+// --------------------------------------------------------- Langevin piston
+// src/CudaLangevinPistonIntegrator.cu:1705-2060 in five kinds of launch:
+//   lp_half   half step, constraint, constraint forces and virial, the
+//             pressure tensor and its static part
+//   lp_ke     (per pass) kinetic energy; last block: piston move (one normal
+//             per piston degree of freedom) and thermostat update
+//   lp_pc     (per pass) atoms follow piston and thermostat; last block:
+//             the pressure difference with the new half-step kinetic term
+//   lp_final  constraints on the new and the scaled reference positions,
+//             on-step velocities, kinetic energy, pressure averages, the box
+constexpr double kAtmosp = 1.4584007e-05;           // atm in AKMA pressure units
+constexpr double kPatmos = 1.0 / kAtmosp;
+constexpr double kSurfaceTensionFactor = 98.6923;   // dyne/cm to atm A
+
+}  // namespace
+
+struct PistonScalars {
+  double box[3], box_pred[3];
+  double vir[9];                 // internal virial of the step with the constraint part
+  double pref[9], dp[9], dp_static[9];
+  double p[9], pavg[9];
+  double pscalar, pavg_scalar;
+  double lp_delta[3], lp_delta_pred[3], lp_delta_prev[3];
+  double lp_onpos[3], lp_halfpos[3], lp_onvel[3], lp_dpress[3];
+  double cf_on[3], cf_half[3];
+  unsigned counter, pad;
+};
+
+namespace {
+
+struct PistonArgs {
+  PistonScalars *ps;
+  curandStatePhilox4_32_10_t *rng;
+  double *partials;
+  const long long *vir_fixed;    // the force manager's virial slots
+  double inv_mass[3], prfwd[3];
+  double palpha, pbfact;
+  double vfac;                   // patmos / V
+  double lp_vfac;                // V pbfact atmosp
+  double st_fac;                 // surface tension x factor / Lz
+  double ke_ref;
+  int crystal, dof, use_nh, use_old, const_st, hol;
+};
+
+template <int N>
+__device__ void block_partials_n(const double (&v)[N], double *partials) {
+  __shared__ double sh[N][kThreads / 32];
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    const double s = warp_sum(v[k]);
+    if ((threadIdx.x & 31) == 0) sh[k][threadIdx.x >> 5] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < N) {
+    double s = 0;
+    for (int w = 0; w < kThreads / 32; ++w) s += sh[threadIdx.x][w];
+    partials[N * blockIdx.x + threadIdx.x] = s;
+  }
+}
+
+// totals of the N partials of every block, in block order, into tot[]
+template <int N>
+__device__ void sum_partials_n(const double *partials, double *tot) {
+  if (threadIdx.x < N) {
+    double s = 0;
+    for (int b = 0; b < (int)gridDim.x; ++b) s += partials[N * b + threadIdx.x];
+    tot[threadIdx.x] = s;
+  }
+  __syncthreads();
+}
+
+// piston move of one predictor-corrector pass (one thread)
+// (UpdateLangevinPistonKernel, src/CudaLangevinPistonIntegrator.cu:1297-1452)
+__device__ void lp_move(const PistonArgs &a, double dt) {
+  PistonScalars *ps = a.ps;
+  double *b = ps->box_pred;
+  const double *dP = ps->dp;
+  const Crystal cr = (Crystal)a.crystal;
+  if (cr == Crystal::Cubic) {
+    ps->lp_dpress[0] = (dP[0] + dP[4] + dP[8]) / b[0];
+  } else if (cr == Crystal::Tetragonal) {
+    ps->lp_dpress[0] = (dP[0] + dP[4]) / b[0];
+    ps->lp_dpress[1] = dP[8] / b[2];
+  } else {
+    ps->lp_dpress[0] = dP[0] / b[0];
+    ps->lp_dpress[1] = dP[4] / b[1];
+    ps->lp_dpress[2] = dP[8] / b[2];
+  }
+  for (int i = 0; i < a.dof; ++i) {
+    curandStatePhilox4_32_10_t st = a.rng[i];
+    ps->lp_delta_prev[i] = ps->lp_delta_pred[i];
+    ps->lp_delta_pred[i] = a.palpha * ps->lp_delta_pred[i] +
+                           a.inv_mass[i] * ps->lp_dpress[i] * a.lp_vfac +
+                           a.pbfact * a.prfwd[i] * curand_normal_double(&st);
+    ps->lp_onvel[i] = 0.5 * (ps->lp_delta_pred[i] + ps->lp_delta_prev[i]) / dt;
+    a.rng[i] = st;
+  }
+  if (cr == Crystal::Cubic) {
+    ps->lp_onpos[0] = (b[0] + b[1] + b[2]) / 3.0;
+  } else if (cr == Crystal::Tetragonal) {
+    ps->lp_onpos[0] = (b[0] + b[1]) / 2.0;
+    ps->lp_onpos[1] = b[2];
+  } else {
+    ps->lp_onpos[0] = b[0];
+    ps->lp_onpos[1] = b[1];
+    ps->lp_onpos[2] = b[2];
+  }
+  for (int i = 0; i < a.dof; ++i) {
+    ps->lp_onpos[i] += ps->lp_delta_pred[i];
+    ps->lp_halfpos[i] = ps->lp_onpos[i] - 0.5 * ps->lp_delta_pred[i];
+  }
+  // scaling factors of the edges (on-step: piston velocity over the edge;
+  // half-step: displacement over the half-step edge), then the new edges
+  double *on = ps->cf_on, *hf = ps->cf_half;
+  const double *dl = ps->lp_delta_pred, *hp = ps->lp_halfpos, *op = ps->lp_onpos,
+               *ov = ps->lp_onvel;
+  if (cr == Crystal::Cubic) {
+    on[0] = on[1] = on[2] = dt * ov[0] / b[0];
+    hf[0] = hf[1] = hf[2] = dl[0] / hp[0];
+    b[0] = b[1] = b[2] = op[0];
+  } else if (cr == Crystal::Tetragonal) {
+    on[0] = on[1] = dt * ov[0] / b[0];
+    on[2] = dt * ov[1] / b[2];
+    hf[0] = hf[1] = dl[0] / hp[0];
+    hf[2] = dl[1] / hp[1];
+    b[0] = b[1] = op[0];
+    b[2] = op[1];
+  } else {
+    for (int d = 0; d < 3; ++d) {
+      on[d] = dt * ov[d] / b[d];
+      hf[d] = dl[d] / hp[d];
+      b[d] = op[d];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) lp_half_kernel(Common c, PistonArgs a) {
+  if (*c.err) return;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const double dt = c.dt, dt2 = dt * dt, idt = 1.0 / dt;
+  // [0..8] constraint virial, [9..17] sum d d m/dt^2 of the new half step,
+  // [18..26] the same of the previous half step
+  double v[27];
+#pragma unroll
+  for (int k = 0; k < 27; ++k) v[k] = 0.0;
+  if (g < c.ngroups) {
+    int at[4];
+    const int m = group_atoms(c, g, at);
+    const int2 meta = c.gmeta[g];
+    double4 x[4], vm[4], dp[4];
+    int slot[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (k < m) {
+        const int i = at[k];
+        x[k] = c.coords[i];
+        vm[k] = c.vel[i];
+        dp[k] = c.dprev[i];
+        slot[k] = c.glo2loc[i];
+      }
+    }
+    d3 o[4], n[4], n0[4], du[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (k < m) {
+        const d3 gr = mk((double)c.force[slot[k]] * kInvForceScale,
+                         (double)c.force[c.stride + slot[k]] * kInvForceScale,
+                         (double)c.force[2 * c.stride + slot[k]] * kInvForceScale);
+        o[k] = xyz(x[k]);
+        du[k] = xyz(dp[k]) - (dt2 * vm[k].w) * gr;
+        n[k] = o[k] + du[k];
+        n0[k] = n[k];
+      }
+    }
+    if (a.hol) apply_constraint(meta.x, m, o, n, c.sk, c.shake_p, meta.y);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (k < m) {
+        const int i = at[k];
+        const double f = 1.0 / (dt2 * vm[k].w);
+        d3 d = du[k];
+        if (a.hol) {
+          // constraint force m (x_constrained - x_free) / dt^2 and its virial
+          // (ComputeHolonomicConstraintForces/VirialKernel)
+          const d3 fc = mk(f * (n[k].x - o[k].x - du[k].x), f * (n[k].y - o[k].y - du[k].y),
+                           f * (n[k].z - o[k].z - du[k].z));
+          const double r[3] = {o[k].x, o[k].y, o[k].z}, q[3] = {fc.x, fc.y, fc.z};
+#pragma unroll
+          for (int u = 0; u < 3; ++u)
+#pragma unroll
+            for (int w = 0; w < 3; ++w) v[3 * u + w] += r[u] * q[w];
+          d = n[k] - o[k];
+        }
+        const double dd[3] = {d.x, d.y, d.z}, pp[3] = {dp[k].x, dp[k].y, dp[k].z};
+#pragma unroll
+        for (int u = 0; u < 3; ++u)
+#pragma unroll
+          for (int w = 0; w < 3; ++w) {
+            v[9 + 3 * u + w] += f * dd[u] * dd[w];
+            v[18 + 3 * u + w] += f * pp[u] * pp[w];
+          }
+        c.ref[i] = x[k];
+        c.delta[i] = make_double4(d.x, d.y, d.z, 0.0);
+        c.dpred[i] = make_double4(d.x, d.y, d.z, 0.0);
+        const d3 xn = o[k] + d;
+        c.coords[i] = make_double4(a.hol ? n[k].x : xn.x, a.hol ? n[k].y : xn.y,
+                                   a.hol ? n[k].z : xn.z, x[k].w);
+        // a constraint pass adds its displacement over dt to the velocities
+        // (src/CudaHolonomicConstraint.cu:94-106): the first pass's on-step
+        // kinetic energy sees it
+        const d3 vn = xyz(vm[k]) + idt * (n[k] - n0[k]);
+        c.vel[i] = make_double4(vn.x, vn.y, vn.z, vm[k].w);
+      }
+    }
+  }
+  block_partials_n<27>(v, a.partials);
+  if (is_last_block(&a.ps->counter)) {
+    __shared__ double tot[27];
+    sum_partials_n<27>(a.partials, tot);
+    if (threadIdx.x == 0) {
+      PistonScalars *ps = a.ps;
+      for (int k = 0; k < 9; ++k) {
+        ps->vir[k] = (double)a.vir_fixed[k] * kInvEnergyScale + tot[k];
+        const double kin = 0.5 * (tot[9 + k] + tot[18 + k]);
+        ps->p[k] = a.vfac * (kin + ps->vir[k]);
+        ps->dp[k] = ps->p[k] - ps->pref[k];
+      }
+      ps->pscalar = (ps->p[0] + ps->p[4] + ps->p[8]) / 3.0;
+      if (a.const_st) {
+        ps->pref[0] = ps->pref[8] - a.st_fac;
+        ps->pref[4] = ps->pref[0];
+      }
+      for (int k = 0; k < 9; ++k) ps->dp_static[k] = ps->dp[k] - 0.25 * a.vfac * tot[9 + k];
+      c.sc->piston_v_prev = c.sc->piston_v;
+      c.sc->piston_f_prev = c.sc->piston_f;
+      ps->counter = 0;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) lp_ke_kernel(Common c, PistonArgs a, int natom) {
+  if (*c.err) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const double dt = c.dt, idt = 1.0 / dt;
+  double v[2] = {0.0, 0.0};
+  if (i < natom) {
+    const double4 vm = c.vel[i];
+    const d3 u1 = idt * xyz(c.dprev[i]), u2 = idt * xyz(c.dpred[i]), w = xyz(vm);
+    const double kon = 0.5 * dot(w, w) / vm.w;
+    v[0] = (0.5 * dot(u1, u1) / vm.w + kon + 0.5 * dot(u2, u2) / vm.w) / 3.0;
+    v[1] = kon;
+  }
+  block_partials_n<2>(v, a.partials);
+  if (is_last_block(&a.ps->counter)) {
+    __shared__ double tot[2];
+    sum_partials_n<2>(a.partials, tot);
+    if (threadIdx.x == 0) {
+      PistonScalars *ps = a.ps;
+      for (int d = 0; d < 3; ++d) {
+        ps->box_pred[d] = ps->box[d];
+        ps->lp_delta_pred[d] = ps->lp_delta[d];
+      }
+      lp_move(a, dt);
+      piston_update(c.sc, a.use_old ? tot[1] : tot[0], a.ke_ref, dt);
+      ps->counter = 0;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) lp_pc_kernel(Common c, PistonArgs a, int natom) {
+  if (*c.err) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const double dt = c.dt, dt2 = dt * dt, fact = 0.5 / dt;
+  const PistonScalars *ps = a.ps;
+  const double nh = a.use_nh ? dt2 * c.sc->piston_v : 0.0;
+  double v[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) v[k] = 0.0;
+  if (i < natom) {
+    const d3 dprev = xyz(c.dprev[i]), dpred = xyz(c.dpred[i]), d = xyz(c.delta[i]);
+    const d3 r = xyz(c.ref[i]);
+    const double4 x = c.coords[i];
+    const d3 u = fact * (dprev + dpred);
+    const d3 np = mk(d.x - (nh + dt * ps->cf_on[0]) * u.x, d.y - (nh + dt * ps->cf_on[1]) * u.y,
+                     d.z - (nh + dt * ps->cf_on[2]) * u.z);
+    c.dpred[i] = make_double4(np.x, np.y, np.z, 0.0);
+    const double im = c.vel[i].w;
+    c.vel[i] = make_double4(u.x, u.y, u.z, im);
+    const d3 h = 0.5 * (r + xyz(x));
+    c.coords[i] = make_double4(r.x + np.x + ps->cf_half[0] * h.x, r.y + np.y + ps->cf_half[1] * h.y,
+                               r.z + np.z + ps->cf_half[2] * h.z, x.w);
+    const double f = 1.0 / (dt2 * im);
+    const double nn[3] = {np.x, np.y, np.z};
+#pragma unroll
+    for (int p = 0; p < 3; ++p)
+#pragma unroll
+      for (int q = 0; q < 3; ++q) v[3 * p + q] = f * nn[p] * nn[q];
+  }
+  block_partials_n<9>(v, a.partials);
+  if (is_last_block(&a.ps->counter)) {
+    __shared__ double tot[9];
+    sum_partials_n<9>(a.partials, tot);
+    if (threadIdx.x == 0) {
+      for (int k = 0; k < 9; ++k) a.ps->dp[k] = a.ps->dp_static[k] + 0.25 * a.vfac * tot[k];
+      a.ps->counter = 0;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) lp_final_kernel(Common c, PistonArgs a) {
+  if (*c.err) return;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const double dt = c.dt, dt2 = dt * dt, idt = 1.0 / dt, fact = 0.5 / dt;
+  // [0] 3-term kinetic energy, [1] on-step, [2..10] sum (d d + dp dp) m/dt^2
+  double v[11];
+#pragma unroll
+  for (int k = 0; k < 11; ++k) v[k] = 0.0;
+  if (g < c.ngroups) {
+    int at[4];
+    const int m = group_atoms(c, g, at);
+    const int2 meta = c.gmeta[g];
+    d3 o[4], n[4], dp[4], dn[4], rs[4];
+    double q[4], im[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (k < m) {
+        const int i = at[k];
+        o[k] = xyz(c.ref[i]);
+        const double4 x = c.coords[i];
+        n[k] = xyz(x);
+        q[k] = x.w;
+        dp[k] = xyz(c.dprev[i]);
+        dn[k] = xyz(c.dpred[i]);
+        im[k] = c.vel[i].w;
+      }
+    }
+    if (a.hol) {
+      // the new positions onto the constraints, the reference positions
+      // scaled with the box and constrained against the new ones, the
+      // displacement between them (src/CudaLangevinPistonIntegrator.cu:1955-1980)
+      apply_constraint(meta.x, m, o, n, c.sk, c.shake_p, meta.y);
+      const PistonScalars *ps = a.ps;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        if (k < m) {
+          const d3 h = 0.5 * (o[k] + n[k]);
+          rs[k] = o[k] + mk(ps->cf_half[0] * h.x, ps->cf_half[1] * h.y, ps->cf_half[2] * h.z);
+        }
+      }
+      apply_constraint(meta.x, m, n, rs, c.sk, c.shake_p, meta.y);
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (k < m) dn[k] = n[k] - rs[k];
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (k < m) {
+        const int i = at[k];
+        const d3 d = dn[k];
+        const d3 u = fact * (d + dp[k]);
+        const d3 u1 = idt * dp[k], u2 = idt * d;
+        const double kon = 0.5 * dot(u, u) / im[k];
+        v[0] += (0.5 * dot(u1, u1) / im[k] + kon + 0.5 * dot(u2, u2) / im[k]) / 3.0;
+        v[1] += kon;
+        const double f = 1.0 / (dt2 * im[k]);
+        const double dd[3] = {d.x, d.y, d.z}, pp[3] = {dp[k].x, dp[k].y, dp[k].z};
+#pragma unroll
+        for (int s = 0; s < 3; ++s)
+#pragma unroll
+          for (int w = 0; w < 3; ++w) v[2 + 3 * s + w] += f * (dd[s] * dd[w] + pp[s] * pp[w]);
+        c.delta[i] = make_double4(d.x, d.y, d.z, 0.0);
+        c.dprev[i] = make_double4(d.x, d.y, d.z, 0.0);
+        c.vel[i] = make_double4(u.x, u.y, u.z, im[k]);
+        c.coords[i] = make_double4(n[k].x, n[k].y, n[k].z, q[k]);
+        c.xyzq[i] = make_float4((float)n[k].x, (float)n[k].y, (float)n[k].z, (float)q[k]);
+      }
+    }
+  }
+  block_partials_n<11>(v, a.partials);
+  if (is_last_block(&a.ps->counter)) {
+    __shared__ double tot[11];
+    sum_partials_n<11>(a.partials, tot);
+    if (threadIdx.x == 0) {
+      PistonScalars *ps = a.ps;
+      piston_update(c.sc, a.use_old ? tot[1] : tot[0], a.ke_ref, dt);
+      const double s = (double)(c.sc->window + 1);
+      for (int k = 0; k < 9; ++k) {
+        ps->p[k] = a.vfac * (0.5 * tot[2 + k] + ps->vir[k]);
+        ps->pavg[k] += (ps->p[k] - ps->pavg[k]) / s;
+      }
+      ps->pscalar = (ps->p[0] + ps->p[4] + ps->p[8]) / 3.0;
+      ps->pavg_scalar += (ps->pscalar - ps->pavg_scalar) / s;
+      finish_temperature(c, tot[0], tot[1]);
+      for (int d = 0; d < 3; ++d) {
+        ps->box[d] = ps->box_pred[d];
+        ps->lp_delta[d] = ps->lp_delta_pred[d];
+      }
+      c.sc->step += 1;
+      ps->counter = 0;
+    }
+  }
+}
+
+// one Philox state per piston degree of freedom: subsequence = dof index,
+// then `pos` draws skipped (InitializeRngKernel)
+__global__ void lp_rng_init_kernel(curandStatePhilox4_32_10_t *st, int n,
+                                   unsigned long long seed, unsigned long long pos) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  curand_init(seed, (unsigned long long)i, 0ull, st + i);
+  skipahead(pos, st + i);
+}
+
 template <typename T>
 void upload(DeviceArray<T> &d, const std::vector<T> &v) {
   d.upload(v.empty() ? std::vector<T>(1) : v);
@@ -1295,6 +1709,289 @@ void CudaNoseHooverIntegrator::stepKernels(cudaStream_t s) {
   nh_pc_kernel<false><<<S.blocks_atoms, kThreads, 0, s>>>(S.c, S.natom, ke_ref, old);
   nh_final_kernel<<<S.blocks_groups, kThreads, 0, s>>>(S.c, ke_ref, old);
   APO_LAUNCH_CHECK();
+}
+
+// --------------------------------------------------------- Langevin piston
+
+struct PistonState {
+  DeviceArray<PistonScalars> ps;
+  DeviceArray<curandStatePhilox4_32_10_t> rng;
+  DeviceArray<double> partials;
+  double *h_box = nullptr;  // pinned: the box after each step
+  PistonState() {
+    APO_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&h_box), 3 * sizeof(double),
+                           cudaHostAllocDefault));
+  }
+  ~PistonState() {
+    if (h_box) cudaFreeHost(h_box);
+  }
+};
+
+CudaLangevinPistonIntegrator::CudaLangevinPistonIntegrator(double ps) : CudaIntegrator(ps) {
+  std::random_device rd;
+  m_Seed = rd();
+  m_KernelsPerStep = 2 + 2 * m_MaxPC;
+}
+
+CudaLangevinPistonIntegrator::~CudaLangevinPistonIntegrator() = default;
+
+void CudaLangevinPistonIntegrator::setCrystalType(Crystal c) {
+  switch (c) {
+    case Crystal::Cubic: m_Dof = 1; break;
+    case Crystal::Tetragonal: m_Dof = 2; break;
+    case Crystal::Orthorhombic: m_Dof = 3; break;
+    default:
+      throw std::invalid_argument("CudaLangevinPiston::setCrystalType: crystalType must be either "
+                                  "CRYSTAL::CUBIC, CRYSTAL::TETRAGONAL, or CRYSTAL::ORTHORHOMBIC");
+  }
+  m_Crystal = c;
+  // default piston mass 0.02 x total mass and no friction, as the reference
+  // sets them with the crystal type (src/CudaLangevinPistonIntegrator.cu:183-213)
+  double tm = -9999.9999;
+  if (m_Ctx) {
+    tm = 0.0;
+    for (double mm : m_Ctx->getForceManager()->topology().mass) tm += mm;
+    tm *= 0.02;
+  }
+  m_PMass.assign(m_Dof, tm);
+  m_PGamma = 0.0;
+  m_RngDirty = true;
+}
+
+void CudaLangevinPistonIntegrator::setPressure(const std::vector<double> &p) {
+  if (p.size() != 9)
+    throw std::invalid_argument("CudaLangevinPistonIntegrator::setPressure: reference pressure "
+                                "must be of length 9 (XX, XY, XZ, YX, YY, YZ, ZX, ZY, ZZ)");
+  m_Pref = p;
+  if (m_P) {
+    APO_CUDA(cudaStreamSynchronize(stream()));
+    APO_CUDA(cudaMemcpy(reinterpret_cast<char *>(m_P->ps.p) + offsetof(PistonScalars, pref),
+                        m_Pref.data(), 9 * sizeof(double), cudaMemcpyHostToDevice));
+  }
+}
+
+void CudaLangevinPistonIntegrator::setLangevinPistonMass(const std::vector<double> &m) {
+  if (m_Dof == -1)
+    throw std::runtime_error("CudaLangevinPistonIntegrator::setLangevinPistonMass: CrystalType "
+                             "must be set before Langevin piston mass");
+  if ((int)m.size() != m_Dof)
+    throw std::invalid_argument("CudaLangevinPistonIntegrator::setLangevinPistonMass: length of "
+                                "input vector must be equal to the degrees of freedom of the "
+                                "Langevin piston (" + std::to_string(m_Dof) + ")");
+  m_PMass = m;
+}
+
+void CudaLangevinPistonIntegrator::setNoseHooverPistonMass(double m) {
+  m_NHMass = m;
+  if (m_P) {
+    APO_CUDA(cudaStreamSynchronize(stream()));
+    APO_CUDA(cudaMemcpy(reinterpret_cast<char *>(m_S->sc.p) + offsetof(Scalars, piston_mass), &m,
+                        sizeof(double), cudaMemcpyHostToDevice));
+  }
+}
+
+void CudaLangevinPistonIntegrator::setLangevinPistonFrictionSeed(uint64_t seed) {
+  m_Seed = seed;
+  m_RngDirty = true;
+}
+
+void CudaLangevinPistonIntegrator::setRngSequencePos(unsigned long long pos) {
+  m_RngPos = pos;
+  m_RngDirty = true;
+}
+
+void CudaLangevinPistonIntegrator::setMaxPredictorCorrectorIterations(int n) {
+  if (n < 1)
+    throw std::invalid_argument("setMaxPredictorCorrectorIterations: at least one pass is needed");
+  m_MaxPC = n;
+  m_KernelsPerStep = 2 + 2 * m_MaxPC;
+}
+
+void CudaLangevinPistonIntegrator::resetAverages() {
+  if (!m_P) return;
+  resetAverageTemperature();
+  PistonScalars h;
+  APO_CUDA(cudaMemcpy(&h, m_P->ps.p, sizeof(h), cudaMemcpyDeviceToHost));
+  for (double &x : h.pavg) x = 0.0;
+  h.pavg_scalar = 0.0;
+  APO_CUDA(cudaMemcpy(m_P->ps.p, &h, sizeof(h), cudaMemcpyHostToDevice));
+}
+
+namespace {
+PistonScalars read_piston(const std::unique_ptr<PistonState> &P, cudaStream_t s) {
+  if (!P) throw std::runtime_error("CudaLangevinPistonIntegrator: no CharmmContext was set");
+  PistonScalars h;
+  APO_CUDA(cudaStreamSynchronize(s));
+  APO_CUDA(cudaMemcpy(&h, P->ps.p, sizeof(h), cudaMemcpyDeviceToHost));
+  return h;
+}
+}  // namespace
+
+std::vector<double> CudaLangevinPistonIntegrator::getInstantaneousPressureTensor() {
+  const PistonScalars h = read_piston(m_P, stream());
+  return std::vector<double>(h.p, h.p + 9);
+}
+double CudaLangevinPistonIntegrator::getInstantaneousPressureScalar() {
+  return read_piston(m_P, stream()).pscalar;
+}
+std::vector<double> CudaLangevinPistonIntegrator::getAveragePressureTensor() {
+  const PistonScalars h = read_piston(m_P, stream());
+  return std::vector<double>(h.pavg, h.pavg + 9);
+}
+double CudaLangevinPistonIntegrator::getAveragePressureScalar() {
+  return read_piston(m_P, stream()).pavg_scalar;
+}
+std::vector<double> CudaLangevinPistonIntegrator::getLangevinPistonOnStepPosition() {
+  const PistonScalars h = read_piston(m_P, stream());
+  return std::vector<double>(h.lp_onpos, h.lp_onpos + std::max(m_Dof, 0));
+}
+std::vector<double> CudaLangevinPistonIntegrator::getLangevinPistonDeltaPosition() {
+  const PistonScalars h = read_piston(m_P, stream());
+  return std::vector<double>(h.lp_delta, h.lp_delta + std::max(m_Dof, 0));
+}
+
+void CudaLangevinPistonIntegrator::initialize() {
+  auto fm = m_Ctx->getForceManager();
+  if (fm->isMulti())
+    throw std::invalid_argument("the Langevin piston scales one box: it is not available for a "
+                                "multi-system context");
+  if (m_Dof == -1)
+    throw std::runtime_error("CudaLangevinPistonIntegrator::initialize: CrystalType must be set "
+                             "before initialization (try setting the crystal type before setting "
+                             "the Charmm Context)");
+  double tm = 0.0;
+  for (double mm : fm->topology().mass) tm += mm;
+  if (m_NHMass == -9999.9999) m_NHMass = 0.2 * tm;
+  if (m_PMass.empty() || m_PMass[0] == -9999.9999) m_PMass.assign(m_Dof, 0.02 * tm);
+  IntegratorState &S = *m_S;
+  cudaStream_t s = m_Ctx->stream();
+  m_P = std::make_unique<PistonState>();
+  PistonState &P = *m_P;
+  P.ps.alloc(1);
+  P.rng.alloc(3);
+  P.partials.alloc((size_t)27 * std::max(S.blocks_groups, S.blocks_atoms) + 32);
+  PistonScalars h{};
+  const auto &box = fm->getBoxDimensions();
+  for (int d = 0; d < 3; ++d) h.box[d] = h.box_pred[d] = box[d];
+  for (int k = 0; k < 9; ++k) h.pref[k] = m_Pref[k];
+  APO_CUDA(cudaMemcpy(P.ps.p, &h, sizeof(h), cudaMemcpyHostToDevice));
+  Scalars sc{};
+  sc.piston_mass = m_NHMass;
+  APO_CUDA(cudaMemcpy(S.sc.p, &sc, sizeof(sc), cudaMemcpyHostToDevice));
+  lp_rng_init_kernel<<<1, 32, 0, s>>>(P.rng.p, m_Dof, m_Seed, m_RngPos);
+  m_RngDirty = false;
+  // as Nose-Hoover: constraints, first forces, the position-Verlet deltas
+  // (src/CudaLangevinPistonIntegrator.cu:626-704)
+  if (m_Ctx->isUsingHolonomicConstraints())
+    init_constrain_kernel<<<S.blocks_groups, kThreads, 0, s>>>(S.c, 0);
+  fm->calcForceChecked(m_Ctx->xyzq(), false, false, s);
+  init_delta_kernel<<<S.blocks_atoms, kThreads, 0, s>>>(S.c, S.natom, 0.0);
+  if (m_Ctx->isUsingHolonomicConstraints())
+    init_constrain_kernel<<<S.blocks_groups, kThreads, 0, s>>>(S.c, 1);
+  APO_LAUNCH_CHECK();
+  APO_CUDA(cudaStreamSynchronize(s));
+}
+
+// the step after the forces: half step, the predictor-corrector passes and
+// the final pass, with the piston constants of the current settings and
+// the volume of the current box
+void CudaLangevinPistonIntegrator::stepKernels(cudaStream_t s) {
+  IntegratorState &S = *m_S;
+  PistonState &P = *m_P;
+  auto fm = m_Ctx->getForceManager();
+  const auto &box = fm->getBoxDimensions();
+  const double V = box[0] * box[1] * box[2];
+  PistonArgs a{};
+  a.ps = P.ps.p;
+  a.rng = P.rng.p;
+  a.partials = P.partials.p;
+  a.vir_fixed = fm->deviceVirial();
+  // piston friction terms (setLangevinPistonFriction,
+  // src/CudaLangevinPistonIntegrator.cu:262-283)
+  const double kbt = kBoltz * m_RefT;
+  const double pgam = kTimfac * m_Dt * m_PGamma;
+  a.palpha = (1.0 - 0.5 * pgam) / (1.0 + 0.5 * pgam);
+  a.pbfact = m_Dt * m_Dt / (1.0 + 0.5 * pgam);
+  for (int i = 0; i < m_Dof; ++i) {
+    a.inv_mass[i] = m_PMass[i] == 0.0 ? 0.0 : 1.0 / m_PMass[i];
+    a.prfwd[i] = std::sqrt(2.0 * a.inv_mass[i] * pgam * kbt) / m_Dt;
+  }
+  a.vfac = kPatmos / V;
+  a.lp_vfac = V * a.pbfact * kAtmosp;
+  a.st_fac = m_SurfaceTension * kSurfaceTensionFactor / box[2];
+  a.ke_ref = 0.5 * (double)m_Ctx->getDegreesOfFreedom() * kBoltz * m_RefT;
+  a.crystal = (int)m_Crystal;
+  a.dof = m_Dof;
+  a.use_nh = m_UseNH ? 1 : 0;
+  a.use_old = m_OldT ? 1 : 0;
+  a.const_st = m_ConstST ? 1 : 0;
+  a.hol = m_Ctx->isUsingHolonomicConstraints() ? 1 : 0;
+  lp_half_kernel<<<S.blocks_groups, kThreads, 0, s>>>(S.c, a);
+  for (int k = 0; k < m_MaxPC; ++k) {
+    lp_ke_kernel<<<S.blocks_atoms, kThreads, 0, s>>>(S.c, a, S.natom);
+    lp_pc_kernel<<<S.blocks_atoms, kThreads, 0, s>>>(S.c, a, S.natom);
+  }
+  lp_final_kernel<<<S.blocks_groups, kThreads, 0, s>>>(S.c, a);
+  APO_LAUNCH_CHECK();
+}
+
+// One step at a time: centre-of-mass removal (on the device step counter),
+// a list build at the current box, forces with the virial, the step, then
+// the new box to the host and into the force manager (the reference ends
+// its step the same way, src/CudaLangevinPistonIntegrator.cu:2052-2056).  A
+// list that overflowed leaves the step kernels idle: the list is grown and
+// the step taken again.
+void CudaLangevinPistonIntegrator::propagate(int numSteps) {
+  if (!m_Ctx)
+    throw std::invalid_argument("CudaIntegrator::propagate: no CharmmContext was set for this CudaIntegrator.");
+  if (numSteps <= 0) return;
+  cudaStream_t s = m_Ctx->stream();
+  IntegratorState &S = *m_S;
+  PistonState &P = *m_P;
+  auto fm = m_Ctx->getForceManager();
+  if (m_RngDirty) {
+    lp_rng_init_kernel<<<1, 32, 0, s>>>(P.rng.p, m_Dof, m_Seed, m_RngPos);
+    APO_LAUNCH_CHECK();
+    m_RngDirty = false;
+  }
+  m_Ctx->ensureListBuffers();
+  int regrowths = 0;
+  for (int k = 0; k < numSteps;) {
+    if (m_ComFreq > 0) {
+      com_sum_kernel<<<S.blocks_atoms, kThreads, 0, s>>>(S.c, S.natom, m_ComFreq);
+      com_apply_kernel<<<S.blocks_atoms, kThreads, 0, s>>>(S.c, S.natom, m_ComFreq);
+      APO_LAUNCH_CHECK();
+    }
+    m_Ctx->resetNeighborList(s);
+    fm->calcForce(m_Ctx->xyzq(), false, true, s, /*clear=*/true);
+    stepKernels(s);
+    APO_CUDA(cudaMemcpyAsync(P.h_box, reinterpret_cast<char *>(P.ps.p) + offsetof(PistonScalars, box),
+                             3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    APO_CUDA(cudaStreamSynchronize(s));
+    const unsigned e = fm->readDeviceError(s);
+    if (e) {
+      if (e & kErrNaN)
+        throw std::runtime_error("non-finite coordinates during propagation (state kept at step " +
+                                 std::to_string(m_Step) + ")");
+      if (e & kErrCopyTimeout)
+        throw std::runtime_error("a tensor copy of the reciprocal-space grid did not complete "
+                                 "(state kept at step " + std::to_string(m_Step) + ")");
+      if (e & kErrColumnOverflow)
+        throw std::runtime_error("neighbour list: a cell column outgrew the column sort during "
+                                 "propagation (state kept at step " + std::to_string(m_Step) + ")");
+      if (++regrowths > 8)
+        throw std::runtime_error("neighbour list capacity exceeded repeatedly during propagation "
+                                 "(device error " + std::to_string(e) + ")");
+      fm->growNeighborList(m_Ctx->xyzq(), s);
+      continue;
+    }
+    m_RngPos += (unsigned long long)m_MaxPC;
+    fm->updateBoxDimensions({P.h_box[0], P.h_box[1], P.h_box[2]});
+    ++k;
+    ++m_Step;
+    for (auto &sub : m_Subscribers)
+      if (m_Step % sub->getReportFrequency() == 0) sub->update(*m_Ctx, m_Step, getTimeStep());
+  }
 }
 
 // ---------------------------------------------------------------- leapfrog

@@ -51,7 +51,7 @@ class CudaIntegrator : public std::enable_shared_from_this<CudaIntegrator> {
   // stops the reports of one subscriber (src/CudaIntegrator.cu unsubscribe);
   // true when it was subscribed
   bool unsubscribe(const std::shared_ptr<Subscriber> &sub);
-  void propagate(int numSteps);
+  virtual void propagate(int numSteps);
   long long getCurrentPropagatedStep() const { return m_Step; }
   double getInstantaneousTemperature();  // "Jung" estimate of the last step
   double getAverageTemperature();
@@ -132,6 +132,79 @@ class CudaNoseHooverIntegrator : public CudaIntegrator {
   void stepKernels(cudaStream_t s) override;
   double m_RefT = 300.0, m_PistonMass = -9999.9999;
   bool m_OldT = false;
+};
+
+// Constant pressure: Langevin piston on the box edges (Feller, Zhang, Pastor
+// & Brooks, J. Chem. Phys. 103, 4613 (1995)) with an optional Nose-Hoover
+// thermostat, after src/CudaLangevinPistonIntegrator.cu:1705-2060: a half
+// step, the constraint forces and their virial, the pressure tensor from
+// the half-step kinetic terms and the virial, then predictor-corrector
+// passes that move the piston (one Philox normal per piston degree of
+// freedom and pass, curand_init(seed, dof, 0) + skipahead), the thermostat
+// and the atoms together, the constraints applied to the new and the scaled
+// reference positions, and the on-step velocities.  Cubic, tetragonal and
+// orthorhombic cells.  Every step ends with the new box on the host, as in
+// the reference: the force manager takes it (updateBoxDimensions) and the
+// list is rebuilt at the next step, so steps are launched one by one
+// rather than as captured segments.
+enum class Crystal : int { None = 0, Cubic = 1, Orthorhombic = 2, Tetragonal = 3 };
+
+struct PistonState;  // device scalars, defined in integrators.cu
+
+class CudaLangevinPistonIntegrator : public CudaIntegrator {
+ public:
+  explicit CudaLangevinPistonIntegrator(double timeStepPs);
+  ~CudaLangevinPistonIntegrator() override;
+  void setCrystalType(Crystal c);
+  Crystal getCrystalType() const { return m_Crystal; }
+  int getPistonDegreesOfFreedom() const { return m_Dof; }
+  // reference pressure tensor (atm), row-major XX XY XZ YX YY YZ ZX ZY ZZ
+  void setPressure(const std::vector<double> &p);
+  std::vector<double> getReferencePressureTensor() const { return m_Pref; }
+  void setConstantSurfaceTension(bool f) { m_ConstST = f; }
+  void setSurfaceTension(double dyneCm) { m_SurfaceTension = dyneCm; }
+  // amu, one per piston degree of freedom; default 0.02 x total mass
+  void setLangevinPistonMass(const std::vector<double> &m);
+  std::vector<double> getLangevinPistonMass() const { return m_PMass; }
+  void setLangevinPistonFriction(double perPs) { m_PGamma = perPs; }
+  double getLangevinPistonFriction() const { return m_PGamma; }
+  void setLangevinPistonFrictionSeed(uint64_t seed);
+  uint64_t getLangevinPistonFrictionSeed() const { return m_Seed; }
+  void setRngSequencePos(unsigned long long pos);
+  unsigned long long getRngSequencePos() const { return m_RngPos; }
+  void setReferenceTemperature(double t) { m_RefT = t; }
+  double getReferenceTemperature() const { return m_RefT; }
+  void useNoseHooverThermostat(bool f) { m_UseNH = f; }
+  void setNoseHooverPistonMass(double m);
+  double getNoseHooverPistonMass() const { return m_NHMass; }
+  void useOldTemperature(bool f) { m_OldT = f; }
+  void setMaxPredictorCorrectorIterations(int n);
+  int getMaxPredictorCorrectorIterations() const { return m_MaxPC; }
+  void resetAverages();
+  // pressure tensor (atm) of the last step and its running average
+  std::vector<double> getInstantaneousPressureTensor();
+  double getInstantaneousPressureScalar();
+  std::vector<double> getAveragePressureTensor();
+  double getAveragePressureScalar();
+  // piston positions (box edges, A) and their last displacement
+  std::vector<double> getLangevinPistonOnStepPosition();
+  std::vector<double> getLangevinPistonDeltaPosition();
+  void propagate(int numSteps) override;
+
+ protected:
+  void initialize() override;
+  void stepKernels(cudaStream_t s) override;
+  void uploadPiston();
+  Crystal m_Crystal = Crystal::None;
+  int m_Dof = -1, m_MaxPC = 3;
+  std::vector<double> m_Pref{1, 0, 0, 0, 1, 0, 0, 0, 1};
+  std::vector<double> m_PMass;
+  double m_PGamma = 0.0, m_RefT = 300.0, m_NHMass = -9999.9999, m_SurfaceTension = 0.0;
+  bool m_UseNH = true, m_OldT = false, m_ConstST = false;
+  uint64_t m_Seed;
+  unsigned long long m_RngPos = 0;
+  bool m_RngDirty = true;
+  std::unique_ptr<PistonState> m_P;
 };
 
 class CudaLeapFrogIntegrator : public CudaIntegrator {

@@ -701,6 +701,20 @@ void NeighborList::refresh(cudaStream_t s) {
   APO_LAUNCH_CHECK();
 }
 
+void NeighborList::set_box(int sys, double Lx, double Ly, double Lz) {
+  if (sys < 0 || sys >= (int)m_sys_h.size()) throw std::invalid_argument("NeighborList: no such system");
+  if (!(Lx > 0.0 && Ly > 0.0 && Lz > 0.0) || Lx > 65536.0 || Ly > 65536.0 || Lz > 65536.0)
+    throw std::invalid_argument("NeighborList: box lengths must be in (0, 65536] A");
+  NbSysDims &d = m_sys_h[sys];
+  d.Lx = (float)Lx;
+  d.Ly = (float)Ly;
+  d.Lz = (float)Lz;
+  d.Lxd = Lx;
+  d.Lyd = Ly;
+  d.Lzd = Lz;
+  APO_CUDA(cudaMemcpy(m_sys + sys, &d, sizeof(NbSysDims), cudaMemcpyHostToDevice));
+}
+
 void NeighborList::set_capacity(int tile_cap, int work_cap) {
   if (tile_cap < 1 || work_cap < 1) throw std::invalid_argument("NeighborList: capacities must be positive");
   m_d.tile_cap = tile_cap;

@@ -89,6 +89,10 @@ class NeighborList {
   // tile and work-item capacity set by hand (the buffers are reallocated)
   void set_capacity(int tile_cap, int work_cap);
   void clear_error(cudaStream_t s);
+  // a new box for system `sys` with the same columns (a box that changes
+  // every step under pressure control); the next build uses it.  The
+  // caller has synchronised the stream the list's kernels run on.
+  void set_box(int sys, double Lx, double Ly, double Lz);
 
   const NbListDims &dims() const { return m_d; }
   const std::vector<NbSysDims> &system_dims() const { return m_sys_h; }

@@ -118,6 +118,16 @@ class Pme {
   // where the driver offers the encoder); a copy that does not complete sets
   // kErrCopyTimeout in `err`
   void set_tensor_copies(bool on) { m_tma_on = on; }
+  // a new box on the same grid (the influence function is formed from the
+  // box at every evaluation)
+  void set_box(double Lx, double Ly, double Lz) {
+    m_d.Lx = (float)Lx;
+    m_d.Ly = (float)Ly;
+    m_d.Lz = (float)Lz;
+    m_d.rLx = 1.0 / Lx;
+    m_d.rLy = 1.0 / Ly;
+    m_d.rLz = 1.0 / Lz;
+  }
   bool tensor_copies() const { return m_tma_on && m_tma; }
   void set_error_word(unsigned *err) { m_err = err; }
   int *qgrid = nullptr;     // nz*ny*nx int32 fixed point (zeroed by plane_fwd)

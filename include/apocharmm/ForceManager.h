@@ -139,7 +139,12 @@ class ForceManager {
   void setPmeSplineOrder(const int order) {
     apocharmm_detail::check(apo_force_manager_set_spline_order(m_H, order));
   }
-  std::vector<double> &getBoxDimensions(void) { return m_Box; }
+  // the box in force (the Langevin piston changes it every step)
+  std::vector<double> &getBoxDimensions(void) {
+    m_Box.resize(3);
+    apocharmm_detail::check(apo_force_manager_get_box_dimensions(m_Box.data(), 3, m_H));
+    return m_Box;
+  }
   std::shared_ptr<CharmmPSF> getPsf(void) { return m_Psf; }
   std::shared_ptr<CharmmParameters> getPrm(void) { return m_Prm; }
   int getNumAtoms() const {

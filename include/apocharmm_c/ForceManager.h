@@ -17,6 +17,8 @@ typedef struct apo_force_manager apo_force_manager;
 APOCHARMM_C_API apo_status apo_force_manager_create(apo_force_manager **out, const apo_charmm_psf *psf, const apo_charmm_parameters *parameters); /* :24 */
 APOCHARMM_C_API void apo_force_manager_destroy(apo_force_manager *force_manager); /* :28 */
 APOCHARMM_C_API apo_status apo_force_manager_set_box_dimensions(apo_force_manager *force_manager, const double x, const double y, const double z); /* :31 */
+/* the box in force (3 edges, A): changes every step under the Langevin piston */
+APOCHARMM_C_API apo_status apo_force_manager_get_box_dimensions(double *box, const size_t len, const apo_force_manager *force_manager);
 /* additions: ForceManager::setKappa/setCutoff/setCtonnb/setCtofnb/setFFTGrid/setPmeSplineOrder */
 APOCHARMM_C_API apo_status apo_force_manager_set_kappa(apo_force_manager *force_manager, const double kappa);
 APOCHARMM_C_API apo_status apo_force_manager_set_cutoff(apo_force_manager *force_manager, const double cutnb);

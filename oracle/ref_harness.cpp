@@ -49,6 +49,7 @@
 #include "CharmmCrd.h"
 #include "CharmmPSF.h"
 #include "CharmmParameters.h"
+#include "CudaLangevinPistonIntegrator.h"
 #include "CudaLangevinThermostatIntegrator.h"
 #include "CudaLeapFrogIntegrator.h"
 #include "CudaNeighborList.h"
@@ -244,12 +245,28 @@ int main(int argc, char **argv) {
       auto nh = std::make_shared<CudaNoseHooverIntegrator>(0.002);
       nh->setReferenceTemperature(300.0);
       integ = nh;
+    } else if (kind == "piston") {
+      // cubic Langevin piston at 1 atm with its Nose-Hoover thermostat at
+      // 300 K; `friction` is the piston's, `seed` its noise seed
+      auto lp = std::make_shared<CudaLangevinPistonIntegrator>(0.002);
+      lp->setCrystalType(CRYSTAL::CUBIC);
+      lp->setReferenceTemperature(300.0);
+      lp->setLangevinPistonFriction(friction);
+      lp->setLangevinPistonFrictionSeed(seed);
+      integ = lp;
     } else {
       std::fprintf(stderr, "unknown integrator %s\n", kind.c_str());
       return 2;
     }
     integ->setCharmmContext(s.ctx);
     if (steps > 0) integ->propagate(steps);
+    if (kind == "piston") {
+      const std::vector<double> b = s.fm->getBoxDimensions();
+      FILE *bf = std::fopen((std::string(argv[19]) + ".box").c_str(), "w");
+      if (!bf) return 3;
+      std::fprintf(bf, "%.17g %.17g %.17g\n", b[0], b[1], b[2]);
+      std::fclose(bf);
+    }
     cudaDeviceSynchronize();
     auto x = from_device(s.ctx->getCoordinatesCharges().getDeviceArray().data(), n);
     auto xf = from_device(s.ctx->getXYZQ().getDeviceArray().data(), n);

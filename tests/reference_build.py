@@ -53,6 +53,14 @@ def traj(paths, box, st, kind, steps, seed, friction, velocities, workdir, timeo
     return a[:, 0:3], a[:, 3:6], a[:, 6:9]
 
 
+def piston(paths, box, st, steps, seed, friction, velocities, workdir, timeout=900):
+    """The reference's cubic Langevin piston (1 atm, Nose-Hoover at 300 K,
+    piston friction and seed as given): (x FP64, x FP32, v, final box)."""
+    x, x32, v = traj(paths, box, st, "piston", steps, seed, friction, velocities, workdir, timeout)
+    b = np.loadtxt(os.path.join(workdir, "traj_piston.txt.box"))
+    return x, x32, v, b
+
+
 def nblist(paths, box, st, radius, workdir, timeout=900):
     """The reference's tile-list pairs within `radius`: (i, j, excluded) rows."""
     out = os.path.join(workdir, "ref_pairs.bin")

@@ -255,3 +255,46 @@ def test_dcd_subscriber_writes_frames(tmp_path):
     assert len(raw) == header + 4 * frame
     assert raw[4:8] == b"CORD"
     assert int.from_bytes(raw[8:12], "little") == 4
+
+
+def test_langevin_piston_orthorhombic_box_and_pressure(tmp_path):
+    """The orthorhombic Langevin piston (src/CudaLangevinPistonIntegrator.cu)
+    on a relaxed water box: every edge moves on its own, SETTLE holds the
+    waters at every new box, the pressure is finite, a DCD subscriber sees
+    the steps, a second run from the same state and seeds repeats the first
+    bit for bit, and a restart subscriber is refused as for the reference's
+    unsupported integrators."""
+    runs = []
+    for rep in range(2):
+        s, keep = _setup(tmp_path / f"r{rep}")
+        fm, ctx = keep[2], keep[3]
+        it = api.CudaLangevinPistonIntegrator(0.002)
+        it.setCrystalType(it.ORTHORHOMBIC)
+        it.setReferenceTemperature(300.0)
+        it.setLangevinPistonFriction(10.0)
+        it.setLangevinPistonFrictionSeed(11)
+        it.setCharmmContext(ctx)
+        assert len(it.getLangevinPistonMass()) == 3
+        dcd = api.DcdSubscriber(str(tmp_path / f"r{rep}.dcd"), 10)
+        it.subscribe(dcd)
+        it.propagate(30)
+        box = fm.getBoxDimensions()
+        x = ctx.getCoordinates()
+        runs.append((box, x, ctx.getVelocities(), it.getInstantaneousPressureScalar()))
+        assert it.getCurrentPropagatedStep() == 30
+        assert it.getRngSequencePos() == 90
+        assert np.all(np.abs(box - s.box) > 1e-7) and len(set(box.tolist())) == 3
+        np.testing.assert_allclose(it.getLangevinPistonOnStepPosition(), box, rtol=0, atol=1e-12)
+        d1, d2, d3 = _water_geometry(x)
+        assert np.abs(d1 - 0.9572).max() < 1e-6 and np.abs(d3 - np.sqrt(2.29189321)).max() < 1e-6
+        p = it.getInstantaneousPressureTensor()
+        assert np.isfinite(p).all() and np.isfinite(it.getAveragePressureScalar())
+        assert os.path.getsize(tmp_path / f"r{rep}.dcd") > 0
+        if rep == 1:
+            rst = api.RestartSubscriber(str(tmp_path / "p.rst"), 5)
+            it.subscribe(rst)
+            with pytest.raises(Exception):
+                it.propagate(5)
+    assert np.array_equal(runs[0][0], runs[1][0])
+    assert np.array_equal(runs[0][1], runs[1][1])
+    assert np.array_equal(runs[0][2], runs[1][2])

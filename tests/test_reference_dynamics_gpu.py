@@ -5,7 +5,8 @@ The reference's integrators: Langevin src/CudaLangevinThermostatIntegrator.cu
 (position update :576-640, noise curand_init(seed, atom, 0) + skipahead +
 curand_normal4 :805-814), Nose-Hoover src/CudaNoseHooverIntegrator.cu:838,
 leapfrog src/CudaLeapFrogIntegrator.cu:22-79 (no constraints, advances the
-single-precision coordinates only), SHAKE src/CudaHolonomicConstraint.cu:
+single-precision coordinates only), Langevin piston
+src/CudaLangevinPistonIntegrator.cu:1705-2060, SHAKE src/CudaHolonomicConstraint.cu:
 324-468.  The solute is ethylene glycol, whose X-H clusters have 2 and 3
 atoms: the reference's 4-atom SHAKE kernel (src/CudaHolonomicConstraint.cu:
 468-600) computes its multipliers but never moves the atoms, so a CH3 group
@@ -121,6 +122,42 @@ def test_leapfrog_trajectory_matches_reference_build(glycol):
     # ~2e-6 A on a bond of 545 kcal/mol/A^2 moves a hydrogen's velocity by
     # ~1e-4 of its size over 10 steps
     assert np.linalg.norm(vb - vr) / np.linalg.norm(vr) < 1e-4
+
+
+@pytest.mark.parametrize("friction", [0.0, 20.0])
+def test_langevin_piston_trajectory_matches_reference_build(glycol, friction):
+    """Constant pressure: the reference's cubic Langevin piston at 1 atm with
+    its Nose-Hoover thermostat at 300 K (src/CudaLangevinPistonIntegrator.cu:
+    1705-2060), same coordinates, velocities and piston seed.  After 10 steps
+    (SETTLE and SHAKE, three predictor-corrector passes a step, a new box
+    every step) the box edge and the coordinates agree; at 20/ps the piston
+    noise dominates the box motion, so agreement shows equal noise streams."""
+    tmp, s, paths, pos, v = glycol
+    xr, _, vr, boxr = rb.piston(paths, s.box, s.settings, 10, 77, friction, v, str(tmp))
+    keep = api.system_context(s, str(tmp / f"b200_piston_{friction}"))
+    fm, ctx = keep[2], keep[3]
+    ctx.setCoordinates(pos)
+    ctx.setVelocities(v)
+    it = api.CudaLangevinPistonIntegrator(0.002)
+    it.setCrystalType(it.CUBIC)
+    it.setReferenceTemperature(300.0)
+    it.setLangevinPistonFriction(friction)
+    it.setLangevinPistonFrictionSeed(77)
+    it.setCharmmContext(ctx)
+    it.propagate(10)
+    box = fm.getBoxDimensions()
+    x, vb = ctx.getCoordinates(), ctx.getVelocities()
+    dx = _wrapped_diff(x, xr, box)
+    dbox = np.abs(box - boxr).max()
+    print(f"piston {friction}/ps: box {box[0]:.9f} (reference {boxr[0]:.9f}, start {s.box[0]}), "
+          f"|dbox| {dbox:.2e} A, max |dx| {np.abs(dx).max():.2e} A, velocity rel-RMS "
+          f"{np.linalg.norm(vb - vr) / np.linalg.norm(vr):.2e}; P {it.getInstantaneousPressureScalar():.1f} atm")
+    assert box[0] == box[1] == box[2]
+    assert abs(box[0] - s.box[0]) > 1e-7          # the piston moved
+    assert dbox < 1e-6
+    assert np.abs(dx).max() < 1e-5
+    assert np.linalg.norm(vb - vr) / np.linalg.norm(vr) < 1e-5
+    assert it.getRngSequencePos() == 30
 
 
 def _canonical(pairs, pos, box, radius):
