@@ -1955,6 +1955,7 @@ void CudaLangevinPistonIntegrator::propagate(int numSteps) {
     m_RngDirty = false;
   }
   m_Ctx->ensureListBuffers();
+  fm->rewindKernelTimers();
   int regrowths = 0;
   for (int k = 0; k < numSteps;) {
     if (m_ComFreq > 0) {

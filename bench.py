@@ -59,6 +59,8 @@ FLOP_PER_PAIR = 65
 NB_TRAFFIC = {
     "chain23k": (2193920, "ncu capture of this kernel on this workload "
                           "(dram__bytes_read.sum + dram__bytes_write.sum)"),
+    "chain23k_npt": (2193920, "ncu capture of this kernel on the same system at constant "
+                              "volume (dram__bytes_read.sum + dram__bytes_write.sum)"),
 }
 
 
@@ -173,6 +175,11 @@ WORKLOADS = {
                           "gamma 1/ps, dt 2 fs, SETTLE"),
     # the reference's leapfrog has no constraints (src/CudaLeapFrogIntegrator.cu:43-79):
     # its arm runs this workload with the Langevin integrator at zero friction
+    # the same system at constant pressure (the reference's Langevin piston)
+    "chain23k_npt": dict(factory="config_solvated_chain", integrator="piston", friction=20.0,
+                         desc="chain23k_npt: the chain23k system at 1 atm, cubic Langevin piston "
+                              "(mass 0.02 x total mass, friction 20/ps), Nose-Hoover 300 K, "
+                              "dt 2 fs, SETTLE, a new box every step"),
     "water12k": dict(factory="config_small_water", integrator="leapfrog", friction=0.0,
                      ref_integrator="langevin",
                      desc="water12k: 12,480-atom TIP3P box, 50 A, PME 48^3 order 4, cutoff 10 "
@@ -592,6 +599,12 @@ def make_integrator(api, spec, rank):
         integ.setThermostatRngSeed(777 + rank)
     elif kind == "leapfrog":
         integ = api.CudaLeapFrogIntegrator(DT_PS)
+    elif kind == "piston":
+        integ = api.CudaLangevinPistonIntegrator(DT_PS)
+        integ.setCrystalType(integ.CUBIC)
+        integ.setReferenceTemperature(300.0)
+        integ.setLangevinPistonFriction(spec["friction"])
+        integ.setLangevinPistonFrictionSeed(777 + rank)
     else:
         integ = api.CudaNoseHooverIntegrator(DT_PS)
         integ.setReferenceTemperature(300.0)
@@ -769,7 +782,10 @@ def main():
         if not args.no_cpu_baseline:
             cb = cpu_baseline(s)
         kps = integ.getKernelsPerStep()
-        launches = args.steps * (12 + SEG * (7 + kps))
+        if spec["integrator"] == "piston":  # a list build every step, no graphs
+            launches = args.steps * SEG * (11 + 7 + kps + 2)
+        else:
+            launches = args.steps * (12 + SEG * (7 + kps))
         line = {
             "metric": "ns/day", "value": value, "unit": "ns/day", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,

@@ -4,6 +4,7 @@
 // getCurrentPropagatedStep, initializeFromRestartFile),
 // include/CudaLangevinThermostatIntegrator.h:24-34,
 // include/CudaNoseHooverIntegrator.h, include/CudaLeapFrogIntegrator.h,
+// include/CudaLangevinPistonIntegrator.h:18-60 (constant pressure),
 // include/Subscriber.h, include/DcdSubscriber.h, include/RestartSubscriber.h,
 // header-only over the C ABI.  An integrator keeps its context and its
 // subscribers alive.
@@ -18,6 +19,7 @@
 #include "apocharmm/CharmmContext.h"
 #include "apocharmm/Check.h"
 #include "apocharmm_c/CudaIntegrator.h"
+#include "apocharmm_c/CudaLangevinPistonIntegrator.h"
 #include "apocharmm_c/CudaLangevinThermostatIntegrator.h"
 #include "apocharmm_c/CudaNoseHooverIntegrator.h"
 #include "apocharmm_c/DcdSubscriber.h"
@@ -237,4 +239,107 @@ class CudaLeapFrogIntegrator : public CudaIntegrator {
 
  private:
   apo_cuda_leap_frog_integrator *m_H = nullptr;
+};
+
+// the reference's enum CRYSTAL (include/PBC.h:15)
+enum class CRYSTAL { NONE = 0, CUBIC = 1, ORTHORHOMBIC = 2, TETRAGONAL = 3 };
+
+class CudaLangevinPistonIntegrator : public CudaIntegrator {
+ public:
+  explicit CudaLangevinPistonIntegrator(const double timeStep) : CudaIntegrator(timeStep) {
+    apocharmm_detail::check(apo_cuda_langevin_piston_integrator_create(&m_H, timeStep));
+    apocharmm_detail::check(apo_cuda_langevin_piston_integrator_as_cuda_integrator(&m_Base, m_H));
+  }
+  ~CudaLangevinPistonIntegrator() override { apo_cuda_langevin_piston_integrator_destroy(m_H); }
+  void setCrystalType(const CRYSTAL crystalType) {
+    apocharmm_detail::check(apo_cuda_langevin_piston_integrator_set_crystal_type(m_H, (int)crystalType));
+  }
+  void setPressure(const std::vector<double> &referencePressure) {
+    apocharmm_detail::check(apo_cuda_langevin_piston_integrator_set_pressure(
+        m_H, referencePressure.data(), referencePressure.size()));
+  }
+  void setLangevinPistonMass(const std::vector<double> &mass) {
+    apocharmm_detail::check(
+        apo_cuda_langevin_piston_integrator_set_langevin_piston_mass(m_H, mass.data(), mass.size()));
+  }
+  std::vector<double> getLangevinPistonMass(void) const {
+    std::vector<double> m(3);
+    size_t n = 0;
+    apocharmm_detail::check(
+        apo_cuda_langevin_piston_integrator_get_langevin_piston_mass(m.data(), m.size(), &n, m_H));
+    m.resize(n);
+    return m;
+  }
+  void setLangevinPistonFriction(const double pgamma) {
+    apocharmm_detail::check(apo_cuda_langevin_piston_integrator_set_langevin_piston_friction(m_H, pgamma));
+  }
+  void setLangevinPistonFrictionSeed(const std::uint64_t seed) {
+    apocharmm_detail::check(
+        apo_cuda_langevin_piston_integrator_set_langevin_piston_friction_seed(m_H, seed));
+  }
+  void setRngSequencePos(const unsigned long long pos) {
+    apocharmm_detail::check(apo_cuda_langevin_piston_integrator_set_rng_sequence_pos(m_H, pos));
+  }
+  unsigned long long getRngSequencePos(void) const {
+    unsigned long long p = 0;
+    apocharmm_detail::check(apo_cuda_langevin_piston_integrator_get_rng_sequence_pos(&p, m_H));
+    return p;
+  }
+  void setReferenceTemperature(const double referenceTemperature) {
+    apocharmm_detail::check(
+        apo_cuda_langevin_piston_integrator_set_reference_temperature(m_H, referenceTemperature));
+  }
+  void useNoseHooverThermostat(const bool flag) {
+    apocharmm_detail::check(apo_cuda_langevin_piston_integrator_use_nose_hoover_thermostat(m_H, flag));
+  }
+  void setNoseHooverPistonMass(const double mass) {
+    apocharmm_detail::check(apo_cuda_langevin_piston_integrator_set_nose_hoover_piston_mass(m_H, mass));
+  }
+  void useOldTemperature(const bool flag) {
+    apocharmm_detail::check(apo_cuda_langevin_piston_integrator_use_old_temperature(m_H, flag));
+  }
+  void setMaxPredictorCorrectorIterations(const int n) {
+    apocharmm_detail::check(
+        apo_cuda_langevin_piston_integrator_set_max_predictor_corrector_iterations(m_H, n));
+  }
+  void setConstantSurfaceTension(const bool flag, const double surfaceTension = 0.0) {
+    apocharmm_detail::check(
+        apo_cuda_langevin_piston_integrator_set_constant_surface_tension(m_H, flag, surfaceTension));
+  }
+  void resetAverages(void) {
+    apocharmm_detail::check(apo_cuda_langevin_piston_integrator_reset_averages(m_H));
+  }
+  std::vector<double> getInstantaneousPressureTensor(void) {
+    std::vector<double> p(9);
+    apocharmm_detail::check(
+        apo_cuda_langevin_piston_integrator_get_instantaneous_pressure_tensor(p.data(), p.size(), m_H));
+    return p;
+  }
+  std::vector<double> getAveragePressureTensor(void) {
+    std::vector<double> p(9);
+    apocharmm_detail::check(
+        apo_cuda_langevin_piston_integrator_get_average_pressure_tensor(p.data(), p.size(), m_H));
+    return p;
+  }
+  double getInstantaneousPressureScalar(void) {
+    double p = 0.0;
+    apocharmm_detail::check(apo_cuda_langevin_piston_integrator_get_instantaneous_pressure_scalar(&p, m_H));
+    return p;
+  }
+  double getAveragePressureScalar(void) {
+    double p = 0.0;
+    apocharmm_detail::check(apo_cuda_langevin_piston_integrator_get_average_pressure_scalar(&p, m_H));
+    return p;
+  }
+  std::vector<double> getLangevinPistonOnStepPosition(void) {
+    std::vector<double> x(3);
+    size_t n = 0;
+    apocharmm_detail::check(apo_cuda_langevin_piston_integrator_get_langevin_piston_on_step_position(
+        x.data(), x.size(), &n, m_H));
+    x.resize(n);
+    return x;
+  }
+
+ private:
+  apo_cuda_langevin_piston_integrator *m_H = nullptr;
 };

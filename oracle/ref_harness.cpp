@@ -190,6 +190,13 @@ int main(int argc, char **argv) {
       auto nh = std::make_shared<CudaNoseHooverIntegrator>(0.002);
       nh->setReferenceTemperature(300.0);
       integ = nh;
+    } else if (kind == "piston") {
+      auto lp = std::make_shared<CudaLangevinPistonIntegrator>(0.002);
+      lp->setCrystalType(CRYSTAL::CUBIC);
+      lp->setReferenceTemperature(300.0);
+      lp->setLangevinPistonFriction(std::atof(argv[17]));
+      lp->setLangevinPistonFrictionSeed(seed);
+      integ = lp;
     } else {
       std::fprintf(stderr, "unknown integrator %s\n", kind.c_str());
       return 2;

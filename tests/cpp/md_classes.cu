@@ -95,6 +95,19 @@ int main(int argc, char **argv) {
     leap.setCharmmContext(ctx);
     leap.propagate(5);
     res << "leapfrog_step " << leap.getCurrentPropagatedStep() << "\n";
+
+    // and at constant pressure (cubic Langevin piston, 1 atm)
+    CudaLangevinPistonIntegrator piston(0.001);
+    piston.setCrystalType(CRYSTAL::CUBIC);
+    piston.setReferenceTemperature(300.0);
+    piston.setLangevinPistonFriction(10.0);
+    piston.setLangevinPistonFrictionSeed(5);
+    piston.setCharmmContext(ctx);
+    piston.propagate(5);
+    const auto b = ctx->getBoxDimensions();
+    res << "piston_box " << b[0] << " " << b[1] << " " << b[2] << "\n";
+    res << "piston_pressure " << piston.getInstantaneousPressureScalar() << " "
+        << piston.getLangevinPistonMass().size() << " " << piston.getRngSequencePos() << "\n";
     res << "done\n";
   } catch (const std::exception &ex) {
     std::fprintf(stderr, "error: %s\n", ex.what());

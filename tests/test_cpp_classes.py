@@ -244,3 +244,6 @@ def test_md_classes_match_python_api(tmp_path):
         np.testing.assert_array_equal(a[key], b[key])
     assert os.path.getsize(out / "traj.dcd") == os.path.getsize(py / "traj.dcd") > 0
     assert res["leapfrog_step"] == ["5"]
+    pb = [float(x) for x in res["piston_box"]]
+    assert pb[0] == pb[1] == pb[2] and pb[0] != s.box[0]
+    assert np.isfinite(float(res["piston_pressure"][0])) and res["piston_pressure"][1:] == ["1", "15"]
