@@ -1542,10 +1542,11 @@ RestartRecord CudaIntegrator::restartRecord() {
   if (!m_S || !m_Ctx) throw std::runtime_error("restart: no CharmmContext was set for this integrator");
   auto *lt = dynamic_cast<CudaLangevinThermostatIntegrator *>(this);
   auto *nh = dynamic_cast<CudaNoseHooverIntegrator *>(this);
-  if (!lt && !nh)
+  auto *lp = dynamic_cast<CudaLangevinPistonIntegrator *>(this);
+  if (!lt && !nh && !lp)
     throw std::runtime_error("Attempted to write a restart file for an unsupported integrator type. "
-                             "The supported integrators are CudaLangevinThermostatIntegrator and "
-                             "CudaNoseHooverIntegrator.");
+                             "The supported integrators are CudaNoseHooverIntegrator, "
+                             "CudaLangevinPistonIntegrator and CudaLangevinThermostatIntegrator.");
   if (m_Ctx->getForceManager()->isMulti())
     throw std::runtime_error("restart files describe one system: not available for a "
                              "multi-system context");
@@ -1568,6 +1569,15 @@ RestartRecord CudaIntegrator::restartRecord() {
     r.pnhv = h.piston_v;
     r.pnhf = h.piston_f;
   }
+  if (lp) {  // src/RestartSubscriber.cu:124-139, 246-250
+    r.seed = lp->getLangevinPistonFrictionSeed();
+    r.has_rng = true;
+    r.rngpos = lp->getRngSequencePos();
+    const Crystal c = lp->getCrystalType();
+    r.crystal = c == Crystal::Cubic ? "CUBI" : (c == Crystal::Tetragonal ? "TETR" : "ORTH");
+    const auto d = lp->getLangevinPistonDeltaPosition();
+    for (size_t k = 0; k < d.size() && k < 3; ++k) r.hdot[k] = d[k];
+  }
   r.xold = m_Ctx->getCoordinates();
   r.vel = m_Ctx->getVelocities();
   std::vector<double4> d(m_S->natom);
@@ -1587,9 +1597,10 @@ void CudaIntegrator::initializeFromRestartFile(const std::string &path) {
     throw std::runtime_error("CharmmContext must be set before initializing from a restart file");
   auto *lt = dynamic_cast<CudaLangevinThermostatIntegrator *>(this);
   auto *nh = dynamic_cast<CudaNoseHooverIntegrator *>(this);
-  if (!lt && !nh)
-    throw std::runtime_error("initializeFromRestartFile: only the Langevin thermostat and "
-                             "Nose-Hoover integrators read restart files");
+  auto *lp = dynamic_cast<CudaLangevinPistonIntegrator *>(this);
+  if (!lt && !nh && !lp)
+    throw std::runtime_error("initializeFromRestartFile: only the Langevin thermostat, "
+                             "Nose-Hoover and Langevin piston integrators read restart files");
   auto fm = m_Ctx->getForceManager();
   if (fm->isMulti())
     throw std::runtime_error("restart files describe one system: not available for a "
@@ -1637,6 +1648,7 @@ void CudaIntegrator::initializeFromRestartFile(const std::string &path) {
   APO_CUDA(cudaMemcpy(m_S->sc.p, &h, sizeof(h), cudaMemcpyHostToDevice));
   m_Step = r.npriv;
   clearGraphs();  // the captured launches hold the seed
+  if (lp) lp->applyRestartRecord(r);
 }
 
 unsigned long long CudaLangevinThermostatIntegrator::getRngSequencePos() {
@@ -1890,6 +1902,32 @@ void CudaLangevinPistonIntegrator::initialize() {
     init_constrain_kernel<<<S.blocks_groups, kThreads, 0, s>>>(S.c, 1);
   APO_LAUNCH_CHECK();
   APO_CUDA(cudaStreamSynchronize(s));
+}
+
+void CudaLangevinPistonIntegrator::applyRestartRecord(const RestartRecord &r) {
+  const Crystal c = r.crystal == "CUBI" ? Crystal::Cubic
+                    : r.crystal == "TETR" ? Crystal::Tetragonal
+                    : r.crystal == "ORTH" ? Crystal::Orthorhombic
+                                          : Crystal::None;
+  if (c == Crystal::None)
+    throw std::runtime_error("restart file: crystal type \"" + r.crystal +
+                             "\" is not one the Langevin piston moves");
+  // another crystal type resets the piston mass and friction to their
+  // defaults, as the reference's reader does (it always calls setCrystalType)
+  if (c != m_Crystal) setCrystalType(c);
+  auto fm = m_Ctx->getForceManager();
+  APO_CUDA(cudaStreamSynchronize(stream()));
+  fm->updateBoxDimensions(r.box);
+  PistonScalars h;
+  APO_CUDA(cudaMemcpy(&h, m_P->ps.p, sizeof(h), cudaMemcpyDeviceToHost));
+  for (int d = 0; d < 3; ++d) {
+    h.box[d] = h.box_pred[d] = r.box[d];
+    h.lp_delta[d] = d < m_Dof ? r.hdot[d] : 0.0;
+  }
+  APO_CUDA(cudaMemcpy(m_P->ps.p, &h, sizeof(h), cudaMemcpyHostToDevice));
+  setLangevinPistonFrictionSeed(r.seed);
+  // a file without the APO tag carries no RNG position (as the reference reads it)
+  setRngSequencePos((r.apo && r.has_rng) ? r.rngpos : 0ull);
 }
 
 // the step after the forces: half step, the predictor-corrector passes and

@@ -190,11 +190,14 @@ class CudaLangevinPistonIntegrator : public CudaIntegrator {
   std::vector<double> getLangevinPistonOnStepPosition();
   std::vector<double> getLangevinPistonDeltaPosition();
   void propagate(int numSteps) override;
+  // the piston part of a restart record (crystal tag, HDOT, box, seed and
+  // RNG position), after the base class has restored the atoms and the
+  // thermostat (src/CudaLangevinPistonIntegrator.cu:706-1020)
+  void applyRestartRecord(const RestartRecord &r);
 
  protected:
   void initialize() override;
   void stepKernels(cudaStream_t s) override;
-  void uploadPiston();
   Crystal m_Crystal = Crystal::None;
   int m_Dof = -1, m_MaxPC = 3;
   std::vector<double> m_Pref{1, 0, 0, 0, 1, 0, 0, 0, 1};

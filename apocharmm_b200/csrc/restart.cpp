@@ -113,7 +113,10 @@ void writeRestartFile(const std::string &path, const RestartRecord &r) {
     throw std::invalid_argument("restart file: per-atom arrays must hold 3 x NATOM values");
   std::ostringstream o;
   const auto &b = r.box;
-  const char *crystal = (b[0] == b[1] && b[0] == b[2]) ? "CUBI" : (b[0] == b[1] ? "TETR" : "ORTH");
+  std::string crystal = r.crystal;
+  if (crystal.empty())
+    crystal = (b[0] == b[1] && b[0] == b[2]) ? "CUBI" : (b[0] == b[1] ? "TETR" : "ORTH");
+  if (crystal.size() != 4) throw std::invalid_argument("restart file: crystal tag must have 4 characters");
   o << "REST" << pad_left(std::to_string(kVersion), 6) << pad_left("1", 6) << "  " << crystal
     << "  " << "    " << "  " << "APO" << "\n\n";
   o << pad_left("2", 8) << " !NTITLE followed by title\n";
@@ -121,7 +124,7 @@ void writeRestartFile(const std::string &path, const RestartRecord &r) {
   o << "* USED FOR CONTINUING MOLECULAR DYNAMICS TRAJECTORY\n\n";
   o << " !CRYSTAL PARAMETERS\n";
   o << line_of({b[0], 0.0, b[1]}) << line_of({0.0, 0.0, b[2]});
-  o << line_of({0.0, 0.0, 0.0}) << line_of({0.0, 0.0, 0.0});       // HDOT
+  o << line_of({r.hdot[0], r.hdot[1], r.hdot[2]}) << line_of({0.0, 0.0, 0.0});  // HDOT
   o << line_of({0.0, r.pnhv, r.pnhf});                              // PNH, PNHV, PNHF
   for (int k = 0; k < 8; ++k) o << line_of({0.0, 0.0, 0.0});        // UC1A..UC2B
   o << line_of({0.0, 0.0, 0.0}) << line_of({0.0}) << "\n";          // GRAD1A..GRAD2B
@@ -171,6 +174,7 @@ RestartRecord readRestartFile(const std::string &path) {
   if (!getline_checked(in, line) || line.compare(0, 4, "REST") != 0)
     throw std::runtime_error("\"" + path + "\" is not a restart file");
   r.apo = line.size() >= 33 && line.substr(30, 3) == "APO";
+  if (line.size() >= 22) r.crystal = line.substr(18, 4);
   find_section(in, " !CRYSTAL PARAMETERS", path);
   std::vector<std::string> cry(5);
   for (auto &l : cry)
@@ -178,6 +182,7 @@ RestartRecord readRestartFile(const std::string &path) {
   r.box[0] = parseRestartDouble(field(cry[0], 0, kWidth, "XTLABC"));
   r.box[1] = parseRestartDouble(field(cry[0], 44, kWidth, "XTLABC"));
   r.box[2] = parseRestartDouble(field(cry[1], 44, kWidth, "XTLABC"));
+  for (int k = 0; k < 3; ++k) r.hdot[k] = parseRestartDouble(field(cry[2], k * kWidth, kWidth, "HDOT"));
   r.pnhv = parseRestartDouble(field(cry[4], 22, kWidth, "PNHV"));
   r.pnhf = parseRestartDouble(field(cry[4], 44, kWidth, "PNHF"));
   find_section(in, " !NATOM,NPRIV,NSTEP,NSAVC,NSAVV,JHSTRT,NDEGF,SEED,NSAVL", path);

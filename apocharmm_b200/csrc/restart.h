@@ -30,14 +30,18 @@ namespace apo {
 
 struct RestartRecord {
   std::array<double, 3> box{};       // orthorhombic cell edges (A)
+  // crystal tag of the header ("CUBI", "TETR", "ORTH"); empty: from the box
+  // edges when writing, as the reference does for its thermostats
+  std::string crystal;
+  std::array<double, 3> hdot{};      // Langevin piston displacement (HDOT)
   double pnhv = 0.0, pnhf = 0.0;     // Nose-Hoover piston velocity and force
   int natom = 0;
   long long npriv = 0;               // steps taken since the run began
   long long nstep = 0;               // steps of the run that wrote the file
   int nsavc = 0;                     // report frequency of the writer
   int ndegf = 0;
-  uint64_t seed = 0;                 // Langevin thermostat seed
-  bool has_rng = false;              // RNG position present (Langevin thermostat)
+  uint64_t seed = 0;                 // Langevin thermostat or piston seed
+  bool has_rng = false;              // RNG position present (Langevin thermostat or piston)
   unsigned long long rngpos = 0;     // Philox sequence position
   double avetem = 0.0;               // running average temperature
   bool apo = true;                   // header carries the "APO" tag

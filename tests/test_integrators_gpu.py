@@ -262,8 +262,8 @@ def test_langevin_piston_orthorhombic_box_and_pressure(tmp_path):
     on a relaxed water box: every edge moves on its own, SETTLE holds the
     waters at every new box, the pressure is finite, a DCD subscriber sees
     the steps, a second run from the same state and seeds repeats the first
-    bit for bit, and a restart subscriber is refused as for the reference's
-    unsupported integrators."""
+    bit for bit, and a restart subscriber records the piston's box, seed and
+    noise position."""
     runs = []
     for rep in range(2):
         s, keep = _setup(tmp_path / f"r{rep}")
@@ -293,8 +293,10 @@ def test_langevin_piston_orthorhombic_box_and_pressure(tmp_path):
         if rep == 1:
             rst = api.RestartSubscriber(str(tmp_path / "p.rst"), 5)
             it.subscribe(rst)
-            with pytest.raises(Exception):
-                it.propagate(5)
+            it.propagate(5)
+            head = api.read_restart_file(tmp_path / "p.rst")
+            assert head["npriv"] == 35 and head["seed"] == 11 and head["rngpos"] == 105
+            np.testing.assert_array_equal(head["box"], fm.getBoxDimensions())
     assert np.array_equal(runs[0][0], runs[1][0])
     assert np.array_equal(runs[0][1], runs[1][1])
     assert np.array_equal(runs[0][2], runs[1][2])

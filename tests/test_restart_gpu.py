@@ -156,3 +156,45 @@ def test_restart_errors(tmp_path):
     it.setCharmmContext(keep2[3])
     with pytest.raises(ApoCharmmError, match="NATOM mismatch"):
         it.initializeFromRestartFile(str(tmp_path / "small.rst"))
+
+
+def test_piston_resumed_run_matches_uninterrupted_run(tmp_path):
+    """The Langevin piston's restart file (crystal tag, HDOT, box, thermostat
+    piston, seed and noise position, src/RestartSubscriber.cu:124-139) lets a
+    fresh context continue the run bit for bit, the box included.  Piston
+    friction 0: the reference re-seeds the noise by skipping the count of
+    normals drawn, which does not resume the same stream once noise has
+    weight, and this engine reads the file the same way."""
+    def make():
+        it = api.CudaLangevinPistonIntegrator(0.002)
+        it.setCrystalType(it.ORTHORHOMBIC)
+        it.setReferenceTemperature(300.0)
+        it.setLangevinPistonFrictionSeed(5)
+        return it
+
+    s, keep1 = _context(tmp_path / "a")
+    start = keep1[3].getCoordinates()
+    it1 = make()
+    it1.setCharmmContext(keep1[3])
+    rst = tmp_path / "run.rst"
+    it1.subscribe(api.RestartSubscriber(str(rst), 40))
+    it1.propagate(40)
+    saved = tmp_path / "at40.rst"
+    shutil.copy(rst, saved)
+    it1.propagate(60)
+    x1, v1, b1 = keep1[3].getCoordinates(), keep1[3].getVelocities(), keep1[2].getBoxDimensions()
+
+    s2, keep2 = _context(tmp_path / "b", relax=False)
+    keep2[3].setCoordinates(start)
+    it2 = make()
+    it2.setCharmmContext(keep2[3])
+    it2.initializeFromRestartFile(str(saved))
+    head = api.read_restart_file(saved)
+    assert head["npriv"] == 40 and it2.getCurrentPropagatedStep() == 40
+    assert not np.array_equal(head["box"], s.box)
+    it2.propagate(60)
+    x2, v2, b2 = keep2[3].getCoordinates(), keep2[3].getVelocities(), keep2[2].getBoxDimensions()
+    assert np.array_equal(b1, b2), b1 - b2
+    assert np.array_equal(x1, x2), np.abs(x1 - x2).max()
+    assert np.array_equal(v1, v2), np.abs(v1 - v2).max()
+    assert it2.getCurrentPropagatedStep() == 100
