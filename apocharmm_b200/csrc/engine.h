@@ -108,7 +108,10 @@ class ForceManager {
   // without a new initialisation; the list is rebuilt at the next
   // evaluation and graphs captured with the old box are dropped.  The
   // caller has synchronised the context's stream.
-  void updateBoxDimensions(const std::array<double, 3> &box);
+  // keep_list: the built list follows the box (its periodic shifts are
+  // rescaled on stream s) instead of being rebuilt at the next evaluation
+  void updateBoxDimensions(const std::array<double, 3> &box, bool keep_list = false,
+                           cudaStream_t s = nullptr);
   void setKappa(double k) { m_Kappa = k; m_Initialized = false; }
   void setCutoff(double c) { m_Cutoff = c; m_Initialized = false; }
   void setCtonnb(double c) { m_Ctonnb = c; m_Initialized = false; }

@@ -1974,11 +1974,11 @@ void CudaLangevinPistonIntegrator::stepKernels(cudaStream_t s) {
 }
 
 // One step at a time: centre-of-mass removal (on the device step counter),
-// a list build at the current box, forces with the virial, the step, then
-// the new box to the host and into the force manager (the reference ends
-// its step the same way, src/CudaLangevinPistonIntegrator.cu:2052-2056).  A
-// list that overflowed leaves the step kernels idle: the list is grown and
-// the step taken again.
+// a list build every m_ListFreq steps, forces with the virial, the step,
+// then the new box to the host and into the force manager (the reference
+// ends its step the same way, src/CudaLangevinPistonIntegrator.cu:2052-2056),
+// whose list follows the box until the next build.  A list that overflowed
+// leaves the step kernels idle: the list is grown and the step taken again.
 void CudaLangevinPistonIntegrator::propagate(int numSteps) {
   if (!m_Ctx)
     throw std::invalid_argument("CudaIntegrator::propagate: no CharmmContext was set for this CudaIntegrator.");
@@ -2001,13 +2001,16 @@ void CudaLangevinPistonIntegrator::propagate(int numSteps) {
       com_apply_kernel<<<S.blocks_atoms, kThreads, 0, s>>>(S.c, S.natom, m_ComFreq);
       APO_LAUNCH_CHECK();
     }
-    m_Ctx->resetNeighborList(s);
+    // the list is built at the reference's cadence (every m_ListFreq steps
+    // from the start of the call) and follows the box in between
+    if (k % m_ListFreq == 0) m_Ctx->resetNeighborList(s);
     fm->calcForce(m_Ctx->xyzq(), false, true, s, /*clear=*/true);
     stepKernels(s);
     APO_CUDA(cudaMemcpyAsync(P.h_box, reinterpret_cast<char *>(P.ps.p) + offsetof(PistonScalars, box),
                              3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    APO_CUDA(cudaMemcpyAsync(&S.h_err[0], S.c.err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     APO_CUDA(cudaStreamSynchronize(s));
-    const unsigned e = fm->readDeviceError(s);
+    const unsigned e = S.h_err[0];
     if (e) {
       if (e & kErrNaN)
         throw std::runtime_error("non-finite coordinates during propagation (state kept at step " +
@@ -2025,7 +2028,7 @@ void CudaLangevinPistonIntegrator::propagate(int numSteps) {
       continue;
     }
     m_RngPos += (unsigned long long)m_MaxPC;
-    fm->updateBoxDimensions({P.h_box[0], P.h_box[1], P.h_box[2]});
+    fm->updateBoxDimensions({P.h_box[0], P.h_box[1], P.h_box[2]}, /*keep_list=*/true, s);
     ++k;
     ++m_Step;
     for (auto &sub : m_Subscribers)

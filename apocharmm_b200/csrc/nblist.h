@@ -93,6 +93,10 @@ class NeighborList {
   // every step under pressure control); the next build uses it.  The
   // caller has synchronised the stream the list's kernels run on.
   void set_box(int sys, double Lx, double Ly, double Lz);
+  // the same, keeping the built list: every slot's periodic shift k L moves
+  // with the box (k kept), so the list stays valid between builds while the
+  // box changes a little every step
+  void rescale_box(int sys, double Lx, double Ly, double Lz, cudaStream_t s);
 
   const NbListDims &dims() const { return m_d; }
   const std::vector<NbSysDims> &system_dims() const { return m_sys_h; }

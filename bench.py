@@ -782,8 +782,8 @@ def main():
         if not args.no_cpu_baseline:
             cb = cpu_baseline(s)
         kps = integ.getKernelsPerStep()
-        if spec["integrator"] == "piston":  # a list build every step, no graphs
-            launches = args.steps * SEG * (11 + 7 + kps + 2)
+        if spec["integrator"] == "piston":  # steps launched one by one, box rescale each step
+            launches = args.steps * (11 + SEG * (7 + kps + 2 + 1))
         else:
             launches = args.steps * (12 + SEG * (7 + kps))
         line = {
