@@ -716,13 +716,14 @@ __global__ void com_apply_kernel(Common c, int natom, int freq) {
 }
 
 // --------------------------------------------------------- Langevin piston
-// src/CudaLangevinPistonIntegrator.cu:1705-2060 in five kinds of launch:
+// src/CudaLangevinPistonIntegrator.cu:1705-2060 in three kinds of launch:
 //   lp_half   half step, constraint, constraint forces and virial, the
-//             pressure tensor and its static part
-//   lp_ke     (per pass) kinetic energy; last block: piston move (one normal
-//             per piston degree of freedom) and thermostat update
+//             pressure tensor and its static part; last block: the first
+//             pass's piston move (one normal per piston degree of freedom)
+//             and thermostat update from its kinetic energy
 //   lp_pc     (per pass) atoms follow piston and thermostat; last block:
-//             the pressure difference with the new half-step kinetic term
+//             the pressure difference with the new half-step kinetic term,
+//             then the next pass's piston move and thermostat update
 //   lp_final  constraints on the new and the scaled reference positions,
 //             on-step velocities, kinetic energy, pressure averages, the box
 constexpr double kAtmosp = 1.4584007e-05;           // atm in AKMA pressure units
@@ -851,15 +852,30 @@ __device__ void lp_move(const PistonArgs &a, double dt) {
   }
 }
 
+// start of a predictor-corrector pass (one thread): the piston moves from
+// the step's box and displacement with the current pressure difference, the
+// thermostat from the kinetic energy (ke0 three-term, ke1 on-step)
+__device__ void lp_pass_start(const Common &c, const PistonArgs &a, double ke0, double ke1,
+                              double dt) {
+  PistonScalars *ps = a.ps;
+  for (int d = 0; d < 3; ++d) {
+    ps->box_pred[d] = ps->box[d];
+    ps->lp_delta_pred[d] = ps->lp_delta[d];
+  }
+  lp_move(a, dt);
+  piston_update(c.sc, a.use_old ? ke1 : ke0, a.ke_ref, dt);
+}
+
 __global__ void __launch_bounds__(kThreads) lp_half_kernel(Common c, PistonArgs a) {
   if (*c.err) return;
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   const double dt = c.dt, dt2 = dt * dt, idt = 1.0 / dt;
   // [0..8] constraint virial, [9..17] sum d d m/dt^2 of the new half step,
-  // [18..26] the same of the previous half step
-  double v[27];
+  // [18..26] the same of the previous half step, [27..28] the kinetic
+  // energy of the first predictor-corrector pass
+  double v[29];
 #pragma unroll
-  for (int k = 0; k < 27; ++k) v[k] = 0.0;
+  for (int k = 0; k < 29; ++k) v[k] = 0.0;
   if (g < c.ngroups) {
     int at[4];
     const int m = group_atoms(c, g, at);
@@ -927,13 +943,17 @@ __global__ void __launch_bounds__(kThreads) lp_half_kernel(Common c, PistonArgs 
         // kinetic energy sees it
         const d3 vn = xyz(vm[k]) + idt * (n[k] - n0[k]);
         c.vel[i] = make_double4(vn.x, vn.y, vn.z, vm[k].w);
+        const d3 u1 = idt * xyz(dp[k]), u2 = idt * d;
+        const double kon = 0.5 * dot(vn, vn) / vm[k].w;
+        v[27] += (0.5 * dot(u1, u1) / vm[k].w + kon + 0.5 * dot(u2, u2) / vm[k].w) / 3.0;
+        v[28] += kon;
       }
     }
   }
-  block_partials_n<27>(v, a.partials);
+  block_partials_n<29>(v, a.partials);
   if (is_last_block(&a.ps->counter)) {
-    __shared__ double tot[27];
-    sum_partials_n<27>(a.partials, tot);
+    __shared__ double tot[29];
+    sum_partials_n<29>(a.partials, tot);
     if (threadIdx.x == 0) {
       PistonScalars *ps = a.ps;
       for (int k = 0; k < 9; ++k) {
@@ -950,49 +970,26 @@ __global__ void __launch_bounds__(kThreads) lp_half_kernel(Common c, PistonArgs 
       for (int k = 0; k < 9; ++k) ps->dp_static[k] = ps->dp[k] - 0.25 * a.vfac * tot[9 + k];
       c.sc->piston_v_prev = c.sc->piston_v;
       c.sc->piston_f_prev = c.sc->piston_f;
+      lp_pass_start(c, a, tot[27], tot[28], dt);
       ps->counter = 0;
     }
   }
 }
 
-__global__ void __launch_bounds__(kThreads) lp_ke_kernel(Common c, PistonArgs a, int natom) {
+// predictor-corrector pass over atoms: atoms follow piston and thermostat;
+// the last block forms the new pressure difference and, when another pass
+// follows (`more`), starts it from the kinetic energy of the new velocities
+__global__ void __launch_bounds__(kThreads) lp_pc_kernel(Common c, PistonArgs a, int natom,
+                                                         int more) {
   if (*c.err) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const double dt = c.dt, idt = 1.0 / dt;
-  double v[2] = {0.0, 0.0};
-  if (i < natom) {
-    const double4 vm = c.vel[i];
-    const d3 u1 = idt * xyz(c.dprev[i]), u2 = idt * xyz(c.dpred[i]), w = xyz(vm);
-    const double kon = 0.5 * dot(w, w) / vm.w;
-    v[0] = (0.5 * dot(u1, u1) / vm.w + kon + 0.5 * dot(u2, u2) / vm.w) / 3.0;
-    v[1] = kon;
-  }
-  block_partials_n<2>(v, a.partials);
-  if (is_last_block(&a.ps->counter)) {
-    __shared__ double tot[2];
-    sum_partials_n<2>(a.partials, tot);
-    if (threadIdx.x == 0) {
-      PistonScalars *ps = a.ps;
-      for (int d = 0; d < 3; ++d) {
-        ps->box_pred[d] = ps->box[d];
-        ps->lp_delta_pred[d] = ps->lp_delta[d];
-      }
-      lp_move(a, dt);
-      piston_update(c.sc, a.use_old ? tot[1] : tot[0], a.ke_ref, dt);
-      ps->counter = 0;
-    }
-  }
-}
-
-__global__ void __launch_bounds__(kThreads) lp_pc_kernel(Common c, PistonArgs a, int natom) {
-  if (*c.err) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const double dt = c.dt, dt2 = dt * dt, fact = 0.5 / dt;
+  const double dt = c.dt, dt2 = dt * dt, idt = 1.0 / dt, fact = 0.5 / dt;
   const PistonScalars *ps = a.ps;
   const double nh = a.use_nh ? dt2 * c.sc->piston_v : 0.0;
-  double v[9];
+  // [0..8] sum d d m/dt^2 of the predicted half step, [9..10] kinetic energy
+  double v[11];
 #pragma unroll
-  for (int k = 0; k < 9; ++k) v[k] = 0.0;
+  for (int k = 0; k < 11; ++k) v[k] = 0.0;
   if (i < natom) {
     const d3 dprev = xyz(c.dprev[i]), dpred = xyz(c.dpred[i]), d = xyz(c.delta[i]);
     const d3 r = xyz(c.ref[i]);
@@ -1012,13 +1009,20 @@ __global__ void __launch_bounds__(kThreads) lp_pc_kernel(Common c, PistonArgs a,
     for (int p = 0; p < 3; ++p)
 #pragma unroll
       for (int q = 0; q < 3; ++q) v[3 * p + q] = f * nn[p] * nn[q];
+    if (more) {
+      const d3 u1 = idt * dprev, u2 = idt * np;
+      const double kon = 0.5 * dot(u, u) / im;
+      v[9] = (0.5 * dot(u1, u1) / im + kon + 0.5 * dot(u2, u2) / im) / 3.0;
+      v[10] = kon;
+    }
   }
-  block_partials_n<9>(v, a.partials);
+  block_partials_n<11>(v, a.partials);
   if (is_last_block(&a.ps->counter)) {
-    __shared__ double tot[9];
-    sum_partials_n<9>(a.partials, tot);
+    __shared__ double tot[11];
+    sum_partials_n<11>(a.partials, tot);
     if (threadIdx.x == 0) {
       for (int k = 0; k < 9; ++k) a.ps->dp[k] = a.ps->dp_static[k] + 0.25 * a.vfac * tot[k];
+      if (more) lp_pass_start(c, a, tot[9], tot[10], dt);
       a.ps->counter = 0;
     }
   }
@@ -1742,7 +1746,7 @@ struct PistonState {
 CudaLangevinPistonIntegrator::CudaLangevinPistonIntegrator(double ps) : CudaIntegrator(ps) {
   std::random_device rd;
   m_Seed = rd();
-  m_KernelsPerStep = 2 + 2 * m_MaxPC;
+  m_KernelsPerStep = 2 + m_MaxPC;
 }
 
 CudaLangevinPistonIntegrator::~CudaLangevinPistonIntegrator() = default;
@@ -1816,7 +1820,7 @@ void CudaLangevinPistonIntegrator::setMaxPredictorCorrectorIterations(int n) {
   if (n < 1)
     throw std::invalid_argument("setMaxPredictorCorrectorIterations: at least one pass is needed");
   m_MaxPC = n;
-  m_KernelsPerStep = 2 + 2 * m_MaxPC;
+  m_KernelsPerStep = 2 + m_MaxPC;
 }
 
 void CudaLangevinPistonIntegrator::resetAverages() {
@@ -1881,7 +1885,7 @@ void CudaLangevinPistonIntegrator::initialize() {
   PistonState &P = *m_P;
   P.ps.alloc(1);
   P.rng.alloc(3);
-  P.partials.alloc((size_t)27 * std::max(S.blocks_groups, S.blocks_atoms) + 32);
+  P.partials.alloc((size_t)32 * std::max(S.blocks_groups, S.blocks_atoms) + 32);
   PistonScalars h{};
   const auto &box = fm->getBoxDimensions();
   for (int d = 0; d < 3; ++d) h.box[d] = h.box_pred[d] = box[d];
@@ -1965,10 +1969,8 @@ void CudaLangevinPistonIntegrator::stepKernels(cudaStream_t s) {
   a.const_st = m_ConstST ? 1 : 0;
   a.hol = m_Ctx->isUsingHolonomicConstraints() ? 1 : 0;
   lp_half_kernel<<<S.blocks_groups, kThreads, 0, s>>>(S.c, a);
-  for (int k = 0; k < m_MaxPC; ++k) {
-    lp_ke_kernel<<<S.blocks_atoms, kThreads, 0, s>>>(S.c, a, S.natom);
-    lp_pc_kernel<<<S.blocks_atoms, kThreads, 0, s>>>(S.c, a, S.natom);
-  }
+  for (int k = 0; k < m_MaxPC; ++k)
+    lp_pc_kernel<<<S.blocks_atoms, kThreads, 0, s>>>(S.c, a, S.natom, k + 1 < m_MaxPC ? 1 : 0);
   lp_final_kernel<<<S.blocks_groups, kThreads, 0, s>>>(S.c, a);
   APO_LAUNCH_CHECK();
 }
