@@ -252,14 +252,19 @@ int main(int argc, char **argv) {
       auto nh = std::make_shared<CudaNoseHooverIntegrator>(0.002);
       nh->setReferenceTemperature(300.0);
       integ = nh;
-    } else if (kind == "piston") {
-      // cubic Langevin piston at 1 atm with its Nose-Hoover thermostat at
-      // 300 K; `friction` is the piston's, `seed` its noise seed
+    } else if (kind.rfind("piston", 0) == 0) {
+      // Langevin piston at 1 atm with its Nose-Hoover thermostat at 300 K
+      // ("piston": cubic; "piston_tetra", "piston_ortho": those crystal
+      // types; "piston_nonh": cubic without the thermostat); `friction` is
+      // the piston's, `seed` its noise seed
       auto lp = std::make_shared<CudaLangevinPistonIntegrator>(0.002);
-      lp->setCrystalType(CRYSTAL::CUBIC);
+      lp->setCrystalType(kind == "piston_tetra"   ? CRYSTAL::TETRAGONAL
+                         : kind == "piston_ortho" ? CRYSTAL::ORTHORHOMBIC
+                                                  : CRYSTAL::CUBIC);
       lp->setReferenceTemperature(300.0);
       lp->setLangevinPistonFriction(friction);
       lp->setLangevinPistonFrictionSeed(seed);
+      if (kind == "piston_nonh") lp->useNoseHooverThermostat(false);
       integ = lp;
     } else {
       std::fprintf(stderr, "unknown integrator %s\n", kind.c_str());
@@ -267,7 +272,7 @@ int main(int argc, char **argv) {
     }
     integ->setCharmmContext(s.ctx);
     if (steps > 0) integ->propagate(steps);
-    if (kind == "piston") {
+    if (kind.rfind("piston", 0) == 0) {
       const std::vector<double> b = s.fm->getBoxDimensions();
       FILE *bf = std::fopen((std::string(argv[19]) + ".box").c_str(), "w");
       if (!bf) return 3;

@@ -53,11 +53,13 @@ def traj(paths, box, st, kind, steps, seed, friction, velocities, workdir, timeo
     return a[:, 0:3], a[:, 3:6], a[:, 6:9]
 
 
-def piston(paths, box, st, steps, seed, friction, velocities, workdir, timeout=900):
-    """The reference's cubic Langevin piston (1 atm, Nose-Hoover at 300 K,
-    piston friction and seed as given): (x FP64, x FP32, v, final box)."""
-    x, x32, v = traj(paths, box, st, "piston", steps, seed, friction, velocities, workdir, timeout)
-    b = np.loadtxt(os.path.join(workdir, "traj_piston.txt.box"))
+def piston(paths, box, st, steps, seed, friction, velocities, workdir, timeout=900, kind="piston"):
+    """The reference's Langevin piston (1 atm, Nose-Hoover at 300 K, piston
+    friction and seed as given; kind "piston" cubic, "piston_tetra",
+    "piston_ortho", "piston_nonh" cubic without the thermostat):
+    (x FP64, x FP32, v, final box)."""
+    x, x32, v = traj(paths, box, st, kind, steps, seed, friction, velocities, workdir, timeout)
+    b = np.loadtxt(os.path.join(workdir, f"traj_{kind}.txt.box"))
     return x, x32, v, b
 
 

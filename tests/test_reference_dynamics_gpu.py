@@ -160,6 +160,44 @@ def test_langevin_piston_trajectory_matches_reference_build(glycol, friction):
     assert it.getRngSequencePos() == 30
 
 
+@pytest.mark.parametrize("kind", ["piston_tetra", "piston_ortho", "piston_nonh"])
+def test_langevin_piston_crystal_types_match_reference_build(glycol, kind):
+    """The tetragonal and orthorhombic pistons (x and y edges together, z on
+    its own; three edges on their own) and the cubic piston without its
+    Nose-Hoover thermostat, against the reference build over 10 steps at
+    piston friction 10/ps."""
+    tmp, s, paths, pos, v = glycol
+    xr, _, vr, boxr = rb.piston(paths, s.box, s.settings, 10, 91, 10.0, v, str(tmp), kind=kind)
+    keep = api.system_context(s, str(tmp / f"b200_{kind}"))
+    fm, ctx = keep[2], keep[3]
+    ctx.setCoordinates(pos)
+    ctx.setVelocities(v)
+    it = api.CudaLangevinPistonIntegrator(0.002)
+    it.setCrystalType({"piston_tetra": it.TETRAGONAL, "piston_ortho": it.ORTHORHOMBIC,
+                       "piston_nonh": it.CUBIC}[kind])
+    it.setReferenceTemperature(300.0)
+    it.setLangevinPistonFriction(10.0)
+    it.setLangevinPistonFrictionSeed(91)
+    if kind == "piston_nonh":
+        it.useNoseHooverThermostat(False)
+    it.setCharmmContext(ctx)
+    it.propagate(10)
+    box = fm.getBoxDimensions()
+    x, vb = ctx.getCoordinates(), ctx.getVelocities()
+    dx = _wrapped_diff(x, xr, box)
+    dbox = np.abs(box - boxr).max()
+    print(f"{kind}: box {box} (reference {boxr}), |dbox| {dbox:.2e} A, max |dx| "
+          f"{np.abs(dx).max():.2e} A, velocity rel-RMS {np.linalg.norm(vb - vr) / np.linalg.norm(vr):.2e}")
+    assert np.abs(box - s.box).min() > 1e-7
+    if kind == "piston_tetra":
+        assert box[0] == box[1] != box[2]
+    if kind == "piston_ortho":
+        assert len(set(box.tolist())) == 3
+    assert dbox < 1e-6
+    assert np.abs(dx).max() < 1e-5
+    assert np.linalg.norm(vb - vr) / np.linalg.norm(vr) < 1e-5
+
+
 def _canonical(pairs, pos, box, radius):
     """{(min g, max g): excluded} for the pairs within `radius` (FP64,
     minimum image, from the coordinates both engines read); a pair that
