@@ -241,7 +241,28 @@ void ForceManager::updateBoxDimensions(const std::array<double, 3> &box, bool ke
     m_ListDirty = true;
   }
   m_Pme.set_box(m_Box[0], m_Box[1], m_Box[2]);
+  if (m_DevBox.p) {
+    const double4 b = make_double4(m_Box[0], m_Box[1], m_Box[2], 0.0);
+    APO_CUDA(cudaMemcpy(m_DevBox.p, &b, sizeof(b), cudaMemcpyHostToDevice));
+  }
   ++m_PluginGen;  // captured graphs hold the old box
+}
+
+void ForceManager::useDeviceBox() {
+  if (!m_Initialized) throw std::runtime_error("ForceManager is not initialized");
+  if (m_Multi) throw std::invalid_argument("useDeviceBox: one system only");
+  if (!m_DevBox.p) m_DevBox.alloc(1);
+  const double4 b = make_double4(m_Box[0], m_Box[1], m_Box[2], 0.0);
+  APO_CUDA(cudaMemcpy(m_DevBox.p, &b, sizeof(b), cudaMemcpyHostToDevice));
+  m_Pme.set_device_box(m_DevBox.p);
+  ++m_PluginGen;  // captured graphs hold the launches without it
+}
+
+void ForceManager::adoptDeviceBox(const std::array<double, 3> &box) {
+  m_Box = box;
+  m_HostSetup = make_nb_setup(m_Box[0], m_Box[1], m_Box[2], m_Kappa, m_Ctofnb, m_Ctonnb);
+  m_Nbl.set_box_host(0, m_Box[0], m_Box[1], m_Box[2]);
+  m_Pme.set_box(m_Box[0], m_Box[1], m_Box[2]);
 }
 
 void ForceManager::setFFTGrid(int nx, int ny, int nz) {
@@ -1179,6 +1200,10 @@ void CharmmContext::imageCentering(cudaStream_t s) {
   if (m_Fm->isMulti())
     launch_image_centering(m_Coords.p, m_Xyzq.p, m_Groups.p, (int)m_Groups.n, m_NumBigGroups,
                            b[0], b[1], b[2], s, m_Fm->sysOfAtom(), m_Fm->systemBoxes());
+  else if (m_Fm->hasDeviceBox())  // the box may have changed on the device
+    launch_image_centering(m_Coords.p, m_Xyzq.p, m_Groups.p, (int)m_Groups.n, m_NumBigGroups,
+                           b[0], b[1], b[2], s, m_Fm->neighborList().sys_of_atom,
+                           m_Fm->deviceBox());
   else
     launch_image_centering(m_Coords.p, m_Xyzq.p, m_Groups.p, (int)m_Groups.n, m_NumBigGroups,
                            b[0], b[1], b[2], s);

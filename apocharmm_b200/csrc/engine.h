@@ -112,6 +112,17 @@ class ForceManager {
   // rescaled on stream s) instead of being rebuilt at the next evaluation
   void updateBoxDimensions(const std::array<double, 3> &box, bool keep_list = false,
                            cudaStream_t s = nullptr);
+  // device-resident box (one system): PME and image centering read the box
+  // from deviceBox(), so kernels that change the box on the device (the
+  // Langevin piston) need no host round trip; they write deviceBox(), the
+  // direct-space set-up (deviceSetup()) and the list's dims (deviceListDims())
+  void useDeviceBox();
+  bool hasDeviceBox() const { return m_DevBox.p != nullptr; }
+  double4 *deviceBox() { return m_DevBox.p; }
+  NbSetup *deviceSetup() { return m_Setup.p; }
+  NbSysDims *deviceListDims() { return m_Nbl.device_dims(); }
+  // the host copies of a box the device already holds (after such kernels)
+  void adoptDeviceBox(const std::array<double, 3> &box);
   void setKappa(double k) { m_Kappa = k; m_Initialized = false; }
   void setCutoff(double c) { m_Cutoff = c; m_Initialized = false; }
   void setCtonnb(double c) { m_Ctonnb = c; m_Initialized = false; }
@@ -244,6 +255,7 @@ class ForceManager {
   int m_EStride = 0;  // energy slots per system (energies + virial)
   PmeMulti m_PmeMulti;
   DeviceArray<double4> m_Boxes;
+  DeviceArray<double4> m_DevBox;  // one system's box in device memory (useDeviceBox)
   std::array<double, 3> m_Box{{-9999.9999, -9999.9999, -9999.9999}};
   double m_Kappa = 0.34, m_Cutoff = 14.0, m_Ctonnb = 12.0, m_Ctofnb = 10.0;
   int m_Nfft[3] = {-1, -1, -1};

@@ -741,6 +741,9 @@ struct PistonScalars {
   double lp_delta[3], lp_delta_pred[3], lp_delta_prev[3];
   double lp_onpos[3], lp_halfpos[3], lp_onvel[3], lp_dpress[3];
   double cf_on[3], cf_half[3];
+  double box_old[3];             // the box before the last step (for the list's shifts)
+  double vfac, lp_vfac;          // patm / V and V pbfact atmosp of the step's box
+  unsigned long long rngpos;     // normals drawn per piston degree of freedom
   unsigned counter, pad;
 };
 
@@ -751,11 +754,12 @@ struct PistonArgs {
   curandStatePhilox4_32_10_t *rng;
   double *partials;
   const long long *vir_fixed;    // the force manager's virial slots
+  NbSetup *setup;                // the force manager's direct-space set-up
+  NbSysDims *lsys;               // the list's dims
+  double4 *dbox;                 // the force manager's device box
   double inv_mass[3], prfwd[3];
   double palpha, pbfact;
-  double vfac;                   // patmos / V
-  double lp_vfac;                // V pbfact atmosp
-  double st_fac;                 // surface tension x factor / Lz
+  double st;                     // surface tension x dyne/cm factor
   double ke_ref;
   int crystal, dof, use_nh, use_old, const_st, hol;
 };
@@ -808,11 +812,12 @@ __device__ void lp_move(const PistonArgs &a, double dt) {
     curandStatePhilox4_32_10_t st = a.rng[i];
     ps->lp_delta_prev[i] = ps->lp_delta_pred[i];
     ps->lp_delta_pred[i] = a.palpha * ps->lp_delta_pred[i] +
-                           a.inv_mass[i] * ps->lp_dpress[i] * a.lp_vfac +
+                           a.inv_mass[i] * ps->lp_dpress[i] * ps->lp_vfac +
                            a.pbfact * a.prfwd[i] * curand_normal_double(&st);
     ps->lp_onvel[i] = 0.5 * (ps->lp_delta_pred[i] + ps->lp_delta_prev[i]) / dt;
     a.rng[i] = st;
   }
+  ps->rngpos += 1;
   if (cr == Crystal::Cubic) {
     ps->lp_onpos[0] = (b[0] + b[1] + b[2]) / 3.0;
   } else if (cr == Crystal::Tetragonal) {
@@ -956,18 +961,21 @@ __global__ void __launch_bounds__(kThreads) lp_half_kernel(Common c, PistonArgs 
     sum_partials_n<29>(a.partials, tot);
     if (threadIdx.x == 0) {
       PistonScalars *ps = a.ps;
+      const double V = ps->box[0] * ps->box[1] * ps->box[2];
+      ps->vfac = kPatmos / V;
+      ps->lp_vfac = V * a.pbfact * kAtmosp;
       for (int k = 0; k < 9; ++k) {
         ps->vir[k] = (double)a.vir_fixed[k] * kInvEnergyScale + tot[k];
         const double kin = 0.5 * (tot[9 + k] + tot[18 + k]);
-        ps->p[k] = a.vfac * (kin + ps->vir[k]);
+        ps->p[k] = ps->vfac * (kin + ps->vir[k]);
         ps->dp[k] = ps->p[k] - ps->pref[k];
       }
       ps->pscalar = (ps->p[0] + ps->p[4] + ps->p[8]) / 3.0;
       if (a.const_st) {
-        ps->pref[0] = ps->pref[8] - a.st_fac;
+        ps->pref[0] = ps->pref[8] - a.st / ps->box[2];
         ps->pref[4] = ps->pref[0];
       }
-      for (int k = 0; k < 9; ++k) ps->dp_static[k] = ps->dp[k] - 0.25 * a.vfac * tot[9 + k];
+      for (int k = 0; k < 9; ++k) ps->dp_static[k] = ps->dp[k] - 0.25 * ps->vfac * tot[9 + k];
       c.sc->piston_v_prev = c.sc->piston_v;
       c.sc->piston_f_prev = c.sc->piston_f;
       lp_pass_start(c, a, tot[27], tot[28], dt);
@@ -1021,7 +1029,7 @@ __global__ void __launch_bounds__(kThreads) lp_pc_kernel(Common c, PistonArgs a,
     __shared__ double tot[11];
     sum_partials_n<11>(a.partials, tot);
     if (threadIdx.x == 0) {
-      for (int k = 0; k < 9; ++k) a.ps->dp[k] = a.ps->dp_static[k] + 0.25 * a.vfac * tot[k];
+      for (int k = 0; k < 9; ++k) a.ps->dp[k] = a.ps->dp_static[k] + 0.25 * a.ps->vfac * tot[k];
       if (more) lp_pass_start(c, a, tot[9], tot[10], dt);
       a.ps->counter = 0;
     }
@@ -1106,16 +1114,39 @@ __global__ void __launch_bounds__(kThreads) lp_final_kernel(Common c, PistonArgs
       piston_update(c.sc, a.use_old ? tot[1] : tot[0], a.ke_ref, dt);
       const double s = (double)(c.sc->window + 1);
       for (int k = 0; k < 9; ++k) {
-        ps->p[k] = a.vfac * (0.5 * tot[2 + k] + ps->vir[k]);
+        ps->p[k] = ps->vfac * (0.5 * tot[2 + k] + ps->vir[k]);
         ps->pavg[k] += (ps->p[k] - ps->pavg[k]) / s;
       }
       ps->pscalar = (ps->p[0] + ps->p[4] + ps->p[8]) / 3.0;
       ps->pavg_scalar += (ps->pscalar - ps->pavg_scalar) / s;
       finish_temperature(c, tot[0], tot[1]);
       for (int d = 0; d < 3; ++d) {
+        ps->box_old[d] = ps->box[d];
         ps->box[d] = ps->box_pred[d];
         ps->lp_delta[d] = ps->lp_delta_pred[d];
       }
+      // the new box where the next step's kernels read it: the force
+      // manager's device box, its direct-space set-up (the conversions of
+      // make_nb_setup) and the list's dims
+      const double L[3] = {ps->box[0], ps->box[1], ps->box[2]};
+      *a.dbox = make_double4(L[0], L[1], L[2], 0.0);
+      NbSetup &st = *a.setup;
+      st.Lxd = L[0];
+      st.Lyd = L[1];
+      st.Lzd = L[2];
+      st.Lx_lo = (float)(L[0] - (double)(float)L[0]);
+      st.Ly_lo = (float)(L[1] - (double)(float)L[1]);
+      st.Lz_lo = (float)(L[2] - (double)(float)L[2]);
+      st.Lx = (float)L[0];
+      st.Ly = (float)L[1];
+      st.Lz = (float)L[2];
+      NbSysDims &ls = *a.lsys;
+      ls.Lx = (float)L[0];
+      ls.Ly = (float)L[1];
+      ls.Lz = (float)L[2];
+      ls.Lxd = L[0];
+      ls.Lyd = L[1];
+      ls.Lzd = L[2];
       c.sc->step += 1;
       ps->counter = 0;
     }
@@ -1125,8 +1156,10 @@ __global__ void __launch_bounds__(kThreads) lp_final_kernel(Common c, PistonArgs
 // one Philox state per piston degree of freedom: subsequence = dof index,
 // then `pos` draws skipped (InitializeRngKernel)
 __global__ void lp_rng_init_kernel(curandStatePhilox4_32_10_t *st, int n,
-                                   unsigned long long seed, unsigned long long pos) {
+                                   unsigned long long seed, unsigned long long pos,
+                                   PistonScalars *ps) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) ps->rngpos = pos;
   if (i >= n) return;
   curand_init(seed, (unsigned long long)i, 0ull, st + i);
   skipahead(pos, st + i);
@@ -1452,6 +1485,7 @@ void CudaIntegrator::propagate(int numSteps) {
           break;
         }
         m_Step = step0 + launched;
+        beforeReport();
         for (auto &sub : m_Subscribers)
           if (launched % sub->getReportFrequency() == 0) sub->update(*m_Ctx, m_Step, getTimeStep());
       }
@@ -1690,6 +1724,15 @@ CudaNoseHooverIntegrator::CudaNoseHooverIntegrator(double ps) : CudaIntegrator(p
   m_KernelsPerStep = 5;
 }
 
+void CudaNoseHooverIntegrator::setNoseHooverPistonMass(double m) {
+  m_PistonMass = m;
+  if (m_S) {  // after initialisation the mass lives on the device
+    APO_CUDA(cudaStreamSynchronize(stream()));
+    APO_CUDA(cudaMemcpy(reinterpret_cast<char *>(m_S->sc.p) + offsetof(Scalars, piston_mass), &m,
+                        sizeof(double), cudaMemcpyHostToDevice));
+  }
+}
+
 void CudaNoseHooverIntegrator::initialize() {
   if (m_Ctx->getForceManager()->isMulti())
     throw std::invalid_argument("Nose-Hoover couples all atoms through one piston: it is not "
@@ -1733,20 +1776,12 @@ struct PistonState {
   DeviceArray<PistonScalars> ps;
   DeviceArray<curandStatePhilox4_32_10_t> rng;
   DeviceArray<double> partials;
-  double *h_box = nullptr;  // pinned: the box after each step
-  PistonState() {
-    APO_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&h_box), 3 * sizeof(double),
-                           cudaHostAllocDefault));
-  }
-  ~PistonState() {
-    if (h_box) cudaFreeHost(h_box);
-  }
 };
 
 CudaLangevinPistonIntegrator::CudaLangevinPistonIntegrator(double ps) : CudaIntegrator(ps) {
   std::random_device rd;
   m_Seed = rd();
-  m_KernelsPerStep = 2 + m_MaxPC;
+  m_KernelsPerStep = 3 + m_MaxPC;
 }
 
 CudaLangevinPistonIntegrator::~CudaLangevinPistonIntegrator() = default;
@@ -1807,6 +1842,9 @@ void CudaLangevinPistonIntegrator::setNoseHooverPistonMass(double m) {
 }
 
 void CudaLangevinPistonIntegrator::setLangevinPistonFrictionSeed(uint64_t seed) {
+  // the states are drawn again from the new seed at the current position
+  // (the reference's initializeRng with m_RngSequencePos)
+  m_RngPos = getRngSequencePos();
   m_Seed = seed;
   m_RngDirty = true;
 }
@@ -1816,11 +1854,19 @@ void CudaLangevinPistonIntegrator::setRngSequencePos(unsigned long long pos) {
   m_RngDirty = true;
 }
 
+unsigned long long CudaLangevinPistonIntegrator::getRngSequencePos() {
+  if (!m_P || m_RngDirty) return m_RngPos;
+  PistonScalars h;
+  APO_CUDA(cudaStreamSynchronize(stream()));
+  APO_CUDA(cudaMemcpy(&h, m_P->ps.p, sizeof(h), cudaMemcpyDeviceToHost));
+  return h.rngpos;
+}
+
 void CudaLangevinPistonIntegrator::setMaxPredictorCorrectorIterations(int n) {
   if (n < 1)
     throw std::invalid_argument("setMaxPredictorCorrectorIterations: at least one pass is needed");
   m_MaxPC = n;
-  m_KernelsPerStep = 2 + m_MaxPC;
+  m_KernelsPerStep = 3 + m_MaxPC;
 }
 
 void CudaLangevinPistonIntegrator::resetAverages() {
@@ -1894,8 +1940,10 @@ void CudaLangevinPistonIntegrator::initialize() {
   Scalars sc{};
   sc.piston_mass = m_NHMass;
   APO_CUDA(cudaMemcpy(S.sc.p, &sc, sizeof(sc), cudaMemcpyHostToDevice));
-  lp_rng_init_kernel<<<1, 32, 0, s>>>(P.rng.p, m_Dof, m_Seed, m_RngPos);
+  lp_rng_init_kernel<<<1, 32, 0, s>>>(P.rng.p, m_Dof, m_Seed, m_RngPos, P.ps.p);
   m_RngDirty = false;
+  fm->useDeviceBox();
+  clearGraphs();
   // as Nose-Hoover: constraints, first forces, the position-Verlet deltas
   // (src/CudaLangevinPistonIntegrator.cu:626-704)
   if (m_Ctx->isUsingHolonomicConstraints())
@@ -1934,20 +1982,22 @@ void CudaLangevinPistonIntegrator::applyRestartRecord(const RestartRecord &r) {
   setRngSequencePos((r.apo && r.has_rng) ? r.rngpos : 0ull);
 }
 
-// the step after the forces: half step, the predictor-corrector passes and
-// the final pass, with the piston constants of the current settings and
-// the volume of the current box
+// the step after the forces: half step, the predictor-corrector passes, the
+// final pass and the list's shifts moved with the new box, with the piston
+// constants of the current settings (a setter drops the captured segments);
+// the box itself is read and written on the device only
 void CudaLangevinPistonIntegrator::stepKernels(cudaStream_t s) {
   IntegratorState &S = *m_S;
   PistonState &P = *m_P;
   auto fm = m_Ctx->getForceManager();
-  const auto &box = fm->getBoxDimensions();
-  const double V = box[0] * box[1] * box[2];
   PistonArgs a{};
   a.ps = P.ps.p;
   a.rng = P.rng.p;
   a.partials = P.partials.p;
   a.vir_fixed = fm->deviceVirial();
+  a.setup = fm->deviceSetup();
+  a.lsys = fm->deviceListDims();
+  a.dbox = fm->deviceBox();
   // piston friction terms (setLangevinPistonFriction,
   // src/CudaLangevinPistonIntegrator.cu:262-283)
   const double kbt = kBoltz * m_RefT;
@@ -1958,9 +2008,7 @@ void CudaLangevinPistonIntegrator::stepKernels(cudaStream_t s) {
     a.inv_mass[i] = m_PMass[i] == 0.0 ? 0.0 : 1.0 / m_PMass[i];
     a.prfwd[i] = std::sqrt(2.0 * a.inv_mass[i] * pgam * kbt) / m_Dt;
   }
-  a.vfac = kPatmos / V;
-  a.lp_vfac = V * a.pbfact * kAtmosp;
-  a.st_fac = m_SurfaceTension * kSurfaceTensionFactor / box[2];
+  a.st = m_SurfaceTension * kSurfaceTensionFactor;
   a.ke_ref = 0.5 * (double)m_Ctx->getDegreesOfFreedom() * kBoltz * m_RefT;
   a.crystal = (int)m_Crystal;
   a.dof = m_Dof;
@@ -1973,69 +2021,48 @@ void CudaLangevinPistonIntegrator::stepKernels(cudaStream_t s) {
     lp_pc_kernel<<<S.blocks_atoms, kThreads, 0, s>>>(S.c, a, S.natom, k + 1 < m_MaxPC ? 1 : 0);
   lp_final_kernel<<<S.blocks_groups, kThreads, 0, s>>>(S.c, a);
   APO_LAUNCH_CHECK();
+  const char *ps = reinterpret_cast<const char *>(P.ps.p);
+  fm->neighborList().rescale_box_device(
+      reinterpret_cast<const double *>(ps + offsetof(PistonScalars, box_old)),
+      reinterpret_cast<const double *>(ps + offsetof(PistonScalars, box)), S.c.err, s);
 }
 
-// One step at a time: centre-of-mass removal (on the device step counter),
-// a list build every m_ListFreq steps, forces with the virial, the step,
-// then the new box to the host and into the force manager (the reference
-// ends its step the same way, src/CudaLangevinPistonIntegrator.cu:2052-2056),
-// whose list follows the box until the next build.  A list that overflowed
-// leaves the step kernels idle: the list is grown and the step taken again.
+void CudaLangevinPistonIntegrator::forcesForStep(cudaStream_t s) {
+  // forces and virial; the sorted coordinates refreshed from the FP64 state
+  // the step kernels wrote, the gradient slots cleared
+  m_Ctx->getForceManager()->calcForce(m_Ctx->xyzq(), false, true, s, /*clear=*/true);
+}
+
+void CudaLangevinPistonIntegrator::adoptBox() {
+  if (!m_P) return;
+  PistonScalars h;
+  APO_CUDA(cudaStreamSynchronize(stream()));
+  APO_CUDA(cudaMemcpy(&h, m_P->ps.p, sizeof(h), cudaMemcpyDeviceToHost));
+  m_Ctx->getForceManager()->adoptDeviceBox({h.box[0], h.box[1], h.box[2]});
+}
+
+void CudaLangevinPistonIntegrator::beforeReport() { adoptBox(); }
+
+// Captured 20-step segments as for the other integrators (a list build,
+// then the steps; the list follows the box in between, the box never
+// leaves the device); the host copies of the box are refreshed before
+// every subscriber report and at the end.
 void CudaLangevinPistonIntegrator::propagate(int numSteps) {
   if (!m_Ctx)
     throw std::invalid_argument("CudaIntegrator::propagate: no CharmmContext was set for this CudaIntegrator.");
   if (numSteps <= 0) return;
-  cudaStream_t s = m_Ctx->stream();
-  IntegratorState &S = *m_S;
-  PistonState &P = *m_P;
-  auto fm = m_Ctx->getForceManager();
   if (m_RngDirty) {
-    lp_rng_init_kernel<<<1, 32, 0, s>>>(P.rng.p, m_Dof, m_Seed, m_RngPos);
+    lp_rng_init_kernel<<<1, 32, 0, stream()>>>(m_P->rng.p, m_Dof, m_Seed, m_RngPos, m_P->ps.p);
     APO_LAUNCH_CHECK();
     m_RngDirty = false;
   }
-  m_Ctx->ensureListBuffers();
-  fm->rewindKernelTimers();
-  int regrowths = 0;
-  for (int k = 0; k < numSteps;) {
-    if (m_ComFreq > 0) {
-      com_sum_kernel<<<S.blocks_atoms, kThreads, 0, s>>>(S.c, S.natom, m_ComFreq);
-      com_apply_kernel<<<S.blocks_atoms, kThreads, 0, s>>>(S.c, S.natom, m_ComFreq);
-      APO_LAUNCH_CHECK();
-    }
-    // the list is built at the reference's cadence (every m_ListFreq steps
-    // from the start of the call) and follows the box in between
-    if (k % m_ListFreq == 0) m_Ctx->resetNeighborList(s);
-    fm->calcForce(m_Ctx->xyzq(), false, true, s, /*clear=*/true);
-    stepKernels(s);
-    APO_CUDA(cudaMemcpyAsync(P.h_box, reinterpret_cast<char *>(P.ps.p) + offsetof(PistonScalars, box),
-                             3 * sizeof(double), cudaMemcpyDeviceToHost, s));
-    APO_CUDA(cudaMemcpyAsync(&S.h_err[0], S.c.err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
-    APO_CUDA(cudaStreamSynchronize(s));
-    const unsigned e = S.h_err[0];
-    if (e) {
-      if (e & kErrNaN)
-        throw std::runtime_error("non-finite coordinates during propagation (state kept at step " +
-                                 std::to_string(m_Step) + ")");
-      if (e & kErrCopyTimeout)
-        throw std::runtime_error("a tensor copy of the reciprocal-space grid did not complete "
-                                 "(state kept at step " + std::to_string(m_Step) + ")");
-      if (e & kErrColumnOverflow)
-        throw std::runtime_error("neighbour list: a cell column outgrew the column sort during "
-                                 "propagation (state kept at step " + std::to_string(m_Step) + ")");
-      if (++regrowths > 8)
-        throw std::runtime_error("neighbour list capacity exceeded repeatedly during propagation "
-                                 "(device error " + std::to_string(e) + ")");
-      fm->growNeighborList(m_Ctx->xyzq(), s);
-      continue;
-    }
-    m_RngPos += (unsigned long long)m_MaxPC;
-    fm->updateBoxDimensions({P.h_box[0], P.h_box[1], P.h_box[2]}, /*keep_list=*/true, s);
-    ++k;
-    ++m_Step;
-    for (auto &sub : m_Subscribers)
-      if (m_Step % sub->getReportFrequency() == 0) sub->update(*m_Ctx, m_Step, getTimeStep());
+  try {
+    CudaIntegrator::propagate(numSteps);
+  } catch (...) {
+    adoptBox();
+    throw;
   }
+  adoptBox();
 }
 
 // ---------------------------------------------------------------- leapfrog

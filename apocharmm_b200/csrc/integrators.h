@@ -85,7 +85,8 @@ class CudaIntegrator : public std::enable_shared_from_this<CudaIntegrator> {
   virtual void stepKernels(cudaStream_t s) = 0;  // the integration after forces
   void segment(int nsteps, cudaStream_t s);      // rebuild + nsteps steps
   void launchSegment(int nsteps, cudaStream_t s);  // as a captured graph (cached) or eagerly
-  void forcesForStep(cudaStream_t s);
+  virtual void forcesForStep(cudaStream_t s);
+  virtual void beforeReport() {}  // host state the subscribers read, after a synchronisation
   double m_Dt;  // AKMA
   int m_ListFreq = 20, m_ComFreq = 1000;
   bool m_UseGraphs = true;
@@ -106,9 +107,10 @@ class CudaLangevinThermostatIntegrator : public CudaIntegrator {
   explicit CudaLangevinThermostatIntegrator(double timeStepPs);
   void setThermostatFriction(double frictionPerPs);
   double getThermostatFriction() const { return m_Friction; }
-  void setReferenceTemperature(double t) { m_RefT = t; }
+  // a setting change drops the captured segments, which hold the old value
+  void setReferenceTemperature(double t) { m_RefT = t; clearGraphs(); }
   double getReferenceTemperature() const { return m_RefT; }
-  void setThermostatRngSeed(uint64_t seed) { m_Seed = seed; }
+  void setThermostatRngSeed(uint64_t seed) { m_Seed = seed; clearGraphs(); }
   uint64_t getThermostatRngSeed() const { return m_Seed; }
   unsigned long long getRngSequencePos();
 
@@ -122,10 +124,10 @@ class CudaLangevinThermostatIntegrator : public CudaIntegrator {
 class CudaNoseHooverIntegrator : public CudaIntegrator {
  public:
   explicit CudaNoseHooverIntegrator(double timeStepPs);
-  void setReferenceTemperature(double t) { m_RefT = t; }
+  void setReferenceTemperature(double t) { m_RefT = t; clearGraphs(); }
   double getReferenceTemperature() const { return m_RefT; }
-  void setNoseHooverPistonMass(double m) { m_PistonMass = m; }
-  void useOldTemperature(bool f) { m_OldT = f; }
+  void setNoseHooverPistonMass(double m);
+  void useOldTemperature(bool f) { m_OldT = f; clearGraphs(); }
 
  protected:
   void initialize() override;
@@ -143,10 +145,12 @@ class CudaNoseHooverIntegrator : public CudaIntegrator {
 // freedom and pass, curand_init(seed, dof, 0) + skipahead), the thermostat
 // and the atoms together, the constraints applied to the new and the scaled
 // reference positions, and the on-step velocities.  Cubic, tetragonal and
-// orthorhombic cells.  Every step ends with the new box on the host, as in
-// the reference: the force manager takes it (updateBoxDimensions) and the
-// list is rebuilt at the next step, so steps are launched one by one
-// rather than as captured segments.
+// orthorhombic cells.  The box lives in device memory (the force manager's
+// device box, its direct-space set-up and its list dims, all rewritten by
+// the last kernel of the step; the list's periodic shifts follow the box
+// between builds), so piston steps run as captured 20-step segments like
+// the other integrators; the host copies are brought up to date after
+// every segment a subscriber reports on and at the end of propagate.
 enum class Crystal : int { None = 0, Cubic = 1, Orthorhombic = 2, Tetragonal = 3 };
 
 struct PistonState;  // device scalars, defined in integrators.cu
@@ -161,23 +165,23 @@ class CudaLangevinPistonIntegrator : public CudaIntegrator {
   // reference pressure tensor (atm), row-major XX XY XZ YX YY YZ ZX ZY ZZ
   void setPressure(const std::vector<double> &p);
   std::vector<double> getReferencePressureTensor() const { return m_Pref; }
-  void setConstantSurfaceTension(bool f) { m_ConstST = f; }
-  void setSurfaceTension(double dyneCm) { m_SurfaceTension = dyneCm; }
+  void setConstantSurfaceTension(bool f) { m_ConstST = f; clearGraphs(); }
+  void setSurfaceTension(double dyneCm) { m_SurfaceTension = dyneCm; clearGraphs(); }
   // amu, one per piston degree of freedom; default 0.02 x total mass
   void setLangevinPistonMass(const std::vector<double> &m);
   std::vector<double> getLangevinPistonMass() const { return m_PMass; }
-  void setLangevinPistonFriction(double perPs) { m_PGamma = perPs; }
+  void setLangevinPistonFriction(double perPs) { m_PGamma = perPs; clearGraphs(); }
   double getLangevinPistonFriction() const { return m_PGamma; }
   void setLangevinPistonFrictionSeed(uint64_t seed);
   uint64_t getLangevinPistonFrictionSeed() const { return m_Seed; }
   void setRngSequencePos(unsigned long long pos);
-  unsigned long long getRngSequencePos() const { return m_RngPos; }
-  void setReferenceTemperature(double t) { m_RefT = t; }
+  unsigned long long getRngSequencePos();
+  void setReferenceTemperature(double t) { m_RefT = t; clearGraphs(); }
   double getReferenceTemperature() const { return m_RefT; }
-  void useNoseHooverThermostat(bool f) { m_UseNH = f; }
+  void useNoseHooverThermostat(bool f) { m_UseNH = f; clearGraphs(); }
   void setNoseHooverPistonMass(double m);
   double getNoseHooverPistonMass() const { return m_NHMass; }
-  void useOldTemperature(bool f) { m_OldT = f; }
+  void useOldTemperature(bool f) { m_OldT = f; clearGraphs(); }
   void setMaxPredictorCorrectorIterations(int n);
   int getMaxPredictorCorrectorIterations() const { return m_MaxPC; }
   void resetAverages();
@@ -198,6 +202,9 @@ class CudaLangevinPistonIntegrator : public CudaIntegrator {
  protected:
   void initialize() override;
   void stepKernels(cudaStream_t s) override;
+  void forcesForStep(cudaStream_t s) override;  // with the virial
+  void beforeReport() override;
+  void adoptBox();  // the device's box into the force manager's host copies
   Crystal m_Crystal = Crystal::None;
   int m_Dof = -1, m_MaxPC = 3;
   std::vector<double> m_Pref{1, 0, 0, 0, 1, 0, 0, 0, 1};

@@ -267,6 +267,22 @@ __global__ void rescale_kernel(double4 *__restrict__ slot_off, const float4 *__r
   slot_off[s] = v;
 }
 
+__global__ void rescale_dev_kernel(double4 *__restrict__ slot_off,
+                                   const float4 *__restrict__ cl_origin,
+                                   const double *__restrict__ L0, const double *__restrict__ L1,
+                                   const unsigned *__restrict__ err, const int *__restrict__ counts) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (*err || s >= counts[0]) return;
+  const float4 o = cl_origin[s / kTile];
+  double4 v = slot_off[s];
+  const double kx = rint((v.x + (double)o.x) / L0[0]), ky = rint((v.y + (double)o.y) / L0[1]),
+               kz = rint((v.z + (double)o.z) / L0[2]);
+  v.x = kx * L1[0] - (double)o.x;
+  v.y = ky * L1[1] - (double)o.y;
+  v.z = kz * L1[2] - (double)o.z;
+  slot_off[s] = v;
+}
+
 // sorted, cluster-local coordinates (runs after every coordinate update)
 __global__ void refresh_kernel(const double4 *__restrict__ coords, const int *__restrict__ perm,
                                const double4 *__restrict__ slot_off,
@@ -740,6 +756,25 @@ void NeighborList::rescale_box(int sys, double Lx, double Ly, double Lz, cudaStr
       slot_off, cl_origin, cl_sys, sys, make_double3(d.Lxd, d.Lyd, d.Lzd), make_double3(Lx, Ly, Lz),
       counts);
   APO_LAUNCH_CHECK();
+}
+
+void NeighborList::rescale_box_device(const double *old_box, const double *new_box,
+                                      const unsigned *err, cudaStream_t s) {
+  if (m_sys_h.size() != 1) throw std::invalid_argument("NeighborList: one system only");
+  rescale_dev_kernel<<<(m_d.slot_cap + 255) / 256, 256, 0, s>>>(slot_off, cl_origin, old_box,
+                                                                new_box, err, counts);
+  APO_LAUNCH_CHECK();
+}
+
+void NeighborList::set_box_host(int sys, double Lx, double Ly, double Lz) {
+  if (sys < 0 || sys >= (int)m_sys_h.size()) throw std::invalid_argument("NeighborList: no such system");
+  NbSysDims &d = m_sys_h[sys];
+  d.Lx = (float)Lx;
+  d.Ly = (float)Ly;
+  d.Lz = (float)Lz;
+  d.Lxd = Lx;
+  d.Lyd = Ly;
+  d.Lzd = Lz;
 }
 
 void NeighborList::set_capacity(int tile_cap, int work_cap) {

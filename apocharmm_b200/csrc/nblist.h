@@ -97,6 +97,13 @@ class NeighborList {
   // with the box (k kept), so the list stays valid between builds while the
   // box changes a little every step
   void rescale_box(int sys, double Lx, double Ly, double Lz, cudaStream_t s);
+  // the same with the old and new edges in device memory (3 doubles each;
+  // nothing happens once `err` is set); the device dims are left alone
+  void rescale_box_device(const double *old_box, const double *new_box, const unsigned *err,
+                          cudaStream_t s);
+  // the host copy of a box the device dims already hold
+  void set_box_host(int sys, double Lx, double Ly, double Lz);
+  NbSysDims *device_dims() { return m_sys; }
 
   const NbListDims &dims() const { return m_d; }
   const std::vector<NbSysDims> &system_dims() const { return m_sys_h; }

@@ -335,6 +335,17 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
+// the box held in device memory (a box that changes every step under
+// pressure control): the same conversions as Pme::setup / set_box
+__device__ __forceinline__ void box_from_device(PmeDims &d, const double4 b) {
+  d.Lx = (float)b.x;
+  d.Ly = (float)b.y;
+  d.Lz = (float)b.z;
+  d.rLx = 1.0 / b.x;
+  d.rLy = 1.0 / b.y;
+  d.rLz = 1.0 / b.z;
+}
+
 // ------------------------------------------------------------------------
 // spread
 // ------------------------------------------------------------------------
@@ -344,12 +355,14 @@ __global__ void __launch_bounds__(128) spread_kernel(const float4 *__restrict__ 
                                                      int *__restrict__ qgrid,
                                                      const float4 *__restrict__ origin,
                                                      const PmeSysArgs *__restrict__ multi = nullptr,
-                                                     const int *__restrict__ cl_sys = nullptr) {
+                                                     const int *__restrict__ cl_sys = nullptr,
+                                                     const double4 *__restrict__ dbox = nullptr) {
   if (multi) {  // one block = one 32-slot cluster of one system
     const PmeSysArgs &A = multi[cl_sys[blockIdx.x]];
     d = A.d;
     qgrid = A.qgrid;
   }
+  if (dbox) box_from_device(d, *dbox);
   constexpr int P3 = ORDER * ORDER * ORDER;
   __shared__ int sh_i[3][32];
   __shared__ float sh_q[32];
@@ -555,7 +568,8 @@ __global__ void __launch_bounds__(kPencilThreads) pencil_kernel(const __grid_con
                                                                 const PmeSysArgs *__restrict__ multi,
                                                                 const int *__restrict__ pencil_sys,
                                                                 const __grid_constant__ CUtensorMap tmap,
-                                                                unsigned *__restrict__ err) {
+                                                                unsigned *__restrict__ err,
+                                                                const double4 *__restrict__ dbox = nullptr) {
   // TMA: the slab of 16 complex columns x nz arrives in (and leaves from)
   // buf as one tiled copy of the padded complex grid
   __shared__ __align__(128) float2 buf[256 * kPencilTX];
@@ -578,6 +592,13 @@ __global__ void __launch_bounds__(kPencilThreads) pencil_kernel(const __grid_con
   }
   const PmeDims &d = *dp;
   const int nx = d.nx, ny = d.ny, nz = d.nz, nxc = d.nxc;
+  float Lx = d.Lx, Ly = d.Ly, Lz = d.Lz;  // the box, or the device's copy of it
+  if (dbox) {
+    const double4 b = *dbox;
+    Lx = (float)b.x;
+    Ly = (float)b.y;
+    Lz = (float)b.z;
+  }
   const int tiles_x = (nxc + kPencilTX - 1) / kPencilTX;
   const int py = blk / tiles_x, x0 = (blk - py * tiles_x) * kPencilTX;
   if (TMA) {
@@ -607,10 +628,10 @@ __global__ void __launch_bounds__(kPencilThreads) pencil_kernel(const __grid_con
   fft_dif(buf, kPencilTX, 1, kPencilTX, d.az, twz, -1.f);
   const int ky = dig_unrev(py, d.ay);
   const int nf1 = nx / 2 + (nx & 1), nf2 = ny / 2 + (ny & 1), nf3 = nz / 2 + (nz & 1);
-  const FT m2 = (FT)(ky >= nf2 ? ky - ny : ky) / (FT)d.Ly;
+  const FT m2 = (FT)(ky >= nf2 ? ky - ny : ky) / (FT)Ly;
   const FT pi = (FT)3.14159265358979323846;
   const FT fac = pi * pi / ((FT)d.kappa * (FT)d.kappa);
-  const FT piv_inv = (FT)1 / ((FT)d.Lx * (FT)d.Ly * (FT)d.Lz * pi);
+  const FT piv_inv = (FT)1 / ((FT)Lx * (FT)Ly * (FT)Lz * pi);
   const FT *pf = sizeof(FT) == 8 ? reinterpret_cast<const FT *>(prefac_d)
                                  : reinterpret_cast<const FT *>(prefac);
   const FT pyv = pf[nx + ky];
@@ -621,8 +642,8 @@ __global__ void __launch_bounds__(kPencilThreads) pencil_kernel(const __grid_con
     if (kx >= nxc) continue;
     const int kz = s_unrev_z[pz];
     FT eterm = 0;
-    const FT m1 = (FT)(kx >= nf1 ? kx - nx : kx) / (FT)d.Lx;
-    const FT m3 = (FT)(kz >= nf3 ? kz - nz : kz) / (FT)d.Lz;
+    const FT m1 = (FT)(kx >= nf1 ? kx - nx : kx) / (FT)Lx;
+    const FT m3 = (FT)(kz >= nf3 ? kz - nz : kz) / (FT)Lz;
     const FT msq = m1 * m1 + m2 * m2 + m3 * m3;
     if (kx != 0 || ky != 0 || kz != 0)
       eterm = exp(-fac * msq) * piv_inv * pf[kx] * pyv * pf[nx + ny + kz] / msq;
@@ -695,12 +716,14 @@ __global__ void __launch_bounds__(256) gather_kernel(const float4 *__restrict__ 
                                                      long long *__restrict__ force, int stride,
                                                      const float4 *__restrict__ origin,
                                                      const PmeSysArgs *__restrict__ multi = nullptr,
-                                                     const int *__restrict__ cl_sys = nullptr) {
+                                                     const int *__restrict__ cl_sys = nullptr,
+                                                     const double4 *__restrict__ dbox = nullptr) {
   if (multi) {  // one block = one 32-slot cluster of one system
     const PmeSysArgs &A = multi[cl_sys[blockIdx.x]];
     d = A.d;
     phi = A.phi;
   }
+  if (dbox) box_from_device(d, *dbox);
   const int nslot = counts[0];
   const int s = blockIdx.x * 32 + (threadIdx.x >> 3);
   const int sub = threadIdx.x & 7;
@@ -992,9 +1015,9 @@ void Pme::spread(const float4 *xyzq_s, const int *counts, cudaStream_t s,
                  const float4 *origin) {
   const int blocks = (max_slots + 31) / 32;
   switch (m_d.order) {
-    case 4: spread_kernel<4><<<blocks, 128, 0, s>>>(xyzq_s, counts, m_d, qgrid, origin); break;
-    case 6: spread_kernel<6><<<blocks, 128, 0, s>>>(xyzq_s, counts, m_d, qgrid, origin); break;
-    case 8: spread_kernel<8><<<blocks, 128, 0, s>>>(xyzq_s, counts, m_d, qgrid, origin); break;
+    case 4: spread_kernel<4><<<blocks, 128, 0, s>>>(xyzq_s, counts, m_d, qgrid, origin, nullptr, nullptr, m_dbox); break;
+    case 6: spread_kernel<6><<<blocks, 128, 0, s>>>(xyzq_s, counts, m_d, qgrid, origin, nullptr, nullptr, m_dbox); break;
+    case 8: spread_kernel<8><<<blocks, 128, 0, s>>>(xyzq_s, counts, m_d, qgrid, origin, nullptr, nullptr, m_dbox); break;
   }
   APO_LAUNCH_CHECK();
 }
@@ -1015,10 +1038,12 @@ void Pme::convolve(long long *energy, bool calc_energy, bool fp64, cudaStream_t 
   do {                                                                                         \
     if (tma)                                                                                   \
       pencil_kernel<E, FT, V, true><<<grid, kPencilThreads, 0, s>>>(                           \
-          m_d, cgrid, twz, m_prefac, m_prefac_d, energy, virial, nullptr, nullptr, m_tmap, m_err); \
+          m_d, cgrid, twz, m_prefac, m_prefac_d, energy, virial, nullptr, nullptr, m_tmap, m_err, \
+          m_dbox);                                                                             \
     else                                                                                       \
       pencil_kernel<E, FT, V, false><<<grid, kPencilThreads, 0, s>>>(                          \
-          m_d, cgrid, twz, m_prefac, m_prefac_d, energy, virial, nullptr, nullptr, m_tmap, m_err); \
+          m_d, cgrid, twz, m_prefac, m_prefac_d, energy, virial, nullptr, nullptr, m_tmap, m_err, \
+          m_dbox);                                                                             \
   } while (0)
   if (virial) {
     if (fp64) APO_PENCIL(true, double, true);
@@ -1044,9 +1069,9 @@ void Pme::gather(const float4 *xyzq_s, const int *counts, long long *force, int 
                  cudaStream_t s, const float4 *origin) {
   const int blocks = (max_slots + 31) / 32;
   switch (m_d.order) {
-    case 4: gather_kernel<4><<<blocks, 256, 0, s>>>(xyzq_s, counts, m_d, phi, force, stride, origin); break;
-    case 6: gather_kernel<6><<<blocks, 256, 0, s>>>(xyzq_s, counts, m_d, phi, force, stride, origin); break;
-    case 8: gather_kernel<8><<<blocks, 256, 0, s>>>(xyzq_s, counts, m_d, phi, force, stride, origin); break;
+    case 4: gather_kernel<4><<<blocks, 256, 0, s>>>(xyzq_s, counts, m_d, phi, force, stride, origin, nullptr, nullptr, m_dbox); break;
+    case 6: gather_kernel<6><<<blocks, 256, 0, s>>>(xyzq_s, counts, m_d, phi, force, stride, origin, nullptr, nullptr, m_dbox); break;
+    case 8: gather_kernel<8><<<blocks, 256, 0, s>>>(xyzq_s, counts, m_d, phi, force, stride, origin, nullptr, nullptr, m_dbox); break;
   }
   APO_LAUNCH_CHECK();
 }

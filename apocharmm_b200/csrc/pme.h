@@ -118,6 +118,9 @@ class Pme {
   // where the driver offers the encoder); a copy that does not complete sets
   // kErrCopyTimeout in `err`
   void set_tensor_copies(bool on) { m_tma_on = on; }
+  // the kernels read the box from device memory (x, y, z edges; null: the
+  // box of set-up / set_box), for a box that changes every step
+  void set_device_box(const double4 *p) { m_dbox = p; }
   // a new box on the same grid (the influence function is formed from the
   // box at every evaluation)
   void set_box(double Lx, double Ly, double Lz) {
@@ -143,6 +146,7 @@ class Pme {
   CUtensorMap m_tmap{};     // the padded complex grid as floats [nz][ny][2 nxcp]
   bool m_tma = false, m_tma_on = true;
   unsigned *m_err = nullptr;
+  const double4 *m_dbox = nullptr;
   float2 *m_tw = nullptr;   // twiddles: x (nx), y (ny), z (nz) consecutive
   float *m_prefac = nullptr;  // B-spline moduli 1/|b|^2: x, y, z consecutive
   double *m_prefac_d = nullptr;

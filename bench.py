@@ -782,8 +782,8 @@ def main():
         if not args.no_cpu_baseline:
             cb = cpu_baseline(s)
         kps = integ.getKernelsPerStep()
-        if spec["integrator"] == "piston":  # steps launched one by one, box rescale each step
-            launches = args.steps * (11 + SEG * (7 + kps + 2 + 1))
+        if spec["integrator"] == "piston":  # the sorted coordinates refreshed every step
+            launches = args.steps * (12 + SEG * (8 + kps))
         else:
             launches = args.steps * (12 + SEG * (7 + kps))
         line = {
