@@ -300,3 +300,25 @@ def test_langevin_piston_orthorhombic_box_and_pressure(tmp_path):
     assert np.array_equal(runs[0][0], runs[1][0])
     assert np.array_equal(runs[0][1], runs[1][1])
     assert np.array_equal(runs[0][2], runs[1][2])
+
+
+def test_settings_changed_between_calls_take_effect(tmp_path):
+    """Captured segments hold the thermostat's settings as launch arguments:
+    a setter called between propagate calls must reach the next call (the
+    segments are captured again).  Langevin at 50/ps driven from 300 K to
+    a 900 K bath heats the water box; the same run with the graphs of the
+    first call would stay near 300 K."""
+    s, keep = _setup(tmp_path)
+    ctx = keep[3]
+    it = api.CudaLangevinThermostatIntegrator(0.002)
+    it.setThermostatFriction(50.0)
+    it.setReferenceTemperature(300.0)
+    it.setThermostatRngSeed(3)
+    it.setCharmmContext(ctx)
+    it.propagate(40)
+    t300 = ctx.computeTemperature()
+    it.setReferenceTemperature(900.0)
+    it.propagate(400)
+    t900 = ctx.computeTemperature()
+    assert 200.0 < t300 < 450.0
+    assert t900 > 650.0, (t300, t900)
