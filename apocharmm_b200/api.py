@@ -691,11 +691,48 @@ class CudaLangevinPistonIntegrator(CudaIntegrator):
              self._h)
         return v.value
 
-    def getLangevinPistonOnStepPosition(self) -> np.ndarray:
+    def _vector(self, what) -> np.ndarray:
         a, n = np.zeros(3), _sz()
-        call("apo_cuda_langevin_piston_integrator_get_langevin_piston_on_step_position", _ptr(a),
-             _sz(3), ctypes.byref(n), self._h)
+        call(f"apo_cuda_langevin_piston_integrator_get_langevin_piston_{what}", _ptr(a), _sz(3),
+             ctypes.byref(n), self._h)
         return a[:n.value]
+
+    def getLangevinPistonOnStepPosition(self) -> np.ndarray:
+        return self._vector("on_step_position")
+
+    def getLangevinPistonHalfStepPosition(self) -> np.ndarray:
+        return self._vector("half_step_position")
+
+    def getLangevinPistonOnStepVelocity(self) -> np.ndarray:
+        return self._vector("on_step_velocity")
+
+    def getLangevinPistonDeltaPosition(self) -> np.ndarray:
+        return self._vector("delta_position")
+
+    def getLangevinPistonDeltaPressure(self) -> np.ndarray:
+        return self._vector("delta_pressure")
+
+    def getInstantaneousSurfaceTension(self) -> float:
+        v = _d()
+        call("apo_cuda_langevin_piston_integrator_get_instantaneous_surface_tension",
+             ctypes.byref(v), self._h)
+        return v.value
+
+    def getCrystalType(self) -> int:
+        v = _i()
+        call("apo_cuda_langevin_piston_integrator_get_crystal_type", ctypes.byref(v), self._h)
+        return v.value
+
+    def getNoseHooverPistonState(self) -> np.ndarray:
+        """(velocity, velocity one step back, force, force one step back)"""
+        a = np.zeros(4)
+        call("apo_cuda_langevin_piston_integrator_get_nose_hoover_piston_state", _ptr(a), _sz(4),
+             self._h)
+        return a
+
+    def setNoseHooverPistonState(self, velocity, velocity_previous, force, force_previous):
+        call("apo_cuda_langevin_piston_integrator_set_nose_hoover_piston_state", self._h,
+             _d(velocity), _d(velocity_previous), _d(force), _d(force_previous))
 
 
 def rigid_water_fit(xyz: np.ndarray, waters: np.ndarray) -> np.ndarray:

@@ -654,18 +654,91 @@ extern "C" apo_status apo_cuda_langevin_piston_integrator_get_langevin_piston_ma
   }, fn);
 }
 
-extern "C" apo_status apo_cuda_langevin_piston_integrator_get_langevin_piston_on_step_position(
-    double *x, const size_t len, size_t *num, apo_cuda_langevin_piston_integrator *it) {
-  const char *fn = "apo_cuda_langevin_piston_integrator_get_langevin_piston_on_step_position";
+namespace {
+template <typename G>
+apo_status lp_vector(double *x, size_t len, size_t *num, apo_cuda_langevin_piston_integrator *it,
+                     const char *fn, G get) {
   return guard([&]() -> apo_status {
     APO_RETURN_IF(require_ptr(num, fn, "num"));
     APO_RETURN_IF(require_handle(it, fn, "CudaLangevinPistonIntegrator"));
     if (!it->object->getCharmmContext())
       return set_error(APO_STATUS_NOT_INITIALIZED, std::string(fn) + ": no CharmmContext was set");
-    const auto v = it->object->getLangevinPistonOnStepPosition();
+    const std::vector<double> v = get(*it->object);
     *num = v.size();
-    APO_RETURN_IF(require_buffer(x, len, v.size(), fn, "position"));
+    APO_RETURN_IF(require_buffer(x, len, v.size(), fn, "output"));
     std::copy(v.begin(), v.end(), x);
+    return APO_STATUS_OK;
+  }, fn);
+}
+}  // namespace
+
+#define LP_VECTOR(fname, method)                                                              \
+  extern "C" apo_status fname(double *x, const size_t len, size_t *num,                      \
+                              apo_cuda_langevin_piston_integrator *it) {                     \
+    return lp_vector(x, len, num, it, #fname,                                                 \
+                     [](apo::CudaLangevinPistonIntegrator &o) { return o.method(); });       \
+  }
+LP_VECTOR(apo_cuda_langevin_piston_integrator_get_langevin_piston_on_step_position,
+          getLangevinPistonOnStepPosition)
+LP_VECTOR(apo_cuda_langevin_piston_integrator_get_langevin_piston_half_step_position,
+          getLangevinPistonHalfStepPosition)
+LP_VECTOR(apo_cuda_langevin_piston_integrator_get_langevin_piston_on_step_velocity,
+          getLangevinPistonOnStepVelocity)
+LP_VECTOR(apo_cuda_langevin_piston_integrator_get_langevin_piston_delta_position,
+          getLangevinPistonDeltaPosition)
+LP_VECTOR(apo_cuda_langevin_piston_integrator_get_langevin_piston_delta_pressure,
+          getLangevinPistonDeltaPressure)
+#undef LP_VECTOR
+
+extern "C" apo_status apo_cuda_langevin_piston_integrator_get_instantaneous_surface_tension(
+    double *t, apo_cuda_langevin_piston_integrator *it) {
+  const char *fn = "apo_cuda_langevin_piston_integrator_get_instantaneous_surface_tension";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_ptr(t, fn, "tension"));
+    APO_RETURN_IF(require_handle(it, fn, "CudaLangevinPistonIntegrator"));
+    if (!it->object->getCharmmContext())
+      return set_error(APO_STATUS_NOT_INITIALIZED, std::string(fn) + ": no CharmmContext was set");
+    *t = it->object->getInstantaneousSurfaceTension();
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_cuda_langevin_piston_integrator_get_crystal_type(
+    int *c, const apo_cuda_langevin_piston_integrator *it) {
+  const char *fn = "apo_cuda_langevin_piston_integrator_get_crystal_type";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_ptr(c, fn, "crystal_type"));
+    APO_RETURN_IF(require_handle(it, fn, "CudaLangevinPistonIntegrator"));
+    *c = (int)it->object->getCrystalType();
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_cuda_langevin_piston_integrator_get_nose_hoover_piston_state(
+    double *st, const size_t len, apo_cuda_langevin_piston_integrator *it) {
+  const char *fn = "apo_cuda_langevin_piston_integrator_get_nose_hoover_piston_state";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_buffer(st, len, 4, fn, "state"));
+    APO_RETURN_IF(require_handle(it, fn, "CudaLangevinPistonIntegrator"));
+    if (!it->object->getCharmmContext())
+      return set_error(APO_STATUS_NOT_INITIALIZED, std::string(fn) + ": no CharmmContext was set");
+    const auto v = it->object->getNoseHooverPistonState();
+    std::copy(v.begin(), v.end(), st);
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_cuda_langevin_piston_integrator_set_nose_hoover_piston_state(
+    apo_cuda_langevin_piston_integrator *it, const double v, const double v_prev, const double f,
+    const double f_prev) {
+  const char *fn = "apo_cuda_langevin_piston_integrator_set_nose_hoover_piston_state";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_handle(it, fn, "CudaLangevinPistonIntegrator"));
+    if (!std::isfinite(v) || !std::isfinite(v_prev) || !std::isfinite(f) || !std::isfinite(f_prev))
+      return invalid(fn, "values must be finite");
+    if (!it->object->getCharmmContext())
+      return set_error(APO_STATUS_NOT_INITIALIZED, std::string(fn) + ": no CharmmContext was set");
+    it->object->setNoseHooverPistonState(v, v_prev, f, f_prev);
     return APO_STATUS_OK;
   }, fn);
 }

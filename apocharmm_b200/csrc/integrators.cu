@@ -1912,6 +1912,44 @@ std::vector<double> CudaLangevinPistonIntegrator::getLangevinPistonDeltaPosition
   return std::vector<double>(h.lp_delta, h.lp_delta + std::max(m_Dof, 0));
 }
 
+std::vector<double> CudaLangevinPistonIntegrator::getLangevinPistonHalfStepPosition() {
+  const PistonScalars h = read_piston(m_P, stream());
+  return std::vector<double>(h.lp_halfpos, h.lp_halfpos + std::max(m_Dof, 0));
+}
+std::vector<double> CudaLangevinPistonIntegrator::getLangevinPistonOnStepVelocity() {
+  const PistonScalars h = read_piston(m_P, stream());
+  return std::vector<double>(h.lp_onvel, h.lp_onvel + std::max(m_Dof, 0));
+}
+std::vector<double> CudaLangevinPistonIntegrator::getLangevinPistonDeltaPressure() {
+  const PistonScalars h = read_piston(m_P, stream());
+  return std::vector<double>(h.lp_dpress, h.lp_dpress + std::max(m_Dof, 0));
+}
+double CudaLangevinPistonIntegrator::getInstantaneousSurfaceTension() {
+  // 0.5 Lz (Pzz - (Pxx + Pyy) / 2) / factor
+  // (src/CudaLangevinPistonIntegrator.cu:533-541)
+  const PistonScalars h = read_piston(m_P, stream());
+  return 0.5 * h.box[2] * (h.p[8] - 0.5 * (h.p[0] + h.p[4])) / kSurfaceTensionFactor;
+}
+std::vector<double> CudaLangevinPistonIntegrator::getNoseHooverPistonState() {
+  if (!m_S) throw std::runtime_error("CudaLangevinPistonIntegrator: no CharmmContext was set");
+  Scalars h;
+  APO_CUDA(cudaStreamSynchronize(stream()));
+  APO_CUDA(cudaMemcpy(&h, m_S->sc.p, sizeof(h), cudaMemcpyDeviceToHost));
+  return {h.piston_v, h.piston_v_prev, h.piston_f, h.piston_f_prev};
+}
+void CudaLangevinPistonIntegrator::setNoseHooverPistonState(double v, double v_prev, double f,
+                                                            double f_prev) {
+  if (!m_S) throw std::runtime_error("CudaLangevinPistonIntegrator: no CharmmContext was set");
+  Scalars h;
+  APO_CUDA(cudaStreamSynchronize(stream()));
+  APO_CUDA(cudaMemcpy(&h, m_S->sc.p, sizeof(h), cudaMemcpyDeviceToHost));
+  h.piston_v = v;
+  h.piston_v_prev = v_prev;
+  h.piston_f = f;
+  h.piston_f_prev = f_prev;
+  APO_CUDA(cudaMemcpy(m_S->sc.p, &h, sizeof(h), cudaMemcpyHostToDevice));
+}
+
 void CudaLangevinPistonIntegrator::initialize() {
   auto fm = m_Ctx->getForceManager();
   if (fm->isMulti())

@@ -193,6 +193,16 @@ class CudaLangevinPistonIntegrator : public CudaIntegrator {
   // piston positions (box edges, A) and their last displacement
   std::vector<double> getLangevinPistonOnStepPosition();
   std::vector<double> getLangevinPistonDeltaPosition();
+  std::vector<double> getLangevinPistonHalfStepPosition();
+  std::vector<double> getLangevinPistonOnStepVelocity();
+  std::vector<double> getLangevinPistonDeltaPressure();
+  // surface tension of the last step, dyne/cm (getInstantaneousSurfaceTension)
+  double getInstantaneousSurfaceTension();
+  // the thermostat piston: velocity, its value one step back, the velocity
+  // change ("force") and its value one step back
+  // (set/getNoseHooverPiston{Velocity,VelocityPrevious,Force,ForcePrevious})
+  std::vector<double> getNoseHooverPistonState();
+  void setNoseHooverPistonState(double v, double v_prev, double f, double f_prev);
   void propagate(int numSteps) override;
   // the piston part of a restart record (crystal tag, HDOT, box, seed and
   // RNG position), after the base class has restored the atoms and the

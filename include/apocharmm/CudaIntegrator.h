@@ -332,14 +332,66 @@ class CudaLangevinPistonIntegrator : public CudaIntegrator {
     return p;
   }
   std::vector<double> getLangevinPistonOnStepPosition(void) {
-    std::vector<double> x(3);
-    size_t n = 0;
-    apocharmm_detail::check(apo_cuda_langevin_piston_integrator_get_langevin_piston_on_step_position(
-        x.data(), x.size(), &n, m_H));
-    x.resize(n);
-    return x;
+    return vec(apo_cuda_langevin_piston_integrator_get_langevin_piston_on_step_position);
+  }
+  std::vector<double> getLangevinPistonHalfStepPosition(void) {
+    return vec(apo_cuda_langevin_piston_integrator_get_langevin_piston_half_step_position);
+  }
+  std::vector<double> getLangevinPistonOnStepVelocity(void) {
+    return vec(apo_cuda_langevin_piston_integrator_get_langevin_piston_on_step_velocity);
+  }
+  std::vector<double> getLangevinPistonDeltaPosition(void) {
+    return vec(apo_cuda_langevin_piston_integrator_get_langevin_piston_delta_position);
+  }
+  std::vector<double> getLangevinPistonDeltaPressure(void) {
+    return vec(apo_cuda_langevin_piston_integrator_get_langevin_piston_delta_pressure);
+  }
+  double getInstantaneousSurfaceTension(void) {
+    double t = 0.0;
+    apocharmm_detail::check(apo_cuda_langevin_piston_integrator_get_instantaneous_surface_tension(&t, m_H));
+    return t;
+  }
+  CRYSTAL getCrystalType(void) const {
+    int c = 0;
+    apocharmm_detail::check(apo_cuda_langevin_piston_integrator_get_crystal_type(&c, m_H));
+    return (CRYSTAL)c;
+  }
+  // velocity, velocity one step back, force, force one step back
+  std::vector<double> getNoseHooverPistonState(void) {
+    std::vector<double> v(4);
+    apocharmm_detail::check(
+        apo_cuda_langevin_piston_integrator_get_nose_hoover_piston_state(v.data(), v.size(), m_H));
+    return v;
+  }
+  void setNoseHooverPistonVelocity(const double v) {
+    auto s = getNoseHooverPistonState();
+    setState(v, s[1], s[2], s[3]);
+  }
+  void setNoseHooverPistonVelocityPrevious(const double v) {
+    auto s = getNoseHooverPistonState();
+    setState(s[0], v, s[2], s[3]);
+  }
+  void setNoseHooverPistonForce(const double f) {
+    auto s = getNoseHooverPistonState();
+    setState(s[0], s[1], f, s[3]);
+  }
+  void setNoseHooverPistonForcePrevious(const double f) {
+    auto s = getNoseHooverPistonState();
+    setState(s[0], s[1], s[2], f);
   }
 
  private:
+  using VecFn = apo_status (*)(double *, const size_t, size_t *, apo_cuda_langevin_piston_integrator *);
+  std::vector<double> vec(VecFn fn) {
+    std::vector<double> x(3);
+    size_t n = 0;
+    apocharmm_detail::check(fn(x.data(), x.size(), &n, m_H));
+    x.resize(n);
+    return x;
+  }
+  void setState(double v, double vp, double f, double fp) {
+    apocharmm_detail::check(
+        apo_cuda_langevin_piston_integrator_set_nose_hoover_piston_state(m_H, v, vp, f, fp));
+  }
   apo_cuda_langevin_piston_integrator *m_H = nullptr;
 };

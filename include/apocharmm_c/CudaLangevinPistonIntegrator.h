@@ -45,6 +45,16 @@ APOCHARMM_C_API apo_status apo_cuda_langevin_piston_integrator_get_average_press
 /* one value per piston degree of freedom (1 cubic, 2 tetragonal, 3 orthorhombic) */
 APOCHARMM_C_API apo_status apo_cuda_langevin_piston_integrator_get_langevin_piston_mass(double *mass, const size_t len, size_t *num, const apo_cuda_langevin_piston_integrator *integrator);
 APOCHARMM_C_API apo_status apo_cuda_langevin_piston_integrator_get_langevin_piston_on_step_position(double *position, const size_t len, size_t *num, apo_cuda_langevin_piston_integrator *integrator);
+APOCHARMM_C_API apo_status apo_cuda_langevin_piston_integrator_get_langevin_piston_half_step_position(double *position, const size_t len, size_t *num, apo_cuda_langevin_piston_integrator *integrator);
+APOCHARMM_C_API apo_status apo_cuda_langevin_piston_integrator_get_langevin_piston_on_step_velocity(double *velocity, const size_t len, size_t *num, apo_cuda_langevin_piston_integrator *integrator);
+APOCHARMM_C_API apo_status apo_cuda_langevin_piston_integrator_get_langevin_piston_delta_position(double *delta, const size_t len, size_t *num, apo_cuda_langevin_piston_integrator *integrator);
+APOCHARMM_C_API apo_status apo_cuda_langevin_piston_integrator_get_langevin_piston_delta_pressure(double *pressure, const size_t len, size_t *num, apo_cuda_langevin_piston_integrator *integrator);
+APOCHARMM_C_API apo_status apo_cuda_langevin_piston_integrator_get_instantaneous_surface_tension(double *tension, apo_cuda_langevin_piston_integrator *integrator); /* :533 */
+APOCHARMM_C_API apo_status apo_cuda_langevin_piston_integrator_get_crystal_type(int *crystal_type, const apo_cuda_langevin_piston_integrator *integrator); /* :58 */
+/* the thermostat piston: velocity, velocity one step back, velocity change
+ * ("force"), and that one step back (set/getNoseHooverPiston*, :27-31) */
+APOCHARMM_C_API apo_status apo_cuda_langevin_piston_integrator_get_nose_hoover_piston_state(double *state, const size_t len, apo_cuda_langevin_piston_integrator *integrator);
+APOCHARMM_C_API apo_status apo_cuda_langevin_piston_integrator_set_nose_hoover_piston_state(apo_cuda_langevin_piston_integrator *integrator, const double velocity, const double velocity_previous, const double force, const double force_previous);
 #ifdef __cplusplus
 }
 #endif

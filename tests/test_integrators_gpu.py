@@ -285,12 +285,23 @@ def test_langevin_piston_orthorhombic_box_and_pressure(tmp_path):
         assert it.getRngSequencePos() == 90
         assert np.all(np.abs(box - s.box) > 1e-7) and len(set(box.tolist())) == 3
         np.testing.assert_allclose(it.getLangevinPistonOnStepPosition(), box, rtol=0, atol=1e-12)
+        # half-step edge = on-step edge - half the last displacement
+        np.testing.assert_allclose(it.getLangevinPistonHalfStepPosition(),
+                                   box - 0.5 * it.getLangevinPistonDeltaPosition(), rtol=0, atol=1e-12)
+        assert len(it.getLangevinPistonOnStepVelocity()) == 3
+        assert len(it.getLangevinPistonDeltaPressure()) == 3
+        assert it.getCrystalType() == it.ORTHORHOMBIC
+        assert np.isfinite(it.getInstantaneousSurfaceTension())
+        nh = it.getNoseHooverPistonState()
+        assert np.isfinite(nh).all() and nh[0] != 0.0
         d1, d2, d3 = _water_geometry(x)
         assert np.abs(d1 - 0.9572).max() < 1e-6 and np.abs(d3 - np.sqrt(2.29189321)).max() < 1e-6
         p = it.getInstantaneousPressureTensor()
         assert np.isfinite(p).all() and np.isfinite(it.getAveragePressureScalar())
         assert os.path.getsize(tmp_path / f"r{rep}.dcd") > 0
         if rep == 1:
+            it.setNoseHooverPistonState(*nh)   # a round trip leaves the state as it was
+            np.testing.assert_array_equal(it.getNoseHooverPistonState(), nh)
             rst = api.RestartSubscriber(str(tmp_path / "p.rst"), 5)
             it.subscribe(rst)
             it.propagate(5)
