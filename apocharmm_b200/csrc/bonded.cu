@@ -188,11 +188,16 @@ __global__ void __launch_bounds__(kThreads) bonded_kernel(BondedArgs a) {
   }
   const int b1 = a.nbond, b2 = b1 + a.nub, b3 = b2 + a.nangle, b4 = b3 + a.ndihe,
             b5 = b4 + a.nimp, b6 = b5 + a.nin14, b7 = b6 + a.nex14;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < b7; t += gridDim.x * blockDim.x) {
+  // the loop runs in whole warps (t0 is the same in every lane), so the
+  // virial can be summed across the warp before it reaches shared memory
+  for (int t0 = blockIdx.x * blockDim.x; t0 < b7; t0 += gridDim.x * blockDim.x) {
+    const int t = t0 + threadIdx.x;
     float e = 0.f, e2 = 0.f;
     float w[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     int slot = -1, slot2 = -1;
-    if (t < b1) {
+    if (t >= b7) {
+      // past the last term: contributes nothing
+    } else if (t < b1) {
       e = bond_term<VIRIAL>(a, a.bond_ij[t].x, a.bond_ij[t].y, a.bond_p[t], w);
       slot = kEBond;
     } else if (t < b2) {
@@ -225,7 +230,7 @@ __global__ void __launch_bounds__(kThreads) bonded_kernel(BondedArgs a) {
       slot = kEEwex;
     }
     if (MULTI) {
-      if (ENERGY) {  // straight to this term's system
+      if (ENERGY && t < b7) {  // straight to this term's system
         int first;
         if (t < b1) first = a.bond_ij[t].x;
         else if (t < b2) first = a.ub_ij[t - b1].x;
@@ -245,15 +250,20 @@ __global__ void __launch_bounds__(kThreads) bonded_kernel(BondedArgs a) {
       }
       continue;
     }
-    if (ENERGY) {
+    if (ENERGY && slot >= 0) {
       atomicAdd(&sh_e[slot], (unsigned long long)__double2ll_rn((double)e * kEnergyScale));
       if (slot2 >= 0)
         atomicAdd(&sh_e[slot2], (unsigned long long)__double2ll_rn((double)e2 * kEnergyScale));
     }
     if (VIRIAL) {
+      // fixed-point sums: the same integers in any order
 #pragma unroll
-      for (int k = 0; k < 9; ++k)
-        atomicAdd(&sh_v[k], (unsigned long long)__double2ll_rn((double)w[k] * kEnergyScale));
+      for (int k = 0; k < 9; ++k) {
+        long long v = __double2ll_rn((double)w[k] * kEnergyScale);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0 && v) atomicAdd(&sh_v[k], (unsigned long long)v);
+      }
     }
   }
   if (ENERGY && !MULTI) {
