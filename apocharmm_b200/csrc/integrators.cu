@@ -1807,6 +1807,7 @@ void CudaLangevinPistonIntegrator::setCrystalType(Crystal c) {
   m_PMass.assign(m_Dof, tm);
   m_PGamma = 0.0;
   m_RngDirty = true;
+  clearGraphs();  // the captured steps hold the crystal type and the piston constants
 }
 
 void CudaLangevinPistonIntegrator::setPressure(const std::vector<double> &p) {
@@ -1830,6 +1831,7 @@ void CudaLangevinPistonIntegrator::setLangevinPistonMass(const std::vector<doubl
                                 "input vector must be equal to the degrees of freedom of the "
                                 "Langevin piston (" + std::to_string(m_Dof) + ")");
   m_PMass = m;
+  clearGraphs();
 }
 
 void CudaLangevinPistonIntegrator::setNoseHooverPistonMass(double m) {
@@ -1867,6 +1869,7 @@ void CudaLangevinPistonIntegrator::setMaxPredictorCorrectorIterations(int n) {
     throw std::invalid_argument("setMaxPredictorCorrectorIterations: at least one pass is needed");
   m_MaxPC = n;
   m_KernelsPerStep = 3 + m_MaxPC;
+  clearGraphs();
 }
 
 void CudaLangevinPistonIntegrator::resetAverages() {
