@@ -177,3 +177,56 @@ def test_static_reciprocal_argument_checks_without_gpu():
     msg = _lib.lib().apo_last_error()
     msg = msg.decode() if isinstance(msg, bytes) else str(msg)
     assert "order" in msg
+
+
+def test_langevin_piston_handle_without_gpu():
+    """The Langevin piston's settings and their checks need no device: the
+    crystal type sets the piston's degrees of freedom, masses follow it,
+    out-of-range arguments and calls that need a context are refused with
+    a status and a message (include/CudaLangevinPistonIntegrator.h,
+    src/CudaLangevinPistonIntegrator.cu:166-283)."""
+    import ctypes
+    from apocharmm_b200._lib import lib
+    L = lib()
+    L.apo_last_error.restype = ctypes.c_char_p
+    h = ctypes.c_void_p()
+    assert L.apo_cuda_langevin_piston_integrator_create(ctypes.byref(h), ctypes.c_double(-1.0)) == 1
+    assert L.apo_cuda_langevin_piston_integrator_create(ctypes.byref(h), ctypes.c_double(0.002)) == 0
+    m3 = (ctypes.c_double * 3)(1000.0, 2000.0, 3000.0)
+    n = ctypes.c_size_t()
+    # masses before the crystal type: refused, as in the reference
+    assert L.apo_cuda_langevin_piston_integrator_set_langevin_piston_mass(h, m3, ctypes.c_size_t(3)) == 2
+    assert b"CrystalType" in L.apo_last_error()
+    assert L.apo_cuda_langevin_piston_integrator_set_crystal_type(h, 5) == 1
+    assert L.apo_cuda_langevin_piston_integrator_set_crystal_type(h, 2) == 0   # orthorhombic
+    c = ctypes.c_int()
+    assert L.apo_cuda_langevin_piston_integrator_get_crystal_type(ctypes.byref(c), h) == 0 and c.value == 2
+    out = (ctypes.c_double * 3)()
+    assert L.apo_cuda_langevin_piston_integrator_get_langevin_piston_mass(out, ctypes.c_size_t(3),
+                                                                           ctypes.byref(n), h) == 0
+    assert n.value == 3
+    assert L.apo_cuda_langevin_piston_integrator_set_langevin_piston_mass(h, m3, ctypes.c_size_t(2)) == 2
+    assert L.apo_cuda_langevin_piston_integrator_set_langevin_piston_mass(h, m3, ctypes.c_size_t(3)) == 0
+    assert L.apo_cuda_langevin_piston_integrator_get_langevin_piston_mass(out, ctypes.c_size_t(3),
+                                                                           ctypes.byref(n), h) == 0
+    assert list(out) == [1000.0, 2000.0, 3000.0]
+    p9 = (ctypes.c_double * 9)(*([1.0, 0, 0, 0, 1.0, 0, 0, 0, 1.0]))
+    assert L.apo_cuda_langevin_piston_integrator_set_pressure(h, p9, ctypes.c_size_t(8)) == 2
+    assert L.apo_cuda_langevin_piston_integrator_set_pressure(h, p9, ctypes.c_size_t(9)) == 0
+    assert L.apo_cuda_langevin_piston_integrator_set_langevin_piston_friction(h, ctypes.c_double(-1.0)) == 1
+    assert L.apo_cuda_langevin_piston_integrator_set_max_predictor_corrector_iterations(h, 0) == 2
+    pos = ctypes.c_ulonglong(99)
+    assert L.apo_cuda_langevin_piston_integrator_set_rng_sequence_pos(h, ctypes.c_ulonglong(17)) == 0
+    assert L.apo_cuda_langevin_piston_integrator_get_rng_sequence_pos(ctypes.byref(pos), h) == 0
+    assert pos.value == 17
+    # no context yet: the pressure and piston state are not there
+    p_out = (ctypes.c_double * 9)()
+    assert L.apo_cuda_langevin_piston_integrator_get_instantaneous_pressure_tensor(
+        p_out, ctypes.c_size_t(9), h) == 4
+    assert L.apo_cuda_langevin_piston_integrator_get_nose_hoover_piston_state(
+        p_out, ctypes.c_size_t(4), h) == 4
+    base = ctypes.c_void_p()
+    assert L.apo_cuda_langevin_piston_integrator_as_cuda_integrator(ctypes.byref(base), h) == 0
+    assert base.value
+    assert L.apo_cuda_integrator_propagate(base, 10) != 0
+    L.apo_cuda_langevin_piston_integrator_destroy(h)
