@@ -451,10 +451,13 @@ def read_restart_file(path) -> dict:
     n = natom.value
     xold, vel, delta = (np.zeros((max(n, 1), 3)) for _ in range(3))
     call("apo_restart_file_read", _enc(path), _i(n), _ptr(xold), _ptr(vel), _ptr(delta))
+    crystal = ctypes.create_string_buffer(5)
+    hdot = np.zeros(3)
+    call("apo_restart_file_read_crystal", _enc(path), crystal, _ptr(hdot))
     return {"natom": n, "npriv": npriv.value, "ndegf": ndegf.value, "seed": seed.value,
             "rngpos": rngpos.value if has_rng.value else None, "box": box,
-            "pnhv": pnhv.value, "pnhf": pnhf.value,
-            "xold": xold[:n], "vel": vel[:n], "delta": delta[:n]}
+            "pnhv": pnhv.value, "pnhf": pnhf.value, "crystal": crystal.value.decode(),
+            "hdot": hdot, "xold": xold[:n], "vel": vel[:n], "delta": delta[:n]}
 
 
 def write_restart_file(path, xold, vel, delta, box, npriv: int = 0, ndegf: int = 0,

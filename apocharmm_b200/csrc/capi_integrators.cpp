@@ -8,6 +8,7 @@
 #include "apocharmm_c/RestartSubscriber.h"
 #include "apocharmm_c/Subscriber.h"
 #include <algorithm>
+#include <cstdio>
 
 #include "capi_internal.h"
 #include "integrators.h"
@@ -421,6 +422,18 @@ extern "C" apo_status apo_restart_file_read_header(const char *path, int *natom,
     for (int d = 0; d < 3; ++d) box3[d] = r.box[d];
     *pnhv = r.pnhv;
     *pnhf = r.pnhf;
+    return APO_STATUS_OK;
+  }, fn);
+}
+
+extern "C" apo_status apo_restart_file_read_crystal(const char *path, char *crystal5, double *hdot3) {
+  const char *fn = "apo_restart_file_read_crystal";
+  return guard([&]() -> apo_status {
+    APO_RETURN_IF(require_string(path, fn, "path"));
+    if (!crystal5 || !hdot3) return invalid(fn, "null output pointer");
+    const apo::RestartRecord r = apo::readRestartFile(path);
+    std::snprintf(crystal5, 5, "%s", r.crystal.c_str());
+    for (int d = 0; d < 3; ++d) hdot3[d] = r.hdot[d];
     return APO_STATUS_OK;
   }, fn);
 }

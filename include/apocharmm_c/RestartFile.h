@@ -18,6 +18,10 @@ APOCHARMM_C_API apo_status apo_restart_file_read_header(const char *path, int *n
                                                         int *ndegf, unsigned long long *seed,
                                                         unsigned long long *rngpos, int *has_rng,
                                                         double *box3, double *pnhv, double *pnhf);
+/* the crystal tag of the header ("CUBI", "TETR", "ORTH"; 5 chars with the
+ * terminating zero) and the Langevin piston displacement HDOT (3 values),
+ * as src/CudaLangevinPistonIntegrator.cu:706-830 reads them */
+APOCHARMM_C_API apo_status apo_restart_file_read_crystal(const char *path, char *crystal5, double *hdot3);
 /* per-atom sections, natom x 3 each: XOLD (coordinates), VX (velocities),
  * X (position-Verlet delta); natom must match the file */
 APOCHARMM_C_API apo_status apo_restart_file_read(const char *path, const int natom, double *xold,

@@ -55,6 +55,7 @@ def test_layout_follows_the_reference(tmp_path):
                            seed=42, rngpos=400)
     lines = p.read_text().split("\n")
     assert lines[0].startswith("REST    50     1  ORTH")
+    assert api.read_restart_file(p)["crystal"] == "ORTH"
     assert lines[0][30:33] == "APO"
     assert lines[2] == "       2 !NTITLE followed by title"
     cry = lines.index(" !CRYSTAL PARAMETERS")
@@ -88,10 +89,10 @@ def test_reads_the_reference_sixteen_digit_form(tmp_path):
     def tri(a):
         return "".join(f(v) for v in a) + "\n"
 
-    head = ("REST    50     1  CUBI          APO\n\n       2 !NTITLE followed by title\n"
+    head = ("REST    50     1  TETR          APO\n\n       2 !NTITLE followed by title\n"
             "* APOCHARMM RESTART FILE\n* USED FOR CONTINUING MOLECULAR DYNAMICS TRAJECTORY\n\n"
             " !CRYSTAL PARAMETERS\n")
-    body = tri([40.0, 0.0, 40.0]) + tri([0.0, 0.0, 40.0]) + tri([0, 0, 0]) + tri([0, 0, 0])
+    body = tri([40.0, 0.0, 40.0]) + tri([0.0, 0.0, 40.0]) + tri([1.5e-4, -2.25e-4, 0]) + tri([0, 0, 0])
     body += tri([0.0, 0.25, -0.5]) + tri([0, 0, 0]) * 8 + tri([0, 0, 0]) + f(0.0) + "\n\n"
     body += " !NATOM,NPRIV,NSTEP,NSAVC,NSAVV,JHSTRT,NDEGF,SEED,NSAVL\n"
     body += "".join(str(v).rjust(12) for v in (n, 2000, 2000, 1000, 0, 0, 9)) + "7".rjust(22)
@@ -107,6 +108,9 @@ def test_reads_the_reference_sixteen_digit_form(tmp_path):
     assert r["natom"] == n and r["npriv"] == 2000 and r["ndegf"] == 9
     assert r["seed"] == 7 and r["rngpos"] == 8000
     assert r["pnhv"] == 0.25 and r["pnhf"] == -0.5
+    # the Langevin piston's part (src/CudaLangevinPistonIntegrator.cu:706-830)
+    assert r["crystal"] == "TETR"
+    np.testing.assert_array_equal(r["hdot"], [1.5e-4, -2.25e-4, 0.0])
     for key, arr in (("xold", xold), ("vel", vel), ("delta", delta)):
         want = np.array([[float(f(v).replace("D", "e")) for v in row] for row in arr])
         np.testing.assert_array_equal(r[key], want)

@@ -192,6 +192,7 @@ def test_piston_resumed_run_matches_uninterrupted_run(tmp_path):
     head = api.read_restart_file(saved)
     assert head["npriv"] == 40 and it2.getCurrentPropagatedStep() == 40
     assert not np.array_equal(head["box"], s.box)
+    assert head["crystal"] == "ORTH" and np.all(head["hdot"] != 0.0)
     it2.propagate(60)
     x2, v2, b2 = keep2[3].getCoordinates(), keep2[3].getVelocities(), keep2[2].getBoxDimensions()
     assert np.array_equal(b1, b2), b1 - b2
