@@ -317,7 +317,7 @@ def test_settings_changed_between_calls_take_effect(tmp_path):
     """Captured segments hold the thermostat's settings as launch arguments:
     a setter called between propagate calls must reach the next call (the
     segments are captured again).  Langevin at 50/ps driven from 300 K to
-    a 900 K bath heats the water box; the same run with the graphs of the
+    a 600 K bath heats the water box; the same run with the graphs of the
     first call would stay near 300 K."""
     s, keep = _setup(tmp_path)
     ctx = keep[3]
@@ -328,8 +328,8 @@ def test_settings_changed_between_calls_take_effect(tmp_path):
     it.setCharmmContext(ctx)
     it.propagate(40)
     t300 = ctx.computeTemperature()
-    it.setReferenceTemperature(900.0)
-    it.propagate(400)
-    t900 = ctx.computeTemperature()
+    it.setReferenceTemperature(600.0)
+    it.propagate(300)
+    t600 = ctx.computeTemperature()
     assert 200.0 < t300 < 450.0
-    assert t900 > 650.0, (t300, t900)
+    assert t600 > 480.0, (t300, t600)
