@@ -217,8 +217,7 @@ void ForceManager::setBoxDimensions(const std::array<double, 3> &box) {
   m_Initialized = false;
 }
 
-void ForceManager::updateBoxDimensions(const std::array<double, 3> &box, bool keep_list,
-                                       cudaStream_t s) {
+void ForceManager::updateBoxDimensions(const std::array<double, 3> &box) {
   if (!m_Initialized) throw std::runtime_error("ForceManager is not initialized");
   if (m_Multi)
     throw std::invalid_argument("updateBoxDimensions: a multi-system force manager keeps its boxes");
@@ -234,12 +233,8 @@ void ForceManager::updateBoxDimensions(const std::array<double, 3> &box, bool ke
   m_Box = box;
   m_HostSetup = make_nb_setup(m_Box[0], m_Box[1], m_Box[2], m_Kappa, m_Ctofnb, m_Ctonnb);
   APO_CUDA(cudaMemcpy(m_Setup.p, &m_HostSetup, sizeof(NbSetup), cudaMemcpyHostToDevice));
-  if (keep_list && m_ListBuilt && !m_ListDirty) {
-    m_Nbl.rescale_box(0, m_Box[0], m_Box[1], m_Box[2], s);
-  } else {
-    m_Nbl.set_box(0, m_Box[0], m_Box[1], m_Box[2]);
-    m_ListDirty = true;
-  }
+  m_Nbl.set_box(0, m_Box[0], m_Box[1], m_Box[2]);
+  m_ListDirty = true;
   m_Pme.set_box(m_Box[0], m_Box[1], m_Box[2]);
   if (m_DevBox.p) {
     const double4 b = make_double4(m_Box[0], m_Box[1], m_Box[2], 0.0);

@@ -108,10 +108,7 @@ class ForceManager {
   // without a new initialisation; the list is rebuilt at the next
   // evaluation and graphs captured with the old box are dropped.  The
   // caller has synchronised the context's stream.
-  // keep_list: the built list follows the box (its periodic shifts are
-  // rescaled on stream s) instead of being rebuilt at the next evaluation
-  void updateBoxDimensions(const std::array<double, 3> &box, bool keep_list = false,
-                           cudaStream_t s = nullptr);
+  void updateBoxDimensions(const std::array<double, 3> &box);
   // device-resident box (one system): PME and image centering read the box
   // from deviceBox(), so kernels that change the box on the device (the
   // Langevin piston) need no host round trip; they write deviceBox(), the

@@ -252,21 +252,6 @@ __global__ void origin_kernel(const float4 *__restrict__ xyzq, const int *__rest
 
 // a new box for the built list: slot_off = k L - origin becomes k L' - origin
 // (k recovered from the old box; the origins stay)
-__global__ void rescale_kernel(double4 *__restrict__ slot_off, const float4 *__restrict__ cl_origin,
-                               const int *__restrict__ cl_sys, int sys, double3 L0, double3 L1,
-                               const int *__restrict__ counts) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= counts[0] || cl_sys[s / kTile] != sys) return;
-  const float4 o = cl_origin[s / kTile];
-  double4 v = slot_off[s];
-  const double kx = rint((v.x + (double)o.x) / L0.x), ky = rint((v.y + (double)o.y) / L0.y),
-               kz = rint((v.z + (double)o.z) / L0.z);
-  v.x = kx * L1.x - (double)o.x;
-  v.y = ky * L1.y - (double)o.y;
-  v.z = kz * L1.z - (double)o.z;
-  slot_off[s] = v;
-}
-
 __global__ void rescale_dev_kernel(double4 *__restrict__ slot_off,
                                    const float4 *__restrict__ cl_origin,
                                    const double *__restrict__ L0, const double *__restrict__ L1,
@@ -746,16 +731,6 @@ void NeighborList::set_box(int sys, double Lx, double Ly, double Lz) {
   d.Lyd = Ly;
   d.Lzd = Lz;
   APO_CUDA(cudaMemcpy(m_sys + sys, &d, sizeof(NbSysDims), cudaMemcpyHostToDevice));
-}
-
-void NeighborList::rescale_box(int sys, double Lx, double Ly, double Lz, cudaStream_t s) {
-  if (sys < 0 || sys >= (int)m_sys_h.size()) throw std::invalid_argument("NeighborList: no such system");
-  const NbSysDims d = m_sys_h[sys];
-  set_box(sys, Lx, Ly, Lz);
-  rescale_kernel<<<(m_d.slot_cap + 255) / 256, 256, 0, s>>>(
-      slot_off, cl_origin, cl_sys, sys, make_double3(d.Lxd, d.Lyd, d.Lzd), make_double3(Lx, Ly, Lz),
-      counts);
-  APO_LAUNCH_CHECK();
 }
 
 void NeighborList::rescale_box_device(const double *old_box, const double *new_box,

@@ -93,12 +93,11 @@ class NeighborList {
   // every step under pressure control); the next build uses it.  The
   // caller has synchronised the stream the list's kernels run on.
   void set_box(int sys, double Lx, double Ly, double Lz);
-  // the same, keeping the built list: every slot's periodic shift k L moves
-  // with the box (k kept), so the list stays valid between builds while the
-  // box changes a little every step
-  void rescale_box(int sys, double Lx, double Ly, double Lz, cudaStream_t s);
-  // the same with the old and new edges in device memory (3 doubles each;
-  // nothing happens once `err` is set); the device dims are left alone
+  // keep the built list under a new box: every slot's periodic shift k L
+  // moves with the box (k kept), so the list stays valid between builds
+  // while the box changes a little every step; the old and new edges are
+  // in device memory (3 doubles each; nothing happens once `err` is set)
+  // and the device dims are left alone
   void rescale_box_device(const double *old_box, const double *new_box, const unsigned *err,
                           cudaStream_t s);
   // the host copy of a box the device dims already hold
