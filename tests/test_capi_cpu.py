@@ -230,3 +230,18 @@ def test_langevin_piston_handle_without_gpu():
     assert base.value
     assert L.apo_cuda_integrator_propagate(base, 10) != 0
     L.apo_cuda_langevin_piston_integrator_destroy(h)
+
+
+def test_box_getter_without_gpu(tmp_path):
+    """apo_force_manager_get_box_dimensions gives back the box in force (the
+    one set, before any device work)."""
+    s = water_box(64, 14.0, seed=3)
+    paths = write_charmm_files(s, str(tmp_path))
+    fm = api.ForceManager(api.CharmmPsf(paths["psf"]), api.CharmmParameters(paths["prm"]))
+    fm.setBoxDimensions([14.0, 15.0, 16.5])
+    np.testing.assert_array_equal(fm.getBoxDimensions(), [14.0, 15.0, 16.5])
+    import ctypes
+    from apocharmm_b200._lib import lib
+    L = lib()
+    out = (ctypes.c_double * 2)()
+    assert L.apo_force_manager_get_box_dimensions(out, ctypes.c_size_t(2), fm.handle) == 1
